@@ -1,0 +1,216 @@
+"""Resolved parameter block of the hot path (mirror of ``AtjupParams`` in include/atjup_gpu.h).
+
+The reference reads ~200 ``ATJUP_*`` environment knobs into function-local statics at first use
+(e.g. planet/cJupiterModel.h:725-943, planet/RHS_Jup_Turb.cpp:103-117, planet/PressureSolver.h:
+168-205). The GPU layer never reads the environment: ``resolve_params`` reads the same variables
+with the reference's defaults once, on the host, and hands the device a fixed block, so both arms
+of a comparison see identical knobs. Knob values the kernels do not implement are rejected by
+``check_supported`` with the knob's name.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from typing import Mapping
+
+ABI_VERSION = 1
+
+# field ids (include/atjup_gpu.h)
+F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, \
+    F_AUX_U, F_AUX_V, F_AUX_W, F_P_BARO, F_Q_RAD, F_Q_PRECIP = range(16)
+FIELD_IDS = {
+    "t": F_T, "u": F_U, "v": F_V, "w": F_W, "p_dyn": F_P_DYN, "p_hydro": F_P_HYDRO,
+    "p_stat": F_P_STAT, "rho_mix": F_RHO_MIX, "wall_nue": F_WALL_NUE, "nue": F_NUE,
+    "aux_u": F_AUX_U, "aux_v": F_AUX_V, "aux_w": F_AUX_W, "p_baro": F_P_BARO,
+    "Q_rad": F_Q_RAD, "Q_precip": F_Q_PRECIP,
+}
+
+SOLVE_SWEEPS, SOLVE_RESIDUAL = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+BC_RADIUS, BC_THETA, BC_PHI, BC_SOLID, BC_ALL = 1, 2, 4, 8, 15
+
+_FIELDS = [
+    ("abi_version", ctypes.c_int32), ("im", ctypes.c_int32), ("jm", ctypes.c_int32),
+    ("km", ctypes.c_int32),
+    ("dr", ctypes.c_double), ("dthe", ctypes.c_double), ("dphi", ctypes.c_double),
+    ("dt", ctypes.c_double),
+    ("re", ctypes.c_double), ("pr", ctypes.c_double), ("g", ctypes.c_double),
+    ("omega", ctypes.c_double), ("u_0", ctypes.c_double), ("t_ref", ctypes.c_double),
+    ("L_atm", ctypes.c_double),
+    ("r_mix", ctypes.c_double), ("R_mix", ctypes.c_double), ("cp_mix", ctypes.c_double),
+    ("Coriolis", ctypes.c_double), ("centrifugal", ctypes.c_double), ("buoyancy", ctypes.c_double),
+    ("sinthe_min", ctypes.c_double), ("p_dyn_to_bar", ctypes.c_double),
+    ("t_diff_scale", ctypes.c_double),
+    ("nd_cor", ctypes.c_double), ("nd_cent", ctypes.c_double), ("nd_buoy", ctypes.c_double),
+    ("buoy_scale", ctypes.c_double), ("buoy_ramp", ctypes.c_double),
+    ("pgrad_scale", ctypes.c_double), ("rad_coupling", ctypes.c_double),
+    ("precip_coupling", ctypes.c_double), ("turb_coupling", ctypes.c_double),
+    ("pgrad_wall", ctypes.c_int32), ("pgrad_wrap", ctypes.c_int32),
+    ("adiabatic", ctypes.c_int32), ("adiabatic_rho", ctypes.c_int32),
+    ("metric_split", ctypes.c_int32), ("coriolis_split", ctypes.c_int32),
+    ("hydro_split", ctypes.c_int32), ("cell_hold", ctypes.c_int32),
+    ("precip_rho_local", ctypes.c_int32), ("local_rho", ctypes.c_int32),
+    ("rho_pdyn", ctypes.c_int32), ("has_nue", ctypes.c_int32), ("has_heating", ctypes.c_int32),
+    ("p_dyn_cap", ctypes.c_double), ("press_wall", ctypes.c_int32),
+    ("rigid_lid", ctypes.c_int32), ("press_sweeps", ctypes.c_int32),
+    ("top_taper", ctypes.c_int32), ("lid_u", ctypes.c_int32), ("pole_fill_rows", ctypes.c_int32),
+    ("mount_t_ambient", ctypes.c_int32),
+    ("shapiro_inloop", ctypes.c_int32), ("shapiro_strength", ctypes.c_double),
+    ("v_massbal_stride", ctypes.c_int32), ("v_massbal_zonal", ctypes.c_int32),
+    ("precision", ctypes.c_int32),
+]
+
+
+class AtjupParams(ctypes.Structure):
+    _fields_ = _FIELDS
+
+
+class AtjupSolveOpts(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("sweeps", ctypes.c_int32),
+                ("max_iter", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("rel_tol", ctypes.c_double), ("omega", ctypes.c_double),
+                ("external_rhs", ctypes.c_int32)]
+
+
+class AtjupSolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("inner_solves", ctypes.c_int32),
+                ("rel_residual", ctypes.c_double), ("b_norm", ctypes.c_double)]
+
+
+# Mixture constants the reference derives at start-up from its default composition
+# (ChemistryJup::ThermalPropertiesJup with ATJUP_COMPOSITION=1, ChemistryJup.h:545-650).
+DEFAULT_MIXTURE = {"r_mix": 1.2843999999999998, "R_mix": 3531.1847352206946,
+                   "cp_mix": 11810.757033551794}
+
+
+def _env(env: Mapping[str, str], name: str, default, cast=int):
+    v = env.get(name)
+    if v is None:
+        return default
+    try:
+        return cast(v)
+    except ValueError:
+        # atoi / atof of a non-numeric string is 0 in the reference
+        return cast(0)
+
+
+def resolve_params(env: Mapping[str, str] | None = None, *, im=41, jm=181, km=361,
+                   constants: Mapping[str, float] | None = None, iter_n: int = 0,
+                   has_nue: bool = False, has_heating: bool = False) -> AtjupParams:
+    """Resolve every knob that selects a hot-path branch, with the reference's defaults.
+
+    ``constants`` overrides the model constants (re, pr, g, omega, u_0, t_ref, L_atm, r_mix,
+    R_mix, cp_mix, Coriolis, centrifugal, buoyancy, dt) -- a driver passes its member values.
+    """
+    env = os.environ if env is None else env
+    c = {"re": 1000.0, "pr": 0.69, "g": 25.92, "omega": 0.000176, "u_0": 100.0, "t_ref": 165.0,
+         "L_atm": 140.0, "Coriolis": 1.0, "centrifugal": 1.0, "buoyancy": 1.0}
+    c.update(DEFAULT_MIXTURE)
+    c["dt"] = _env(env, "ATJUP_DT", 0.005, float)                     # cJupiterModel.cpp:106
+    if constants:
+        c.update(constants)
+    p = AtjupParams()
+    p.abi_version = ABI_VERSION
+    p.im, p.jm, p.km = im, jm, km
+    p.dr = 0.025                                                       # cJupiterModel.cpp:172
+    p.dthe = 1.0 / (180.0 / math.pi)                                   # cJupiterModel.cpp:173
+    p.dphi = 1.0 / (180.0 / math.pi)
+    for k in ("dt", "re", "pr", "g", "omega", "u_0", "t_ref", "L_atm", "r_mix", "R_mix",
+              "cp_mix", "Coriolis", "centrifugal", "buoyancy"):
+        setattr(p, k, float(c[k]))
+
+    geo_balance = _env(env, "ATJUP_GEO_BALANCE", 1) != 0               # cJupiterModel.h:857
+    smin = _env(env, "ATJUP_SINTHE_MIN", 0.55, float)                  # cJupiterModel.h:1121
+    p.sinthe_min = smin if 0.0 < smin < 1.0 else 0.55
+    pdyn_units = _env(env, "ATJUP_PDYN_UNITS", 1) != 0                 # cJupiterModel.h:1156
+    p.p_dyn_to_bar = p.r_mix * p.u_0 * p.u_0 * 1.0e-5 if pdyn_units else 1.0
+    p.t_diff_scale = _env(env, "ATJUP_T_DIFF_SCALE", 0.01, float)      # cJupiterModel.h:268
+
+    # body-force scales, RHS_Jup_Turb.cpp:323-346
+    nd_all = _env(env, "ATJUP_NONDIM", 0)
+    nd_cor_on = _env(env, "ATJUP_ND_COR", 1 if geo_balance else -1)
+    nd_cent_on = _env(env, "ATJUP_ND_CENT", -1)
+    nd_buoy_on = _env(env, "ATJUP_ND_BUOY", -1)
+    L_m = p.L_atm * 1.0e3
+    p.nd_cor = L_m / p.u_0 if (nd_cor_on if nd_cor_on >= 0 else nd_all) != 0 else 1.0
+    p.nd_cent = L_m * L_m / (p.u_0 * p.u_0) if (nd_cent_on if nd_cent_on >= 0 else nd_all) != 0 else 1.0
+    p.nd_buoy = 1.0e5 * L_m / (p.u_0 * p.u_0) if (nd_buoy_on if nd_buoy_on >= 0 else nd_all) != 0 else 1.0
+    p.buoy_scale = _env(env, "ATJUP_BUOY_SCALE", 1.0, float)
+    ramp_iters = _env(env, "ATJUP_BUOY_RAMP_ITERS", 0)
+    p.buoy_ramp = min(1.0, float(iter_n) / float(ramp_iters)) if ramp_iters > 0 else 1.0
+    p.pgrad_scale = _env(env, "ATJUP_PGRAD_SCALE", 1.0, float)
+    p.rad_coupling = _env(env, "ATJUP_RAD_COUPLING", 1.0, float)
+    p.precip_coupling = _env(env, "ATJUP_PRECIP_COUPLING", 1.0, float)
+    p.turb_coupling = _env(env, "ATJUP_TURB_COUPLING", 1.0, float)
+    p.pgrad_wall = int(_env(env, "ATJUP_PGRAD_WALL", 1) != 0)
+    p.pgrad_wrap = int(_env(env, "ATJUP_PGRAD_WRAP", 1) != 0)
+    p.adiabatic = int(_env(env, "ATJUP_ADIABATIC", 1) != 0)
+    p.adiabatic_rho = int(_env(env, "ATJUP_ADIABATIC_RHO", 1) != 0)
+    p.metric_split = int(_env(env, "ATJUP_METRIC_SPLIT", 1) != 0)
+    p.coriolis_split = int(_env(env, "ATJUP_CORIOLIS_SPLIT", 1) != 0 and p.metric_split)
+    hs = env.get("ATJUP_HYDRO_SPLIT")
+    p.hydro_split = int((int(hs) if hs is not None else nd_all) != 0)
+    p.cell_hold = int(_env(env, "ATJUP_CELL_HOLD", 1 if geo_balance else 0) != 0)
+    p.precip_rho_local = int(_env(env, "ATJUP_PRECIP_RHO_LOCAL", 1) != 0)
+    p.local_rho = int(_env(env, "ATJUP_LOCAL_RHO", 1) != 0)
+    p.rho_pdyn = int(_env(env, "ATJUP_RHO_PDYN", 0 if geo_balance else 1) != 0)
+    p.has_nue = int(bool(has_nue))
+    p.has_heating = int(bool(has_heating))
+
+    # pressure solver, PressureSolver.h:168-205
+    p.p_dyn_cap = _env(env, "ATJUP_PDYN_CAP", 0.2, float)
+    p.press_wall = int(_env(env, "ATJUP_PRESS_WALL", 1) != 0)
+    p.rigid_lid = int(_env(env, "ATJUP_BC_RIGID_LID", 1) != 0)
+    sw = _env(env, "ATJUP_PRESS_SWEEPS", 1)
+    p.press_sweeps = sw if sw > 0 else 1
+
+    # boundary conditions, BoundaryConditions.h:100-140, BC_Jup.h:77-90
+    p.top_taper = _env(env, "ATJUP_BC_TOP_TAPER", 3)
+    p.lid_u = _env(env, "ATJUP_BC_LID_U", p.rigid_lid)
+    p.pole_fill_rows = 2 if _env(env, "ATJUP_BC_POLE_FILL", 1) != 0 else 0
+    p.mount_t_ambient = _env(env, "ATJUP_MOUNT_T_AMBIENT", 1)
+
+    # per-iteration glue, cJupiterModel.cpp:44-46 and cJupiterModel.h:937
+    p.shapiro_inloop = _env(env, "ATJUP_VEL_SHAPIRO_INLOOP", 0)
+    p.shapiro_strength = _env(env, "ATJUP_SHAPIRO_STRENGTH", 1.0, float)
+    p.v_massbal_stride = _env(env, "ATJUP_V_MASSBAL_STRIDE", 1)
+    vortex = _env(env, "ATJUP_VORTEX", 1) != 0
+    p.v_massbal_zonal = int(_env(env, "ATJUP_V_MASSBAL_ZONAL", 1 if vortex else 0) != 0)
+    p.precision = PREC_FP64
+    return p
+
+
+# Knobs whose non-default values select branches this implementation does not provide.
+_UNSUPPORTED = {
+    "ATJUP_BC_PHI_PERIODIC": ("1", "the periodic phi seam is the only seam implemented"),
+    "ATJUP_PRESS_SRC": ("1", "only the projection source div(aux) is implemented"),
+    "ATJUP_PRESS_INCR": ("0", "the defect-correction source is not implemented"),
+    "ATJUP_PRESS_LINE": ("0", "the reference line pass is replaced by the residual solver"),
+    "ATJUP_PRESS_BAROTROPIC": ("0", "the reference barotropic pass is replaced by the residual solver"),
+    "ATJUP_PBARO_FOLLOW": ("0", "p_baro follow is not implemented"),
+    "ATJUP_T_LIMITER": ("0", "the temperature limiter is not implemented"),
+    "ATJUP_BUOY_PDYN": ("0", "the buoyancy reads p_stat only"),
+    "ATJUP_PHYDRO_TOP_TAPER": ("0", "the p_hydro top taper is not implemented"),
+    "ATJUP_COSTHE_ABS": ("0", "signed cos(theta) only"),
+    "ATJUP_SPECIES_DIVU": ("0", "species flux form is not implemented"),
+    "ATJUP_BC_SEAM_DAMP": ("0", "seam damping applies only to the non-periodic seam"),
+    "ATJUP_BC_T_LID_PIN": ("0", "lid temperature pin is not implemented"),
+    "ATJUP_BC_MOUNT_COPY": ("0", "solid cells use the 2-point extrapolation"),
+    "ATJUP_BC_RADIUS_COPY": ("0", "radial walls use the 2-point Neumann form"),
+    "ATJUP_BC_BOTTOM_FORM": ("0", "radial walls use the 2-point Neumann form"),
+    "ATJUP_BC_POLE_COPY": ("1", "pole rows are copies"),
+    "ATJUP_DAMP_PDYN": ("0", "no Shapiro pass on p_dyn in the loop"),
+    "ATJUP_HYDRO_REF": ("0", "the hydrostatic integral runs upward from the base"),
+}
+
+
+def check_supported(env: Mapping[str, str] | None = None) -> list[str]:
+    """Names (with reasons) of set knobs whose values the kernels do not implement."""
+    env = os.environ if env is None else env
+    bad = []
+    for name, (ok, why) in _UNSUPPORTED.items():
+        v = env.get(name)
+        if v is not None and str(int(float(v)) if v.strip().lstrip("-").replace(".", "", 1).isdigit() else v) != ok:
+            bad.append(f"{name}={v}: {why}")
+    return bad

@@ -1,0 +1,207 @@
+/*
+ * atjup_gpu.h -- C ABI of the B200 (sm_100a) implementation of ATJUP's time-step hot path.
+ *
+ * The reference (RogerGrundmann/ATJUP) runs its time step as member functions of the singleton
+ * cJupiterModel, on jagged `double***` arrays (lib/Array.h:25-31), with ~200 ATJUP_* environment
+ * knobs read into function-local statics. This header replaces those call sites with plain
+ * extern "C" entry points: the device owns the authoritative state (structure of arrays, phi
+ * contiguous and padded), the host resolves every knob once into AtjupParams, and each entry
+ * point returns an int status. Every function below names the reference routine it replaces.
+ *
+ * Layout of a 3-D field on the host side of this ABI: either a contiguous block of
+ * im*jm*km doubles in (i, j, k) order with k fastest (i = radius, j = colatitude, k = longitude),
+ * or the reference's own `double***` (x[i][j] is a row of km doubles).
+ *
+ * Thread safety: one context per model; calls on one context must not overlap. All work is
+ * stream-ordered on the context's stream; entry points return after the work is enqueued unless
+ * they return a host value (download, stats), which synchronises the stream.
+ */
+#ifndef ATJUP_GPU_H
+#define ATJUP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATJUP_ABI_VERSION 1
+
+/* ---- status codes ---- */
+enum {
+    ATJUP_OK = 0,
+    ATJUP_ERR_ARG = 1,            /* bad argument (null pointer, unknown id, size mismatch)  */
+    ATJUP_ERR_UNSUPPORTED = 2,    /* a knob value this implementation does not provide       */
+    ATJUP_ERR_CUDA = 3,           /* a CUDA runtime error; see atjup_gpu_last_error()          */
+    ATJUP_ERR_NOT_CONVERGED = 4,  /* iterative solve hit its iteration cap                    */
+    ATJUP_ERR_NONFINITE = 5,      /* a NaN/Inf census found non-finite values                 */
+    ATJUP_ERR_NO_DEVICE = 6       /* no CUDA device, or the device is not sm_100              */
+};
+
+/* ---- field ids (upload / download / filter targets) ---- */
+enum {
+    ATJUP_F_T = 0, ATJUP_F_U, ATJUP_F_V, ATJUP_F_W,          /* prognostic dynamics           */
+    ATJUP_F_P_DYN, ATJUP_F_P_HYDRO, ATJUP_F_P_STAT,           /* pressures                     */
+    ATJUP_F_RHO_MIX, ATJUP_F_WALL_NUE, ATJUP_F_NUE,           /* frozen per-cell inputs        */
+    ATJUP_F_AUX_U, ATJUP_F_AUX_V, ATJUP_F_AUX_W,              /* projection source (persist)   */
+    ATJUP_F_P_BARO,                                           /* frozen geo-balance rest       */
+    ATJUP_F_Q_RAD, ATJUP_F_Q_PRECIP,                          /* heating inputs                */
+    ATJUP_F_COUNT
+};
+
+/* ---- solver modes for atjup_gpu_pressure_solve ---- */
+enum {
+    ATJUP_SOLVE_SWEEPS = 0,    /* the reference: n red-black Gauss-Seidel sweeps, no residual   */
+    ATJUP_SOLVE_RESIDUAL = 1   /* same discrete operator, iterated to a relative residual       */
+};
+enum { ATJUP_PREC_FP64 = 0, ATJUP_PREC_MIXED = 1 };
+
+/*
+ * Every knob that changes a branch of the hot path, resolved on the host (the reference reads
+ * them from the environment at first use; the values noted are the reference defaults).
+ * atjup_params_default() fills this block with those defaults for the 41x181x361 grid.
+ */
+typedef struct AtjupParams {
+    int32_t abi_version;               /* = ATJUP_ABI_VERSION                                   */
+    int32_t im, jm, km;                /* 41, 181, 361 (cJupiterModel.h:166)                   */
+    double dr, dthe, dphi;             /* 0.025, 1 deg, 1 deg (cJupiterModel.cpp:172-174)      */
+    double dt;                         /* ATJUP_DT 0.005 (cJupiterModel.cpp:106)                */
+    /* model constants (param.py / cJupiterDefaults.cpp.inc and ThermalPropertiesJup)          */
+    double re, pr, g, omega, u_0, t_ref, L_atm;
+    double r_mix, R_mix, cp_mix;
+    double Coriolis, centrifugal, buoyancy;
+    /* resolved knobs of RHS_Jup_Turb.cpp / RungeKutta_Jup_Turb.cpp                            */
+    double sinthe_min;                 /* ATJUP_SINTHE_MIN 0.55 (cJupiterModel.h:1121)          */
+    double p_dyn_to_bar;               /* r_mix u_0^2 1e-5 with ATJUP_PDYN_UNITS (h:1161)       */
+    double t_diff_scale;               /* ATJUP_T_DIFF_SCALE 0.01 (cJupiterModel.h:268)         */
+    double nd_cor, nd_cent, nd_buoy;   /* body-force scales (RHS_Jup_Turb.cpp:323-346)          */
+    double buoy_scale, buoy_ramp;      /* ATJUP_BUOY_SCALE 1, ramp factor for this iteration   */
+    double pgrad_scale;                /* ATJUP_PGRAD_SCALE 1                                   */
+    double rad_coupling;               /* ATJUP_RAD_COUPLING 1                                  */
+    double precip_coupling;            /* ATJUP_PRECIP_COUPLING 1                               */
+    double turb_coupling;              /* ATJUP_TURB_COUPLING 1                                 */
+    int32_t pgrad_wall, pgrad_wrap;    /* 1, 1 (RHS_Jup_Turb.cpp:103-117)                       */
+    int32_t adiabatic, adiabatic_rho;  /* 1, 1 (RHS_Jup_Turb.cpp:459-474)                       */
+    int32_t metric_split;              /* ATJUP_METRIC_SPLIT 1 (cJupiterModel.h:830)            */
+    int32_t coriolis_split;            /* ATJUP_CORIOLIS_SPLIT 1 and metric_split (h:837)       */
+    int32_t hydro_split;               /* ATJUP_HYDRO_SPLIT / ATJUP_NONDIM, 0                   */
+    int32_t cell_hold;                 /* ATJUP_CELL_HOLD (follows geo balance), 1              */
+    int32_t precip_rho_local;          /* ATJUP_PRECIP_RHO_LOCAL 1                              */
+    int32_t local_rho;                 /* ATJUP_LOCAL_RHO 1                                     */
+    int32_t rho_pdyn;                  /* ATJUP_RHO_PDYN (0 with geo balance)                   */
+    int32_t has_nue;                   /* nue field non-zero (turbulence closure on)            */
+    int32_t has_heating;               /* Q_rad / Q_precip fields present                       */
+    /* pressure solver (PressureSolver.h:144-766)                                               */
+    double p_dyn_cap;                  /* ATJUP_PDYN_CAP 0.2                                    */
+    int32_t press_wall;                /* ATJUP_PRESS_WALL 1 (has_obstacle)                     */
+    int32_t rigid_lid;                 /* ATJUP_BC_RIGID_LID 1                                  */
+    int32_t press_sweeps;              /* ATJUP_PRESS_SWEEPS 1                                  */
+    /* boundary conditions (BoundaryConditions.h, BC_Jup.h)                                     */
+    int32_t top_taper;                 /* ATJUP_BC_TOP_TAPER 3                                  */
+    int32_t lid_u;                     /* ATJUP_BC_LID_U = rigid lid, 1                         */
+    int32_t pole_fill_rows;            /* 2 with ATJUP_BC_POLE_FILL 1                           */
+    int32_t mount_t_ambient;           /* ATJUP_MOUNT_T_AMBIENT 1                               */
+    /* per-iteration filters and glue (cJupiterModel.cpp:1328-1354)                             */
+    int32_t shapiro_inloop;            /* ATJUP_VEL_SHAPIRO_INLOOP passes (0 = off)             */
+    double shapiro_strength;           /* ATJUP_SHAPIRO_STRENGTH 1                              */
+    int32_t v_massbal_stride;          /* ATJUP_V_MASSBAL_STRIDE 1                              */
+    int32_t v_massbal_zonal;           /* ATJUP_V_MASSBAL_ZONAL (follows ATJUP_VORTEX), 1       */
+    int32_t precision;                 /* ATJUP_PREC_FP64 or ATJUP_PREC_MIXED                   */
+} AtjupParams;
+
+typedef struct AtjupSolveOpts {
+    int32_t mode;          /* ATJUP_SOLVE_SWEEPS or ATJUP_SOLVE_RESIDUAL                         */
+    int32_t sweeps;        /* SWEEPS: number of red-black sweeps                                  */
+    int32_t max_iter;      /* RESIDUAL: iteration cap (returns ATJUP_ERR_NOT_CONVERGED at it)     */
+    int32_t precision;     /* RESIDUAL: ATJUP_PREC_FP64, or MIXED = FP32 inner / FP64 refinement  */
+    double rel_tol;        /* RESIDUAL: target ||b - A p|| / ||b|| (y-weighted, fluid cells)      */
+    double omega;          /* relaxation factor of the sweeps (reference: 1.0)                    */
+    int32_t external_rhs;  /* RESIDUAL: 1 = solve A p = b for b in atjup_gpu_set_solve_rhs       */
+} AtjupSolveOpts;
+
+typedef struct AtjupSolveStats {
+    int32_t iterations;    /* sweeps or Krylov iterations performed                              */
+    int32_t inner_solves;  /* MIXED: FP32 inner solves under the FP64 refinement loop            */
+    double rel_residual;   /* final ||b - A p|| / ||b||, or -1 when not computed (SWEEPS)       */
+    double b_norm;         /* ||b|| of the projected right-hand side                              */
+} AtjupSolveStats;
+
+typedef struct AtjupCtx AtjupCtx;
+
+/* Defaults of the reference for the 41x181x361 grid (values noted in AtjupParams). */
+void atjup_params_default(AtjupParams* p);
+
+/* Create a device context: allocates the SoA state on the current CUDA device.
+ * Replaces the field allocation of cJupiterModel::resetArrays (cJupiterModel.cpp:1570-1753). */
+int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out);
+int atjup_gpu_destroy(AtjupCtx* ctx);
+
+/* Use a caller-owned cudaStream_t (passed as void*); NULL = the context's own stream. */
+int atjup_gpu_set_stream(AtjupCtx* ctx, void* stream);
+
+/* Geometry and frozen per-(i,j) inputs:
+ *   rad[im]      metric radius rad.z (cJupiterModel.cpp:441-468 shifts it to R/L_atm + i dr)
+ *   the[jm]      colatitude the.z
+ *   solid[im*jm*km]  SeaMount mask (1 = solid), BC_Jup.h:353-458
+ *   i_topo[jm*km]    first fluid level per column (i_topography)
+ *   cell_vbar0 / cell_ubar0 [im*jm]  ATJUP_CELL_HOLD means (may be NULL when cell_hold = 0)   */
+int atjup_gpu_set_grid(AtjupCtx* ctx, const double* rad, const double* the,
+                       const uint8_t* solid, const int32_t* i_topo,
+                       const double* cell_vbar0, const double* cell_ubar0);
+
+/* Copy a contiguous (i,j,k) host field to / from the device (synchronous).
+ * Replaces the host Array as the owner of that field. */
+int atjup_gpu_upload(AtjupCtx* ctx, int32_t field_id, const double* host);
+int atjup_gpu_download(AtjupCtx* ctx, int32_t field_id, double* host);
+/* The same for the reference's jagged Array storage (x[i][j] -> km doubles). */
+int atjup_gpu_upload_array(AtjupCtx* ctx, int32_t field_id, double*** x);
+int atjup_gpu_download_array(AtjupCtx* ctx, int32_t field_id, double*** x);
+
+/* Device pointer of a field (row pitch in elements via *pitch) for zero-copy interop (DLPack). */
+int atjup_gpu_field_ptr(AtjupCtx* ctx, int32_t field_id, void** dev_ptr, int32_t* pitch);
+
+/* cJupiterModel::RungeKuttaJup (RungeKutta_Jup_Turb.cpp:261-583): buoyancy level mean,
+ * hydrostatic pressure, four fused RK stages (RHSJup per cell, RHS_Jup_Turb.cpp:31-1457). */
+int atjup_gpu_rk4_step(AtjupCtx* ctx, int32_t iter_n);
+
+/* PressureSolverJup::run (PressureSolver.h:144-766) incl. prepareProjectionBoundaries
+ * (cJupiterModel.cpp:1842-1864). SWEEPS reproduces the reference; RESIDUAL solves the same
+ * operator to opts->rel_tol. stats may be NULL. */
+int atjup_gpu_pressure_solve(AtjupCtx* ctx, const AtjupSolveOpts* opts, AtjupSolveStats* stats);
+
+/* Right-hand side for an isolated solve (contiguous, i,j,k; interior rows are read). */
+int atjup_gpu_set_solve_rhs(AtjupCtx* ctx, const double* host_b);
+
+/* Boundary passes: BC_Jup::bcRadius, bcTheta, bcPhi, bcSolidGround (BC_Jup.h:185-658). */
+enum { ATJUP_BC_RADIUS = 1, ATJUP_BC_THETA = 2, ATJUP_BC_PHI = 4, ATJUP_BC_SOLID = 8,
+       ATJUP_BC_ALL = 15 };
+int atjup_gpu_bc(AtjupCtx* ctx, int32_t which);
+
+/* JupiterUtils::damp_wiggles (order 2) / damp_wiggles_ho (order 4), lib/Utils.cpp:227-453,
+ * k then j then i passes, with i_topography as the fluid floor when use_topo. */
+int atjup_gpu_shapiro(AtjupCtx* ctx, int32_t field_id, int32_t order, double strength,
+                      int32_t passes, int32_t use_topo);
+
+/* cJupiterModel::computeMixtureDensity (InitValues_Jup.cpp:717-740). */
+int atjup_gpu_mixture_density(AtjupCtx* ctx);
+
+/* cJupiterModel::balanceColumnV (InitValues_Jup.cpp:1500-1538); vshift may be NULL. */
+int atjup_gpu_balance_column_v(AtjupCtx* ctx, double* vshift);
+
+/* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381) for the dry
+ * configuration: pressure solve on even iterations (and when first != 0), mixture density,
+ * RK4, boundary passes, in-loop Shapiro, column balance of v; restoreVar is implicit (the
+ * device state is the time-level n copy). solve may be NULL (= params->press_sweeps sweeps). */
+int atjup_gpu_step(AtjupCtx* ctx, int32_t iter_n, int32_t first, const AtjupSolveOpts* solve);
+
+/* Count of non-finite values in the prognostic fields (NaN/Inf census; no device trap). */
+int atjup_gpu_nonfinite_count(AtjupCtx* ctx, int64_t* count);
+
+int atjup_gpu_synchronize(AtjupCtx* ctx);
+const char* atjup_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATJUP_GPU_H */

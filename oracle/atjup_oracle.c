@@ -1,0 +1,914 @@
+/*
+ * CPU oracle for the ATJUP hot path -- TEST INFRASTRUCTURE ONLY (see atjup_oracle.h).
+ *
+ * Each routine restates one reference routine; the file:line it follows is given at the routine.
+ * Expressions keep the reference's operand order so that, built with FMA contraction off, the
+ * FP64 results are bit-identical to the reference's own -- that is what lets tests pin this file
+ * to the reference exactly rather than to a tolerance.
+ */
+#include "atjup_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IDX(i, j, k) (((size_t)(i) * (size_t)jm + (size_t)(j)) * (size_t)km + (size_t)(k))
+#define C43 (4.0 / 3.0)
+#define C13 (1.0 / 3.0)
+
+static inline int phi_wrap(int periodic, int kk, int km) {
+    /* ATPhys.h:131-135: the ring of km-1 distinct meridians */
+    if (!periodic) return kk;
+    const int n = km - 1;
+    return kk < 0 ? kk + n : (kk >= n ? kk - n : kk);
+}
+
+static inline double dmax(double a, double b) { return a < b ? b : a; }   /* std::max(a, b) */
+static inline double dmin(double a, double b) { return b < a ? b : a; }   /* std::min(a, b) */
+
+/* Geometry of one (i, j) row, built as RungeKutta_Jup_Turb.cpp:388-411 builds CellGeometry. */
+typedef struct {
+    double rm, rm2, exp_rm, exp_2_rm, sinthe, sinthe2, costhe, cotanthe;
+    double inv_rm, inv_rm2, inv_rmsinthe, inv_rm2sinthe, inv_rm2sinthe2, costhe_inv_rm2sinthe;
+    double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
+} geom;
+
+static void make_geom(const AtjupParams* P, const ora_grid* G, int i, int j, geom* g) {
+    g->rm = G->rad[i];
+    g->rm2 = g->rm * g->rm;
+    g->exp_rm = 1.0;                         /* coord_stretching = false (param.py:52)      */
+    g->exp_2_rm = g->exp_rm * g->exp_rm;
+    g->sinthe = dmax(P->sinthe_min, fabs(sin(G->the[j])));
+    g->sinthe2 = g->sinthe * g->sinthe;
+    g->costhe = cos(G->the[j]);
+    g->cotanthe = g->costhe / g->sinthe;
+    g->inv_rm = 1.0 / g->rm;
+    g->inv_rm2 = 1.0 / g->rm2;
+    g->inv_rmsinthe = 1.0 / (g->rm * g->sinthe);
+    g->inv_rm2sinthe = g->inv_rm2 / g->sinthe;
+    g->inv_rm2sinthe2 = g->inv_rm2 / g->sinthe2;
+    g->costhe_inv_rm2sinthe = g->costhe * g->inv_rm2sinthe;
+    g->inv_2dr = 1.0 / (2.0 * P->dr);
+    g->inv_2dthe = 1.0 / (2.0 * P->dthe);
+    g->inv_2dphi = 1.0 / (2.0 * P->dphi);
+    g->inv_dr2 = 1.0 / (P->dr * P->dr);
+    g->inv_dthe2 = 1.0 / (P->dthe * P->dthe);
+    g->inv_dphi2 = 1.0 / (P->dphi * P->dphi);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* RungeKutta_Jup_Turb.cpp:47-69 -- sin(theta)-weighted level mean of g p_stat / (r R T t_ref)  */
+void ora_buoy_ref_level(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    for (int i = 0; i < im; i++) {
+        double sum = 0.0, wsum = 0.0;
+        for (int j = 0; j < jm; j++) {
+            const double wgt = sin(G->the[j]);
+            for (int k = 0; k < km; k++) {
+                if (G->solid[IDX(i, j, k)]) continue;
+                const double t = S->t[IDX(i, j, k)];
+                if (!(t > 0.0)) continue;
+                const double b = P->g * S->p_stat[IDX(i, j, k)] / (P->r_mix * P->R_mix * t * P->t_ref);
+                if (!isfinite(b)) continue;
+                sum += wgt * b;
+                wsum += wgt;
+            }
+        }
+        S->buoy_ref[i] = (wsum > 0.0) ? sum / wsum : 0.0;
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* RungeKutta_Jup_Turb.cpp:119-259. With ATJUP_METRIC_SPLIT (default) the column integral carries
+ * (v^2 + w^2)/r + cor * w (plus the buoyancy only under ATJUP_HYDRO_SPLIT); otherwise the
+ * buoyancy alone, integrated upward from the fluid foot of the column.                        */
+static double buoy_term(const AtjupParams* P, const ora_state* S, size_t c, int i) {
+    const double T = S->t[c];
+    if (!(T > 0.0)) return 0.0;
+    const double b = P->g * S->p_stat[c] / (P->r_mix * P->R_mix * T * P->t_ref) - S->buoy_ref[i];
+    /* the ATJUP_BUOY_RHO_LEVEL form follows hydro_split; plain form otherwise */
+    double f;
+    if (P->hydro_split) {
+        const double nd_rel = P->g * (P->L_atm * 1.0e3) / (P->u_0 * P->u_0);
+        f = -nd_rel * P->buoy_scale * P->buoyancy * b / S->buoy_ref[i];
+    } else {
+        f = -P->nd_buoy * P->buoy_scale * P->buoyancy * b;
+    }
+    return isfinite(f) ? f : 0.0;
+}
+
+void ora_hydrostatic(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    for (int j = 0; j < jm; j++) {
+        const double cor = P->coriolis_split
+            ? P->Coriolis * P->nd_cor * 2.0 * P->omega * fabs(sin(G->the[j])) : 0.0;
+        for (int k = 0; k < km; k++) {
+            int i0 = 0;
+            while (i0 < im && G->solid[IDX(i0, j, k)]) { S->p_hydro[IDX(i0, j, k)] = 0.0; i0++; }
+            if (i0 >= im) continue;
+            int i1 = i0;
+            while (i1 + 1 < im && !G->solid[IDX(i1 + 1, j, k)]) i1++;
+            for (int i = i1 + 1; i < im; i++) S->p_hydro[IDX(i, j, k)] = 0.0;
+            if (P->metric_split) {
+                S->p_hydro[IDX(i0, j, k)] = 0.0;
+                double fprev = 0.0;
+                for (int i = i0; i <= i1; i++) {
+                    const size_t c = IDX(i, j, k);
+                    const double vv = S->v[c], ww = S->w[c];
+                    const double f = (P->hydro_split ? buoy_term(P, S, c, i) : 0.0)
+                                   + ((vv * vv + ww * ww) / G->rad[i] + cor * ww) / 1.0;
+                    if (i > i0)
+                        S->p_hydro[c] = S->p_hydro[IDX(i - 1, j, k)] + 0.5 * (fprev + f) * P->dr;
+                    fprev = f;
+                }
+                if (S->p_baro)
+                    for (int i = i0; i <= i1; i++) S->p_hydro[IDX(i, j, k)] += S->p_baro[IDX(i, j, k)];
+            } else {
+                S->p_hydro[IDX(i0, j, k)] = 0.0;
+                for (int i = i0 + 1; i <= i1; i++)
+                    S->p_hydro[IDX(i, j, k)] = S->p_hydro[IDX(i - 1, j, k)]
+                        + 0.5 * (buoy_term(P, S, IDX(i - 1, j, k), i - 1) + buoy_term(P, S, IDX(i, j, k), i)) * P->dr;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* RHS_Jup_Turb.cpp:31-1457, the dynamics equations. Reads the live fields t, u, v, w (the
+ * stage input), writes rhs_t/u/v/w and aux_u/v/w at (i, j, k).                               */
+void ora_rhs_cell(const AtjupParams* P, const ora_grid* G, ora_state* S, int i, int j, int k) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    (void)im;
+    geom g;
+    make_geom(P, G, i, j, &g);
+    const int per = 1;
+    const int kw = phi_wrap(per, k - 1, km), ke = phi_wrap(per, k + 1, km);
+    const size_t c = IDX(i, j, k);
+    const size_t cip = IDX(i + 1, j, k), cim = IDX(i - 1, j, k);
+    const size_t cjp = IDX(i, j + 1, k), cjm = IDX(i, j - 1, k);
+    const size_t ckp = IDX(i, j, ke), ckm = IDX(i, j, kw);
+    const uint8_t* sol = G->solid;
+
+    const double u_ijk = S->u[c], v_ijk = S->v[c], w_ijk = S->w[c];
+
+    /* pgrad: centred difference with solid faces mirrored to the local value (103-130) */
+#define PGRAD(Pf, hi_i, lo_i, inv2d) ( \
+        ((P->pgrad_wall && sol[hi_i]) ? (Pf)[c] : (Pf)[hi_i]) - \
+        ((P->pgrad_wall && sol[lo_i]) ? (Pf)[c] : (Pf)[lo_i])) * (inv2d)
+
+#define DR1(F) ((F[cip] - F[cim]) * g.inv_2dr * g.exp_rm)
+#define DR2(F) ((F[cip] - 2.0 * F[c] + F[cim]) * g.inv_dr2 * g.exp_2_rm)
+#define DT1(F) ((F[cjp] - F[cjm]) * g.inv_2dthe)
+#define DT2(F) ((F[cjp] - 2.0 * F[c] + F[cjm]) * g.inv_dthe2)
+#define DP1(F) ((F[ckp] - F[ckm]) * g.inv_2dphi)
+#define DP2(F) ((F[ckp] - 2.0 * F[c] + F[ckm]) * g.inv_dphi2)
+
+    const double *U = S->u, *V = S->v, *W = S->w, *T = S->t;
+    const double dudr = DR1(U), d2udr2 = DR2(U), dvdr = DR1(V), d2vdr2 = DR2(V);
+    const double dwdr = DR1(W), d2wdr2 = DR2(W), dtdr = DR1(T), d2tdr2 = DR2(T);
+    const double dpdr = PGRAD(S->p_dyn, cip, cim, g.inv_2dr) * g.exp_rm;
+    const double dudthe = DT1(U), d2udthe2 = DT2(U), dvdthe = DT1(V), d2vdthe2 = DT2(V);
+    const double dwdthe = DT1(W), d2wdthe2 = DT2(W), dtdthe = DT1(T), d2tdthe2 = DT2(T);
+    const double dpdthe = PGRAD(S->p_dyn, cjp, cjm, g.inv_2dthe);
+    const double dudphi = DP1(U), d2udphi2 = DP2(U), dvdphi = DP1(V), d2vdphi2 = DP2(V);
+    const double dwdphi = DP1(W), d2wdphi2 = DP2(W), dtdphi = DP1(T), d2tdphi2 = DP2(T);
+    const double dpdphi = PGRAD(S->p_dyn, ckp, ckm, g.inv_2dphi);
+
+    /* body forces (334-423): true sine in Coriolis and centrifugal terms */
+    const double sinthe_true = sqrt(dmax(0.0, 1.0 - g.costhe * g.costhe));
+    const double Coriolis_rad = P->nd_cor * -2.0 * P->omega * sinthe_true * w_ijk;
+    const double Coriolis_the = P->nd_cor * -2.0 * P->omega * g.costhe * w_ijk;
+    double v_cor = v_ijk, u_cor = u_ijk;
+    if (P->cell_hold && G->cell_vbar0) {
+        v_cor -= G->cell_vbar0[(size_t)i * jm + j];
+        u_cor -= G->cell_ubar0[(size_t)i * jm + j];
+    }
+    const double Coriolis_phi = P->nd_cor * +2.0 * P->omega * (+g.costhe * v_cor + sinthe_true * u_cor);
+    const double centrifugal_rad = P->nd_cent * P->omega * P->omega * g.rm * sinthe_true * sinthe_true;
+    const double centrifugal_the = P->nd_cent * P->omega * P->omega * g.rm * sinthe_true * g.costhe;
+    const double coeff_energy_p = P->u_0 * P->u_0 / (P->cp_mix * P->t_ref);
+
+    const double v_invrm = v_ijk * g.inv_rm;
+    const double w_invrs = w_ijk * g.inv_rmsinthe;
+
+    /* compression work with the hydrostatic part (459-482) */
+    double dpstatdr = 0.0;
+    if (P->adiabatic) {
+        const double to_nd = 1.0 / P->p_dyn_to_bar;
+        dpstatdr = (S->p_stat[cip] - S->p_stat[cim]) * g.inv_2dr * g.exp_rm * to_nd;
+        const double rho_l = S->rho_mix[c];
+        if (P->adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr *= P->r_mix / rho_l;
+    }
+    const double pressure_t = coeff_energy_p
+        * (u_ijk * (dpdr + dpstatdr) + v_invrm * dpdthe + w_invrs * dpdphi);
+    const double transport_t = u_ijk * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
+
+    const double metric_on = P->metric_split ? 0.0 : 1.0;
+    const double cor_rad_on = P->coriolis_split ? 0.0 : 1.0;
+    const double transport_u = u_ijk * dudr + v_invrm * dudthe + w_invrs * dudphi
+        - metric_on * (v_ijk * v_ijk + w_ijk * w_ijk) * g.inv_rm;
+    const double transport_v = u_ijk * dvdr + v_invrm * dvdthe + w_invrs * dvdphi
+        + (u_ijk * v_ijk - w_ijk * w_ijk * g.cotanthe) * g.inv_rm;
+    const double transport_w = u_ijk * dwdr + v_invrm * dwdthe + w_invrs * dwdphi
+        + (w_ijk * u_ijk + v_ijk * w_ijk * g.cotanthe) * g.inv_rm;
+
+    /* diffusion (521-545) */
+    const double two_inv_rm = 2.0 * g.inv_rm;
+    const double v_metric = (1.0 + g.costhe / (g.sinthe2)) * g.inv_rm2;
+    const double diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * g.inv_rm2
+        + dtdthe * g.costhe_inv_rm2sinthe + d2tdphi2 * g.inv_rm2sinthe2;
+    const double diffusion_u = d2udr2 + 2.0 * u_ijk * g.inv_rm2 + d2udthe2 * g.inv_rm2
+        + 4.0 * dudr * g.inv_rm + dudthe * g.costhe_inv_rm2sinthe
+        + d2udphi2 * g.inv_rm2sinthe2;
+    const double diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * g.inv_rm2
+        + dvdthe * g.costhe_inv_rm2sinthe - v_metric * v_ijk
+        + d2vdphi2 * g.inv_rm2sinthe2
+        + 2.0 * dudthe * g.inv_rm2
+        - dwdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+    const double diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * g.inv_rm2
+        + dwdthe * g.costhe_inv_rm2sinthe - v_metric * w_ijk
+        + d2wdphi2 * g.inv_rm2sinthe2
+        + 2.0 * dudphi * g.inv_rm2sinthe
+        + dvdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+
+    /* pressure-gradient terms (589-620) */
+    const double dpdr_term = P->pgrad_scale * dpdr;
+    const double dpdthe_term = P->pgrad_scale * dpdthe * g.inv_rm;
+    const double dpdphi_term = P->pgrad_scale * dpdphi * g.inv_rmsinthe;
+    double dphdthe_term = 0.0, dphdphi_term = 0.0;
+    if (P->hydro_split || P->metric_split) {
+        dphdthe_term = PGRAD(S->p_hydro, cjp, cjm, g.inv_2dthe) * g.inv_rm;
+        dphdphi_term = PGRAD(S->p_hydro, ckp, ckm, g.inv_2dphi) * g.inv_rmsinthe;
+    }
+
+    /* radiative and latent heating (646-718) */
+    double radiation_t = 0.0, precip_t = 0.0;
+    if (P->has_heating && S->Q_rad && P->rad_coupling != 0.0) {
+        const double T_phys = S->t[c] * P->t_ref;
+        const double P_phys = S->p_stat[c] * 1.0e5;
+        const double rho_f = S->rho_mix[c];
+        const double rho = (rho_f > 0.0 && isfinite(rho_f)) ? rho_f
+                         : ((T_phys > 1.0) ? P_phys / (P->R_mix * T_phys) : 0.0);
+        const double L_rad = P->L_atm * 1.0e3;
+        if (rho > 0.0 && P->cp_mix > 0.0) {
+            radiation_t = P->rad_coupling * S->Q_rad[c] * L_rad / (rho * P->cp_mix * P->u_0 * P->t_ref);
+            if (!isfinite(radiation_t)) radiation_t = 0.0;
+            else if (radiation_t > 0.5) radiation_t = 0.5;
+            else if (radiation_t < -0.5) radiation_t = -0.5;
+        }
+    }
+    if (P->has_heating && S->Q_precip && P->precip_coupling != 0.0) {
+        const double L_rad = P->L_atm * 1.0e3;
+        double rho_p = P->r_mix;
+        if (P->precip_rho_local && P->local_rho) {
+            const double rr = S->rho_mix[c];
+            rho_p = (rr > 0.0 && isfinite(rr)) ? rr : P->r_mix;
+        }
+        if (rho_p > 0.0 && P->cp_mix > 0.0) {
+            precip_t = P->precip_coupling * S->Q_precip[c] * L_rad / (rho_p * P->cp_mix * P->u_0 * P->t_ref);
+            if (!isfinite(precip_t)) precip_t = 0.0;
+            else if (precip_t > 0.5) precip_t = 0.5;
+            else if (precip_t < -0.5) precip_t = -0.5;
+        }
+    }
+
+    /* eddy and wall viscosity (736-752) */
+    double nue_t = 0.0;
+    if (P->has_nue && S->nue && P->turb_coupling != 0.0 && isfinite(S->nue[c]))
+        nue_t = P->turb_coupling * dmax(0.0, S->nue[c]);
+    const double nue_t_s = nue_t / 0.9;
+    const double nue_wall = S->wall_nue[c];
+
+    S->rhs_t[c] = +pressure_t - transport_t
+        + diffusion_t * (P->t_diff_scale / (P->re * P->pr) + nue_t_s)
+        + radiation_t + precip_t;
+
+    /* Boussinesq buoyancy anomaly (1080-1092) */
+    const double buoyancy_u = (S->t[c] > 0.0)
+        ? -P->nd_buoy * P->buoy_scale * P->buoy_ramp * P->buoyancy
+          * (P->g * S->p_stat[c] / (P->r_mix * P->R_mix * S->t[c] * P->t_ref) - S->buoy_ref[i])
+        : 0.0;
+
+    const double visc = 1.0 / P->re + nue_t + nue_wall;
+    S->rhs_u[c] = -dpdr_term + ((P->hydro_split != 0) ? 0.0 : buoyancy_u) - transport_u
+        + diffusion_u * visc - cor_rad_on * P->Coriolis * Coriolis_rad
+        + P->centrifugal * centrifugal_rad;
+    S->rhs_v[c] = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc
+        - P->Coriolis * Coriolis_the + P->centrifugal * centrifugal_the;
+    S->rhs_w[c] = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc
+        - P->Coriolis * Coriolis_phi;
+
+    S->aux_u[c] = S->rhs_u[c] + dpdr_term;
+    S->aux_v[c] = S->rhs_v[c] + dpdthe_term;
+    S->aux_w[c] = S->rhs_w[c] + dpdphi_term;
+#undef PGRAD
+#undef DR1
+#undef DR2
+#undef DT1
+#undef DT2
+#undef DP1
+#undef DP2
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* RungeKutta_Jup_Turb.cpp:261-583: level mean, hydrostatic pressure, four separated stages
+ * (pass A: RHS everywhere from one consistent state; pass B: accumulate and form the next
+ * stage input), final assembly y = y_n + dt (k1 + 2k2 + 2k3 + k4) / 6.                       */
+void ora_rk4(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    ora_buoy_ref_level(P, G, S);
+    ora_hydrostatic(P, G, S);
+    const double dt = P->dt;
+    for (int stage = 0; stage < 4; stage++) {
+        const double c_in = (stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0);
+        const double wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+        for (int i = 1; i < im - 1; i++)
+            for (int j = 3; j < jm - 3; j++)
+                for (int k = 0; k < km - 1; k++) {
+                    if (G->solid[IDX(i, j, k)]) continue;
+                    ora_rhs_cell(P, G, S, i, j, k);
+                }
+        for (int i = 1; i < im - 1; i++)
+            for (int j = 3; j < jm - 3; j++)
+                for (int k = 0; k < km - 1; k++) {
+                    const size_t c = IDX(i, j, k);
+                    if (G->solid[c]) continue;
+                    S->acc_t[c] = (stage == 0) ? wgt * S->rhs_t[c] : S->acc_t[c] + wgt * S->rhs_t[c];
+                    S->acc_u[c] = (stage == 0) ? wgt * S->rhs_u[c] : S->acc_u[c] + wgt * S->rhs_u[c];
+                    S->acc_v[c] = (stage == 0) ? wgt * S->rhs_v[c] : S->acc_v[c] + wgt * S->rhs_v[c];
+                    S->acc_w[c] = (stage == 0) ? wgt * S->rhs_w[c] : S->acc_w[c] + wgt * S->rhs_w[c];
+                    if (stage < 3) {
+                        S->t[c] = S->tn[c] + c_in * S->rhs_t[c];
+                        S->u[c] = S->un[c] + c_in * S->rhs_u[c];
+                        S->v[c] = S->vn[c] + c_in * S->rhs_v[c];
+                        S->w[c] = S->wn[c] + c_in * S->rhs_w[c];
+                    }
+                }
+    }
+    const double one_sixth = 1.0 / 6.0;
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 3; j < jm - 3; j++)
+            for (int k = 0; k < km - 1; k++) {
+                const size_t c = IDX(i, j, k);
+                if (G->solid[c]) continue;
+                S->t[c] = S->tn[c] + dt * S->acc_t[c] * one_sixth;
+                S->u[c] = S->un[c] + dt * S->acc_u[c] * one_sixth;
+                S->v[c] = S->vn[c] + dt * S->acc_v[c] * one_sixth;
+                S->w[c] = S->wn[c] + dt * S->acc_w[c] * one_sixth;
+            }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* cJupiterModel.cpp:1842-1864: radial walls of the projection source before the divergence.   */
+void ora_prepare_projection(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    (void)G;
+    for (int j = 1; j < jm - 1; j++)
+        for (int k = 0; k < km - 1; k++) {
+            if (P->rigid_lid) {
+                S->aux_u[IDX(0, j, k)] = 0.0;
+                S->aux_u[IDX(im - 1, j, k)] = 0.0;
+            } else {
+                S->aux_u[IDX(0, j, k)] = C43 * S->aux_u[IDX(1, j, k)] - C13 * S->aux_u[IDX(2, j, k)];
+                S->aux_u[IDX(im - 1, j, k)] = C43 * S->aux_u[IDX(im - 2, j, k)] - C13 * S->aux_u[IDX(im - 3, j, k)];
+            }
+            S->aux_v[IDX(0, j, k)] = C43 * S->aux_v[IDX(1, j, k)] - C13 * S->aux_v[IDX(2, j, k)];
+            S->aux_v[IDX(im - 1, j, k)] = C43 * S->aux_v[IDX(im - 2, j, k)] - C13 * S->aux_v[IDX(im - 3, j, k)];
+            S->aux_w[IDX(0, j, k)] = C43 * S->aux_w[IDX(1, j, k)] - C13 * S->aux_w[IDX(2, j, k)];
+            S->aux_w[IDX(im - 1, j, k)] = C43 * S->aux_w[IDX(im - 2, j, k)] - C13 * S->aux_w[IDX(im - 3, j, k)];
+        }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* PressureSolver.h:144-766, pointwise branch. The divergence source of one cell (370-459),
+ * one-sided at solid cells, then the clamp |src| <= cap * den (484-487).                      */
+static double pressure_cell_source(const AtjupParams* P, const ora_grid* G, const ora_state* S,
+                                   int i, int j, int k, double den, const geom* g) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const uint8_t* sol = G->solid;
+    const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+    const double inv_dthe = 1.0 / P->dthe, inv_dphi = 1.0 / P->dphi;
+    const double *Su = S->aux_u, *Sv = S->aux_v, *Sw = S->aux_w;
+    const int sld = sol[IDX(i, j, k)];
+    const int sld_kp1 = sol[IDX(i, j, ke)], sld_km1 = sol[IDX(i, j, kw)];
+    const int sld_kp2 = (k < km - 2) ? sol[IDX(i, j, k + 2)] : 0;
+    const int sld_km2 = (k > 2) ? sol[IDX(i, j, k - 2)] : 0;
+    const int i_in_range = (i < im - 2);
+    const int j_inner = (j > 2) && (j < jm - 2);
+    double du_dr = 0.0, dv_dthe = 0.0, dw_dphi = 0.0;
+    int r_flag = 0, the_flag = 0, phi_flag = 0;
+    if (i_in_range && sld && !sol[IDX(i + 1, j, k)]) {
+        du_dr = (-3.0 * Su[IDX(i, j, k)] + 4.0 * Su[IDX(i + 1, j, k)] - Su[IDX(i + 2, j, k)]) * g->inv_2dr;
+        r_flag = 1;
+    }
+    if (j_inner) {
+        const int air_jp1 = !sol[IDX(i, j + 1, k)], air_jm1 = !sol[IDX(i, j - 1, k)];
+        if (sld && air_jp1 && !sol[IDX(i, j + 2, k)]) {
+            dv_dthe = (-3.0 * Sv[IDX(i, j, k)] + 4.0 * Sv[IDX(i, j + 1, k)] - Sv[IDX(i, j + 2, k)]) * g->inv_2dthe;
+            the_flag = 1;
+        }
+        if (sld && air_jm1 && !sol[IDX(i, j - 2, k)]) {
+            dv_dthe = -(-3.0 * Sv[IDX(i, j, k)] + 4.0 * Sv[IDX(i, j - 1, k)] - Sv[IDX(i, j - 2, k)]) * g->inv_2dthe;
+            the_flag = 1;
+        }
+        if ((sld && air_jp1 && sol[IDX(i, j + 2, k)]) || (j == jm - 2 && !sld && sol[IDX(i, j + 1, k)])) {
+            dv_dthe = (Sv[IDX(i, j + 1, k)] - Sv[IDX(i, j, k)]) * inv_dthe;
+            the_flag = 1;
+        }
+        if ((sld && air_jm1 && sol[IDX(i, j - 2, k)]) || (j == 1 && sld && air_jm1)) {
+            dv_dthe = (Sv[IDX(i, j - 1, k)] - Sv[IDX(i, j, k)]) * inv_dthe;
+            the_flag = 1;
+        }
+    }
+    if (k > 2 && k < km - 2) {
+        const int air_kp1 = !sld_kp1, air_km1 = !sld_km1;
+        if (sld && air_kp1 && !sld_kp2) {
+            dw_dphi = (-3.0 * Sw[IDX(i, j, k)] + 4.0 * Sw[IDX(i, j, k + 1)] - Sw[IDX(i, j, k + 2)]) * g->inv_2dphi;
+            phi_flag = 1;
+        }
+        if (sld && air_km1 && !sld_km2) {
+            dw_dphi = -(-3.0 * Sw[IDX(i, j, k)] + 4.0 * Sw[IDX(i, j, k - 1)] - Sw[IDX(i, j, k - 2)]) * g->inv_2dphi;
+            phi_flag = 1;
+        }
+        if ((sld && air_kp1 && sld_kp2) || (k == km - 2 && !sld && sld_kp1)) {
+            dw_dphi = (Sw[IDX(i, j, k + 1)] - Sw[IDX(i, j, k)]) * inv_dphi;
+            phi_flag = 1;
+        }
+        if ((sld && air_km1 && sld_km2) || (k == 1 && sld && air_km1)) {
+            dw_dphi = (Sw[IDX(i, j, k - 1)] - Sw[IDX(i, j, k)]) * inv_dphi;
+            phi_flag = 1;
+        }
+    }
+    if (!r_flag) du_dr = (Su[IDX(i + 1, j, k)] - Su[IDX(i - 1, j, k)]) * g->inv_2dr;
+    if (!the_flag) dv_dthe = (Sv[IDX(i, j + 1, k)] - Sv[IDX(i, j - 1, k)]) * g->inv_2dthe;
+    if (!phi_flag) dw_dphi = (Sw[IDX(i, j, ke)] - Sw[IDX(i, j, kw)]) * g->inv_2dphi;
+    double div_src = du_dr * g->exp_rm + dv_dthe * g->inv_rm + dw_dphi * g->inv_rmsinthe;
+    const double src_max = den * P->p_dyn_cap;
+    if (!isfinite(div_src)) div_src = 0.0;
+    else if (div_src > src_max) div_src = src_max;
+    else if (div_src < -src_max) div_src = -src_max;
+    return div_src;
+}
+
+/* Stencil weights of row (i, j) (PressureSolver.h:354-357) with the solver's sine table. */
+static void press_weights(const AtjupParams* P, const ora_grid* G, int i, int j, geom* g,
+                          double* num1, double* num2, double* num3) {
+    make_geom(P, G, i, j, g);
+    /* PressureSolver.h:156-162: the same floor; the sine is never 0 on this grid's interior */
+    *num1 = g->exp_2_rm * g->inv_dr2;
+    *num2 = g->inv_rm2 * g->inv_dthe2;
+    *num3 = g->inv_rm2sinthe2 * g->inv_dphi2;
+}
+
+/* Face-dropping sum over the six neighbours (461-479); returns den, writes acc. */
+static double press_gather(const AtjupParams* P, const ora_grid* G, const double* p,
+                           int i, int j, int k, double num1, double num2, double num3,
+                           double* acc_out) {
+    const int jm = P->jm, km = P->km;
+    const uint8_t* sol = G->solid;
+    const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+    const int sld = sol[IDX(i, j, k)];
+    double acc = 0.0, den;
+    if (P->press_wall && !sld) {
+        den = 0.0;
+        if (!sol[IDX(i + 1, j, k)]) { acc += num1 * p[IDX(i + 1, j, k)]; den += num1; }
+        if (!sol[IDX(i - 1, j, k)]) { acc += num1 * p[IDX(i - 1, j, k)]; den += num1; }
+        if (!sol[IDX(i, j + 1, k)]) { acc += num2 * p[IDX(i, j + 1, k)]; den += num2; }
+        if (!sol[IDX(i, j - 1, k)]) { acc += num2 * p[IDX(i, j - 1, k)]; den += num2; }
+        if (!sol[IDX(i, j, ke)]) { acc += num3 * p[IDX(i, j, ke)]; den += num3; }
+        if (!sol[IDX(i, j, kw)]) { acc += num3 * p[IDX(i, j, kw)]; den += num3; }
+    } else {
+        den = 2.0 * num1 + 2.0 * num2 + 2.0 * num3;
+        acc = (p[IDX(i + 1, j, k)] + p[IDX(i - 1, j, k)]) * num1
+            + (p[IDX(i, j + 1, k)] + p[IDX(i, j - 1, k)]) * num2
+            + (p[IDX(i, j, ke)] + p[IDX(i, j, kw)]) * num3;
+    }
+    *acc_out = acc;
+    return den;
+}
+
+/* Boundary folds after each sweep (718-746): 2-point Neumann in r, then theta, seam copy. */
+static void press_fold(const AtjupParams* P, double* p) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    for (int k = 0; k < km; k++)
+        for (int j = 0; j < jm; j++) {
+            p[IDX(0, j, k)] = C43 * p[IDX(1, j, k)] - C13 * p[IDX(2, j, k)];
+            p[IDX(im - 1, j, k)] = C43 * p[IDX(im - 2, j, k)] - C13 * p[IDX(im - 3, j, k)];
+        }
+    for (int k = 0; k < km; k++)
+        for (int i = 0; i < im; i++) {
+            p[IDX(i, 0, k)] = C43 * p[IDX(i, 1, k)] - C13 * p[IDX(i, 2, k)];
+            p[IDX(i, jm - 1, k)] = C43 * p[IDX(i, jm - 2, k)] - C13 * p[IDX(i, jm - 3, k)];
+        }
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++) p[IDX(i, j, km - 1)] = p[IDX(i, j, 0)];
+}
+
+void ora_pressure_source(const AtjupParams* P, const ora_grid* G, ora_state* S, double* src) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    memset(src, 0, sizeof(double) * (size_t)im * jm * km);
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 1; j < jm - 1; j++) {
+            geom g; double n1, n2, n3;
+            press_weights(P, G, i, j, &g, &n1, &n2, &n3);
+            for (int k = 0; k < km - 1; k++) {
+                double acc;
+                const double den = press_gather(P, G, S->p_dyn, i, j, k, n1, n2, n3, &acc);
+                if (den <= 0.0) continue;
+                src[IDX(i, j, k)] = pressure_cell_source(P, G, S, i, j, k, den, &g);
+            }
+        }
+}
+
+void ora_pressure_sweeps(const AtjupParams* P, const ora_grid* G, ora_state* S, int sweeps,
+                         double omega, const double* b) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    ora_prepare_projection(P, G, S);
+    double* p = S->p_dyn;
+    for (int sweep = 0; sweep < sweeps; sweep++) {
+        for (int colour = 0; colour < 2; colour++) {
+            for (int i = 1; i < im - 1; i++)
+                for (int j = 1; j < jm - 1; j++) {
+                    geom g; double n1, n2, n3;
+                    press_weights(P, G, i, j, &g, &n1, &n2, &n3);
+                    for (int k = 0; k < km - 1; k++) {
+                        if (((i + j + k) & 1) != colour) continue;
+                        double acc;
+                        const double den = press_gather(P, G, p, i, j, k, n1, n2, n3, &acc);
+                        if (den <= 0.0) continue;
+                        const double src = b ? b[IDX(i, j, k)]
+                                             : pressure_cell_source(P, G, S, i, j, k, den, &g);
+                        const double pgs = (acc - src) / den;
+                        p[IDX(i, j, k)] = (omega == 1.0) ? pgs
+                                        : p[IDX(i, j, k)] + omega * (pgs - p[IDX(i, j, k)]);
+                    }
+                }
+        }
+        press_fold(P, p);
+    }
+}
+
+/* A p = sum over kept faces of num (p_nb - p), with the boundary values read as the folds set
+ * them from the interior (the fixed point of the sweep satisfies A p = src).                  */
+void ora_pressure_apply(const AtjupParams* P, const ora_grid* G, const double* p_in, double* Ap) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const size_t N = (size_t)im * jm * km;
+    double* p = (double*)malloc(sizeof(double) * N);
+    memcpy(p, p_in, sizeof(double) * N);
+    press_fold(P, p);
+    memset(Ap, 0, sizeof(double) * N);
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 1; j < jm - 1; j++) {
+            geom g; double n1, n2, n3;
+            press_weights(P, G, i, j, &g, &n1, &n2, &n3);
+            for (int k = 0; k < km - 1; k++) {
+                double acc;
+                const double den = press_gather(P, G, p, i, j, k, n1, n2, n3, &acc);
+                if (den <= 0.0) continue;
+                Ap[IDX(i, j, k)] = acc - den * p[IDX(i, j, k)];
+            }
+        }
+    free(p);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+void ora_mixture_density(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    (void)G;
+    const double pdyn_w = P->rho_pdyn ? 1.0 : 0.0;
+    const size_t N = (size_t)im * jm * km;
+    for (size_t c = 0; c < N; c++) {
+        const double T = S->t[c] * P->t_ref;
+        if (!(T > 0.0)) { S->rho_mix[c] = 0.0; continue; }
+        const double p_pa = (S->p_stat[c] + pdyn_w * S->p_dyn[c] * P->p_dyn_to_bar) * 1.0e5;
+        const double rho = p_pa / (P->R_mix * T);
+        S->rho_mix[c] = isfinite(rho) ? rho : 0.0;
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* BC_Jup.h:185-263 wrapping BoundaryConditions.h:151-250 for the dynamics fields t, u, v, w:
+ * zonal means of v, w at levels im-3, im-2 before the pass; 2-point Neumann at both radial
+ * walls; rigid lid u = 0; the top taper, then the zonal-mean-preserving sponge (taper 3).     */
+void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km, kn = km - 1;
+    (void)G;
+    double* zm = NULL;
+    if (P->top_taper == 3) {
+        zm = (double*)calloc((size_t)4 * jm, sizeof(double));
+        for (int j = 0; j < jm; j++)
+            for (int l = 0; l < 2; l++) {
+                const int i = im - 3 + l;
+                double sv = 0.0, sw = 0.0;
+                for (int k = 0; k < kn; k++) { sv += S->v[IDX(i, j, k)]; sw += S->w[IDX(i, j, k)]; }
+                zm[(size_t)(2 * l) * jm + j] = sv / kn;
+                zm[(size_t)(2 * l + 1) * jm + j] = sw / kn;
+            }
+    }
+    double* F[4] = {S->t, S->u, S->v, S->w};
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++)
+            for (int f = 0; f < 4; f++) {
+                F[f][IDX(0, j, k)] = C43 * F[f][IDX(1, j, k)] - C13 * F[f][IDX(2, j, k)];
+                F[f][IDX(im - 1, j, k)] = C43 * F[f][IDX(im - 2, j, k)] - C13 * F[f][IDX(im - 3, j, k)];
+            }
+    if (P->lid_u)
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) { S->u[IDX(0, j, k)] = 0.0; S->u[IDX(im - 1, j, k)] = 0.0; }
+    if (P->top_taper != 0) {
+        const int iml = im - 1;
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) {
+                S->v[IDX(iml, j, k)] = 0.0;
+                S->w[IDX(iml, j, k)] = 0.0;
+                if (P->top_taper == 2) {
+                    S->v[IDX(iml - 1, j, k)] = (1.0 / 3.0) * S->v[IDX(iml - 3, j, k)];
+                    S->w[IDX(iml - 1, j, k)] = (1.0 / 3.0) * S->w[IDX(iml - 3, j, k)];
+                    S->v[IDX(iml - 2, j, k)] = (2.0 / 3.0) * S->v[IDX(iml - 3, j, k)];
+                    S->w[IDX(iml - 2, j, k)] = (2.0 / 3.0) * S->w[IDX(iml - 3, j, k)];
+                } else {
+                    S->v[IDX(iml - 1, j, k)] *= (1.0 / 3.0);
+                    S->w[IDX(iml - 1, j, k)] *= (1.0 / 3.0);
+                    S->v[IDX(iml - 2, j, k)] *= (2.0 / 3.0);
+                    S->w[IDX(iml - 2, j, k)] *= (2.0 / 3.0);
+                }
+            }
+    }
+    if (zm) {
+        for (int j = 0; j < jm; j++) {
+            const double v3 = zm[j], w3 = zm[(size_t)jm + j];
+            const double v2 = zm[(size_t)2 * jm + j], w2 = zm[(size_t)3 * jm + j];
+            for (int k = 0; k < km; k++) {
+                S->v[IDX(im - 3, j, k)] += (1.0 / 3.0) * v3;
+                S->w[IDX(im - 3, j, k)] += (1.0 / 3.0) * w3;
+                S->v[IDX(im - 2, j, k)] += (2.0 / 3.0) * v2;
+                S->w[IDX(im - 2, j, k)] += (2.0 / 3.0) * w2;
+                S->v[IDX(im - 1, j, k)] = v2;
+                S->w[IDX(im - 1, j, k)] = w2;
+            }
+        }
+        free(zm);
+    }
+}
+
+/* BoundaryConditions.h:253-336: fill the rows next to the poles that the RK step does not
+ * integrate (copy for t, u; ramp for v, w), then pole rows (copy; v = w = 0).                 */
+void ora_bc_theta(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    (void)G;
+    const int nfill = P->pole_fill_rows;
+    double* X[2] = {S->t, S->u};
+    double* Z[2] = {S->v, S->w};
+    for (int k = 0; k < km; k++)
+        for (int i = 0; i < im; i++) {
+            if (nfill > 0) {
+                const int jf = nfill + 1;
+                for (int r = 1; r <= nfill; r++) {
+                    const double ramp = (double)r / (double)jf;
+                    for (int f = 0; f < 2; f++) {
+                        X[f][IDX(i, r, k)] = X[f][IDX(i, jf, k)];
+                        X[f][IDX(i, jm - 1 - r, k)] = X[f][IDX(i, jm - 1 - jf, k)];
+                    }
+                    for (int f = 0; f < 2; f++) {
+                        Z[f][IDX(i, r, k)] = ramp * Z[f][IDX(i, jf, k)];
+                        Z[f][IDX(i, jm - 1 - r, k)] = ramp * Z[f][IDX(i, jm - 1 - jf, k)];
+                    }
+                }
+            }
+            for (int f = 0; f < 2; f++) { Z[f][IDX(i, 0, k)] = 0.0; Z[f][IDX(i, jm - 1, k)] = 0.0; }
+            for (int f = 0; f < 2; f++) {
+                X[f][IDX(i, 0, k)] = X[f][IDX(i, 1, k)];              /* pole copy (form COPY) */
+                X[f][IDX(i, jm - 1, k)] = X[f][IDX(i, jm - 2, k)];
+            }
+        }
+}
+
+/* BoundaryConditions.h:339-360: periodic seam, k = km-1 is the copy of k = 0. */
+void ora_bc_phi(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    (void)G;
+    double* F[4] = {S->t, S->u, S->v, S->w};
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++)
+            for (int f = 0; f < 4; f++) F[f][IDX(i, j, km - 1)] = F[f][IDX(i, j, 0)];
+}
+
+/* BC_Jup.h:460-658 for the dynamics fields: velocities 0 in solid cells; surface cells take
+ * the 2-point extrapolation of t, p_stat, p_dyn from the first direction with two fluid cells
+ * (+i, -i, +j, -j, +k, -k), interior cells p_dyn = 0; then solid t = ambient row mean.        */
+void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const uint8_t* sol = G->solid;
+#define SOLID(ii, jj, kk) (((ii) < 0 || (ii) >= im || (jj) < 0 || (jj) >= jm || (kk) < 0 || (kk) >= km) ? 1 : sol[IDX(ii, jj, kk)])
+#define FLUID(ii, jj, kk) (((ii) < 0 || (ii) >= im || (jj) < 0 || (jj) >= jm || (kk) < 0 || (kk) >= km) ? 0 : !sol[IDX(ii, jj, kk)])
+    double* sc[3] = {S->t, S->p_stat, S->p_dyn};
+    const int n_state = 2;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++)
+            for (int i = 0; i < im; i++) {
+                const size_t c = IDX(i, j, k);
+                if (!sol[c]) continue;
+                S->u[c] = 0.0; S->v[c] = 0.0; S->w[c] = 0.0;
+                const int surf = !SOLID(i + 1, j, k) || !SOLID(i - 1, j, k) || !SOLID(i, j + 1, k)
+                              || !SOLID(i, j - 1, k) || !SOLID(i, j, k + 1) || !SOLID(i, j, k - 1);
+                if (!surf) { for (int f = n_state; f < 3; f++) sc[f][c] = 0.0; continue; }
+                int ok = 1; size_t a = 0, b = 0;
+                if (FLUID(i + 1, j, k) && FLUID(i + 2, j, k)) { a = IDX(i + 1, j, k); b = IDX(i + 2, j, k); }
+                else if (FLUID(i - 1, j, k) && FLUID(i - 2, j, k)) { a = IDX(i - 1, j, k); b = IDX(i - 2, j, k); }
+                else if (FLUID(i, j + 1, k) && FLUID(i, j + 2, k)) { a = IDX(i, j + 1, k); b = IDX(i, j + 2, k); }
+                else if (FLUID(i, j - 1, k) && FLUID(i, j - 2, k)) { a = IDX(i, j - 1, k); b = IDX(i, j - 2, k); }
+                else if (FLUID(i, j, k + 1) && FLUID(i, j, k + 2)) { a = IDX(i, j, k + 1); b = IDX(i, j, k + 2); }
+                else if (FLUID(i, j, k - 1) && FLUID(i, j, k - 2)) { a = IDX(i, j, k - 1); b = IDX(i, j, k - 2); }
+                else ok = 0;
+                if (ok) { for (int f = 0; f < 3; f++) sc[f][c] = C43 * sc[f][a] - C13 * sc[f][b]; }
+                else { for (int f = n_state; f < 3; f++) sc[f][c] = 0.0; }
+            }
+    if (P->mount_t_ambient)
+        for (int i = 0; i < im; i++)
+            for (int j = 0; j < jm; j++) {
+                double s = 0.0; int n = 0, any = 0;
+                for (int k = 0; k < km; k++) {
+                    if (sol[IDX(i, j, k)]) { any = 1; continue; }
+                    s += S->t[IDX(i, j, k)]; n++;
+                }
+                if (!any || n == 0) continue;
+                const double t_amb = s / n;
+                for (int k = 0; k < km; k++) if (sol[IDX(i, j, k)]) S->t[IDX(i, j, k)] = t_amb;
+            }
+#undef SOLID
+#undef FLUID
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* lib/Utils.cpp:227-453. Direction-split k (periodic ring of km-1, seam copy), j (clamped),
+ * i (clamped at the fluid floor); every pass reads a full copy of the field.                 */
+void ora_shapiro(const AtjupParams* P, const ora_grid* G, double* f, int order, double strength,
+                 int passes, int use_topo) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const size_t N = (size_t)im * jm * km;
+    double* tmp = (double*)malloc(sizeof(double) * N);
+    const double c4 = strength / 16.0, c2 = strength * 0.25;
+#define TOPO(jj, kk) (use_topo ? (G->topo[(size_t)(jj) * km + (kk)] > 0 ? G->topo[(size_t)(jj) * km + (kk)] : 0) : 0)
+#define INF(ii, jj, kk) ((ii) >= TOPO(jj, kk))
+    for (int pass = 0; pass < passes; pass++) {
+        /* k */
+        memcpy(tmp, f, sizeof(double) * N);
+        for (int i = 0; i < im; i++)
+            for (int j = 0; j < jm; j++) {
+                if (order == 4) {
+                    const int n_k = km - 1;
+                    for (int k = 0; k < n_k; k++) {
+                        if (!INF(i, j, k)) continue;
+                        const int km1 = (k - 1 + n_k) % n_k, kp1 = (k + 1) % n_k;
+                        const int km2 = (k - 2 + n_k) % n_k, kp2 = (k + 2) % n_k;
+                        const double cc = tmp[IDX(i, j, k)];
+                        if (!INF(i, j, km1) || !INF(i, j, kp1)) continue;
+                        if (INF(i, j, km2) && INF(i, j, kp2)) {
+                            const double d4 = tmp[IDX(i, j, kp2)] - 4.0 * tmp[IDX(i, j, kp1)]
+                                + 6.0 * cc - 4.0 * tmp[IDX(i, j, km1)] + tmp[IDX(i, j, km2)];
+                            f[IDX(i, j, k)] = cc - c4 * d4;
+                        } else {
+                            f[IDX(i, j, k)] = cc + c2 * (tmp[IDX(i, j, km1)] - 2.0 * cc + tmp[IDX(i, j, kp1)]);
+                        }
+                    }
+                } else {
+                    for (int k = 0; k < km - 1; k++) {
+                        if (!INF(i, j, k)) continue;
+                        const int km1 = (k == 0) ? km - 2 : k - 1;
+                        const int kp1 = (k == km - 2) ? 0 : k + 1;
+                        const double v_km1 = INF(i, j, km1) ? tmp[IDX(i, j, km1)] : tmp[IDX(i, j, k)];
+                        const double v_kp1 = INF(i, j, kp1) ? tmp[IDX(i, j, kp1)] : tmp[IDX(i, j, k)];
+                        f[IDX(i, j, k)] = tmp[IDX(i, j, k)] + c2 * (v_km1 - 2.0 * tmp[IDX(i, j, k)] + v_kp1);
+                    }
+                }
+                f[IDX(i, j, km - 1)] = f[IDX(i, j, 0)];
+            }
+        /* j */
+        memcpy(tmp, f, sizeof(double) * N);
+        for (int i = 0; i < im; i++)
+            for (int j = 0; j < jm; j++)
+                for (int k = 0; k < km; k++) {
+                    if (!INF(i, j, k)) continue;
+                    const double cc = tmp[IDX(i, j, k)];
+                    if (order == 4) {
+                        const int fm1 = (j - 1 >= 0) && INF(i, j - 1, k);
+                        const int fp1 = (j + 1 <= jm - 1) && INF(i, j + 1, k);
+                        if (!fm1 || !fp1) continue;
+                        const int fm2 = (j - 2 >= 0) && INF(i, j - 2, k);
+                        const int fp2 = (j + 2 <= jm - 1) && INF(i, j + 2, k);
+                        if (fm2 && fp2) {
+                            const double d4 = tmp[IDX(i, j + 2, k)] - 4.0 * tmp[IDX(i, j + 1, k)]
+                                + 6.0 * cc - 4.0 * tmp[IDX(i, j - 1, k)] + tmp[IDX(i, j - 2, k)];
+                            f[IDX(i, j, k)] = cc - c4 * d4;
+                        } else {
+                            f[IDX(i, j, k)] = cc + c2 * (tmp[IDX(i, j - 1, k)] - 2.0 * cc + tmp[IDX(i, j + 1, k)]);
+                        }
+                    } else {
+                        const int jm1 = j - 1 > 0 ? j - 1 : 0, jp1 = j + 1 < jm - 1 ? j + 1 : jm - 1;
+                        const double v_jm1 = INF(i, jm1, k) ? tmp[IDX(i, jm1, k)] : cc;
+                        const double v_jp1 = INF(i, jp1, k) ? tmp[IDX(i, jp1, k)] : cc;
+                        f[IDX(i, j, k)] = cc + c2 * (v_jm1 - 2.0 * cc + v_jp1);
+                    }
+                }
+        /* i */
+        memcpy(tmp, f, sizeof(double) * N);
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) {
+                const int i_surf = TOPO(j, k);
+                for (int i = i_surf; i < im; i++) {
+                    const double cc = tmp[IDX(i, j, k)];
+                    if (order == 4) {
+                        const int fm1 = (i - 1 >= i_surf), fp1 = (i + 1 <= im - 1);
+                        if (!fm1 || !fp1) continue;
+                        const int fm2 = (i - 2 >= i_surf), fp2 = (i + 2 <= im - 1);
+                        if (fm2 && fp2) {
+                            const double d4 = tmp[IDX(i + 2, j, k)] - 4.0 * tmp[IDX(i + 1, j, k)]
+                                + 6.0 * cc - 4.0 * tmp[IDX(i - 1, j, k)] + tmp[IDX(i - 2, j, k)];
+                            f[IDX(i, j, k)] = cc - c4 * d4;
+                        } else {
+                            f[IDX(i, j, k)] = cc + c2 * (tmp[IDX(i - 1, j, k)] - 2.0 * cc + tmp[IDX(i + 1, j, k)]);
+                        }
+                    } else {
+                        const int im1 = i - 1 > i_surf ? i - 1 : i_surf, ip1 = i + 1 < im - 1 ? i + 1 : im - 1;
+                        f[IDX(i, j, k)] = cc + c2 * (tmp[IDX(im1, j, k)] - 2.0 * cc + tmp[IDX(ip1, j, k)]);
+                    }
+                }
+            }
+    }
+#undef TOPO
+#undef INF
+    free(tmp);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* InitValues_Jup.cpp:1500-1538: trapezoid column mean of r v over columns off the obstacle;
+ * zonal form (default with ATJUP_VORTEX): per latitude the mean over meridians k < km-1 of the
+ * column means is removed from every off-obstacle column of the row, all levels.              */
+double ora_balance_column_v(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    double vshift = 0.0;
+    double* dvc = (double*)calloc((size_t)jm * km, sizeof(double));
+    for (int j = 1; j < jm - 1; j++)
+        for (int k = 0; k < km; k++) {
+            const int i0 = G->topo[(size_t)j * km + k];
+            if (i0 > 0) continue;
+            double I1 = 0.0, I0 = 0.0;
+            for (int i = i0; i < im - 1; i++) {
+                I1 += 0.5 * (G->rad[i] * S->v[IDX(i, j, k)] + G->rad[i + 1] * S->v[IDX(i + 1, j, k)]) * P->dr;
+                I0 += 0.5 * (G->rad[i] + G->rad[i + 1]) * P->dr;
+            }
+            const double dv = I1 / I0;
+            if (P->v_massbal_zonal) { dvc[(size_t)j * km + k] = dv; continue; }
+            for (int i = i0; i < im; i++) S->v[IDX(i, j, k)] -= dv;
+            if (fabs(dv) > vshift) vshift = fabs(dv);
+        }
+    if (P->v_massbal_zonal)
+        for (int j = 1; j < jm - 1; j++) {
+            double s = 0.0; int n = 0;
+            for (int k = 0; k < km - 1; k++)
+                if (G->topo[(size_t)j * km + k] == 0) { s += dvc[(size_t)j * km + k]; n++; }
+            if (!n) continue;
+            const double dv = s / n;
+            for (int k = 0; k < km; k++) {
+                if (G->topo[(size_t)j * km + k] > 0) continue;
+                for (int i = 0; i < im; i++) S->v[IDX(i, j, k)] -= dv;
+            }
+            if (fabs(dv) > vshift) vshift = fabs(dv);
+        }
+    free(dvc);
+    return vshift;
+}
+
+void ora_restore(const AtjupParams* P, ora_state* S) {
+    const size_t N = (size_t)P->im * P->jm * P->km;
+    memcpy(S->tn, S->t, sizeof(double) * N);
+    memcpy(S->un, S->u, sizeof(double) * N);
+    memcpy(S->vn, S->v, sizeof(double) * N);
+    memcpy(S->wn, S->w, sizeof(double) * N);
+}
+
+/* cJupiterModel.cpp:1032-1381 with the saturation adjustment, chemistry, radiation,
+ * precipitation, turbulence, convective adjustment and cone projection off (dry config). */
+void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
+                       int first, int sweeps) {
+    if (iter_n % 2 == 0 || first) {
+        ora_pressure_sweeps(P, G, S, sweeps, 1.0, NULL);
+        ora_mixture_density(P, G, S);
+    }
+    ora_rk4(P, G, S);
+    ora_bc_radius(P, G, S);
+    ora_bc_theta(P, G, S);
+    ora_bc_phi(P, G, S);
+    ora_bc_solid(P, G, S);
+    if (P->shapiro_inloop > 0) {
+        ora_shapiro(P, G, S->u, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+        ora_shapiro(P, G, S->v, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+        ora_shapiro(P, G, S->w, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+    }
+    if (P->v_massbal_stride > 0 && iter_n % P->v_massbal_stride == 0)
+        ora_balance_column_v(P, G, S);
+    ora_restore(P, S);
+}
+
+/* Size of the parameter block as compiled here, for binding checks. */
+size_t ora_params_sizeof(void) { return sizeof(AtjupParams); }

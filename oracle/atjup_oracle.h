@@ -1,0 +1,88 @@
+/*
+ * CPU oracle for the ATJUP hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference's time-step routines (RogerGrundmann/ATJUP), written
+ * to check the CUDA implementation. Only tests/, __graft_entry__.smoke() and the cpu_baseline
+ * leg of bench.py load it; the product path never links or calls it.
+ *
+ * Parity pin: every routine here is compared, field by field, with the unmodified reference
+ * built from its own sources (oracle/_ref/libatjup_ref.so via oracle/ref_harness.cpp) on the
+ * reference's own initial state, and with the golden digests under tests/golden/ generated
+ * from it (tests/golden/make_golden.py).
+ *
+ * Storage: contiguous (i, j, k) blocks, k fastest, idx = (i*jm + j)*km + k -- the same order as
+ * the reference's x[i][j][k]. Any im, jm, km >= 5 works (the reference is fixed at 41x181x361;
+ * small grids make fast GPU-vs-oracle tests).
+ */
+#ifndef ATJUP_ORACLE_H
+#define ATJUP_ORACLE_H
+
+#include <stdint.h>
+#include "../include/atjup_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    const double* rad;          /* [im] metric radius                                   */
+    const double* the;          /* [jm] colatitude                                      */
+    const uint8_t* solid;       /* [im*jm*km] SeaMount mask                             */
+    const int32_t* topo;        /* [jm*km] i_topography                                 */
+    const double* cell_vbar0;   /* [im*jm] or NULL                                      */
+    const double* cell_ubar0;   /* [im*jm] or NULL                                      */
+} ora_grid;
+
+typedef struct {
+    double *t, *u, *v, *w;              /* live fields (stage inputs inside the RK step)     */
+    double *tn, *un, *vn, *wn;          /* time-level n copies                                */
+    double *p_dyn, *p_hydro, *p_stat;
+    double *rho_mix, *wall_nue, *nue;   /* nue may be NULL (closure off)                      */
+    double *p_baro;                     /* may be NULL (no geo-balance rest)                  */
+    double *aux_u, *aux_v, *aux_w;
+    double *acc_t, *acc_u, *acc_v, *acc_w;
+    double *rhs_t, *rhs_u, *rhs_v, *rhs_w;
+    double *Q_rad, *Q_precip;           /* may be NULL (no heating)                           */
+    double *buoy_ref;                   /* [im]                                               */
+} ora_state;
+
+/* RungeKutta_Jup_Turb.cpp:47-69 */
+void ora_buoy_ref_level(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* RungeKutta_Jup_Turb.cpp:119-259 (metric/Coriolis split branch and the plain branch) */
+void ora_hydrostatic(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* RHS_Jup_Turb.cpp:31-1457, dynamics part (t, u, v, w, aux) for one cell */
+void ora_rhs_cell(const AtjupParams* P, const ora_grid* G, ora_state* S, int i, int j, int k);
+/* RungeKutta_Jup_Turb.cpp:261-583 for t, u, v, w */
+void ora_rk4(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* cJupiterModel.cpp:1842-1864 */
+void ora_prepare_projection(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* PressureSolver.h:144-766, pointwise red-black branch, `sweeps` sweeps with relaxation omega
+ * (omega = 1 is the reference). b != NULL replaces the divergence source by b (clamp skipped). */
+void ora_pressure_sweeps(const AtjupParams* P, const ora_grid* G, ora_state* S, int sweeps,
+                         double omega, const double* b);
+/* The source the sweep uses at every interior cell (after the clamp) into src[N]. */
+void ora_pressure_source(const AtjupParams* P, const ora_grid* G, ora_state* S, double* src);
+/* A p for the folded-boundary operator the sweep relaxes (interior cells; 0 elsewhere). */
+void ora_pressure_apply(const AtjupParams* P, const ora_grid* G, const double* p, double* Ap);
+/* InitValues_Jup.cpp:717-740 */
+void ora_mixture_density(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* BC_Jup.h:185-263 + BoundaryConditions.h bcRadius/bcTheta/bcPhi; BC_Jup.h:460-658 */
+void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S);
+void ora_bc_theta(const AtjupParams* P, const ora_grid* G, ora_state* S);
+void ora_bc_phi(const AtjupParams* P, const ora_grid* G, ora_state* S);
+void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* lib/Utils.cpp:227-323 (order 2) and 334-453 (order 4) */
+void ora_shapiro(const AtjupParams* P, const ora_grid* G, double* f, int order, double strength,
+                 int passes, int use_topo);
+/* InitValues_Jup.cpp:1500-1538 */
+double ora_balance_column_v(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* restoreVar (cJupiterModel.cpp:1757-1801) for the dynamics fields */
+void ora_restore(const AtjupParams* P, ora_state* S);
+/* One dry iteration of cJupiterModel.cpp:1032-1381 */
+void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
+                       int first, int sweeps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,216 @@
+"""Test-side access to the CPU oracle (oracle/liboracle.so) and to the reference harness
+(oracle/_ref/libatjup_ref.so). Test infrastructure only: the product never imports this."""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from atjup_b200.params import AtjupParams, resolve_params
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_SO = ROOT / "oracle" / "liboracle.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libatjup_ref.so"
+
+# The dry configuration: obstacle on, microphysics / radiation / turbulence / MCA / cone
+# projection off, in-loop 4th-order Shapiro on u, v, w (BASELINE config 0 knobs).
+DRY_ENV = {
+    "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
+    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
+    "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
+    "ATJUP_RESTART_STRIDE": "0", "ATJUP_VTK_STRIDE": "100000", "ATJUP_PANORAMA_STRIDE": "100000",
+}
+
+DYN_FIELDS = ["t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wall_nue",
+              "aux_u", "aux_v", "aux_w"]
+
+
+def build_oracle() -> Path:
+    if not ORACLE_SO.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True, capture_output=True)
+    return ORACLE_SO
+
+
+_P = ctypes.POINTER
+
+
+class OraGrid(ctypes.Structure):
+    _fields_ = [("rad", _P(ctypes.c_double)), ("the", _P(ctypes.c_double)),
+                ("solid", _P(ctypes.c_uint8)), ("topo", _P(ctypes.c_int32)),
+                ("cell_vbar0", _P(ctypes.c_double)), ("cell_ubar0", _P(ctypes.c_double))]
+
+
+_STATE_NAMES = ["t", "u", "v", "w", "tn", "un", "vn", "wn", "p_dyn", "p_hydro", "p_stat",
+                "rho_mix", "wall_nue", "nue", "p_baro", "aux_u", "aux_v", "aux_w",
+                "acc_t", "acc_u", "acc_v", "acc_w", "rhs_t", "rhs_u", "rhs_v", "rhs_w",
+                "Q_rad", "Q_precip", "buoy_ref"]
+
+
+class OraState(ctypes.Structure):
+    _fields_ = [(n, _P(ctypes.c_double)) for n in _STATE_NAMES]
+
+
+def _dp(a):
+    return a.ctypes.data_as(_P(ctypes.c_double)) if a is not None else None
+
+
+class Oracle:
+    """Holds a grid + state as numpy arrays and runs oracle routines on them in place."""
+
+    def __init__(self, params: AtjupParams, grid: dict, fields: dict):
+        self.lib = ctypes.CDLL(str(build_oracle()))
+        self.P = params
+        im, jm, km = params.im, params.jm, params.km
+        self.shape = (im, jm, km)
+        self.g = {k: np.ascontiguousarray(v) for k, v in grid.items()}
+        self.g["rad"] = self.g["rad"].astype(np.float64)
+        self.g["the"] = self.g["the"].astype(np.float64)
+        self.g["solid"] = self.g["solid"].astype(np.uint8)
+        self.g["topo"] = self.g["topo"].astype(np.int32)
+        self.G = OraGrid(_dp(self.g["rad"]), _dp(self.g["the"]),
+                         self.g["solid"].ctypes.data_as(_P(ctypes.c_uint8)),
+                         self.g["topo"].ctypes.data_as(_P(ctypes.c_int32)),
+                         _dp(self.g.get("cell_vbar0")), _dp(self.g.get("cell_ubar0")))
+        self.f = {}
+        for n in _STATE_NAMES:
+            if n == "buoy_ref":
+                self.f[n] = np.zeros(im)
+            elif n in fields and fields[n] is not None:
+                self.f[n] = np.ascontiguousarray(fields[n], dtype=np.float64).reshape(self.shape).copy()
+            elif n in ("nue", "p_baro", "Q_rad", "Q_precip"):
+                self.f[n] = None
+            else:
+                self.f[n] = np.zeros(self.shape)
+        for a, b in (("tn", "t"), ("un", "u"), ("vn", "v"), ("wn", "w")):
+            if a not in fields:
+                self.f[a][...] = self.f[b]
+        self.S = OraState(*[_dp(self.f[n]) for n in _STATE_NAMES])
+        self.lib.ora_balance_column_v.restype = ctypes.c_double
+
+    def call(self, name, *args):
+        fn = getattr(self.lib, name)
+        return fn(ctypes.byref(self.P), ctypes.byref(self.G), ctypes.byref(self.S), *args)
+
+    def rk4(self):
+        self.call("ora_rk4")
+
+    def iteration(self, iter_n, first, sweeps=1):
+        self.call("ora_iteration_dry", ctypes.c_int(iter_n), ctypes.c_int(first), ctypes.c_int(sweeps))
+
+    def pressure(self, sweeps=1, omega=1.0, b=None):
+        self.call("ora_pressure_sweeps", ctypes.c_int(sweeps), ctypes.c_double(omega),
+                  _dp(b) if b is not None else None)
+
+    def shapiro(self, name, order, strength=1.0, passes=1, use_topo=1):
+        self.lib.ora_shapiro(ctypes.byref(self.P), ctypes.byref(self.G), _dp(self.f[name]),
+                             ctypes.c_int(order), ctypes.c_double(strength), ctypes.c_int(passes),
+                             ctypes.c_int(use_topo))
+
+    def apply_A(self, p):
+        out = np.zeros(self.shape)
+        pp = np.ascontiguousarray(p, dtype=np.float64)
+        self.lib.ora_pressure_apply(ctypes.byref(self.P), ctypes.byref(self.G), _dp(pp), _dp(out))
+        return out
+
+    def source(self):
+        out = np.zeros(self.shape)
+        self.call("ora_pressure_source", _dp(out))
+        return out
+
+
+class Reference:
+    """The unmodified reference (oracle/_ref/libatjup_ref.so), one model per process."""
+
+    def __init__(self, env: dict, out_dir: str, threads: int = 0, zero_species: bool = True):
+        os.environ.update(env)
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref)")
+        L = ctypes.CDLL(str(REF_SO))
+        L.ref_scalar.restype = ctypes.c_double
+        L.ref_knob_d.restype = ctypes.c_double
+        L.ref_balance_v.restype = ctypes.c_double
+        self.L = L
+        L.ref_quiet(1)
+        rc = L.ref_create(out_dir.encode(), threads)
+        L.ref_quiet(0)
+        if rc != 0:
+            raise RuntimeError(f"ref_create failed rc={rc}")
+        im, jm, km = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.ref_dims(ctypes.byref(im), ctypes.byref(jm), ctypes.byref(km))
+        self.shape = (im.value, jm.value, km.value)
+        if zero_species:
+            z = np.zeros(self.shape)
+            for n in ("h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3", "nh3_cloud", "nh3_ice",
+                      "ch4", "ch4_cloud", "ch4_ice", "nh4sh", "h2on", "h2o_cloudn", "h2o_icen",
+                      "h2sn", "nh3n", "nh3_cloudn", "nh3_icen", "ch4n", "ch4_cloudn", "ch4_icen",
+                      "nh4shn"):
+                self.set(n, z)
+
+    def scalar(self, n):
+        return self.L.ref_scalar(n.encode())
+
+    def get(self, n):
+        a = np.empty(self.shape)
+        if self.L.ref_get3(n.encode(), a.ctypes.data_as(ctypes.c_void_p)) != 0:
+            raise KeyError(n)
+        return a
+
+    def set(self, n, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if self.L.ref_set3(n.encode(), a.ctypes.data_as(ctypes.c_void_p)) != 0:
+            raise KeyError(n)
+
+    def get1(self, n):
+        cap = self.shape[0] * self.shape[1] * self.shape[2]
+        a = np.empty(cap)
+        m = self.L.ref_get1(n.encode(), a.ctypes.data_as(ctypes.c_void_p), cap)
+        if m < 0:
+            raise KeyError(n)
+        return a[:m].copy()
+
+    def topo(self):
+        a = np.empty(self.shape[1] * self.shape[2], dtype=np.int32)
+        self.L.ref_get_topo(a.ctypes.data_as(ctypes.c_void_p))
+        return a.reshape(self.shape[1], self.shape[2])
+
+    def quiet(self, fn, *args):
+        self.L.ref_quiet(1)
+        try:
+            return fn(*args)
+        finally:
+            self.L.ref_quiet(0)
+
+    def params(self, env: dict | None = None) -> AtjupParams:
+        """AtjupParams with the model's own constants (the knobs resolved from env)."""
+        consts = {n: self.scalar(n) for n in ("dt", "re", "pr", "g", "omega", "u_0", "t_ref",
+                                              "L_atm", "r_mix", "R_mix", "cp_mix", "Coriolis",
+                                              "centrifugal", "buoyancy")}
+        im, jm, km = self.shape
+        return resolve_params(env if env is not None else os.environ, im=im, jm=jm, km=km,
+                              constants=consts)
+
+    def grid(self) -> dict:
+        im, jm, km = self.shape
+        g = {"rad": self.get1("rad"), "the": self.get1("the"),
+             "solid": (self.get("SeaMount") == 1.0).astype(np.uint8), "topo": self.topo()}
+        if self.scalar("cell_hold") == 1.0:
+            g["cell_vbar0"] = self.get1("cell_vbar0")
+            g["cell_ubar0"] = self.get1("cell_ubar0")
+        return g
+
+    def fields(self, names=DYN_FIELDS) -> dict:
+        out = {n: self.get(n) for n in names}
+        if self.scalar("has_p_baro") == 1.0:
+            out["p_baro"] = self.get1("p_baro").reshape(self.shape)
+        return out
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return d / n if n > 0 else d
