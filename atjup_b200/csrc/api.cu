@@ -1,0 +1,535 @@
+// C ABI of the B200 hot path: context, geometry, field transfer and the step schedule.
+// The declarations and the reference routine each entry point replaces are in
+// include/atjup_gpu.h.
+#include "ctx.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace atjup {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+int cuda_status(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return ATJUP_ERR_CUDA;
+}
+
+void timer_begin(AtjupCtx* c, int cls) {
+    if (!c->timing) return;
+    if ((size_t)(2 * c->tn + 2) > c->tev.size()) {
+        for (int q = 0; q < 512; q++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) { c->timing = false; return; }
+            c->tev.push_back(e);
+        }
+    }
+    c->tcls.resize(c->tn + 1);
+    c->tcls[c->tn] = cls;
+    cudaEventRecord(c->tev[2 * c->tn], c->stream);
+}
+
+void timer_end(AtjupCtx* c) {
+    if (!c->timing) return;
+    cudaEventRecord(c->tev[2 * c->tn + 1], c->stream);
+    c->tn++;
+}
+
+namespace {
+
+struct Timed {
+    AtjupCtx* c;
+    Timed(AtjupCtx* c_, int cls) : c(c_) { timer_begin(c, cls); }
+    ~Timed() { timer_end(c); }
+};
+
+int alloc(double** p, size_t n) {
+    ATJUP_CUDA(cudaMalloc(p, n * sizeof(double)));
+    ATJUP_CUDA(cudaMemset(*p, 0, n * sizeof(double)));
+    return ATJUP_OK;
+}
+
+void free_all(AtjupCtx* c) {
+    for (auto& p : c->f) { cudaFree(p); p = nullptr; }
+    for (int q = 0; q < 4; q++) {
+        cudaFree(c->X1[q]); cudaFree(c->X2[q]); cudaFree(c->acc[q]);
+    }
+    for (auto& p : c->kr) { cudaFree(p); p = nullptr; }
+    for (auto& p : c->kf) { cudaFree(p); p = nullptr; }
+    cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red);
+    cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
+    cudaFree(c->solve_b); cudaFree(c->dsum);
+    if (c->hsum) cudaFreeHost(c->hsum);
+    cudaFree(c->solid); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
+    cudaFree(c->sin_the); cudaFree(c->rad); cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
+    cudaFree(c->solid_list); cudaFree(c->amb_rows); cudaFree(c->yw);
+    cudaFree(c->line_a); cudaFree(c->line_c); cudaFree(c->line_m);
+    for (auto e : c->tev) cudaEventDestroy(e);
+    c->tev.clear();
+}
+
+bool valid_field(int id) { return id >= 0 && id < ATJUP_F_COUNT; }
+
+// The Krylov/IR vectors are allocated on first use of the residual solver.
+}  // namespace
+}  // namespace atjup
+
+using namespace atjup;
+
+extern "C" {
+
+void atjup_params_default(AtjupParams* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->abi_version = ATJUP_ABI_VERSION;
+    p->im = 41; p->jm = 181; p->km = 361;
+    p->dr = 0.025;
+    p->dthe = 1.0 / (180.0 / M_PI);
+    p->dphi = 1.0 / (180.0 / M_PI);
+    p->dt = 0.005;
+    p->re = 1000.0; p->pr = 0.69; p->g = 25.92; p->omega = 0.000176; p->u_0 = 100.0;
+    p->t_ref = 165.0; p->L_atm = 140.0;
+    p->r_mix = 1.2843999999999998; p->R_mix = 3531.1847352206946; p->cp_mix = 11810.757033551794;
+    p->Coriolis = 1.0; p->centrifugal = 1.0; p->buoyancy = 1.0;
+    p->sinthe_min = 0.55;
+    p->p_dyn_to_bar = p->r_mix * p->u_0 * p->u_0 * 1.0e-5;
+    p->t_diff_scale = 0.01;
+    p->nd_cor = p->L_atm * 1.0e3 / p->u_0;
+    p->nd_cent = 1.0; p->nd_buoy = 1.0;
+    p->buoy_scale = 1.0; p->buoy_ramp = 1.0; p->pgrad_scale = 1.0;
+    p->rad_coupling = 1.0; p->precip_coupling = 1.0; p->turb_coupling = 1.0;
+    p->pgrad_wall = 1; p->pgrad_wrap = 1; p->adiabatic = 1; p->adiabatic_rho = 1;
+    p->metric_split = 1; p->coriolis_split = 1; p->hydro_split = 0; p->cell_hold = 1;
+    p->precip_rho_local = 1; p->local_rho = 1; p->rho_pdyn = 0;
+    p->has_nue = 0; p->has_heating = 0;
+    p->p_dyn_cap = 0.2; p->press_wall = 1; p->rigid_lid = 1; p->press_sweeps = 1;
+    p->top_taper = 3; p->lid_u = 1; p->pole_fill_rows = 2; p->mount_t_ambient = 1;
+    p->shapiro_inloop = 0; p->shapiro_strength = 1.0;
+    p->v_massbal_stride = 1; p->v_massbal_zonal = 1;
+    p->precision = ATJUP_PREC_FP64;
+}
+
+const char* atjup_gpu_last_error(void) { return g_err.c_str(); }
+
+int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
+    if (!params || !out) { set_error("create: null argument"); return ATJUP_ERR_ARG; }
+    *out = nullptr;
+    const AtjupParams& P = *params;
+    if (P.abi_version != ATJUP_ABI_VERSION) { set_error("create: ABI version mismatch"); return ATJUP_ERR_ARG; }
+    if (P.im < 5 || P.jm < 8 || P.km < 8 || ((P.km - 1) & 1)) {
+        set_error("create: need im >= 5, jm >= 8, km >= 8 and an even number km-1 of meridians");
+        return ATJUP_ERR_ARG;
+    }
+    if (!P.pgrad_wrap || !P.press_wall || !P.metric_split || P.hydro_split) {
+        set_error("create: pgrad_wrap, press_wall and metric_split must be 1, hydro_split 0");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    if (P.top_taper < 0 || P.top_taper > 3 || P.pole_fill_rows < 0 || P.pole_fill_rows > 3) {
+        set_error("create: top_taper must be 0..3, pole_fill_rows 0..3");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { cuda_status(e, "cudaGetDevice"); return ATJUP_ERR_NO_DEVICE; }
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) { cuda_status(e, "cudaGetDeviceProperties"); return ATJUP_ERR_NO_DEVICE; }
+    if (prop.major != 10) {
+        set_error("create: this library is built for sm_100a (B200); device is sm_" +
+                  std::to_string(prop.major) + std::to_string(prop.minor));
+        return ATJUP_ERR_NO_DEVICE;
+    }
+    AtjupCtx* c = new AtjupCtx();
+    c->P = P;
+    c->device = dev;
+    c->KP = (P.km + 15) / 16 * 16;
+    c->NP = (size_t)P.im * P.jm * c->KP;
+    int rc = ATJUP_OK;
+    auto A = [&](double** p, size_t n) { if (rc == ATJUP_OK) rc = alloc(p, n); };
+    for (int q = 0; q < ATJUP_F_COUNT; q++) A(&c->f[q], c->NP);
+    for (int q = 0; q < 4; q++) { A(&c->X1[q], c->NP); A(&c->X2[q], c->NP); A(&c->acc[q], c->NP); }
+    A(&c->src, c->NP);
+    A(&c->tmp, c->NP);
+    A(&c->tmp2, c->NP);
+    A(&c->red, 4096);
+    A(&c->buoy_ref, (size_t)P.im);
+    A(&c->zm, (size_t)4 * P.jm);
+    A(&c->dvc, (size_t)P.jm * c->KP);
+    A(&c->dvrow, (size_t)P.jm);
+    if (rc == ATJUP_OK) {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamCreate");
+        else c->own_stream = true;
+    }
+    if (rc != ATJUP_OK) { free_all(c); delete c; return rc; }
+    *out = c;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_destroy(AtjupCtx* c) {
+    if (!c) return ATJUP_OK;
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_set_stream(AtjupCtx* c, void* stream) {
+    if (!c) return ATJUP_ERR_ARG;
+    if (c->own_stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+    if (stream) { c->stream = (cudaStream_t)stream; c->own_stream = false; }
+    else {
+        ATJUP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const uint8_t* solid,
+                       const int32_t* i_topo, const double* cell_vbar0, const double* cell_ubar0) {
+    if (!c || !rad || !the || !solid || !i_topo) { set_error("set_grid: null argument"); return ATJUP_ERR_ARG; }
+    const AtjupParams& P = c->P;
+    const int im = P.im, jm = P.jm, km = P.km, KP = c->KP;
+    // geometry rows, built as RungeKutta_Jup_Turb.cpp:298-303, 388-411 builds them
+    std::vector<GeoIJ> geo((size_t)im * jm);
+    const double A = P.nd_cor * -2.0 * P.omega;
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++) {
+            GeoIJ& g = geo[(size_t)i * jm + j];
+            std::memset(&g, 0, sizeof(g));
+            const double rm = rad[i];
+            const double rm2 = rm * rm;
+            const double sinthe = std::max(P.sinthe_min, std::fabs(std::sin(the[j])));
+            const double sinthe2 = sinthe * sinthe;
+            const double costhe = std::cos(the[j]);
+            g.rm = rm;
+            g.inv_rm = 1.0 / rm;
+            g.inv_rm2 = 1.0 / rm2;
+            g.inv_rmsinthe = 1.0 / (rm * sinthe);
+            g.inv_rm2sinthe = g.inv_rm2 / sinthe;
+            g.inv_rm2sinthe2 = g.inv_rm2 / sinthe2;
+            g.costhe_inv_rm2sinthe = costhe * g.inv_rm2sinthe;
+            g.v_metric = (1.0 + costhe / (sinthe2)) * g.inv_rm2;
+            g.cotanthe = costhe / sinthe;
+            g.costhe = costhe;
+            const double st = std::sqrt(std::max(0.0, 1.0 - costhe * costhe));
+            g.sinthe_true = st;
+            g.cent_rad = P.nd_cent * P.omega * P.omega * rm * st * st;
+            g.cent_the = P.nd_cent * P.omega * P.omega * rm * st * costhe;
+            g.cor_rad = A * st;
+            g.cor_the = A * costhe;
+            g.num2 = g.inv_rm2 * (1.0 / (P.dthe * P.dthe));
+            g.num3 = g.inv_rm2sinthe2 * (1.0 / (P.dphi * P.dphi));
+        }
+    std::vector<double> cor_col(jm), sin_the(jm);
+    for (int j = 0; j < jm; j++) {
+        cor_col[j] = P.coriolis_split ? P.Coriolis * P.nd_cor * 2.0 * P.omega * std::fabs(std::sin(the[j])) : 0.0;
+        sin_the[j] = std::sin(the[j]);
+    }
+    // padded mask
+    std::vector<uint8_t> s_pad(c->NP, 0);
+    for (size_t r = 0; r < (size_t)im * jm; r++)
+        for (int k = 0; k < km; k++) s_pad[r * KP + k] = solid[r * km + k] ? 1 : 0;
+    // solid-cell list for bcSolidGround (BC_Jup.h:496-590): first direction with two fluid cells
+    auto sol = [&](int i, int j, int k) -> bool {
+        if (i < 0 || i >= im || j < 0 || j >= jm || k < 0 || k >= km) return true;
+        return solid[((size_t)i * jm + j) * km + k] != 0;
+    };
+    auto flu = [&](int i, int j, int k) -> bool {
+        if (i < 0 || i >= im || j < 0 || j >= jm || k < 0 || k >= km) return false;
+        return solid[((size_t)i * jm + j) * km + k] == 0;
+    };
+    std::vector<SolidCell> L;
+    std::vector<int32_t> rows;
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++) {
+            bool any = false;
+            for (int k = 0; k < km; k++) {
+                if (!sol(i, j, k)) continue;
+                any = true;
+                SolidCell sc{};
+                sc.c = (int64_t)(((size_t)i * jm + j) * KP + k);
+                const bool surf = !sol(i + 1, j, k) || !sol(i - 1, j, k) || !sol(i, j + 1, k) ||
+                                  !sol(i, j - 1, k) || !sol(i, j, k + 1) || !sol(i, j, k - 1);
+                const int dirs[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+                sc.kind = 0;
+                if (surf)
+                    for (const auto& d : dirs)
+                        if (flu(i + d[0], j + d[1], k + d[2]) && flu(i + 2 * d[0], j + 2 * d[1], k + 2 * d[2])) {
+                            sc.kind = 1;
+                            sc.a = (int64_t)(((size_t)(i + d[0]) * jm + (j + d[1])) * KP + (k + d[2]));
+                            sc.b = (int64_t)(((size_t)(i + 2 * d[0]) * jm + (j + 2 * d[1])) * KP + (k + 2 * d[2]));
+                            break;
+                        }
+                L.push_back(sc);
+            }
+            if (any) rows.push_back(i * jm + j);
+        }
+    if (!c->solid) {
+        ATJUP_CUDA(cudaMalloc(&c->solid, c->NP));
+        ATJUP_CUDA(cudaMalloc(&c->topo, sizeof(int32_t) * (size_t)jm * km));
+        ATJUP_CUDA(cudaMalloc(&c->geo, sizeof(GeoIJ) * geo.size()));
+        ATJUP_CUDA(cudaMalloc(&c->cor_col, sizeof(double) * jm));
+        ATJUP_CUDA(cudaMalloc(&c->sin_the, sizeof(double) * jm));
+        ATJUP_CUDA(cudaMalloc(&c->rad, sizeof(double) * im));
+    }
+    ATJUP_CUDA(cudaMemcpy(c->solid, s_pad.data(), c->NP, cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->topo, i_topo, sizeof(int32_t) * (size_t)jm * km, cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->geo, geo.data(), sizeof(GeoIJ) * geo.size(), cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->cor_col, cor_col.data(), sizeof(double) * jm, cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->sin_the, sin_the.data(), sizeof(double) * jm, cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->rad, rad, sizeof(double) * im, cudaMemcpyHostToDevice));
+    cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
+    c->cell_vbar0 = c->cell_ubar0 = nullptr;
+    if (cell_vbar0 && cell_ubar0) {
+        ATJUP_CUDA(cudaMalloc(&c->cell_vbar0, sizeof(double) * (size_t)im * jm));
+        ATJUP_CUDA(cudaMalloc(&c->cell_ubar0, sizeof(double) * (size_t)im * jm));
+        ATJUP_CUDA(cudaMemcpy(c->cell_vbar0, cell_vbar0, sizeof(double) * (size_t)im * jm, cudaMemcpyHostToDevice));
+        ATJUP_CUDA(cudaMemcpy(c->cell_ubar0, cell_ubar0, sizeof(double) * (size_t)im * jm, cudaMemcpyHostToDevice));
+    }
+    cudaFree(c->solid_list); c->solid_list = nullptr;
+    cudaFree(c->amb_rows); c->amb_rows = nullptr;
+    c->n_solid = (int)L.size();
+    c->n_amb_rows = (int)rows.size();
+    if (c->n_solid > 0) {
+        ATJUP_CUDA(cudaMalloc(&c->solid_list, sizeof(SolidCell) * L.size()));
+        ATJUP_CUDA(cudaMemcpy(c->solid_list, L.data(), sizeof(SolidCell) * L.size(), cudaMemcpyHostToDevice));
+        ATJUP_CUDA(cudaMalloc(&c->amb_rows, sizeof(int32_t) * rows.size()));
+        ATJUP_CUDA(cudaMemcpy(c->amb_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice));
+    }
+    cudaFree(c->yw); c->yw = nullptr;   // rebuilt by the residual solver for this mask
+    c->grid_set = true;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_upload(AtjupCtx* c, int32_t id, const double* host) {
+    if (!c || !host || !valid_field(id)) { set_error("upload: bad argument"); return ATJUP_ERR_ARG; }
+    const AtjupParams& P = c->P;
+    ATJUP_CUDA(cudaMemcpy2DAsync(c->f[id], sizeof(double) * c->KP, host, sizeof(double) * P.km,
+                                 sizeof(double) * P.km, (size_t)P.im * P.jm,
+                                 cudaMemcpyHostToDevice, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+int atjup_gpu_download(AtjupCtx* c, int32_t id, double* host) {
+    if (!c || !host || !valid_field(id)) { set_error("download: bad argument"); return ATJUP_ERR_ARG; }
+    const AtjupParams& P = c->P;
+    ATJUP_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * P.km, c->f[id], sizeof(double) * c->KP,
+                                 sizeof(double) * P.km, (size_t)P.im * P.jm,
+                                 cudaMemcpyDeviceToHost, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+int atjup_gpu_upload_array(AtjupCtx* c, int32_t id, double*** x) {
+    if (!c || !x || !valid_field(id)) { set_error("upload_array: bad argument"); return ATJUP_ERR_ARG; }
+    const AtjupParams& P = c->P;
+    std::vector<double> h((size_t)P.im * P.jm * P.km);
+    for (int i = 0; i < P.im; i++)
+        for (int j = 0; j < P.jm; j++)
+            std::memcpy(&h[((size_t)i * P.jm + j) * P.km], x[i][j], sizeof(double) * P.km);
+    return atjup_gpu_upload(c, id, h.data());
+}
+
+int atjup_gpu_download_array(AtjupCtx* c, int32_t id, double*** x) {
+    if (!c || !x || !valid_field(id)) { set_error("download_array: bad argument"); return ATJUP_ERR_ARG; }
+    const AtjupParams& P = c->P;
+    std::vector<double> h((size_t)P.im * P.jm * P.km);
+    int rc = atjup_gpu_download(c, id, h.data());
+    if (rc != ATJUP_OK) return rc;
+    for (int i = 0; i < P.im; i++)
+        for (int j = 0; j < P.jm; j++)
+            std::memcpy(x[i][j], &h[((size_t)i * P.jm + j) * P.km], sizeof(double) * P.km);
+    return ATJUP_OK;
+}
+
+int atjup_gpu_field_ptr(AtjupCtx* c, int32_t id, void** dev_ptr, int32_t* pitch) {
+    if (!c || !dev_ptr || !valid_field(id)) { set_error("field_ptr: bad argument"); return ATJUP_ERR_ARG; }
+    *dev_ptr = c->f[id];
+    if (pitch) *pitch = c->KP;
+    return ATJUP_OK;
+}
+
+static int need_grid(AtjupCtx* c, const char* what) {
+    if (!c) { set_error(std::string(what) + ": null context"); return ATJUP_ERR_ARG; }
+    if (!c->grid_set) { set_error(std::string(what) + ": atjup_gpu_set_grid was not called"); return ATJUP_ERR_ARG; }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
+    (void)iter_n;
+    int rc = need_grid(c, "rk4_step");
+    if (rc) return rc;
+    double* Y[4] = {c->f[ATJUP_F_T], c->f[ATJUP_F_U], c->f[ATJUP_F_V], c->f[ATJUP_F_W]};
+    {
+        Timed tm(c, TK_RK_AUX);
+        if ((rc = launch_buoy_ref(c, Y[0]))) return rc;
+        if ((rc = launch_hydrostatic(c, Y[2], Y[3]))) return rc;
+    }
+    const double* in0[4] = {Y[0], Y[1], Y[2], Y[3]};
+    const double* in1[4] = {c->X1[0], c->X1[1], c->X1[2], c->X1[3]};
+    const double* in2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
+    const double* const* ins[4] = {in0, in1, in2, in1};
+    double* const* outs[4] = {c->X1, c->X2, c->X1, nullptr};
+    for (int s = 0; s < 4; s++) {
+        Timed tm(c, TK_RK_STAGE);
+        if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
+    }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_pressure_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st) {
+    int rc = need_grid(c, "pressure_solve");
+    if (rc) return rc;
+    AtjupSolveOpts def{};
+    def.mode = ATJUP_SOLVE_SWEEPS;
+    def.sweeps = c->P.press_sweeps;
+    def.omega = 1.0;
+    if (!o) o = &def;
+    if (o->mode == ATJUP_SOLVE_RESIDUAL) {
+        Timed tm(c, TK_SOLVER);
+        return pressure_residual_solve(c, o, st);
+    }
+    Timed tm(c, TK_PRESSURE);
+    if (o->mode != ATJUP_SOLVE_SWEEPS || o->sweeps < 1) { set_error("pressure_solve: bad options"); return ATJUP_ERR_ARG; }
+    if ((rc = launch_prepare_projection(c))) return rc;
+    if ((rc = launch_pressure_source(c))) return rc;
+    const double omega = (o->omega > 0.0) ? o->omega : 1.0;
+    for (int s = 0; s < o->sweeps; s++) {
+        if ((rc = launch_pressure_sweep(c, 0, omega))) return rc;
+        if ((rc = launch_pressure_sweep(c, 1, omega))) return rc;
+        if ((rc = launch_pressure_fold(c, c->f[ATJUP_F_P_DYN]))) return rc;
+    }
+    if (st) { st->iterations = o->sweeps; st->inner_solves = 0; st->rel_residual = -1.0; st->b_norm = -1.0; }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_bc(AtjupCtx* c, int32_t which) {
+    int rc = need_grid(c, "bc");
+    if (rc) return rc;
+    Timed tm(c, TK_BC);
+    return launch_bc(c, which);
+}
+
+int atjup_gpu_shapiro(AtjupCtx* c, int32_t id, int32_t order, double strength, int32_t passes,
+                      int32_t use_topo) {
+    int rc = need_grid(c, "shapiro");
+    if (rc) return rc;
+    if (!valid_field(id) || (order != 2 && order != 4) || passes < 0) {
+        set_error("shapiro: bad argument");
+        return ATJUP_ERR_ARG;
+    }
+    Timed tm(c, TK_SHAPIRO);
+    return launch_shapiro(c, c->f[id], order, strength, passes, use_topo);
+}
+
+int atjup_gpu_mixture_density(AtjupCtx* c) {
+    int rc = need_grid(c, "mixture_density");
+    if (rc) return rc;
+    Timed tm(c, TK_MIXTURE);
+    return launch_mixture_density(c);
+}
+
+int atjup_gpu_balance_column_v(AtjupCtx* c, double* vshift) {
+    int rc = need_grid(c, "balance_column_v");
+    if (rc) return rc;
+    {
+        Timed tm(c, TK_BALANCE_V);
+        if ((rc = launch_balance_v(c))) return rc;
+    }
+    if (vshift) {
+        const AtjupParams& P = c->P;
+        std::vector<double> h(P.jm);
+        ATJUP_CUDA(cudaMemcpyAsync(h.data(), c->dvrow, sizeof(double) * P.jm, cudaMemcpyDeviceToHost, c->stream));
+        ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+        double m = 0.0;
+        for (int j = 1; j < P.jm - 1; j++) m = std::max(m, std::fabs(h[j]));
+        *vshift = m;
+    }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveOpts* solve) {
+    int rc = need_grid(c, "step");
+    if (rc) return rc;
+    const AtjupParams& P = c->P;
+    if (iter_n % 2 == 0 || first) {
+        if ((rc = atjup_gpu_pressure_solve(c, solve, nullptr))) return rc;
+        if ((rc = atjup_gpu_mixture_density(c))) return rc;
+    }
+    if ((rc = atjup_gpu_rk4_step(c, iter_n))) return rc;
+    if ((rc = atjup_gpu_bc(c, ATJUP_BC_ALL))) return rc;
+    if (P.shapiro_inloop > 0) {
+        for (int f = ATJUP_F_U; f <= ATJUP_F_W; f++)
+            if ((rc = atjup_gpu_shapiro(c, f, 4, P.shapiro_strength, P.shapiro_inloop, 1))) return rc;
+    }
+    if (P.v_massbal_stride > 0 && iter_n % P.v_massbal_stride == 0) {
+        Timed tm(c, TK_BALANCE_V);
+        if ((rc = launch_balance_v(c))) return rc;
+    }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_nonfinite_count(AtjupCtx* c, int64_t* count) {
+    if (!c || !count) return ATJUP_ERR_ARG;
+    unsigned long long* d = nullptr;
+    ATJUP_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
+    ATJUP_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->stream));
+    int rc = launch_nonfinite(c, d);
+    unsigned long long h = 0;
+    if (rc == ATJUP_OK) {
+        cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = cuda_status(e, "nonfinite_count");
+    }
+    cudaFree(d);
+    *count = (int64_t)h;
+    if (rc == ATJUP_OK && h > 0) rc = ATJUP_ERR_NONFINITE;
+    return rc;
+}
+
+int atjup_gpu_timing(AtjupCtx* c, int32_t enable) {
+    if (!c) return ATJUP_ERR_ARG;
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    c->tn = 0;
+    c->tcls.clear();
+    c->timing = enable != 0;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_timing_read(AtjupCtx* c, int32_t cls, double* total_ms, int64_t* count) {
+    if (!c || cls < 0 || cls >= TK_COUNT) return ATJUP_ERR_ARG;
+    double tot = 0.0;
+    int64_t n = 0;
+    for (int q = 0; q < c->tn; q++) {
+        if (c->tcls[q] != cls) continue;
+        ATJUP_CUDA(cudaEventSynchronize(c->tev[2 * q + 1]));
+        float ms = 0.f;
+        ATJUP_CUDA(cudaEventElapsedTime(&ms, c->tev[2 * q], c->tev[2 * q + 1]));
+        tot += ms;
+        n++;
+    }
+    if (total_ms) *total_ms = tot;
+    if (count) *count = n;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_launch_count(AtjupCtx* c, int64_t* launches) {
+    if (!c || !launches) return ATJUP_ERR_ARG;
+    *launches = c->launches;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_synchronize(AtjupCtx* c) {
+    if (!c) return ATJUP_ERR_ARG;
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+}  // extern "C"

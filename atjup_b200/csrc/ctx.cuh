@@ -1,0 +1,142 @@
+// Device context and shared helpers of the ATJUP B200 hot path.
+//
+// HBM layout: every 3-D field is a structure-of-arrays block [i][j][KP] of doubles with the
+// longitude index k fastest and rows padded from km = 361 to KP = 368 elements, so each
+// (i, j) row starts on a 128-byte boundary (368 * 8 = 23 * 128). Cell (i, j, k) lives at
+// (i * jm + j) * KP + k. Padding elements are never read as data.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/atjup_gpu.h"
+
+#define ATJUP_MAX_SOLVE_PARTIALS 1024
+
+namespace atjup {
+
+// Per-(i, j) geometry, computed on the host in double with the same expressions as the
+// reference's CellGeometry (RungeKutta_Jup_Turb.cpp:388-411) and uploaded once.
+struct GeoIJ {
+    double rm, inv_rm, inv_rm2, inv_rmsinthe;
+    double inv_rm2sinthe, inv_rm2sinthe2, costhe_inv_rm2sinthe, v_metric;
+    double cotanthe, costhe, sinthe_true, cent_rad;
+    double cent_the, cor_rad, cor_the, num2;   // cor_*: (nd_cor * -2 * omega) * sine / cosine
+    double num3, pad0, pad1, pad2;             // num2 / num3: Poisson face weights of the row
+};
+
+// One solid cell of the obstacle with its bcSolidGround treatment (BC_Jup.h:496-590), found
+// once from the static mask: a/b are the two fluid cells of the extrapolation (kind 1), or
+// kind 0 (interior or no pair: p_dyn = 0).
+struct SolidCell {
+    int64_t c, a, b;
+    int32_t kind, pad;
+};
+
+struct AtjupCtxImpl;
+
+}  // namespace atjup
+
+struct AtjupCtx {
+    AtjupParams P;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int KP = 0;              // padded row pitch (elements)
+    size_t NP = 0;           // im * jm * KP
+    bool grid_set = false;
+
+    // state and inputs (FP64); index by ATJUP_F_*
+    double* f[ATJUP_F_COUNT] = {};
+    // RK stage buffers and accumulators for t, u, v, w
+    double* X1[4] = {};
+    double* X2[4] = {};
+    double* acc[4] = {};
+    // scratch
+    double* src = nullptr;       // Poisson source, one value per cell
+    double* tmp = nullptr;       // filter ping-pong buffers
+    double* tmp2 = nullptr;
+    double* red = nullptr;       // reduction partials
+    double* buoy_ref = nullptr;  // [im]
+    double* zm = nullptr;        // [4 * jm] zonal means for the top sponge
+    double* dvc = nullptr;       // [jm * KP] column means of v
+    double* dvrow = nullptr;     // [jm]
+    // Krylov solver vectors (allocated on first RESIDUAL solve)
+    double* kr[8] = {};
+    float* kf[8] = {};
+    double* solve_b = nullptr;   // external right-hand side
+    double* dsum = nullptr;      // [ATJUP_MAX_SOLVE_PARTIALS * 4] dot-product partials
+    double* hsum = nullptr;      // pinned host copy of the final dot products
+
+    // static grid
+    uint8_t* solid = nullptr;
+    int32_t* topo = nullptr;
+    atjup::GeoIJ* geo = nullptr;   // [im * jm]
+    double* cor_col = nullptr;     // [jm] Coriolis factor of the hydrostatic integral
+    double* sin_the = nullptr;     // [jm] sin(the_j), the area weight of the level mean
+    double* rad = nullptr;         // [im]
+    double* cell_vbar0 = nullptr;  // [im * jm]
+    double* cell_ubar0 = nullptr;
+    atjup::SolidCell* solid_list = nullptr;
+    int n_solid = 0;
+    int32_t* amb_rows = nullptr;   // (i, j) rows that contain solid cells
+    int n_amb_rows = 0;
+    double* yw = nullptr;          // [NP] left null vector weight a_i d_j on fluid unknowns
+    double* line_a = nullptr;      // radial line factors for the preconditioner
+    double* line_c = nullptr;
+    double* line_m = nullptr;
+    double yw_sum = 0.0;
+
+    // instrumentation: kernel launches issued, and CUDA-event timing per kernel class
+    long long launches = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;     // event pool, two per timed launch
+    std::vector<int> tcls;            // class of each timed launch
+    int tn = 0;                       // timed launches recorded
+};
+
+namespace atjup {
+
+void set_error(const std::string& msg);
+
+// kernel classes of the timing hook (atjup_gpu_timing)
+enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
+       TK_SOLVER, TK_COUNT };
+void timer_begin(AtjupCtx* c, int cls);
+void timer_end(AtjupCtx* c);
+int cuda_status(cudaError_t e, const char* what);
+
+inline size_t cell(const AtjupCtx* c, int i, int j, int k) {
+    return ((size_t)i * c->P.jm + j) * c->KP + k;
+}
+
+// launchers (return ATJUP_OK or an error code)
+int launch_buoy_ref(AtjupCtx* c, const double* t);
+int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w);
+int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* const* Xout);
+int launch_mixture_density(AtjupCtx* c);
+int launch_prepare_projection(AtjupCtx* c);
+int launch_pressure_source(AtjupCtx* c);
+int launch_pressure_sweep(AtjupCtx* c, int colour, double omega);
+int launch_pressure_fold(AtjupCtx* c, double* p);
+int launch_bc(AtjupCtx* c, int which);
+int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passes, int use_topo);
+int launch_balance_v(AtjupCtx* c);
+int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
+int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
+
+}  // namespace atjup
+
+#define ATJUP_CUDA(call)                                                       \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) return atjup::cuda_status(e_, #call);           \
+    } while (0)
+
+#define ATJUP_CHECK_LAUNCH(what)                                               \
+    do {                                                                       \
+        cudaError_t e_ = cudaGetLastError();                                   \
+        if (e_ != cudaSuccess) return atjup::cuda_status(e_, what);            \
+    } while (0)

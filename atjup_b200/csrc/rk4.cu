@@ -1,0 +1,458 @@
+// RK4 time step of the dynamics: buoyancy level mean, hydrostatic column integral, the fused
+// RHS + stage kernel, and the mixture density.
+//
+// Reference: cJupiterModel::RungeKuttaJup (RungeKutta_Jup_Turb.cpp:261-583) with RHSJup
+// (RHS_Jup_Turb.cpp:31-1457). The reference runs every stage as two passes over the grid (RHS
+// everywhere into rhs_*, then accumulate and form the next stage input) and copies y -> y_n after
+// the step. Here one kernel per stage reads the stage input X_s (7-point stencil), the time-level
+// n state Y and the accumulator at the cell, and writes X_{s+1} and the accumulator; stage 3
+// writes Y itself. Non-integrated cells (radial walls, the three rows next to each pole, the
+// seam copy k = km-1, solid cells) keep their start-of-step values: stages 0-2 copy Y into
+// X_{s+1} there, which is what the reference's untouched live fields hold.
+#include "ctx.cuh"
+
+namespace atjup {
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+struct StageConst {
+    int im, jm, km, KP;
+    int stage;
+    double c_in, wgt, dt, one_sixth;
+    double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
+    double cor_phi_f;          // (nd_cor * 2) * omega
+    double coeff_energy_p;     // u_0^2 / (cp_mix t_ref)
+    double to_nd, r_mix, rR, g, t_ref, R_mix, cp_mix, u_0, L_rad;
+    double t_visc;             // t_diff_scale / (re pr)
+    double inv_re;
+    double buoy_k;             // -nd_buoy * buoy_scale * buoy_ramp * buoyancy
+    double metric_on, cor_rad_on, Coriolis, centrifugal, pgrad_scale;
+    double rad_coupling, precip_coupling, turb_coupling;
+    int pgrad_wall, adiabatic, adiabatic_rho, hydro_split, use_hp, cell_hold;
+    int has_nue, has_heating, precip_local;
+};
+
+struct StagePtrs {
+    const double* X[4];
+    double* Xo[4];
+    double* Y[4];
+    double* acc[4];
+    const double *p_dyn, *p_hydro, *p_stat, *rho, *wall_nue, *nue, *Q_rad, *Q_precip;
+    double *aux_u, *aux_v, *aux_w;
+    const uint8_t* solid;
+    const GeoIJ* geo;
+    const double* buoy_ref;
+    const double *cell_vbar0, *cell_ubar0;
+};
+
+__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+
+__global__ void __launch_bounds__(BX * BY)
+rk_stage_kernel(StagePtrs a, StageConst q) {
+    const int k = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= q.km || j >= q.jm) return;
+    const size_t row = (size_t)q.KP;
+    const size_t plane = (size_t)q.jm * row;
+    const size_t c = (size_t)i * plane + (size_t)j * row + k;
+    const bool integ = (i >= 1) && (i <= q.im - 2) && (j >= 3) && (j <= q.jm - 4) &&
+                       (k <= q.km - 2) && !a.solid[c];
+    if (!integ) {
+        if (q.stage < 3) {
+#pragma unroll
+            for (int f = 0; f < 4; f++) a.Xo[f][c] = a.Y[f][c];
+        }
+        return;
+    }
+    const GeoIJ& g = a.geo[i * q.jm + j];
+    const int kw = (k == 0) ? q.km - 2 : k - 1;
+    const int ke = (k == q.km - 2) ? 0 : k + 1;
+    const size_t cip = c + plane, cim = c - plane, cjp = c + row, cjm = c - row;
+    const size_t ckp = c - k + ke, ckm = c - k + kw;
+
+    const double* T = a.X[0];
+    const double* U = a.X[1];
+    const double* V = a.X[2];
+    const double* W = a.X[3];
+    const double t0 = ld(T + c), u0 = ld(U + c), v0 = ld(V + c), w0 = ld(W + c);
+
+    // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
+#define DERIVS(F, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
+    const double d1r = (ld(F + cip) - ld(F + cim)) * q.inv_2dr;               \
+    const double d2r = (ld(F + cip) - 2.0 * f0 + ld(F + cim)) * q.inv_dr2;    \
+    const double d1t = (ld(F + cjp) - ld(F + cjm)) * q.inv_2dthe;             \
+    const double d2t = (ld(F + cjp) - 2.0 * f0 + ld(F + cjm)) * q.inv_dthe2;  \
+    const double d1p = (ld(F + ckp) - ld(F + ckm)) * q.inv_2dphi;             \
+    const double d2p = (ld(F + ckp) - 2.0 * f0 + ld(F + ckm)) * q.inv_dphi2;
+    DERIVS(T, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
+    DERIVS(U, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
+    DERIVS(V, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
+    DERIVS(W, w0, dwdr, d2wdr2, dwdthe, d2wdthe2, dwdphi, d2wdphi2)
+#undef DERIVS
+
+    // pressure gradients with solid faces mirrored to the local value (RHS_Jup_Turb.cpp:119-130)
+    const uint8_t s_ip = a.solid[cip], s_im = a.solid[cim], s_jp = a.solid[cjp];
+    const uint8_t s_jm = a.solid[cjm], s_kp = a.solid[ckp], s_km = a.solid[ckm];
+    const double pc = ld(a.p_dyn + c);
+    auto pg = [&](const double* P, size_t hi, size_t lo, uint8_t sh, uint8_t sl, double loc,
+                  double inv2d) -> double {
+        const double h = (q.pgrad_wall && sh) ? loc : ld(P + hi);
+        const double l = (q.pgrad_wall && sl) ? loc : ld(P + lo);
+        return (h - l) * inv2d;
+    };
+    const double dpdr = pg(a.p_dyn, cip, cim, s_ip, s_im, pc, q.inv_2dr);
+    const double dpdthe = pg(a.p_dyn, cjp, cjm, s_jp, s_jm, pc, q.inv_2dthe);
+    const double dpdphi = pg(a.p_dyn, ckp, ckm, s_kp, s_km, pc, q.inv_2dphi);
+
+    // body forces (RHS_Jup_Turb.cpp:384-423)
+    const double Coriolis_rad = g.cor_rad * w0;
+    const double Coriolis_the = g.cor_the * w0;
+    double v_cor = v0, u_cor = u0;
+    if (q.cell_hold) {
+        v_cor -= ld(a.cell_vbar0 + i * q.jm + j);
+        u_cor -= ld(a.cell_ubar0 + i * q.jm + j);
+    }
+    const double Coriolis_phi = q.cor_phi_f * (+g.costhe * v_cor + g.sinthe_true * u_cor);
+
+    const double v_invrm = v0 * g.inv_rm;
+    const double w_invrs = w0 * g.inv_rmsinthe;
+
+    // compression work with the hydrostatic part (RHS_Jup_Turb.cpp:459-482)
+    const double rho_l = ld(a.rho + c);
+    double dpstatdr = 0.0;
+    if (q.adiabatic) {
+        dpstatdr = (ld(a.p_stat + cip) - ld(a.p_stat + cim)) * q.inv_2dr * q.to_nd;
+        if (q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr *= q.r_mix / rho_l;
+    }
+    const double pressure_t = q.coeff_energy_p *
+        (u0 * (dpdr + dpstatdr) + v_invrm * dpdthe + w_invrs * dpdphi);
+    const double transport_t = u0 * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
+    const double transport_u = u0 * dudr + v_invrm * dudthe + w_invrs * dudphi -
+                               q.metric_on * (v0 * v0 + w0 * w0) * g.inv_rm;
+    const double transport_v = u0 * dvdr + v_invrm * dvdthe + w_invrs * dvdphi +
+                               (u0 * v0 - w0 * w0 * g.cotanthe) * g.inv_rm;
+    const double transport_w = u0 * dwdr + v_invrm * dwdthe + w_invrs * dwdphi +
+                               (w0 * u0 + v0 * w0 * g.cotanthe) * g.inv_rm;
+
+    // diffusion (RHS_Jup_Turb.cpp:521-545)
+    const double two_inv_rm = 2.0 * g.inv_rm;
+    const double diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * g.inv_rm2 +
+                               dtdthe * g.costhe_inv_rm2sinthe + d2tdphi2 * g.inv_rm2sinthe2;
+    const double diffusion_u = d2udr2 + 2.0 * u0 * g.inv_rm2 + d2udthe2 * g.inv_rm2 +
+                               4.0 * dudr * g.inv_rm + dudthe * g.costhe_inv_rm2sinthe +
+                               d2udphi2 * g.inv_rm2sinthe2;
+    const double diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * g.inv_rm2 +
+                               dvdthe * g.costhe_inv_rm2sinthe - g.v_metric * v0 +
+                               d2vdphi2 * g.inv_rm2sinthe2 + 2.0 * dudthe * g.inv_rm2 -
+                               dwdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+    const double diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * g.inv_rm2 +
+                               dwdthe * g.costhe_inv_rm2sinthe - g.v_metric * w0 +
+                               d2wdphi2 * g.inv_rm2sinthe2 + 2.0 * dudphi * g.inv_rm2sinthe +
+                               dvdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+
+    const double dpdr_term = q.pgrad_scale * dpdr;
+    const double dpdthe_term = q.pgrad_scale * dpdthe * g.inv_rm;
+    const double dpdphi_term = q.pgrad_scale * dpdphi * g.inv_rmsinthe;
+    double dphdthe_term = 0.0, dphdphi_term = 0.0;
+    if (q.use_hp) {
+        const double hc = ld(a.p_hydro + c);
+        dphdthe_term = pg(a.p_hydro, cjp, cjm, s_jp, s_jm, hc, q.inv_2dthe) * g.inv_rm;
+        dphdphi_term = pg(a.p_hydro, ckp, ckm, s_kp, s_km, hc, q.inv_2dphi) * g.inv_rmsinthe;
+    }
+
+    // radiative and latent heating (RHS_Jup_Turb.cpp:646-718)
+    double radiation_t = 0.0, precip_t = 0.0;
+    if (q.has_heating) {
+        if (q.rad_coupling != 0.0) {
+            const double T_phys = t0 * q.t_ref;
+            const double P_phys = ld(a.p_stat + c) * 1.0e5;
+            const double rho = (rho_l > 0.0 && isfinite(rho_l))
+                                   ? rho_l
+                                   : ((T_phys > 1.0) ? P_phys / (q.R_mix * T_phys) : 0.0);
+            if (rho > 0.0 && q.cp_mix > 0.0) {
+                radiation_t = q.rad_coupling * ld(a.Q_rad + c) * q.L_rad /
+                              (rho * q.cp_mix * q.u_0 * q.t_ref);
+                if (!isfinite(radiation_t)) radiation_t = 0.0;
+                else if (radiation_t > 0.5) radiation_t = 0.5;
+                else if (radiation_t < -0.5) radiation_t = -0.5;
+            }
+        }
+        if (q.precip_coupling != 0.0) {
+            double rho_p = q.r_mix;
+            if (q.precip_local) rho_p = (rho_l > 0.0 && isfinite(rho_l)) ? rho_l : q.r_mix;
+            if (rho_p > 0.0 && q.cp_mix > 0.0) {
+                precip_t = q.precip_coupling * ld(a.Q_precip + c) * q.L_rad /
+                           (rho_p * q.cp_mix * q.u_0 * q.t_ref);
+                if (!isfinite(precip_t)) precip_t = 0.0;
+                else if (precip_t > 0.5) precip_t = 0.5;
+                else if (precip_t < -0.5) precip_t = -0.5;
+            }
+        }
+    }
+
+    double nue_t = 0.0;
+    if (q.has_nue) {
+        const double nn = ld(a.nue + c);
+        if (q.turb_coupling != 0.0 && isfinite(nn)) nue_t = q.turb_coupling * fmax(0.0, nn);
+    }
+    const double nue_t_s = nue_t / 0.9;
+    const double visc = q.inv_re + nue_t + ld(a.wall_nue + c);
+
+    const double rhs_t = +pressure_t - transport_t + diffusion_t * (q.t_visc + nue_t_s) +
+                         radiation_t + precip_t;
+    const double buoyancy_u =
+        (t0 > 0.0) ? q.buoy_k * (q.g * ld(a.p_stat + c) / (q.rR * t0 * q.t_ref) - a.buoy_ref[i])
+                   : 0.0;
+    const double rhs_u = -dpdr_term + (q.hydro_split ? 0.0 : buoyancy_u) - transport_u +
+                         diffusion_u * visc - q.cor_rad_on * q.Coriolis * Coriolis_rad +
+                         q.centrifugal * g.cent_rad;
+    const double rhs_v = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc -
+                         q.Coriolis * Coriolis_the + q.centrifugal * g.cent_the;
+    const double rhs_w = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc -
+                         q.Coriolis * Coriolis_phi;
+
+    // accumulate (RungeKutta_Jup_Turb.cpp:419-490) and form the next stage input / the result
+    const double rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
+    if (q.stage == 0) {
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            a.acc[f][c] = q.wgt * rhs[f];
+            a.Xo[f][c] = a.Y[f][c] + q.c_in * rhs[f];
+        }
+    } else if (q.stage < 3) {
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            a.acc[f][c] = a.acc[f][c] + q.wgt * rhs[f];
+            a.Xo[f][c] = a.Y[f][c] + q.c_in * rhs[f];
+        }
+    } else {
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            const double acc3 = a.acc[f][c] + q.wgt * rhs[f];
+            a.Y[f][c] = a.Y[f][c] + q.dt * acc3 * q.one_sixth;
+        }
+        // the projection source the next pressure solve reads (the last stage's values)
+        a.aux_u[c] = rhs_u + dpdr_term;
+        a.aux_v[c] = rhs_v + dpdthe_term;
+        a.aux_w[c] = rhs_w + dpdphi_term;
+    }
+}
+
+// ---- buoyancy level mean (RungeKutta_Jup_Turb.cpp:47-69): fixed-order two-level reduction
+constexpr int BR_BLOCKS = 16, BR_THREADS = 256;
+
+__global__ void __launch_bounds__(BR_THREADS)
+buoy_partial_kernel(const double* __restrict__ t, const double* __restrict__ p_stat,
+                    const uint8_t* __restrict__ solid, const double* __restrict__ sin_the,
+                    double* __restrict__ part, int jm, int km, int KP, double g, double rR,
+                    double t_ref) {
+    const int i = blockIdx.y, b = blockIdx.x;
+    double s = 0.0, ws = 0.0;
+    for (int j = b; j < jm; j += BR_BLOCKS) {
+        const double wgt = sin_the[j];
+        const size_t row = ((size_t)i * jm + j) * KP;
+        for (int k = threadIdx.x; k < km; k += BR_THREADS) {
+            if (solid[row + k]) continue;
+            const double tt = t[row + k];
+            if (!(tt > 0.0)) continue;
+            const double bb = g * p_stat[row + k] / (rR * tt * t_ref);
+            if (!isfinite(bb)) continue;
+            s += wgt * bb;
+            ws += wgt;
+        }
+    }
+    __shared__ double sh_s[BR_THREADS / 32], sh_w[BR_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        ws += __shfl_down_sync(0xffffffffu, ws, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sh_s[threadIdx.x >> 5] = s; sh_w[threadIdx.x >> 5] = ws; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0.0, tw = 0.0;
+        for (int q = 0; q < BR_THREADS / 32; q++) { ts += sh_s[q]; tw += sh_w[q]; }
+        part[(i * BR_BLOCKS + b) * 2 + 0] = ts;
+        part[(i * BR_BLOCKS + b) * 2 + 1] = tw;
+    }
+}
+
+__global__ void buoy_final_kernel(const double* __restrict__ part, double* __restrict__ out, int im) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= im) return;
+    double s = 0.0, ws = 0.0;
+    for (int b = 0; b < BR_BLOCKS; b++) {
+        s += part[(i * BR_BLOCKS + b) * 2 + 0];
+        ws += part[(i * BR_BLOCKS + b) * 2 + 1];
+    }
+    out[i] = (ws > 0.0) ? s / ws : 0.0;
+}
+
+// ---- hydrostatic pressure (RungeKutta_Jup_Turb.cpp:119-259), one thread per column.
+// metric/Coriolis branch: f(i) = (v^2 + w^2) / r + cor * w over the fluid run [i0, i1] from
+// zero at its foot, plus the frozen p_baro; solid cells below and cells above the run are 0.
+__global__ void hydrostatic_kernel(const double* __restrict__ v, const double* __restrict__ w,
+                                   const double* __restrict__ p_baro,
+                                   const uint8_t* __restrict__ solid,
+                                   const double* __restrict__ rad,
+                                   const double* __restrict__ cor_col, double* __restrict__ ph,
+                                   int im, int jm, int km, int KP, double dr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (k >= km) return;
+    const size_t plane = (size_t)jm * KP;
+    const size_t base = (size_t)j * KP + k;
+    int i0 = 0;
+    while (i0 < im && solid[base + i0 * plane]) { ph[base + i0 * plane] = 0.0; i0++; }
+    if (i0 >= im) return;
+    int i1 = i0;
+    while (i1 + 1 < im && !solid[base + (i1 + 1) * plane]) i1++;
+    for (int i = i1 + 1; i < im; i++) ph[base + i * plane] = 0.0;
+    const double cor = cor_col[j];
+    double acc = 0.0, fprev = 0.0;
+    for (int i = i0; i <= i1; i++) {
+        const size_t c = base + i * plane;
+        const double vv = v[c], ww = w[c];
+        const double f = 0.0 + ((vv * vv + ww * ww) / rad[i] + cor * ww) / 1.0;
+        if (i > i0) acc = acc + 0.5 * (fprev + f) * dr;
+        fprev = f;
+        ph[c] = acc + (p_baro ? p_baro[c] : 0.0);
+    }
+}
+
+__global__ void mixture_density_kernel(const double* __restrict__ t, const double* __restrict__ ps,
+                                       const double* __restrict__ pd, double* __restrict__ rho,
+                                       size_t NP, double t_ref, double pdyn_w, double to_bar,
+                                       double R_mix) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= NP) return;
+    const double T = t[c] * t_ref;
+    if (!(T > 0.0)) { rho[c] = 0.0; return; }
+    const double p_pa = (ps[c] + pdyn_w * pd[c] * to_bar) * 1.0e5;
+    const double r = p_pa / (R_mix * T);
+    rho[c] = isfinite(r) ? r : 0.0;
+}
+
+}  // namespace
+
+int launch_buoy_ref(AtjupCtx* c, const double* t) {
+    const AtjupParams& P = c->P;
+    dim3 grid(BR_BLOCKS, P.im);
+    c->launches++;
+    buoy_partial_kernel<<<grid, BR_THREADS, 0, c->stream>>>(
+        t, c->f[ATJUP_F_P_STAT], c->solid, c->sin_the, c->red, P.jm, P.km, c->KP, P.g,
+        P.r_mix * P.R_mix, P.t_ref);
+    c->launches++;
+    buoy_final_kernel<<<1, 64, 0, c->stream>>>(c->red, c->buoy_ref, P.im);
+    ATJUP_CHECK_LAUNCH("buoy_ref");
+    return ATJUP_OK;
+}
+
+int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w) {
+    const AtjupParams& P = c->P;
+    if (!P.metric_split || P.hydro_split) {
+        set_error("hydrostatic pressure: only the ATJUP_METRIC_SPLIT=1, ATJUP_HYDRO_SPLIT=0 form is implemented");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    dim3 grid((P.km + 127) / 128, P.jm);
+    c->launches++;
+    hydrostatic_kernel<<<grid, 128, 0, c->stream>>>(v, w, c->f[ATJUP_F_P_BARO], c->solid, c->rad,
+                                                   c->cor_col, c->f[ATJUP_F_P_HYDRO], P.im, P.jm,
+                                                   P.km, c->KP, P.dr);
+    ATJUP_CHECK_LAUNCH("hydrostatic");
+    return ATJUP_OK;
+}
+
+int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* const* Xout) {
+    const AtjupParams& P = c->P;
+    StagePtrs a{};
+    for (int f = 0; f < 4; f++) {
+        a.X[f] = Xin[f];
+        a.Xo[f] = Xout ? Xout[f] : nullptr;
+        a.Y[f] = c->f[ATJUP_F_T + f];
+        a.acc[f] = c->acc[f];
+    }
+    a.p_dyn = c->f[ATJUP_F_P_DYN];
+    a.p_hydro = c->f[ATJUP_F_P_HYDRO];
+    a.p_stat = c->f[ATJUP_F_P_STAT];
+    a.rho = c->f[ATJUP_F_RHO_MIX];
+    a.wall_nue = c->f[ATJUP_F_WALL_NUE];
+    a.nue = c->f[ATJUP_F_NUE];
+    a.Q_rad = c->f[ATJUP_F_Q_RAD];
+    a.Q_precip = c->f[ATJUP_F_Q_PRECIP];
+    a.aux_u = c->f[ATJUP_F_AUX_U];
+    a.aux_v = c->f[ATJUP_F_AUX_V];
+    a.aux_w = c->f[ATJUP_F_AUX_W];
+    a.solid = c->solid;
+    a.geo = c->geo;
+    a.buoy_ref = c->buoy_ref;
+    a.cell_vbar0 = c->cell_vbar0;
+    a.cell_ubar0 = c->cell_ubar0;
+
+    StageConst q{};
+    q.im = P.im; q.jm = P.jm; q.km = P.km; q.KP = c->KP;
+    q.stage = stage;
+    q.c_in = (stage == 0 || stage == 1) ? 0.5 * P.dt : (stage == 2 ? P.dt : 0.0);
+    q.wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+    q.dt = P.dt;
+    q.one_sixth = 1.0 / 6.0;
+    q.inv_2dr = 1.0 / (2.0 * P.dr);
+    q.inv_2dthe = 1.0 / (2.0 * P.dthe);
+    q.inv_2dphi = 1.0 / (2.0 * P.dphi);
+    q.inv_dr2 = 1.0 / (P.dr * P.dr);
+    q.inv_dthe2 = 1.0 / (P.dthe * P.dthe);
+    q.inv_dphi2 = 1.0 / (P.dphi * P.dphi);
+    q.cor_phi_f = P.nd_cor * +2.0 * P.omega;
+    q.coeff_energy_p = P.u_0 * P.u_0 / (P.cp_mix * P.t_ref);
+    q.to_nd = 1.0 / P.p_dyn_to_bar;
+    q.r_mix = P.r_mix;
+    q.rR = P.r_mix * P.R_mix;
+    q.g = P.g;
+    q.t_ref = P.t_ref;
+    q.R_mix = P.R_mix;
+    q.cp_mix = P.cp_mix;
+    q.u_0 = P.u_0;
+    q.L_rad = P.L_atm * 1.0e3;
+    q.t_visc = P.t_diff_scale / (P.re * P.pr);
+    q.inv_re = 1.0 / P.re;
+    q.buoy_k = -P.nd_buoy * P.buoy_scale * P.buoy_ramp * P.buoyancy;
+    q.metric_on = P.metric_split ? 0.0 : 1.0;
+    q.cor_rad_on = P.coriolis_split ? 0.0 : 1.0;
+    q.Coriolis = P.Coriolis;
+    q.centrifugal = P.centrifugal;
+    q.pgrad_scale = P.pgrad_scale;
+    q.rad_coupling = P.rad_coupling;
+    q.precip_coupling = P.precip_coupling;
+    q.turb_coupling = P.turb_coupling;
+    q.pgrad_wall = P.pgrad_wall;
+    q.adiabatic = P.adiabatic;
+    q.adiabatic_rho = P.adiabatic_rho;
+    q.hydro_split = P.hydro_split;
+    q.use_hp = (P.hydro_split || P.metric_split) ? 1 : 0;
+    q.cell_hold = (P.cell_hold && c->cell_vbar0) ? 1 : 0;
+    q.has_nue = (P.has_nue && a.nue) ? 1 : 0;
+    q.has_heating = (P.has_heating && a.Q_rad && a.Q_precip) ? 1 : 0;
+    q.precip_local = (P.precip_rho_local && P.local_rho) ? 1 : 0;
+
+    dim3 block(BX, BY);
+    dim3 grid((P.km + BX - 1) / BX, (P.jm + BY - 1) / BY, P.im);
+    c->launches++;
+    rk_stage_kernel<<<grid, block, 0, c->stream>>>(a, q);
+    ATJUP_CHECK_LAUNCH("rk_stage");
+    return ATJUP_OK;
+}
+
+int launch_mixture_density(AtjupCtx* c) {
+    const AtjupParams& P = c->P;
+    const int th = 256;
+    const size_t nb = (c->NP + th - 1) / th;
+    c->launches++;
+    mixture_density_kernel<<<(unsigned)nb, th, 0, c->stream>>>(
+        c->f[ATJUP_F_T], c->f[ATJUP_F_P_STAT], c->f[ATJUP_F_P_DYN], c->f[ATJUP_F_RHO_MIX], c->NP,
+        P.t_ref, P.rho_pdyn ? 1.0 : 0.0, P.p_dyn_to_bar, P.R_mix);
+    ATJUP_CHECK_LAUNCH("mixture_density");
+    return ATJUP_OK;
+}
+
+}  // namespace atjup

@@ -1,0 +1,212 @@
+"""Python binding of the B200 C ABI (include/atjup_gpu.h) -- the host-side mirror of the
+reference's model object for the time-step hot path.
+
+The reference exposes the model as ``pyatjup.Jupiter`` (python/pyatjup.pyx.template:35-97) whose
+``run()`` calls ``cJupiterModel::Run``; the hot path inside it is a sequence of member functions
+(cJupiterModel.cpp:1032-1381). ``GpuModel`` exposes the same routines by their reference names,
+on a device-resident state: ``pressure_solver()``, ``runge_kutta()``, ``bc_radius()`` ...,
+``step()`` for one whole iteration. Fields move in and out as numpy arrays in the reference's
+(i, j, k) order. There is no CPU fallback: construction fails if the CUDA library is missing or
+no sm_100 device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import params as _p
+
+_LIB_PATH = Path(__file__).resolve().parent / "libatjup_gpu.so"
+_lib = None
+
+
+class AtjupError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"atjup_gpu error {code}: {msg}")
+        self.code = code
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libatjup_gpu.so (built by ``python -m atjup_b200.build``); raise if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(f"{_LIB_PATH} is missing: build it with `python -m atjup_b200.build`")
+    L = ctypes.CDLL(str(_LIB_PATH))
+    vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+    L.atjup_gpu_last_error.restype = ctypes.c_char_p
+    L.atjup_gpu_create.argtypes = [ctypes.POINTER(_p.AtjupParams), ctypes.POINTER(vp)]
+    L.atjup_gpu_destroy.argtypes = [vp]
+    L.atjup_gpu_set_stream.argtypes = [vp, vp]
+    L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.atjup_gpu_upload.argtypes = [vp, i32, vp]
+    L.atjup_gpu_download.argtypes = [vp, i32, vp]
+    L.atjup_gpu_field_ptr.argtypes = [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(i32)]
+    L.atjup_gpu_rk4_step.argtypes = [vp, i32]
+    L.atjup_gpu_pressure_solve.argtypes = [vp, ctypes.POINTER(_p.AtjupSolveOpts),
+                                           ctypes.POINTER(_p.AtjupSolveStats)]
+    L.atjup_gpu_set_solve_rhs.argtypes = [vp, vp]
+    L.atjup_gpu_bc.argtypes = [vp, i32]
+    L.atjup_gpu_shapiro.argtypes = [vp, i32, i32, dbl, i32, i32]
+    L.atjup_gpu_mixture_density.argtypes = [vp]
+    L.atjup_gpu_balance_column_v.argtypes = [vp, ctypes.POINTER(dbl)]
+    L.atjup_gpu_step.argtypes = [vp, i32, i32, ctypes.POINTER(_p.AtjupSolveOpts)]
+    L.atjup_gpu_nonfinite_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.atjup_gpu_synchronize.argtypes = [vp]
+    L.atjup_params_default.argtypes = [ctypes.POINTER(_p.AtjupParams)]
+    L.atjup_gpu_timing.argtypes = [vp, i32]
+    L.atjup_gpu_timing_read.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int64)]
+    L.atjup_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise AtjupError(rc, load_library().atjup_gpu_last_error().decode())
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class GpuModel:
+    """Device-resident hot-path state of one model (one CUDA context, one stream)."""
+
+    def __init__(self, params: _p.AtjupParams, grid: dict):
+        self.L = load_library()
+        self.P = params
+        self.shape = (params.im, params.jm, params.km)
+        self.ctx = ctypes.c_void_p()
+        _check(self.L.atjup_gpu_create(ctypes.byref(params), ctypes.byref(self.ctx)))
+        self._keep = {}
+        self.set_grid(grid)
+
+    def close(self):
+        if self.ctx:
+            self.L.atjup_gpu_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- grid and fields ----
+    def set_grid(self, g: dict):
+        im, jm, km = self.shape
+        rad = np.ascontiguousarray(g["rad"], np.float64)
+        the = np.ascontiguousarray(g["the"], np.float64)
+        solid = np.ascontiguousarray(g["solid"], np.uint8).reshape(im, jm, km)
+        topo = np.ascontiguousarray(g["topo"], np.int32).reshape(jm, km)
+        cv = g.get("cell_vbar0")
+        cu = g.get("cell_ubar0")
+        cv = None if cv is None else np.ascontiguousarray(cv, np.float64)
+        cu = None if cu is None else np.ascontiguousarray(cu, np.float64)
+        _check(self.L.atjup_gpu_set_grid(self.ctx, _ptr(rad), _ptr(the), _ptr(solid), _ptr(topo),
+                                         _ptr(cv) if cv is not None else None,
+                                         _ptr(cu) if cu is not None else None))
+
+    def upload(self, name: str, a) -> None:
+        a = np.ascontiguousarray(a, np.float64).reshape(self.shape)
+        _check(self.L.atjup_gpu_upload(self.ctx, _p.FIELD_IDS[name], _ptr(a)))
+
+    def download(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape)
+        _check(self.L.atjup_gpu_download(self.ctx, _p.FIELD_IDS[name], _ptr(out)))
+        return out
+
+    def upload_state(self, fields: dict) -> None:
+        for n, a in fields.items():
+            if n in _p.FIELD_IDS and a is not None:
+                self.upload(n, a)
+
+    def field_ptr(self, name: str):
+        p = ctypes.c_void_p()
+        pitch = ctypes.c_int32()
+        _check(self.L.atjup_gpu_field_ptr(self.ctx, _p.FIELD_IDS[name], ctypes.byref(p),
+                                          ctypes.byref(pitch)))
+        return p.value, pitch.value
+
+    def set_stream(self, stream_handle: int | None):
+        _check(self.L.atjup_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
+
+    # ---- the hot path, by the reference's routine names ----
+    def runge_kutta(self, iter_n: int = 0):
+        """cJupiterModel::RungeKuttaJup (RungeKutta_Jup_Turb.cpp:261-583)."""
+        _check(self.L.atjup_gpu_rk4_step(self.ctx, iter_n))
+
+    def pressure_solver(self, mode=_p.SOLVE_SWEEPS, sweeps=None, omega=1.0, rel_tol=1e-10,
+                        max_iter=2000, precision=_p.PREC_FP64, external_rhs=False):
+        """PressureSolverJup::run (PressureSolver.h:144-766); returns AtjupSolveStats."""
+        o = _p.AtjupSolveOpts(mode, sweeps if sweeps is not None else self.P.press_sweeps,
+                              max_iter, precision, rel_tol, omega, int(external_rhs))
+        st = _p.AtjupSolveStats()
+        _check(self.L.atjup_gpu_pressure_solve(self.ctx, ctypes.byref(o), ctypes.byref(st)))
+        return st
+
+    def set_solve_rhs(self, b) -> None:
+        b = np.ascontiguousarray(b, np.float64).reshape(self.shape)
+        _check(self.L.atjup_gpu_set_solve_rhs(self.ctx, _ptr(b)))
+
+    def bc(self, which=_p.BC_ALL):
+        """BC_Jup::bcRadius / bcTheta / bcPhi / bcSolidGround (BC_Jup.h:185-658)."""
+        _check(self.L.atjup_gpu_bc(self.ctx, which))
+
+    def shapiro(self, name: str, order: int, strength=1.0, passes=1, use_topo=True):
+        """JupiterUtils::damp_wiggles / damp_wiggles_ho (lib/Utils.cpp:227-453)."""
+        _check(self.L.atjup_gpu_shapiro(self.ctx, _p.FIELD_IDS[name], order, strength, passes,
+                                        int(use_topo)))
+
+    def mixture_density(self):
+        """cJupiterModel::computeMixtureDensity (InitValues_Jup.cpp:717-740)."""
+        _check(self.L.atjup_gpu_mixture_density(self.ctx))
+
+    def balance_column_v(self) -> float:
+        """cJupiterModel::balanceColumnV (InitValues_Jup.cpp:1500-1538); returns the shift."""
+        s = ctypes.c_double()
+        _check(self.L.atjup_gpu_balance_column_v(self.ctx, ctypes.byref(s)))
+        return s.value
+
+    def step(self, iter_n: int, first: bool = False, solve: _p.AtjupSolveOpts | None = None):
+        """One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381)."""
+        _check(self.L.atjup_gpu_step(self.ctx, iter_n, int(first),
+                                     ctypes.byref(solve) if solve is not None else None))
+
+    def nonfinite_count(self) -> int:
+        n = ctypes.c_int64()
+        rc = self.L.atjup_gpu_nonfinite_count(self.ctx, ctypes.byref(n))
+        if rc not in (0, 5):
+            _check(rc)
+        return n.value
+
+    def synchronize(self):
+        _check(self.L.atjup_gpu_synchronize(self.ctx))
+
+    # ---- instrumentation ----
+    TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
+                      "mixture", "solver")
+
+    def timing(self, on: bool):
+        """Start (reset) or stop CUDA-event timing of the library's kernel launches."""
+        _check(self.L.atjup_gpu_timing(self.ctx, int(on)))
+
+    def timing_read(self, cls: int):
+        """(total ms, launches) of one kernel class since timing(True)."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        _check(self.L.atjup_gpu_timing_read(self.ctx, cls, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        n = ctypes.c_int64()
+        _check(self.L.atjup_gpu_launch_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
+    @staticmethod
+    def _rc(rc: int):
+        _check(rc)

@@ -1,0 +1,115 @@
+"""Seeded synthetic model state with the shapes and value ranges of ATJUP's initial state.
+
+The reference builds its start state with a long initialisation chain (cJupiterModel.cpp:392-745:
+temperature profile, polytropic / isothermal static pressure, measured jets, geostrophic balance,
+vortex, SeaMount cone). That chain is not part of the time-step hot path, so benchmarks and
+small-grid tests use this generator instead: the same grid geometry (metric radius R/L_atm + i dr,
+1-degree colatitude and longitude), the same obstacle construction (an elliptic cone of
+half-axes 18 x 12 cells at the base shrinking to 6 x 4 at level 26, centred at j = 112,
+k = 180 -- BC_Jup.h:386-413 with ATJUP_CONE_GEOM = 2), a parabolic pole-to-equator temperature
+with a 2 K/km lapse clamped at 110 K (InitValues_Jup.cpp:186-264), a polytropic / isothermal
+static pressure (InitValues_Jup.cpp:633-693), banded zonal jets, and the i.i.d. Gaussian
+perturbations of the dry benchmark configuration (u, v ~ N(0, 0.1 m/s), w ~ N(0, 0.01 m/s),
+T ~ N(0, 0.05 K), zero inside the obstacle). Values are nondimensional as in the model.
+On grids smaller than 41 x 181 x 361 the obstacle and jets are scaled to the grid.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+R_PLANET_KM = 69911.0
+
+
+def grid(im=41, jm=181, km=361, L_atm=140.0, dr=0.025, cone=True):
+    """rad, the, solid mask, i_topography for an (im, jm, km) shell."""
+    r0 = R_PLANET_KM / L_atm
+    rad = r0 + dr * np.arange(im)
+    dthe = 1.0 / (180.0 / math.pi)
+    the = dthe * np.arange(jm) * (180.0 / (jm - 1))       # 0 .. pi over jm points
+    solid = np.zeros((im, jm, km), np.uint8)
+    if cone:
+        sj, sk = (jm - 1) / 180.0, (km - 1) / 360.0
+        j0, k0 = int(round(112 * sj)), int(round(180 * sk))
+        i_top = min(26, im - 3)
+        base_a, base_b = max(2.0, 18 * sk), max(2.0, 12 * sj)
+        a_top, b_top = max(1.0, 6 * sk), max(1.0, 4 * sj)
+        for i in range(i_top + 1):
+            f = i / i_top
+            ai = round(base_a + (a_top - base_a) * f)
+            bi = round(base_b + (b_top - base_b) * f)
+            for k in range(k0 - ai, k0 + ai + 1):
+                for j in range(j0 - bi, j0 + bi + 1):
+                    x, y = (k - k0) / ai, (j - j0) / bi
+                    if x * x + y * y <= 1.0 + 1e-9 and 0 <= j < jm and 0 <= k < km:
+                        solid[i, j, k] = 1
+    topo = np.zeros((jm, km), np.int32)
+    for j in range(jm):
+        for k in range(km):
+            i = 0
+            while i < im and solid[i, j, k]:
+                i += 1
+            topo[j, k] = i
+    return rad, the, solid, topo
+
+
+def state(im=41, jm=181, km=361, seed=20261203, cone=True, t_ref=165.0, u_0=100.0,
+          r_mix=1.2844, R_mix=3531.1847352206946, g=25.92, L_atm=140.0, dr=0.025):
+    """Dict of grid arrays and fields (contiguous (i, j, k) float64 arrays)."""
+    rad, the, solid, topo = grid(im, jm, km, L_atm, dr, cone)
+    rng = np.random.Generator(np.random.Philox(seed))
+    shape = (im, jm, km)
+    jj = np.arange(jm)
+    ratio = jj / ((jm - 1) / 2.0)
+    t_pole, t_eq, gam = 310.0, 330.0, 2.0
+    t0 = (t_pole + (t_eq - t_pole) * (1.0 - (ratio - 1.0) ** 2))          # K at the base
+    height = np.arange(im) * (L_atm / (im - 1))                          # km
+    T = t0[None, :] - gam * height[:, None]
+    T = np.maximum(T, 110.0) / t_ref
+    t = np.broadcast_to(T[:, :, None], shape).copy()
+    # polytropic below the clamp, isothermal above
+    exp_p = g / (gam * R_mix * 1e-3)
+    p_poly = (t * t_ref / t_ref) ** exp_p * 1.0
+    p_stat = p_poly.copy()
+    for j in range(jm):
+        clamp = np.where(T[:, j] * t_ref <= 110.0 + 1e-9)[0]
+        if len(clamp):
+            ic = clamp[0]
+            H = R_mix * 110.0 / g
+            z = height * 1e3
+            p_stat[ic:, j, :] = p_stat[ic - 1, j, :][None, :] * np.exp(-(z[ic:] - z[ic - 1]) / H)[:, None]
+    # banded zonal jets (w), weak meridional cells (v), tiny radial wind (u)
+    lat = math.pi / 2 - the
+    jet = 1.2 * np.sin(6 * lat) * np.cos(lat) ** 2
+    w = np.broadcast_to((jet[None, :] * (0.3 + 0.7 * np.arange(im)[:, None] / (im - 1)))[:, :, None], shape).copy()
+    v = np.broadcast_to((0.05 * np.sin(2 * lat)[None, :] * np.cos(math.pi * np.arange(im) / (im - 1))[:, None])[:, :, None], shape).copy()
+    u = np.zeros(shape)
+    # perturbations of the dry benchmark configuration (model units: / u_0, / t_ref)
+    w += rng.normal(0.0, 0.1 / u_0, shape)
+    v += rng.normal(0.0, 0.1 / u_0, shape)
+    u += rng.normal(0.0, 0.01 / u_0, shape)
+    t += rng.normal(0.0, 0.05 / t_ref, shape)
+    fluid = solid == 0
+    for a in (u, v, w):
+        a *= fluid
+    p_dyn = 0.5 * np.broadcast_to(np.cos(2 * the)[None, :, None], shape) * (1.0 + 0.1 * rng.standard_normal(shape))
+    p_baro = -0.2 * np.broadcast_to(np.cos(the)[None, :, None], shape).copy()
+    rho_mix = p_stat * 1e5 / (R_mix * t * t_ref)
+    wall_nue = np.zeros(shape)
+    # wall viscosity near the obstacle: 0.004 on fluid cells touching it
+    if solid.any():
+        near = np.zeros(shape, bool)
+        for ax in range(3):
+            for d in (-1, 1):
+                near |= np.roll(solid, d, axis=ax).astype(bool)
+        wall_nue[(near & fluid)] = 0.004
+    cell_vbar0 = np.zeros(im * jm)
+    cell_ubar0 = np.zeros(im * jm)
+    return {
+        "rad": rad, "the": the, "solid": solid, "topo": topo,
+        "cell_vbar0": cell_vbar0, "cell_ubar0": cell_ubar0,
+        "t": t, "u": u, "v": v, "w": w, "p_dyn": p_dyn, "p_hydro": np.zeros(shape),
+        "p_stat": p_stat, "rho_mix": rho_mix, "wall_nue": wall_nue, "p_baro": p_baro,
+        "aux_u": np.zeros(shape), "aux_v": np.zeros(shape), "aux_w": np.zeros(shape),
+    }

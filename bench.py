@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark of ATJUP's time step on B200: one model iteration of the dry configuration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the dry dynamics configuration on the 41 x 181 x 361 shell (2.68 M cells, FP64):
+each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381) -- the
+red-black pressure pass on even iterations, mixture density, the four RK4 stages, the boundary
+passes, the in-loop 4th-order Shapiro filter of u, v, w and the column balance of v. The state is
+a seeded synthetic one with the shapes and value ranges of the model's own initial state
+(atjup_b200/synthetic.py); it is device-resident when the timed region starts.
+
+Prints one JSON line. `value` is seconds per step for the whole job (N replicas: max-over-ranks
+device time / (N * K)); `e2e` is the same metric through the public C ABI with host buffers
+(pinned), the host->device upload of the step's state and the device->host read of its result
+inside the timed region. With --impl reference the line times the reference's own CPU code of
+the same iteration (built from its sources into oracle/_ref) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+IM, JM, KM = 41, 181, 361
+N_CELLS = IM * JM * KM
+METRIC = "s per RK4 step (dry FP64 dynamics, 41x181x361: one model iteration incl. pressure pass)"
+UNIT = "s/step"
+CONFIG = {
+    "workload": "dry dynamics iteration on the 41x181x361 shell (BASELINE config 0 knobs): "
+                "pressure red-black pass on even iterations, RK4 (4 stages), BCs, 4th-order "
+                "Shapiro on u,v,w, column balance of v",
+    "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
+    "l2": "no flush: inputs larger than L2 (each RK stage streams ~0.47 GB)",
+    "parallelism": "replicas (the path does not shard)",
+}
+# Algorithmic bytes of one RK stage launch: N * b * (17 F + 4 A) / 4 + N bytes of mask, with
+# F = 4 prognostic fields (t, u, v, w) and A = 5 frozen inputs (p_dyn, p_hydro, p_stat, rho_mix,
+# wall_nue), b = 8 (FP64): one RK4 step of 1.89 GB over its four stage launches.
+RK_STEP_BYTES = N_CELLS * 8 * (17 * 4 + 4 * 5) + 4 * N_CELLS
+RK_STAGE_BYTES = RK_STEP_BYTES / 4
+# DRAM bytes (read + write) of one rk_stage_kernel launch from an ncu capture
+# (profiles/rk_stage_kernel_dry_41x181x361.md); None until captured.
+RK_STAGE_TRAFFIC = None
+
+DRY_ENV = {
+    "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
+    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
+    "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
+}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(steps=3, warmup=1):
+    """The reference's own CPU iteration (oracle/_ref) timed on this host's cores."""
+    cmd = [sys.executable, str(ROOT / "oracle" / "ref_bench.py"), "--steps", str(steps),
+           "--warmup", str(warmup)]
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600).stdout
+        d = json.loads(out.strip().splitlines()[-1])
+    except Exception as e:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"unavailable: {e}"}
+    if "unavailable" in d:
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "unavailable: " + d["unavailable"]}
+    return {"value": d["s_per_step"], "unit": UNIT, "cores": d["threads"], "kind": "reference",
+            "sample": f"{d['steps']} dry iterations of the reference (built at -O3 from its "
+                      f"sources, OpenMP {d['threads']} threads) after {warmup} warm-up, on its own "
+                      f"initial state"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cb = cpu_baseline(steps=args.steps, warmup=args.warmup)
+    if cb["value"] is None:
+        print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
+        return
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "the reference's own initial state (dry knobs)", "config": CONFIG,
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    args.warmup = max(args.warmup, 3)
+
+    import numpy as np
+    import torch
+
+    from atjup_b200 import synthetic
+    from atjup_b200.gpu import GpuModel
+    from atjup_b200.params import resolve_params, FIELD_IDS
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    P = resolve_params(DRY_ENV, im=IM, jm=JM, km=KM)
+    s = synthetic.state(IM, JM, KM, seed=20261203 + rank)
+    grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
+    fields = {k: v for k, v in s.items() if k not in grid}
+    m = GpuModel(P, grid)
+    m.upload_state(fields)
+    stream = torch.cuda.Stream()
+    m.set_stream(stream.cuda_stream)
+
+    it = [0]
+
+    def step():
+        it[0] += 1
+        m.step(it[0], it[0] == 1)
+
+    for _ in range(args.warmup):
+        step()
+    m.synchronize()
+    if m.nonfinite_count() != 0:
+        raise SystemExit("non-finite state after warm-up")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region ----
+    clocks = ClockSampler(local_rank)
+    n0 = m.launch_count()
+    m.timing(True)
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    barrier()
+    t_ms = ev0.elapsed_time(ev1)
+    launches = m.launch_count() - n0
+    st_ms, st_n = m.timing_read(0)          # rk_stage_kernel
+    m.timing(False)
+    if dist is not None:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    value = t_ms / 1e3 / (args.steps * world)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    names = ["t", "u", "v", "w", "p_dyn"]
+    host_in = {n: torch.from_numpy(np.ascontiguousarray(fields[n])).pin_memory() for n in names}
+    host_out = {n: torch.empty((IM, JM, KM), dtype=torch.float64).pin_memory() for n in names}
+    import ctypes
+
+    def up(n):
+        m._rc(m.L.atjup_gpu_upload(m.ctx, FIELD_IDS[n], ctypes.c_void_p(host_in[n].data_ptr())))
+
+    def down(n):
+        m._rc(m.L.atjup_gpu_download(m.ctx, FIELD_IDS[n], ctypes.c_void_p(host_out[n].data_ptr())))
+
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for n in names:
+            up(n)
+        step()
+        for n in names:
+            down(n)
+    m.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    nbytes = len(names) * N_CELLS * 8
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = (RK_STAGE_BYTES / (st_ms / st_n / 1e3)) / 1e9 if st_n else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; shapes and value ranges of the model's initial state)",
+        "config": CONFIG,
+        "roofline": {"kernel": "rk_stage_kernel", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None,
+                     "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
+                     "traffic": RK_STAGE_TRAFFIC, "algorithmic_bytes_per_launch": RK_STAGE_BYTES,
+                     "avg_launch_ms": st_ms / st_n if st_n else None, "launches": st_n},
+        "e2e": {"value": e2e_s / (e2e_steps * world), "unit": UNIT, "steps": e2e_steps,
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if dist is not None:
+        dist.barrier()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    m.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -198,6 +198,16 @@ int atjup_gpu_step(AtjupCtx* ctx, int32_t iter_n, int32_t first, const AtjupSolv
 /* Count of non-finite values in the prognostic fields (NaN/Inf census; no device trap). */
 int atjup_gpu_nonfinite_count(AtjupCtx* ctx, int64_t* count);
 
+/* Instrumentation (no reference counterpart: the reference prints wall-clock timers per routine,
+ * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
+ * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */
+enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
+       ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_COUNT };
+int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
+int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
+/* Number of kernels this context has launched since creation. */
+int atjup_gpu_launch_count(AtjupCtx* ctx, int64_t* launches);
+
 int atjup_gpu_synchronize(AtjupCtx* ctx);
 const char* atjup_gpu_last_error(void);
 
