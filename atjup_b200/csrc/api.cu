@@ -55,6 +55,7 @@ int alloc(double** p, size_t n) {
 }
 
 void free_all(AtjupCtx* c) {
+    solver_free(c);
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
     for (int q = 0; q < 4; q++) {
         cudaFree(c->X1[q]); cudaFree(c->X2[q]); cudaFree(c->acc[q]);
@@ -302,7 +303,7 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
         ATJUP_CUDA(cudaMalloc(&c->amb_rows, sizeof(int32_t) * rows.size()));
         ATJUP_CUDA(cudaMemcpy(c->amb_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice));
     }
-    cudaFree(c->yw); c->yw = nullptr;   // rebuilt by the residual solver for this mask
+    solver_free(c);                      // rebuilt by the residual solver for this mask
     c->grid_set = true;
     return ATJUP_OK;
 }

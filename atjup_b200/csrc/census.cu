@@ -31,11 +31,7 @@ int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count) {
     return ATJUP_OK;
 }
 
-int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st) {
-    (void)c; (void)o; (void)st;
-    set_error("pressure_solve: RESIDUAL mode not built yet");
-    return ATJUP_ERR_UNSUPPORTED;
-}
+
 
 }  // namespace atjup
 

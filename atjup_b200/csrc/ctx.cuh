@@ -88,6 +88,7 @@ struct AtjupCtx {
     double* line_c = nullptr;
     double* line_m = nullptr;
     double yw_sum = 0.0;
+    void* solver = nullptr;           // residual-solver state (solver.cu), built on first use
 
     // instrumentation: kernel launches issued, and CUDA-event timing per kernel class
     long long launches = 0;
@@ -126,6 +127,7 @@ int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passe
 int launch_balance_v(AtjupCtx* c);
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
+void solver_free(AtjupCtx* c);
 
 }  // namespace atjup
 

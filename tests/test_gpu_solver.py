@@ -1,0 +1,75 @@
+"""Residual-controlled pressure solve (ATJUP_SOLVE_RESIDUAL) on the GPU, checked with the CPU
+oracle's own application of the reference operator (the sweep's fixed-point equation, oracle
+ora_pressure_apply): ||b - A p|| / ||b|| <= the requested tolerance (x2 for the CPU/GPU rounding
+of A p), for FP64 and for FP32-inner / FP64-refinement solves."""
+import numpy as np
+import pytest
+
+from atjup_b200 import synthetic
+from atjup_b200.params import PREC_FP64, PREC_MIXED, SOLVE_RESIDUAL
+from helpers import gpu_from, oracle_from, synthetic_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _projected(o, b):
+    """b minus its y-component on fluid interior cells (the solver's compatibility step)."""
+    im, jm, km = o.shape
+    s = o.g["solid"].reshape(o.shape)
+    a = np.ones(im); a[[1, im - 2]] = 1.5
+    d = np.ones(jm); d[[1, jm - 2]] = 1.5
+    mask = np.zeros(o.shape, bool)
+    mask[1:im - 1, 1:jm - 1, :km - 1] = True
+    mask &= (s == 0)
+    y = (a[:, None, None] * d[None, :, None]) * mask
+    bb = np.where(mask, b, 0.0)
+    return bb - (y * bb).sum() / y.sum() * mask, mask
+
+
+def _rel_residual(o, p, b):
+    bp, mask = _projected(o, b)
+    r = np.where(mask, bp - o.apply_A(p), 0.0)
+    return np.linalg.norm(r) / np.linalg.norm(bp)
+
+
+@pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(13, 37, 49), (41, 61, 97)], ids=lambda s: "x".join(map(str, s)))
+def test_residual_solve_small(shape, prec):
+    p, g, f = synthetic_case(*shape)
+    b = synthetic.poisson_rhs(*shape, seed=3)
+    o = oracle_from(p, g, f)
+    m = gpu_from(p, g, f)
+    m.set_solve_rhs(b)
+    st = m.pressure_solver(mode=SOLVE_RESIDUAL, rel_tol=1e-10, max_iter=3000, precision=prec,
+                           external_rhs=True)
+    assert st.rel_residual <= 1e-10
+    e = _rel_residual(o, m.download("p_dyn"), b)
+    assert e <= 2e-10, f"oracle residual {e:.3e} (solver says {st.rel_residual:.3e}, {st.iterations} it)"
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED], ids=["fp64", "mixed"])
+def test_residual_solve_full_grid(prec):
+    """BASELINE config 1 on the 41x181x361 shell with the obstacle, to 1e-10."""
+    p, g, f = synthetic_case(41, 181, 361)
+    b = synthetic.poisson_rhs(41, 181, 361)
+    o = oracle_from(p, g, f)
+    m = gpu_from(p, g, f)
+    m.set_solve_rhs(b)
+    st = m.pressure_solver(mode=SOLVE_RESIDUAL, rel_tol=1e-10, max_iter=5000, precision=prec,
+                           external_rhs=True)
+    e = _rel_residual(o, m.download("p_dyn"), b)
+    assert e <= 2e-10, f"oracle residual {e:.3e} ({st.iterations} it)"
+
+
+def test_residual_solve_in_loop_source():
+    """The in-loop use: the divergence source of aux, warm-started from p_dyn."""
+    p, g, f = synthetic_case(13, 37, 49)
+    o = oracle_from(p, g, f)
+    m = gpu_from(p, g, f)
+    o.rk4()
+    m.runge_kutta()
+    src = o.source()
+    st = m.pressure_solver(mode=SOLVE_RESIDUAL, rel_tol=1e-10, max_iter=3000)
+    e = _rel_residual(o, m.download("p_dyn"), src)
+    assert e <= 2e-10, f"oracle residual {e:.3e} ({st.iterations} it)"
