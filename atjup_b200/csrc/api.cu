@@ -407,7 +407,10 @@ int atjup_gpu_pressure_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveSta
         if ((rc = launch_pressure_sweep(c, 1, omega))) return rc;
         if ((rc = launch_pressure_fold(c, c->f[ATJUP_F_P_DYN]))) return rc;
     }
-    if (st) { st->iterations = o->sweeps; st->inner_solves = 0; st->rel_residual = -1.0; st->b_norm = -1.0; }
+    if (st) {
+        st->iterations = o->sweeps; st->inner_solves = 0; st->rel_residual = -1.0; st->b_norm = -1.0;
+        st->rel_floor = -1.0;
+    }
     return ATJUP_OK;
 }
 

@@ -24,6 +24,7 @@
 #include "ctx.cuh"
 
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 namespace atjup {
@@ -86,26 +87,21 @@ apply_kernel(const T* __restrict__ x, T* __restrict__ y, const uint8_t* __restri
             const T xc = x[c];
             const int kw = (k == 0) ? q.km - 2 : k - 1;
             const int ke = (k == q.km - 2) ? 0 : k + 1;
-            T acc = 0, den = 0;
-            if (!s[c + plane]) {
-                acc += n1 * ((i + 1 == q.im - 1) ? (T)kC43 * xc - (T)kC13 * x[c - plane] : x[c + plane]);
-                den += n1;
-            }
-            if (!s[c - plane]) {
-                acc += n1 * ((i - 1 == 0) ? (T)kC43 * xc - (T)kC13 * x[c + plane] : x[c - plane]);
-                den += n1;
-            }
-            if (!s[c + row]) {
-                acc += n2 * ((j + 1 == q.jm - 1) ? (T)kC43 * xc - (T)kC13 * x[c - row] : x[c + row]);
-                den += n2;
-            }
-            if (!s[c - row]) {
-                acc += n2 * ((j - 1 == 0) ? (T)kC43 * xc - (T)kC13 * x[c + row] : x[c - row]);
-                den += n2;
-            }
-            if (!s[c - k + ke]) { acc += n3 * x[c - k + ke]; den += n3; }
-            if (!s[c - k + kw]) { acc += n3 * x[c - k + kw]; den += n3; }
-            out = acc - den * xc;
+            // a sum of differences (no cancellation of a large smooth x); a folded boundary face
+            // contributes num (1/3)(x_c - x_inward)
+            const T t13 = (T)kC13;
+            T acc = 0;
+            if (!s[c + plane])
+                acc += (i + 1 == q.im - 1) ? n1 * t13 * (xc - x[c - plane]) : n1 * (x[c + plane] - xc);
+            if (!s[c - plane])
+                acc += (i - 1 == 0) ? n1 * t13 * (xc - x[c + plane]) : n1 * (x[c - plane] - xc);
+            if (!s[c + row])
+                acc += (j + 1 == q.jm - 1) ? n2 * t13 * (xc - x[c - row]) : n2 * (x[c + row] - xc);
+            if (!s[c - row])
+                acc += (j - 1 == 0) ? n2 * t13 * (xc - x[c + row]) : n2 * (x[c - row] - xc);
+            if (!s[c - k + ke]) acc += n3 * (x[c - k + ke] - xc);
+            if (!s[c - k + kw]) acc += n3 * (x[c - k + kw] - xc);
+            out = acc;
             if (part) acc_dot += yw[c] * (double)xc * (double)out;
         }
         y[c] = out;
@@ -250,12 +246,20 @@ __global__ void theta_solve_kernel(T* __restrict__ gh, const T* __restrict__ ta,
         return;
     }
     T* e = gh + (size_t)part * (NM + 1) * J + (size_t)m * J;
+    T mean0 = 0;
+    if (m == 0) {
+        // the zonal-mean problem is singular (constant null vector): drop the incompatible part
+        // of its right-hand side, sum_j ghat_j = 0, before pinning the gauge
+        double sg = 0.0;
+        for (int jj = 0; jj < J; jj++) sg += (double)e[jj];
+        mean0 = (T)(sg / J);
+    }
     const T* a = ta + (size_t)m * J;
     const T* cp = tcp + (size_t)m * J;
     const T* mm = tm + (size_t)m * J;
     T prev = 0;
     for (int jj = 0; jj < J; jj++) {
-        T rhs = e[jj] / dj[jj + 1];
+        T rhs = (e[jj] - mean0) / dj[jj + 1];
         if (m == 0 && jj == 0) rhs = 0;                   // pinned gauge row
         prev = (rhs - a[jj] * prev) * mm[jj];
         e[jj] = prev;
@@ -323,26 +327,67 @@ __global__ void add_kernel(double* __restrict__ p, const double* __restrict__ e,
         p[c] += e[c];
 }
 
-// r = b - A x (A x already in ax), masked; partial sums of r^2
+// r = b - A p in FP64 on fluid interior cells, with partial sums of r^2 and of v^2, v = the
+// sum of |face terms| of A p: eps * ||v|| is the rounding floor of the residual of an FP64 p.
 __global__ void __launch_bounds__(RB)
-residual_kernel(const double* __restrict__ b, const double* __restrict__ ax, double* __restrict__ r,
-                size_t n, double* __restrict__ part) {
-    double acc = 0.0;
-    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+residual_kernel(const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ r,
+                const uint8_t* __restrict__ s, const GeoIJ* __restrict__ geo,
+                const double* __restrict__ yw, OpC q, double* __restrict__ part) {
+    const size_t plane = (size_t)q.jm * q.KP, row = q.KP;
+    const size_t NP = (size_t)q.im * plane;
+    double acc_r = 0.0, acc_v = 0.0;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < NP;
          c += (size_t)gridDim.x * blockDim.x) {
-        const double v = b[c] - ax[c];
-        r[c] = v;
-        acc += v * v;
+        double out = 0.0;
+        if (yw[c] > 0.0) {
+            const int k = (int)(c % row);
+            const int j = (int)((c / row) % q.jm);
+            const int i = (int)(c / plane);
+            const GeoIJ& g = geo[i * q.jm + j];
+            const double n1 = q.n1, n2 = g.num2, n3 = g.num3, xc = x[c];
+            const int kw = (k == 0) ? q.km - 2 : k - 1;
+            const int ke = (k == q.km - 2) ? 0 : k + 1;
+            double t[6] = {0, 0, 0, 0, 0, 0};
+            if (!s[c + plane]) t[0] = (i + 1 == q.im - 1) ? n1 * kC13 * (xc - x[c - plane]) : n1 * (x[c + plane] - xc);
+            if (!s[c - plane]) t[1] = (i - 1 == 0) ? n1 * kC13 * (xc - x[c + plane]) : n1 * (x[c - plane] - xc);
+            if (!s[c + row]) t[2] = (j + 1 == q.jm - 1) ? n2 * kC13 * (xc - x[c - row]) : n2 * (x[c + row] - xc);
+            if (!s[c - row]) t[3] = (j - 1 == 0) ? n2 * kC13 * (xc - x[c + row]) : n2 * (x[c - row] - xc);
+            if (!s[c - k + ke]) t[4] = n3 * (x[c - k + ke] - xc);
+            if (!s[c - k + kw]) t[5] = n3 * (x[c - k + kw] - xc);
+            const double ax = ((t[0] + t[1]) + (t[2] + t[3])) + (t[4] + t[5]);
+            const double v = fabs(t[0]) + fabs(t[1]) + fabs(t[2]) + fabs(t[3]) + fabs(t[4]) + fabs(t[5]);
+            out = b[c] - ax;
+            acc_r += out * out;
+            acc_v += v * v;
+        }
+        r[c] = out;
     }
-    __shared__ double sh[RB / 32];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __shared__ double sh[2][RB / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_r += __shfl_down_sync(0xffffffffu, acc_r, o);
+        acc_v += __shfl_down_sync(0xffffffffu, acc_v, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = acc_r; sh[1][threadIdx.x >> 5] = acc_v; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < RB / 32; w++) t += sh[w];
-        part[blockIdx.x] = t;
+        double tr = 0.0, tv = 0.0;
+        for (int w = 0; w < RB / 32; w++) { tr += sh[0][w]; tv += sh[1][w]; }
+        part[blockIdx.x] = tr;
+        part[NRED + blockIdx.x] = tv;
     }
+}
+
+// r -= (y.r / y.1) on fluid interior cells: keeps the recursive residual in the range of A
+__global__ void reproject_kernel(float* __restrict__ r32, double* __restrict__ r64,
+                                 const double* __restrict__ yw, const double* __restrict__ scal,
+                                 size_t n) {
+    const double mean = scal[11] / scal[6];
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (size_t)gridDim.x * blockDim.x)
+        if (yw[c] > 0.0) {
+            if (r32) r32[c] -= (float)mean;
+            if (r64) r64[c] -= mean;
+        }
 }
 
 // b (masked copy of the source or the external right-hand side) and p (masked warm start)
@@ -603,6 +648,13 @@ int pcg(AtjupCtx* c, Solver* S, Vecs<T>& V, double tol, int max_iter, int* iters
         if ((rc = precond(0))) return rc;
         direction_kernel<T><<<nb, RB, 0, st>>>(V.d, V.z, S->scal, NP, 0); c->launches++;
         if (it % check == 0 || it == max_iter) {
+            // drop the rounding drift of r out of the range of A (its y-component)
+            dot_kernel<double, T><<<nb, RB, 0, st>>>(S->yw, V.r, nullptr, NP, part);
+            finalize_kernel<<<1, 1, 0, st>>>(part, nb, S->scal, 11, 0);
+            reproject_kernel<<<nb, RB, 0, st>>>(std::is_same<T, float>::value ? (float*)V.r : nullptr,
+                                                std::is_same<T, double>::value ? (double*)V.r : nullptr,
+                                                S->yw, S->scal, NP);
+            c->launches += 3;
             ATJUP_CUDA(cudaMemcpyAsync(S->hs, S->scal, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
             ATJUP_CUDA(cudaStreamSynchronize(st));
             rr = S->hs[3];
@@ -674,21 +726,25 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
     ATJUP_CUDA(cudaStreamSynchronize(stm));
     const double bnorm = std::sqrt(S->hs[9]);
     int total_it = 0, inner = 0;
-    double rel = 0.0;
+    double rel = 0.0, floor_rel = 0.0, prev = 1e300;
     const bool mixed = (o->precision == ATJUP_PREC_MIXED);
-    // FP64 iterative refinement: r = b - A p (FP64); correction solve A e = r; p += e.
-    // FP64 inner solves converge in one pass; FP32 inner solves run to 1e-5 each.
-    const int max_outer = mixed ? 12 : 4;
-    for (int outer = 0; outer < max_outer; outer++) {
-        apply_kernel<double><<<nb, RB, 0, stm>>>(p64, V.q, c->solid, c->geo, S->yw, q, nullptr);
-        residual_kernel<<<nb, RB, 0, stm>>>(b64, V.q, V.b, NP, S->part);
+    // Iterative refinement with the residual formed in FP64: r = b - A p; solve A e = r
+    // (FP64 PCG, or FP32 PCG for the mixed form); p += e. Stops at the tolerance, or when the
+    // residual no longer falls (it has reached the rounding floor of an FP64 p, reported).
+    const int max_outer = mixed ? 24 : 8;
+    for (int outer = 0; outer <= max_outer; outer++) {
+        residual_kernel<<<nb, RB, 0, stm>>>(b64, p64, V.b, c->solid, c->geo, S->yw, q, S->part);
         finalize_kernel<<<1, 1, 0, stm>>>(S->part, nb, S->scal, 10, 0);
+        finalize_kernel<<<1, 1, 0, stm>>>(S->part + NRED, nb, S->scal, 12, 0);
         c->launches += 3;
         ATJUP_CUDA(cudaMemcpyAsync(S->hs, S->scal, sizeof(double) * 16, cudaMemcpyDeviceToHost, stm));
         ATJUP_CUDA(cudaStreamSynchronize(stm));
         rel = (bnorm > 0.0) ? std::sqrt(S->hs[10]) / bnorm : 0.0;
+        floor_rel = (bnorm > 0.0) ? 2.220446049250313e-16 * std::sqrt(S->hs[12]) / bnorm : 0.0;
         if (!std::isfinite(rel)) { set_error("pressure_solve: non-finite residual"); return ATJUP_ERR_NONFINITE; }
-        if (rel <= o->rel_tol || total_it >= o->max_iter) break;
+        if (rel <= o->rel_tol || total_it >= o->max_iter || outer == max_outer) break;
+        if (outer > 0 && rel > 0.5 * prev) break;            // stalled at the FP64 floor
+        prev = rel;
         int it = 0;
         double inner_rel = 0.0;
         const int budget = o->max_iter - total_it;
@@ -696,12 +752,12 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
             Vecs<float>& W = S->v32;
             convert_kernel<double, float><<<nb, RB, 0, stm>>>(V.b, W.b, NP);
             c->launches++;
-            if ((rc = pcg<float>(c, S, W, 1e-5, budget, &it, &inner_rel))) return rc;
+            if ((rc = pcg<float>(c, S, W, 1e-4, budget, &it, &inner_rel))) return rc;
             refine_kernel<<<nb, RB, 0, stm>>>(p64, W.p, NP);
             c->launches++;
         } else {
-            const double tgt = std::max(o->rel_tol * bnorm / std::max(std::sqrt(S->hs[10]), 1e-300), 1e-14);
-            if ((rc = pcg<double>(c, S, V, std::min(0.5, tgt * 0.5), budget, &it, &inner_rel))) return rc;
+            const double tgt = o->rel_tol * bnorm / std::max(std::sqrt(S->hs[10]), 1e-300);
+            if ((rc = pcg<double>(c, S, V, std::min(1e-3, std::max(0.5 * tgt, 1e-12)), budget, &it, &inner_rel))) return rc;
             add_kernel<<<nb, RB, 0, stm>>>(p64, V.p, NP);
             c->launches++;
         }
@@ -723,8 +779,10 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
         st->inner_solves = inner;
         st->rel_residual = rel;
         st->b_norm = bnorm;
+        st->rel_floor = floor_rel;
     }
-    if (rel > o->rel_tol) {
+    // converged: at the tolerance, or within a small factor of the FP64 floor above it
+    if (rel > o->rel_tol && rel > 8.0 * floor_rel) {
         set_error("pressure_solve: residual " + std::to_string(rel) + " above tolerance after " +
                   std::to_string(total_it) + " iterations");
         return ATJUP_ERR_NOT_CONVERGED;

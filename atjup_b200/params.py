@@ -75,7 +75,8 @@ class AtjupSolveOpts(ctypes.Structure):
 
 class AtjupSolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("inner_solves", ctypes.c_int32),
-                ("rel_residual", ctypes.c_double), ("b_norm", ctypes.c_double)]
+                ("rel_residual", ctypes.c_double), ("b_norm", ctypes.c_double),
+                ("rel_floor", ctypes.c_double)]
 
 
 # Mixture constants the reference derives at start-up from its default composition

@@ -125,6 +125,9 @@ typedef struct AtjupSolveStats {
     int32_t inner_solves;  /* MIXED: FP32 inner solves under the FP64 refinement loop            */
     double rel_residual;   /* final ||b - A p|| / ||b||, or -1 when not computed (SWEEPS)       */
     double b_norm;         /* ||b|| of the projected right-hand side                              */
+    double rel_floor;      /* eps * || sum_faces |num (p_nb - p)| || / ||b||: the rounding floor  */
+                           /* of the relative residual of an FP64 p (RESIDUAL); the solve counts  */
+                           /* as converged at rel_tol or, when rel_tol is below it, at <= 8 floor */
 } AtjupSolveStats;
 
 typedef struct AtjupCtx AtjupCtx;

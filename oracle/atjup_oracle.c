@@ -549,26 +549,39 @@ void ora_pressure_sweeps(const AtjupParams* P, const ora_grid* G, ora_state* S, 
 }
 
 /* A p = sum over kept faces of num (p_nb - p), with the boundary values read as the folds set
- * them from the interior (the fixed point of the sweep satisfies A p = src).                  */
-void ora_pressure_apply(const AtjupParams* P, const ora_grid* G, const double* p_in, double* Ap) {
+ * them from the interior (the fixed point of the sweep satisfies A p = src). Evaluated as a sum of
+ * differences so that a large smooth p (the solution's column-constant part is ~1e6 times the
+ * source) loses no digits to cancellation: a folded face contributes num (1/3)(p_c - p_in).   */
+void ora_pressure_apply(const AtjupParams* P, const ora_grid* G, const double* p, double* Ap) {
     const int im = P->im, jm = P->jm, km = P->km;
     const size_t N = (size_t)im * jm * km;
-    double* p = (double*)malloc(sizeof(double) * N);
-    memcpy(p, p_in, sizeof(double) * N);
-    press_fold(P, p);
+    const uint8_t* sol = G->solid;
     memset(Ap, 0, sizeof(double) * N);
     for (int i = 1; i < im - 1; i++)
         for (int j = 1; j < jm - 1; j++) {
             geom g; double n1, n2, n3;
             press_weights(P, G, i, j, &g, &n1, &n2, &n3);
             for (int k = 0; k < km - 1; k++) {
-                double acc;
-                const double den = press_gather(P, G, p, i, j, k, n1, n2, n3, &acc);
-                if (den <= 0.0) continue;
-                Ap[IDX(i, j, k)] = acc - den * p[IDX(i, j, k)];
+                const size_t c = IDX(i, j, k);
+                const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+                const double pc = p[c];
+                double s = 0.0;
+                if (!sol[c] || !P->press_wall) {
+                    /* radial faces */
+                    if (!sol[IDX(i + 1, j, k)] || !P->press_wall)
+                        s += (i + 1 == im - 1) ? n1 * C13 * (pc - p[IDX(i - 1, j, k)]) : n1 * (p[IDX(i + 1, j, k)] - pc);
+                    if (!sol[IDX(i - 1, j, k)] || !P->press_wall)
+                        s += (i - 1 == 0) ? n1 * C13 * (pc - p[IDX(i + 1, j, k)]) : n1 * (p[IDX(i - 1, j, k)] - pc);
+                    if (!sol[IDX(i, j + 1, k)] || !P->press_wall)
+                        s += (j + 1 == jm - 1) ? n2 * C13 * (pc - p[IDX(i, j - 1, k)]) : n2 * (p[IDX(i, j + 1, k)] - pc);
+                    if (!sol[IDX(i, j - 1, k)] || !P->press_wall)
+                        s += (j - 1 == 0) ? n2 * C13 * (pc - p[IDX(i, j + 1, k)]) : n2 * (p[IDX(i, j - 1, k)] - pc);
+                    if (!sol[IDX(i, j, ke)] || !P->press_wall) s += n3 * (p[IDX(i, j, ke)] - pc);
+                    if (!sol[IDX(i, j, kw)] || !P->press_wall) s += n3 * (p[IDX(i, j, kw)] - pc);
+                }
+                Ap[c] = s;
             }
         }
-    free(p);
 }
 
 /* ------------------------------------------------------------------------------------------ */
