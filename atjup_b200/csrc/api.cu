@@ -66,7 +66,7 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->solve_b); cudaFree(c->dsum);
     if (c->hsum) cudaFreeHost(c->hsum);
-    cudaFree(c->solid); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
+    cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
     cudaFree(c->sin_the); cudaFree(c->rad); cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
     cudaFree(c->solid_list); cudaFree(c->amb_rows); cudaFree(c->yw);
     cudaFree(c->line_a); cudaFree(c->line_c); cudaFree(c->line_m);
@@ -147,7 +147,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     AtjupCtx* c = new AtjupCtx();
     c->P = P;
     c->device = dev;
-    c->KP = (P.km + 15) / 16 * 16;
+    c->KP = (P.km + 3 + 15) / 16 * 16;   // >= km + 3: 4-byte flag copies near the row end stay in the row
     c->NP = (size_t)P.im * P.jm * c->KP;
     int rc = ATJUP_OK;
     auto A = [&](double** p, size_t n) { if (rc == ATJUP_OK) rc = alloc(p, n); };
@@ -236,6 +236,28 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
     std::vector<uint8_t> s_pad(c->NP, 0);
     for (size_t r = 0; r < (size_t)im * jm; r++)
         for (int k = 0; k < km; k++) s_pad[r * KP + k] = solid[r * km + k] ? 1 : 0;
+    // per-cell flags for the RK stage: bit 0 solid, 1..6 solid neighbour (i+1, i-1, j+1, j-1,
+    // k+1 and k-1 on the meridian ring), 7 integrated by the RK step
+    std::vector<uint8_t> nbh(c->NP, 0);
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) {
+                auto S_ = [&](int ii, int jj, int kk) -> bool {
+                    if (ii < 0 || ii >= im || jj < 0 || jj >= jm || kk < 0 || kk >= km) return false;
+                    return solid[((size_t)ii * jm + jj) * km + kk] != 0;
+                };
+                const int ke = (k >= km - 2) ? 0 : k + 1, kw = (k == 0) ? km - 2 : k - 1;
+                uint8_t f = 0;
+                if (S_(i, j, k)) f |= 1;
+                if (S_(i + 1, j, k)) f |= 2;
+                if (S_(i - 1, j, k)) f |= 4;
+                if (S_(i, j + 1, k)) f |= 8;
+                if (S_(i, j - 1, k)) f |= 16;
+                if (S_(i, j, ke)) f |= 32;
+                if (S_(i, j, kw)) f |= 64;
+                if (i >= 1 && i <= im - 2 && j >= 3 && j <= jm - 4 && k <= km - 2 && !(f & 1)) f |= 128;
+                nbh[((size_t)i * jm + j) * KP + k] = f;
+            }
     // solid-cell list for bcSolidGround (BC_Jup.h:496-590): first direction with two fluid cells
     auto sol = [&](int i, int j, int k) -> bool {
         if (i < 0 || i >= im || j < 0 || j >= jm || k < 0 || k >= km) return true;
@@ -273,6 +295,7 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
         }
     if (!c->solid) {
         ATJUP_CUDA(cudaMalloc(&c->solid, c->NP));
+        ATJUP_CUDA(cudaMalloc(&c->nbflags, c->NP));
         ATJUP_CUDA(cudaMalloc(&c->topo, sizeof(int32_t) * (size_t)jm * km));
         ATJUP_CUDA(cudaMalloc(&c->geo, sizeof(GeoIJ) * geo.size()));
         ATJUP_CUDA(cudaMalloc(&c->cor_col, sizeof(double) * jm));
@@ -280,6 +303,7 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
         ATJUP_CUDA(cudaMalloc(&c->rad, sizeof(double) * im));
     }
     ATJUP_CUDA(cudaMemcpy(c->solid, s_pad.data(), c->NP, cudaMemcpyHostToDevice));
+    ATJUP_CUDA(cudaMemcpy(c->nbflags, nbh.data(), c->NP, cudaMemcpyHostToDevice));
     ATJUP_CUDA(cudaMemcpy(c->topo, i_topo, sizeof(int32_t) * (size_t)jm * km, cudaMemcpyHostToDevice));
     ATJUP_CUDA(cudaMemcpy(c->geo, geo.data(), sizeof(GeoIJ) * geo.size(), cudaMemcpyHostToDevice));
     ATJUP_CUDA(cudaMemcpy(c->cor_col, cor_col.data(), sizeof(double) * jm, cudaMemcpyHostToDevice));

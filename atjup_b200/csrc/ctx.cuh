@@ -72,6 +72,7 @@ struct AtjupCtx {
 
     // static grid
     uint8_t* solid = nullptr;
+    uint8_t* nbflags = nullptr;    // per-cell neighbour-solid and integrated flags (rk4.cu)
     int32_t* topo = nullptr;
     atjup::GeoIJ* geo = nullptr;   // [im * jm]
     double* cor_col = nullptr;     // [jm] Coriolis factor of the hydrostatic integral
@@ -125,6 +126,9 @@ int launch_pressure_fold(AtjupCtx* c, double* p);
 int launch_bc(AtjupCtx* c, int which);
 int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passes, int use_topo);
 int launch_balance_v(AtjupCtx* c);
+int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, double* dvc,
+                             double* dvrow, int im, int jm, int km, int pitch, double dr,
+                             int zonal, cudaStream_t st);
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);

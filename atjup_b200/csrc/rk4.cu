@@ -14,7 +14,20 @@
 namespace atjup {
 namespace {
 
-constexpr int BX = 32, BY = 8;
+// Block tile: TK meridians x TJ colatitude rows, marching through a chunk of the radial planes.
+// The tiles cover the km-1 = 360 distinct meridians exactly (10 x 36); the seam copy k = km-1 is
+// never read by a stage (the ring wraps 359 -> 0) and is left alone.
+constexpr int TK = 36, TJ = 7, NT = 256, NL = TK * TJ;   // 252 live threads of 256
+constexpr int NCH = 3;                                   // radial chunks per column tile
+constexpr int HK = TK + 2, HJ = TJ + 2, HC = HK * HJ;   // halo tile of one plane
+constexpr int NF = 6;                                   // t, u, v, w, p_dyn, p_hydro
+constexpr int NX = 10;                                  // per-cell inputs: Y[4], acc[4], rho, wall_nue
+
+// Per-cell flags, precomputed from the static mask (atjup_gpu_set_grid): bit 0 solid, 1 solid i+1,
+// 2 solid i-1, 3 solid j+1, 4 solid j-1, 5 solid k+1 (ring), 6 solid k-1 (ring), 7 integrated
+// (i in [1, im-2], j in [3, jm-4], k in [0, km-2], not solid).
+enum : uint8_t { NB_S = 1, NB_IP = 2, NB_IM = 4, NB_JP = 8, NB_JM = 16, NB_KP = 32, NB_KM = 64,
+                 NB_INT = 128 };
 
 struct StageConst {
     int im, jm, km, KP;
@@ -40,203 +53,322 @@ struct StagePtrs {
     double* acc[4];
     const double *p_dyn, *p_hydro, *p_stat, *rho, *wall_nue, *nue, *Q_rad, *Q_precip;
     double *aux_u, *aux_v, *aux_w;
-    const uint8_t* solid;
+    const uint8_t* nb;
     const GeoIJ* geo;
     const double* buoy_ref;
     const double *cell_vbar0, *cell_ubar0;
 };
 
+struct __align__(16) StageSmem {
+    double tile[3][NF][HC];   // planes i, i+1, i+2 (in flight) with a one-cell halo in j and k
+    double ps[3][NT];         // p_stat at the cells of the same three planes
+    double ex[2][NX][NT];     // per-cell inputs of planes i and i+1
+    GeoIJ geo[2][TJ];         // geometry rows of planes i and i+1
+    double cm[2][2][TJ];      // cell-hold means (v, u) of planes i and i+1
+    uint8_t nb[2][NT];        // per-cell flags of planes i and i+1
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 
-__global__ void __launch_bounds__(BX * BY)
+// Issue the asynchronous copies of plane i's halo tile and p_stat into ring slot i % 3.
+__device__ __forceinline__ void issue_tile(StageSmem& S, const StagePtrs& a, const StageConst& q,
+                                           int i, int j0, int k0, int tid) {
+    const int sl = i % 3;
+    const size_t base = (size_t)i * q.jm * q.KP;
+    const double* src[NF] = {a.X[0], a.X[1], a.X[2], a.X[3], a.p_dyn, a.p_hydro};
+    for (int e = tid; e < NF * HC; e += NT) {
+        const int f = e / HC, h = e - f * HC;
+        const int hj = h / HK, hk = h - hj * HK;
+        int j = j0 - 1 + hj;
+        j = j < 0 ? 0 : (j > q.jm - 1 ? q.jm - 1 : j);
+        int k = k0 - 1 + hk;          // the ring of km-1 meridians: k-1 of 0 is km-2, k+1 of km-2 is 0
+        k = (k < 0) ? q.km - 2 : (k >= q.km - 1 ? 0 : k);   // (beyond km-1: unused lanes)
+        cp_async8(&S.tile[sl][f][h], src[f] + base + (size_t)j * q.KP + k);
+    }
+    if (tid < NL) {
+        const int tx = tid % TK, ty = tid / TK;
+        const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
+        cp_async8(&S.ps[sl][tid], a.p_stat + base + (size_t)j * q.KP + k);
+    }
+}
+
+// Issue the copies of plane i's per-cell inputs, geometry rows and cell means into slot i % 2.
+__device__ __forceinline__ void issue_extra(StageSmem& S, const StagePtrs& a, const StageConst& q,
+                                            int i, int j0, int k0, int tid) {
+    const int sl = i & 1;
+    if (tid < NL) {
+        const int tx = tid % TK, ty = tid / TK;
+        const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
+        const size_t c = ((size_t)i * q.jm + j) * q.KP + k;
+        if (q.stage > 0) {
+#pragma unroll
+            for (int f = 0; f < 4; f++) {
+                cp_async8(&S.ex[sl][f][tid], a.Y[f] + c);
+                cp_async8(&S.ex[sl][4 + f][tid], a.acc[f] + c);
+            }
+        }
+        cp_async8(&S.ex[sl][8][tid], a.rho + c);
+        cp_async8(&S.ex[sl][9][tid], a.wall_nue + c);
+    }
+    // flags: 4 bytes per copy along a tile row (k0 and the row pitch are multiples of 4)
+    if (tid < TJ * (TK / 4) && k0 + 4 * (tid % (TK / 4)) <= q.km - 2) {
+        const int ty = tid / (TK / 4), kq = tid % (TK / 4);
+        const int j = min(j0 + ty, q.jm - 1);
+        cp_async4(&S.nb[sl][ty * TK + 4 * kq], a.nb + ((size_t)i * q.jm + j) * q.KP + k0 + 4 * kq);
+    }
+    // geometry rows (sizeof(GeoIJ) / 8 doubles per row) and the cell-hold means
+    constexpr int GD = (int)(sizeof(GeoIJ) / 8);
+    for (int e = tid; e < TJ * GD; e += NT) {
+        const int r = e / GD, f = e % GD;
+        const int j = min(j0 + r, q.jm - 1);
+        cp_async8(reinterpret_cast<double*>(&S.geo[sl][r]) + f,
+                  reinterpret_cast<const double*>(a.geo + (size_t)i * q.jm + j) + f);
+    }
+    if (q.cell_hold && tid < 2 * TJ) {
+        const int f = tid / TJ, r = tid % TJ;
+        const int j = min(j0 + r, q.jm - 1);
+        cp_async8(&S.cm[sl][f][r], (f == 0 ? a.cell_vbar0 : a.cell_ubar0) + (size_t)i * q.jm + j);
+    }
+}
+
+// One RK stage: every (j, k) column of the block's tile, plane by plane.
+__global__ void __launch_bounds__(NT, 2)
 rk_stage_kernel(StagePtrs a, StageConst q) {
-    const int k = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= q.km || j >= q.jm) return;
-    const size_t row = (size_t)q.KP;
-    const size_t plane = (size_t)q.jm * row;
-    const size_t c = (size_t)i * plane + (size_t)j * row + k;
-    const bool integ = (i >= 1) && (i <= q.im - 2) && (j >= 3) && (j <= q.jm - 4) &&
-                       (k <= q.km - 2) && !a.solid[c];
-    if (!integ) {
-        if (q.stage < 3) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    const int tid = threadIdx.x;
+    const int tx = tid % TK, ty = tid / TK;
+    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+    const int k = k0 + tx, j = j0 + ty;
+    const bool live = (tid < NL) && (k <= q.km - 2) && (j < q.jm);
+    const size_t row = (size_t)q.KP, plane = (size_t)q.jm * row;
+    const int h = (ty + 1) * HK + (tx + 1);           // this cell in the halo tile
+    // radial chunk [i_lo, i_hi); the march starts one plane below to fill the radial window
+    const int per = (q.im + NCH - 1) / NCH;
+    const int i_lo = blockIdx.z * per, i_hi = min(q.im, i_lo + per);
+    const int i_st = (i_lo > 0) ? i_lo - 1 : 0;
+
+    issue_tile(S, a, q, i_st, j0, k0, tid);
+    issue_extra(S, a, q, i_st, j0, k0, tid);
+    cp_commit();
+    if (i_st + 1 < q.im) issue_tile(S, a, q, i_st + 1, j0, k0, tid);
+    cp_commit();
+
+    // radial window: the cell's values in plane i-1 (t, u, v, w, p_dyn, p_stat)
+    double m_t = 0.0, m_u = 0.0, m_v = 0.0, m_w = 0.0, m_pd = 0.0, m_ps = 0.0;
+
+    for (int i = i_st; i < i_hi; i++) {
+        if (i + 2 < q.im && i + 2 <= i_hi) issue_tile(S, a, q, i + 2, j0, k0, tid);
+        if (i + 1 < i_hi) issue_extra(S, a, q, i + 1, j0, k0, tid);
+        cp_commit();
+        cp_wait1();
+        __syncthreads();
+
+        const int cs = i % 3, ns = (i + 1) % 3, xs = i & 1;
+        const double* Tt = S.tile[cs][0];
+        const double* Ut = S.tile[cs][1];
+        const double* Vt = S.tile[cs][2];
+        const double* Wt = S.tile[cs][3];
+        const double* Pt = S.tile[cs][4];
+        const double* Ht = S.tile[cs][5];
+        if (live && i >= i_lo) {
+            const size_t c = (size_t)i * plane + (size_t)j * row + k;
+            const uint8_t nbm = S.nb[xs][tid];
+            if (!(nbm & NB_INT)) {
+                if (q.stage == 0) {
 #pragma unroll
-            for (int f = 0; f < 4; f++) a.Xo[f][c] = a.Y[f][c];
-        }
-        return;
-    }
-    const GeoIJ& g = a.geo[i * q.jm + j];
-    const int kw = (k == 0) ? q.km - 2 : k - 1;
-    const int ke = (k == q.km - 2) ? 0 : k + 1;
-    const size_t cip = c + plane, cim = c - plane, cjp = c + row, cjm = c - row;
-    const size_t ckp = c - k + ke, ckm = c - k + kw;
-
-    const double* T = a.X[0];
-    const double* U = a.X[1];
-    const double* V = a.X[2];
-    const double* W = a.X[3];
-    const double t0 = ld(T + c), u0 = ld(U + c), v0 = ld(V + c), w0 = ld(W + c);
-
-    // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
-#define DERIVS(F, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
-    const double d1r = (ld(F + cip) - ld(F + cim)) * q.inv_2dr;               \
-    const double d2r = (ld(F + cip) - 2.0 * f0 + ld(F + cim)) * q.inv_dr2;    \
-    const double d1t = (ld(F + cjp) - ld(F + cjm)) * q.inv_2dthe;             \
-    const double d2t = (ld(F + cjp) - 2.0 * f0 + ld(F + cjm)) * q.inv_dthe2;  \
-    const double d1p = (ld(F + ckp) - ld(F + ckm)) * q.inv_2dphi;             \
-    const double d2p = (ld(F + ckp) - 2.0 * f0 + ld(F + ckm)) * q.inv_dphi2;
-    DERIVS(T, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
-    DERIVS(U, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
-    DERIVS(V, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
-    DERIVS(W, w0, dwdr, d2wdr2, dwdthe, d2wdthe2, dwdphi, d2wdphi2)
+                    for (int f = 0; f < 4; f++) a.Xo[f][c] = ld(a.Y[f] + c);
+                } else if (q.stage < 3) {
+#pragma unroll
+                    for (int f = 0; f < 4; f++) a.Xo[f][c] = S.ex[xs][f][tid];
+                }
+            } else {
+                const GeoIJ& g = S.geo[xs][ty];
+                const double t0 = Tt[h], u0 = Ut[h], v0 = Vt[h], w0 = Wt[h];
+                const double* Tn = S.tile[ns][0];
+                const double* Un = S.tile[ns][1];
+                const double* Vn = S.tile[ns][2];
+                const double* Wn = S.tile[ns][3];
+                // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
+#define DERIVS(F, FN, FM, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
+    const double d1r = (FN[h] - FM) * q.inv_2dr;                                      \
+    const double d2r = (FN[h] - 2.0 * f0 + FM) * q.inv_dr2;                           \
+    const double d1t = (F[h + HK] - F[h - HK]) * q.inv_2dthe;                         \
+    const double d2t = (F[h + HK] - 2.0 * f0 + F[h - HK]) * q.inv_dthe2;              \
+    const double d1p = (F[h + 1] - F[h - 1]) * q.inv_2dphi;                           \
+    const double d2p = (F[h + 1] - 2.0 * f0 + F[h - 1]) * q.inv_dphi2;
+                DERIVS(Tt, Tn, m_t, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
+                DERIVS(Ut, Un, m_u, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
+                DERIVS(Vt, Vn, m_v, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
+                DERIVS(Wt, Wn, m_w, w0, dwdr, d2wdr2, dwdthe, d2wdthe2, dwdphi, d2wdphi2)
 #undef DERIVS
+                // pressure gradients, solid faces mirrored to the local value (RHS_Jup_Turb.cpp:119-130)
+                const bool wall = q.pgrad_wall;
+                const double pc = Pt[h];
+                const double pip = (wall && (nbm & NB_IP)) ? pc : S.tile[ns][4][h];
+                const double pim = (wall && (nbm & NB_IM)) ? pc : m_pd;
+                const double pjp = (wall && (nbm & NB_JP)) ? pc : Pt[h + HK];
+                const double pjm = (wall && (nbm & NB_JM)) ? pc : Pt[h - HK];
+                const double pkp = (wall && (nbm & NB_KP)) ? pc : Pt[h + 1];
+                const double pkm = (wall && (nbm & NB_KM)) ? pc : Pt[h - 1];
+                const double dpdr = (pip - pim) * q.inv_2dr;
+                const double dpdthe = (pjp - pjm) * q.inv_2dthe;
+                const double dpdphi = (pkp - pkm) * q.inv_2dphi;
 
-    // pressure gradients with solid faces mirrored to the local value (RHS_Jup_Turb.cpp:119-130)
-    const uint8_t s_ip = a.solid[cip], s_im = a.solid[cim], s_jp = a.solid[cjp];
-    const uint8_t s_jm = a.solid[cjm], s_kp = a.solid[ckp], s_km = a.solid[ckm];
-    const double pc = ld(a.p_dyn + c);
-    auto pg = [&](const double* P, size_t hi, size_t lo, uint8_t sh, uint8_t sl, double loc,
-                  double inv2d) -> double {
-        const double h = (q.pgrad_wall && sh) ? loc : ld(P + hi);
-        const double l = (q.pgrad_wall && sl) ? loc : ld(P + lo);
-        return (h - l) * inv2d;
-    };
-    const double dpdr = pg(a.p_dyn, cip, cim, s_ip, s_im, pc, q.inv_2dr);
-    const double dpdthe = pg(a.p_dyn, cjp, cjm, s_jp, s_jm, pc, q.inv_2dthe);
-    const double dpdphi = pg(a.p_dyn, ckp, ckm, s_kp, s_km, pc, q.inv_2dphi);
+                // body forces (RHS_Jup_Turb.cpp:384-423)
+                const double Coriolis_rad = g.cor_rad * w0;
+                const double Coriolis_the = g.cor_the * w0;
+                double v_cor = v0, u_cor = u0;
+                if (q.cell_hold) {
+                    v_cor -= S.cm[xs][0][ty];
+                    u_cor -= S.cm[xs][1][ty];
+                }
+                const double Coriolis_phi = q.cor_phi_f * (+g.costhe * v_cor + g.sinthe_true * u_cor);
+                const double v_invrm = v0 * g.inv_rm;
+                const double w_invrs = w0 * g.inv_rmsinthe;
 
-    // body forces (RHS_Jup_Turb.cpp:384-423)
-    const double Coriolis_rad = g.cor_rad * w0;
-    const double Coriolis_the = g.cor_the * w0;
-    double v_cor = v0, u_cor = u0;
-    if (q.cell_hold) {
-        v_cor -= ld(a.cell_vbar0 + i * q.jm + j);
-        u_cor -= ld(a.cell_ubar0 + i * q.jm + j);
-    }
-    const double Coriolis_phi = q.cor_phi_f * (+g.costhe * v_cor + g.sinthe_true * u_cor);
+                // compression work with the hydrostatic part (RHS_Jup_Turb.cpp:459-482)
+                const double rho_l = S.ex[xs][8][tid];
+                double dpstatdr = 0.0;
+                if (q.adiabatic) {
+                    dpstatdr = (S.ps[ns][tid] - m_ps) * q.inv_2dr * q.to_nd;
+                    if (q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr *= q.r_mix / rho_l;
+                }
+                const double pressure_t = q.coeff_energy_p *
+                    (u0 * (dpdr + dpstatdr) + v_invrm * dpdthe + w_invrs * dpdphi);
+                const double transport_t = u0 * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
+                const double transport_u = u0 * dudr + v_invrm * dudthe + w_invrs * dudphi -
+                                           q.metric_on * (v0 * v0 + w0 * w0) * g.inv_rm;
+                const double transport_v = u0 * dvdr + v_invrm * dvdthe + w_invrs * dvdphi +
+                                           (u0 * v0 - w0 * w0 * g.cotanthe) * g.inv_rm;
+                const double transport_w = u0 * dwdr + v_invrm * dwdthe + w_invrs * dwdphi +
+                                           (w0 * u0 + v0 * w0 * g.cotanthe) * g.inv_rm;
 
-    const double v_invrm = v0 * g.inv_rm;
-    const double w_invrs = w0 * g.inv_rmsinthe;
+                // diffusion (RHS_Jup_Turb.cpp:521-545)
+                const double two_inv_rm = 2.0 * g.inv_rm;
+                const double diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * g.inv_rm2 +
+                                           dtdthe * g.costhe_inv_rm2sinthe + d2tdphi2 * g.inv_rm2sinthe2;
+                const double diffusion_u = d2udr2 + 2.0 * u0 * g.inv_rm2 + d2udthe2 * g.inv_rm2 +
+                                           4.0 * dudr * g.inv_rm + dudthe * g.costhe_inv_rm2sinthe +
+                                           d2udphi2 * g.inv_rm2sinthe2;
+                const double diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * g.inv_rm2 +
+                                           dvdthe * g.costhe_inv_rm2sinthe - g.v_metric * v0 +
+                                           d2vdphi2 * g.inv_rm2sinthe2 + 2.0 * dudthe * g.inv_rm2 -
+                                           dwdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+                const double diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * g.inv_rm2 +
+                                           dwdthe * g.costhe_inv_rm2sinthe - g.v_metric * w0 +
+                                           d2wdphi2 * g.inv_rm2sinthe2 + 2.0 * dudphi * g.inv_rm2sinthe +
+                                           dvdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
 
-    // compression work with the hydrostatic part (RHS_Jup_Turb.cpp:459-482)
-    const double rho_l = ld(a.rho + c);
-    double dpstatdr = 0.0;
-    if (q.adiabatic) {
-        dpstatdr = (ld(a.p_stat + cip) - ld(a.p_stat + cim)) * q.inv_2dr * q.to_nd;
-        if (q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr *= q.r_mix / rho_l;
-    }
-    const double pressure_t = q.coeff_energy_p *
-        (u0 * (dpdr + dpstatdr) + v_invrm * dpdthe + w_invrs * dpdphi);
-    const double transport_t = u0 * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
-    const double transport_u = u0 * dudr + v_invrm * dudthe + w_invrs * dudphi -
-                               q.metric_on * (v0 * v0 + w0 * w0) * g.inv_rm;
-    const double transport_v = u0 * dvdr + v_invrm * dvdthe + w_invrs * dvdphi +
-                               (u0 * v0 - w0 * w0 * g.cotanthe) * g.inv_rm;
-    const double transport_w = u0 * dwdr + v_invrm * dwdthe + w_invrs * dwdphi +
-                               (w0 * u0 + v0 * w0 * g.cotanthe) * g.inv_rm;
+                const double dpdr_term = q.pgrad_scale * dpdr;
+                const double dpdthe_term = q.pgrad_scale * dpdthe * g.inv_rm;
+                const double dpdphi_term = q.pgrad_scale * dpdphi * g.inv_rmsinthe;
+                double dphdthe_term = 0.0, dphdphi_term = 0.0;
+                if (q.use_hp) {
+                    const double hc = Ht[h];
+                    const double hjp = (wall && (nbm & NB_JP)) ? hc : Ht[h + HK];
+                    const double hjm = (wall && (nbm & NB_JM)) ? hc : Ht[h - HK];
+                    const double hkp = (wall && (nbm & NB_KP)) ? hc : Ht[h + 1];
+                    const double hkm = (wall && (nbm & NB_KM)) ? hc : Ht[h - 1];
+                    dphdthe_term = (hjp - hjm) * q.inv_2dthe * g.inv_rm;
+                    dphdphi_term = (hkp - hkm) * q.inv_2dphi * g.inv_rmsinthe;
+                }
 
-    // diffusion (RHS_Jup_Turb.cpp:521-545)
-    const double two_inv_rm = 2.0 * g.inv_rm;
-    const double diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * g.inv_rm2 +
-                               dtdthe * g.costhe_inv_rm2sinthe + d2tdphi2 * g.inv_rm2sinthe2;
-    const double diffusion_u = d2udr2 + 2.0 * u0 * g.inv_rm2 + d2udthe2 * g.inv_rm2 +
-                               4.0 * dudr * g.inv_rm + dudthe * g.costhe_inv_rm2sinthe +
-                               d2udphi2 * g.inv_rm2sinthe2;
-    const double diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * g.inv_rm2 +
-                               dvdthe * g.costhe_inv_rm2sinthe - g.v_metric * v0 +
-                               d2vdphi2 * g.inv_rm2sinthe2 + 2.0 * dudthe * g.inv_rm2 -
-                               dwdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
-    const double diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * g.inv_rm2 +
-                               dwdthe * g.costhe_inv_rm2sinthe - g.v_metric * w0 +
-                               d2wdphi2 * g.inv_rm2sinthe2 + 2.0 * dudphi * g.inv_rm2sinthe +
-                               dvdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+                // radiative and latent heating (RHS_Jup_Turb.cpp:646-718)
+                double radiation_t = 0.0, precip_t = 0.0;
+                if (q.has_heating) {
+                    if (q.rad_coupling != 0.0) {
+                        const double T_phys = t0 * q.t_ref;
+                        const double P_phys = S.ps[cs][tid] * 1.0e5;
+                        const double rho = (rho_l > 0.0 && isfinite(rho_l))
+                                               ? rho_l
+                                               : ((T_phys > 1.0) ? P_phys / (q.R_mix * T_phys) : 0.0);
+                        if (rho > 0.0 && q.cp_mix > 0.0) {
+                            radiation_t = q.rad_coupling * ld(a.Q_rad + c) * q.L_rad /
+                                          (rho * q.cp_mix * q.u_0 * q.t_ref);
+                            if (!isfinite(radiation_t)) radiation_t = 0.0;
+                            else if (radiation_t > 0.5) radiation_t = 0.5;
+                            else if (radiation_t < -0.5) radiation_t = -0.5;
+                        }
+                    }
+                    if (q.precip_coupling != 0.0) {
+                        double rho_p = q.r_mix;
+                        if (q.precip_local) rho_p = (rho_l > 0.0 && isfinite(rho_l)) ? rho_l : q.r_mix;
+                        if (rho_p > 0.0 && q.cp_mix > 0.0) {
+                            precip_t = q.precip_coupling * ld(a.Q_precip + c) * q.L_rad /
+                                       (rho_p * q.cp_mix * q.u_0 * q.t_ref);
+                            if (!isfinite(precip_t)) precip_t = 0.0;
+                            else if (precip_t > 0.5) precip_t = 0.5;
+                            else if (precip_t < -0.5) precip_t = -0.5;
+                        }
+                    }
+                }
 
-    const double dpdr_term = q.pgrad_scale * dpdr;
-    const double dpdthe_term = q.pgrad_scale * dpdthe * g.inv_rm;
-    const double dpdphi_term = q.pgrad_scale * dpdphi * g.inv_rmsinthe;
-    double dphdthe_term = 0.0, dphdphi_term = 0.0;
-    if (q.use_hp) {
-        const double hc = ld(a.p_hydro + c);
-        dphdthe_term = pg(a.p_hydro, cjp, cjm, s_jp, s_jm, hc, q.inv_2dthe) * g.inv_rm;
-        dphdphi_term = pg(a.p_hydro, ckp, ckm, s_kp, s_km, hc, q.inv_2dphi) * g.inv_rmsinthe;
-    }
+                double nue_t = 0.0;
+                if (q.has_nue) {
+                    const double nn = ld(a.nue + c);
+                    if (q.turb_coupling != 0.0 && isfinite(nn)) nue_t = q.turb_coupling * fmax(0.0, nn);
+                }
+                const double nue_t_s = nue_t / 0.9;
+                const double visc = q.inv_re + nue_t + S.ex[xs][9][tid];
 
-    // radiative and latent heating (RHS_Jup_Turb.cpp:646-718)
-    double radiation_t = 0.0, precip_t = 0.0;
-    if (q.has_heating) {
-        if (q.rad_coupling != 0.0) {
-            const double T_phys = t0 * q.t_ref;
-            const double P_phys = ld(a.p_stat + c) * 1.0e5;
-            const double rho = (rho_l > 0.0 && isfinite(rho_l))
-                                   ? rho_l
-                                   : ((T_phys > 1.0) ? P_phys / (q.R_mix * T_phys) : 0.0);
-            if (rho > 0.0 && q.cp_mix > 0.0) {
-                radiation_t = q.rad_coupling * ld(a.Q_rad + c) * q.L_rad /
-                              (rho * q.cp_mix * q.u_0 * q.t_ref);
-                if (!isfinite(radiation_t)) radiation_t = 0.0;
-                else if (radiation_t > 0.5) radiation_t = 0.5;
-                else if (radiation_t < -0.5) radiation_t = -0.5;
+                const double rhs_t = +pressure_t - transport_t + diffusion_t * (q.t_visc + nue_t_s) +
+                                     radiation_t + precip_t;
+                const double buoyancy_u =
+                    (t0 > 0.0) ? q.buoy_k * (q.g * S.ps[cs][tid] / (q.rR * t0 * q.t_ref) - a.buoy_ref[i])
+                               : 0.0;
+                const double rhs_u = -dpdr_term + (q.hydro_split ? 0.0 : buoyancy_u) - transport_u +
+                                     diffusion_u * visc - q.cor_rad_on * q.Coriolis * Coriolis_rad +
+                                     q.centrifugal * g.cent_rad;
+                const double rhs_v = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc -
+                                     q.Coriolis * Coriolis_the + q.centrifugal * g.cent_the;
+                const double rhs_w = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc -
+                                     q.Coriolis * Coriolis_phi;
+
+                // accumulate (RungeKutta_Jup_Turb.cpp:419-490), form the next stage input / result
+                const double rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
+                if (q.stage == 0) {
+                    const double y0[4] = {t0, u0, v0, w0};
+#pragma unroll
+                    for (int f = 0; f < 4; f++) {
+                        a.acc[f][c] = q.wgt * rhs[f];
+                        a.Xo[f][c] = y0[f] + q.c_in * rhs[f];
+                    }
+                } else if (q.stage < 3) {
+#pragma unroll
+                    for (int f = 0; f < 4; f++) {
+                        a.acc[f][c] = S.ex[xs][4 + f][tid] + q.wgt * rhs[f];
+                        a.Xo[f][c] = S.ex[xs][f][tid] + q.c_in * rhs[f];
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 4; f++) {
+                        const double acc3 = S.ex[xs][4 + f][tid] + q.wgt * rhs[f];
+                        a.Y[f][c] = S.ex[xs][f][tid] + q.dt * acc3 * q.one_sixth;
+                    }
+                    // the projection source the next pressure solve reads (the last stage's values)
+                    a.aux_u[c] = rhs_u + dpdr_term;
+                    a.aux_v[c] = rhs_v + dpdthe_term;
+                    a.aux_w[c] = rhs_w + dpdphi_term;
+                }
             }
         }
-        if (q.precip_coupling != 0.0) {
-            double rho_p = q.r_mix;
-            if (q.precip_local) rho_p = (rho_l > 0.0 && isfinite(rho_l)) ? rho_l : q.r_mix;
-            if (rho_p > 0.0 && q.cp_mix > 0.0) {
-                precip_t = q.precip_coupling * ld(a.Q_precip + c) * q.L_rad /
-                           (rho_p * q.cp_mix * q.u_0 * q.t_ref);
-                if (!isfinite(precip_t)) precip_t = 0.0;
-                else if (precip_t > 0.5) precip_t = 0.5;
-                else if (precip_t < -0.5) precip_t = -0.5;
-            }
+        if (live) {   // slide the radial window up one plane
+            m_t = Tt[h]; m_u = Ut[h]; m_v = Vt[h]; m_w = Wt[h]; m_pd = Pt[h];
+            m_ps = S.ps[cs][tid];
         }
-    }
-
-    double nue_t = 0.0;
-    if (q.has_nue) {
-        const double nn = ld(a.nue + c);
-        if (q.turb_coupling != 0.0 && isfinite(nn)) nue_t = q.turb_coupling * fmax(0.0, nn);
-    }
-    const double nue_t_s = nue_t / 0.9;
-    const double visc = q.inv_re + nue_t + ld(a.wall_nue + c);
-
-    const double rhs_t = +pressure_t - transport_t + diffusion_t * (q.t_visc + nue_t_s) +
-                         radiation_t + precip_t;
-    const double buoyancy_u =
-        (t0 > 0.0) ? q.buoy_k * (q.g * ld(a.p_stat + c) / (q.rR * t0 * q.t_ref) - a.buoy_ref[i])
-                   : 0.0;
-    const double rhs_u = -dpdr_term + (q.hydro_split ? 0.0 : buoyancy_u) - transport_u +
-                         diffusion_u * visc - q.cor_rad_on * q.Coriolis * Coriolis_rad +
-                         q.centrifugal * g.cent_rad;
-    const double rhs_v = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc -
-                         q.Coriolis * Coriolis_the + q.centrifugal * g.cent_the;
-    const double rhs_w = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc -
-                         q.Coriolis * Coriolis_phi;
-
-    // accumulate (RungeKutta_Jup_Turb.cpp:419-490) and form the next stage input / the result
-    const double rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
-    if (q.stage == 0) {
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            a.acc[f][c] = q.wgt * rhs[f];
-            a.Xo[f][c] = a.Y[f][c] + q.c_in * rhs[f];
-        }
-    } else if (q.stage < 3) {
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            a.acc[f][c] = a.acc[f][c] + q.wgt * rhs[f];
-            a.Xo[f][c] = a.Y[f][c] + q.c_in * rhs[f];
-        }
-    } else {
-#pragma unroll
-        for (int f = 0; f < 4; f++) {
-            const double acc3 = a.acc[f][c] + q.wgt * rhs[f];
-            a.Y[f][c] = a.Y[f][c] + q.dt * acc3 * q.one_sixth;
-        }
-        // the projection source the next pressure solve reads (the last stage's values)
-        a.aux_u[c] = rhs_u + dpdr_term;
-        a.aux_v[c] = rhs_v + dpdthe_term;
-        a.aux_w[c] = rhs_w + dpdphi_term;
+        __syncthreads();
     }
 }
 
@@ -384,7 +516,7 @@ int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* co
     a.aux_u = c->f[ATJUP_F_AUX_U];
     a.aux_v = c->f[ATJUP_F_AUX_V];
     a.aux_w = c->f[ATJUP_F_AUX_W];
-    a.solid = c->solid;
+    a.nb = c->nbflags;
     a.geo = c->geo;
     a.buoy_ref = c->buoy_ref;
     a.cell_vbar0 = c->cell_vbar0;
@@ -435,10 +567,15 @@ int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* co
     q.has_heating = (P.has_heating && a.Q_rad && a.Q_precip) ? 1 : 0;
     q.precip_local = (P.precip_rho_local && P.local_rho) ? 1 : 0;
 
-    dim3 block(BX, BY);
-    dim3 grid((P.km + BX - 1) / BX, (P.jm + BY - 1) / BY, P.im);
+    static bool attr_set = false;
+    if (!attr_set) {
+        ATJUP_CUDA(cudaFuncSetAttribute(rk_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(StageSmem)));
+        attr_set = true;
+    }
+    dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
     c->launches++;
-    rk_stage_kernel<<<grid, block, 0, c->stream>>>(a, q);
+    rk_stage_kernel<<<grid, NT, sizeof(StageSmem), c->stream>>>(a, q);
     ATJUP_CHECK_LAUNCH("rk_stage");
     return ATJUP_OK;
 }

@@ -24,6 +24,7 @@
 #include "ctx.cuh"
 
 #include <cmath>
+#include <cstdio>
 #include <type_traits>
 #include <vector>
 
@@ -177,17 +178,17 @@ update_kernel(T* __restrict__ p, T* __restrict__ r, const T* __restrict__ d, con
 }
 
 template <typename T>
-__global__ void direction_kernel(T* __restrict__ d, const T* __restrict__ z,
+__global__ void direction_kernel(double* __restrict__ d, const T* __restrict__ z,
                                  const double* __restrict__ scal, size_t n, int first) {
-    const T beta = first ? (T)0 : (T)scal[2];
+    const double beta = first ? 0.0 : scal[2];
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
          c += (size_t)gridDim.x * blockDim.x)
-        d[c] = first ? z[c] : z[c] + beta * d[c];
+        d[c] = first ? (double)z[c] : (double)z[c] + beta * d[c];
 }
 
 // Radial line solve A_line z = r per (j, k) column, and the column sum g = sum_i y r.
 template <typename T>
-__global__ void line_kernel(const T* __restrict__ r, T* __restrict__ z, const T* __restrict__ la,
+__global__ void line_kernel(const double* __restrict__ r, T* __restrict__ z, const T* __restrict__ la,
                             const T* __restrict__ lc, const T* __restrict__ lm,
                             const double* __restrict__ yw, T* __restrict__ g, OpC q) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -200,8 +201,8 @@ __global__ void line_kernel(const T* __restrict__ r, T* __restrict__ z, const T*
         const size_t c = b + (size_t)i * plane;
         const T m = lm[c];
         if (m == (T)0) { prev = 0; continue; }           // not a fluid interior cell
-        gs += yw[c] * (double)r[c];
-        prev = (r[c] - la[c] * prev) * m;
+        gs += yw[c] * r[c];
+        prev = ((T)r[c] - la[c] * prev) * m;
         z[c] = prev;
     }
     T next = 0;
@@ -275,7 +276,7 @@ __global__ void theta_solve_kernel(T* __restrict__ gh, const T* __restrict__ ta,
 template <typename T>
 __global__ void __launch_bounds__(128)
 dft_inv_kernel(const T* __restrict__ gh, const T* __restrict__ cs, const T* __restrict__ sn,
-               T* __restrict__ z, const T* __restrict__ r, const double* __restrict__ yw,
+               T* __restrict__ z, const double* __restrict__ r, const double* __restrict__ yw,
                const T* __restrict__ lm, OpC q, int N, int NM, int J, double* __restrict__ part) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int jj = blockIdx.y;
@@ -296,7 +297,7 @@ dft_inv_kernel(const T* __restrict__ gh, const T* __restrict__ cs, const T* __re
             if (lm[c] == (T)0) continue;
             const T zn = z[c] + (T)e;
             z[c] = zn;
-            acc += yw[c] * (double)r[c] * (double)zn;
+            acc += yw[c] * r[c] * (double)zn;
         }
     }
     __shared__ double sh[4];
@@ -306,20 +307,6 @@ dft_inv_kernel(const T* __restrict__ gh, const T* __restrict__ cs, const T* __re
     if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = sh[0] + sh[1] + sh[2] + sh[3];
 }
 
-template <typename Ts, typename Td>
-__global__ void convert_kernel(const Ts* __restrict__ a, Td* __restrict__ b, size_t n) {
-    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
-         c += (size_t)gridDim.x * blockDim.x)
-        b[c] = (Td)a[c];
-}
-
-// p64 += e32 (the refinement update)
-__global__ void refine_kernel(double* __restrict__ p, const float* __restrict__ e, size_t n) {
-    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
-         c += (size_t)gridDim.x * blockDim.x)
-        p[c] += (double)e[c];
-}
-
 // p64 += e64
 __global__ void add_kernel(double* __restrict__ p, const double* __restrict__ e, size_t n) {
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -327,8 +314,8 @@ __global__ void add_kernel(double* __restrict__ p, const double* __restrict__ e,
         p[c] += e[c];
 }
 
-// r = b - A p in FP64 on fluid interior cells, with partial sums of r^2 and of v^2, v = the
-// sum of |face terms| of A p: eps * ||v|| is the rounding floor of the residual of an FP64 p.
+// r = b - A p in FP64 on fluid interior cells, with partial sums of r^2 and of v^2, v = |A| |p|:
+// eps * ||v|| is the rounding floor of the residual of an FP64 p (one ulp of p moves it that much).
 __global__ void __launch_bounds__(RB)
 residual_kernel(const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ r,
                 const uint8_t* __restrict__ s, const GeoIJ* __restrict__ geo,
@@ -355,7 +342,15 @@ residual_kernel(const double* __restrict__ b, const double* __restrict__ x, doub
             if (!s[c - k + ke]) t[4] = n3 * (x[c - k + ke] - xc);
             if (!s[c - k + kw]) t[5] = n3 * (x[c - k + kw] - xc);
             const double ax = ((t[0] + t[1]) + (t[2] + t[3])) + (t[4] + t[5]);
-            const double v = fabs(t[0]) + fabs(t[1]) + fabs(t[2]) + fabs(t[3]) + fabs(t[4]) + fabs(t[5]);
+            // (|A| |x|)_c: the size of the terms whose rounding bounds the residual of an FP64 x
+            double den = 0.0, nb = 0.0;
+            if (!s[c + plane]) { const double w = (i + 1 == q.im - 1) ? n1 * kC13 : n1; den += w; nb += w * fabs((i + 1 == q.im - 1) ? x[c - plane] : x[c + plane]); }
+            if (!s[c - plane]) { const double w = (i - 1 == 0) ? n1 * kC13 : n1; den += w; nb += w * fabs((i - 1 == 0) ? x[c + plane] : x[c - plane]); }
+            if (!s[c + row]) { const double w = (j + 1 == q.jm - 1) ? n2 * kC13 : n2; den += w; nb += w * fabs((j + 1 == q.jm - 1) ? x[c - row] : x[c + row]); }
+            if (!s[c - row]) { const double w = (j - 1 == 0) ? n2 * kC13 : n2; den += w; nb += w * fabs((j - 1 == 0) ? x[c + row] : x[c - row]); }
+            if (!s[c - k + ke]) { den += n3; nb += n3 * fabs(x[c - k + ke]); }
+            if (!s[c - k + kw]) { den += n3; nb += n3 * fabs(x[c - k + kw]); }
+            const double v = den * fabs(xc) + nb;
             out = b[c] - ax;
             acc_r += out * out;
             acc_v += v * v;
@@ -423,9 +418,13 @@ __global__ void scatter_kernel(const double* __restrict__ p, const double* __res
 
 // ---------------------------------------------------------------------------------------------
 template <typename T>
-int alloc_vecs(Vecs<T>& v, size_t NP, int jm, int km, int NM, int N, int J) {
-    T** big[] = {&v.b, &v.p, &v.r, &v.z, &v.d, &v.q, &v.la, &v.lc, &v.lm};
-    for (T** p : big) { ATJUP_CUDA(cudaMalloc(p, sizeof(T) * NP)); ATJUP_CUDA(cudaMemset(*p, 0, sizeof(T) * NP)); }
+int alloc_vecs(Vecs<T>& v, size_t NP, int jm, int km, int NM, int N, int J, bool krylov) {
+    T** big[] = {&v.z, &v.la, &v.lc, &v.lm, &v.b, &v.p, &v.r, &v.d, &v.q};
+    const int nbig = krylov ? 9 : 4;        // the FP32 set carries the preconditioner only
+    for (int q = 0; q < nbig; q++) {
+        ATJUP_CUDA(cudaMalloc(big[q], sizeof(T) * NP));
+        ATJUP_CUDA(cudaMemset(*big[q], 0, sizeof(T) * NP));
+    }
     ATJUP_CUDA(cudaMalloc(&v.g, sizeof(T) * (size_t)jm * km));
     ATJUP_CUDA(cudaMemset(v.g, 0, sizeof(T) * (size_t)jm * km));
     ATJUP_CUDA(cudaMalloc(&v.gh, sizeof(T) * 2 * (size_t)(NM + 1) * J));
@@ -577,8 +576,8 @@ int setup(AtjupCtx* c, Solver* S) {
         }
     }
     int rc;
-    if ((rc = alloc_vecs(S->v64, NP, jm, km, NM, N, J))) return rc;
-    if ((rc = alloc_vecs(S->v32, NP, jm, km, NM, N, J))) return rc;
+    if ((rc = alloc_vecs(S->v64, NP, jm, km, NM, N, J, true))) return rc;
+    if ((rc = alloc_vecs(S->v32, NP, jm, km, NM, N, J, false))) return rc;
     if ((rc = upload_setup(S->v64, NP, la, lc, lm, cs, sn, ta, tcp, tm, S3d, dj))) return rc;
     if ((rc = upload_setup(S->v32, NP, la, lc, lm, cs, sn, ta, tcp, tm, S3d, dj))) return rc;
     ATJUP_CUDA(cudaMalloc(&S->yw, sizeof(double) * NP));
@@ -594,10 +593,12 @@ int setup(AtjupCtx* c, Solver* S) {
 
 Solver* get_solver(AtjupCtx* c) { return reinterpret_cast<Solver*>(c->solver); }
 
-// One preconditioned CG solve of A x = rhs in precision T, x from zero, to ||r|| <= tol ||rhs||.
-// rhs, x live in V.b / V.p. Returns iterations; *rel gets the final recursive ||r|| / ||rhs||.
+// One preconditioned CG solve of A x = rhs, x from zero, to ||r|| <= tol ||rhs||. The Krylov
+// vectors (V.b = rhs, V.p = x, r, d, q) are FP64; the preconditioner (radial lines and column
+// modes, set M) runs in precision T. Returns iterations; *rel = final recursive ||r|| / ||rhs||.
 template <typename T>
-int pcg(AtjupCtx* c, Solver* S, Vecs<T>& V, double tol, int max_iter, int* iters, double* rel) {
+int pcg(AtjupCtx* c, Solver* S, Vecs<double>& V, Vecs<T>& M, double tol, int max_iter, int* iters,
+        double* rel) {
     const AtjupParams& P = c->P;
     const size_t NP = c->NP;
     OpC q{P.im, P.jm, P.km, c->KP, 1.0 / (P.dr * P.dr)};
@@ -607,9 +608,9 @@ int pcg(AtjupCtx* c, Solver* S, Vecs<T>& V, double tol, int max_iter, int* iters
     double* part2 = S->part + 2 * NRED;      // partials of the inverse DFT (J * blocks)
     const int kblocks = (S->N + 127) / 128;
     // r = b (x = 0), ||b||
-    ATJUP_CUDA(cudaMemcpyAsync(V.r, V.b, sizeof(T) * NP, cudaMemcpyDeviceToDevice, st));
-    ATJUP_CUDA(cudaMemsetAsync(V.p, 0, sizeof(T) * NP, st));
-    dot_kernel<T, T><<<nb, RB, 0, st>>>(V.r, V.r, nullptr, NP, part); c->launches++;
+    ATJUP_CUDA(cudaMemcpyAsync(V.r, V.b, sizeof(double) * NP, cudaMemcpyDeviceToDevice, st));
+    ATJUP_CUDA(cudaMemsetAsync(V.p, 0, sizeof(double) * NP, st));
+    dot_kernel<double, double><<<nb, RB, 0, st>>>(V.r, V.r, nullptr, NP, part); c->launches++;
     finalize_kernel<<<1, 1, 0, st>>>(part, nb, S->scal, 7, 0); c->launches++;
     ATJUP_CUDA(cudaMemcpyAsync(S->hs, S->scal, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
     ATJUP_CUDA(cudaStreamSynchronize(st));
@@ -619,13 +620,13 @@ int pcg(AtjupCtx* c, Solver* S, Vecs<T>& V, double tol, int max_iter, int* iters
     if (bnorm == 0.0) return ATJUP_OK;
     auto precond = [&](int first) -> int {
         line_kernel<T><<<dim3((P.km - 1 + 127) / 128, P.jm - 2), 128, 0, st>>>(
-            V.r, V.z, V.la, V.lc, V.lm, S->yw, V.g, q);
+            V.r, M.z, M.la, M.lc, M.lm, S->yw, M.g, q);
         dft_fwd_kernel<T><<<dim3((S->NM + 1 + 127) / 128, S->J), 128, 0, st>>>(
-            V.g, V.cs, V.sn, V.gh, S->N, S->NM, S->J, P.km);
+            M.g, M.cs, M.sn, M.gh, S->N, S->NM, S->J, P.km);
         theta_solve_kernel<T><<<dim3((S->NM + 1 + 63) / 64, 2), 64, 0, st>>>(
-            V.gh, V.ta, V.tcp, V.tm, V.dj, S->NM, S->J, S->N);
-        dft_inv_kernel<T><<<dim3(kblocks, S->J), 128, 0, st>>>(V.gh, V.cs, V.sn, V.z, V.r, S->yw,
-                                                               V.lm, q, S->N, S->NM, S->J, part2);
+            M.gh, M.ta, M.tcp, M.tm, M.dj, S->NM, S->J, S->N);
+        dft_inv_kernel<T><<<dim3(kblocks, S->J), 128, 0, st>>>(M.gh, M.cs, M.sn, M.z, V.r, S->yw,
+                                                               M.lm, q, S->N, S->NM, S->J, part2);
         finalize_kernel<<<1, 1, 0, st>>>(part2, kblocks * S->J, S->scal, 8, first ? 0 : 2);
         c->launches += 5;
         if (first) {   // rho = y r z
@@ -635,25 +636,23 @@ int pcg(AtjupCtx* c, Solver* S, Vecs<T>& V, double tol, int max_iter, int* iters
     };
     int rc;
     if ((rc = precond(1))) return rc;
-    direction_kernel<T><<<nb, RB, 0, st>>>(V.d, V.z, S->scal, NP, 1); c->launches++;
+    direction_kernel<T><<<nb, RB, 0, st>>>(V.d, M.z, S->scal, NP, 1); c->launches++;
     const int check = 4;
     double rr = bnorm * bnorm;
     int it = 0;
     for (it = 1; it <= max_iter; it++) {
-        apply_kernel<T><<<nb, RB, 0, st>>>(V.d, V.q, c->solid, c->geo, S->yw, q, part);
+        apply_kernel<double><<<nb, RB, 0, st>>>(V.d, V.q, c->solid, c->geo, S->yw, q, part);
         finalize_kernel<<<1, 1, 0, st>>>(part, nb, S->scal, 4, 1);
-        update_kernel<T><<<nb, RB, 0, st>>>(V.p, V.r, V.d, V.q, S->scal, NP, part);
+        update_kernel<double><<<nb, RB, 0, st>>>(V.p, V.r, V.d, V.q, S->scal, NP, part);
         finalize_kernel<<<1, 1, 0, st>>>(part, nb, S->scal, 3, 0);
         c->launches += 4;
         if ((rc = precond(0))) return rc;
-        direction_kernel<T><<<nb, RB, 0, st>>>(V.d, V.z, S->scal, NP, 0); c->launches++;
+        direction_kernel<T><<<nb, RB, 0, st>>>(V.d, M.z, S->scal, NP, 0); c->launches++;
         if (it % check == 0 || it == max_iter) {
             // drop the rounding drift of r out of the range of A (its y-component)
-            dot_kernel<double, T><<<nb, RB, 0, st>>>(S->yw, V.r, nullptr, NP, part);
+            dot_kernel<double, double><<<nb, RB, 0, st>>>(S->yw, V.r, nullptr, NP, part);
             finalize_kernel<<<1, 1, 0, st>>>(part, nb, S->scal, 11, 0);
-            reproject_kernel<<<nb, RB, 0, st>>>(std::is_same<T, float>::value ? (float*)V.r : nullptr,
-                                                std::is_same<T, double>::value ? (double*)V.r : nullptr,
-                                                S->yw, S->scal, NP);
+            reproject_kernel<<<nb, RB, 0, st>>>(nullptr, V.r, S->yw, S->scal, NP);
             c->launches += 3;
             ATJUP_CUDA(cudaMemcpyAsync(S->hs, S->scal, sizeof(double) * 16, cudaMemcpyDeviceToHost, st));
             ATJUP_CUDA(cudaStreamSynchronize(st));
@@ -728,10 +727,13 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
     int total_it = 0, inner = 0;
     double rel = 0.0, floor_rel = 0.0, prev = 1e300;
     const bool mixed = (o->precision == ATJUP_PREC_MIXED);
-    // Iterative refinement with the residual formed in FP64: r = b - A p; solve A e = r
-    // (FP64 PCG, or FP32 PCG for the mixed form); p += e. Stops at the tolerance, or when the
-    // residual no longer falls (it has reached the rounding floor of an FP64 p, reported).
-    const int max_outer = mixed ? 24 : 8;
+    // Iterative refinement with the residual formed in FP64: r = b - A p; solve A e = r by PCG
+    // with FP64 Krylov vectors (the preconditioner in FP32 for the mixed form: the operator's
+    // condition number, ~1e9, is above 1/eps of FP32, so FP32 can carry the preconditioner -- whose
+    // radial-line and column-mode systems have condition numbers ~1e5 -- but not the residual);
+    // p += e. Stops at the tolerance, or when the residual no longer falls (it has reached the
+    // rounding floor of an FP64 p, which is reported).
+    const int max_outer = 8;
     for (int outer = 0; outer <= max_outer; outer++) {
         residual_kernel<<<nb, RB, 0, stm>>>(b64, p64, V.b, c->solid, c->geo, S->yw, q, S->part);
         finalize_kernel<<<1, 1, 0, stm>>>(S->part, nb, S->scal, 10, 0);
@@ -748,19 +750,13 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
         int it = 0;
         double inner_rel = 0.0;
         const int budget = o->max_iter - total_it;
-        if (mixed) {
-            Vecs<float>& W = S->v32;
-            convert_kernel<double, float><<<nb, RB, 0, stm>>>(V.b, W.b, NP);
-            c->launches++;
-            if ((rc = pcg<float>(c, S, W, 1e-4, budget, &it, &inner_rel))) return rc;
-            refine_kernel<<<nb, RB, 0, stm>>>(p64, W.p, NP);
-            c->launches++;
-        } else {
-            const double tgt = o->rel_tol * bnorm / std::max(std::sqrt(S->hs[10]), 1e-300);
-            if ((rc = pcg<double>(c, S, V, std::min(1e-3, std::max(0.5 * tgt, 1e-12)), budget, &it, &inner_rel))) return rc;
-            add_kernel<<<nb, RB, 0, stm>>>(p64, V.p, NP);
-            c->launches++;
-        }
+        const double tgt = o->rel_tol * bnorm / std::max(std::sqrt(S->hs[10]), 1e-300);
+        const double itol = std::min(1e-3, std::max(0.5 * tgt, 1e-12));
+        if (mixed) rc = pcg<float>(c, S, V, S->v32, itol, budget, &it, &inner_rel);
+        else rc = pcg<double>(c, S, V, V, itol, budget, &it, &inner_rel);
+        if (rc) return rc;
+        add_kernel<<<nb, RB, 0, stm>>>(p64, V.p, NP);
+        c->launches++;
         total_it += it;
         inner++;
     }
@@ -783,8 +779,10 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
     }
     // converged: at the tolerance, or within a small factor of the FP64 floor above it
     if (rel > o->rel_tol && rel > 8.0 * floor_rel) {
-        set_error("pressure_solve: residual " + std::to_string(rel) + " above tolerance after " +
-                  std::to_string(total_it) + " iterations");
+        char msg[160];
+        snprintf(msg, sizeof(msg), "pressure_solve: relative residual %.3e above tolerance %.1e "
+                 "(FP64 floor %.2e) after %d iterations", rel, o->rel_tol, floor_rel, total_it);
+        set_error(msg);
         return ATJUP_ERR_NOT_CONVERGED;
     }
     return ATJUP_OK;

@@ -114,7 +114,8 @@ typedef struct AtjupSolveOpts {
     int32_t mode;          /* ATJUP_SOLVE_SWEEPS or ATJUP_SOLVE_RESIDUAL                         */
     int32_t sweeps;        /* SWEEPS: number of red-black sweeps                                  */
     int32_t max_iter;      /* RESIDUAL: iteration cap (returns ATJUP_ERR_NOT_CONVERGED at it)     */
-    int32_t precision;     /* RESIDUAL: ATJUP_PREC_FP64, or MIXED = FP32 inner / FP64 refinement  */
+    int32_t precision;     /* RESIDUAL: ATJUP_PREC_FP64, or MIXED = the preconditioner in FP32     */
+                           /* under FP64 Krylov vectors and FP64 iterative refinement             */
     double rel_tol;        /* RESIDUAL: target ||b - A p|| / ||b|| (y-weighted, fluid cells)      */
     double omega;          /* relaxation factor of the sweeps (reference: 1.0)                    */
     int32_t external_rhs;  /* RESIDUAL: 1 = solve A p = b for b in atjup_gpu_set_solve_rhs       */
@@ -125,9 +126,9 @@ typedef struct AtjupSolveStats {
     int32_t inner_solves;  /* MIXED: FP32 inner solves under the FP64 refinement loop            */
     double rel_residual;   /* final ||b - A p|| / ||b||, or -1 when not computed (SWEEPS)       */
     double b_norm;         /* ||b|| of the projected right-hand side                              */
-    double rel_floor;      /* eps * || sum_faces |num (p_nb - p)| || / ||b||: the rounding floor  */
-                           /* of the relative residual of an FP64 p (RESIDUAL); the solve counts  */
-                           /* as converged at rel_tol or, when rel_tol is below it, at <= 8 floor */
+    double rel_floor;      /* eps * || |A| |p| || / ||b||: the rounding floor of the relative     */
+                           /* residual of an FP64 p (RESIDUAL); the solve counts as converged at  */
+                           /* rel_tol or, when rel_tol is below the floor, at <= 8 floor          */
 } AtjupSolveStats;
 
 typedef struct AtjupCtx AtjupCtx;
@@ -191,6 +192,20 @@ int atjup_gpu_mixture_density(AtjupCtx* ctx);
 
 /* cJupiterModel::balanceColumnV (InitValues_Jup.cpp:1500-1538); vshift may be NULL. */
 int atjup_gpu_balance_column_v(AtjupCtx* ctx, double* vshift);
+
+/* The column balance of v for callers that cannot allocate device memory. No counterpart in the
+ * reference: it computes what atjup_gpu_balance_column_v computes, on the caller's own device
+ * buffers -- v (in/out, [im][jm][pitch] doubles), i_topo ([jm * km] int32), rad ([im]) -- and keeps
+ * its scratch in a fixed file-scope device array instead of allocating. For hosts whose memory is
+ * preallocated, code inside stream capture, or embeddings that must not fail on an allocation.
+ * Limits: jm <= ATJUP_NOALLOC_MAX_J, pitch <= ATJUP_NOALLOC_MAX_PITCH, else ATJUP_ERR_ARG. The
+ * first call on each device looks up the array's address (make it before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race. stream: a cudaStream_t or NULL. */
+#define ATJUP_NOALLOC_MAX_J 256
+#define ATJUP_NOALLOC_MAX_PITCH 512
+int atjup_gpu_balance_column_v_noalloc(double* v, const int32_t* i_topo, const double* rad,
+                                       int32_t im, int32_t jm, int32_t km, int32_t pitch,
+                                       double dr, int32_t zonal, void* stream);
 
 /* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381) for the dry
  * configuration: pressure solve on even iterations (and when first != 0), mixture density,
