@@ -217,4 +217,17 @@ int launch_balance_v(AtjupCtx* c) {
     return ATJUP_OK;
 }
 
+// The column balance of v on caller-supplied buffers (the no-allocation entry point in
+// noalloc.cu supplies its file-scope scratch): v [im][jm][pitch], topo [jm * km], rad [im],
+// dvc [jm * pitch], dvrow [jm].
+int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, double* dvc,
+                             double* dvrow, int im, int jm, int km, int pitch, double dr,
+                             int zonal, cudaStream_t st) {
+    vcol_kernel<<<dim3((km + 127) / 128, jm - 2), 128, 0, st>>>(v, topo, rad, dvc, im, jm, km, pitch, dr);
+    if (zonal) vrow_kernel<<<jm - 2, 32, 0, st>>>(dvc, topo, dvrow, jm, km, pitch);
+    vsub_kernel<<<dim3((km + 127) / 128, jm - 2, im), 128, 0, st>>>(v, topo, dvrow, dvc, jm, km, pitch, zonal);
+    ATJUP_CHECK_LAUNCH("balance_v_buffers");
+    return ATJUP_OK;
+}
+
 }  // namespace atjup
