@@ -182,6 +182,7 @@ def main():
     from atjup_b200 import synthetic
     from atjup_b200.gpu import GpuModel
     from atjup_b200.params import resolve_params, FIELD_IDS
+    from atjup_b200.replicas import max_over_ranks, whole_job_seconds_per_step
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -235,11 +236,8 @@ def main():
     launches = m.launch_count() - n0
     st_ms, st_n = m.timing_read(0)          # rk_stage_kernel
     m.timing(False)
-    if dist is not None:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-    value = t_ms / 1e3 / (args.steps * world)
+    t_ms = max_over_ranks(t_ms, device="cuda")
+    value = whole_job_seconds_per_step(t_ms / 1e3, args.steps, world)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     names = ["t", "u", "v", "w", "p_dyn"]
@@ -264,10 +262,7 @@ def main():
             down(n)
     m.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, device="cuda")
     nbytes = len(names) * N_CELLS * 8
 
     peak, peak_kind = measured_peak_hbm()
@@ -284,7 +279,8 @@ def main():
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
                      "traffic": RK_STAGE_TRAFFIC, "algorithmic_bytes_per_launch": RK_STAGE_BYTES,
                      "avg_launch_ms": st_ms / st_n if st_n else None, "launches": st_n},
-        "e2e": {"value": e2e_s / (e2e_steps * world), "unit": UNIT, "steps": e2e_steps,
+        "e2e": {"value": whole_job_seconds_per_step(e2e_s, e2e_steps, world), "unit": UNIT,
+                "steps": e2e_steps,
                 "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
         "gpu_launches": launches,
         "clocks": clk,
