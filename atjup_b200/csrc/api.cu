@@ -62,7 +62,7 @@ void free_all(AtjupCtx* c) {
     }
     for (auto& p : c->kr) { cudaFree(p); p = nullptr; }
     for (auto& p : c->kf) { cudaFree(p); p = nullptr; }
-    cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red);
+    cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red); cudaFree(c->stage);
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->solve_b); cudaFree(c->dsum);
     if (c->hsum) cudaFreeHost(c->hsum);
@@ -156,6 +156,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     A(&c->src, c->NP);
     A(&c->tmp, c->NP);
     A(&c->tmp2, c->NP);
+    A(&c->stage, (size_t)P.im * P.jm * P.km);
     A(&c->red, 4096);
     A(&c->buoy_ref, (size_t)P.im);
     A(&c->zm, (size_t)4 * P.jm);
@@ -332,12 +333,15 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
     return ATJUP_OK;
 }
 
+// One contiguous host<->device copy through the staging buffer, and the row padding on the
+// device (a pitched 2-D copy would move 7421 short rows per field).
 int atjup_gpu_upload(AtjupCtx* c, int32_t id, const double* host) {
     if (!c || !host || !valid_field(id)) { set_error("upload: bad argument"); return ATJUP_ERR_ARG; }
     const AtjupParams& P = c->P;
-    ATJUP_CUDA(cudaMemcpy2DAsync(c->f[id], sizeof(double) * c->KP, host, sizeof(double) * P.km,
-                                 sizeof(double) * P.km, (size_t)P.im * P.jm,
-                                 cudaMemcpyHostToDevice, c->stream));
+    const size_t n = (size_t)P.im * P.jm * P.km;
+    ATJUP_CUDA(cudaMemcpyAsync(c->stage, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    int rc = launch_pad(c, c->stage, c->f[id]);
+    if (rc) return rc;
     ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     return ATJUP_OK;
 }
@@ -345,9 +349,10 @@ int atjup_gpu_upload(AtjupCtx* c, int32_t id, const double* host) {
 int atjup_gpu_download(AtjupCtx* c, int32_t id, double* host) {
     if (!c || !host || !valid_field(id)) { set_error("download: bad argument"); return ATJUP_ERR_ARG; }
     const AtjupParams& P = c->P;
-    ATJUP_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * P.km, c->f[id], sizeof(double) * c->KP,
-                                 sizeof(double) * P.km, (size_t)P.im * P.jm,
-                                 cudaMemcpyDeviceToHost, c->stream));
+    const size_t n = (size_t)P.im * P.jm * P.km;
+    int rc = launch_unpad(c, c->f[id], c->stage);
+    if (rc) return rc;
+    ATJUP_CUDA(cudaMemcpyAsync(host, c->stage, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
     ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     return ATJUP_OK;
 }

@@ -19,7 +19,34 @@ __global__ void nonfinite_kernel(const double* __restrict__ a, const double* __r
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, n);
 }
 
+__global__ void pad_kernel(const double* __restrict__ flat, double* __restrict__ padded,
+                           size_t rows, int km, int KP, int dir) {
+    const size_t n = rows * (size_t)km;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = q / km, k = q - r * km;
+        if (dir == 0) padded[r * KP + k] = flat[q];
+        else const_cast<double*>(flat)[q] = padded[r * KP + k];
+    }
+}
+
 }  // namespace
+
+int launch_pad(AtjupCtx* c, const double* flat, double* padded) {
+    c->launches++;
+    pad_kernel<<<148 * 8, 256, 0, c->stream>>>(flat, padded, (size_t)c->P.im * c->P.jm, c->P.km,
+                                               c->KP, 0);
+    ATJUP_CHECK_LAUNCH("pad");
+    return ATJUP_OK;
+}
+
+int launch_unpad(AtjupCtx* c, const double* padded, double* flat) {
+    c->launches++;
+    pad_kernel<<<148 * 8, 256, 0, c->stream>>>(flat, const_cast<double*>(padded),
+                                               (size_t)c->P.im * c->P.jm, c->P.km, c->KP, 1);
+    ATJUP_CHECK_LAUNCH("unpad");
+    return ATJUP_OK;
+}
 
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count) {
     c->launches++;

@@ -58,6 +58,7 @@ struct AtjupCtx {
     double* src = nullptr;       // Poisson source, one value per cell
     double* tmp = nullptr;       // filter ping-pong buffers
     double* tmp2 = nullptr;
+    double* stage = nullptr;     // contiguous (unpadded) transfer buffer, im*jm*km doubles
     double* red = nullptr;       // reduction partials
     double* buoy_ref = nullptr;  // [im]
     double* zm = nullptr;        // [4 * jm] zonal means for the top sponge
@@ -130,6 +131,8 @@ int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, 
                              double* dvrow, int im, int jm, int km, int pitch, double dr,
                              int zonal, cudaStream_t st);
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
+int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) km -> KP rows
+int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);
 
