@@ -64,7 +64,7 @@ void free_all(AtjupCtx* c) {
     for (auto& p : c->kf) { cudaFree(p); p = nullptr; }
     cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red); cudaFree(c->stage);
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
-    cudaFree(c->solve_b); cudaFree(c->dsum);
+    cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
     cudaFree(c->sin_the); cudaFree(c->rad); cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
@@ -162,6 +162,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     A(&c->zm, (size_t)4 * P.jm);
     A(&c->dvc, (size_t)P.jm * c->KP);
     A(&c->dvrow, (size_t)P.jm);
+    A(reinterpret_cast<double**>(&c->counters), 8);
     if (rc == ATJUP_OK) {
         e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamCreate");
@@ -467,6 +468,28 @@ int atjup_gpu_mixture_density(AtjupCtx* c) {
     if (rc) return rc;
     Timed tm(c, TK_MIXTURE);
     return launch_mixture_density(c);
+}
+
+int atjup_gpu_satadj(AtjupCtx* c, int32_t gas, const AtjupGasParams* gp, AtjupSatStats* stats) {
+    int rc = need_grid(c, "satadj");
+    if (rc) return rc;
+    if (!gp || gas < ATJUP_GAS_H2O || gas > ATJUP_GAS_CH4) {
+        set_error("satadj: bad argument (gas id or null parameter block)");
+        return ATJUP_ERR_ARG;
+    }
+    {
+        Timed tm(c, TK_SATADJ);
+        if ((rc = launch_satadj(c, gas, *gp))) return rc;
+    }
+    if (stats) {
+        unsigned long long h[3];
+        ATJUP_CUDA(cudaMemcpyAsync(h, c->counters, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+        ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+        stats->adjusted = (int64_t)h[0];
+        stats->not_converged = (int64_t)h[1];
+        stats->dry_exits = (int64_t)h[2];
+    }
+    return ATJUP_OK;
 }
 
 int atjup_gpu_balance_column_v(AtjupCtx* c, double* vshift) {

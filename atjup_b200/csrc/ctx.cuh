@@ -70,6 +70,7 @@ struct AtjupCtx {
     double* solve_b = nullptr;   // external right-hand side
     double* dsum = nullptr;      // [ATJUP_MAX_SOLVE_PARTIALS * 4] dot-product partials
     double* hsum = nullptr;      // pinned host copy of the final dot products
+    unsigned long long* counters = nullptr;  // [8] event counters of the last satadj call
 
     // static grid
     uint8_t* solid = nullptr;
@@ -106,7 +107,7 @@ void set_error(const std::string& msg);
 
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
-       TK_SOLVER, TK_COUNT };
+       TK_SOLVER, TK_SATADJ, TK_COUNT };
 void timer_begin(AtjupCtx* c, int cls);
 void timer_end(AtjupCtx* c);
 int cuda_status(cudaError_t e, const char* what);
@@ -133,6 +134,7 @@ int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, 
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
 int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) km -> KP rows
 int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
+int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);
 

@@ -60,6 +60,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_timing.argtypes = [vp, i32]
     L.atjup_gpu_timing_read.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int64)]
     L.atjup_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.atjup_gpu_satadj.argtypes = [vp, i32, ctypes.POINTER(_p.AtjupGasParams),
+                                   ctypes.POINTER(_p.AtjupSatStats)]
     _lib = L
     return L
 
@@ -172,6 +174,15 @@ class GpuModel:
         _check(self.L.atjup_gpu_balance_column_v(self.ctx, ctypes.byref(s)))
         return s.value
 
+    def satadj(self, gas: str, gp: _p.AtjupGasParams, stats: bool = True):
+        """SaturationAdjustmentJup(*this).run(gas, ...) (SaturationAdjustment.h:255-746) on the
+        device fields of gas ("H2O", "NH3" or "CH4"); returns (adjusted, not converged, dry
+        exits) when stats, else None (no synchronisation)."""
+        st = _p.AtjupSatStats() if stats else None
+        _check(self.L.atjup_gpu_satadj(self.ctx, _p.GAS_IDS[gas], ctypes.byref(gp),
+                                       ctypes.byref(st) if st is not None else None))
+        return (st.adjusted, st.not_converged, st.dry_exits) if st is not None else None
+
     def step(self, iter_n: int, first: bool = False, solve: _p.AtjupSolveOpts | None = None):
         """One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381)."""
         _check(self.L.atjup_gpu_step(self.ctx, iter_n, int(first),
@@ -189,7 +200,7 @@ class GpuModel:
 
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
-                      "mixture", "solver")
+                      "mixture", "solver", "satadj")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

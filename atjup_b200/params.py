@@ -18,17 +18,29 @@ ABI_VERSION = 1
 
 # field ids (include/atjup_gpu.h)
 F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, \
-    F_AUX_U, F_AUX_V, F_AUX_W, F_P_BARO, F_Q_RAD, F_Q_PRECIP = range(16)
+    F_AUX_U, F_AUX_V, F_AUX_W, F_P_BARO, F_Q_RAD, F_Q_PRECIP, \
+    F_H2O, F_H2O_CLOUD, F_H2O_ICE, F_NH3, F_NH3_CLOUD, F_NH3_ICE, \
+    F_CH4, F_CH4_CLOUD, F_CH4_ICE = range(25)
 FIELD_IDS = {
     "t": F_T, "u": F_U, "v": F_V, "w": F_W, "p_dyn": F_P_DYN, "p_hydro": F_P_HYDRO,
     "p_stat": F_P_STAT, "rho_mix": F_RHO_MIX, "wall_nue": F_WALL_NUE, "nue": F_NUE,
     "aux_u": F_AUX_U, "aux_v": F_AUX_V, "aux_w": F_AUX_W, "p_baro": F_P_BARO,
     "Q_rad": F_Q_RAD, "Q_precip": F_Q_PRECIP,
+    "h2o": F_H2O, "h2o_cloud": F_H2O_CLOUD, "h2o_ice": F_H2O_ICE,
+    "nh3": F_NH3, "nh3_cloud": F_NH3_CLOUD, "nh3_ice": F_NH3_ICE,
+    "ch4": F_CH4, "ch4_cloud": F_CH4_CLOUD, "ch4_ice": F_CH4_ICE,
 }
+
+# gas ids of atjup_gpu_satadj, in the order cJupiterModel.cpp:1060-1080 calls them
+GAS_H2O, GAS_NH3, GAS_CH4 = 0, 1, 2
+GAS_IDS = {"H2O": GAS_H2O, "NH3": GAS_NH3, "CH4": GAS_CH4}
 
 SOLVE_SWEEPS, SOLVE_RESIDUAL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 BC_RADIUS, BC_THETA, BC_PHI, BC_SOLID, BC_ALL = 1, 2, 4, 8, 15
+
+GAS_CONST_NAMES = ("t_0", "t_00", "ep", "lv", "ls", "C", "L0", "R", "del_alf", "del_bet",
+                   "C_i", "L0_i", "del_alf_i", "del_bet_i")
 
 _FIELDS = [
     ("abi_version", ctypes.c_int32), ("im", ctypes.c_int32), ("jm", ctypes.c_int32),
@@ -77,6 +89,54 @@ class AtjupSolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("inner_solves", ctypes.c_int32),
                 ("rel_residual", ctypes.c_double), ("b_norm", ctypes.c_double),
                 ("rel_floor", ctypes.c_double)]
+
+
+class AtjupGasParams(ctypes.Structure):
+    """Mirror of AtjupGasParams: the 14 constants of SaturationAdjustmentJup::run
+    (SaturationAdjustment.h:236-243) and the ATJUP_SATADJ_* knobs."""
+    _fields_ = [(n, ctypes.c_double) for n in GAS_CONST_NAMES] + [
+        (n, ctypes.c_int32) for n in ("conserve", "newton", "evap", "ice_entry", "bergeron",
+                                      "freeze", "dry_exit", "reserved")]
+
+
+class AtjupSatStats(ctypes.Structure):
+    _fields_ = [("adjusted", ctypes.c_int64), ("not_converged", ctypes.c_int64),
+                ("dry_exits", ctypes.c_int64)]
+
+
+# The 14 constants of each gas as cJupiterModel derives them at start-up with its default
+# composition and vapour-pressure sets (InitValues_Jup.cpp:880-950, ATPhys.h:55-67), in
+# GAS_CONST_NAMES order. A host model passes its own; these serve the synthetic workloads.
+DEFAULT_GASES = {
+    "H2O": (273.15, 210.15, 7.651416982890988, 2500900.0, 2833900.0, 25.096, 3148.2, 461.52,
+            0.0, -0.0087, -1.962499, 2641.4013, 1.629479, -0.003361398),
+    "NH3": (195.5, 140.0, 7.232930612074716, 1372000.0, 1832000.0, 196.077451, 3586.5634,
+            488.21, -15.978352, 0.02837146, 16.086062, 1857.9898, 0.098768, -0.001179989),
+    "CH4": (90.69, 67.36, 6.813102176498581, 511000.0, 511000.0, 1.627, 553.1, 518.28, 1.002,
+            -0.0041, 1.627, 553.1, 1.002, -0.0041),
+}
+
+
+def resolve_gas(constants, env: Mapping[str, str] | None = None) -> AtjupGasParams:
+    """Gas block from the 14 constants (sequence in GAS_CONST_NAMES order, or a mapping) and the
+    ATJUP_SATADJ_* knobs with cJupiterModel's defaults (SaturationAdjustment.h:277-307,
+    cJupiterModel.h:1045-1057): CONSERVE 1, NEWTON 1, EVAP 1, ICE_ENTRY 0, BERGERON 2,
+    FREEZE 0, DRY_EXIT 1."""
+    env = os.environ if env is None else env
+    if isinstance(constants, Mapping):
+        vals = [float(constants[n]) for n in GAS_CONST_NAMES]
+    else:
+        vals = [float(v) for v in constants]
+    if len(vals) != len(GAS_CONST_NAMES):
+        raise ValueError(f"expected {len(GAS_CONST_NAMES)} gas constants, got {len(vals)}")
+    knobs = [int(_env(env, "ATJUP_SATADJ_CONSERVE", 1) != 0),
+             int(_env(env, "ATJUP_SATADJ_NEWTON", 1) != 0),
+             int(_env(env, "ATJUP_SATADJ_EVAP", 1) != 0),
+             int(_env(env, "ATJUP_SATADJ_ICE_ENTRY", 0) != 0),
+             int(_env(env, "ATJUP_SATADJ_BERGERON", 2)),
+             int(_env(env, "ATJUP_SATADJ_FREEZE", 0) != 0),
+             int(_env(env, "ATJUP_SATADJ_DRY_EXIT", 1) != 0), 0]
+    return AtjupGasParams(*vals, *knobs)
 
 
 # Mixture constants the reference derives at start-up from its default composition

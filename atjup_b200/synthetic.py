@@ -115,6 +115,42 @@ def state(im=41, jm=181, km=361, seed=20261203, cone=True, t_ref=165.0, u_0=100.
     }
 
 
+def saturation_density(T_K, p_bar, rho, gas_consts, ice=False):
+    """rho * ep * E(T) / p with E the vapour-pressure fit exp(C + (-L0/T + a ln T + b T) /
+    (1e-3 R)) [bar] (the form of ATPhys.h:49-52); used only to place synthetic species near
+    saturation."""
+    (t_0, t_00, ep, lv, ls, C, L0, R, da, db, Ci, L0i, dai, dbi) = gas_consts
+    if ice:
+        C, L0, da, db = Ci, L0i, dai, dbi
+    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+        E = np.exp(C + (-L0 / T_K + da * np.log(T_K) + db * T_K) / (1e-3 * R))
+        return rho * ep * E / p_bar
+
+
+def moist(s: dict, gases: dict, seed: int = 20261205, t_ref: float = 165.0) -> dict:
+    """Species fields (vapour, cloud, ice of H2O, NH3, CH4) for a state from state(): vapour at
+    U(0.3, 1.7) times the liquid saturation density of the cell (capped at 2 % of the mixture
+    density), cloud and ice seeded in a third of the fluid cells each at up to half the vapour.
+    Every path of the saturation adjustment is taken: condensation, evaporation, melting above
+    t_0, the Bergeron branch, dry exits. Zero in solid cells."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    t, p, rho = s["t"], s["p_stat"], s["rho_mix"]
+    shape = t.shape
+    fluid = s["solid"] == 0
+    out = {}
+    for gas, cst in gases.items():
+        sat = saturation_density(t * t_ref, p, rho, cst)
+        sat = np.where(np.isfinite(sat), np.minimum(sat, 0.02 * rho), 0.0)
+        vap = sat * rng.uniform(0.3, 1.7, shape)
+        cl = np.where(rng.uniform(size=shape) < 1 / 3, 0.5 * vap * rng.uniform(size=shape), 0.0)
+        ic = np.where(rng.uniform(size=shape) < 1 / 3, 0.5 * vap * rng.uniform(size=shape), 0.0)
+        name = gas.lower()
+        out[name] = np.where(fluid, vap, 0.0)
+        out[name + "_cloud"] = np.where(fluid, cl, 0.0)
+        out[name + "_ice"] = np.where(fluid, ic, 0.0)
+    return out
+
+
 def smooth121(f: np.ndarray, passes: int = 3) -> np.ndarray:
     """`passes` Shapiro 1-2-1 passes in k (ring of km-1 meridians, seam copy), then j (clamped at
     the poles), then i (clamped), no fluid floor -- damp_wiggles with i_surface = nullptr

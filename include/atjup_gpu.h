@@ -47,6 +47,9 @@ enum {
     ATJUP_F_AUX_U, ATJUP_F_AUX_V, ATJUP_F_AUX_W,              /* projection source (persist)   */
     ATJUP_F_P_BARO,                                           /* frozen geo-balance rest       */
     ATJUP_F_Q_RAD, ATJUP_F_Q_PRECIP,                          /* heating inputs                */
+    ATJUP_F_H2O, ATJUP_F_H2O_CLOUD, ATJUP_F_H2O_ICE,          /* condensable species [kg/m3]   */
+    ATJUP_F_NH3, ATJUP_F_NH3_CLOUD, ATJUP_F_NH3_ICE,          /* (vapour, cloud, ice per gas)  */
+    ATJUP_F_CH4, ATJUP_F_CH4_CLOUD, ATJUP_F_CH4_ICE,
     ATJUP_F_COUNT
 };
 
@@ -207,6 +210,40 @@ int atjup_gpu_balance_column_v_noalloc(double* v, const int32_t* i_topo, const d
                                        int32_t im, int32_t jm, int32_t km, int32_t pitch,
                                        double dr, int32_t zonal, void* stream);
 
+/* ---- saturation adjustment (SaturationAdjustment.h:255-746, Tao et al. 1988) ---- */
+enum { ATJUP_GAS_H2O = 0, ATJUP_GAS_NH3 = 1, ATJUP_GAS_CH4 = 2 };
+
+/* One gas: the 14 constants cJupiterModel passes to SaturationAdjustmentJup::run
+ * (SaturationAdjustment.h:236-243, cJupiterModel.cpp:1060-1080) and the knobs the routine reads
+ * once per planet (ATJUP_SATADJ_*, SaturationAdjustment.h:277-307; defaults cJupiterModel.h:
+ * 1045-1057). The saturation vapour pressure is exp(C + (-L0/T + del_alf ln T + del_bet T) /
+ * (1e-3 R)) [bar] (ATPhys.h:49-52); the *_i set is the ice one. */
+typedef struct AtjupGasParams {
+    double t_0, t_00;            /* all-liquid above t_0, all-ice below t_00 [K]                 */
+    double ep, lv, ls;           /* molar-mass ratio, latent heats of vaporisation / sublimation */
+    double C, L0, R, del_alf, del_bet;          /* liquid vapour-pressure set, R [J/(kg K)]     */
+    double C_i, L0_i, del_alf_i, del_bet_i;     /* ice vapour-pressure set                      */
+    int32_t conserve;            /* ATJUP_SATADJ_CONSERVE 1: melt (not delete) ice above t_0     */
+    int32_t newton;              /* ATJUP_SATADJ_NEWTON 1: damped Newton step of the target      */
+    int32_t evap;                /* ATJUP_SATADJ_EVAP 1: cells with condensate off target enter  */
+    int32_t ice_entry;           /* ATJUP_SATADJ_ICE_ENTRY 0: temperature-split entry target     */
+    int32_t bergeron;            /* ATJUP_SATADJ_BERGERON 2                                      */
+    int32_t freeze;              /* ATJUP_SATADJ_FREEZE 0: liquid below t_00 freezes             */
+    int32_t dry_exit;            /* ATJUP_SATADJ_DRY_EXIT 1: stop a dry, subsaturated cell       */
+    int32_t reserved;
+} AtjupGasParams;
+
+typedef struct AtjupSatStats {
+    int64_t adjusted;            /* cells that entered the mixed-phase iteration                 */
+    int64_t not_converged;       /* of those, cells that used all 15 passes                      */
+    int64_t dry_exits;           /* of those, cells that left through the dry exit               */
+} AtjupSatStats;
+
+/* SaturationAdjustmentJup(*this).run(gas, ...) on the device fields of one gas (vapour, cloud,
+ * ice: ATJUP_F_H2O.. / NH3.. / CH4..), with t, p_stat, rho_mix (ATJUP_LOCAL_RHO) and the solid
+ * mask; updates t and the three species in place. stats may be NULL. */
+int atjup_gpu_satadj(AtjupCtx* ctx, int32_t gas, const AtjupGasParams* gp, AtjupSatStats* stats);
+
 /* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381) for the dry
  * configuration: pressure solve on even iterations (and when first != 0), mixture density,
  * RK4, boundary passes, in-loop Shapiro, column balance of v; restoreVar is implicit (the
@@ -220,7 +257,7 @@ int atjup_gpu_nonfinite_count(AtjupCtx* ctx, int64_t* count);
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
  * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */
 enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
-       ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_COUNT };
+       ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */

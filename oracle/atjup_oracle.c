@@ -925,3 +925,220 @@ void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, in
 
 /* Size of the parameter block as compiled here, for binding checks. */
 size_t ora_params_sizeof(void) { return sizeof(AtjupParams); }
+size_t ora_gas_params_sizeof(void) { return sizeof(AtjupGasParams); }
+size_t ora_sat_stats_sizeof(void) { return sizeof(AtjupSatStats); }
+
+/* ---------------------------------------------------------------------------------------------
+ * Saturation adjustment of one gas (SaturationAdjustment.h:255-746; Tao, Simpson and McCumber
+ * 1988). Every expression keeps the reference's operand order, so with the same libm this is
+ * bit-identical to it. Print-only parts (budget sums, DIAG counters, the reported cell) are
+ * left out; counts[0..2] = cells that entered the iteration, that used every pass, that left
+ * through the dry exit.
+ * ------------------------------------------------------------------------------------------- */
+
+/* ATPhys.h:49-52: Clausius-Clapeyron fit [bar]; R in J/(kg K), coefficients per J/(g K). */
+static double ora_svp(double T, double C, double L0, double R, double da, double db) {
+    return exp(C + (-L0 / T + da * log(T) + db * T) / (1e-3 * R));
+}
+
+enum { SAT_PASSES = 15 };                 /* iter_prec_end, SaturationAdjustment.h:250 */
+static const double SAT_Q_DIFF_MIN = 1.0e-3;  /* q_diff_min, SaturationAdjustment.h:251 */
+
+/* Vapour target of a cell holding q_c liquid and q_i ice at temperature T, given the liquid and
+ * ice saturation densities (SaturationAdjustment.h:513-520 and the same choice at 564-571). */
+static double sat_target(const AtjupGasParams* g, double T, double q_c, double q_i, double q_l,
+                         double q_s, double t_range_inv) {
+    if (q_c > 0.0 && q_i > 0.0) return (q_c * q_l + q_i * q_s) / (q_c + q_i);
+    if (g->bergeron >= 2 && q_c <= 0.0 && q_i <= 0.0 && T < g->t_0) return q_s;
+    if (g->ice_entry && q_c <= 0.0 && q_i <= 0.0) {
+        const double cn = T <= g->t_00 ? 0.0 : (T >= g->t_0 ? 1.0 : (T - g->t_00) * t_range_inv);
+        return cn * q_l + (1.0 - cn) * q_s;
+    }
+    if (q_i == 0.0) return q_l;
+    return q_s;
+}
+
+void ora_satadj(const AtjupParams* P, const ora_grid* G, const AtjupGasParams* g, double* t,
+                const double* p_stat, const double* rho_mix, double* c, double* cloud,
+                double* ice, long long* counts) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const size_t N = (size_t)im * jm * km;
+    const double t_range_inv = 1.0 / (g->t_0 - g->t_00);
+    const int freeze_on = g->freeze && g->conserve && g->t_00 > 0.0 && g->t_00 < g->t_0;
+    const double Lf = g->ls - g->lv;
+    const double cp = P->cp_mix;
+    long long n_adj = 0, n_nc = 0, n_dry = 0;
+
+    for (size_t q = 0; q < N; q++) {
+        double t_u = t[q] * P->t_ref;
+        const double p_u = p_stat[q];
+        if (!(t_u > 0.0) || !(p_u > 0.0) || G->solid[q]) continue;
+        /* rho_at (cJupiterModel.h:1212-1216) */
+        double rho = P->r_mix;
+        if (P->local_rho && rho_mix[q] > 0.0 && isfinite(rho_mix[q])) rho = rho_mix[q];
+
+        /* entry bounds (SaturationAdjustment.h:368-407) */
+        if (t_u > g->t_0) {
+            if (g->conserve) {
+                if (ice[q] > 0.0) {
+                    double dm = ice[q];
+                    if (Lf > 0.0) {
+                        const double hc = cp * rho;
+                        const double cap = hc * (t_u - g->t_0) / Lf;
+                        if (dm > cap) dm = cap;
+                        t_u -= Lf * dm / hc;
+                        t[q] = t_u / P->t_ref;
+                    }
+                    ice[q] -= dm;
+                    cloud[q] += dm;
+                }
+            } else {
+                ice[q] = 0.0;
+            }
+        }
+        if (freeze_on && t_u < g->t_00 && cloud[q] > 0.0) {
+            double dm = cloud[q];
+            if (Lf > 0.0) {
+                const double hc = cp * rho;
+                const double cap = hc * (g->t_00 - t_u) / Lf;
+                if (dm > cap) dm = cap;
+                t_u += Lf * dm / hc;
+                t[q] = t_u / P->t_ref;
+            }
+            cloud[q] -= dm;
+            ice[q] += dm;
+        }
+        if (c[q] < 0.0) c[q] = 0.0;
+        if (cloud[q] < 0.0) cloud[q] = 0.0;
+        if (ice[q] < 0.0) ice[q] = 0.0;
+
+        /* entry test (SaturationAdjustment.h:422-452) */
+        const double rho_c = rho;
+        const double q_rain0 = rho_c * g->ep * ora_svp(t_u, g->C, g->L0, g->R, g->del_alf,
+                                                        g->del_bet) / p_u;
+        if (q_rain0 <= 0.0) continue;
+        double q_entry = q_rain0;
+        if (g->ice_entry && cloud[q] <= 0.0 && ice[q] <= 0.0) {
+            const double cnd0 = t_u <= g->t_00 ? 0.0
+                              : (t_u >= g->t_0 ? 1.0 : (t_u - g->t_00) * t_range_inv);
+            if (cnd0 < 1.0)
+                q_entry = cnd0 * q_rain0 + (1.0 - cnd0) * rho_c * g->ep
+                        * ora_svp(t_u, g->C_i, g->L0_i, g->R, g->del_alf_i, g->del_bet_i) / p_u;
+        }
+        if (g->bergeron >= 2 && cloud[q] <= 0.0 && ice[q] <= 0.0 && t_u < g->t_0)
+            q_entry = rho_c * g->ep * ora_svp(t_u, g->C_i, g->L0_i, g->R, g->del_alf_i,
+                                              g->del_bet_i) / p_u;
+        if (c[q] <= q_entry) {
+            const double qc0 = cloud[q], qi0 = ice[q];
+            if (!g->evap || !g->conserve || (qc0 <= 0.0 && qi0 <= 0.0)) continue;
+            const double q_ice0 = rho_c * g->ep * ora_svp(t_u, g->C_i, g->L0_i, g->R,
+                                                          g->del_alf_i, g->del_bet_i) / p_u;
+            double q_t0;
+            if (qc0 > 0.0 && qi0 > 0.0) q_t0 = (qc0 * q_rain0 + qi0 * q_ice0) / (qc0 + qi0);
+            else if (qi0 <= 0.0) q_t0 = q_rain0;
+            else q_t0 = q_ice0;
+            if (fabs(c[q] - q_t0) <= SAT_Q_DIFF_MIN * q_t0) continue;
+        }
+
+        /* mixed-phase iteration (SaturationAdjustment.h:454-604) */
+        double qv = c[q], qc = cloud[q], qi = ice[q], T = t_u, hyp = qv;
+        double q_rain_now = q_rain0;
+        int found = 0, dry = 0;
+        const double heat = cp * rho_c;
+        for (int itr = 1; itr <= SAT_PASSES; itr++) {
+            double CND = (T - g->t_00) * t_range_inv;
+            double DEP = (g->t_0 - T) * t_range_inv;
+            if (T <= g->t_00) { CND = 0.0; DEP = 1.0; }
+            if (T >= g->t_0) { CND = 1.0; DEP = 0.0; }
+            const int berg = g->bergeron != 0 && T < g->t_0 && qv <= q_rain_now
+                          && (qi > 0.0 || (g->bergeron >= 2 && qc <= 0.0));
+            if (berg) {
+                CND = 0.0; DEP = 1.0;
+                if (qc > 0.0) {
+                    T -= g->lv * qc / heat;
+                    qv += qc;
+                    qc = 0.0;
+                }
+            }
+            double dv = hyp - qv;
+            double dc = -dv * CND;
+            double di = -dv * DEP;
+            if (g->conserve) {
+                if (dv < -qv) { dv = -qv; dc = -dv * CND; di = -dv * DEP; }
+                if (qc + dc < 0.0) { const double ex = -(qc + dc); dc = -qc; di -= ex; }
+                if (qi + di < 0.0) {
+                    const double ex = -(qi + di); di = -qi; dc -= ex;
+                    if (qc + dc < 0.0) dc = -qc;
+                }
+                dv = -(dc + di);
+            }
+            T += (g->lv * dc + g->ls * di) / heat;
+            qv += dv;
+            qc += dc;
+            qi += di;
+            if (qv < 0.0) qv = 0.0;
+            if (qc < 0.0) qc = 0.0;
+            if (qi < 0.0) qi = 0.0;
+
+            const double q_l = rho_c * g->ep * ora_svp(T, g->C, g->L0, g->R, g->del_alf,
+                                                       g->del_bet) / p_u;
+            const double q_s = rho_c * g->ep * ora_svp(T, g->C_i, g->L0_i, g->R, g->del_alf_i,
+                                                       g->del_bet_i) / p_u;
+            q_rain_now = q_l;
+            hyp = sat_target(g, T, qc, qi, q_l, q_s, t_range_inv);
+
+            if (T >= g->t_0) {
+                if (g->conserve) {
+                    if (qi > 0.0) {
+                        double dm = qi;
+                        if (Lf > 0.0) {
+                            const double cap = heat * (T - g->t_0) / Lf;
+                            if (dm > cap) dm = cap;
+                            T -= Lf * dm / heat;
+                        }
+                        qi -= dm;
+                        qc += dm;
+                    }
+                } else {
+                    qi = 0.0;
+                }
+            }
+            const double q_diff = fabs(qv - hyp) / (hyp + 1e-20);
+            if (q_diff <= SAT_Q_DIFF_MIN) { found = 1; break; }
+            if (g->dry_exit && g->conserve && qc <= 0.0 && qi <= 0.0 && qv < hyp) { dry = 1; break; }
+            if (g->newton) {
+                const double dT = 0.1;
+                const double q_ld = rho_c * g->ep * ora_svp(T + dT, g->C, g->L0, g->R,
+                                                            g->del_alf, g->del_bet) / p_u;
+                const double q_sd = rho_c * g->ep * ora_svp(T + dT, g->C_i, g->L0_i, g->R,
+                                                            g->del_alf_i, g->del_bet_i) / p_u;
+                const double hyp_d = sat_target(g, T, qc, qi, q_ld, q_sd, t_range_inv);
+                double CNDn = (T - g->t_00) * t_range_inv;
+                if (T <= g->t_00) CNDn = 0.0;
+                if (T >= g->t_0) CNDn = 1.0;
+                if (berg) CNDn = 0.0;
+                const double G2 = (g->lv * CNDn + g->ls * (1.0 - CNDn)) / heat
+                                * (hyp_d - hyp) / dT;
+                double wgt = 1.0 / (1.0 + dmax(G2, 0.0));
+                if (wgt < 0.05) wgt = 0.05;
+                hyp = qv + wgt * (hyp - qv);
+            } else {
+                hyp = 0.5 * (hyp + qv);
+            }
+        }
+        n_adj++;
+        if (!found && !dry) n_nc++;
+        if (dry) n_dry++;
+        c[q] = qv;
+        cloud[q] = qc;
+        ice[q] = qi;
+        t[q] = T / P->t_ref;
+    }
+    /* final clamp (SaturationAdjustment.h:673-685) */
+    for (size_t q = 0; q < N; q++) {
+        if (c[q] <= 0.0) c[q] = 0.0;
+        if (cloud[q] <= 0.0) cloud[q] = 0.0;
+        if (ice[q] <= 0.0) ice[q] = 0.0;
+    }
+    if (counts) { counts[0] = n_adj; counts[1] = n_nc; counts[2] = n_dry; }
+}

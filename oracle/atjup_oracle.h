@@ -78,6 +78,11 @@ void ora_shapiro(const AtjupParams* P, const ora_grid* G, double* f, int order, 
 double ora_balance_column_v(const AtjupParams* P, const ora_grid* G, ora_state* S);
 /* restoreVar (cJupiterModel.cpp:1757-1801) for the dynamics fields */
 void ora_restore(const AtjupParams* P, ora_state* S);
+/* SaturationAdjustment.h:255-746 for one gas (in place on t, c, cloud, ice); counts may be
+ * NULL, else counts[0..2] = cells adjusted, not converged, dry exits. */
+void ora_satadj(const AtjupParams* P, const ora_grid* G, const AtjupGasParams* g, double* t,
+                const double* p_stat, const double* rho_mix, double* c, double* cloud,
+                double* ice, long long* counts);
 /* One dry iteration of cJupiterModel.cpp:1032-1381 */
 void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
                        int first, int sweeps);

@@ -317,6 +317,22 @@ void ref_clamp_species() { g_m->clampNegativeSpecies(); }
 void ref_restore() { g_m->restoreVar(1.0); }
 void ref_mixture_density() { g_m->computeMixtureDensity(); }
 void ref_satadj(const char* gas) { gas_adjust(*g_m, gas); }
+
+// The 14 per-gas constants cJupiterModel passes to SaturationAdjustmentJup::run
+// (cJupiterModel.cpp:1060-1080), in the order of SaturationAdjustment.h:236-243:
+// t_0, t_00, ep, lv, ls, C, L0, R, del_alf, del_bet, C_i, L0_i, del_alf_i, del_bet_i.
+int ref_gas_consts(const char* gas, double* out) {
+    cJupiterModel& m = *g_m;
+    const std::string g(gas);
+#define G(s) { const double v[14] = {m.t_0_##s, m.t_00_##s, m.ep_##s, m.lv_##s, m.ls_##s, \
+        m.C_##s, m.L0_##s, m.R_##s, m.del_alf_##s, m.del_bet_##s, m.C_##s##_ice, m.L0_##s##_ice, \
+        m.del_alf_##s##_ice, m.del_bet_##s##_ice}; std::memcpy(out, v, sizeof v); return 0; }
+    if (g == "H2O") G(h2o)
+    if (g == "NH3") G(nh3)
+    if (g == "CH4") G(ch4)
+#undef G
+    return 1;
+}
 void ref_turbulence() { TurbulenceJup(*g_m).run(); turb_wall_omega(*g_m); }
 
 // One Shapiro filter call on a named field: order 2 = damp_wiggles, 4 = damp_wiggles_ho
@@ -426,6 +442,8 @@ int ref_knob(const char* name) {
     if (n == "precip") return k_precip();
     if (n == "phi_periodic") return ATPhys::phi_periodic<cJupiterModel>() ? 1 : 0;
     if (n == "nh4sh_eq") return ChemistryJup::nh4sh_eq() ? 1 : 0;
+    if (n == "local_rho") return cJupiterModel::local_rho() ? 1 : 0;
+    (void)m;
     return -999;
 }
 double ref_knob_d(const char* name) {

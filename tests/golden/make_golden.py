@@ -11,6 +11,10 @@ field, a digest: the L2 norm, the sum, the maximum magnitude, the SHA-256 of the
   rk4    one cJupiterModel::RungeKuttaJup on it
   press  one PressureSolverJup::run on it (1 red-black sweep)
   iter3  three iterations of the dry loop schedule (cJupiterModel.cpp:1032-1381)
+  satadj SaturationAdjustmentJup for H2O, NH3, CH4 (cJupiterModel.cpp:1060-1080) on the seeded
+         synthetic moist shell of atjup_b200.synthetic (state + moist, 41x181x361; its cone is
+         set as the reference's SeaMount), with t and the gas's fields after each gas, and the
+         14 constants of each gas as the reference derives them
 
 tests/test_oracle_ref.py compares the C oracle with these digests (and with the reference run
 live when it is built). This script is the only writer of tests/golden/*.json.
@@ -54,8 +58,27 @@ CASES = {
 }
 
 
+def satadj_case(d: dict) -> dict:
+    fields = {}
+    for gas in ("H2O", "NH3", "CH4"):
+        l = gas.lower()
+        for n in ("t", l, l + "_cloud", l + "_ice"):
+            fields[f"{gas}/{n}"] = digest(d[f"sat_{gas}_{n}"])
+    return {"case": "satadj", "flags": ["--satadj-synthetic"],
+            "source": "reference (oracle/_ref) SaturationAdjustmentJup on the synthetic moist shell",
+            "gases": {g: [float(x) for x in d["gas_" + g]] for g in ("H2O", "NH3", "CH4")},
+            "fields": fields}
+
+
 def main():
     from helpers import ref_dump
+    if "--only-satadj" not in sys.argv:
+        write_cases(ref_dump)
+    (HERE / "golden_satadj.json").write_text(json.dumps(satadj_case(ref_dump("--satadj-synthetic"))))
+    print("satadj written")
+
+
+def write_cases(ref_dump):
     for name, (flags, fields, prefix) in CASES.items():
         d = ref_dump(*flags)
         out = {"case": name, "flags": flags, "source": "reference (oracle/_ref), dry knobs",

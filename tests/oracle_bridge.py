@@ -214,3 +214,17 @@ def rel_l2(a, b):
     d = np.linalg.norm((a - b).ravel())
     n = np.linalg.norm(b.ravel())
     return d / n if n > 0 else d
+
+
+def oracle_satadj(params: AtjupParams, grid: dict, gas, t, p_stat, rho_mix, c, cloud, ice):
+    """ora_satadj on float64 C-contiguous (i, j, k) arrays, in place on t, c, cloud, ice.
+    Returns (adjusted, not_converged, dry_exits)."""
+    lib = ctypes.CDLL(str(build_oracle()))
+    solid = np.ascontiguousarray(grid["solid"], dtype=np.uint8)
+    G = OraGrid(None, None, solid.ctypes.data_as(_P(ctypes.c_uint8)), None, None, None)
+    for a in (t, p_stat, rho_mix, c, cloud, ice):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    counts = (ctypes.c_longlong * 3)()
+    lib.ora_satadj(ctypes.byref(params), ctypes.byref(G), ctypes.byref(gas), _dp(t), _dp(p_stat),
+                   _dp(rho_mix), _dp(c), _dp(cloud), _dp(ice), counts)
+    return tuple(counts)

@@ -1,15 +1,19 @@
 """Run the reference (oracle/_ref/libatjup_ref.so) in a child process and dump its state.
 
-    python tests/ref_dump.py OUT.npz [--iters N] [--rk4] [--moist] [--threads T]
+    python tests/ref_dump.py OUT.npz [--iters N] [--rk4] [--moist] [--satadj] [--threads T]
 
 Writes the reference's dry initial state (species zeroed unless --moist), its grid, its model
 constants, and -- with --iters N -- the state after N iterations of the harness loop
 (cJupiterModel.cpp:1032-1381 schedule), or with --rk4 the state after one RungeKuttaJup.
+With --satadj: the moist initial state, perturbed by seeded noise (perturb_moist) so that every
+branch of the adjustment is taken, then SaturationAdjustmentJup for H2O, NH3 and CH4 in the
+order of cJupiterModel.cpp:1060-1080, with t and the gas's fields recorded after each gas.
 Test infrastructure only.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import os
 import sys
 import tempfile
@@ -22,8 +26,33 @@ sys.path.insert(0, str(Path(__file__).resolve().parent))
 
 from oracle_bridge import DRY_ENV, DYN_FIELDS, Reference  # noqa: E402
 
+SPECIES = ("h2o", "h2o_cloud", "h2o_ice", "nh3", "nh3_cloud", "nh3_ice",
+           "ch4", "ch4_cloud", "ch4_ice")
+GASES = ("H2O", "NH3", "CH4")
+SATADJ_SEED = 20261204
+
 CONSTS = ("dt", "re", "pr", "g", "omega", "u_0", "t_ref", "L_atm", "r_mix", "R_mix", "cp_mix",
           "Coriolis", "centrifugal", "buoyancy")
+
+
+def perturb_moist(f: dict, solid: np.ndarray, seed: int = SATADJ_SEED) -> dict:
+    """Seeded perturbation of a moist state that sends cells down every path of the adjustment:
+    temperature noise of 2 % (warm cells melt ice, cold ones take the Bergeron branch), vapour
+    scaled by U(0.3, 1.7) (super- and subsaturated cells), and cloud and ice seeded in a third of
+    the cells each, at up to half the local vapour (mixed-phase and evaporating cells)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = {k: np.array(v, dtype=np.float64, copy=True) for k, v in f.items()}
+    shape = out["t"].shape
+    fluid = solid == 0
+    out["t"] = np.where(fluid, out["t"] * (1.0 + 0.02 * rng.standard_normal(shape)), out["t"])
+    for gas in ("h2o", "nh3", "ch4"):
+        vap = out[gas] * rng.uniform(0.3, 1.7, shape)
+        cl = np.where(rng.uniform(size=shape) < 1 / 3, 0.5 * vap * rng.uniform(size=shape), 0.0)
+        ic = np.where(rng.uniform(size=shape) < 1 / 3, 0.5 * vap * rng.uniform(size=shape), 0.0)
+        out[gas] = np.where(fluid, vap, out[gas])
+        out[gas + "_cloud"] = np.where(fluid, out[gas + "_cloud"] + cl, out[gas + "_cloud"])
+        out[gas + "_ice"] = np.where(fluid, out[gas + "_ice"] + ic, out[gas + "_ice"])
+    return out
 
 
 def main():
@@ -33,10 +62,12 @@ def main():
     ap.add_argument("--rk4", action="store_true")
     ap.add_argument("--pressure", action="store_true")
     ap.add_argument("--moist", action="store_true")
+    ap.add_argument("--satadj", action="store_true")
+    ap.add_argument("--satadj-synthetic", action="store_true")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
-    ref = Reference(dict(DRY_ENV), out_dir + "/run", threads=a.threads, zero_species=not a.moist)
+    ref = Reference(dict(DRY_ENV), out_dir + "/run", threads=a.threads, zero_species=not (a.moist or a.satadj or a.satadj_synthetic))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -45,7 +76,34 @@ def main():
         data["in_" + n] = v
     for c in CONSTS:
         data["const_" + c] = np.array(ref.scalar(c))
-    if a.rk4:
+    if a.satadj or a.satadj_synthetic:
+        if a.satadj:
+            f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
+        else:
+            # the synthetic shell of atjup_b200.synthetic on the reference's grid size, its cone
+            # standing in for the SeaMount mask (the only grid input of the adjustment)
+            from atjup_b200 import synthetic
+            from atjup_b200.params import DEFAULT_GASES
+            s = synthetic.state(*ref.shape)
+            f = {n: s[n] for n in ("t", "p_stat", "rho_mix")}
+            f.update(synthetic.moist(s, DEFAULT_GASES))
+            ref.set("SeaMount", s["solid"].astype(np.float64))
+            data["grid_solid"] = s["solid"].astype(np.uint8)
+        for n, v in f.items():
+            ref.set(n, v)
+            data["in_" + n] = v
+        data["knob_local_rho"] = np.array(ref.L.ref_knob(b"local_rho"))
+        for gas in GASES:
+            cst = np.zeros(14)
+            if ref.L.ref_gas_consts(gas.encode(), cst.ctypes.data_as(ctypes.c_void_p)) != 0:
+                raise SystemExit(f"no constants for {gas}")
+            data["gas_" + gas] = cst
+            ref.quiet(ref.L.ref_satadj, gas.encode())
+            data[f"sat_{gas}_t"] = ref.get("t")
+            for n in SPECIES:
+                if n.startswith(gas.lower()):
+                    data[f"sat_{gas}_{n}"] = ref.get(n)
+    elif a.rk4:
         ref.quiet(ref.L.ref_rk4)
         for n in DYN_FIELDS:
             data["out_" + n] = ref.get(n)

@@ -47,6 +47,10 @@ def test_params_struct_size_matches_oracle():
     so = ctypes.CDLL(str(build_oracle()))
     so.ora_params_sizeof.restype = ctypes.c_size_t
     assert so.ora_params_sizeof() == ctypes.sizeof(P.AtjupParams)
+    so.ora_gas_params_sizeof.restype = ctypes.c_size_t
+    assert so.ora_gas_params_sizeof() == ctypes.sizeof(P.AtjupGasParams)
+    so.ora_sat_stats_sizeof.restype = ctypes.c_size_t
+    assert so.ora_sat_stats_sizeof() == ctypes.sizeof(P.AtjupSatStats)
 
 
 def test_create_without_device_reports_no_device(lib):
