@@ -57,6 +57,13 @@ int alloc(double** p, size_t n) {
 void free_all(AtjupCtx* c) {
     solver_free(c);
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
+    for (auto& p : c->f2) { cudaFree(p); p = nullptr; }
+    for (auto& p : c->fn) { cudaFree(p); p = nullptr; }
+    for (int q = 0; q < ATJUP_S_COUNT + 2; q++) {
+        cudaFree(c->S1[q]); cudaFree(c->S2[q]); cudaFree(c->Sacc[q]);
+        c->S1[q] = c->S2[q] = c->Sacc[q] = nullptr;
+    }
+    cudaFree(c->layer_h); c->layer_h = nullptr;
     for (int q = 0; q < 4; q++) {
         cudaFree(c->X1[q]); cudaFree(c->X2[q]); cudaFree(c->acc[q]);
     }
@@ -152,6 +159,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     int rc = ATJUP_OK;
     auto A = [&](double** p, size_t n) { if (rc == ATJUP_OK) rc = alloc(p, n); };
     for (int q = 0; q < ATJUP_F_COUNT; q++) A(&c->f[q], c->NP);
+    for (int q = 0; q < ATJUP_F2_COUNT; q++) A(&c->f2[q], (size_t)P.jm * c->KP);
     for (int q = 0; q < 4; q++) { A(&c->X1[q], c->NP); A(&c->X2[q], c->NP); A(&c->acc[q], c->NP); }
     A(&c->src, c->NP);
     A(&c->tmp, c->NP);
@@ -409,9 +417,102 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
     const double* const* ins[4] = {in0, in1, in2, in1};
     double* const* outs[4] = {c->X1, c->X2, c->X1, nullptr};
     for (int s = 0; s < 4; s++) {
+        if (c->phys_on) {
+            // species and closure first: they read the same stage input velocities, and the
+            // dynamics stage 3 writes its result over the stage-0 input
+            Timed tm(c, TK_PHYS);
+            if ((rc = launch_phys_stage(c, s, ins[s]))) return rc;
+        }
         Timed tm(c, TK_RK_STAGE);
         if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
     }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_set_physics(AtjupCtx* c, const AtjupPhysics* ph, const float* layer_heights_km) {
+    if (!c) { set_error("set_physics: null context"); return ATJUP_ERR_ARG; }
+    if (!ph) { c->phys_on = false; return ATJUP_OK; }
+    if (!layer_heights_km) { set_error("set_physics: layer heights required"); return ATJUP_ERR_ARG; }
+    if (ph->turb_model < ATJUP_TURB_K_EPSILON || ph->turb_model > ATJUP_TURB_K_OMEGA_SST) {
+        set_error("set_physics: unknown turbulence model " + std::to_string(ph->turb_model));
+        return ATJUP_ERR_ARG;
+    }
+    const AtjupParams& P = c->P;
+    int rc = ATJUP_OK;
+    auto A = [&](double** p, size_t n) { if (rc == ATJUP_OK && !*p) rc = alloc(p, n); };
+    for (int s = 0; s < ATJUP_S_COUNT + 2; s++) {
+        A(&c->fn[kScalarField[s]], c->NP);
+        A(&c->S1[s], c->NP);
+        A(&c->S2[s], c->NP);
+        A(&c->Sacc[s], c->NP);
+    }
+    if (rc) return rc;
+    if (!c->layer_h) ATJUP_CUDA(cudaMalloc(&c->layer_h, sizeof(float) * P.im));
+    ATJUP_CUDA(cudaMemcpy(c->layer_h, layer_heights_km, sizeof(float) * P.im,
+                          cudaMemcpyHostToDevice));
+    c->phys = *ph;
+    c->phys_on = (ph->species_on || ph->turb_on);
+    return ATJUP_OK;
+}
+
+namespace {
+bool is_scalar_field(int id) {
+    for (int s = 0; s < ATJUP_S_COUNT + 2; s++)
+        if (kScalarField[s] == id) return true;
+    return false;
+}
+}  // namespace
+
+int atjup_gpu_upload_n(AtjupCtx* c, int32_t id, const double* host) {
+    if (!c || !host || !is_scalar_field(id) || !c->fn[id]) {
+        set_error("upload_n: not a transported scalar, or physics not set");
+        return ATJUP_ERR_ARG;
+    }
+    const size_t n = (size_t)c->P.im * c->P.jm * c->P.km;
+    ATJUP_CUDA(cudaMemcpyAsync(c->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int rc = launch_pad(c, c->stage, c->fn[id]);
+    if (rc) return rc;
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+int atjup_gpu_download_n(AtjupCtx* c, int32_t id, double* host) {
+    if (!c || !host || !is_scalar_field(id) || !c->fn[id]) {
+        set_error("download_n: not a transported scalar, or physics not set");
+        return ATJUP_ERR_ARG;
+    }
+    const size_t n = (size_t)c->P.im * c->P.jm * c->P.km;
+    int rc = launch_unpad(c, c->fn[id], c->stage);
+    if (rc) return rc;
+    ATJUP_CUDA(cudaMemcpyAsync(host, c->stage, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+int atjup_gpu_restore_scalars(AtjupCtx* c) {
+    if (!c) { set_error("restore_scalars: null context"); return ATJUP_ERR_ARG; }
+    if (!c->phys_on) return ATJUP_OK;
+    for (int s = 0; s < ATJUP_S_COUNT + 2; s++) {
+        const int id = kScalarField[s];
+        ATJUP_CUDA(cudaMemcpyAsync(c->fn[id], c->f[id], c->NP * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_upload2d(AtjupCtx* c, int32_t id, const double* host) {
+    if (!c || !host || id < 0 || id >= ATJUP_F2_COUNT) { set_error("upload2d: bad argument"); return ATJUP_ERR_ARG; }
+    ATJUP_CUDA(cudaMemcpy2DAsync(c->f2[id], c->KP * sizeof(double), host, c->P.km * sizeof(double),
+                                 c->P.km * sizeof(double), c->P.jm, cudaMemcpyHostToDevice, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    return ATJUP_OK;
+}
+
+int atjup_gpu_download2d(AtjupCtx* c, int32_t id, double* host) {
+    if (!c || !host || id < 0 || id >= ATJUP_F2_COUNT) { set_error("download2d: bad argument"); return ATJUP_ERR_ARG; }
+    ATJUP_CUDA(cudaMemcpy2DAsync(host, c->P.km * sizeof(double), c->f2[id], c->KP * sizeof(double),
+                                 c->P.km * sizeof(double), c->P.jm, cudaMemcpyDeviceToHost, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     return ATJUP_OK;
 }
 

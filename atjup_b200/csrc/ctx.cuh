@@ -50,6 +50,17 @@ struct AtjupCtx {
 
     // state and inputs (FP64); index by ATJUP_F_*
     double* f[ATJUP_F_COUNT] = {};
+    double* f2[ATJUP_F2_COUNT] = {};   // 2-D fields [jm][KP]
+    // full physics (atjup_gpu_set_physics): time-level-n copies of the transported scalars
+    // (indexed by field id, allocated for the scalars only), their stage buffers and
+    // accumulators (indexed ATJUP_S_*, then k*, omega*), the closure's layer heights
+    bool phys_on = false;
+    AtjupPhysics phys{};
+    double* fn[ATJUP_F_COUNT] = {};
+    double* S1[ATJUP_S_COUNT + 2] = {};
+    double* S2[ATJUP_S_COUNT + 2] = {};
+    double* Sacc[ATJUP_S_COUNT + 2] = {};
+    float* layer_h = nullptr;
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
     double* X2[4] = {};
@@ -107,7 +118,7 @@ void set_error(const std::string& msg);
 
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
-       TK_SOLVER, TK_SATADJ, TK_COUNT };
+       TK_SOLVER, TK_SATADJ, TK_PHYS, TK_COUNT };
 void timer_begin(AtjupCtx* c, int cls);
 void timer_end(AtjupCtx* c);
 int cuda_status(cudaError_t e, const char* what);
@@ -135,6 +146,8 @@ int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
 int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) km -> KP rows
 int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
+extern const int kScalarField[ATJUP_S_COUNT + 2];
+int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);
 

@@ -62,6 +62,12 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.atjup_gpu_satadj.argtypes = [vp, i32, ctypes.POINTER(_p.AtjupGasParams),
                                    ctypes.POINTER(_p.AtjupSatStats)]
+    L.atjup_gpu_set_physics.argtypes = [vp, ctypes.POINTER(_p.AtjupPhysics), vp]
+    L.atjup_gpu_upload_n.argtypes = [vp, i32, vp]
+    L.atjup_gpu_download_n.argtypes = [vp, i32, vp]
+    L.atjup_gpu_restore_scalars.argtypes = [vp]
+    L.atjup_gpu_upload2d.argtypes = [vp, i32, vp]
+    L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
     _lib = L
     return L
 
@@ -85,6 +91,7 @@ class GpuModel:
         self.ctx = ctypes.c_void_p()
         _check(self.L.atjup_gpu_create(ctypes.byref(params), ctypes.byref(self.ctx)))
         self._keep = {}
+        self._phys = False
         self.set_grid(grid)
 
     def close(self):
@@ -123,9 +130,52 @@ class GpuModel:
         return out
 
     def upload_state(self, fields: dict) -> None:
+        """Upload every known field in fields; with physics set, also the time-level-n copies
+        of the transported scalars (key name + "n", else the live field) and vel_star."""
         for n, a in fields.items():
             if n in _p.FIELD_IDS and a is not None:
                 self.upload(n, a)
+        if self._phys:
+            for n in _p.SCALARS:
+                src = fields.get(n + "n", fields.get(n))
+                if src is not None:
+                    self.upload_n(n, src)
+            if fields.get("vel_star") is not None:
+                self.upload2d("vel_star", fields["vel_star"])
+
+    # ---- full physics ----
+    def set_physics(self, phys: "_p.AtjupPhysics | None", layer_heights=None):
+        """atjup_gpu_set_physics: species and k*, omega* join the RK4 step (None: dynamics only).
+        layer_heights: the model's m_layer_heights [km] per level (float32)."""
+        if phys is None:
+            _check(self.L.atjup_gpu_set_physics(self.ctx, None, None))
+            self._phys = False
+            return
+        lh = np.ascontiguousarray(layer_heights, np.float32)
+        assert lh.shape == (self.shape[0],)
+        _check(self.L.atjup_gpu_set_physics(self.ctx, ctypes.byref(phys), _ptr(lh)))
+        self._phys = True
+
+    def upload_n(self, name: str, a) -> None:
+        a = np.ascontiguousarray(a, np.float64).reshape(self.shape)
+        _check(self.L.atjup_gpu_upload_n(self.ctx, _p.FIELD_IDS[name], _ptr(a)))
+
+    def download_n(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape)
+        _check(self.L.atjup_gpu_download_n(self.ctx, _p.FIELD_IDS[name], _ptr(out)))
+        return out
+
+    def restore_scalars(self) -> None:
+        _check(self.L.atjup_gpu_restore_scalars(self.ctx))
+
+    def upload2d(self, name: str, a) -> None:
+        a = np.ascontiguousarray(a, np.float64).reshape(self.shape[1:])
+        _check(self.L.atjup_gpu_upload2d(self.ctx, {"vel_star": _p.F2_VEL_STAR}[name], _ptr(a)))
+
+    def download2d(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape[1:])
+        _check(self.L.atjup_gpu_download2d(self.ctx, {"vel_star": _p.F2_VEL_STAR}[name], _ptr(out)))
+        return out
 
     def field_ptr(self, name: str):
         p = ctypes.c_void_p()
@@ -200,7 +250,7 @@ class GpuModel:
 
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
-                      "mixture", "solver", "satadj")
+                      "mixture", "solver", "satadj", "phys")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

@@ -20,7 +20,13 @@ ABI_VERSION = 1
 F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, \
     F_AUX_U, F_AUX_V, F_AUX_W, F_P_BARO, F_Q_RAD, F_Q_PRECIP, \
     F_H2O, F_H2O_CLOUD, F_H2O_ICE, F_NH3, F_NH3_CLOUD, F_NH3_ICE, \
-    F_CH4, F_CH4_CLOUD, F_CH4_ICE = range(25)
+    F_CH4, F_CH4_CLOUD, F_CH4_ICE, F_H2S, F_NH4SH, F_TKE, F_DIS, \
+    F_S_PRECIP_H2O, F_S_PRECIP_H2O_CLOUD, F_S_PRECIP_H2O_ICE, \
+    F_S_PRECIP_NH3, F_S_PRECIP_NH3_CLOUD, F_S_PRECIP_NH3_ICE, \
+    F_S_PRECIP_CH4, F_S_PRECIP_CH4_CLOUD, F_S_PRECIP_CH4_ICE, \
+    F_MASSFLUX_H2S, F_MASSFLUX_NH3, F_MASSFLUX_NH4SH, F_FLUXLIM_NH4SH, \
+    F_PROD, F_TKE_SOURCE, F_DIS_SOURCE = range(45)
+F2_VEL_STAR = 0
 FIELD_IDS = {
     "t": F_T, "u": F_U, "v": F_V, "w": F_W, "p_dyn": F_P_DYN, "p_hydro": F_P_HYDRO,
     "p_stat": F_P_STAT, "rho_mix": F_RHO_MIX, "wall_nue": F_WALL_NUE, "nue": F_NUE,
@@ -29,7 +35,26 @@ FIELD_IDS = {
     "h2o": F_H2O, "h2o_cloud": F_H2O_CLOUD, "h2o_ice": F_H2O_ICE,
     "nh3": F_NH3, "nh3_cloud": F_NH3_CLOUD, "nh3_ice": F_NH3_ICE,
     "ch4": F_CH4, "ch4_cloud": F_CH4_CLOUD, "ch4_ice": F_CH4_ICE,
+    "h2s": F_H2S, "nh4sh": F_NH4SH, "tke": F_TKE, "dis": F_DIS,
+    "S_precip_h2o": F_S_PRECIP_H2O, "S_precip_h2o_cloud": F_S_PRECIP_H2O_CLOUD,
+    "S_precip_h2o_ice": F_S_PRECIP_H2O_ICE, "S_precip_nh3": F_S_PRECIP_NH3,
+    "S_precip_nh3_cloud": F_S_PRECIP_NH3_CLOUD, "S_precip_nh3_ice": F_S_PRECIP_NH3_ICE,
+    "S_precip_ch4": F_S_PRECIP_CH4, "S_precip_ch4_cloud": F_S_PRECIP_CH4_CLOUD,
+    "S_precip_ch4_ice": F_S_PRECIP_CH4_ICE,
+    "massflux_h2s": F_MASSFLUX_H2S, "massflux_nh3": F_MASSFLUX_NH3,
+    "massflux_nh4sh": F_MASSFLUX_NH4SH, "fluxlim_nh4sh": F_FLUXLIM_NH4SH,
+    "prod": F_PROD, "tke_source": F_TKE_SOURCE, "dis_source": F_DIS_SOURCE,
 }
+
+# transported scalars in the order of the physics block (ATJUP_S_*), and the fields whose
+# time-level-n copies the RK step keeps (the species, then k*, omega*)
+SPECIES = ("h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3", "nh3_cloud", "nh3_ice", "ch4",
+           "ch4_cloud", "ch4_ice", "nh4sh")
+SCALARS = SPECIES + ("tke", "dis")
+S_PRECIP = ("S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+            "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4", "S_precip_ch4_cloud",
+            "S_precip_ch4_ice")
+TURB_K_EPSILON, TURB_K_OMEGA, TURB_K_OMEGA_SST = 0, 1, 2
 
 # gas ids of atjup_gpu_satadj, in the order cJupiterModel.cpp:1060-1080 calls them
 GAS_H2O, GAS_NH3, GAS_CH4 = 0, 1, 2
@@ -97,6 +122,54 @@ class AtjupGasParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in GAS_CONST_NAMES] + [
         (n, ctypes.c_int32) for n in ("conserve", "newton", "evap", "ice_entry", "bergeron",
                                       "freeze", "dry_exit", "reserved")]
+
+
+class AtjupPhysics(ctypes.Structure):
+    """Mirror of AtjupPhysics (full physics in the RK4 step)."""
+    _fields_ = [("species_on", ctypes.c_int32), ("turb_on", ctypes.c_int32),
+                ("turb_model", ctypes.c_int32), ("turb_buoy", ctypes.c_int32)] + [
+        (n, ctypes.c_double) for n in ("species_diff_scale", "sc_h2o", "sc_h2s", "sc_nh3",
+                                       "sc_ch4", "sc_nh4sh", "chemical_reaction", "r_p_nh4sh",
+                                       "rg_nh4sh", "mue_mix", "re_turb", "nue_max_phys",
+                                       "tke_max_phys", "turb_buoy_prt")]
+
+
+# cJupiterModel's constants of the species transport (cJupiterModel.h:290, 470-477, 594) and the
+# closure (Turbulence.h:123); mue_mix, chemical_reaction and re_turb are the values the reference
+# derives at start-up with its default composition and parameters.
+DEFAULT_PHYSICS = {"species_diff_scale": 0.01, "sc_h2o": 0.61, "sc_h2s": 0.94, "sc_nh3": 0.61,
+                   "sc_ch4": 0.99, "sc_nh4sh": 0.7, "r_p_nh4sh": 1.0e-5, "rg_nh4sh": 1170.0,
+                   "nue_max_phys": 1.0e5}
+
+
+def resolve_physics(env: Mapping[str, str] | None = None, constants: Mapping[str, float] | None = None,
+                    species_on: bool = True) -> AtjupPhysics:
+    """Physics block from the environment with the reference's defaults: ATJUP_TURB (else on
+    unless ATJUP_TURB_MODEL / turb_model is empty, none or laminar; cJupiterModel.cpp:61-78), ATJUP_TURB_MODEL
+    (k_omega_SST), ATJUP_TURB_BUOY 0, ATJUP_SPECIES_DIFF_SCALE 0.01, ATJUP_NUE_MAX 1e5,
+    ATJUP_TKE_MAX 1000, ATJUP_TURB_BUOY_PRT 0.9. constants supplies mue_mix,
+    chemical_reaction and re_turb (and may override any DEFAULT_PHYSICS entry)."""
+    env = os.environ if env is None else env
+    c = dict(DEFAULT_PHYSICS)
+    c.update({"mue_mix": 1.0819029080091497e-05, "chemical_reaction": 1.0,
+              "re_turb": 2222.2222222222226})
+    if constants:
+        c.update({k: float(v) for k, v in constants.items() if k in c or k in ("mue_mix", "chemical_reaction", "re_turb")})
+    model = env.get("ATJUP_TURB_MODEL", "k_omega_SST")
+    turb_model = {"k_epsilon": TURB_K_EPSILON, "k_omega": TURB_K_OMEGA}.get(model, TURB_K_OMEGA_SST)
+    if "ATJUP_TURB" in env:
+        turb_on = _env(env, "ATJUP_TURB", 1) != 0
+    else:
+        turb_on = model not in ("", "none", "laminar")
+    c["species_diff_scale"] = _env(env, "ATJUP_SPECIES_DIFF_SCALE", c["species_diff_scale"], float)
+    c["nue_max_phys"] = _env(env, "ATJUP_NUE_MAX", c["nue_max_phys"], float)
+    ph = AtjupPhysics(int(species_on), int(turb_on), turb_model, _env(env, "ATJUP_TURB_BUOY", 0))
+    for n in ("species_diff_scale", "sc_h2o", "sc_h2s", "sc_nh3", "sc_ch4", "sc_nh4sh",
+              "chemical_reaction", "r_p_nh4sh", "rg_nh4sh", "mue_mix", "re_turb", "nue_max_phys"):
+        setattr(ph, n, c[n])
+    ph.tke_max_phys = _env(env, "ATJUP_TKE_MAX", 1000.0, float)
+    ph.turb_buoy_prt = _env(env, "ATJUP_TURB_BUOY_PRT", 0.9, float)
+    return ph
 
 
 class AtjupSatStats(ctypes.Structure):

@@ -151,6 +151,41 @@ def moist(s: dict, gases: dict, seed: int = 20261205, t_ref: float = 165.0) -> d
     return out
 
 
+def physics(s: dict, gases: dict, seed: int = 20261206, u_0: float = 100.0,
+            L_atm: float = 140.0) -> dict:
+    """Full-physics fields for a state from state(): the species of moist(), h2s and nh4sh,
+    k* = k / u_0^2 with k = 1e-4 m2/s2 x U(0.5, 1.5), omega* = omega L / u_0 with
+    omega = 1e-3 1/s x U(0.5, 1.5), their time-level-n copies (equal to the live fields), a
+    frozen eddy viscosity nue* = k*/omega*, seeded frozen microphysics and chemistry sources of
+    1e-6 scale, heating rates of 0.05 W/m3 scale, the friction velocity 0.05 m/s and the level
+    heights [km] (float32). Zero in solid cells."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    t = s["t"]
+    shape = t.shape
+    im = shape[0]
+    fluid = s["solid"] == 0
+    out = moist(s, gases, seed=seed + 1)
+    out["h2s"] = np.where(fluid, 1e-3 * rng.uniform(0.5, 1.5, shape), 0.0)
+    out["nh4sh"] = np.where(fluid, 1e-5 * rng.uniform(0.0, 1.0, shape), 0.0)
+    tke = 1e-4 / u_0 ** 2 * rng.uniform(0.5, 1.5, shape)
+    om = 1e-3 * (L_atm * 1e3 / u_0) * rng.uniform(0.5, 1.5, shape)
+    out["tke"] = np.where(fluid, tke, 0.0)
+    out["dis"] = np.where(fluid, om, 0.0)
+    out["nue"] = np.where(fluid, tke / om, 0.0)
+    for n in ("S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+              "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4", "S_precip_ch4_cloud",
+              "S_precip_ch4_ice", "massflux_h2s", "massflux_nh3", "massflux_nh4sh",
+              "fluxlim_nh4sh"):
+        out[n] = np.where(fluid, 1e-6 * rng.standard_normal(shape), 0.0)
+    out["Q_rad"] = np.where(fluid, 0.05 * rng.standard_normal(shape), 0.0)
+    out["Q_precip"] = np.where(fluid, 0.05 * rng.standard_normal(shape), 0.0)
+    for n in ("prod", "tke_source", "dis_source"):
+        out[n] = np.zeros(shape)
+    out["vel_star"] = np.full(shape[1:], 0.05)
+    out["layer_heights"] = (np.arange(im) * (L_atm / (im - 1))).astype(np.float32)
+    return out
+
+
 def smooth121(f: np.ndarray, passes: int = 3) -> np.ndarray:
     """`passes` Shapiro 1-2-1 passes in k (ring of km-1 meridians, seam copy), then j (clamped at
     the poles), then i (clamped), no fluid floor -- damp_wiggles with i_surface = nullptr

@@ -50,8 +50,20 @@ enum {
     ATJUP_F_H2O, ATJUP_F_H2O_CLOUD, ATJUP_F_H2O_ICE,          /* condensable species [kg/m3]   */
     ATJUP_F_NH3, ATJUP_F_NH3_CLOUD, ATJUP_F_NH3_ICE,          /* (vapour, cloud, ice per gas)  */
     ATJUP_F_CH4, ATJUP_F_CH4_CLOUD, ATJUP_F_CH4_ICE,
+    ATJUP_F_H2S, ATJUP_F_NH4SH,                               /* chemistry species [kg/m3]     */
+    ATJUP_F_TKE, ATJUP_F_DIS,                                 /* turbulence k*, omega* (or eps)*/
+    ATJUP_F_S_PRECIP_H2O, ATJUP_F_S_PRECIP_H2O_CLOUD, ATJUP_F_S_PRECIP_H2O_ICE,
+    ATJUP_F_S_PRECIP_NH3, ATJUP_F_S_PRECIP_NH3_CLOUD, ATJUP_F_S_PRECIP_NH3_ICE,
+    ATJUP_F_S_PRECIP_CH4, ATJUP_F_S_PRECIP_CH4_CLOUD, ATJUP_F_S_PRECIP_CH4_ICE,
+                                                              /* frozen microphysics sources   */
+    ATJUP_F_MASSFLUX_H2S, ATJUP_F_MASSFLUX_NH3, ATJUP_F_MASSFLUX_NH4SH,
+    ATJUP_F_FLUXLIM_NH4SH,                                    /* frozen chemistry sources      */
+    ATJUP_F_PROD, ATJUP_F_TKE_SOURCE, ATJUP_F_DIS_SOURCE,     /* closure diagnostics (out)     */
     ATJUP_F_COUNT
 };
+
+/* 2-D (jm x km) fields: the friction velocity of the k-epsilon wall term (Turbulence.h:336-377) */
+enum { ATJUP_F2_VEL_STAR = 0, ATJUP_F2_COUNT };
 
 /* ---- solver modes for atjup_gpu_pressure_solve ---- */
 enum {
@@ -210,6 +222,44 @@ int atjup_gpu_balance_column_v_noalloc(double* v, const int32_t* i_topo, const d
                                        int32_t im, int32_t jm, int32_t km, int32_t pitch,
                                        double dr, int32_t zonal, void* stream);
 
+/* ---- full physics in the RK4 step (RHS_Jup_Turb.cpp:132-303, 459-998, 1266-1452) ---- */
+
+/* The transported scalars, in the order RHSJup writes them (RHS_Jup_Turb.cpp:1273-1333). */
+enum { ATJUP_S_H2O = 0, ATJUP_S_H2O_CLOUD, ATJUP_S_H2O_ICE, ATJUP_S_H2S, ATJUP_S_NH3,
+       ATJUP_S_NH3_CLOUD, ATJUP_S_NH3_ICE, ATJUP_S_CH4, ATJUP_S_CH4_CLOUD, ATJUP_S_CH4_ICE,
+       ATJUP_S_NH4SH, ATJUP_S_COUNT };
+enum { ATJUP_TURB_K_EPSILON = 0, ATJUP_TURB_K_OMEGA = 1, ATJUP_TURB_K_OMEGA_SST = 2 };
+
+typedef struct AtjupPhysics {
+    int32_t species_on;          /* 1: the 11 species are integrated with the dynamics           */
+    int32_t turb_on;             /* use_turbulence_model (ATJUP_TURB, turb_model; default on)     */
+    int32_t turb_model;          /* ATJUP_TURB_MODEL / turb_model, default k_omega_SST            */
+    int32_t turb_buoy;           /* ATJUP_TURB_BUOY 0: buoyancy production of k* (RHS:963-981)   */
+    double species_diff_scale;   /* ATJUP_SPECIES_DIFF_SCALE 0.01 (cJupiterModel.h:470)          */
+    double sc_h2o, sc_h2s, sc_nh3, sc_ch4, sc_nh4sh;   /* Schmidt numbers (cJupiterModel.h:473) */
+    double chemical_reaction;    /* coupling of the chemistry mass fluxes                        */
+    double r_p_nh4sh, rg_nh4sh;  /* NH4SH crystal radius [m] and density [kg/m3] (Stokes fall)   */
+    double mue_mix;              /* dynamic viscosity of the mixture                              */
+    double re_turb;              /* k-epsilon near-wall term scale (TurbulenceJup)                */
+    double nue_max_phys;         /* ATJUP_NUE_MAX 1e5 m2/s (Turbulence.h:123)                     */
+    double tke_max_phys;         /* ATJUP_TKE_MAX 1000 m2/s2 (RungeKutta_Jup_Turb.cpp:269)        */
+    double turb_buoy_prt;        /* ATJUP_TURB_BUOY_PRT 0.9                                       */
+} AtjupPhysics;
+
+/* Switch the RK4 step to full physics: the 11 species and (turb_on) k*, omega* are integrated
+ * with t, u, v, w, each with its own time-level-n copy (the reference's h2on .. disn).
+ * layer_heights_km[im] is m_layer_heights (float, km), the wall distance of the closure.
+ * Allocates the scalar stage buffers on first use. phys = NULL switches back to dynamics only. */
+int atjup_gpu_set_physics(AtjupCtx* ctx, const AtjupPhysics* phys, const float* layer_heights_km);
+/* The time-level-n copy of a transported scalar (field ids ATJUP_F_H2O .. ATJUP_F_DIS). */
+int atjup_gpu_upload_n(AtjupCtx* ctx, int32_t field_id, const double* host);
+int atjup_gpu_download_n(AtjupCtx* ctx, int32_t field_id, double* host);
+/* restoreVar for the scalars (cJupiterModel.cpp:1757-1801): n copy <- live field. */
+int atjup_gpu_restore_scalars(AtjupCtx* ctx);
+/* 2-D fields, contiguous (j, k). */
+int atjup_gpu_upload2d(AtjupCtx* ctx, int32_t field_id, const double* host);
+int atjup_gpu_download2d(AtjupCtx* ctx, int32_t field_id, double* host);
+
 /* ---- saturation adjustment (SaturationAdjustment.h:255-746, Tao et al. 1988) ---- */
 enum { ATJUP_GAS_H2O = 0, ATJUP_GAS_NH3 = 1, ATJUP_GAS_CH4 = 2 };
 
@@ -257,7 +307,8 @@ int atjup_gpu_nonfinite_count(AtjupCtx* ctx, int64_t* count);
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
  * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */
 enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
-       ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_COUNT };
+       ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_PHYS,
+       ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */

@@ -1142,3 +1142,363 @@ void ora_satadj(const AtjupParams* P, const ora_grid* G, const AtjupGasParams* g
     }
     if (counts) { counts[0] = n_adj; counts[1] = n_nc; counts[2] = n_dry; }
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * Full physics in the RK4 step: the 11 species and k*, omega* (RHS_Jup_Turb.cpp:132-303 for the
+ * derivatives, 482-545 transport and diffusion, 736-998 the closure sources, 1266-1452 the
+ * right-hand sides; RungeKutta_Jup_Turb.cpp:419-568 the stage and final updates).
+ * ------------------------------------------------------------------------------------------- */
+
+/* m_layer_heights is float [km]; get_layer_height(i) is -1 outside 0..im-1 (cJupiterModel.h:
+ * 133-138), layer_thickness_m(i) -1 outside 0..im-2 and the float difference times 1e3. */
+static double layer_h(const ora_phys* X, int im, int i) {
+    if (i < 0 || i > im - 1) return (double)(-1.0f);
+    return (double)X->layer_heights[i];
+}
+static double layer_dz_m(const ora_phys* X, int im, int i) {
+    if (i < 0 || i > im - 2) return -1.0;
+    return (double)(X->layer_heights[i + 1] - X->layer_heights[i]) * 1.0e3;
+}
+
+/* Per-species diffusion Schmidt number and source terms (RHS_Jup_Turb.cpp:1273-1340). */
+static double species_sc(const AtjupPhysics* PH, int s) {
+    switch (s) {
+    case ATJUP_S_H2O: case ATJUP_S_H2O_CLOUD: case ATJUP_S_H2O_ICE: return PH->sc_h2o;
+    case ATJUP_S_H2S: return PH->sc_h2s;
+    case ATJUP_S_NH3: case ATJUP_S_NH3_CLOUD: case ATJUP_S_NH3_ICE: return PH->sc_nh3;
+    case ATJUP_S_CH4: case ATJUP_S_CH4_CLOUD: case ATJUP_S_CH4_ICE: return PH->sc_ch4;
+    default: return PH->sc_nh4sh;
+    }
+}
+
+/* index of the species' S_precip field in ora_phys.s_precip (-1: none) */
+static int species_precip(int s) {
+    switch (s) {
+    case ATJUP_S_H2O: return 0;
+    case ATJUP_S_H2O_CLOUD: return 1;
+    case ATJUP_S_H2O_ICE: return 2;
+    case ATJUP_S_NH3: return 3;
+    case ATJUP_S_NH3_CLOUD: return 4;
+    case ATJUP_S_NH3_ICE: return 5;
+    case ATJUP_S_CH4: return 6;
+    case ATJUP_S_CH4_CLOUD: return 7;
+    case ATJUP_S_CH4_ICE: return 8;
+    default: return -1;
+    }
+}
+
+/* Right-hand sides of the species and of k*, omega* at one cell, from the live fields. */
+void ora_rhs_phys_cell(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G,
+                       ora_state* S, ora_phys* X, int i, int j, int k) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    geom g;
+    make_geom(P, G, i, j, &g);
+    const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+    const size_t c = IDX(i, j, k);
+    const size_t cip = IDX(i + 1, j, k), cim = IDX(i - 1, j, k);
+    const size_t cjp = IDX(i, j + 1, k), cjm = IDX(i, j - 1, k);
+    const size_t ckp = IDX(i, j, ke), ckm = IDX(i, j, kw);
+    const double u_ijk = S->u[c], v_ijk = S->v[c], w_ijk = S->w[c];
+    const double v_invrm = v_ijk * g.inv_rm;
+    const double w_invrs = w_ijk * g.inv_rmsinthe;
+    const double two_inv_rm = 2.0 * g.inv_rm;
+
+    double nue_t = 0.0;
+    if (P->has_nue && S->nue && P->turb_coupling != 0.0 && isfinite(S->nue[c]))
+        nue_t = P->turb_coupling * dmax(0.0, S->nue[c]);
+    const double nue_t_s = nue_t / 0.9;
+
+#define DR1(F) ((F[cip] - F[cim]) * g.inv_2dr * g.exp_rm)
+#define DR2(F) ((F[cip] - 2.0 * F[c] + F[cim]) * g.inv_dr2 * g.exp_2_rm)
+#define DT1(F) ((F[cjp] - F[cjm]) * g.inv_2dthe)
+#define DT2(F) ((F[cjp] - 2.0 * F[c] + F[cjm]) * g.inv_dthe2)
+#define DP1(F) ((F[ckp] - F[ckm]) * g.inv_2dphi)
+#define DP2(F) ((F[ckp] - 2.0 * F[c] + F[ckm]) * g.inv_dphi2)
+
+    if (PH->species_on) {
+        const double v_stokes = (2.0 / 9.0) * PH->r_p_nh4sh * PH->r_p_nh4sh
+                              * (PH->rg_nh4sh - S->rho_mix[c]) * P->g / PH->mue_mix;
+        for (int s = 0; s < ATJUP_S_COUNT; s++) {
+            const double* F = X->q[s];
+            const double d1r = DR1(F), d2r = DR2(F), d1t = DT1(F), d2t = DT2(F);
+            const double d1p = DP1(F), d2p = DP2(F);
+            const double transport = u_ijk * d1r + v_invrm * d1t + w_invrs * d1p;
+            const double diffusion = d2r + d1r * two_inv_rm + d2t * g.inv_rm2
+                + d1t * g.costhe_inv_rm2sinthe + d2p * g.inv_rm2sinthe2;
+            const double coef = PH->species_diff_scale / (species_sc(PH, s) * P->re) + nue_t_s;
+            const int ip = species_precip(s);
+            double r;
+            if (s == ATJUP_S_H2S) {
+                r = -transport + diffusion * coef + PH->chemical_reaction * X->massflux_h2s[c];
+            } else if (s == ATJUP_S_NH3) {
+                r = -transport + diffusion * coef + PH->chemical_reaction * X->massflux_nh3[c]
+                  + P->precip_coupling * X->s_precip[ip][c];
+            } else if (s == ATJUP_S_NH4SH) {
+                r = -transport + X->fluxlim_nh4sh[c] + diffusion * coef
+                  + PH->chemical_reaction * X->massflux_nh4sh[c] + (v_stokes / P->u_0) * d1r;
+            } else {
+                r = -transport + diffusion * coef + P->precip_coupling * X->s_precip[ip][c];
+            }
+            X->rhs_q[s][c] = r;
+        }
+    }
+
+    if (!PH->turb_on) {
+        X->rhs_tke[c] = 0.0;
+        X->rhs_dis[c] = 0.0;
+        return;
+    }
+    /* derivatives of k*, omega*: central, solid neighbours replaced by the cell (257-303) */
+    const double *TK = X->tke, *DS = X->dis;
+    const uint8_t* sol = G->solid;
+    double dtkedr = DR1(TK), d2tkedr2 = DR2(TK), ddisdr = DR1(DS), d2disdr2 = DR2(DS);
+    double dtkedthe = DT1(TK), d2tkedthe2 = DT2(TK), ddisdthe = DT1(DS), d2disdthe2 = DT2(DS);
+    double dtkedphi = DP1(TK), d2tkedphi2 = DP2(TK), ddisdphi = DP1(DS), d2disdphi2 = DP2(DS);
+    {
+        const int s_im = sol[cim], s_ip = sol[cip], s_jm = sol[cjm], s_jp = sol[cjp];
+        const int s_km = sol[ckm], s_kp = sol[ckp];
+        if (s_im || s_ip) {
+            const double tm = s_im ? TK[c] : TK[cim], tp = s_ip ? TK[c] : TK[cip];
+            const double dm = s_im ? DS[c] : DS[cim], dp = s_ip ? DS[c] : DS[cip];
+            dtkedr = (tp - tm) * g.inv_2dr * g.exp_rm;
+            d2tkedr2 = (tp - 2.0 * TK[c] + tm) * g.inv_dr2 * g.exp_2_rm;
+            ddisdr = (dp - dm) * g.inv_2dr * g.exp_rm;
+            d2disdr2 = (dp - 2.0 * DS[c] + dm) * g.inv_dr2 * g.exp_2_rm;
+        }
+        if (s_jm || s_jp) {
+            const double tm = s_jm ? TK[c] : TK[cjm], tp = s_jp ? TK[c] : TK[cjp];
+            const double dm = s_jm ? DS[c] : DS[cjm], dp = s_jp ? DS[c] : DS[cjp];
+            dtkedthe = (tp - tm) * g.inv_2dthe;
+            d2tkedthe2 = (tp - 2.0 * TK[c] + tm) * g.inv_dthe2;
+            ddisdthe = (dp - dm) * g.inv_2dthe;
+            d2disdthe2 = (dp - 2.0 * DS[c] + dm) * g.inv_dthe2;
+        }
+        if (s_km || s_kp) {
+            const double tm = s_km ? TK[c] : TK[ckm], tp = s_kp ? TK[c] : TK[ckp];
+            const double dm = s_km ? DS[c] : DS[ckm], dp = s_kp ? DS[c] : DS[ckp];
+            dtkedphi = (tp - tm) * g.inv_2dphi;
+            d2tkedphi2 = (tp - 2.0 * TK[c] + tm) * g.inv_dphi2;
+            ddisdphi = (dp - dm) * g.inv_2dphi;
+            d2disdphi2 = (dp - 2.0 * DS[c] + dm) * g.inv_dphi2;
+        }
+    }
+    const double *U = S->u, *V = S->v, *W = S->w;
+    const double dudr = DR1(U), dvdr = DR1(V), dwdr = DR1(W);
+    const double dudthe = DT1(U), dvdthe = DT1(V), dwdthe = DT1(W);
+    const double dudphi = DP1(U), dvdphi = DP1(V), dwdphi = DP1(W);
+#undef DR1
+#undef DR2
+#undef DT1
+#undef DT2
+#undef DP1
+#undef DP2
+    const double transport_tke = u_ijk * dtkedr + v_invrm * dtkedthe + w_invrs * dtkedphi;
+    const double transport_dis = u_ijk * ddisdr + v_invrm * ddisdthe + w_invrs * ddisdphi;
+    const double diffusion_tke = d2tkedr2 + dtkedr * two_inv_rm + d2tkedthe2 * g.inv_rm2
+        + dtkedthe * g.costhe_inv_rm2sinthe + d2tkedphi2 * g.inv_rm2sinthe2;
+    const double diffusion_dis = d2disdr2 + ddisdr * two_inv_rm + d2disdthe2 * g.inv_rm2
+        + ddisdthe * g.costhe_inv_rm2sinthe + d2disdphi2 * g.inv_rm2sinthe2;
+
+    /* closure sources (781-998) */
+    const double C_nue = 0.028, dis_min = 1.0e-10, nue_gas_phys = 1.8e-5;
+    const double L_m = P->L_atm * 1.0e3;
+    const double nue_max = PH->nue_max_phys / (P->u_0 * L_m);
+    const double nue_here = (S->nue && isfinite(S->nue[c])) ? dmax(0.0, S->nue[c]) : 0.0;
+    const double tke_c = TK[c], dis_c = DS[c];
+    const double tke_s = dmax(tke_c, dis_min);
+    const double dis_s = dmax(dis_c, dis_min);
+    const double dudr_s = dudr, dvdr_s = dvdr, dwdr_s = dwdr;
+    const double dudthe_s = dudthe * g.inv_rm, dvdthe_s = dvdthe * g.inv_rm;
+    const double dwdthe_s = dwdthe * g.inv_rm;
+    const double dudphi_s = dudphi * g.inv_rmsinthe, dvdphi_s = dvdphi * g.inv_rmsinthe;
+    const double dwdphi_s = dwdphi * g.inv_rmsinthe;
+    const double dtkedthe_s = dtkedthe * g.inv_rm, ddisdthe_s = ddisdthe * g.inv_rm;
+    const double dtkedphi_s = dtkedphi * g.inv_rmsinthe, ddisdphi_s = ddisdphi * g.inv_rmsinthe;
+    const double grad_dot = dtkedr * ddisdr + dtkedthe_s * ddisdthe_s + dtkedphi_s * ddisdphi_s;
+    double cnue = (PH->turb_model == ATJUP_TURB_K_EPSILON) ? C_nue * tke_s * tke_s / dis_s
+                                                           : tke_s / dis_s;
+    cnue = dmin(cnue, nue_max);
+    const double der = 0.66667 * (dudr_s + dvdthe_s + dwdphi_s);
+    const double P_full = dmax(0.0,
+          (cnue * (2.0 * dudr_s - der) - 0.66667 * tke_c) * dudr_s
+        + (cnue * (dudthe_s + dvdr_s)) * dudthe_s
+        + (cnue * (dudphi_s + dwdr_s)) * dudphi_s
+        + (cnue * (2.0 * dvdthe_s - der) - 0.66667 * tke_c) * dvdthe_s
+        + (cnue * (dvdr_s + dudthe_s)) * dvdr_s
+        + (cnue * (dvdphi_s + dwdthe_s)) * dvdphi_s
+        + (cnue * (2.0 * dwdphi_s - der) - 0.66667 * tke_c) * dwdphi_s
+        + (cnue * (dwdr_s + dudphi_s)) * dwdr_s
+        + (cnue * (dwdthe_s + dvdphi_s)) * dwdthe_s);
+    X->prod[c] = P_full;
+
+    const double y_mount = layer_h(X, im, G->topo[(size_t)j * km + k]) * 1.0e3;
+    const double dz_layer = dmax(1.0, layer_dz_m(X, im, i - 1 > 0 ? i - 1 : 0));
+    const double y_phys = dmax(layer_h(X, im, i) * 1.0e3 - y_mount, dz_layer);
+    const double y_star = y_phys / L_m;
+
+    double diffusion_tke_re = 0.0, diffusion_dis_re = 0.0, tke_src = 0.0, dis_src = 0.0;
+    double c_w_prod = 0.0;
+    if (PH->turb_model == ATJUP_TURB_K_EPSILON) {           /* Chien 1982 (799-829) */
+        const double sig_k = 1.0, sig_w = 1.3, C_eps_1 = 1.35, C_eps_2 = 1.80;
+        diffusion_tke_re = 1.0 / P->re + nue_here / sig_k;
+        diffusion_dis_re = 1.0 / P->re + nue_here / sig_w;
+        const double d_plus = y_phys * X->vel_star[(size_t)j * km + k] / nue_gas_phys;
+        const double Re_T = tke_s * tke_s * P->u_0 * L_m / (dis_s * nue_gas_phys);
+        const double f_2 = 1.0 - 0.4 / 1.8 * exp(-Re_T * Re_T / 36.0);
+        const double y_star2 = y_star * y_star;
+        const double L_k = -2.0 * tke_c / y_star2;
+        const double L_w = -2.0 * dis_c / y_star2 * exp(-0.5 * d_plus);
+        const double P_k = P_full;
+        const double Y_k = dis_c;
+        const double P_w = C_eps_1 * dis_c / tke_s * P_k;
+        const double Y_w = C_eps_2 * f_2 * dis_c * dis_c / tke_s;
+        tke_src = P_k - Y_k + L_k / PH->re_turb;
+        dis_src = P_w - Y_w + L_w / PH->re_turb;
+        c_w_prod = C_eps_1;
+    } else if (PH->turb_model == ATJUP_TURB_K_OMEGA) {       /* Wilcox (830-875) */
+        const double sig_k = 0.6, sig_w = 0.5, bet_star = 0.09, gam = 0.52, bet_0 = 0.0708;
+        diffusion_tke_re = 1.0 / P->re + sig_k * nue_here;
+        diffusion_dis_re = 1.0 / P->re + sig_w * nue_here;
+        const double S11 = dudr_s, S22 = dvdthe_s, S33 = dwdphi_s;
+        const double S12 = 0.5 * (dudthe_s + dvdr_s);
+        const double S13 = 0.5 * (dudphi_s + dwdr_s);
+        const double S23 = 0.5 * (dvdphi_s + dwdthe_s);
+        const double S_mag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33
+                                         + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
+        const double W12 = dudthe_s - dvdr_s;
+        const double W13 = dudphi_s - dwdr_s;
+        const double W23 = dvdphi_s - dwdthe_s;
+        const double Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
+        const double chi_w = fabs(Omega * Omega * S_mag / pow(bet_star * dis_s, 3));
+        const double f_bet = (1.0 + 85.0 * chi_w) / (1.0 + 100.0 * chi_w);
+        const double bet_wc = bet_0 * f_bet;
+        const double sig_d = (grad_dot <= 0.0) ? 0.0 : 0.125;
+        const double P_k = dmin(P_full, 20.0 * bet_star * tke_s * dis_s);
+        const double Y_k = bet_star * tke_s * dis_s;
+        const double P_w = gam * dis_s / tke_s * P_k;
+        const double Y_w = bet_wc * dis_s * dis_s;
+        const double D_w = sig_d / dis_s * grad_dot;
+        tke_src = P_k - Y_k;
+        dis_src = P_w - Y_w + D_w;
+        c_w_prod = gam;
+    } else {                                                  /* SST, Menter 1994 (876-960) */
+        const double bet_star = 0.09, sig_k1 = 1.176, sig_k2 = 1.0, sig_w1 = 2.0, sig_w2 = 1.168;
+        const double bet1 = 0.0333, bet2 = 0.0368, gam1 = 0.413, gam2 = 0.2;
+        const double nue_air_nd = nue_gas_phys / (P->u_0 * L_m);
+        const double CD_kw = dmax(2.0 * sig_w2 / dis_s * grad_dot, 1.0e-20);
+        const double arg1 = dmin(
+            dmax(sqrt(dmax(tke_c, 0.0)) / (bet_star * dis_s * y_star),
+                 500.0 * nue_air_nd / (y_star * y_star * dis_s)),
+            4.0 * sig_w2 * tke_s / (CD_kw * y_star * y_star));
+        const double F1 = tanh(pow(arg1, 4));
+        const double sig_k = F1 * sig_k1 + (1.0 - F1) * sig_k2;
+        const double sig_w = F1 * sig_w1 + (1.0 - F1) * sig_w2;
+        diffusion_tke_re = 1.0 / P->re + nue_here / sig_k;
+        diffusion_dis_re = 1.0 / P->re + nue_here / sig_w;
+        const double P_k = dmin(P_full, 20.0 * bet_star * tke_s * dis_s);
+        const double Y_k = bet_star * tke_s * dis_s;
+        const double P_w = (F1 * gam1 + (1.0 - F1) * gam2) * P_k * dis_s / tke_s;
+        const double Y_w = (F1 * bet1 + (1.0 - F1) * bet2) * dis_s * dis_s;
+        const double D_w = 2.0 * (1.0 - F1) * sig_w2 / dis_s * grad_dot;
+        tke_src = P_k - Y_k;
+        dis_src = P_w - Y_w + D_w;
+        c_w_prod = F1 * gam1 + (1.0 - F1) * gam2;
+    }
+    if (PH->turb_buoy) {                                      /* ATJUP_TURB_BUOY (963-981) */
+        const int ip = (i + 1 < im - 1) ? i + 1 : im - 1, imn = (i - 1 > 0) ? i - 1 : 0;
+        const double dz_m = (layer_h(X, im, ip) - layer_h(X, im, imn)) * 1.0e3;
+        const double T_K = dmax(S->t[c] * P->t_ref, 1.0);
+        const double dTdz = (S->t[IDX(ip, j, k)] - S->t[IDX(imn, j, k)]) * P->t_ref / dmax(dz_m, 1.0);
+        const double N2 = P->g / T_K * (dTdz + P->g / P->cp_mix);
+        const double tscale = L_m / P->u_0;
+        const double G_b = -(cnue / PH->turb_buoy_prt) * N2 * tscale * tscale;
+        if (isfinite(G_b)) {
+            tke_src += G_b;
+            dis_src += c_w_prod * dis_s / tke_s * dmax(G_b, 0.0);
+        }
+    }
+    const double tke_src_max = 20.0 * tke_s * dis_s;
+    const double dis_src_max = 20.0 * dis_s * dis_s;
+    if (!isfinite(tke_src)) tke_src = 0.0;
+    if (!isfinite(dis_src)) dis_src = 0.0;
+    tke_src = dmax(-tke_src_max, dmin(tke_src_max, tke_src));
+    dis_src = dmax(-dis_src_max, dmin(dis_src_max, dis_src));
+    X->tke_source[c] = tke_src;
+    X->dis_source[c] = dis_src;
+    X->rhs_tke[c] = -transport_tke + diffusion_tke * diffusion_tke_re + tke_src;
+    X->rhs_dis[c] = -transport_dis + diffusion_dis * diffusion_dis_re + dis_src;
+}
+
+/* The bit pattern test of RungeKutta_Jup_Turb.cpp:273-278: NaN or +-Inf -> lo. */
+static double safe_clamp(double v, double lo, double hi) {
+    uint64_t bits;
+    memcpy(&bits, &v, sizeof bits);
+    if ((bits & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL) return lo;
+    return (v < lo) ? lo : ((v > hi) ? hi : v);
+}
+
+/* RungeKutta_Jup_Turb.cpp:261-583 with every transported field. */
+void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,
+                  ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    ora_buoy_ref_level(P, G, S);
+    ora_hydrostatic(P, G, S);
+    const double dt = P->dt;
+    const double tke_max_nd = PH->tke_max_phys / (P->u_0 * P->u_0);
+    const double dis_min_nd = 1.0e-10;
+    for (int stage = 0; stage < 4; stage++) {
+        const double c_in = (stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0);
+        const double wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+        for (int i = 1; i < im - 1; i++)
+            for (int j = 3; j < jm - 3; j++)
+                for (int k = 0; k < km - 1; k++) {
+                    if (G->solid[IDX(i, j, k)]) continue;
+                    ora_rhs_cell(P, G, S, i, j, k);
+                    ora_rhs_phys_cell(P, PH, G, S, X, i, j, k);
+                }
+        for (int i = 1; i < im - 1; i++)
+            for (int j = 3; j < jm - 3; j++)
+                for (int k = 0; k < km - 1; k++) {
+                    const size_t c = IDX(i, j, k);
+                    if (G->solid[c]) continue;
+                    S->acc_t[c] = (stage == 0) ? wgt * S->rhs_t[c] : S->acc_t[c] + wgt * S->rhs_t[c];
+                    S->acc_u[c] = (stage == 0) ? wgt * S->rhs_u[c] : S->acc_u[c] + wgt * S->rhs_u[c];
+                    S->acc_v[c] = (stage == 0) ? wgt * S->rhs_v[c] : S->acc_v[c] + wgt * S->rhs_v[c];
+                    S->acc_w[c] = (stage == 0) ? wgt * S->rhs_w[c] : S->acc_w[c] + wgt * S->rhs_w[c];
+                    for (int s = 0; s < ATJUP_S_COUNT; s++)
+                        X->acc_q[s][c] = (stage == 0) ? wgt * X->rhs_q[s][c]
+                                                      : X->acc_q[s][c] + wgt * X->rhs_q[s][c];
+                    X->acc_tke[c] = (stage == 0) ? wgt * X->rhs_tke[c] : X->acc_tke[c] + wgt * X->rhs_tke[c];
+                    X->acc_dis[c] = (stage == 0) ? wgt * X->rhs_dis[c] : X->acc_dis[c] + wgt * X->rhs_dis[c];
+                    if (stage < 3) {
+                        S->t[c] = S->tn[c] + c_in * S->rhs_t[c];
+                        S->u[c] = S->un[c] + c_in * S->rhs_u[c];
+                        S->v[c] = S->vn[c] + c_in * S->rhs_v[c];
+                        S->w[c] = S->wn[c] + c_in * S->rhs_w[c];
+                        for (int s = 0; s < ATJUP_S_COUNT; s++)
+                            X->q[s][c] = X->qn[s][c] + c_in * X->rhs_q[s][c];
+                        X->tke[c] = safe_clamp(X->tken[c] + c_in * X->rhs_tke[c], 0.0, tke_max_nd);
+                        X->dis[c] = dmax(dis_min_nd, X->disn[c] + c_in * X->rhs_dis[c]);
+                    }
+                }
+    }
+    const double one_sixth = 1.0 / 6.0;
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 3; j < jm - 3; j++)
+            for (int k = 0; k < km - 1; k++) {
+                const size_t c = IDX(i, j, k);
+                if (G->solid[c]) continue;
+                S->t[c] = S->tn[c] + dt * S->acc_t[c] * one_sixth;
+                S->u[c] = S->un[c] + dt * S->acc_u[c] * one_sixth;
+                S->v[c] = S->vn[c] + dt * S->acc_v[c] * one_sixth;
+                S->w[c] = S->wn[c] + dt * S->acc_w[c] * one_sixth;
+                for (int s = 0; s < ATJUP_S_COUNT; s++) {
+                    const double q = X->qn[s][c] + dt * X->acc_q[s][c] * one_sixth;
+                    /* std::max(0.0, q), except NH4SH's explicit `if (q < 0) q = 0` (547-549),
+                     * which keeps a NaN and a -0 */
+                    X->q[s][c] = (s == ATJUP_S_NH4SH) ? (q < 0.0 ? 0.0 : q) : dmax(0.0, q);
+                }
+                X->tke[c] = safe_clamp(X->tken[c] + dt * X->acc_tke[c] * one_sixth, 0.0, tke_max_nd);
+                X->dis[c] = dmax(dis_min_nd, X->disn[c] + dt * X->acc_dis[c] * one_sixth);
+            }
+}

@@ -46,6 +46,19 @@ typedef struct {
     double *buoy_ref;                   /* [im]                                               */
 } ora_state;
 
+/* The full-physics fields of the RK4 step: the 11 species in ATJUP_S_* order and k*, omega*
+ * (live, time-level n, accumulator, right-hand side), their frozen sources, the closure's
+ * outputs and inputs. */
+typedef struct {
+    double *q[ATJUP_S_COUNT], *qn[ATJUP_S_COUNT], *acc_q[ATJUP_S_COUNT], *rhs_q[ATJUP_S_COUNT];
+    double *tke, *dis, *tken, *disn, *acc_tke, *acc_dis, *rhs_tke, *rhs_dis;
+    const double* s_precip[9];   /* h2o, h2o_cloud, h2o_ice, nh3, .., ch4_ice                  */
+    const double *massflux_h2s, *massflux_nh3, *massflux_nh4sh, *fluxlim_nh4sh;
+    double *prod, *tke_source, *dis_source;
+    const double* vel_star;      /* [jm*km], k-epsilon only                                    */
+    const float* layer_heights;  /* [im] km                                                     */
+} ora_phys;
+
 /* RungeKutta_Jup_Turb.cpp:47-69 */
 void ora_buoy_ref_level(const AtjupParams* P, const ora_grid* G, ora_state* S);
 /* RungeKutta_Jup_Turb.cpp:119-259 (metric/Coriolis split branch and the plain branch) */
@@ -54,6 +67,12 @@ void ora_hydrostatic(const AtjupParams* P, const ora_grid* G, ora_state* S);
 void ora_rhs_cell(const AtjupParams* P, const ora_grid* G, ora_state* S, int i, int j, int k);
 /* RungeKutta_Jup_Turb.cpp:261-583 for t, u, v, w */
 void ora_rk4(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* RHS_Jup_Turb.cpp species and closure part for one cell (after ora_rhs_cell's dynamics) */
+void ora_rhs_phys_cell(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G,
+                       ora_state* S, ora_phys* X, int i, int j, int k);
+/* RungeKutta_Jup_Turb.cpp:261-583 with the species and k*, omega* */
+void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,
+                  ora_phys* X);
 /* cJupiterModel.cpp:1842-1864 */
 void ora_prepare_projection(const AtjupParams* P, const ora_grid* G, ora_state* S);
 /* PressureSolver.h:144-766, pointwise red-black branch, `sweeps` sweeps with relaxation omega

@@ -443,7 +443,15 @@ int ref_knob(const char* name) {
     if (n == "phi_periodic") return ATPhys::phi_periodic<cJupiterModel>() ? 1 : 0;
     if (n == "nh4sh_eq") return ChemistryJup::nh4sh_eq() ? 1 : 0;
     if (n == "local_rho") return cJupiterModel::local_rho() ? 1 : 0;
-    (void)m;
+    if (n == "turb_model") {   // TurbulenceJup's parse: k_epsilon 0, k_omega 1, anything else SST 2
+        const char* e = getenv("ATJUP_TURB_MODEL");
+        const std::string t = e ? std::string(e) : m.turb_model;
+        return t == "k_epsilon" ? 0 : (t == "k_omega" ? 1 : 2);
+    }
+    if (n == "turb_buoy") { const char* e = getenv("ATJUP_TURB_BUOY"); return e ? atoi(e) : 0; }
+    if (n == "nh4sh_cap") { const char* e = getenv("ATJUP_NH4SH_CAP"); return e ? atoi(e) : 0; }
+    if (n == "t_limiter") { const char* e = getenv("ATJUP_T_LIMITER"); return e ? atoi(e) : 0; }
+    if (n == "rk_scalar_sync") { const char* e = getenv("ATJUP_RK_SCALAR_SYNC"); return e ? atoi(e) : 2; }
     return -999;
 }
 double ref_knob_d(const char* name) {
@@ -451,6 +459,10 @@ double ref_knob_d(const char* name) {
     const std::string n(name);
     (void)m;
     if (n == "shapiro_strength") return k_shapiro_strength();
+    if (n == "nue_max_phys") return TurbulenceJup::nue_max_phys();
+    if (n == "tke_max") { const char* e = getenv("ATJUP_TKE_MAX"); return e ? atof(e) : 1000.0; }
+    if (n == "turb_buoy_prt") { const char* e = getenv("ATJUP_TURB_BUOY_PRT"); return e ? atof(e) : 0.9; }
+    if (n == "species_divu") { const char* e = getenv("ATJUP_SPECIES_DIVU"); return e ? atof(e) : 0.0; }
     return std::nan("");
 }
 

@@ -24,6 +24,9 @@ DRY_ENV = {
     "ATJUP_RESTART_STRIDE": "0", "ATJUP_VTK_STRIDE": "100000", "ATJUP_PANORAMA_STRIDE": "100000",
 }
 
+# Full physics in the RK step: the dry knobs with the k_omega_SST closure switched on.
+PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1"}
+
 DYN_FIELDS = ["t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wall_nue",
               "aux_u", "aux_v", "aux_w"]
 
@@ -228,3 +231,67 @@ def oracle_satadj(params: AtjupParams, grid: dict, gas, t, p_stat, rho_mix, c, c
     lib.ora_satadj(ctypes.byref(params), ctypes.byref(G), ctypes.byref(gas), _dp(t), _dp(p_stat),
                    _dp(rho_mix), _dp(c), _dp(cloud), _dp(ice), counts)
     return tuple(counts)
+
+
+class OraPhys(ctypes.Structure):
+    _D = _P(ctypes.c_double)
+    _fields_ = [("q", _D * 11), ("qn", _D * 11), ("acc_q", _D * 11), ("rhs_q", _D * 11),
+                ("tke", _D), ("dis", _D), ("tken", _D), ("disn", _D), ("acc_tke", _D),
+                ("acc_dis", _D), ("rhs_tke", _D), ("rhs_dis", _D), ("s_precip", _D * 9),
+                ("massflux_h2s", _D), ("massflux_nh3", _D), ("massflux_nh4sh", _D),
+                ("fluxlim_nh4sh", _D), ("prod", _D), ("tke_source", _D), ("dis_source", _D),
+                ("vel_star", _D), ("layer_heights", _P(ctypes.c_float))]
+
+
+def oracle_rk4_phys(params, phys, grid: dict, fields: dict) -> dict:
+    """ora_rk4_phys on copies of fields (dynamics as for Oracle, plus the species, k*, omega*,
+    their *n copies, the sources, nue, vel_star [jm, km] and layer_heights [im] float32).
+    Returns every field after the step."""
+    from atjup_b200.params import S_PRECIP, SCALARS, SPECIES
+    o = Oracle(params, grid, fields)
+    shape = o.shape
+    keep = {}
+
+    def arr(name, default_zero=True):
+        if name in fields and fields[name] is not None:
+            a = np.ascontiguousarray(fields[name], dtype=np.float64).reshape(shape).copy()
+        else:
+            a = np.zeros(shape)
+        keep[name] = a
+        return a
+
+    for n in SCALARS:
+        arr(n)
+        keep[n + "n"] = np.ascontiguousarray(fields.get(n + "n", fields[n]), dtype=np.float64).reshape(shape).copy()
+        keep["acc_" + n] = np.zeros(shape)
+        keep["rhs_" + n] = np.zeros(shape)
+    for n in S_PRECIP + ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh"):
+        arr(n)
+    for n in ("prod", "tke_source", "dis_source"):
+        arr(n)       # cells the step does not visit keep their values
+    vs = np.ascontiguousarray(fields.get("vel_star", np.zeros(shape[1:])), dtype=np.float64).reshape(shape[1:]).copy()
+    lh = np.ascontiguousarray(fields["layer_heights"], dtype=np.float32).copy()
+    keep["vel_star"], keep["layer_heights"] = vs, lh
+    D = _P(ctypes.c_double)
+    X = OraPhys()
+    for s_, n in enumerate(SPECIES):
+        X.q[s_] = _dp(keep[n])
+        X.qn[s_] = _dp(keep[n + "n"])
+        X.acc_q[s_] = _dp(keep["acc_" + n])
+        X.rhs_q[s_] = _dp(keep["rhs_" + n])
+    for a in ("tke", "dis"):
+        setattr(X, a, _dp(keep[a]))
+        setattr(X, a + "n", _dp(keep[a + "n"]))
+        setattr(X, "acc_" + a, _dp(keep["acc_" + a]))
+        setattr(X, "rhs_" + a, _dp(keep["rhs_" + a]))
+    for s_, n in enumerate(S_PRECIP):
+        X.s_precip[s_] = _dp(keep[n])
+    for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "prod",
+              "tke_source", "dis_source", "vel_star"):
+        setattr(X, n, _dp(keep[n]))
+    X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    o.lib.ora_rk4_phys(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(o.G),
+                       ctypes.byref(o.S), ctypes.byref(X))
+    out = {n: o.f[n] for n in ("t", "u", "v", "w", "p_hydro", "aux_u", "aux_v", "aux_w", "buoy_ref")}
+    out.update({n: keep[n] for n in SCALARS + ("prod", "tke_source", "dis_source")})
+    return out

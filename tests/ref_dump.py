@@ -24,7 +24,7 @@ import numpy as np
 sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 
-from oracle_bridge import DRY_ENV, DYN_FIELDS, Reference  # noqa: E402
+from oracle_bridge import DRY_ENV, DYN_FIELDS, PHYS_ENV, Reference  # noqa: E402
 
 SPECIES = ("h2o", "h2o_cloud", "h2o_ice", "nh3", "nh3_cloud", "nh3_ice",
            "ch4", "ch4_cloud", "ch4_ice")
@@ -55,6 +55,56 @@ def perturb_moist(f: dict, solid: np.ndarray, seed: int = SATADJ_SEED) -> dict:
     return out
 
 
+PHYS_FIELDS = ("h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3", "nh3_cloud", "nh3_ice", "ch4",
+               "ch4_cloud", "ch4_ice", "nh4sh", "tke", "dis")
+PHYS_SOURCES = ("S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+                "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4", "S_precip_ch4_cloud",
+                "S_precip_ch4_ice", "massflux_h2s", "massflux_nh3", "massflux_nh4sh",
+                "fluxlim_nh4sh", "Q_rad", "Q_precip")
+
+
+def rk4_phys_case(ref, g, data, seed=SATADJ_SEED + 1):
+    """One RungeKuttaJup with every transported field, on the moist initial state with the
+    closure on (k_omega_SST): the live k*, omega* and species differ from their time-level-n
+    copies by seeded noise (as after the closure's wall passes), the frozen sources are seeded
+    fields of realistic size, and so are nue and the heating rates."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    shape = ref.shape
+    fluid = g["solid"] == 0
+    for n in PHYS_FIELDS:
+        live = ref.get(n)
+        data["in_" + n + "n"] = live.copy()
+        ref.set(n + "n", live)
+        if n in ("tke", "dis", "h2s", "nh4sh"):
+            live = np.where(fluid, live * rng.uniform(0.9, 1.1, shape), live)
+        ref.set(n, live)
+        data["in_" + n] = live
+    nue = np.where(fluid, np.abs(ref.get("nue")) + 1e-4 * rng.uniform(size=shape), 0.0)
+    ref.set("nue", nue)
+    data["in_nue"] = nue
+    for n in PHYS_SOURCES:
+        scale = {"Q_rad": 0.05, "Q_precip": 0.05}.get(n, 1e-4)
+        f = np.where(fluid, scale * rng.standard_normal(shape), 0.0)
+        ref.set(n, f)
+        data["in_" + n] = f
+    for n in ("prod", "tke_source", "dis_source"):
+        data["in_" + n] = ref.get(n)
+    data["in_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for k in ("turb_model", "turb_buoy", "nh4sh_cap", "t_limiter", "rk_scalar_sync"):
+        data["knob_" + k] = np.array(ref.L.ref_knob(k.encode()))
+    for k in ("nue_max_phys", "tke_max", "turb_buoy_prt", "species_divu"):
+        data["knobd_" + k] = np.array(ref.L.ref_knob_d(k.encode()))
+    for c in ("species_diff_scale", "sc_h2o", "sc_h2s", "sc_nh3", "sc_ch4", "sc_nh4sh",
+              "chemical_reaction", "r_p_nh4sh", "rg_nh4sh", "mue_mix", "re_turb",
+              "use_turbulence_model"):
+        data["phys_" + c] = np.array(ref.scalar(c))
+    ref.quiet(ref.L.ref_rk4)
+    for n in list(DYN_FIELDS) + list(PHYS_FIELDS) + ["prod", "tke_source", "dis_source"]:
+        data["out_" + n] = ref.get(n)
+    data["out_buoy_ref"] = ref.get1("buoy_ref_level")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -64,10 +114,16 @@ def main():
     ap.add_argument("--moist", action="store_true")
     ap.add_argument("--satadj", action="store_true")
     ap.add_argument("--satadj-synthetic", action="store_true")
+    ap.add_argument("--rk4-phys", action="store_true")
+    ap.add_argument("--env", action="append", default=[],
+                    help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
-    ref = Reference(dict(DRY_ENV), out_dir + "/run", threads=a.threads, zero_species=not (a.moist or a.satadj or a.satadj_synthetic))
+    env = dict(PHYS_ENV) if a.rk4_phys else dict(DRY_ENV)
+    env.update(dict(kv.split("=", 1) for kv in a.env))
+    ref = Reference(env, out_dir + "/run", threads=a.threads,
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -76,7 +132,9 @@ def main():
         data["in_" + n] = v
     for c in CONSTS:
         data["const_" + c] = np.array(ref.scalar(c))
-    if a.satadj or a.satadj_synthetic:
+    if a.rk4_phys:
+        rk4_phys_case(ref, g, data)
+    elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
         else:

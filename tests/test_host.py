@@ -105,3 +105,16 @@ def test_replica_timing_is_max_over_ranks():
         out = mgr.dict()
         mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
         assert out[0] == out[1] == (2.5, 2.5 / 20)
+
+
+def test_field_ids_match_the_header():
+    """The Python field ids (atjup_b200.params) are the header's enum, in order."""
+    src = (ROOT / "include" / "atjup_gpu.h").read_text()
+    body = src[src.index("ATJUP_F_T = 0"):src.index("ATJUP_F_COUNT")]
+    names = re.findall(r"ATJUP_F_(\w+)", body)
+    py = {v: k for k, v in P.FIELD_IDS.items()}
+    assert len(names) == len(P.FIELD_IDS)
+    for i, n in enumerate(names):
+        assert py[i].lower() == n.lower(), (i, n, py[i])
+    s_body = src[src.index("ATJUP_S_H2O = 0"):src.index("ATJUP_S_COUNT")]
+    assert [x.lower() for x in re.findall(r"ATJUP_S_(\w+)", s_body)] == list(P.SPECIES)
