@@ -452,7 +452,28 @@ int atjup_gpu_set_physics(AtjupCtx* c, const AtjupPhysics* ph, const float* laye
                           cudaMemcpyHostToDevice));
     c->phys = *ph;
     c->phys_on = (ph->species_on || ph->turb_on);
+    {
+        // clamp_nue's taper depth: the first level above abl_height and the one below it
+        auto hm = [&](int i) {
+            return ((i < 0 || i > P.im - 1) ? (double)(-1.0f) : (double)layer_heights_km[i]) * 1.0e3;
+        };
+        int i_abl = 0;
+        while (i_abl < P.im - 1 && hm(i_abl) <= ph->abl_height) i_abl++;
+        const double d = hm(std::min(i_abl, P.im - 1)) - hm(std::max(i_abl - 1, 0));
+        c->turb_taper_dz = (1.0 < d) ? d : 1.0;
+    }
     return ATJUP_OK;
+}
+
+int atjup_gpu_turbulence(AtjupCtx* c) {
+    int rc = need_grid(c, "turbulence");
+    if (rc) return rc;
+    if (!c->phys_on || !c->phys.turb_on) {
+        set_error("turbulence: the closure is off (atjup_gpu_set_physics with turb_on = 1 first)");
+        return ATJUP_ERR_ARG;
+    }
+    Timed tm(c, TK_PHYS);
+    return launch_turbulence(c);
 }
 
 namespace {

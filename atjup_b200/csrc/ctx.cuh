@@ -61,6 +61,7 @@ struct AtjupCtx {
     double* S2[ATJUP_S_COUNT + 2] = {};
     double* Sacc[ATJUP_S_COUNT + 2] = {};
     float* layer_h = nullptr;
+    double turb_taper_dz = 1.0;        // clamp_nue's taper depth (Turbulence.h:569-573) [m]
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
     double* X2[4] = {};
@@ -148,6 +149,7 @@ int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
 int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin);
+int launch_turbulence(AtjupCtx* c);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);
 

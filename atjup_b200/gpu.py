@@ -67,6 +67,7 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_download_n.argtypes = [vp, i32, vp]
     L.atjup_gpu_restore_scalars.argtypes = [vp]
     L.atjup_gpu_upload2d.argtypes = [vp, i32, vp]
+    L.atjup_gpu_turbulence.argtypes = [vp]
     L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
     _lib = L
     return L
@@ -164,6 +165,11 @@ class GpuModel:
         out = np.empty(self.shape)
         _check(self.L.atjup_gpu_download_n(self.ctx, _p.FIELD_IDS[name], _ptr(out)))
         return out
+
+    def turbulence(self) -> None:
+        """Turbulence<cJupiterModel>::run + turbWallOmega (Turbulence.h:307-882,
+        cJupiterModel.cpp:360-377)."""
+        _check(self.L.atjup_gpu_turbulence(self.ctx))
 
     def restore_scalars(self) -> None:
         _check(self.L.atjup_gpu_restore_scalars(self.ctx))

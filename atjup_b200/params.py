@@ -131,7 +131,9 @@ class AtjupPhysics(ctypes.Structure):
         (n, ctypes.c_double) for n in ("species_diff_scale", "sc_h2o", "sc_h2s", "sc_nh3",
                                        "sc_ch4", "sc_nh4sh", "chemical_reaction", "r_p_nh4sh",
                                        "rg_nh4sh", "mue_mix", "re_turb", "nue_max_phys",
-                                       "tke_max_phys", "turb_buoy_prt")]
+                                       "tke_max_phys", "turb_buoy_prt")] + [
+        (n, ctypes.c_int32) for n in ("turb_free", "turb_curv", "abl_taper", "turb_wall_omega")] + [
+        (n, ctypes.c_double) for n in ("turb_k_bg", "vel_star_max", "abl_height")]
 
 
 # cJupiterModel's constants of the species transport (cJupiterModel.h:290, 470-477, 594) and the
@@ -169,6 +171,13 @@ def resolve_physics(env: Mapping[str, str] | None = None, constants: Mapping[str
         setattr(ph, n, c[n])
     ph.tke_max_phys = _env(env, "ATJUP_TKE_MAX", 1000.0, float)
     ph.turb_buoy_prt = _env(env, "ATJUP_TURB_BUOY_PRT", 0.9, float)
+    ph.turb_free = _env(env, "ATJUP_TURB_FREE", 1)
+    ph.turb_curv = int(_env(env, "ATJUP_TURB_CURV", 1) != 0)
+    ph.abl_taper = int(_env(env, "ATJUP_ABL_TAPER", 0) != 0)
+    ph.turb_wall_omega = _env(env, "ATJUP_TURB_WALL_OMEGA", 1)
+    ph.turb_k_bg = _env(env, "ATJUP_TURB_K_BG", 1.0, float)
+    ph.vel_star_max = _env(env, "ATJUP_VEL_STAR_MAX", math.sqrt(0.002) * 200.0, float)
+    ph.abl_height = float((constants or {}).get("abl_height", 20000.0))
     return ph
 
 

@@ -244,6 +244,14 @@ typedef struct AtjupPhysics {
     double nue_max_phys;         /* ATJUP_NUE_MAX 1e5 m2/s (Turbulence.h:123)                     */
     double tke_max_phys;         /* ATJUP_TKE_MAX 1000 m2/s2 (RungeKutta_Jup_Turb.cpp:269)        */
     double turb_buoy_prt;        /* ATJUP_TURB_BUOY_PRT 0.9                                       */
+    /* the closure update between steps (Turbulence.h:307-882, atjup_gpu_turbulence)              */
+    int32_t turb_free;           /* ATJUP_TURB_FREE 1: no surface law, u_tau = 0.05 m/s           */
+    int32_t turb_curv;           /* ATJUP_TURB_CURV 1: curvature terms of the velocity gradient   */
+    int32_t abl_taper;           /* ATJUP_ABL_TAPER 0: taper nue above the boundary layer         */
+    int32_t turb_wall_omega;     /* ATJUP_TURB_WALL_OMEGA 1 (cJupiterModel.cpp:360-377)           */
+    double turb_k_bg;            /* ATJUP_TURB_K_BG 1 m2/s2: background k floor (TURB_FREE)       */
+    double vel_star_max;         /* ATJUP_VEL_STAR_MAX sqrt(0.002) 200 m/s                        */
+    double abl_height;           /* abl_height 20000 m (cJupiterModel.h:1534)                     */
 } AtjupPhysics;
 
 /* Switch the RK4 step to full physics: the 11 species and (turb_on) k*, omega* are integrated
@@ -256,6 +264,11 @@ int atjup_gpu_upload_n(AtjupCtx* ctx, int32_t field_id, const double* host);
 int atjup_gpu_download_n(AtjupCtx* ctx, int32_t field_id, double* host);
 /* restoreVar for the scalars (cJupiterModel.cpp:1757-1801): n copy <- live field. */
 int atjup_gpu_restore_scalars(AtjupCtx* ctx);
+/* Turbulence<cJupiterModel>::run (Turbulence.h:307-328: friction velocity, production and
+ * sources with the two clamp passes, wall law, obstacle zeroing, nue clamp, seam and lid copies)
+ * followed by the driver's turbWallOmega (cJupiterModel.cpp:360-377). Updates tke, dis, their
+ * time-level-n copies where the reference does, nue, prod, tke_source, dis_source, vel_star. */
+int atjup_gpu_turbulence(AtjupCtx* ctx);
 /* 2-D fields, contiguous (j, k). */
 int atjup_gpu_upload2d(AtjupCtx* ctx, int32_t field_id, const double* host);
 int atjup_gpu_download2d(AtjupCtx* ctx, int32_t field_id, double* host);

@@ -1502,3 +1502,336 @@ void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* 
                 X->dis[c] = dmax(dis_min_nd, X->disn[c] + dt * X->acc_dis[c] * one_sixth);
             }
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * The closure update between steps: Turbulence<cJupiterModel>::run (Turbulence.h:307-328) --
+ * compute_vel_star (336-360), compute_sources with the separate clamp passes (614-882) and the
+ * model routines (886-1106), apply_wall_bc (383-422), zero_land_cells (592-610), clamp_nue
+ * (565-588), seam_copy (543-559), fill_lid_corners (511-536) -- then the driver's turbWallOmega
+ * (cJupiterModel.cpp:360-377). ATJUP_TURB_CLAMP_PASS = 1 (the default) only.
+ * ------------------------------------------------------------------------------------------- */
+static double clamp3(double x, double lo, double hi) { return (x < lo) ? lo : ((x > hi) ? hi : x); }
+
+void ora_turbulence(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,
+                    ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const size_t N = (size_t)im * jm * km;
+    const uint8_t* sol = G->solid;
+    const double C_nue = 0.028, dis_min = 1.0e-10, nue_air = 1.8e-5;
+    const double L_m = P->L_atm * 1.0e3;
+    const double nue_max = PH->nue_max_phys / (P->u_0 * L_m);
+    const int model = PH->turb_model;
+    const double *U = S->u, *V = S->v, *W = S->w;
+    double *TK = X->tke, *DS = X->dis;
+#define HM(i_) (layer_h(X, im, (i_)) * 1.0e3)   /* height_m (Turbulence.h:263-265) */
+
+    /* compute_vel_star */
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            double* vs = &X->vel_star[(size_t)j * km + k];
+            if (PH->turb_free) { *vs = 0.05; continue; }
+            int is = G->topo[(size_t)j * km + k] + 1;
+            if (is > im - 1) is = im - 1;
+            const double v_s = V[IDX(is, j, k)], w_s = W[IDX(is, j, k)];
+            const double vw2 = v_s * v_s + w_s * w_s;
+            if (!isfinite(vw2)) { *vs = 0.05; continue; }
+            const double U_h = P->u_0 * sqrt(vw2);
+            *vs = clamp3(sqrt(0.002) * U_h, 0.05, PH->vel_star_max);
+        }
+
+    /* compute_sources: clamp-in pass */
+    for (int j = 1; j < jm - 1; j++)
+        for (int k = 0; k < km - 1; k++)
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                if (sol[c]) continue;
+                TK[c] = dmax(0.0, TK[c]);
+                DS[c] = dmax(dis_min, DS[c]);
+            }
+    /* sources per cell */
+    for (int j = 1; j < jm - 1; j++)
+        for (int k = 0; k < km - 1; k++) {
+            const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+            const double y_mount = HM(G->topo[(size_t)j * km + k]);
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                if (sol[c]) continue;
+                const size_t cip = IDX(i + 1, j, k), cim = IDX(i - 1, j, k);
+                const size_t cjp = IDX(i, j + 1, k), cjm = IDX(i, j - 1, k);
+                const size_t ckp = IDX(i, j, ke), ckm = IDX(i, j, kw);
+                const double rm = G->rad[i];
+                const double exp_rm = 1.0;
+                double sinthe = sin(G->the[j]);
+                if (sinthe == 0.0) sinthe = 1.0e-5;
+                const double costhe = cos(G->the[j]);
+                const double cotanthe = costhe / sinthe;
+                const double inv_rm = 1.0 / rm;
+                const double rmsinthe = rm * sinthe;
+                const double inv_2dr = 1.0 / (2.0 * P->dr);
+                const double inv_2dthe = 1.0 / (2.0 * P->dthe);
+                const double inv_2dphi = 1.0 / (2.0 * P->dphi);
+                const double inv_rm2dthe = inv_2dthe / rm;
+                const double inv_rmsinthe2dphi = inv_2dphi / rmsinthe;
+
+                const double dudr = (U[cip] - U[cim]) * inv_2dr * exp_rm;
+                const double dvdr = (V[cip] - V[cim]) * inv_2dr * exp_rm;
+                const double dwdr = (W[cip] - W[cim]) * inv_2dr * exp_rm;
+                const double dudthe = (U[cjp] - U[cjm]) * inv_rm2dthe;
+                const double dvdthe = (V[cjp] - V[cjm]) * inv_rm2dthe;
+                const double dwdthe = (W[cjp] - W[cjm]) * inv_rm2dthe;
+                const double dudphi = (U[ckp] - U[ckm]) * inv_rmsinthe2dphi;
+                const double dvdphi = (V[ckp] - V[ckm]) * inv_rmsinthe2dphi;
+                const double dwdphi = (W[ckp] - W[ckm]) * inv_rmsinthe2dphi;
+
+                const int nb = sol[cim], njm = sol[cjm], njp = sol[cjp], nkm = sol[ckm], nkp = sol[ckp];
+                const double tk0 = TK[c], ds0 = DS[c];
+                const double tke_im1 = nb ? tk0 : TK[cim], dis_im1 = nb ? ds0 : DS[cim];
+                const double tke_jm1 = njm ? tk0 : TK[cjm], tke_jp1 = njp ? tk0 : TK[cjp];
+                const double dis_jm1 = njm ? ds0 : DS[cjm], dis_jp1 = njp ? ds0 : DS[cjp];
+                const double tke_km1 = nkm ? tk0 : TK[ckm], tke_kp1 = nkp ? tk0 : TK[ckp];
+                const double dis_km1 = nkm ? ds0 : DS[ckm], dis_kp1 = nkp ? ds0 : DS[ckp];
+                const double dtkedr = (TK[cip] - tke_im1) * inv_2dr * exp_rm;
+                const double ddisdr = (DS[cip] - dis_im1) * inv_2dr * exp_rm;
+                const double dtkedthe = (tke_jp1 - tke_jm1) * inv_rm2dthe;
+                const double ddisdthe = (dis_jp1 - dis_jm1) * inv_rm2dthe;
+                const double dtkedphi = (tke_kp1 - tke_km1) * inv_rmsinthe2dphi;
+                const double ddisdphi = (dis_kp1 - dis_km1) * inv_rmsinthe2dphi;
+                /* passed to the model routines, which form their own theta/phi differences */
+                (void)dtkedthe; (void)ddisdthe; (void)dtkedphi; (void)ddisdphi;
+
+                double cnue;
+                {
+                    const double dis_here = dmax(ds0, dis_min);
+                    const double tke_here = dmax(tk0, 0.0);
+                    cnue = (model == ATJUP_TURB_K_EPSILON) ? C_nue * tke_here * tke_here / dis_here
+                                                           : tke_here / dis_here;
+                    cnue = dmin(cnue, nue_max);
+                }
+                const int curv = PH->turb_curv;
+                const double u_r = curv ? U[c] * inv_rm : 0.0;
+                const double v_r = curv ? V[c] * inv_rm : 0.0;
+                const double w_r = curv ? W[c] * inv_rm : 0.0;
+                const double v_cot_r = v_r * cotanthe;
+                const double w_cot_r = w_r * cotanthe;
+                const double g_rr = dudr, g_rt = dudthe - v_r, g_rp = dudphi - w_r;
+                const double g_tr = dvdr, g_tt = dvdthe + u_r, g_tp = dvdphi - w_cot_r;
+                const double g_pr = dwdr, g_pt = dwdthe, g_pp = dwdphi + u_r + v_cot_r;
+                const double der = 0.66667 * (g_rr + g_tt + g_pp);
+                X->prod[c] = dmax(0.0,
+                      (cnue * (2.0 * g_rr - der) - 0.66667 * tk0) * g_rr
+                    + (cnue * (g_rt + g_tr)) * g_rt
+                    + (cnue * (g_rp + g_pr)) * g_rp
+                    + (cnue * (2.0 * g_tt - der) - 0.66667 * tk0) * g_tt
+                    + (cnue * (g_tr + g_rt)) * g_tr
+                    + (cnue * (g_tp + g_pt)) * g_tp
+                    + (cnue * (2.0 * g_pp - der) - 0.66667 * tk0) * g_pp
+                    + (cnue * (g_pr + g_rp)) * g_pr
+                    + (cnue * (g_pt + g_tp)) * g_pt);
+                const double W12 = g_rt - g_tr, W13 = g_rp - g_pr, W23 = g_tp - g_pt;
+                const double Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
+
+                if (model == ATJUP_TURB_K_EPSILON) {                      /* 886-927 */
+                    const double C_eps_1 = 1.35, C_eps_2 = 1.80;
+                    const double y_phys = PH->turb_free ? 1.0e20 : dmax(HM(i) - y_mount, L_m);
+                    const double y_star = y_phys / L_m;
+                    X->nue_out[c] = C_nue * tk0 * tk0 / dmax(ds0, dis_min);
+                    const double d_plus = y_phys * X->vel_star[(size_t)j * km + k] / nue_air;
+                    const double f_nue = 1.0 - exp(-0.0115 * d_plus);
+                    const double Re_T = tk0 * tk0 * P->u_0 * L_m / dmax(ds0 * nue_air, dis_min * nue_air);
+                    const double f_2 = 1.0 - 0.4 / 1.8 * exp(-Re_T * Re_T / 36.0);
+                    X->nue_out[c] *= f_nue;
+                    const double y_star2 = y_star * y_star;
+                    const double L_k = -2.0 * tk0 / y_star2;
+                    const double L_w = -2.0 * ds0 / y_star2 * exp(-d_plus / 2.0);
+                    const double P_k = X->prod[c];
+                    const double Y_k = ds0;
+                    const double tke_safe = dmax(tk0, dis_min);
+                    const double P_w = C_eps_1 * ds0 / tke_safe * P_k;
+                    const double Y_w = C_eps_2 * f_2 * ds0 * ds0 / tke_safe;
+                    X->tke_source[c] = P_k - Y_k + L_k / PH->re_turb;
+                    X->dis_source[c] = P_w - Y_w + L_w / PH->re_turb;
+                } else if (model == ATJUP_TURB_K_OMEGA) {                 /* 930-1017 */
+                    const double bet_star = 0.09, gam = 0.52, C_lim = 0.875, bet_0 = 0.0708;
+                    const double exp_rm_k = 1.0 / (rm + 1.0);
+                    const double dtkedr_neu = nb ? (TK[cip] - tk0) * (1.0 / (2.0 * P->dr)) * exp_rm_k : dtkedr;
+                    const double ddisdr_neu = nb ? (DS[cip] - ds0) * (1.0 / (2.0 * P->dr)) * exp_rm_k : ddisdr;
+                    const double dtkedthe_neu = (tke_jp1 - tke_jm1) / (rm * 2.0 * P->dthe);
+                    const double ddisdthe_neu = (dis_jp1 - dis_jm1) / (rm * 2.0 * P->dthe);
+                    const double dtkedphi_neu = (tke_kp1 - tke_km1) / (rmsinthe * 2.0 * P->dphi);
+                    const double ddisdphi_neu = (dis_kp1 - dis_km1) / (rmsinthe * 2.0 * P->dphi);
+                    const double dudr_k = (U[cip] - U[cim]) / (2.0 * P->dr) / (rm + 1.0);
+                    const double dvdthe_k = (V[cjp] - V[cjm]) / (rm * 2.0 * P->dthe);
+                    const double dwdphi_k = (W[ckp] - W[ckm]) / (rmsinthe * 2.0 * P->dphi);
+                    const double dudthe_u = (U[cjp] - U[cjm]) / (rm * 2.0 * P->dthe);
+                    const double dudphi_u = (U[ckp] - U[ckm]) / (rmsinthe * 2.0 * P->dphi);
+                    const double dvdr_u = (V[cip] - V[cim]) / (2.0 * P->dr) / (rm + 1.0);
+                    const double dwdr_u = (W[cip] - W[cim]) / (2.0 * P->dr) / (rm + 1.0);
+                    const double dvdphi_u = (V[ckp] - V[ckm]) / (rmsinthe * 2.0 * P->dphi);
+                    const double dwdthe_u = (W[cjp] - W[cjm]) / (rm * 2.0 * P->dthe);
+                    const double S11 = dudr_k, S22 = dvdthe_k, S33 = dwdphi_k;
+                    const double S12 = 0.5 * (dudthe_u + dvdr_u);
+                    const double S13 = 0.5 * (dudphi_u + dwdr_u);
+                    const double S23 = 0.5 * (dvdphi_u + dwdthe_u);
+                    const double S_mag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33
+                                                     + 2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
+                    const double w_hat = dmax(ds0, C_lim * S_mag / sqrt(bet_star));
+                    double sig_d = dtkedr_neu * ddisdr_neu + dtkedthe_neu * ddisdthe_neu + dtkedphi_neu * ddisdphi_neu;
+                    sig_d = (sig_d <= 0.0) ? 0.0 : 0.125;
+                    const double chi_w = fabs(Omega * Omega * S_mag / pow(bet_star * dmax(ds0, 1.0e-20), 3));
+                    const double f_bet = (1.0 + 85.0 * chi_w) / (1.0 + 100.0 * chi_w);
+                    const double bet_wc = bet_0 * f_bet;
+                    X->nue_out[c] = tk0 / dmax(w_hat, 1.0e-20);
+                    const double P_k = dmin(X->prod[c], 20.0 * bet_star * tk0 * ds0);
+                    const double Y_k = bet_star * tk0 * ds0;
+                    const double P_w = gam * ds0 / dmax(tk0, 1.0e-20) * P_k;
+                    const double Y_w = bet_wc * ds0 * ds0;
+                    const double D_w = sig_d / dmax(ds0, 1.0e-20)
+                        * (dtkedr_neu * ddisdr_neu + dtkedthe_neu * ddisdthe_neu + dtkedphi_neu * ddisdphi_neu);
+                    X->tke_source[c] = P_k - Y_k;
+                    X->dis_source[c] = P_w - Y_w + D_w;
+                } else {                                                  /* 1021-1106 */
+                    const double a1 = 0.31, bet_star = 0.09, bet1 = 0.0333, bet2 = 0.0368;
+                    const double gam1 = 0.413, gam2 = 0.2, sig_w2 = 1.168;
+                    const double nue_air_nd = nue_air / (P->u_0 * L_m);
+                    const double dz_layer = dmax(1.0, layer_dz_m(X, im, i - 1 > 0 ? i - 1 : 0));
+                    const double y_phys = PH->turb_free ? 1.0e20 : dmax(HM(i) - y_mount, dz_layer);
+                    const double y_star = y_phys / L_m;
+                    const double exp_rm_k = 1.0 / (rm + 1.0);
+                    const double dtkedr_neu = nb ? (TK[cip] - tk0) * (1.0 / (2.0 * P->dr)) * exp_rm_k : dtkedr;
+                    const double ddisdr_neu = nb ? (DS[cip] - ds0) * (1.0 / (2.0 * P->dr)) * exp_rm_k : ddisdr;
+                    const double dtkedthe_neu = (tke_jp1 - tke_jm1) / (rm * 2.0 * P->dthe);
+                    const double ddisdthe_neu = (dis_jp1 - dis_jm1) / (rm * 2.0 * P->dthe);
+                    const double dtkedphi_neu = (tke_kp1 - tke_km1) / (rmsinthe * 2.0 * P->dphi);
+                    const double ddisdphi_neu = (dis_kp1 - dis_km1) / (rmsinthe * 2.0 * P->dphi);
+                    const double grad_dot = dtkedr_neu * ddisdr_neu + dtkedthe_neu * ddisdthe_neu
+                                          + dtkedphi_neu * ddisdphi_neu;
+                    const double CD_kw = dmax(2.0 * sig_w2 / dmax(ds0, 1.0e-20) * grad_dot, 1.0e-20);
+                    const double dis_safe = dmax(ds0, 1.0e-20);
+                    const double arg1 = dmin(
+                        dmax(sqrt(tk0) / (bet_star * dis_safe * y_star),
+                             500.0 * nue_air_nd / (y_star * y_star * dis_safe)),
+                        4.0 * sig_w2 * tk0 / (CD_kw * y_star * y_star));
+                    const double arg2 = dmax(
+                        2.0 * sqrt(tk0) / (bet_star * dis_safe * y_star),
+                        500.0 * nue_air_nd / (y_star * y_star * dis_safe));
+                    const double F1 = tanh(pow(arg1, 4));
+                    const double F2 = tanh(pow(arg2, 2));
+                    X->nue_out[c] = a1 * tk0 / dmax(a1 * dis_safe, Omega * F2);
+                    const double tke_safe = dmax(tk0, 1.0e-20);
+                    const double P_k = dmin(X->prod[c], 20.0 * bet_star * tke_safe * dis_safe);
+                    const double Y_k = bet_star * tke_safe * dis_safe;
+                    const double P_w = (F1 * gam1 + (1.0 - F1) * gam2) * P_k * dis_safe / tke_safe;
+                    const double Y_w = (F1 * bet1 + (1.0 - F1) * bet2) * dis_safe * dis_safe;
+                    const double D_w = 2.0 * (1.0 - F1) * sig_w2 / dis_safe * grad_dot;
+                    X->tke_source[c] = P_k - Y_k;
+                    X->dis_source[c] = P_w - Y_w + D_w;
+                }
+                if (PH->turb_buoy != 0) {                                 /* 843-867, buoy 1 or 2 */
+                    const double Pr_t = 0.9;
+                    const double T = S->t[c] * P->t_ref;
+                    const double dz = HM(i + 1) - HM(i - 1);
+                    const double dTdz = (S->t[cip] - S->t[cim]) * P->t_ref / dz;
+                    const double Gam = P->g / P->cp_mix, fac = 1.0;
+                    const double N2 = (T > 0.0 && dz > 0.0) ? P->g / T * (dTdz + Gam) * fac : 0.0;
+                    if (isfinite(N2) && (N2 > 0.0 || PH->turb_buoy == 2)) {
+                        const double tL = L_m / P->u_0;
+                        X->tke_source[c] -= dmax(0.0, X->nue_out[c]) * N2 * tL * tL / Pr_t;
+                    }
+                }
+            }
+        }
+    /* clamp-out pass */
+    for (int j = 1; j < jm - 1; j++)
+        for (int k = 0; k < km - 1; k++) {
+            const double vs = X->vel_star[(size_t)j * km + k];
+            const double k_bg_nd = PH->turb_free ? PH->turb_k_bg / (P->u_0 * P->u_0)
+                                 : 0.01 * vs * vs / (sqrt(C_nue) * P->u_0 * P->u_0);
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                if (sol[c]) continue;
+                TK[c] = dmax(k_bg_nd, TK[c]);
+                DS[c] = dmax(dis_min, DS[c]);
+                X->nue_out[c] = clamp3(X->nue_out[c], 0.0, nue_max);
+                const double dis_src_max = 20.0 * DS[c] * DS[c];
+                X->dis_source[c] = clamp3(X->dis_source[c], -dis_src_max, dis_src_max);
+                const double tke_src_max = 20.0 * TK[c] * DS[c];
+                X->tke_source[c] = clamp3(X->tke_source[c], -tke_src_max, tke_src_max);
+            }
+        }
+    /* apply_wall_bc */
+    const double nd_omega = L_m / P->u_0;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            const int i_w = G->topo[(size_t)j * km + k];
+            if (!PH->turb_free && i_w > 0 && i_w < im - 1) {
+                const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
+                const double vs = X->vel_star[(size_t)j * km + k];
+                const size_t cw = IDX(i_w, j, k);
+                TK[cw] = vs * vs / (sqrt(C_nue) * P->u_0 * P->u_0);
+                X->nue_out[cw] = 0.0;
+                if (model == ATJUP_TURB_K_EPSILON) DS[cw] = 0.0;
+                else if (model == ATJUP_TURB_K_OMEGA) DS[cw] = 6.0 * nue_air / (0.075 * y1 * y1) * nd_omega;
+                else DS[cw] = 60.0 * nue_air / (0.0333 * y1 * y1) * nd_omega;
+            } else {
+                TK[IDX(0, j, k)] = TK[IDX(1, j, k)];
+                DS[IDX(0, j, k)] = DS[IDX(1, j, k)];
+                X->nue_out[IDX(0, j, k)] = X->nue_out[IDX(1, j, k)];
+            }
+        }
+    /* zero_land_cells */
+    for (size_t c = 0; c < N; c++)
+        if (sol[c]) {
+            TK[c] = 0.0; X->tken[c] = 0.0; DS[c] = 0.0; X->disn[c] = 0.0;
+            X->nue_out[c] = 0.0; X->prod[c] = 0.0; X->tke_source[c] = 0.0; X->dis_source[c] = 0.0;
+        }
+    /* clamp_nue */
+    {
+        int i_abl = 0;
+        while (i_abl < im - 1 && HM(i_abl) <= PH->abl_height) i_abl++;
+        const double taper_dz = dmax(1.0, HM(i_abl < im - 1 ? i_abl : im - 1) - HM(i_abl - 1 > 0 ? i_abl - 1 : 0));
+        for (int i = 0; i < im; i++)
+            for (int j = 0; j < jm; j++)
+                for (int k = 0; k < km; k++) {
+                    double f = 1.0;
+                    if (PH->abl_taper) {
+                        const double z_agl = HM(i) - HM(G->topo[(size_t)j * km + k]);
+                        f = clamp3((PH->abl_height + taper_dz - z_agl) / taper_dz, 0.0, 1.0);
+                    }
+                    const size_t c = IDX(i, j, k);
+                    X->nue_out[c] = clamp3(X->nue_out[c], 0.0, nue_max) * f;
+                }
+    }
+    /* seam_copy */
+    double* eight[8] = {TK, DS, X->tken, X->disn, X->nue_out, X->prod, X->tke_source, X->dis_source};
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++)
+            for (int q = 0; q < 8; q++) eight[q][IDX(i, j, km - 1)] = eight[q][IDX(i, j, 0)];
+    /* fill_lid_corners (TURB_FREE, bc_turb_active() false on ATJUP) */
+    if (PH->turb_free) {
+        const int il = im - 1;
+        for (int j = 1; j < jm - 1; j++)
+            for (int k = 0; k < km; k++)
+                for (int q = 0; q < 8; q++) eight[q][IDX(il, j, k)] = eight[q][IDX(il - 1, j, k)];
+        for (int i = 0; i < im; i++)
+            for (int k = 0; k < km; k++)
+                for (int q = 0; q < 8; q++) {
+                    eight[q][IDX(i, 0, k)] = eight[q][IDX(i, 1, k)];
+                    eight[q][IDX(i, jm - 1, k)] = eight[q][IDX(i, jm - 2, k)];
+                }
+    }
+    /* turbWallOmega */
+    if (PH->turb_wall_omega != 0 && model != ATJUP_TURB_K_EPSILON) {
+        const double bet_star = 0.09, bet_1 = 0.0333, kappa = 0.41;
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++) {
+                const int i_w = G->topo[(size_t)j * km + k];
+                if (i_w <= 0 || i_w >= im - 1) continue;
+                const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
+                const double y = 0.5 * y1;
+                const double om_vis = 60.0 * nue_air / (bet_1 * y1 * y1);
+                const double om_log = X->vel_star[(size_t)j * km + k] / (sqrt(bet_star) * kappa * y);
+                DS[IDX(i_w, j, k)] = sqrt(om_vis * om_vis + om_log * om_log) * nd_omega;
+            }
+    }
+#undef HM
+}

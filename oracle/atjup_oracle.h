@@ -55,7 +55,8 @@ typedef struct {
     const double* s_precip[9];   /* h2o, h2o_cloud, h2o_ice, nh3, .., ch4_ice                  */
     const double *massflux_h2s, *massflux_nh3, *massflux_nh4sh, *fluxlim_nh4sh;
     double *prod, *tke_source, *dis_source;
-    const double* vel_star;      /* [jm*km], k-epsilon only                                    */
+    double* vel_star;            /* [jm*km] friction velocity (written by ora_turbulence)      */
+    double* nue_out;             /* the eddy viscosity ora_turbulence writes (the model's nue)  */
     const float* layer_heights;  /* [im] km                                                     */
 } ora_phys;
 
@@ -73,6 +74,10 @@ void ora_rhs_phys_cell(const AtjupParams* P, const AtjupPhysics* PH, const ora_g
 /* RungeKutta_Jup_Turb.cpp:261-583 with the species and k*, omega* */
 void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,
                   ora_phys* X);
+/* Turbulence<cJupiterModel>::run (Turbulence.h:307-882) + turbWallOmega (cJupiterModel.cpp:
+ * 360-377): reads u, v, w, t (S), tke/dis and their n copies, nue, vel_star (X); writes them. */
+void ora_turbulence(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,
+                    ora_phys* X);
 /* cJupiterModel.cpp:1842-1864 */
 void ora_prepare_projection(const AtjupParams* P, const ora_grid* G, ora_state* S);
 /* PressureSolver.h:144-766, pointwise red-black branch, `sweeps` sweeps with relaxation omega

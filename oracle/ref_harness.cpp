@@ -457,12 +457,15 @@ int ref_knob(const char* name) {
 double ref_knob_d(const char* name) {
     cJupiterModel& m = *g_m;
     const std::string n(name);
-    (void)m;
     if (n == "shapiro_strength") return k_shapiro_strength();
     if (n == "nue_max_phys") return TurbulenceJup::nue_max_phys();
     if (n == "tke_max") { const char* e = getenv("ATJUP_TKE_MAX"); return e ? atof(e) : 1000.0; }
     if (n == "turb_buoy_prt") { const char* e = getenv("ATJUP_TURB_BUOY_PRT"); return e ? atof(e) : 0.9; }
     if (n == "species_divu") { const char* e = getenv("ATJUP_SPECIES_DIVU"); return e ? atof(e) : 0.0; }
+    if (n == "abl_height") return m.abl_height;
+    if (n == "turb_free") return TurbulenceJup::turb_free();
+    if (n == "turb_k_bg") return TurbulenceJup::turb_k_bg();
+    if (n == "turb_clamp_pass") return TurbulenceJup::turb_clamp_pass();
     return std::nan("");
 }
 

@@ -240,7 +240,7 @@ class OraPhys(ctypes.Structure):
                 ("acc_dis", _D), ("rhs_tke", _D), ("rhs_dis", _D), ("s_precip", _D * 9),
                 ("massflux_h2s", _D), ("massflux_nh3", _D), ("massflux_nh4sh", _D),
                 ("fluxlim_nh4sh", _D), ("prod", _D), ("tke_source", _D), ("dis_source", _D),
-                ("vel_star", _D), ("layer_heights", _P(ctypes.c_float))]
+                ("vel_star", _D), ("nue_out", _D), ("layer_heights", _P(ctypes.c_float))]
 
 
 def oracle_rk4_phys(params, phys, grid: dict, fields: dict) -> dict:
@@ -290,8 +290,31 @@ def oracle_rk4_phys(params, phys, grid: dict, fields: dict) -> dict:
               "tke_source", "dis_source", "vel_star"):
         setattr(X, n, _dp(keep[n]))
     X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    X.nue_out = _dp(o.f["nue"]) if o.f.get("nue") is not None else None
     o.lib.ora_rk4_phys(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(o.G),
                        ctypes.byref(o.S), ctypes.byref(X))
     out = {n: o.f[n] for n in ("t", "u", "v", "w", "p_hydro", "aux_u", "aux_v", "aux_w", "buoy_ref")}
     out.update({n: keep[n] for n in SCALARS + ("prod", "tke_source", "dis_source")})
     return out
+
+
+def oracle_turbulence(params, phys, grid: dict, fields: dict) -> dict:
+    """ora_turbulence on copies of fields (u, v, w, t, tke, dis, tken, disn, nue, prod,
+    tke_source, dis_source, vel_star, layer_heights). Returns the fields it writes."""
+    o = Oracle(params, grid, fields)
+    shape = o.shape
+    keep = {}
+    for n in ("tke", "dis", "nue", "prod", "tke_source", "dis_source"):
+        keep[n] = np.ascontiguousarray(fields[n], dtype=np.float64).reshape(shape).copy()
+    for n in ("tke", "dis"):
+        keep[n + "n"] = np.ascontiguousarray(fields.get(n + "n", fields[n]), dtype=np.float64).reshape(shape).copy()
+    keep["vel_star"] = np.ascontiguousarray(fields["vel_star"], dtype=np.float64).reshape(shape[1:]).copy()
+    lh = np.ascontiguousarray(fields["layer_heights"], dtype=np.float32).copy()
+    X = OraPhys()
+    for n in ("tke", "dis", "tken", "disn", "prod", "tke_source", "dis_source", "vel_star"):
+        setattr(X, n, _dp(keep[n]))
+    X.nue_out = _dp(keep["nue"])
+    X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    o.lib.ora_turbulence(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(o.G),
+                         ctypes.byref(o.S), ctypes.byref(X))
+    return keep

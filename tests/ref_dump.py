@@ -105,6 +105,47 @@ def rk4_phys_case(ref, g, data, seed=SATADJ_SEED + 1):
     data["out_buoy_ref"] = ref.get1("buoy_ref_level")
 
 
+TURB_FIELDS = ("tke", "dis", "tken", "disn", "nue", "prod", "tke_source", "dis_source")
+
+
+def turb_case(ref, g, data, seed=SATADJ_SEED + 2):
+    """One TurbulenceJup::run + turbWallOmega on the moist initial state with the closure on:
+    the velocities carry seeded noise of 1 m/s (so the production term is exercised), k* and
+    omega* seeded noise of 10 % with some cells driven negative (the clamp passes), the n copies
+    are the restored live fields."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    shape = ref.shape
+    fluid = g["solid"] == 0
+    for n in ("u", "v", "w"):
+        f = ref.get(n)
+        f = np.where(fluid, f + 0.01 * rng.standard_normal(shape), f)
+        ref.set(n, f)
+        data["in_" + n] = f
+    for n in ("tke", "dis"):
+        f = ref.get(n)
+        f = np.where(fluid, f * rng.uniform(0.9, 1.1, shape), f)
+        neg = fluid & (rng.uniform(size=shape) < 0.01)
+        f = np.where(neg, -np.abs(f), f)
+        ref.set(n, f)
+        ref.set(n + "n", f)
+        data["in_" + n] = f
+        data["in_" + n + "n"] = f
+    for n in ("nue", "prod", "tke_source", "dis_source", "t"):
+        data["in_" + n] = ref.get(n)
+    data["in_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for k in ("turb_model", "turb_buoy"):
+        data["knob_" + k] = np.array(ref.L.ref_knob(k.encode()))
+    for k in ("nue_max_phys", "abl_height", "turb_free", "turb_k_bg", "turb_clamp_pass"):
+        data["knobd_" + k] = np.array(ref.L.ref_knob_d(k.encode()))
+    for c in ("re_turb", "mue_mix", "chemical_reaction"):
+        data["phys_" + c] = np.array(ref.scalar(c))
+    ref.quiet(ref.L.ref_turbulence)
+    for n in TURB_FIELDS:
+        data["out_" + n] = ref.get(n)
+    data["out_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -115,15 +156,16 @@ def main():
     ap.add_argument("--satadj", action="store_true")
     ap.add_argument("--satadj-synthetic", action="store_true")
     ap.add_argument("--rk4-phys", action="store_true")
+    ap.add_argument("--turb", action="store_true")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
-    env = dict(PHYS_ENV) if a.rk4_phys else dict(DRY_ENV)
+    env = dict(PHYS_ENV) if (a.rk4_phys or a.turb) else dict(DRY_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -134,6 +176,8 @@ def main():
         data["const_" + c] = np.array(ref.scalar(c))
     if a.rk4_phys:
         rk4_phys_case(ref, g, data)
+    elif a.turb:
+        turb_case(ref, g, data)
     elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
