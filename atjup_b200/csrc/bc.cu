@@ -1,4 +1,5 @@
-// Boundary passes of the dynamics fields after the RK step.
+// Boundary passes after the RK step, over the dynamics fields and, with the physics on, the
+// species, the chemistry mass fluxes and the closure fields.
 //
 // Reference: BC_Jup::bcRadius (BC_Jup.h:185-263) around BoundaryConditions<M>::bcRadius
 // (BoundaryConditions.h:151-250), bcTheta (253-336), bcPhi (339-360, periodic seam), and
@@ -31,7 +32,18 @@ __global__ void zonal_mean_kernel(const double* __restrict__ v, const double* __
     }
 }
 
-__global__ void radius_kernel(double* __restrict__ t, double* __restrict__ u,
+// A list of fields a pass treats alike (the reference's bc_fields_* lists, BC_Jup.h:275-350).
+struct FieldList {
+    double* f[32];
+    int n;
+};
+
+// One (j, k) column: 2-point Neumann at both radial walls for every listed field
+// (BoundaryConditions.h:176-193), the rigid lid u = 0, the top taper of v, w (taper 3: zonal-mean
+// preserving, BC_Jup.h:186-229), then the species wall copy at i = 0 and positivity at both
+// walls (BC_Jup.h:231-262). Each step is column-local, so doing them per column in the
+// reference's order equals the reference's sequence of whole-grid passes.
+__global__ void radius_kernel(FieldList L, FieldList Q, double* __restrict__ u,
                               double* __restrict__ v, double* __restrict__ w,
                               const double* __restrict__ zm, int im, int jm, int km, int KP,
                               int lid_u, int taper) {
@@ -39,10 +51,8 @@ __global__ void radius_kernel(double* __restrict__ t, double* __restrict__ u,
     const int j = blockIdx.y;
     if (k >= km) return;
     const size_t plane = (size_t)jm * KP, b = (size_t)j * KP + k;
-    double* F[4] = {t, u, v, w};
-#pragma unroll
-    for (int f = 0; f < 4; f++) {
-        double* x = F[f];
+    for (int f = 0; f < L.n; f++) {
+        double* x = L.f[f];
         x[b] = kC43 * x[b + plane] - kC13 * x[b + 2 * plane];
         x[b + (im - 1) * plane] = kC43 * x[b + (im - 2) * plane] - kC13 * x[b + (im - 3) * plane];
     }
@@ -76,13 +86,19 @@ __global__ void radius_kernel(double* __restrict__ t, double* __restrict__ u,
         v[c1] = v2;
         w[c1] = w2;
     }
+    for (int f = 0; f < Q.n; f++) {
+        double* x = Q.f[f];
+        double x0 = x[b + plane];                  // wall copy
+        if (x0 < 0.0) x0 = 0.0;                    // positivity
+        x[b] = x0;
+        if (x[c1] < 0.0) x[c1] = 0.0;
+    }
 }
 
-// Pole rows (BoundaryConditions.h:253-336): rows 1..nfill copy row nfill+1 for t, u and ramp
-// r/(nfill+1) of it for v, w; the pole row copies row 1 (t, u) and is zero (v, w).
-__global__ void theta_kernel(double* __restrict__ t, double* __restrict__ u,
-                             double* __restrict__ v, double* __restrict__ w, int im, int jm,
-                             int km, int KP, int nfill) {
+// Pole rows (BoundaryConditions.h:253-336): rows 1..nfill copy row nfill+1 for the extrapolated
+// list and ramp r/(nfill+1) of it for the zero list; the pole row copies row 1 (extrapolated
+// list) or is zero (zero list).
+__global__ void theta_kernel(FieldList X, FieldList Z, int im, int jm, int km, int KP, int nfill) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (k >= km) return;
@@ -92,56 +108,82 @@ __global__ void theta_kernel(double* __restrict__ t, double* __restrict__ u,
         const int jf = nfill + 1;
         for (int r = 1; r <= nfill; r++) {
             const double ramp = (double)r / (double)jf;
-            t[at(r)] = t[at(jf)];
-            t[at(jm - 1 - r)] = t[at(jm - 1 - jf)];
-            u[at(r)] = u[at(jf)];
-            u[at(jm - 1 - r)] = u[at(jm - 1 - jf)];
-            v[at(r)] = ramp * v[at(jf)];
-            v[at(jm - 1 - r)] = ramp * v[at(jm - 1 - jf)];
-            w[at(r)] = ramp * w[at(jf)];
-            w[at(jm - 1 - r)] = ramp * w[at(jm - 1 - jf)];
+            for (int f = 0; f < X.n; f++) {
+                double* x = X.f[f];
+                x[at(r)] = x[at(jf)];
+                x[at(jm - 1 - r)] = x[at(jm - 1 - jf)];
+            }
+            for (int f = 0; f < Z.n; f++) {
+                double* x = Z.f[f];
+                x[at(r)] = ramp * x[at(jf)];
+                x[at(jm - 1 - r)] = ramp * x[at(jm - 1 - jf)];
+            }
         }
     }
-    v[at(0)] = 0.0;
-    v[at(jm - 1)] = 0.0;
-    w[at(0)] = 0.0;
-    w[at(jm - 1)] = 0.0;
-    t[at(0)] = t[at(1)];
-    t[at(jm - 1)] = t[at(jm - 2)];
-    u[at(0)] = u[at(1)];
-    u[at(jm - 1)] = u[at(jm - 2)];
+    for (int f = 0; f < Z.n; f++) {
+        Z.f[f][at(0)] = 0.0;
+        Z.f[f][at(jm - 1)] = 0.0;
+    }
+    for (int f = 0; f < X.n; f++) {
+        double* x = X.f[f];
+        x[at(0)] = x[at(1)];
+        x[at(jm - 1)] = x[at(jm - 2)];
+    }
 }
 
-__global__ void phi_kernel(double* __restrict__ t, double* __restrict__ u,
-                           double* __restrict__ v, double* __restrict__ w, int jm, int km,
-                           int KP) {
+__global__ void phi_kernel(FieldList L, int jm, int km, int KP) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j >= jm) return;
     const size_t b = ((size_t)i * jm + j) * KP;
-    t[b + km - 1] = t[b];
-    u[b + km - 1] = u[b];
-    v[b + km - 1] = v[b];
-    w[b + km - 1] = w[b];
+    for (int f = 0; f < L.n; f++) L.f[f][b + km - 1] = L.f[f][b];
 }
 
-__global__ void solid_kernel(const SolidCell* __restrict__ L, int n, double* __restrict__ t,
+// Solid cells (BC_Jup.h:496-590): velocities 0; surface cells with an extrapolation pair take
+// the 2-point extrapolation of every listed scalar; the others set the list from index 2 (p_dyn)
+// on to 0, keeping t and p_stat.
+__global__ void solid_kernel(const SolidCell* __restrict__ Ls, int n, FieldList S,
                              double* __restrict__ u, double* __restrict__ v,
-                             double* __restrict__ w, double* __restrict__ ps,
-                             double* __restrict__ pd) {
+                             double* __restrict__ w) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
-    const SolidCell s = L[q];
+    const SolidCell s = Ls[q];
     u[s.c] = 0.0;
     v[s.c] = 0.0;
     w[s.c] = 0.0;
     if (s.kind == 1) {
-        t[s.c] = kC43 * t[s.a] - kC13 * t[s.b];
-        ps[s.c] = kC43 * ps[s.a] - kC13 * ps[s.b];
-        pd[s.c] = kC43 * pd[s.a] - kC13 * pd[s.b];
+        for (int f = 0; f < S.n; f++) S.f[f][s.c] = kC43 * S.f[f][s.a] - kC13 * S.f[f][s.b];
     } else {
-        pd[s.c] = 0.0;
+        for (int f = 2; f < S.n; f++) S.f[f][s.c] = 0.0;
     }
+}
+
+__device__ __forceinline__ double safe_clamp(double v, double lo, double hi) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    if ((b & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL) return lo;
+    return (v < lo) ? lo : ((v > hi) ? hi : v);
+}
+
+// The sanitising clamps of the closure fields over the whole grid (BC_Jup.h:627-655), with the
+// fixed bounds of that routine: k* in [0, 1000 m2/s2], omega* in [1e-10, 1e6], nue* in
+// [0, 1e5 m2/s], prod in [0, 1e4], sources in [-1e4, 1e4]; NaN and Inf go to the lower bound.
+struct SanArgs {
+    double *tke, *tken, *dis, *disn, *nue, *prod, *tsrc, *dsrc;
+    size_t n;
+    double tke_max, nue_max;
+};
+__global__ void sanitise_kernel(SanArgs a) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.n) return;
+    const double prod_max = 1.0e4, dis_max = 1.0e6;
+    a.tke[c] = safe_clamp(a.tke[c], 0.0, a.tke_max);
+    a.tken[c] = safe_clamp(a.tken[c], 0.0, a.tke_max);
+    a.dis[c] = safe_clamp(a.dis[c], 1.0e-10, dis_max);
+    a.disn[c] = safe_clamp(a.disn[c], 1.0e-10, dis_max);
+    a.nue[c] = safe_clamp(a.nue[c], 0.0, a.nue_max);
+    a.prod[c] = safe_clamp(a.prod[c], 0.0, prod_max);
+    a.tsrc[c] = safe_clamp(a.tsrc[c], -prod_max, prod_max);
+    a.dsrc[c] = safe_clamp(a.dsrc[c], -prod_max, prod_max);
 }
 
 // Ambient temperature of the solid cells of one (i, j) row: the mean of t over its fluid cells.
@@ -173,35 +215,73 @@ int launch_bc(AtjupCtx* c, int which) {
     double* u = c->f[ATJUP_F_U];
     double* v = c->f[ATJUP_F_V];
     double* w = c->f[ATJUP_F_W];
+    const bool ph = c->phys_on;
+    // the field lists of the passes (BC_Jup.h:275-350) over the fields the device holds
+    auto add = [](FieldList& L, double* x) { L.f[L.n++] = x; };
+    auto add_species = [&](FieldList& L) {
+        for (int s = 0; s < ATJUP_S_COUNT; s++) add(L, c->f[kScalarField[s]]);
+    };
+    auto add_turb = [&](FieldList& L) {
+        add(L, c->f[ATJUP_F_TKE]); add(L, c->f[ATJUP_F_DIS]); add(L, c->f[ATJUP_F_NUE]);
+        add(L, c->f[ATJUP_F_PROD]); add(L, c->f[ATJUP_F_TKE_SOURCE]); add(L, c->f[ATJUP_F_DIS_SOURCE]);
+    };
+    auto add_massflux = [&](FieldList& L, bool fluxlim) {
+        add(L, c->f[ATJUP_F_MASSFLUX_H2S]); add(L, c->f[ATJUP_F_MASSFLUX_NH3]);
+        add(L, c->f[ATJUP_F_MASSFLUX_NH4SH]);
+        if (fluxlim) add(L, c->f[ATJUP_F_FLUXLIM_NH4SH]);
+    };
     if (which & ATJUP_BC_RADIUS) {
+        FieldList L{}, Q{};
+        add(L, t); add(L, u); add(L, v); add(L, w);
+        if (ph) { add_species(L); add_massflux(L, false); add_turb(L); add_species(Q); }
         if (P.top_taper == 3) {
             c->launches++;
             zonal_mean_kernel<<<dim3(P.jm, 2), 32, 0, c->stream>>>(v, w, c->zm, P.im, P.jm, P.km, c->KP);
         }
         c->launches++;
         radius_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
-            t, u, v, w, c->zm, P.im, P.jm, P.km, c->KP, P.lid_u, P.top_taper);
+            L, Q, u, v, w, c->zm, P.im, P.jm, P.km, c->KP, P.lid_u, P.top_taper);
         ATJUP_CHECK_LAUNCH("bc_radius");
     }
     if (which & ATJUP_BC_THETA) {
+        FieldList X{}, Z{};
+        add(X, t); add(X, u);
+        add(Z, v); add(Z, w);
+        if (ph) { add_species(X); add_turb(X); add_massflux(Z, true); }
         c->launches++;
         theta_kernel<<<dim3((P.km + 127) / 128, P.im), 128, 0, c->stream>>>(
-            t, u, v, w, P.im, P.jm, P.km, c->KP, P.pole_fill_rows);
+            X, Z, P.im, P.jm, P.km, c->KP, P.pole_fill_rows);
         ATJUP_CHECK_LAUNCH("bc_theta");
     }
     if (which & ATJUP_BC_PHI) {
+        FieldList L{};
+        add(L, t); add(L, u); add(L, v); add(L, w);
+        if (ph) { add_species(L); add_massflux(L, true); add_turb(L); }
         c->launches++;
-        phi_kernel<<<dim3((P.jm + 127) / 128, P.im), 128, 0, c->stream>>>(t, u, v, w, P.jm, P.km, c->KP);
+        phi_kernel<<<dim3((P.jm + 127) / 128, P.im), 128, 0, c->stream>>>(L, P.jm, P.km, c->KP);
         ATJUP_CHECK_LAUNCH("bc_phi");
     }
-    if ((which & ATJUP_BC_SOLID) && c->n_solid > 0) {
-        c->launches++;
-        solid_kernel<<<(c->n_solid + 127) / 128, 128, 0, c->stream>>>(
-            c->solid_list, c->n_solid, t, u, v, w, c->f[ATJUP_F_P_STAT], c->f[ATJUP_F_P_DYN]);
-        if (P.mount_t_ambient && c->n_amb_rows > 0) {
+    if (which & ATJUP_BC_SOLID) {
+        if (c->n_solid > 0) {
+            FieldList S{};
+            add(S, t); add(S, c->f[ATJUP_F_P_STAT]); add(S, c->f[ATJUP_F_P_DYN]);
+            if (ph) { add_species(S); add_massflux(S, true); }
             c->launches++;
-            ambient_kernel<<<c->n_amb_rows, 32, 0, c->stream>>>(c->amb_rows, c->solid, t, P.jm,
-                                                               P.km, c->KP);
+            solid_kernel<<<(c->n_solid + 127) / 128, 128, 0, c->stream>>>(c->solid_list, c->n_solid,
+                                                                           S, u, v, w);
+            if (P.mount_t_ambient && c->n_amb_rows > 0) {
+                c->launches++;
+                ambient_kernel<<<c->n_amb_rows, 32, 0, c->stream>>>(c->amb_rows, c->solid, t, P.jm,
+                                                                   P.km, c->KP);
+            }
+        }
+        if (ph) {
+            SanArgs a{c->f[ATJUP_F_TKE], c->fn[ATJUP_F_TKE], c->f[ATJUP_F_DIS], c->fn[ATJUP_F_DIS],
+                      c->f[ATJUP_F_NUE], c->f[ATJUP_F_PROD], c->f[ATJUP_F_TKE_SOURCE],
+                      c->f[ATJUP_F_DIS_SOURCE], c->NP, 1000.0 / (P.u_0 * P.u_0),
+                      1.0e5 / (P.u_0 * P.L_atm * 1.0e3)};
+            c->launches++;
+            sanitise_kernel<<<(unsigned)((c->NP + 255) / 256), 256, 0, c->stream>>>(a);
         }
         ATJUP_CHECK_LAUNCH("bc_solid");
     }

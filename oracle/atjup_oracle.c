@@ -26,6 +26,14 @@ static inline int phi_wrap(int periodic, int kk, int km) {
 static inline double dmax(double a, double b) { return a < b ? b : a; }   /* std::max(a, b) */
 static inline double dmin(double a, double b) { return b < a ? b : a; }   /* std::min(a, b) */
 
+/* The bit pattern test of RungeKutta_Jup_Turb.cpp:273-278: NaN or +-Inf -> lo. */
+static double safe_clamp(double v, double lo, double hi) {
+    uint64_t bits;
+    memcpy(&bits, &v, sizeof bits);
+    if ((bits & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL) return lo;
+    return (v < lo) ? lo : ((v > hi) ? hi : v);
+}
+
 /* Geometry of one (i, j) row, built as RungeKutta_Jup_Turb.cpp:388-411 builds CellGeometry. */
 typedef struct {
     double rm, rm2, exp_rm, exp_2_rm, sinthe, sinthe2, costhe, cotanthe;
@@ -603,7 +611,68 @@ void ora_mixture_density(const AtjupParams* P, const ora_grid* G, ora_state* S) 
 /* BC_Jup.h:185-263 wrapping BoundaryConditions.h:151-250 for the dynamics fields t, u, v, w:
  * zonal means of v, w at levels im-3, im-2 before the pass; 2-point Neumann at both radial
  * walls; rigid lid u = 0; the top taper, then the zonal-mean-preserving sponge (taper 3).     */
-void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+/* The field lists of the boundary passes (BC_Jup.h:275-350), restricted to the fields of the
+ * hot path: the diagnostics of the chemistry and force routines (j_*, jT_*, w_*, difflux_*,
+ * thermalmassflux, the force arrays, Q_Latent, Q_Sensible) and chrom (off by default) are not
+ * part of it. X == NULL: the dynamics fields only. */
+enum { BCL_RADIUS, BCL_THETA_X, BCL_THETA_Z, BCL_PHI, BCL_SOLID, BCL_SPECIES };
+static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
+    int n = 0;
+    switch (which) {
+    case BCL_RADIUS:
+        L[n++] = S->t; L[n++] = S->u; L[n++] = S->v; L[n++] = S->w;
+        if (X) {
+            for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
+            L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
+            L[n++] = (double*)X->massflux_nh4sh;
+            L[n++] = X->tke; L[n++] = X->dis; L[n++] = X->nue_out; L[n++] = X->prod;
+            L[n++] = X->tke_source; L[n++] = X->dis_source;
+        }
+        break;
+    case BCL_THETA_X:
+        L[n++] = S->t; L[n++] = S->u;
+        if (X) {
+            for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
+            L[n++] = X->tke; L[n++] = X->dis; L[n++] = X->nue_out; L[n++] = X->prod;
+            L[n++] = X->tke_source; L[n++] = X->dis_source;
+        }
+        break;
+    case BCL_THETA_Z:
+        L[n++] = S->v; L[n++] = S->w;
+        if (X) {
+            L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
+            L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
+        }
+        break;
+    case BCL_PHI:
+        L[n++] = S->t; L[n++] = S->u; L[n++] = S->v; L[n++] = S->w;
+        if (X) {
+            for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
+            L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
+            L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
+            L[n++] = X->tke; L[n++] = X->dis; L[n++] = X->nue_out; L[n++] = X->prod;
+            L[n++] = X->tke_source; L[n++] = X->dis_source;
+        }
+        break;
+    case BCL_SOLID:   /* t and p_stat first: they keep their value where nothing is extrapolated */
+        L[n++] = S->t; L[n++] = S->p_stat; L[n++] = S->p_dyn;
+        if (X) {
+            for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
+            L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
+            L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
+        }
+        break;
+    case BCL_SPECIES:
+        if (X) for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
+        break;
+    }
+    return n;
+}
+
+/* BC_Jup::bcRadius (BC_Jup.h:185-263) around BoundaryConditions::bcRadius (151-250): 2-point
+ * Neumann at both radial walls for every listed field, rigid lid u = 0, the top taper of v, w
+ * (3 = zonal-mean preserving), then the species wall copy at i = 0 and positivity at both walls. */
+void ora_bc_radius_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X) {
     const int im = P->im, jm = P->jm, km = P->km, kn = km - 1;
     (void)G;
     double* zm = NULL;
@@ -618,10 +687,11 @@ void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S) {
                 zm[(size_t)(2 * l + 1) * jm + j] = sw / kn;
             }
     }
-    double* F[4] = {S->t, S->u, S->v, S->w};
+    double* F[40];
+    const int nf = bc_list(BCL_RADIUS, S, X, F);
     for (int j = 0; j < jm; j++)
         for (int k = 0; k < km; k++)
-            for (int f = 0; f < 4; f++) {
+            for (int f = 0; f < nf; f++) {
                 F[f][IDX(0, j, k)] = C43 * F[f][IDX(1, j, k)] - C13 * F[f][IDX(2, j, k)];
                 F[f][IDX(im - 1, j, k)] = C43 * F[f][IDX(im - 2, j, k)] - C13 * F[f][IDX(im - 3, j, k)];
             }
@@ -662,59 +732,76 @@ void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S) {
         }
         free(zm);
     }
+    /* species: wall copy (ATJUP_BC_SPECIES_WALL_COPY 1), positivity (ATJUP_BC_RADIUS_POSITIVE 1) */
+    double* Q[ATJUP_S_COUNT];
+    const int nq = bc_list(BCL_SPECIES, S, X, Q);
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++)
+            for (int f = 0; f < nq; f++) Q[f][IDX(0, j, k)] = Q[f][IDX(1, j, k)];
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++)
+            for (int f = 0; f < nq; f++) {
+                if (Q[f][IDX(0, j, k)] < 0.0) Q[f][IDX(0, j, k)] = 0.0;
+                if (Q[f][IDX(im - 1, j, k)] < 0.0) Q[f][IDX(im - 1, j, k)] = 0.0;
+            }
 }
 
 /* BoundaryConditions.h:253-336: fill the rows next to the poles that the RK step does not
- * integrate (copy for t, u; ramp for v, w), then pole rows (copy; v = w = 0).                 */
-void ora_bc_theta(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+ * integrate (copy for the extrapolated list, ramp for the zero list), then the pole rows (copy;
+ * zero list = 0).                                                                              */
+void ora_bc_theta_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X) {
     const int im = P->im, jm = P->jm, km = P->km;
     (void)G;
     const int nfill = P->pole_fill_rows;
-    double* X[2] = {S->t, S->u};
-    double* Z[2] = {S->v, S->w};
+    double *XL[40], *Z[40];
+    const int nx = bc_list(BCL_THETA_X, S, X, XL), nz = bc_list(BCL_THETA_Z, S, X, Z);
     for (int k = 0; k < km; k++)
         for (int i = 0; i < im; i++) {
             if (nfill > 0) {
                 const int jf = nfill + 1;
                 for (int r = 1; r <= nfill; r++) {
                     const double ramp = (double)r / (double)jf;
-                    for (int f = 0; f < 2; f++) {
-                        X[f][IDX(i, r, k)] = X[f][IDX(i, jf, k)];
-                        X[f][IDX(i, jm - 1 - r, k)] = X[f][IDX(i, jm - 1 - jf, k)];
+                    for (int f = 0; f < nx; f++) {
+                        XL[f][IDX(i, r, k)] = XL[f][IDX(i, jf, k)];
+                        XL[f][IDX(i, jm - 1 - r, k)] = XL[f][IDX(i, jm - 1 - jf, k)];
                     }
-                    for (int f = 0; f < 2; f++) {
+                    for (int f = 0; f < nz; f++) {
                         Z[f][IDX(i, r, k)] = ramp * Z[f][IDX(i, jf, k)];
                         Z[f][IDX(i, jm - 1 - r, k)] = ramp * Z[f][IDX(i, jm - 1 - jf, k)];
                     }
                 }
             }
-            for (int f = 0; f < 2; f++) { Z[f][IDX(i, 0, k)] = 0.0; Z[f][IDX(i, jm - 1, k)] = 0.0; }
-            for (int f = 0; f < 2; f++) {
-                X[f][IDX(i, 0, k)] = X[f][IDX(i, 1, k)];              /* pole copy (form COPY) */
-                X[f][IDX(i, jm - 1, k)] = X[f][IDX(i, jm - 2, k)];
+            for (int f = 0; f < nz; f++) { Z[f][IDX(i, 0, k)] = 0.0; Z[f][IDX(i, jm - 1, k)] = 0.0; }
+            for (int f = 0; f < nx; f++) {
+                XL[f][IDX(i, 0, k)] = XL[f][IDX(i, 1, k)];             /* pole copy (form COPY) */
+                XL[f][IDX(i, jm - 1, k)] = XL[f][IDX(i, jm - 2, k)];
             }
         }
 }
 
 /* BoundaryConditions.h:339-360: periodic seam, k = km-1 is the copy of k = 0. */
-void ora_bc_phi(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+void ora_bc_phi_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X) {
     const int im = P->im, jm = P->jm, km = P->km;
     (void)G;
-    double* F[4] = {S->t, S->u, S->v, S->w};
+    double* F[40];
+    const int nf = bc_list(BCL_PHI, S, X, F);
     for (int i = 0; i < im; i++)
         for (int j = 0; j < jm; j++)
-            for (int f = 0; f < 4; f++) F[f][IDX(i, j, km - 1)] = F[f][IDX(i, j, 0)];
+            for (int f = 0; f < nf; f++) F[f][IDX(i, j, km - 1)] = F[f][IDX(i, j, 0)];
 }
 
-/* BC_Jup.h:460-658 for the dynamics fields: velocities 0 in solid cells; surface cells take
- * the 2-point extrapolation of t, p_stat, p_dyn from the first direction with two fluid cells
- * (+i, -i, +j, -j, +k, -k), interior cells p_dyn = 0; then solid t = ambient row mean.        */
-void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) {
+/* BC_Jup.h:460-658: velocities 0 in solid cells; surface cells take the 2-point extrapolation
+ * of every listed scalar from the first direction with two fluid cells (+i, -i, +j, -j, +k, -k),
+ * interior cells (and surface cells without a pair) set the list from p_dyn on to 0; then solid
+ * t = ambient row mean; then (with the physics fields) the sanitising clamps of k*, omega*, nue,
+ * prod and the sources over the whole grid, n copies included. */
+void ora_bc_solid_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X) {
     const int im = P->im, jm = P->jm, km = P->km;
     const uint8_t* sol = G->solid;
 #define SOLID(ii, jj, kk) (((ii) < 0 || (ii) >= im || (jj) < 0 || (jj) >= jm || (kk) < 0 || (kk) >= km) ? 1 : sol[IDX(ii, jj, kk)])
 #define FLUID(ii, jj, kk) (((ii) < 0 || (ii) >= im || (jj) < 0 || (jj) >= jm || (kk) < 0 || (kk) >= km) ? 0 : !sol[IDX(ii, jj, kk)])
-    double* sc[3] = {S->t, S->p_stat, S->p_dyn};
+    double* sc[40];
+    const int ns = bc_list(BCL_SOLID, S, X, sc);
     const int n_state = 2;
     for (int j = 0; j < jm; j++)
         for (int k = 0; k < km; k++)
@@ -724,7 +811,7 @@ void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) {
                 S->u[c] = 0.0; S->v[c] = 0.0; S->w[c] = 0.0;
                 const int surf = !SOLID(i + 1, j, k) || !SOLID(i - 1, j, k) || !SOLID(i, j + 1, k)
                               || !SOLID(i, j - 1, k) || !SOLID(i, j, k + 1) || !SOLID(i, j, k - 1);
-                if (!surf) { for (int f = n_state; f < 3; f++) sc[f][c] = 0.0; continue; }
+                if (!surf) { for (int f = n_state; f < ns; f++) sc[f][c] = 0.0; continue; }
                 int ok = 1; size_t a = 0, b = 0;
                 if (FLUID(i + 1, j, k) && FLUID(i + 2, j, k)) { a = IDX(i + 1, j, k); b = IDX(i + 2, j, k); }
                 else if (FLUID(i - 1, j, k) && FLUID(i - 2, j, k)) { a = IDX(i - 1, j, k); b = IDX(i - 2, j, k); }
@@ -733,8 +820,8 @@ void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) {
                 else if (FLUID(i, j, k + 1) && FLUID(i, j, k + 2)) { a = IDX(i, j, k + 1); b = IDX(i, j, k + 2); }
                 else if (FLUID(i, j, k - 1) && FLUID(i, j, k - 2)) { a = IDX(i, j, k - 1); b = IDX(i, j, k - 2); }
                 else ok = 0;
-                if (ok) { for (int f = 0; f < 3; f++) sc[f][c] = C43 * sc[f][a] - C13 * sc[f][b]; }
-                else { for (int f = n_state; f < 3; f++) sc[f][c] = 0.0; }
+                if (ok) { for (int f = 0; f < ns; f++) sc[f][c] = C43 * sc[f][a] - C13 * sc[f][b]; }
+                else { for (int f = n_state; f < ns; f++) sc[f][c] = 0.0; }
             }
     if (P->mount_t_ambient)
         for (int i = 0; i < im; i++)
@@ -748,9 +835,30 @@ void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) {
                 const double t_amb = s / n;
                 for (int k = 0; k < km; k++) if (sol[IDX(i, j, k)]) S->t[IDX(i, j, k)] = t_amb;
             }
+    if (X) {
+        const size_t N = (size_t)im * jm * km;
+        const double tke_max_nd = 1000.0 / (P->u_0 * P->u_0);
+        const double nue_max = 1.0e5 / (P->u_0 * P->L_atm * 1.0e3);
+        const double prod_max = 1.0e4, dis_max = 1.0e6;
+        for (size_t c = 0; c < N; c++) {
+            X->tke[c] = safe_clamp(X->tke[c], 0.0, tke_max_nd);
+            X->tken[c] = safe_clamp(X->tken[c], 0.0, tke_max_nd);
+            X->dis[c] = safe_clamp(X->dis[c], 1.0e-10, dis_max);
+            X->disn[c] = safe_clamp(X->disn[c], 1.0e-10, dis_max);
+            X->nue_out[c] = safe_clamp(X->nue_out[c], 0.0, nue_max);
+            X->prod[c] = safe_clamp(X->prod[c], 0.0, prod_max);
+            X->tke_source[c] = safe_clamp(X->tke_source[c], -prod_max, prod_max);
+            X->dis_source[c] = safe_clamp(X->dis_source[c], -prod_max, prod_max);
+        }
+    }
 #undef SOLID
 #undef FLUID
 }
+
+void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S) { ora_bc_radius_x(P, G, S, NULL); }
+void ora_bc_theta(const AtjupParams* P, const ora_grid* G, ora_state* S) { ora_bc_theta_x(P, G, S, NULL); }
+void ora_bc_phi(const AtjupParams* P, const ora_grid* G, ora_state* S) { ora_bc_phi_x(P, G, S, NULL); }
+void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S) { ora_bc_solid_x(P, G, S, NULL); }
 
 /* ------------------------------------------------------------------------------------------ */
 /* lib/Utils.cpp:227-453. Direction-split k (periodic ring of km-1, seam copy), j (clamped),
@@ -1429,13 +1537,6 @@ void ora_rhs_phys_cell(const AtjupParams* P, const AtjupPhysics* PH, const ora_g
     X->rhs_dis[c] = -transport_dis + diffusion_dis * diffusion_dis_re + dis_src;
 }
 
-/* The bit pattern test of RungeKutta_Jup_Turb.cpp:273-278: NaN or +-Inf -> lo. */
-static double safe_clamp(double v, double lo, double hi) {
-    uint64_t bits;
-    memcpy(&bits, &v, sizeof bits);
-    if ((bits & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL) return lo;
-    return (v < lo) ? lo : ((v > hi) ? hi : v);
-}
 
 /* RungeKutta_Jup_Turb.cpp:261-583 with every transported field. */
 void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_state* S,

@@ -95,6 +95,11 @@ void ora_bc_radius(const AtjupParams* P, const ora_grid* G, ora_state* S);
 void ora_bc_theta(const AtjupParams* P, const ora_grid* G, ora_state* S);
 void ora_bc_phi(const AtjupParams* P, const ora_grid* G, ora_state* S);
 void ora_bc_solid(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* the same passes over the full-physics field lists (X = NULL: the dynamics fields only) */
+void ora_bc_radius_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X);
+void ora_bc_theta_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X);
+void ora_bc_phi_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X);
+void ora_bc_solid_x(const AtjupParams* P, const ora_grid* G, ora_state* S, ora_phys* X);
 /* lib/Utils.cpp:227-323 (order 2) and 334-453 (order 4) */
 void ora_shapiro(const AtjupParams* P, const ora_grid* G, double* f, int order, double strength,
                  int passes, int use_topo);

@@ -318,3 +318,36 @@ def oracle_turbulence(params, phys, grid: dict, fields: dict) -> dict:
     o.lib.ora_turbulence(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(o.G),
                          ctypes.byref(o.S), ctypes.byref(X))
     return keep
+
+
+def oracle_bc(params, grid: dict, fields: dict, steps=("radius", "theta", "phi", "solid"),
+              physics=True) -> dict:
+    """The boundary passes in order on copies of fields; returns {step: {field: array}} after
+    each step. physics=False: the dynamics fields only (ora_bc_*)."""
+    from atjup_b200.params import SPECIES
+    o = Oracle(params, grid, fields)
+    shape = o.shape
+    keep = {}
+    X = None
+    if physics:
+        names = list(SPECIES) + ["tke", "dis", "tken", "disn", "nue", "prod", "tke_source",
+                                 "dis_source", "massflux_h2s", "massflux_nh3", "massflux_nh4sh",
+                                 "fluxlim_nh4sh"]
+        for n in names:
+            keep[n] = np.ascontiguousarray(fields[n], dtype=np.float64).reshape(shape).copy()
+        X = OraPhys()
+        for s_, n in enumerate(SPECIES):
+            X.q[s_] = _dp(keep[n])
+        for n in ("tke", "dis", "tken", "disn", "prod", "tke_source", "dis_source",
+                  "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh"):
+            setattr(X, n, _dp(keep[n]))
+        X.nue_out = _dp(keep["nue"])
+    out = {}
+    for step in steps:
+        fn = getattr(o.lib, f"ora_bc_{step}_x")
+        fn(ctypes.byref(params), ctypes.byref(o.G), ctypes.byref(o.S),
+           ctypes.byref(X) if X is not None else None)
+        snap = {n: o.f[n].copy() for n in ("t", "u", "v", "w", "p_stat", "p_dyn")}
+        snap.update({n: a.copy() for n, a in keep.items()})
+        out[step] = snap
+    return out

@@ -146,6 +146,39 @@ def turb_case(ref, g, data, seed=SATADJ_SEED + 2):
     data["out_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
 
 
+BC_FIELDS = ("t", "u", "v", "w", "p_stat", "p_dyn") + PHYS_FIELDS + (
+    "tken", "disn", "nue", "prod", "tke_source", "dis_source", "massflux_h2s", "massflux_nh3",
+    "massflux_nh4sh", "fluxlim_nh4sh")
+
+
+def bc_case(ref, g, data, seed=SATADJ_SEED + 3):
+    """The four boundary passes of one iteration (BC_Jup::bcRadius, bcTheta, bcPhi,
+    bcSolidGround, cJupiterModel.cpp:1263-1272) on the moist initial state with the closure on,
+    every listed field carrying seeded noise (a tenth of the species negative, k* and omega*
+    with some NaN-free out-of-range values) so that each pass has something to overwrite; the
+    state after each pass is recorded."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    shape = ref.shape
+    for n in BC_FIELDS:
+        f = ref.get(n)
+        scale = np.abs(f).max()
+        scale = scale if scale > 0 else 1e-4
+        f = f + 0.05 * scale * rng.standard_normal(shape)
+        if n in PHYS_FIELDS[:11]:
+            f = np.where(rng.uniform(size=shape) < 0.1, -np.abs(f), f)
+        if n in ("tke", "tken", "dis", "disn", "nue", "prod"):
+            f = np.where(rng.uniform(size=shape) < 0.01, -np.abs(f), f)
+            f = np.where(rng.uniform(size=shape) < 0.001, 1e7, f)
+        ref.set(n, f)
+        data["in_" + n] = f
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for step, fn in (("radius", ref.L.ref_bc_radius), ("theta", ref.L.ref_bc_theta),
+                     ("phi", ref.L.ref_bc_phi), ("solid", ref.L.ref_bc_solid)):
+        ref.quiet(fn)
+        for n in BC_FIELDS:
+            data[f"bc_{step}_{n}"] = ref.get(n)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -157,15 +190,16 @@ def main():
     ap.add_argument("--satadj-synthetic", action="store_true")
     ap.add_argument("--rk4-phys", action="store_true")
     ap.add_argument("--turb", action="store_true")
+    ap.add_argument("--bc", action="store_true")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
-    env = dict(PHYS_ENV) if (a.rk4_phys or a.turb) else dict(DRY_ENV)
+    env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -178,6 +212,8 @@ def main():
         rk4_phys_case(ref, g, data)
     elif a.turb:
         turb_case(ref, g, data)
+    elif a.bc:
+        bc_case(ref, g, data)
     elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
