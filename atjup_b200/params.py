@@ -25,7 +25,7 @@ F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, 
     F_S_PRECIP_NH3, F_S_PRECIP_NH3_CLOUD, F_S_PRECIP_NH3_ICE, \
     F_S_PRECIP_CH4, F_S_PRECIP_CH4_CLOUD, F_S_PRECIP_CH4_ICE, \
     F_MASSFLUX_H2S, F_MASSFLUX_NH3, F_MASSFLUX_NH4SH, F_FLUXLIM_NH4SH, \
-    F_PROD, F_TKE_SOURCE, F_DIS_SOURCE = range(45)
+    F_PROD, F_TKE_SOURCE, F_DIS_SOURCE, F_DIFFLUX_H2S, F_DIFFLUX_NH3, F_DIFFLUX_NH4SH = range(48)
 F2_VEL_STAR = 0
 FIELD_IDS = {
     "t": F_T, "u": F_U, "v": F_V, "w": F_W, "p_dyn": F_P_DYN, "p_hydro": F_P_HYDRO,
@@ -44,6 +44,7 @@ FIELD_IDS = {
     "massflux_h2s": F_MASSFLUX_H2S, "massflux_nh3": F_MASSFLUX_NH3,
     "massflux_nh4sh": F_MASSFLUX_NH4SH, "fluxlim_nh4sh": F_FLUXLIM_NH4SH,
     "prod": F_PROD, "tke_source": F_TKE_SOURCE, "dis_source": F_DIS_SOURCE,
+    "difflux_h2s": F_DIFFLUX_H2S, "difflux_nh3": F_DIFFLUX_NH3, "difflux_nh4sh": F_DIFFLUX_NH4SH,
 }
 
 # transported scalars in the order of the physics block (ATJUP_S_*), and the fields whose
@@ -179,6 +180,59 @@ def resolve_physics(env: Mapping[str, str] | None = None, constants: Mapping[str
     ph.vel_star_max = _env(env, "ATJUP_VEL_STAR_MAX", math.sqrt(0.002) * 200.0, float)
     ph.abl_height = float((constants or {}).get("abl_height", 20000.0))
     return ph
+
+
+class AtjupMicro(ctypes.Structure):
+    """Mirror of AtjupMicro (the loop's radiation, precipitation and chemistry)."""
+    _fields_ = [(n, ctypes.c_int32) for n in ("radiation_on", "precip_on", "nh4sh_eq", "satadj_on",
+                                               "solar_on", "rad_bottom", "precip_coupling_on", "pad")] + [
+        (n, ctypes.c_double) for n in ("F_int", "S_solar", "albedo_bond", "x_H2", "x_He",
+                                       "cia_strength", "opacity_strength", "solar_strength",
+                                       "sw_tau_per_bar", "precip_rate_scale", "m_nh3", "m_h2s",
+                                       "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh",
+                                       "polar_divisor_floor")] + [("gas", AtjupGasParams * 3)]
+
+
+# cJupiterModel's radiation constants (cJupiterModel.h:1109-1118), molar masses (255-270) and the
+# diffusivities mue / (rg sc) of the chemistry fluxes (ChemistryJup.h:383-385) with its defaults
+# (the active set of cJupiterModel.h:385-387 has mue_nh4sh = 0, so NH4SH does not diffuse).
+DEFAULT_MICRO = {"F_int": 5.4, "S_solar": 50.5, "albedo_bond": 0.343, "x_H2": 0.863,
+                 "x_He": 0.134, "m_nh3": 17.03052, "m_h2s": 34.08088, "m_nh4sh": 51.1114,
+                 "D_nh3": 0.92e-5 / (817.0 * 0.61), "D_h2s": 1.3e-5 / (949.0 * 0.94),
+                 "D_nh4sh": 0.0, "polar_divisor_floor": 0.4}
+
+
+def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, float] | None = None,
+                  gases: Mapping | None = None) -> AtjupMicro:
+    """Microphysics block from the environment with the reference's defaults (ATJUP_RADIATION 1,
+    ATJUP_PRECIP 1, ATJUP_NH4SH_EQ 1, ATJUP_SOLAR 1, ATJUP_RAD_BOTTOM 0, ATJUP_PRECIP_COUPLING 1,
+    ATJUP_CIA_STRENGTH 3.9, ATJUP_OPACITY_STRENGTH 1, ATJUP_SOLAR_STRENGTH 1,
+    ATJUP_SW_TAU_PER_BAR 1, ATJUP_PRECIP_SCALE 1); constants override DEFAULT_MICRO, gases
+    the three gas constant sets (DEFAULT_GASES)."""
+    env = os.environ if env is None else env
+    c = dict(DEFAULT_MICRO)
+    if constants:
+        c.update({k: float(v) for k, v in constants.items() if k in c})
+    mc = AtjupMicro()
+    mc.radiation_on = int(_env(env, "ATJUP_RADIATION", 1) != 0)
+    mc.precip_on = int(_env(env, "ATJUP_PRECIP", 1) != 0)
+    mc.nh4sh_eq = int(_env(env, "ATJUP_NH4SH_EQ", 1) != 0)
+    mc.satadj_on = 1
+    mc.solar_on = _env(env, "ATJUP_SOLAR", 1)
+    mc.rad_bottom = _env(env, "ATJUP_RAD_BOTTOM", 0)
+    mc.precip_coupling_on = int(_env(env, "ATJUP_PRECIP_COUPLING", 1.0, float) != 0.0)
+    mc.cia_strength = _env(env, "ATJUP_CIA_STRENGTH", 3.9, float)
+    mc.opacity_strength = _env(env, "ATJUP_OPACITY_STRENGTH", 1.0, float)
+    mc.solar_strength = _env(env, "ATJUP_SOLAR_STRENGTH", 1.0, float)
+    mc.sw_tau_per_bar = _env(env, "ATJUP_SW_TAU_PER_BAR", 1.0, float)
+    mc.precip_rate_scale = _env(env, "ATJUP_PRECIP_SCALE", 1.0, float)
+    for n in ("F_int", "S_solar", "albedo_bond", "x_H2", "x_He", "m_nh3", "m_h2s", "m_nh4sh",
+              "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor"):
+        setattr(mc, n, c[n])
+    gases = gases or DEFAULT_GASES
+    for q, g in enumerate(("H2O", "NH3", "CH4")):
+        mc.gas[q] = resolve_gas(gases[g], env)
+    return mc
 
 
 class AtjupSatStats(ctypes.Structure):

@@ -59,6 +59,8 @@ enum {
     ATJUP_F_MASSFLUX_H2S, ATJUP_F_MASSFLUX_NH3, ATJUP_F_MASSFLUX_NH4SH,
     ATJUP_F_FLUXLIM_NH4SH,                                    /* frozen chemistry sources      */
     ATJUP_F_PROD, ATJUP_F_TKE_SOURCE, ATJUP_F_DIS_SOURCE,     /* closure diagnostics (out)     */
+    ATJUP_F_DIFFLUX_H2S, ATJUP_F_DIFFLUX_NH3, ATJUP_F_DIFFLUX_NH4SH,
+                                                              /* diffusive chemistry fluxes    */
     ATJUP_F_COUNT
 };
 
@@ -306,6 +308,52 @@ typedef struct AtjupSatStats {
  * ice: ATJUP_F_H2O.. / NH3.. / CH4..), with t, p_stat, rho_mix (ATJUP_LOCAL_RHO) and the solid
  * mask; updates t and the three species in place. stats may be NULL. */
 int atjup_gpu_satadj(AtjupCtx* ctx, int32_t gas, const AtjupGasParams* gp, AtjupSatStats* stats);
+
+/* ---- the loop's microphysics (Radiation.h, Precipitation.h, ChemistryJup.h) ---- */
+
+/* Every constant and knob of the moist part of the iteration, resolved on the host. */
+typedef struct AtjupMicro {
+    int32_t radiation_on;        /* ATJUP_RADIATION 1                                             */
+    int32_t precip_on;           /* ATJUP_PRECIP 1                                                */
+    int32_t nh4sh_eq;            /* ATJUP_NH4SH_EQ 1: NH4SH by equilibrium (ChemistryJup.h:285)    */
+    int32_t satadj_on;           /* the three gas adjustments (always on in the reference)        */
+    int32_t solar_on;            /* ATJUP_SOLAR 1                                                 */
+    int32_t rad_bottom;          /* ATJUP_RAD_BOTTOM 0: lower boundary of the thermal stream      */
+    int32_t precip_coupling_on;  /* ATJUP_PRECIP_COUPLING != 0: sources, not in-place removal     */
+    int32_t pad;
+    /* radiation (Radiation.h:166-487, cJupiterModel.h:1109-1118)                                 */
+    double F_int, S_solar, albedo_bond, x_H2, x_He;
+    double cia_strength;         /* ATJUP_CIA_STRENGTH 3.9                                        */
+    double opacity_strength;     /* ATJUP_OPACITY_STRENGTH 1                                      */
+    double solar_strength;       /* ATJUP_SOLAR_STRENGTH 1                                        */
+    double sw_tau_per_bar;       /* ATJUP_SW_TAU_PER_BAR 1                                        */
+    /* precipitation (Precipitation.h:93-140)                                                     */
+    double precip_rate_scale;    /* ATJUP_PRECIP_SCALE 1                                          */
+    /* chemistry (ChemistryJup.h:283-543, FluxLimiter.h)                                          */
+    double m_nh3, m_h2s, m_nh4sh;          /* molar masses [kg/kmol]                              */
+    double D_nh3, D_h2s, D_nh4sh;          /* mue / (rg sc): diffusivities of the mass fluxes     */
+    double polar_divisor_floor;            /* 0.4 (ATPhys.h:104-108)                              */
+    AtjupGasParams gas[3];                 /* H2O, NH3, CH4                                        */
+} AtjupMicro;
+
+/* Set (or with NULL clear) the microphysics of the iteration; with it and the physics block set,
+ * atjup_gpu_step runs the full-physics schedule of the loop. */
+int atjup_gpu_set_micro(AtjupCtx* ctx, const AtjupMicro* micro);
+/* Radiation<cJupiterModel>::run (Radiation.h:251-487): grey two-stream fluxes per column -> Q_rad. */
+int atjup_gpu_radiation(AtjupCtx* ctx);
+/* Precipitation<cJupiterModel>::run (Precipitation.h:191-445): the three-category column scheme of
+ * H2O, NH3, CH4 -> S_precip_* and Q_precip (or in-place removal when the coupling is off). */
+int atjup_gpu_precipitation(AtjupCtx* ctx);
+/* ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373): the NH4SH / NH3 + H2S
+ * equilibrium per cell by bisection, with its latent heat. */
+int atjup_gpu_nh4sh_equilibrium(AtjupCtx* ctx);
+/* The chemistry block of the loop: DiffMassFluxJup's diffusive fluxes (ChemistryJup.h:375-538),
+ * their 1-2-1 smoothing, ChemMassRateJup (59-281; with the equilibrium on, massflux = difflux),
+ * FluxLimiterNH4SH (FluxLimiter.h) and the smoothing of the mass fluxes (cJupiterModel.cpp:
+ * 1144-1162). */
+int atjup_gpu_chemistry(AtjupCtx* ctx);
+/* cJupiterModel::clampNegativeSpecies (FileIO_Jup.cpp:494-548): species < 0 or NaN -> 0. */
+int atjup_gpu_clamp_species(AtjupCtx* ctx);
 
 /* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381) for the dry
  * configuration: pressure solve on even iterations (and when first != 0), mixture density,

@@ -1936,3 +1936,343 @@ void ora_turbulence(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid
     }
 #undef HM
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * The loop's microphysics: radiation, precipitation, the NH4SH equilibrium, the chemistry fluxes
+ * and the species clamp. Operand order as in the reference throughout.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Radiation.h:251-456: per (j, k) column from the first fluid level to the top, layer optical
+ * depths of collision-induced H2 absorption, CH4/NH3 bands and clouds, the grey downward and
+ * upward thermal fluxes, the shortwave attenuated by pressure, and the heating of each layer. */
+void ora_radiation(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                   ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const double t_ref = P->t_ref, g = P->g;
+    const double sigma = 5.670374419e-8, P0_phys = 1.0e5, he_ratio = 0.6, C_cia = 3.5e-6;
+    const double kappa_ch4 = 0.003, kappa_nh3 = 1.5, kappa_cloud = 25.0, kappa_ice = 12.0;
+    const double tau_cloud_cap = 0.4, opac_cal = 0.025;
+    const double pi_ = 3.14159265358979323846;
+    const double comp = MC->x_H2 * MC->x_H2 + he_ratio * MC->x_H2 * MC->x_He;
+    const double cia_coeff = C_cia * MC->cia_strength * comp / g;
+    const double opac_mult = MC->opacity_strength;
+    double B[128], eps[128], Fd[130], Fu[130], Fsw[130];
+    if (im > 127) return;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            int i_base = G->topo[(size_t)j * km + k];
+            if (i_base < 0) i_base = 0;
+            const int i_top = im - 1;
+            if (i_base >= i_top) continue;
+            for (int i = i_base; i <= i_top; i++) {
+                const size_t c = IDX(i, j, k);
+                const double T = S->t[c] * t_ref;
+                B[i] = sigma * T * T * T * T;
+                const double P_lo = S->p_stat[c] * P0_phys;
+                const double P_hi = (i < i_top) ? S->p_stat[IDX(i + 1, j, k)] * P0_phys : 0.0;
+                double dP = P_lo - P_hi;
+                if (dP < 0.0) dP = 0.0;
+                const double P_mean = 0.5 * (P_lo + P_hi);
+                const double dm = dP / g;
+                const double tau_cia = (T > 0.0) ? cia_coeff * (P_mean / T) * dP : 0.0;
+                const double rho_c = S->rho_mix[c];
+                const double inv_rho = (rho_c > 0.0 && isfinite(rho_c)) ? 1.0 / rho_c : 0.0;
+                const double q_ch4 = dmax(0.0, X->q[ATJUP_S_CH4][c]) * inv_rho;
+                const double q_nh3 = dmax(0.0, X->q[ATJUP_S_NH3][c]) * inv_rho;
+                const double tau_gas = opac_mult * opac_cal * (kappa_ch4 * q_ch4 + kappa_nh3 * q_nh3) * dm;
+                const double q_liq = (dmax(0.0, X->q[ATJUP_S_H2O_CLOUD][c])
+                                    + dmax(0.0, X->q[ATJUP_S_NH3_CLOUD][c])
+                                    + dmax(0.0, X->q[ATJUP_S_CH4_CLOUD][c])) * inv_rho;
+                const double q_ice = (dmax(0.0, X->q[ATJUP_S_H2O_ICE][c])
+                                    + dmax(0.0, X->q[ATJUP_S_NH3_ICE][c])
+                                    + dmax(0.0, X->q[ATJUP_S_CH4_ICE][c])) * inv_rho;
+                double tau_cloud = opac_mult * opac_cal * (kappa_cloud * q_liq + kappa_ice * q_ice) * dm;
+                if (tau_cloud > tau_cloud_cap) tau_cloud = tau_cloud_cap;
+                const double tau_l = tau_cia + tau_gas + tau_cloud;
+                eps[i] = 1.0 - exp(-tau_l);
+            }
+            for (int i = 0; i <= im + 1; i++) Fsw[i] = 0.0;
+            if (MC->solar_on != 0) {
+                const double colat = pi_ * (double)j / (double)(jm - 1);
+                const double cos_lat = dmax(0.0, sin(colat));
+                const double F_sun_toa = MC->solar_strength * MC->S_solar * (1.0 - MC->albedo_bond) * cos_lat / pi_;
+                for (int i = i_base; i <= i_top + 1; i++) {
+                    const double p_bar = (i <= i_top) ? S->p_stat[IDX(i, j, k)] : 0.0;
+                    Fsw[i] = F_sun_toa * exp(-MC->sw_tau_per_bar * dmax(0.0, p_bar));
+                }
+            }
+            Fd[i_top + 1] = 0.0;
+            for (int i = i_top; i >= i_base; i--) Fd[i] = Fd[i + 1] * (1.0 - eps[i]) + eps[i] * B[i];
+            if (MC->rad_bottom == 1) Fu[i_base] = dmax(0.0, 2.0 * B[i_base] - Fd[i_base + 1]);
+            else Fu[i_base] = Fd[i_base] + MC->F_int + Fsw[i_base];
+            for (int i = i_base; i <= i_top; i++) Fu[i + 1] = Fu[i] * (1.0 - eps[i]) + eps[i] * B[i];
+            for (int i = i_base; i <= i_top; i++) {
+                const double net_bot = Fu[i] - Fd[i];
+                const double net_top = Fu[i + 1] - Fd[i + 1];
+                double dz = (i < i_top) ? layer_dz_m(X, im, i) : layer_dz_m(X, im, i - 1);
+                if (dz <= 0.0) dz = 1.0;
+                const double sw_absorbed = Fsw[i + 1] - Fsw[i];
+                const double Q_sw = sw_absorbed / dz;
+                S->Q_rad[IDX(i, j, k)] = (net_bot - net_top) / dz + Q_sw;
+            }
+            for (int i = 0; i < i_base; i++) S->Q_rad[IDX(i, j, k)] = 0.0;
+        }
+}
+
+/* Precipitation.h:273-445 for one species (gas q: 0 H2O, 1 NH3, 2 CH4). */
+static void precip_column(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                          ora_state* S, ora_phys* X, int q) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const AtjupGasParams* gs = &MC->gas[q];
+    const int sv = q == 0 ? ATJUP_S_H2O : (q == 1 ? ATJUP_S_NH3 : ATJUP_S_CH4);
+    double *vap = X->q[sv], *cld = X->q[sv + 1], *ice = X->q[sv + 2];
+    double *Sv = (double*)X->s_precip[3 * q], *Sc = (double*)X->s_precip[3 * q + 1];
+    double *Si = (double*)X->s_precip[3 * q + 2];
+    const double t_ref = P->t_ref;
+    const double Lf = gs->ls - gs->lv;
+    const double P_max_flux = 1.0e-4, dep_frac = 1.0, ratio_cap = 5.0, rs = MC->precip_rate_scale;
+    const double c_c_au = 2.0e-8, c_i_au = 5.0e-8, q_c_crit = 5.0e-4, c_ac = 1.0e-7;
+    const double c_rim = 1.0e-8, z_csg = 2.5e-8, a_ev = 2.76e-3, c_melt_K = 0.2, c_frz_K = 0.2;
+    const double P_ref = 1.0e-4, v_fall = 2.0;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            int i_base = G->topo[(size_t)j * km + k];
+            if (i_base < 0) i_base = 0;
+            const int i_top = im - 1;
+            if (i_base >= i_top) continue;
+            double Pr = 0.0, Ps = 0.0, Pg = 0.0;   /* the fluxes leaving the layer above */
+            for (int i = i_top - 1; i >= i_base; i--) {
+                const size_t c = IDX(i, j, k);
+                const double T = S->t[c] * t_ref;
+                const double p_u = S->p_stat[c];
+                const double q_v = dmax(0.0, vap[c]), q_c = dmax(0.0, cld[c]), q_i = dmax(0.0, ice[c]);
+                const double E_r = ora_svp(T, gs->C, gs->L0, gs->R, gs->del_alf, gs->del_bet);
+                double rho = P->r_mix;
+                if (P->local_rho && S->rho_mix[c] > 0.0 && isfinite(S->rho_mix[c])) rho = S->rho_mix[c];
+                const double q_sat = (p_u > E_r) ? rho * gs->ep * E_r / p_u : q_v;
+                const double dz = dmax(0.0, layer_dz_m(X, im, i));
+                if (dz <= 0.0) continue;   /* the fluxes pass through unchanged */
+                const double F_r_in = Pr, F_s_in = Ps, F_g_in = Pg;
+                const double Rain = dmin(ratio_cap, F_r_in / P_ref);
+                const double Snow = dmin(ratio_cap, F_s_in / P_ref);
+                const double Graupel = dmin(ratio_cap, F_g_in / P_ref);
+                const double Rain_79 = (Rain > 0.0) ? pow(Rain, 7.0 / 9.0) : 0.0;
+                const double Rain_49 = (Rain > 0.0) ? pow(Rain, 4.0 / 9.0) : 0.0;
+                const int warm = (T >= gs->t_0);
+                const double S_c_au = (warm && q_c > q_c_crit) ? (rs * c_c_au) * (q_c - q_c_crit) : 0.0;
+                const double S_i_au = (!warm && T >= gs->t_00) ? (rs * c_i_au) * q_i : 0.0;
+                const double S_ac = warm ? (rs * c_ac) * q_c * Rain_79 : 0.0;
+                const double S_s_rim = !warm ? (rs * c_rim) * q_c * Snow : 0.0;
+                const double S_g_rim = !warm ? (rs * c_rim) * q_c * Graupel : 0.0;
+                const double S_csg = (!warm && q_c > q_c_crit) ? (rs * z_csg) * q_c * Snow : 0.0;
+                const double f_melt = warm ? dmin(1.0, c_melt_K * (T - gs->t_0)) : 0.0;
+                const double f_frz = warm ? 0.0 : dmin(1.0, c_frz_K * (gs->t_0 - T));
+                const double F_s_melt = f_melt * F_s_in, F_g_melt = f_melt * F_g_in;
+                const double F_r_frz = f_frz * F_r_in;
+                const double F_r_avail = dmax(0.0, F_r_in - F_r_frz + F_s_melt + F_g_melt
+                                                   + (S_c_au + S_ac) * dz);
+                const double S_ev_raw = (warm && Rain > 0.0 && q_v < q_sat)
+                                      ? a_ev * (q_sat - q_v) * Rain_49 : 0.0;
+                const double F_ev_sat = dmax(0.0, q_sat - q_v) * v_fall;
+                const double F_ev = dmin(dmin(S_ev_raw * dz, F_r_avail), F_ev_sat);
+                const double S_ev = F_ev / dz;
+                S->Q_precip[c] += Lf * (S_s_rim + S_g_rim + S_csg)
+                                + Lf * (F_r_frz - F_s_melt - F_g_melt) / dz
+                                - gs->lv * F_ev / dz;
+                const double tau = dz / v_fall;
+                const double d_c = dmin(dep_frac * q_c, (S_c_au + S_ac + S_s_rim + S_g_rim + S_csg) * tau);
+                const double d_i = dmin(dep_frac * q_i, S_i_au * tau);
+                if (MC->precip_coupling_on) {
+                    const double nd = (P->L_atm * 1.0e3) / P->u_0;
+                    Sc[c] = -dmax(0.0, d_c) / tau * nd;
+                    Si[c] = -dmax(0.0, d_i) / tau * nd;
+                    Sv[c] = +S_ev * nd;
+                } else {
+                    cld[c] = q_c - dmax(0.0, d_c);
+                    ice[c] = q_i - dmax(0.0, d_i);
+                    vap[c] = q_v + S_ev * tau;
+                }
+                const double F_r = F_r_in - F_r_frz + F_s_melt + F_g_melt - F_ev + (S_c_au + S_ac) * dz;
+                const double F_s = F_s_in - F_s_melt + (S_i_au + S_s_rim - S_csg) * dz;
+                const double F_g = F_g_in - F_g_melt + F_r_frz + (S_g_rim + S_csg) * dz;
+                Pr = dmin(P_max_flux, dmax(0.0, F_r));
+                Ps = dmin(P_max_flux, dmax(0.0, F_s));
+                Pg = dmin(P_max_flux, dmax(0.0, F_g));
+            }
+        }
+}
+
+void ora_precipitation(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                       ora_state* S, ora_phys* X) {
+    const size_t N = (size_t)P->im * P->jm * P->km;
+    for (size_t c = 0; c < N; c++) {
+        S->Q_precip[c] = 0.0;
+        for (int q = 0; q < 9; q++) ((double*)X->s_precip[q])[c] = 0.0;
+    }
+    for (int q = 0; q < 3; q++) precip_column(P, MC, G, S, X, q);
+}
+
+/* ChemistryJup.h:291-373 (loop mode): per fluid cell, the extent x of NH3 + H2S -> NH4SH that
+ * brings p_NH3 p_H2S to K_p(T) with the latent heat of formation, by bisection. */
+void ora_nh4sh_eq(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                  ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const double R_univ = 8314.46, atm = 101325.0;
+    const double L_f = 4705.0 * log(10.0) * 8314.46 / 51.1114;
+    double *nh3 = X->q[ATJUP_S_NH3], *h2s = X->q[ATJUP_S_H2S], *nh4sh = X->q[ATJUP_S_NH4SH];
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++)
+            for (int i = 0; i < im; i++) {
+                const size_t c = IDX(i, j, k);
+                if (G->solid[c]) continue;
+                const double T0 = S->t[c] * P->t_ref;
+                if (!(T0 > 0.0)) continue;
+                double rho = S->rho_mix[c];
+                if (!(rho > 0.0) || !isfinite(rho)) rho = P->r_mix;
+                const double a = dmax(0.0, nh3[c]) / MC->m_nh3;
+                const double b = dmax(0.0, h2s[c]) / MC->m_h2s;
+                const double s = dmax(0.0, nh4sh[c]) / MC->m_nh4sh;
+                const double heat = L_f * MC->m_nh4sh / (P->cp_mix * rho);
+#define KP_(T_) (pow(10.0, 14.82 - 4705.0 / (T_)) * atm * atm)
+#define F_(x_) ((a - (x_)) * (b - (x_)) * (R_univ * (T0 + heat * (x_))) * (R_univ * (T0 + heat * (x_))) - KP_(T0 + heat * (x_)))
+                const double f0 = F_(0.0);
+                double lo, hi;
+                if (f0 > 0.0) { lo = 0.0; hi = dmin(a, b); }
+                else if (s > 0.0) {
+                    if (F_(-s) <= 0.0) { lo = hi = -s; }
+                    else { lo = -s; hi = 0.0; }
+                } else continue;
+                if (hi > lo)
+                    for (int it = 0; it < 80; it++) {
+                        const double xm = 0.5 * (lo + hi);
+                        if (F_(xm) > 0.0) lo = xm; else hi = xm;
+                        if (hi - lo <= 1.0e-15 * dmax(a, dmax(b, s))) break;
+                    }
+#undef F_
+#undef KP_
+                const double x = (f0 > 0.0) ? lo : hi;
+                if (x == 0.0) continue;
+                nh3[c] = dmax(0.0, nh3[c] - MC->m_nh3 * x);
+                h2s[c] = dmax(0.0, h2s[c] - MC->m_h2s * x);
+                nh4sh[c] = dmax(0.0, nh4sh[c] + MC->m_nh4sh * x);
+                const double dT = heat * x;
+                S->t[c] = (T0 + dT) / P->t_ref;
+            }
+}
+
+/* ChemistryJup.h:756-780: the spherical Laplacian of the diffusive mass fluxes, with the polar
+ * floor on sin(theta) in the metric terms. */
+static double chem_laplacian(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                             const double* c, int i, int j, int k) {
+    const int jm = P->jm, km = P->km;
+    const double rm = G->rad[i];
+    const double exp_rm = 1.0, exp_2_rm = exp_rm * exp_rm;
+    const double sinthe = sin(G->the[j]);
+    const double costhe = cos(G->the[j]);
+    const double rmsinthe = rm * dmax(sinthe, MC->polar_divisor_floor);
+    const double c0 = c[IDX(i, j, k)];
+    const double d2cdr2 = (c[IDX(i + 1, j, k)] - 2.0 * c0 + c[IDX(i - 1, j, k)]) / (P->dr * P->dr) * exp_2_rm;
+    const double d2cdthe2 = (c[IDX(i, j + 1, k)] - 2.0 * c0 + c[IDX(i, j - 1, k)]) / (P->dthe * P->dthe);
+    const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+    const double d2cdphi2 = (c[IDX(i, j, ke)] - 2.0 * c0 + c[IDX(i, j, kw)]) / (P->dphi * P->dphi);
+    const double dcdr = (c[IDX(i + 1, j, k)] - c[IDX(i - 1, j, k)]) / (2.0 * P->dr) * exp_rm;
+    const double dcdthe = (c[IDX(i, j + 1, k)] - c[IDX(i, j - 1, k)]) / (2.0 * P->dthe);
+    return d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) + costhe / (rm * rmsinthe) * dcdthe
+         + d2cdphi2 / (rmsinthe * rmsinthe);
+}
+
+static double superbee_phi(double r) {                /* FluxLimiter.h TVD::superbee_phi */
+    return dmax(0.0, dmax(dmin(2.0 * r, 1.0), dmin(r, 2.0)));
+}
+
+void ora_chemistry(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                   ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const uint8_t* sol = G->solid;
+    double* spec[3] = {X->q[ATJUP_S_H2S], X->q[ATJUP_S_NH3], X->q[ATJUP_S_NH4SH]};
+    const double D[3] = {MC->D_h2s, MC->D_nh3, MC->D_nh4sh};
+    double* mf[3] = {(double*)X->massflux_h2s, (double*)X->massflux_nh3, (double*)X->massflux_nh4sh};
+    /* DiffMassFluxJup (ChemistryJup.h:375-538): only difflux reaches the dynamics */
+    for (int k = 0; k < km - 1; k++)
+        for (int j = 1; j < jm - 1; j++)
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                if (!(S->t[c] > 0.0) || sol[c]) {
+                    for (int q = 0; q < 3; q++) X->difflux[q][c] = 0.0;
+                    continue;
+                }
+                for (int q = 0; q < 3; q++) X->difflux[q][c] = D[q] * chem_laplacian(P, MC, G, spec[q], i, j, k);
+            }
+    for (int q = 0; q < 3; q++) ora_shapiro(P, G, X->difflux[q], 2, 1.0, 1, 1);
+    /* ChemMassRateJup (59-281) with the equilibrium on: the reaction rates are 0 */
+    for (int i = 0; i < im; i++)
+        for (int k = 0; k < km; k++) {
+            for (int j = 0; j < 3; j++)
+                for (int q = 0; q < 3; q++) mf[q][IDX(i, j, k)] = 0.0;
+            for (int j = jm - 3; j < jm; j++)
+                for (int q = 0; q < 3; q++) mf[q][IDX(i, j, k)] = 0.0;
+        }
+    for (int k = 0; k < km - 1; k++)
+        for (int j = 3; j < jm - 3; j++)
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                if (sol[c] && sol[IDX(i - 1, j, k)] && sol[IDX(i + 1, j, k)] && sol[IDX(i, j - 1, k)]
+                    && sol[IDX(i, j + 1, k)] && sol[IDX(i, j, phi_wrap(1, k - 1, km))]
+                    && sol[IDX(i, j, phi_wrap(1, k + 1, km))]) {
+                    for (int q = 0; q < 3; q++) mf[q][c] = 0.0;
+                    continue;
+                }
+                for (int q = 0; q < 3; q++) mf[q][c] = 0.0 + X->difflux[q][c];
+            }
+    /* FluxLimiter<cJupiterModel>::nh4sh (FluxLimiter.h): superbee anti-diffusion of NH4SH */
+    const double* Q = X->q[ATJUP_S_NH4SH];
+    double* fl = (double*)X->fluxlim_nh4sh;
+    const double eps = 1.0e-12;
+    for (int k = 0; k < km - 1; k++)
+        for (int j = 1; j < jm - 1; j++)
+            for (int i = 1; i < im - 1; i++) {
+                const size_t c = IDX(i, j, k);
+                const double q = Q[c];
+                const double q_rp = Q[IDX(i + 1, j, k)], q_rm = Q[IDX(i - 1, j, k)];
+                const double q_tp = Q[IDX(i, j + 1, k)], q_tm = Q[IDX(i, j - 1, k)];
+                const double q_pp = Q[IDX(i, j, phi_wrap(1, k + 1, km))];
+                const double q_pm = Q[IDX(i, j, phi_wrap(1, k - 1, km))];
+                const double u = S->u[c], v = S->v[c], w = S->w[c];
+                const double rm = G->rad[i];
+                const double sinthe = dmax(MC->polar_divisor_floor, fabs(sin(G->the[j])));
+                const double inv_rm = 1.0 / rm;
+                const double inv_rmsinthe = 1.0 / (rm * sinthe);
+                double corr = 0.0;
+                {
+                    const double df = q_rp - q, db = q - q_rm;
+                    const double denom = df + (df >= 0.0 ? eps : -eps);
+                    const double r = (u >= 0.0) ? db / denom
+                                   : ((i + 2 < im ? Q[IDX(i + 2, j, k)] : q_rp) - q_rp) / denom;
+                    corr += (1.0 - superbee_phi(r)) * fabs(u) * (df - db) / (2.0 * P->dr);
+                }
+                {
+                    const double df = q_tp - q, db = q - q_tm;
+                    const double denom = df + (df >= 0.0 ? eps : -eps);
+                    const double q_far = (j + 2 < jm) ? Q[IDX(i, j + 2, k)] : (C43 * q_tp - C13 * q);
+                    const double r = (v >= 0.0) ? db / denom : (q_far - q_tp) / denom;
+                    corr += (1.0 - superbee_phi(r)) * fabs(v) * inv_rm * (df - db) / (2.0 * P->dthe);
+                }
+                {
+                    const double df = q_pp - q, db = q - q_pm;
+                    const double denom = df + (df >= 0.0 ? eps : -eps);
+                    const double r = (w >= 0.0) ? db / denom
+                                   : (Q[IDX(i, j, phi_wrap(1, k + 2, km))] - q_pp) / denom;
+                    corr += (1.0 - superbee_phi(r)) * fabs(w) * inv_rmsinthe * (df - db) / (2.0 * P->dphi);
+                }
+                fl[c] = corr;
+            }
+    for (int q = 0; q < 3; q++) ora_shapiro(P, G, mf[q], 2, 1.0, 1, 1);
+    ora_shapiro(P, G, fl, 2, 1.0, 1, 1);
+}
+
+void ora_clamp_species(const AtjupParams* P, ora_phys* X) {
+    const size_t N = (size_t)P->im * P->jm * P->km;
+    for (int s = 0; s < ATJUP_S_COUNT; s++)
+        for (size_t c = 0; c < N; c++)
+            if (!(X->q[s][c] >= 0.0)) X->q[s][c] = 0.0;
+}

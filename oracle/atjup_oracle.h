@@ -58,6 +58,7 @@ typedef struct {
     double* vel_star;            /* [jm*km] friction velocity (written by ora_turbulence)      */
     double* nue_out;             /* the eddy viscosity ora_turbulence writes (the model's nue)  */
     const float* layer_heights;  /* [im] km                                                     */
+    double* difflux[3];          /* diffusive fluxes of h2s, nh3, nh4sh (chemistry block)      */
 } ora_phys;
 
 /* RungeKutta_Jup_Turb.cpp:47-69 */
@@ -112,6 +113,21 @@ void ora_restore(const AtjupParams* P, ora_state* S);
 void ora_satadj(const AtjupParams* P, const ora_grid* G, const AtjupGasParams* g, double* t,
                 const double* p_stat, const double* rho_mix, double* c, double* cloud,
                 double* ice, long long* counts);
+/* Radiation<cJupiterModel>::run (Radiation.h:251-487) -> S->Q_rad */
+void ora_radiation(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                   ora_phys* X);
+/* Precipitation<cJupiterModel>::run (Precipitation.h:191-445) -> S_precip_*, S->Q_precip */
+void ora_precipitation(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                       ora_state* S, ora_phys* X);
+/* ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373) */
+void ora_nh4sh_eq(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                  ora_phys* X);
+/* The loop's chemistry block with the NH4SH equilibrium on: DiffMassFluxJup's difflux, 1-2-1
+ * smoothing, ChemMassRateJup (massflux = difflux), FluxLimiterNH4SH, smoothing of the fluxes */
+void ora_chemistry(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G, ora_state* S,
+                   ora_phys* X);
+/* clampNegativeSpecies (FileIO_Jup.cpp:494-548) */
+void ora_clamp_species(const AtjupParams* P, ora_phys* X);
 /* One dry iteration of cJupiterModel.cpp:1032-1381 */
 void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
                        int first, int sweeps);

@@ -247,6 +247,26 @@ double ref_scalar(const char* name) {
     if (n == "sc_nh4sh") return m.sc_nh4sh;
     if (n == "rg_nh4sh") return m.rg_nh4sh;
     if (n == "r_p_nh4sh") return m.r_p_nh4sh;
+    if (n == "m_nh3") return m.m_nh3;
+    if (n == "m_h2s") return m.m_h2s;
+    if (n == "m_nh4sh") return m.m_nh4sh;
+    if (n == "D_nh3") return m.mue_nh3 / (m.rg_nh3 * m.sc_nh3);
+    if (n == "D_h2s") return m.mue_h2s / (m.rg_h2s * m.sc_h2s);
+    if (n == "D_nh4sh") return m.mue_nh4sh / (m.rg_nh4sh * m.sc_nh4sh);
+    if (n == "polar_divisor_floor") return ATPhys::polar_divisor_floor<cJupiterModel>();
+    if (n == "rad_F_int") return cJupiterModel::rad_F_int();
+    if (n == "rad_S_solar") return cJupiterModel::rad_S_solar();
+    if (n == "rad_albedo_bond") return cJupiterModel::rad_albedo_bond();
+    if (n == "rad_x_H2") return cJupiterModel::rad_x_H2();
+    if (n == "rad_x_He") return cJupiterModel::rad_x_He();
+    if (n == "rad_cia_strength") return ATPhys::env_double("ATJUP", "CIA_STRENGTH", cJupiterModel::rad_default_cia_strength());
+    if (n == "rad_opacity_strength") return ATPhys::env_double("ATJUP", "OPACITY_STRENGTH", 1.0);
+    if (n == "rad_solar") return ATPhys::env_int("ATJUP", "SOLAR", 1);
+    if (n == "rad_solar_strength") return ATPhys::env_double("ATJUP", "SOLAR_STRENGTH", 1.0);
+    if (n == "rad_sw_tau_per_bar") return ATPhys::env_double("ATJUP", "SW_TAU_PER_BAR", 1.0);
+    if (n == "rad_bottom") return ATPhys::env_int("ATJUP", "RAD_BOTTOM", cJupiterModel::rad_default_bottom());
+    if (n == "precip_rate_scale") return PrecipitationJup::rate_scale();
+    if (n == "precip_coupling_on") return PrecipitationJup::coupling_on() ? 1.0 : 0.0;
     return std::nan("");
 }
 
@@ -314,6 +334,26 @@ void ref_bc_phi() { BC_Jup(*g_m).bcPhi(); }
 void ref_bc_solid() { BC_Jup(*g_m).bcSolidGround(); }
 double ref_balance_v() { return g_m->balanceColumnV(nullptr); }
 void ref_clamp_species() { g_m->clampNegativeSpecies(); }
+void ref_radiation() { RadiationJup(*g_m).run(); }
+void ref_precipitation() { PrecipitationJup(*g_m).run(); }
+void ref_nh4sh_eq() { ChemistryJup(*g_m).EquilibriumNH4SH("loop"); }
+// The chemistry block of the loop (cJupiterModel.cpp:1144-1162 in the order ref_iteration runs
+// it): diffusive fluxes, their 1-2-1 smoothing, the mass rate, the NH4SH flux limiter and the
+// smoothing of the mass fluxes.
+void ref_chem_fluxes() {
+    cJupiterModel& m = *g_m;
+    ChemistryJup(m).DiffMassFluxJup();
+    JupiterUtils::damp_wiggles(m.difflux_h2s, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.difflux_nh3, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.difflux_nh4sh, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.thermalmassflux, &m.i_topography, true, true, true);
+    ChemistryJup(m).ChemMassRateJup();
+    ChemistryJup(m).FluxLimiterNH4SH();
+    JupiterUtils::damp_wiggles(m.massflux_h2s, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.massflux_nh3, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.massflux_nh4sh, &m.i_topography, true, true, true);
+    JupiterUtils::damp_wiggles(m.fluxlim_nh4sh, &m.i_topography, true, true, true);
+}
 void ref_restore() { g_m->restoreVar(1.0); }
 void ref_mixture_density() { g_m->computeMixtureDensity(); }
 void ref_satadj(const char* gas) { gas_adjust(*g_m, gas); }

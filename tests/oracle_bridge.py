@@ -26,6 +26,9 @@ DRY_ENV = {
 
 # Full physics in the RK step: the dry knobs with the k_omega_SST closure switched on.
 PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1"}
+# The full-physics iteration: the closure, radiation, precipitation and the NH4SH equilibrium on
+# (their reference defaults); moist convective adjustment and the cone projection stay off.
+MOIST_ENV = {**PHYS_ENV, "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1", "ATJUP_NH4SH_EQ": "1"}
 
 DYN_FIELDS = ["t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wall_nue",
               "aux_u", "aux_v", "aux_w"]
@@ -240,7 +243,8 @@ class OraPhys(ctypes.Structure):
                 ("acc_dis", _D), ("rhs_tke", _D), ("rhs_dis", _D), ("s_precip", _D * 9),
                 ("massflux_h2s", _D), ("massflux_nh3", _D), ("massflux_nh4sh", _D),
                 ("fluxlim_nh4sh", _D), ("prod", _D), ("tke_source", _D), ("dis_source", _D),
-                ("vel_star", _D), ("nue_out", _D), ("layer_heights", _P(ctypes.c_float))]
+                ("vel_star", _D), ("nue_out", _D), ("layer_heights", _P(ctypes.c_float)),
+                ("difflux", _D * 3)]
 
 
 def oracle_rk4_phys(params, phys, grid: dict, fields: dict) -> dict:
@@ -348,6 +352,54 @@ def oracle_bc(params, grid: dict, fields: dict, steps=("radius", "theta", "phi",
         fn(ctypes.byref(params), ctypes.byref(o.G), ctypes.byref(o.S),
            ctypes.byref(X) if X is not None else None)
         snap = {n: o.f[n].copy() for n in ("t", "u", "v", "w", "p_stat", "p_dyn")}
+        snap.update({n: a.copy() for n, a in keep.items()})
+        out[step] = snap
+    return out
+
+
+MICRO_SPECIES_SOURCES = ("S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+                         "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4",
+                         "S_precip_ch4_cloud", "S_precip_ch4_ice")
+MICRO_FIELDS = ("t", "Q_rad", "Q_precip") + MICRO_SPECIES_SOURCES + (
+    "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
+    "difflux_nh3", "difflux_nh4sh")
+
+
+def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
+    """The microphysics routines in order on copies of fields (steps from radiation,
+    precipitation, nh4sh_eq, chemistry, clamp_species); returns {step: {field: array}}."""
+    from atjup_b200.params import SPECIES
+    f = dict(fields)
+    f.setdefault("Q_rad", np.zeros(np.shape(fields["t"])))
+    f.setdefault("Q_precip", np.zeros(np.shape(fields["t"])))
+    o = Oracle(params, grid, f)
+    shape = o.shape
+    keep = {}
+    names = list(SPECIES) + list(MICRO_SPECIES_SOURCES) + [
+        "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
+        "difflux_nh3", "difflux_nh4sh"]
+    for n in names:
+        keep[n] = np.ascontiguousarray(fields.get(n, np.zeros(shape)), dtype=np.float64).reshape(shape).copy()
+    X = OraPhys()
+    for s_, n in enumerate(SPECIES):
+        X.q[s_] = _dp(keep[n])
+    for s_, n in enumerate(MICRO_SPECIES_SOURCES):
+        X.s_precip[s_] = _dp(keep[n])
+    for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh"):
+        setattr(X, n, _dp(keep[n]))
+    for q, n in enumerate(("difflux_h2s", "difflux_nh3", "difflux_nh4sh")):
+        X.difflux[q] = _dp(keep[n])
+    lh = np.ascontiguousarray(fields["layer_heights"], dtype=np.float32).copy()
+    X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    out = {}
+    for step in steps:
+        fn = getattr(o.lib, "ora_" + step)
+        if step == "clamp_species":
+            fn(ctypes.byref(params), ctypes.byref(X))
+        else:
+            fn(ctypes.byref(params), ctypes.byref(micro), ctypes.byref(o.G), ctypes.byref(o.S),
+               ctypes.byref(X))
+        snap = {n: o.f[n].copy() for n in ("t", "Q_rad", "Q_precip")}
         snap.update({n: a.copy() for n, a in keep.items()})
         out[step] = snap
     return out

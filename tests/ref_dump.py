@@ -24,7 +24,7 @@ import numpy as np
 sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 
-from oracle_bridge import DRY_ENV, DYN_FIELDS, PHYS_ENV, Reference  # noqa: E402
+from oracle_bridge import DRY_ENV, DYN_FIELDS, MICRO_FIELDS, MOIST_ENV, PHYS_ENV, Reference  # noqa: E402
 
 SPECIES = ("h2o", "h2o_cloud", "h2o_ice", "nh3", "nh3_cloud", "nh3_ice",
            "ch4", "ch4_cloud", "ch4_ice")
@@ -179,6 +179,52 @@ def bc_case(ref, g, data, seed=SATADJ_SEED + 3):
             data[f"bc_{step}_{n}"] = ref.get(n)
 
 
+MICRO_CONSTS = ("m_nh3", "m_h2s", "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor",
+                "rad_F_int", "rad_S_solar", "rad_albedo_bond", "rad_x_H2", "rad_x_He",
+                "rad_cia_strength", "rad_opacity_strength", "rad_solar", "rad_solar_strength",
+                "rad_sw_tau_per_bar", "rad_bottom", "precip_rate_scale", "precip_coupling_on")
+
+
+def micro_case(ref, g, data, seed=SATADJ_SEED + 4):
+    """Radiation, precipitation, the NH4SH equilibrium, the chemistry block and the species clamp
+    of one iteration, in the loop's order, on the moist initial state: the species carry seeded
+    noise of 20 % with a few negative cells, NH4SH is seeded in a third of the cells (so it
+    both forms and decomposes), cloud and ice are seeded where there is none (so it rains and
+    snows); the state after each routine is recorded."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    shape = ref.shape
+    fluid = g["solid"] == 0
+    for n in PHYS_FIELDS[:11]:
+        f = ref.get(n)
+        f = np.where(fluid, f * rng.uniform(0.8, 1.2, shape), f)
+        if n.endswith(("_cloud", "_ice")):
+            base = ref.get(n.split("_")[0])
+            f = np.where(fluid & (rng.uniform(size=shape) < 0.3), f + 0.3 * base * rng.uniform(size=shape), f)
+        if n == "nh4sh":
+            f = np.where(fluid & (rng.uniform(size=shape) < 0.3), 1e-4 * rng.uniform(size=shape), f)
+        f = np.where(fluid & (rng.uniform(size=shape) < 0.005), -np.abs(f) - 1e-9, f)
+        ref.set(n, f)
+        data["in_" + n] = f
+    for n in ("u", "v", "w"):
+        data["in_" + n] = ref.get(n)
+    for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
+              "difflux_nh3", "difflux_nh4sh"):
+        data["in_" + n] = ref.get(n)
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for c in MICRO_CONSTS:
+        data["micro_" + c] = np.array(ref.scalar(c))
+    for gas in GASES:
+        cst = np.zeros(14)
+        ref.L.ref_gas_consts(gas.encode(), cst.ctypes.data_as(ctypes.c_void_p))
+        data["gas_" + gas] = cst
+    for step, fn in (("radiation", ref.L.ref_radiation), ("precipitation", ref.L.ref_precipitation),
+                     ("nh4sh_eq", ref.L.ref_nh4sh_eq), ("chemistry", ref.L.ref_chem_fluxes),
+                     ("clamp_species", ref.L.ref_clamp_species)):
+        ref.quiet(fn)
+        for n in MICRO_FIELDS + PHYS_FIELDS[:11]:
+            data[f"mc_{step}_{n}"] = ref.get(n)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -191,15 +237,18 @@ def main():
     ap.add_argument("--rk4-phys", action="store_true")
     ap.add_argument("--turb", action="store_true")
     ap.add_argument("--bc", action="store_true")
+    ap.add_argument("--micro", action="store_true")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
     env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
+    if a.micro:
+        env = dict(MOIST_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -214,6 +263,8 @@ def main():
         turb_case(ref, g, data)
     elif a.bc:
         bc_case(ref, g, data)
+    elif a.micro:
+        micro_case(ref, g, data)
     elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])

@@ -1,0 +1,107 @@
+"""The loop's microphysics: Radiation::run (Radiation.h:251-487), Precipitation::run
+(Precipitation.h:191-445), ChemistryJup::EquilibriumNH4SH (ChemistryJup.h:291-373), the chemistry
+block (DiffMassFluxJup, ChemMassRateJup, FluxLimiterNH4SH and their smoothing) and
+clampNegativeSpecies (FileIO_Jup.cpp:494-548), run in the loop's order.
+
+The oracle is bit-exact with the reference after every routine. The GPU kernels use CUDA's exp,
+pow and sin, contract multiply-adds, and the NH4SH bisection compares f(x) against 0, so a value
+that sits on a decision can move by the bisection's own tolerance (1e-15 of the column's
+concentrations): per field relative L2 <= 1e-12."""
+import numpy as np
+import pytest
+
+from atjup_b200 import synthetic
+from atjup_b200.params import DEFAULT_GASES, SPECIES, resolve_micro, resolve_physics
+from helpers import dump_fields, dump_grid, dump_params, ref_dump, synthetic_case
+from oracle_bridge import MICRO_FIELDS, MOIST_ENV, oracle_micro, rel_l2
+
+MICRO_TOL = 1e-12
+STEPS = ("radiation", "precipitation", "nh4sh_eq", "chemistry", "clamp_species")
+RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "albedo_bond",
+          "rad_x_H2": "x_H2", "rad_x_He": "x_He"}
+
+
+def ref_micro_case():
+    d = ref_dump("--micro")
+    P = dump_params(d, env=MOIST_ENV)
+    consts = {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items() if k.startswith("micro_")}
+    MC = resolve_micro(MOIST_ENV, consts, {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
+    return d, P, MC
+
+
+@pytest.mark.slow
+def test_oracle_micro_bit_exact(ref_required):
+    d, P, MC = ref_micro_case()
+    out = oracle_micro(P, MC, dump_grid(d), dump_fields(d), STEPS)
+    for step in STEPS:
+        for n in MICRO_FIELDS + SPECIES:
+            assert np.array_equal(out[step][n], d[f"mc_{step}_{n}"], equal_nan=True), \
+                f"after {step}: {n} differs from the reference"
+    # the case is not trivial: it rains, NH4SH forms and decomposes, the fluxes are non-zero
+    assert (d["mc_precipitation_S_precip_h2o"] != 0).sum() > 10000
+    dn = d["mc_nh4sh_eq_nh4sh"] - d["mc_precipitation_nh4sh"]
+    assert (dn > 0).sum() > 10000 and (dn < 0).sum() > 10000
+    assert (d["mc_chemistry_fluxlim_nh4sh"] != 0).sum() > 10000
+
+
+def test_resolve_micro_defaults():
+    mc = resolve_micro({})
+    assert (mc.radiation_on, mc.precip_on, mc.nh4sh_eq, mc.solar_on, mc.rad_bottom,
+            mc.precip_coupling_on) == (1, 1, 1, 1, 0, 1)
+    assert mc.cia_strength == 3.9 and mc.D_nh4sh == 0.0 and mc.polar_divisor_floor == 0.4
+    assert mc.gas[2].t_0 == DEFAULT_GASES["CH4"][0]
+    assert resolve_micro({"ATJUP_PRECIP_COUPLING": "0"}).precip_coupling_on == 0
+
+
+def micro_case(im, jm, km, seed=31):
+    P, g, f = synthetic_case(im, jm, km, seed=seed, env=MOIST_ENV)
+    s = dict(f)
+    s["solid"] = g["solid"]
+    f.update(synthetic.physics(s, DEFAULT_GASES, seed=seed + 1))
+    rng = np.random.Generator(np.random.Philox(seed + 2))
+    fluid = g["solid"] == 0
+    shape = f["t"].shape
+    f["nh4sh"] = np.where(fluid & (rng.uniform(size=shape) < 0.3), 1e-4 * rng.uniform(size=shape), 0.0)
+    f["nh3"] = np.where(fluid, f["nh3"] + 2e-3 * rng.uniform(size=shape), 0.0)
+    for n in SPECIES:
+        f[n] = np.where(fluid & (rng.uniform(size=shape) < 0.005), -np.abs(f[n]) - 1e-9, f[n])
+    for n in ("difflux_h2s", "difflux_nh3", "difflux_nh4sh"):
+        f[n] = np.zeros(shape)
+    return P, resolve_physics(MOIST_ENV), resolve_micro(MOIST_ENV), g, f
+
+
+def gpu_micro(P, PH, MC, g, f, steps=STEPS):
+    from atjup_b200.gpu import GpuModel
+    m = GpuModel(P, g)
+    m.set_physics(PH, f["layer_heights"])
+    m.set_micro(MC)
+    m.upload_state(f)
+    out = {}
+    for step in steps:
+        getattr(m, step)()
+        out[step] = {n: m.download(n) for n in MICRO_FIELDS + SPECIES}
+    m.close()
+    return out
+
+
+def check(got, want, where=""):
+    for step in STEPS:
+        for n in MICRO_FIELDS + SPECIES:
+            assert np.isfinite(got[step][n]).all(), f"{where}after {step}: {n} non-finite"
+            r = rel_l2(got[step][n], want[step][n])
+            assert r <= MICRO_TOL, f"{where}after {step}: {n} relative L2 {r:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(13, 37, 49), (41, 61, 97)])
+def test_gpu_micro_matches_oracle(shape):
+    P, PH, MC, g, f = micro_case(*shape)
+    check(gpu_micro(P, PH, MC, g, f), oracle_micro(P, MC, g, f, STEPS), f"{shape}: ")
+
+
+@pytest.mark.gpu
+def test_gpu_micro_matches_reference_full_grid(ref_required):
+    d, P, MC = ref_micro_case()
+    f = dump_fields(d)
+    got = gpu_micro(P, resolve_physics(MOIST_ENV), MC, dump_grid(d), f)
+    check(got, {s: {n: d[f"mc_{s}_{n}"] for n in MICRO_FIELDS + SPECIES} for s in STEPS}, "full grid: ")
