@@ -64,6 +64,7 @@ void free_all(AtjupCtx* c) {
         c->S1[q] = c->S2[q] = c->Sacc[q] = nullptr;
     }
     cudaFree(c->layer_h); c->layer_h = nullptr;
+    cudaFree(c->cos_lat); c->cos_lat = nullptr;
     for (int q = 0; q < 4; q++) {
         cudaFree(c->X1[q]); cudaFree(c->X2[q]); cudaFree(c->acc[q]);
     }
@@ -464,6 +465,46 @@ int atjup_gpu_set_physics(AtjupCtx* c, const AtjupPhysics* ph, const float* laye
     }
     return ATJUP_OK;
 }
+
+int atjup_gpu_set_micro(AtjupCtx* c, const AtjupMicro* mc) {
+    if (!c) { set_error("set_micro: null context"); return ATJUP_ERR_ARG; }
+    if (!mc) { c->micro_on = false; return ATJUP_OK; }
+    if (!mc->nh4sh_eq) {
+        set_error("set_micro: ATJUP_NH4SH_EQ=0 (NH4SH by reaction rates) is not implemented");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    const int jm = c->P.jm;
+    std::vector<double> cl(jm);
+    const double pi_ = 3.14159265358979323846;
+    for (int j = 0; j < jm; j++) {
+        const double s = std::sin(pi_ * (double)j / (double)(jm - 1));
+        cl[j] = (0.0 < s) ? s : 0.0;
+    }
+    if (!c->cos_lat) ATJUP_CUDA(cudaMalloc(&c->cos_lat, sizeof(double) * jm));
+    ATJUP_CUDA(cudaMemcpy(c->cos_lat, cl.data(), sizeof(double) * jm, cudaMemcpyHostToDevice));
+    c->micro = *mc;
+    c->micro_on = true;
+    return ATJUP_OK;
+}
+
+namespace {
+int micro_call(AtjupCtx* c, int what, const char* name) {
+    int rc = need_grid(c, name);
+    if (rc) return rc;
+    if (!c->micro_on || !c->phys_on) {
+        set_error(std::string(name) + ": set the physics and microphysics blocks first");
+        return ATJUP_ERR_ARG;
+    }
+    Timed tm(c, TK_PHYS);
+    return launch_micro(c, what);
+}
+}  // namespace
+
+int atjup_gpu_radiation(AtjupCtx* c) { return micro_call(c, MICRO_RADIATION, "radiation"); }
+int atjup_gpu_precipitation(AtjupCtx* c) { return micro_call(c, MICRO_PRECIP, "precipitation"); }
+int atjup_gpu_nh4sh_equilibrium(AtjupCtx* c) { return micro_call(c, MICRO_NH4SH, "nh4sh_equilibrium"); }
+int atjup_gpu_chemistry(AtjupCtx* c) { return micro_call(c, MICRO_CHEMISTRY, "chemistry"); }
+int atjup_gpu_clamp_species(AtjupCtx* c) { return micro_call(c, MICRO_CLAMP, "clamp_species"); }
 
 int atjup_gpu_turbulence(AtjupCtx* c) {
     int rc = need_grid(c, "turbulence");

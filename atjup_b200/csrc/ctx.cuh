@@ -62,6 +62,10 @@ struct AtjupCtx {
     double* Sacc[ATJUP_S_COUNT + 2] = {};
     float* layer_h = nullptr;
     double turb_taper_dz = 1.0;        // clamp_nue's taper depth (Turbulence.h:569-573) [m]
+    // the loop's microphysics (atjup_gpu_set_micro)
+    bool micro_on = false;
+    AtjupMicro micro{};
+    double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
     double* X2[4] = {};
@@ -150,6 +154,8 @@ int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
 int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin);
 int launch_turbulence(AtjupCtx* c);
+enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP };
+int launch_micro(AtjupCtx* c, int what);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);
 

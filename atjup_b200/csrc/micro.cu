@@ -1,0 +1,456 @@
+// The loop's microphysics on the device: radiation, precipitation, the NH4SH equilibrium, the
+// chemistry mass fluxes and the species clamp.
+//
+//   radiation_kernel      Radiation<cJupiterModel>::run (Radiation.h:251-456)
+//   precip_kernel         Precipitation<cJupiterModel>::run / column (Precipitation.h:191-445)
+//   nh4sh_kernel          ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373)
+//   difflux_kernel        the diffusive fluxes of DiffMassFluxJup (ChemistryJup.h:375-538, 756-780)
+//   massflux_kernel       ChemMassRateJup with the equilibrium on (ChemistryJup.h:59-281)
+//   fluxlim_kernel        FluxLimiter<cJupiterModel>::nh4sh (FluxLimiter.h)
+//   clamp_species_kernel  clampNegativeSpecies (FileIO_Jup.cpp:494-548)
+//
+// Radiation and precipitation are vertical sweeps through a column (the thermal fluxes down then
+// up, the falling hydrometeor fluxes top-down), so each is one thread per (j, k) column, k fastest
+// so that a warp's loads at one level are consecutive, with the column's levels in local arrays
+// and the fluxes carried in registers. The rest are pointwise or 7-point stencils, one thread per
+// cell. The column's sweep order and every expression's operand order follow the reference, and
+// the file is compiled without FMA contraction: the precipitation's fluxes cancel to exactly zero
+// when a layer evaporates all the rain that reaches it, and the next layer branches on that zero.
+#include "ctx.cuh"
+
+namespace atjup {
+namespace {
+
+constexpr int MAX_IM = 64;   // levels a column kernel holds (the reference grid has 41)
+
+__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }
+
+struct MicroArgs {
+    const double *p_stat, *rho_mix, *u, *v, *w;
+    double* t;
+    double* q[ATJUP_S_COUNT];          // species (ATJUP_S_* order)
+    double* sprec[9];
+    double *Q_rad, *Q_precip;
+    double *difflux[3], *massflux[3], *fluxlim;
+    const int32_t* topo;
+    const float* layer_h;
+    const uint8_t* solid;
+    const double* rad;
+    const double* sin_the;             // [jm] sin(the_j)
+    const double* cos_lat;             // [jm] max(0, sin(pi j / (jm - 1))): the solar geometry
+    const GeoIJ* geo;
+    AtjupMicro mc;
+    int im, jm, km, KP, local_rho;
+    double t_ref, g, r_mix, cp_mix, L_atm, u_0, dr, dthe, dphi;
+};
+
+__device__ __forceinline__ double layer_dz_m(const MicroArgs& a, int i) {
+    if (i < 0 || i > a.im - 2) return -1.0;
+    return (double)(a.layer_h[i + 1] - a.layer_h[i]) * 1.0e3;
+}
+
+// ATPhys::saturation_vapour_pressure (ATPhys.h:49-52) [bar]
+__device__ __forceinline__ double svp(double T, double C, double L0, double R, double da, double db) {
+    return exp(C + (-L0 / T + da * log(T) + db * T) / (1e-3 * R));
+}
+
+__global__ void radiation_kernel(MicroArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (k >= a.km) return;
+    const double sigma = 5.670374419e-8, P0_phys = 1.0e5, he_ratio = 0.6, C_cia = 3.5e-6;
+    const double kappa_ch4 = 0.003, kappa_nh3 = 1.5, kappa_cloud = 25.0, kappa_ice = 12.0;
+    const double tau_cloud_cap = 0.4, opac_cal = 0.025, pi_ = 3.14159265358979323846;
+    const AtjupMicro& mc = a.mc;
+    const double comp = mc.x_H2 * mc.x_H2 + he_ratio * mc.x_H2 * mc.x_He;
+    const double cia_coeff = C_cia * mc.cia_strength * comp / a.g;
+    const double opac_mult = mc.opacity_strength;
+    const size_t plane = (size_t)a.jm * a.KP, c0 = (size_t)j * a.KP + k;
+    int i_base = a.topo[(size_t)j * a.km + k];
+    if (i_base < 0) i_base = 0;
+    const int i_top = a.im - 1;
+    if (i_base >= i_top) return;
+    double B[MAX_IM], eps[MAX_IM], Fd[MAX_IM + 1], Fu[MAX_IM + 1], Fsw[MAX_IM + 2];
+    for (int i = i_base; i <= i_top; i++) {
+        const size_t c = c0 + (size_t)i * plane;
+        const double T = a.t[c] * a.t_ref;
+        B[i] = sigma * T * T * T * T;
+        const double P_lo = a.p_stat[c] * P0_phys;
+        const double P_hi = (i < i_top) ? a.p_stat[c + plane] * P0_phys : 0.0;
+        double dP = P_lo - P_hi;
+        if (dP < 0.0) dP = 0.0;
+        const double P_mean = 0.5 * (P_lo + P_hi);
+        const double dm = dP / a.g;
+        const double tau_cia = (T > 0.0) ? cia_coeff * (P_mean / T) * dP : 0.0;
+        const double rho_c = a.rho_mix[c];
+        const double inv_rho = (rho_c > 0.0 && isfinite(rho_c)) ? 1.0 / rho_c : 0.0;
+        const double q_ch4 = dmax(0.0, a.q[ATJUP_S_CH4][c]) * inv_rho;
+        const double q_nh3 = dmax(0.0, a.q[ATJUP_S_NH3][c]) * inv_rho;
+        const double tau_gas = opac_mult * opac_cal * (kappa_ch4 * q_ch4 + kappa_nh3 * q_nh3) * dm;
+        const double q_liq = (dmax(0.0, a.q[ATJUP_S_H2O_CLOUD][c]) + dmax(0.0, a.q[ATJUP_S_NH3_CLOUD][c]) +
+                              dmax(0.0, a.q[ATJUP_S_CH4_CLOUD][c])) * inv_rho;
+        const double q_ice = (dmax(0.0, a.q[ATJUP_S_H2O_ICE][c]) + dmax(0.0, a.q[ATJUP_S_NH3_ICE][c]) +
+                              dmax(0.0, a.q[ATJUP_S_CH4_ICE][c])) * inv_rho;
+        double tau_cloud = opac_mult * opac_cal * (kappa_cloud * q_liq + kappa_ice * q_ice) * dm;
+        if (tau_cloud > tau_cloud_cap) tau_cloud = tau_cloud_cap;
+        eps[i] = 1.0 - exp(-(tau_cia + tau_gas + tau_cloud));
+    }
+    for (int i = i_base; i <= i_top + 1; i++) Fsw[i] = 0.0;
+    if (mc.solar_on != 0) {
+        const double F_sun_toa = mc.solar_strength * mc.S_solar * (1.0 - mc.albedo_bond) * a.cos_lat[j] / pi_;
+        for (int i = i_base; i <= i_top + 1; i++) {
+            const double p_bar = (i <= i_top) ? a.p_stat[c0 + (size_t)i * plane] : 0.0;
+            Fsw[i] = F_sun_toa * exp(-mc.sw_tau_per_bar * dmax(0.0, p_bar));
+        }
+    }
+    Fd[i_top + 1] = 0.0;
+    for (int i = i_top; i >= i_base; i--) Fd[i] = Fd[i + 1] * (1.0 - eps[i]) + eps[i] * B[i];
+    if (mc.rad_bottom == 1) Fu[i_base] = dmax(0.0, 2.0 * B[i_base] - Fd[i_base + 1]);
+    else Fu[i_base] = Fd[i_base] + mc.F_int + Fsw[i_base];
+    for (int i = i_base; i <= i_top; i++) Fu[i + 1] = Fu[i] * (1.0 - eps[i]) + eps[i] * B[i];
+    for (int i = i_base; i <= i_top; i++) {
+        const double net_bot = Fu[i] - Fd[i];
+        const double net_top = Fu[i + 1] - Fd[i + 1];
+        double dz = (i < i_top) ? layer_dz_m(a, i) : layer_dz_m(a, i - 1);
+        if (dz <= 0.0) dz = 1.0;
+        const double Q_sw = (Fsw[i + 1] - Fsw[i]) / dz;
+        a.Q_rad[c0 + (size_t)i * plane] = (net_bot - net_top) / dz + Q_sw;
+    }
+    for (int i = 0; i < i_base; i++) a.Q_rad[c0 + (size_t)i * plane] = 0.0;
+}
+
+__global__ void precip_kernel(MicroArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (k >= a.km) return;
+    const size_t plane = (size_t)a.jm * a.KP, c0 = (size_t)j * a.KP + k;
+    for (int i = 0; i < a.im; i++) {
+        const size_t c = c0 + (size_t)i * plane;
+        a.Q_precip[c] = 0.0;
+        for (int q = 0; q < 9; q++) a.sprec[q][c] = 0.0;
+    }
+    int i_base = a.topo[(size_t)j * a.km + k];
+    if (i_base < 0) i_base = 0;
+    const int i_top = a.im - 1;
+    if (i_base >= i_top) return;
+    const AtjupMicro& mc = a.mc;
+    const double P_max_flux = 1.0e-4, dep_frac = 1.0, ratio_cap = 5.0, rs = mc.precip_rate_scale;
+    const double c_c_au = 2.0e-8, c_i_au = 5.0e-8, q_c_crit = 5.0e-4, c_ac = 1.0e-7;
+    const double c_rim = 1.0e-8, z_csg = 2.5e-8, a_ev = 2.76e-3, c_melt_K = 0.2, c_frz_K = 0.2;
+    const double P_ref = 1.0e-4, v_fall = 2.0;
+    const double nd = (a.L_atm * 1.0e3) / a.u_0;
+    for (int gq = 0; gq < 3; gq++) {
+        const AtjupGasParams& gs = mc.gas[gq];
+        const int sv = gq == 0 ? ATJUP_S_H2O : (gq == 1 ? ATJUP_S_NH3 : ATJUP_S_CH4);
+        double *vap = a.q[sv], *cld = a.q[sv + 1], *ice = a.q[sv + 2];
+        double *Sv = a.sprec[3 * gq], *Sc = a.sprec[3 * gq + 1], *Si = a.sprec[3 * gq + 2];
+        const double Lf = gs.ls - gs.lv;
+        double Pr = 0.0, Ps = 0.0, Pg = 0.0;
+        for (int i = i_top - 1; i >= i_base; i--) {
+            const size_t c = c0 + (size_t)i * plane;
+            const double T = a.t[c] * a.t_ref;
+            const double p_u = a.p_stat[c];
+            const double q_v = dmax(0.0, vap[c]), q_c = dmax(0.0, cld[c]), q_i = dmax(0.0, ice[c]);
+            const double E_r = svp(T, gs.C, gs.L0, gs.R, gs.del_alf, gs.del_bet);
+            double rho = a.r_mix;
+            if (a.local_rho) {
+                const double r = a.rho_mix[c];
+                if (r > 0.0 && isfinite(r)) rho = r;
+            }
+            const double q_sat = (p_u > E_r) ? rho * gs.ep * E_r / p_u : q_v;
+            const double dz = dmax(0.0, layer_dz_m(a, i));
+            if (dz <= 0.0) continue;
+            const double F_r_in = Pr, F_s_in = Ps, F_g_in = Pg;
+            const double Rain = dmin(ratio_cap, F_r_in / P_ref);
+            const double Snow = dmin(ratio_cap, F_s_in / P_ref);
+            const double Graupel = dmin(ratio_cap, F_g_in / P_ref);
+            const double Rain_79 = (Rain > 0.0) ? pow(Rain, 7.0 / 9.0) : 0.0;
+            const double Rain_49 = (Rain > 0.0) ? pow(Rain, 4.0 / 9.0) : 0.0;
+            const bool warm = (T >= gs.t_0);
+            const double S_c_au = (warm && q_c > q_c_crit) ? (rs * c_c_au) * (q_c - q_c_crit) : 0.0;
+            const double S_i_au = (!warm && T >= gs.t_00) ? (rs * c_i_au) * q_i : 0.0;
+            const double S_ac = warm ? (rs * c_ac) * q_c * Rain_79 : 0.0;
+            const double S_s_rim = !warm ? (rs * c_rim) * q_c * Snow : 0.0;
+            const double S_g_rim = !warm ? (rs * c_rim) * q_c * Graupel : 0.0;
+            const double S_csg = (!warm && q_c > q_c_crit) ? (rs * z_csg) * q_c * Snow : 0.0;
+            const double f_melt = warm ? dmin(1.0, c_melt_K * (T - gs.t_0)) : 0.0;
+            const double f_frz = warm ? 0.0 : dmin(1.0, c_frz_K * (gs.t_0 - T));
+            const double F_s_melt = f_melt * F_s_in, F_g_melt = f_melt * F_g_in;
+            const double F_r_frz = f_frz * F_r_in;
+            const double F_r_avail = dmax(0.0, F_r_in - F_r_frz + F_s_melt + F_g_melt + (S_c_au + S_ac) * dz);
+            const double S_ev_raw = (warm && Rain > 0.0 && q_v < q_sat) ? a_ev * (q_sat - q_v) * Rain_49 : 0.0;
+            const double F_ev_sat = dmax(0.0, q_sat - q_v) * v_fall;
+            const double F_ev = dmin(dmin(S_ev_raw * dz, F_r_avail), F_ev_sat);
+            const double S_ev = F_ev / dz;
+            a.Q_precip[c] += Lf * (S_s_rim + S_g_rim + S_csg) + Lf * (F_r_frz - F_s_melt - F_g_melt) / dz -
+                             gs.lv * F_ev / dz;
+            const double tau = dz / v_fall;
+            const double d_c = dmin(dep_frac * q_c, (S_c_au + S_ac + S_s_rim + S_g_rim + S_csg) * tau);
+            const double d_i = dmin(dep_frac * q_i, S_i_au * tau);
+            if (mc.precip_coupling_on) {
+                Sc[c] = -dmax(0.0, d_c) / tau * nd;
+                Si[c] = -dmax(0.0, d_i) / tau * nd;
+                Sv[c] = +S_ev * nd;
+            } else {
+                cld[c] = q_c - dmax(0.0, d_c);
+                ice[c] = q_i - dmax(0.0, d_i);
+                vap[c] = q_v + S_ev * tau;
+            }
+            const double F_r = F_r_in - F_r_frz + F_s_melt + F_g_melt - F_ev + (S_c_au + S_ac) * dz;
+            const double F_s = F_s_in - F_s_melt + (S_i_au + S_s_rim - S_csg) * dz;
+            const double F_g = F_g_in - F_g_melt + F_r_frz + (S_g_rim + S_csg) * dz;
+            Pr = dmin(P_max_flux, dmax(0.0, F_r));
+            Ps = dmin(P_max_flux, dmax(0.0, F_s));
+            Pg = dmin(P_max_flux, dmax(0.0, F_g));
+        }
+    }
+}
+
+// one thread per cell over the padded block; k < km
+__device__ __forceinline__ bool cell_index(const MicroArgs& a, int& i, int& j, int& k, size_t& c) {
+    k = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y;
+    i = blockIdx.z;
+    if (k >= a.km) return false;
+    c = ((size_t)i * a.jm + j) * a.KP + k;
+    return true;
+}
+
+__device__ __forceinline__ double nh4sh_f(double x, double a_, double b_, double T0, double heat) {
+    const double R_univ = 8314.46, atm = 101325.0;
+    const double T = T0 + heat * x, RT = R_univ * T;
+    return (a_ - x) * (b_ - x) * RT * RT - pow(10.0, 14.82 - 4705.0 / T) * atm * atm;
+}
+
+__global__ void nh4sh_kernel(MicroArgs a, double L_f) {
+    int i, j, k;
+    size_t c;
+    if (!cell_index(a, i, j, k, c) || a.solid[c]) return;
+    const AtjupMicro& mc = a.mc;
+    double *nh3 = a.q[ATJUP_S_NH3], *h2s = a.q[ATJUP_S_H2S], *nh4sh = a.q[ATJUP_S_NH4SH];
+    const double T0 = a.t[c] * a.t_ref;
+    if (!(T0 > 0.0)) return;
+    double rho = a.rho_mix[c];
+    if (!(rho > 0.0) || !isfinite(rho)) rho = a.r_mix;
+    const double av = dmax(0.0, nh3[c]) / mc.m_nh3;
+    const double bv = dmax(0.0, h2s[c]) / mc.m_h2s;
+    const double sv = dmax(0.0, nh4sh[c]) / mc.m_nh4sh;
+    const double heat = L_f * mc.m_nh4sh / (a.cp_mix * rho);
+    const double f0 = nh4sh_f(0.0, av, bv, T0, heat);
+    double lo, hi;
+    if (f0 > 0.0) {
+        lo = 0.0;
+        hi = dmin(av, bv);
+    } else if (sv > 0.0) {
+        if (nh4sh_f(-sv, av, bv, T0, heat) <= 0.0) { lo = hi = -sv; }
+        else { lo = -sv; hi = 0.0; }
+    } else {
+        return;
+    }
+    if (hi > lo)
+        for (int it = 0; it < 80; it++) {
+            const double xm = 0.5 * (lo + hi);
+            if (nh4sh_f(xm, av, bv, T0, heat) > 0.0) lo = xm; else hi = xm;
+            if (hi - lo <= 1.0e-15 * dmax(av, dmax(bv, sv))) break;
+        }
+    const double x = (f0 > 0.0) ? lo : hi;
+    if (x == 0.0) return;
+    nh3[c] = dmax(0.0, nh3[c] - mc.m_nh3 * x);
+    h2s[c] = dmax(0.0, h2s[c] - mc.m_h2s * x);
+    nh4sh[c] = dmax(0.0, nh4sh[c] + mc.m_nh4sh * x);
+    a.t[c] = (T0 + heat * x) / a.t_ref;
+}
+
+__global__ void difflux_kernel(MicroArgs a) {
+    int i, j, k;
+    size_t c;
+    if (!cell_index(a, i, j, k, c)) return;
+    if (k > a.km - 2 || j < 1 || j > a.jm - 2 || i < 1 || i > a.im - 2) return;
+    if (!(a.t[c] > 0.0) || a.solid[c]) {
+        for (int q = 0; q < 3; q++) a.difflux[q][c] = 0.0;
+        return;
+    }
+    const double rm = a.rad[i];
+    const double sinthe = a.sin_the[j];
+    const double costhe = a.geo[(size_t)i * a.jm + j].costhe;
+    const double rmsinthe = rm * dmax(sinthe, a.mc.polar_divisor_floor);
+    const size_t plane = (size_t)a.jm * a.KP, row = c - k;
+    const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
+    const double D[3] = {a.mc.D_h2s, a.mc.D_nh3, a.mc.D_nh4sh};
+    const int sp[3] = {ATJUP_S_H2S, ATJUP_S_NH3, ATJUP_S_NH4SH};
+    for (int q = 0; q < 3; q++) {
+        const double* s = a.q[sp[q]];
+        const double c0 = s[c];
+        const double d2cdr2 = (s[c + plane] - 2.0 * c0 + s[c - plane]) / (a.dr * a.dr) * 1.0;
+        const double d2cdthe2 = (s[c + a.KP] - 2.0 * c0 + s[c - a.KP]) / (a.dthe * a.dthe);
+        const double d2cdphi2 = (s[row + ke] - 2.0 * c0 + s[row + kw]) / (a.dphi * a.dphi);
+        const double dcdr = (s[c + plane] - s[c - plane]) / (2.0 * a.dr) * 1.0;
+        const double dcdthe = (s[c + a.KP] - s[c - a.KP]) / (2.0 * a.dthe);
+        const double lap = d2cdr2 + 2.0 / rm * dcdr + d2cdthe2 / (rm * rm) +
+                           costhe / (rm * rmsinthe) * dcdthe + d2cdphi2 / (rmsinthe * rmsinthe);
+        a.difflux[q][c] = D[q] * lap;
+    }
+}
+
+__global__ void massflux_kernel(MicroArgs a) {
+    int i, j, k;
+    size_t c;
+    if (!cell_index(a, i, j, k, c)) return;
+    if (j < 3 || j >= a.jm - 3) {
+        for (int q = 0; q < 3; q++) a.massflux[q][c] = 0.0;
+        return;
+    }
+    if (k > a.km - 2 || i < 1 || i > a.im - 2) return;
+    const size_t plane = (size_t)a.jm * a.KP, row = c - k;
+    const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
+    const uint8_t* S = a.solid;
+    if (S[c] && S[c - plane] && S[c + plane] && S[c - a.KP] && S[c + a.KP] && S[row + kw] && S[row + ke]) {
+        for (int q = 0; q < 3; q++) a.massflux[q][c] = 0.0;
+        return;
+    }
+    for (int q = 0; q < 3; q++) a.massflux[q][c] = 0.0 + a.difflux[q][c];
+}
+
+__device__ __forceinline__ double superbee_phi(double r) {
+    return dmax(0.0, dmax(dmin(2.0 * r, 1.0), dmin(r, 2.0)));
+}
+
+__global__ void fluxlim_kernel(MicroArgs a) {
+    int i, j, k;
+    size_t c;
+    if (!cell_index(a, i, j, k, c)) return;
+    if (k > a.km - 2 || j < 1 || j > a.jm - 2 || i < 1 || i > a.im - 2) return;
+    const double* Q = a.q[ATJUP_S_NH4SH];
+    const size_t plane = (size_t)a.jm * a.KP, row = c - k;
+    const int n = a.km - 1;
+    auto wrap = [&](int kk) { return kk < 0 ? kk + n : (kk >= n ? kk - n : kk); };
+    const double eps = 1.0e-12;
+    const double q = Q[c];
+    const double q_rp = Q[c + plane], q_rm = Q[c - plane], q_tp = Q[c + a.KP], q_tm = Q[c - a.KP];
+    const double q_pp = Q[row + wrap(k + 1)], q_pm = Q[row + wrap(k - 1)];
+    const double u = a.u[c], v = a.v[c], w = a.w[c];
+    const double rm = a.rad[i];
+    const double sinthe = dmax(a.mc.polar_divisor_floor, fabs(a.sin_the[j]));
+    const double inv_rm = 1.0 / rm;
+    const double inv_rmsinthe = 1.0 / (rm * sinthe);
+    double corr = 0.0;
+    {
+        const double df = q_rp - q, db = q - q_rm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        const double r = (u >= 0.0) ? db / denom : ((i + 2 < a.im ? Q[c + 2 * plane] : q_rp) - q_rp) / denom;
+        corr += (1.0 - superbee_phi(r)) * fabs(u) * (df - db) / (2.0 * a.dr);
+    }
+    {
+        const double df = q_tp - q, db = q - q_tm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        const double q_far = (j + 2 < a.jm) ? Q[c + 2 * a.KP] : ((4.0 / 3.0) * q_tp - (1.0 / 3.0) * q);
+        const double r = (v >= 0.0) ? db / denom : (q_far - q_tp) / denom;
+        corr += (1.0 - superbee_phi(r)) * fabs(v) * inv_rm * (df - db) / (2.0 * a.dthe);
+    }
+    {
+        const double df = q_pp - q, db = q - q_pm;
+        const double denom = df + (df >= 0.0 ? eps : -eps);
+        const double r = (w >= 0.0) ? db / denom : (Q[row + wrap(k + 2)] - q_pp) / denom;
+        corr += (1.0 - superbee_phi(r)) * fabs(w) * inv_rmsinthe * (df - db) / (2.0 * a.dphi);
+    }
+    a.fluxlim[c] = corr;
+}
+
+__global__ void clamp_species_kernel(MicroArgs a) {
+    int i, j, k;
+    size_t c;
+    if (!cell_index(a, i, j, k, c)) return;
+    for (int s = 0; s < ATJUP_S_COUNT; s++)
+        if (!(a.q[s][c] >= 0.0)) a.q[s][c] = 0.0;
+}
+
+MicroArgs make_args(AtjupCtx* c) {
+    const AtjupParams& P = c->P;
+    MicroArgs a{};
+    a.t = c->f[ATJUP_F_T];
+    a.p_stat = c->f[ATJUP_F_P_STAT];
+    a.rho_mix = c->f[ATJUP_F_RHO_MIX];
+    a.u = c->f[ATJUP_F_U];
+    a.v = c->f[ATJUP_F_V];
+    a.w = c->f[ATJUP_F_W];
+    for (int s = 0; s < ATJUP_S_COUNT; s++) a.q[s] = c->f[kScalarField[s]];
+    const int sp[9] = {ATJUP_F_S_PRECIP_H2O, ATJUP_F_S_PRECIP_H2O_CLOUD, ATJUP_F_S_PRECIP_H2O_ICE,
+                       ATJUP_F_S_PRECIP_NH3, ATJUP_F_S_PRECIP_NH3_CLOUD, ATJUP_F_S_PRECIP_NH3_ICE,
+                       ATJUP_F_S_PRECIP_CH4, ATJUP_F_S_PRECIP_CH4_CLOUD, ATJUP_F_S_PRECIP_CH4_ICE};
+    for (int q = 0; q < 9; q++) a.sprec[q] = c->f[sp[q]];
+    a.Q_rad = c->f[ATJUP_F_Q_RAD];
+    a.Q_precip = c->f[ATJUP_F_Q_PRECIP];
+    a.difflux[0] = c->f[ATJUP_F_DIFFLUX_H2S];
+    a.difflux[1] = c->f[ATJUP_F_DIFFLUX_NH3];
+    a.difflux[2] = c->f[ATJUP_F_DIFFLUX_NH4SH];
+    a.massflux[0] = c->f[ATJUP_F_MASSFLUX_H2S];
+    a.massflux[1] = c->f[ATJUP_F_MASSFLUX_NH3];
+    a.massflux[2] = c->f[ATJUP_F_MASSFLUX_NH4SH];
+    a.fluxlim = c->f[ATJUP_F_FLUXLIM_NH4SH];
+    a.topo = c->topo;
+    a.layer_h = c->layer_h;
+    a.solid = c->solid;
+    a.rad = c->rad;
+    a.sin_the = c->sin_the;
+    a.cos_lat = c->cos_lat;
+    a.geo = c->geo;
+    a.mc = c->micro;
+    a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP; a.local_rho = P.local_rho;
+    a.t_ref = P.t_ref; a.g = P.g; a.r_mix = P.r_mix; a.cp_mix = P.cp_mix; a.L_atm = P.L_atm;
+    a.u_0 = P.u_0; a.dr = P.dr; a.dthe = P.dthe; a.dphi = P.dphi;
+    return a;
+}
+
+}  // namespace
+
+int launch_micro(AtjupCtx* c, int what) {
+    const AtjupParams& P = c->P;
+    if (P.im > MAX_IM) {
+        set_error("microphysics: more than 64 radial levels");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    MicroArgs a = make_args(c);
+    const int TB = 128;
+    const dim3 gcol((P.km + TB - 1) / TB, P.jm);
+    const dim3 gcell((P.km + TB - 1) / TB, P.jm, P.im);
+    switch (what) {
+    case MICRO_RADIATION:
+        radiation_kernel<<<gcol, TB, 0, c->stream>>>(a);
+        c->launches++;
+        break;
+    case MICRO_PRECIP:
+        precip_kernel<<<gcol, TB, 0, c->stream>>>(a);
+        c->launches++;
+        break;
+    case MICRO_NH4SH:
+        nh4sh_kernel<<<gcell, TB, 0, c->stream>>>(a, 4705.0 * std::log(10.0) * 8314.46 / 51.1114);
+        c->launches++;
+        break;
+    case MICRO_CHEMISTRY: {
+        int rc;
+        difflux_kernel<<<gcell, TB, 0, c->stream>>>(a);
+        c->launches++;
+        ATJUP_CHECK_LAUNCH("difflux_kernel");
+        for (int q = 0; q < 3; q++)
+            if ((rc = launch_shapiro(c, a.difflux[q], 2, 1.0, 1, 1))) return rc;
+        massflux_kernel<<<gcell, TB, 0, c->stream>>>(a);
+        fluxlim_kernel<<<gcell, TB, 0, c->stream>>>(a);
+        c->launches += 2;
+        ATJUP_CHECK_LAUNCH("massflux/fluxlim kernels");
+        for (int q = 0; q < 3; q++)
+            if ((rc = launch_shapiro(c, a.massflux[q], 2, 1.0, 1, 1))) return rc;
+        if ((rc = launch_shapiro(c, a.fluxlim, 2, 1.0, 1, 1))) return rc;
+        break;
+    }
+    case MICRO_CLAMP:
+        clamp_species_kernel<<<gcell, TB, 0, c->stream>>>(a);
+        c->launches++;
+        break;
+    default:
+        set_error("microphysics: unknown routine");
+        return ATJUP_ERR_ARG;
+    }
+    ATJUP_CHECK_LAUNCH("microphysics");
+    return ATJUP_OK;
+}
+
+}  // namespace atjup

@@ -68,6 +68,9 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_restore_scalars.argtypes = [vp]
     L.atjup_gpu_upload2d.argtypes = [vp, i32, vp]
     L.atjup_gpu_turbulence.argtypes = [vp]
+    L.atjup_gpu_set_micro.argtypes = [vp, ctypes.POINTER(_p.AtjupMicro)]
+    for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species"):
+        getattr(L, "atjup_gpu_" + n).argtypes = [vp]
     L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
     _lib = L
     return L
@@ -170,6 +173,30 @@ class GpuModel:
         """Turbulence<cJupiterModel>::run + turbWallOmega (Turbulence.h:307-882,
         cJupiterModel.cpp:360-377)."""
         _check(self.L.atjup_gpu_turbulence(self.ctx))
+
+    def set_micro(self, micro: "_p.AtjupMicro | None") -> None:
+        """atjup_gpu_set_micro: the loop's radiation, precipitation and chemistry."""
+        _check(self.L.atjup_gpu_set_micro(self.ctx, ctypes.byref(micro) if micro is not None else None))
+
+    def radiation(self) -> None:
+        """Radiation<cJupiterModel>::run (Radiation.h:251-487)."""
+        _check(self.L.atjup_gpu_radiation(self.ctx))
+
+    def precipitation(self) -> None:
+        """Precipitation<cJupiterModel>::run (Precipitation.h:191-445)."""
+        _check(self.L.atjup_gpu_precipitation(self.ctx))
+
+    def nh4sh_eq(self) -> None:
+        """ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373)."""
+        _check(self.L.atjup_gpu_nh4sh_equilibrium(self.ctx))
+
+    def chemistry(self) -> None:
+        """The loop's chemistry block (ChemistryJup.h:59-543, FluxLimiter.h)."""
+        _check(self.L.atjup_gpu_chemistry(self.ctx))
+
+    def clamp_species(self) -> None:
+        """clampNegativeSpecies (FileIO_Jup.cpp:494-548)."""
+        _check(self.L.atjup_gpu_clamp_species(self.ctx))
 
     def restore_scalars(self) -> None:
         _check(self.L.atjup_gpu_restore_scalars(self.ctx))

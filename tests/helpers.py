@@ -71,3 +71,4 @@ def gpu_from(p, grid, fields):
     m = GpuModel(p, grid)
     m.upload_state(fields)
     return m
+

@@ -101,7 +101,7 @@ def test_replica_timing_is_max_over_ranks():
     s.bind(("127.0.0.1", 0))
     port = s.getsockname()[1]
     s.close()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:   # no fork of a process that may hold a GPU
         out = mgr.dict()
         mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
         assert out[0] == out[1] == (2.5, 2.5 / 20)
