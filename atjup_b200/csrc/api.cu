@@ -674,16 +674,59 @@ int atjup_gpu_balance_column_v(AtjupCtx* c, double* vshift) {
     return ATJUP_OK;
 }
 
+namespace {
+// live -> time-level-n copy of the transported scalars with the given ATJUP_S_* indices
+int copy_to_n(AtjupCtx* c, const int* idx, int n) {
+    for (int q = 0; q < n; q++) {
+        const int id = kScalarField[idx[q]];
+        ATJUP_CUDA(cudaMemcpyAsync(c->fn[id], c->f[id], c->NP * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return ATJUP_OK;
+}
+
+// The physics part of the even iterations (cJupiterModel.cpp:1054-1162): radiation, the three
+// saturation adjustments, the NH4SH equilibrium, precipitation, the scalar sync of
+// ATJUP_RK_SCALAR_SYNC = 2 (t needs none: its time-level-n copy is the live field on the
+// device), the closure update and the chemistry block.
+int physics_block(AtjupCtx* c) {
+    int rc;
+    const AtjupMicro& mc = c->micro;
+    if (c->micro_on) {
+        if (mc.radiation_on && (rc = atjup_gpu_radiation(c))) return rc;
+        if (mc.satadj_on) {
+            for (int g = ATJUP_GAS_H2O; g <= ATJUP_GAS_CH4; g++)
+                if ((rc = atjup_gpu_satadj(c, g, &mc.gas[g], nullptr))) return rc;
+        }
+        if (mc.nh4sh_eq && (rc = atjup_gpu_nh4sh_equilibrium(c))) return rc;
+        if (mc.precip_on && (rc = atjup_gpu_precipitation(c))) return rc;
+        const int sync[11] = {ATJUP_S_H2O, ATJUP_S_H2O_CLOUD, ATJUP_S_H2O_ICE, ATJUP_S_NH3,
+                              ATJUP_S_NH3_CLOUD, ATJUP_S_NH3_ICE, ATJUP_S_CH4, ATJUP_S_CH4_CLOUD,
+                              ATJUP_S_CH4_ICE, ATJUP_S_H2S, ATJUP_S_NH4SH};
+        if ((rc = copy_to_n(c, sync, mc.nh4sh_eq ? 11 : 9))) return rc;
+    }
+    if (c->phys.turb_on && (rc = atjup_gpu_turbulence(c))) return rc;
+    if (c->micro_on && (rc = atjup_gpu_chemistry(c))) return rc;
+    return ATJUP_OK;
+}
+}  // namespace
+
 int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveOpts* solve) {
     int rc = need_grid(c, "step");
     if (rc) return rc;
     const AtjupParams& P = c->P;
+    const bool ph = c->phys_on;
     if (iter_n % 2 == 0 || first) {
         if ((rc = atjup_gpu_pressure_solve(c, solve, nullptr))) return rc;
         if ((rc = atjup_gpu_mixture_density(c))) return rc;
+        if (ph && (rc = physics_block(c))) return rc;
     }
     if ((rc = atjup_gpu_rk4_step(c, iter_n))) return rc;
     if ((rc = atjup_gpu_bc(c, ATJUP_BC_ALL))) return rc;
+    if (ph && c->phys.turb_on) {                      // ATJUP_TURB_WALL_HOLD 1
+        Timed tm(c, TK_PHYS);
+        if ((rc = launch_turb_wall_hold(c))) return rc;
+    }
     if (P.shapiro_inloop > 0) {
         for (int f = ATJUP_F_U; f <= ATJUP_F_W; f++)
             if ((rc = atjup_gpu_shapiro(c, f, 4, P.shapiro_strength, P.shapiro_inloop, 1))) return rc;
@@ -691,6 +734,11 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
     if (P.v_massbal_stride > 0 && iter_n % P.v_massbal_stride == 0) {
         Timed tm(c, TK_BALANCE_V);
         if ((rc = launch_balance_v(c))) return rc;
+    }
+    if (ph) {
+        // clampNegativeSpecies, then restoreVar of the scalars (the dynamics need none)
+        if (c->micro_on && (rc = atjup_gpu_clamp_species(c))) return rc;
+        if ((rc = atjup_gpu_restore_scalars(c))) return rc;
     }
     return ATJUP_OK;
 }

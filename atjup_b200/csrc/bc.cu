@@ -229,6 +229,9 @@ int launch_bc(AtjupCtx* c, int which) {
         add(L, c->f[ATJUP_F_MASSFLUX_H2S]); add(L, c->f[ATJUP_F_MASSFLUX_NH3]);
         add(L, c->f[ATJUP_F_MASSFLUX_NH4SH]);
         if (fluxlim) add(L, c->f[ATJUP_F_FLUXLIM_NH4SH]);
+        // the diffusive fluxes travel with the mass fluxes in every list that has them
+        add(L, c->f[ATJUP_F_DIFFLUX_H2S]); add(L, c->f[ATJUP_F_DIFFLUX_NH3]);
+        add(L, c->f[ATJUP_F_DIFFLUX_NH4SH]);
     };
     if (which & ATJUP_BC_RADIUS) {
         FieldList L{}, Q{};

@@ -17,6 +17,7 @@
 // the file is compiled without FMA contraction: the precipitation's fluxes cancel to exactly zero
 // when a layer evaporates all the rain that reaches it, and the next layer branches on that zero.
 #include "ctx.cuh"
+#include "dd_exp10.cuh"
 
 namespace atjup {
 namespace {
@@ -215,10 +216,13 @@ __device__ __forceinline__ bool cell_index(const MicroArgs& a, int& i, int& j, i
     return true;
 }
 
+// f(x) of ChemistryJup.h:297-300; K_p = 10^(14.82 - 4705 / T) through the correctly rounded
+// double-double exponential (dd_exp10.cuh), which agrees with the C library's pow in all but
+// ~0.1 % of arguments, so the bisection's last decisions fall the reference's way
 __device__ __forceinline__ double nh4sh_f(double x, double a_, double b_, double T0, double heat) {
     const double R_univ = 8314.46, atm = 101325.0;
     const double T = T0 + heat * x, RT = R_univ * T;
-    return (a_ - x) * (b_ - x) * RT * RT - pow(10.0, 14.82 - 4705.0 / T) * atm * atm;
+    return (a_ - x) * (b_ - x) * RT * RT - ddx::exp10(14.82 - 4705.0 / T) * atm * atm;
 }
 
 __global__ void nh4sh_kernel(MicroArgs a, double L_f) {

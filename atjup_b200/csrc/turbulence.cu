@@ -35,6 +35,7 @@ struct TurbArgs {
     int im, jm, km, KP, model, turb_free, turb_curv, turb_buoy, abl_taper, wall_omega;
     double dr, dthe, dphi, u_0, L_m, nue_max, t_ref, g, cp_mix, re_turb;
     double k_bg_free, vel_star_max, abl_height, taper_dz;
+    int wall_only;                 // column_kernel: the wall law alone (the loop's wall hold)
 };
 
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
@@ -304,6 +305,7 @@ __global__ void column_kernel(TurbArgs a) {
         a.dis[c0] = a.dis[c0 + plane];
         a.nue[c0] = a.nue[c0 + plane];
     }
+    if (a.wall_only) return;
     const double y_surf = height_m(a, i_w);
     for (int i = 0; i < a.im; i++) {
         const size_t c = c0 + (size_t)i * plane;
@@ -367,29 +369,14 @@ __global__ void wall_omega_kernel(TurbArgs a) {
 
 }  // namespace
 
+namespace {
+TurbArgs turb_args(AtjupCtx* c);
+}
+
 int launch_turbulence(AtjupCtx* c) {
     const AtjupParams& P = c->P;
     const AtjupPhysics& H = c->phys;
-    TurbArgs a{};
-    a.u = c->f[ATJUP_F_U]; a.v = c->f[ATJUP_F_V]; a.w = c->f[ATJUP_F_W]; a.t = c->f[ATJUP_F_T];
-    a.tke = c->f[ATJUP_F_TKE]; a.dis = c->f[ATJUP_F_DIS];
-    a.tken = c->fn[ATJUP_F_TKE]; a.disn = c->fn[ATJUP_F_DIS];
-    a.nue = c->f[ATJUP_F_NUE]; a.prod = c->f[ATJUP_F_PROD];
-    a.tke_source = c->f[ATJUP_F_TKE_SOURCE]; a.dis_source = c->f[ATJUP_F_DIS_SOURCE];
-    a.vel_star = c->f2[ATJUP_F2_VEL_STAR];
-    a.flags = c->nbflags; a.geo = c->geo; a.sin_the = c->sin_the; a.rad = c->rad;
-    a.topo = c->topo; a.layer_h = c->layer_h;
-    a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP;
-    a.model = H.turb_model; a.turb_free = H.turb_free; a.turb_curv = H.turb_curv;
-    a.turb_buoy = H.turb_buoy; a.abl_taper = H.abl_taper; a.wall_omega = H.turb_wall_omega;
-    a.dr = P.dr; a.dthe = P.dthe; a.dphi = P.dphi; a.u_0 = P.u_0;
-    a.L_m = P.L_atm * 1.0e3;
-    a.nue_max = H.nue_max_phys / (P.u_0 * a.L_m);
-    a.t_ref = P.t_ref; a.g = P.g; a.cp_mix = P.cp_mix; a.re_turb = H.re_turb;
-    a.k_bg_free = H.turb_k_bg / (P.u_0 * P.u_0);
-    a.vel_star_max = H.vel_star_max;
-    a.abl_height = H.abl_height;
-    a.taper_dz = c->turb_taper_dz;
+    TurbArgs a = turb_args(c);
     const int TB = 128;
     const dim3 bcol((P.km + TB - 1) / TB, P.jm);
     const dim3 bcell((P.km + TB - 1) / TB, P.jm, P.im);
@@ -412,5 +399,52 @@ int launch_turbulence(AtjupCtx* c) {
     ATJUP_CHECK_LAUNCH("turbulence kernels");
     return ATJUP_OK;
 }
+
+// The loop's wall hold after the boundary passes (ATJUP_TURB_WALL_HOLD 1, cJupiterModel.cpp:
+// 1274-1280): apply_wall_bc and turbWallOmega again.
+int launch_turb_wall_hold(AtjupCtx* c) {
+    const AtjupParams& P = c->P;
+    const AtjupPhysics& H = c->phys;
+    TurbArgs a = turb_args(c);
+    a.wall_only = 1;
+    const int TB = 128;
+    const dim3 bcol((P.km + TB - 1) / TB, P.jm);
+    column_kernel<<<bcol, TB, 0, c->stream>>>(a);
+    c->launches++;
+    if (H.turb_wall_omega != 0 && H.turb_model != ATJUP_TURB_K_EPSILON) {
+        wall_omega_kernel<<<bcol, TB, 0, c->stream>>>(a);
+        c->launches++;
+    }
+    ATJUP_CHECK_LAUNCH("turbulence wall hold");
+    return ATJUP_OK;
+}
+
+namespace {
+TurbArgs turb_args(AtjupCtx* c) {
+    const AtjupParams& P = c->P;
+    const AtjupPhysics& H = c->phys;
+    TurbArgs a{};
+    a.u = c->f[ATJUP_F_U]; a.v = c->f[ATJUP_F_V]; a.w = c->f[ATJUP_F_W]; a.t = c->f[ATJUP_F_T];
+    a.tke = c->f[ATJUP_F_TKE]; a.dis = c->f[ATJUP_F_DIS];
+    a.tken = c->fn[ATJUP_F_TKE]; a.disn = c->fn[ATJUP_F_DIS];
+    a.nue = c->f[ATJUP_F_NUE]; a.prod = c->f[ATJUP_F_PROD];
+    a.tke_source = c->f[ATJUP_F_TKE_SOURCE]; a.dis_source = c->f[ATJUP_F_DIS_SOURCE];
+    a.vel_star = c->f2[ATJUP_F2_VEL_STAR];
+    a.flags = c->nbflags; a.geo = c->geo; a.sin_the = c->sin_the; a.rad = c->rad;
+    a.topo = c->topo; a.layer_h = c->layer_h;
+    a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP;
+    a.model = H.turb_model; a.turb_free = H.turb_free; a.turb_curv = H.turb_curv;
+    a.turb_buoy = H.turb_buoy; a.abl_taper = H.abl_taper; a.wall_omega = H.turb_wall_omega;
+    a.dr = P.dr; a.dthe = P.dthe; a.dphi = P.dphi; a.u_0 = P.u_0;
+    a.L_m = P.L_atm * 1.0e3;
+    a.nue_max = H.nue_max_phys / (P.u_0 * a.L_m);
+    a.t_ref = P.t_ref; a.g = P.g; a.cp_mix = P.cp_mix; a.re_turb = H.re_turb;
+    a.k_bg_free = H.turb_k_bg / (P.u_0 * P.u_0);
+    a.vel_star_max = H.vel_star_max;
+    a.abl_height = H.abl_height;
+    a.taper_dz = c->turb_taper_dz;
+    return a;
+}
+}  // namespace
 
 }  // namespace atjup

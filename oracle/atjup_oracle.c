@@ -616,6 +616,12 @@ void ora_mixture_density(const AtjupParams* P, const ora_grid* G, ora_state* S) 
  * thermalmassflux, the force arrays, Q_Latent, Q_Sensible) and chrom (off by default) are not
  * part of it. X == NULL: the dynamics fields only. */
 enum { BCL_RADIUS, BCL_THETA_X, BCL_THETA_Z, BCL_PHI, BCL_SOLID, BCL_SPECIES };
+/* the diffusive chemistry fluxes are in the radius, theta-zero, phi and solid lists */
+static int add_difflux(ora_phys* X, double** L, int n) {
+    for (int q = 0; q < 3; q++)
+        if (X->difflux[q]) L[n++] = X->difflux[q];
+    return n;
+}
 static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
     int n = 0;
     switch (which) {
@@ -627,6 +633,7 @@ static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
             L[n++] = (double*)X->massflux_nh4sh;
             L[n++] = X->tke; L[n++] = X->dis; L[n++] = X->nue_out; L[n++] = X->prod;
             L[n++] = X->tke_source; L[n++] = X->dis_source;
+            n = add_difflux(X, L, n);
         }
         break;
     case BCL_THETA_X:
@@ -642,6 +649,7 @@ static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
         if (X) {
             L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
             L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
+            n = add_difflux(X, L, n);
         }
         break;
     case BCL_PHI:
@@ -652,6 +660,7 @@ static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
             L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
             L[n++] = X->tke; L[n++] = X->dis; L[n++] = X->nue_out; L[n++] = X->prod;
             L[n++] = X->tke_source; L[n++] = X->dis_source;
+            n = add_difflux(X, L, n);
         }
         break;
     case BCL_SOLID:   /* t and p_stat first: they keep their value where nothing is extrapolated */
@@ -660,6 +669,7 @@ static int bc_list(int which, ora_state* S, ora_phys* X, double** L) {
             for (int s = 0; s < ATJUP_S_COUNT; s++) L[n++] = X->q[s];
             L[n++] = (double*)X->massflux_h2s; L[n++] = (double*)X->massflux_nh3;
             L[n++] = (double*)X->massflux_nh4sh; L[n++] = (double*)X->fluxlim_nh4sh;
+            n = add_difflux(X, L, n);
         }
         break;
     case BCL_SPECIES:
@@ -1604,6 +1614,54 @@ void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* 
             }
 }
 
+/* Turbulence.h:383-422 apply_wall_bc: the wall law at the surface cell of obstacle columns, or
+ * (ATJUP_TURB_FREE) row 0 copied from row 1. */
+void ora_turb_wall_bc(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const double C_nue = 0.028, nue_air = 1.8e-5;
+    const double L_m = P->L_atm * 1.0e3;
+    const int model = PH->turb_model;
+    double *TK = X->tke, *DS = X->dis;
+    const double nd_omega = L_m / P->u_0;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            const int i_w = G->topo[(size_t)j * km + k];
+            if (!PH->turb_free && i_w > 0 && i_w < im - 1) {
+                const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
+                const double vs = X->vel_star[(size_t)j * km + k];
+                const size_t cw = IDX(i_w, j, k);
+                TK[cw] = vs * vs / (sqrt(C_nue) * P->u_0 * P->u_0);
+                X->nue_out[cw] = 0.0;
+                if (model == ATJUP_TURB_K_EPSILON) DS[cw] = 0.0;
+                else if (model == ATJUP_TURB_K_OMEGA) DS[cw] = 6.0 * nue_air / (0.075 * y1 * y1) * nd_omega;
+                else DS[cw] = 60.0 * nue_air / (0.0333 * y1 * y1) * nd_omega;
+            } else {
+                TK[IDX(0, j, k)] = TK[IDX(1, j, k)];
+                DS[IDX(0, j, k)] = DS[IDX(1, j, k)];
+                X->nue_out[IDX(0, j, k)] = X->nue_out[IDX(1, j, k)];
+            }
+        }
+}
+
+/* turbWallOmega (cJupiterModel.cpp:360-377): omega* at the surface cell of obstacle columns
+ * from the viscous and log-layer values. */
+void ora_turb_wall_omega(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    if (!(PH->turb_wall_omega != 0 && PH->turb_model != ATJUP_TURB_K_EPSILON)) return;
+    const double nue_air = 1.8e-5, bet_star = 0.09, bet_1 = 0.0333, kappa = 0.41;
+    const double nd_omega = P->L_atm * 1.0e3 / P->u_0;
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) {
+            const int i_w = G->topo[(size_t)j * km + k];
+            if (i_w <= 0 || i_w >= im - 1) continue;
+            const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
+            const double y = 0.5 * y1;
+            const double om_vis = 60.0 * nue_air / (bet_1 * y1 * y1);
+            const double om_log = X->vel_star[(size_t)j * km + k] / (sqrt(bet_star) * kappa * y);
+            X->dis[IDX(i_w, j, k)] = sqrt(om_vis * om_vis + om_log * om_log) * nd_omega;
+        }
+}
+
 /* ---------------------------------------------------------------------------------------------
  * The closure update between steps: Turbulence<cJupiterModel>::run (Turbulence.h:307-328) --
  * compute_vel_star (336-360), compute_sources with the separate clamp passes (614-882) and the
@@ -1859,26 +1917,7 @@ void ora_turbulence(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid
                 X->tke_source[c] = clamp3(X->tke_source[c], -tke_src_max, tke_src_max);
             }
         }
-    /* apply_wall_bc */
-    const double nd_omega = L_m / P->u_0;
-    for (int j = 0; j < jm; j++)
-        for (int k = 0; k < km; k++) {
-            const int i_w = G->topo[(size_t)j * km + k];
-            if (!PH->turb_free && i_w > 0 && i_w < im - 1) {
-                const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
-                const double vs = X->vel_star[(size_t)j * km + k];
-                const size_t cw = IDX(i_w, j, k);
-                TK[cw] = vs * vs / (sqrt(C_nue) * P->u_0 * P->u_0);
-                X->nue_out[cw] = 0.0;
-                if (model == ATJUP_TURB_K_EPSILON) DS[cw] = 0.0;
-                else if (model == ATJUP_TURB_K_OMEGA) DS[cw] = 6.0 * nue_air / (0.075 * y1 * y1) * nd_omega;
-                else DS[cw] = 60.0 * nue_air / (0.0333 * y1 * y1) * nd_omega;
-            } else {
-                TK[IDX(0, j, k)] = TK[IDX(1, j, k)];
-                DS[IDX(0, j, k)] = DS[IDX(1, j, k)];
-                X->nue_out[IDX(0, j, k)] = X->nue_out[IDX(1, j, k)];
-            }
-        }
+    ora_turb_wall_bc(P, PH, G, X);
     /* zero_land_cells */
     for (size_t c = 0; c < N; c++)
         if (sol[c]) {
@@ -1920,20 +1959,7 @@ void ora_turbulence(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid
                     eight[q][IDX(i, jm - 1, k)] = eight[q][IDX(i, jm - 2, k)];
                 }
     }
-    /* turbWallOmega */
-    if (PH->turb_wall_omega != 0 && model != ATJUP_TURB_K_EPSILON) {
-        const double bet_star = 0.09, bet_1 = 0.0333, kappa = 0.41;
-        for (int j = 0; j < jm; j++)
-            for (int k = 0; k < km; k++) {
-                const int i_w = G->topo[(size_t)j * km + k];
-                if (i_w <= 0 || i_w >= im - 1) continue;
-                const double y1 = dmax(layer_dz_m(X, im, i_w - 1 > 0 ? i_w - 1 : 0), 1.0);
-                const double y = 0.5 * y1;
-                const double om_vis = 60.0 * nue_air / (bet_1 * y1 * y1);
-                const double om_log = X->vel_star[(size_t)j * km + k] / (sqrt(bet_star) * kappa * y);
-                DS[IDX(i_w, j, k)] = sqrt(om_vis * om_vis + om_log * om_log) * nd_omega;
-            }
-    }
+    ora_turb_wall_omega(P, PH, G, X);
 #undef HM
 }
 
@@ -2275,4 +2301,61 @@ void ora_clamp_species(const AtjupParams* P, ora_phys* X) {
     for (int s = 0; s < ATJUP_S_COUNT; s++)
         for (size_t c = 0; c < N; c++)
             if (!(X->q[s][c] >= 0.0)) X->q[s][c] = 0.0;
+}
+
+/* One iteration of the loop with the physics on (cJupiterModel.cpp:1032-1381 with the schedule of
+ * the harness: even iterations and the first run the pressure solve, mixture density, radiation,
+ * the three saturation adjustments, the NH4SH equilibrium, precipitation, the scalar sync of
+ * ATJUP_RK_SCALAR_SYNC = 2, the closure update and the chemistry block; every iteration runs RK4,
+ * the boundary passes, the closure's wall law again, the in-loop Shapiro filter, the column
+ * balance of v, the species clamp and restoreVar). S->nue must be X->nue_out. */
+void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const AtjupMicro* MC,
+                        const ora_grid* G, ora_state* S, ora_phys* X, int iter_n, int first,
+                        int sweeps) {
+    const size_t N = (size_t)P->im * P->jm * P->km;
+    if (iter_n % 2 == 0 || first) {
+        ora_pressure_sweeps(P, G, S, sweeps, 1.0, NULL);
+        ora_mixture_density(P, G, S);
+        if (MC->radiation_on) ora_radiation(P, MC, G, S, X);
+        if (MC->satadj_on) {
+            const int sv[3] = {ATJUP_S_H2O, ATJUP_S_NH3, ATJUP_S_CH4};
+            for (int q = 0; q < 3; q++)
+                ora_satadj(P, G, &MC->gas[q], S->t, S->p_stat, S->rho_mix, X->q[sv[q]],
+                           X->q[sv[q] + 1], X->q[sv[q] + 2], NULL);
+        }
+        if (MC->nh4sh_eq) ora_nh4sh_eq(P, MC, G, S, X);
+        if (MC->precip_on) ora_precipitation(P, MC, G, S, X);
+        /* ATJUP_RK_SCALAR_SYNC = 2 */
+        const int sync[9] = {ATJUP_S_H2O, ATJUP_S_H2O_CLOUD, ATJUP_S_H2O_ICE, ATJUP_S_NH3,
+                             ATJUP_S_NH3_CLOUD, ATJUP_S_NH3_ICE, ATJUP_S_CH4, ATJUP_S_CH4_CLOUD,
+                             ATJUP_S_CH4_ICE};
+        for (int q = 0; q < 9; q++) memcpy(X->qn[sync[q]], X->q[sync[q]], sizeof(double) * N);
+        memcpy(S->tn, S->t, sizeof(double) * N);
+        if (MC->nh4sh_eq) {
+            memcpy(X->qn[ATJUP_S_H2S], X->q[ATJUP_S_H2S], sizeof(double) * N);
+            memcpy(X->qn[ATJUP_S_NH4SH], X->q[ATJUP_S_NH4SH], sizeof(double) * N);
+        }
+        if (PH->turb_on) ora_turbulence(P, PH, G, S, X);
+        ora_chemistry(P, MC, G, S, X);
+    }
+    ora_rk4_phys(P, PH, G, S, X);
+    ora_bc_radius_x(P, G, S, X);
+    ora_bc_theta_x(P, G, S, X);
+    ora_bc_phi_x(P, G, S, X);
+    ora_bc_solid_x(P, G, S, X);
+    if (PH->turb_on) {                       /* ATJUP_TURB_WALL_HOLD 1 */
+        ora_turb_wall_bc(P, PH, G, X);
+        ora_turb_wall_omega(P, PH, G, X);
+    }
+    if (P->shapiro_inloop > 0) {
+        ora_shapiro(P, G, S->u, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+        ora_shapiro(P, G, S->v, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+        ora_shapiro(P, G, S->w, 4, P->shapiro_strength, P->shapiro_inloop, 1);
+    }
+    if (P->v_massbal_stride > 0 && iter_n % P->v_massbal_stride == 0) ora_balance_column_v(P, G, S);
+    ora_clamp_species(P, X);
+    ora_restore(P, S);
+    for (int q = 0; q < ATJUP_S_COUNT; q++) memcpy(X->qn[q], X->q[q], sizeof(double) * N);
+    memcpy(X->tken, X->tke, sizeof(double) * N);
+    memcpy(X->disn, X->dis, sizeof(double) * N);
 }

@@ -128,6 +128,13 @@ void ora_chemistry(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G
                    ora_phys* X);
 /* clampNegativeSpecies (FileIO_Jup.cpp:494-548) */
 void ora_clamp_species(const AtjupParams* P, ora_phys* X);
+/* Turbulence.h:383-422 apply_wall_bc and the driver's turbWallOmega (cJupiterModel.cpp:360-377) */
+void ora_turb_wall_bc(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X);
+void ora_turb_wall_omega(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X);
+/* One iteration of cJupiterModel.cpp:1032-1381 with the physics on */
+void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const AtjupMicro* MC,
+                        const ora_grid* G, ora_state* S, ora_phys* X, int iter_n, int first,
+                        int sweeps);
 /* One dry iteration of cJupiterModel.cpp:1032-1381 */
 void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
                        int first, int sweeps);

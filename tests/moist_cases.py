@@ -1,0 +1,48 @@
+"""Shared set-up of the full-physics iteration tests: the reference's moist iterations and a
+small synthetic moist shell, as (params, physics, micro, grid, fields), and a GpuModel built from
+them. Test infrastructure only."""
+import numpy as np
+
+from atjup_b200 import synthetic
+from atjup_b200.params import DEFAULT_GASES, SCALARS, SPECIES, resolve_micro, resolve_physics
+from helpers import dump_fields, dump_grid, dump_params, ref_dump, synthetic_case
+from oracle_bridge import MOIST_ENV
+
+RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "albedo_bond",
+          "rad_x_H2": "x_H2", "rad_x_He": "x_He"}
+PROGNOSTIC = ("t", "u", "v", "w", "p_dyn") + SCALARS
+
+
+def ref_iters_case(iters=3):
+    d = ref_dump("--phys-iters", str(iters))
+    P = dump_params(d, env=MOIST_ENV)
+    P.has_nue = 1
+    P.has_heating = 1
+    MC = resolve_micro(MOIST_ENV, {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items()
+                                   if k.startswith("micro_")},
+                       {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
+    consts = {k[5:]: float(v) for k, v in d.items() if k.startswith("phys_")}
+    consts["abl_height"] = float(d["knobd_abl_height"])
+    return d, P, resolve_physics(MOIST_ENV, consts), MC, dump_grid(d), dump_fields(d)
+
+
+def synthetic_moist_case(im, jm, km, seed=41):
+    P, g, f = synthetic_case(im, jm, km, seed=seed, env=MOIST_ENV)
+    P.has_nue = 1
+    P.has_heating = 1
+    s = dict(f)
+    s["solid"] = g["solid"]
+    f.update(synthetic.physics(s, DEFAULT_GASES, seed=seed + 1))
+    shape = f["t"].shape
+    for n in ("difflux_h2s", "difflux_nh3", "difflux_nh4sh"):
+        f[n] = np.zeros(shape)
+    return P, resolve_physics(MOIST_ENV), resolve_micro(MOIST_ENV), g, f
+
+
+def gpu_moist_model(P, PH, MC, g, f):
+    from atjup_b200.gpu import GpuModel
+    m = GpuModel(P, g)
+    m.set_physics(PH, f["layer_heights"])
+    m.set_micro(MC)
+    m.upload_state(f)
+    return m

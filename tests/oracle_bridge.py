@@ -403,3 +403,59 @@ def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
         snap.update({n: a.copy() for n, a in keep.items()})
         out[step] = snap
     return out
+
+
+def oracle_iteration_phys(params, phys, micro, grid: dict, fields: dict, iters, sweeps=1,
+                          snapshots=()) -> dict:
+    """ora_iteration_phys for iterations 1..iters (the first with first = 1) on copies of fields;
+    returns {iteration: {field: array}} for the iterations in snapshots (and the last)."""
+    from atjup_b200.params import S_PRECIP, SCALARS, SPECIES
+    o = Oracle(params, grid, fields)
+    shape = o.shape
+    keep = {}
+    extra = list(SCALARS) + [n + "n" for n in SCALARS] + ["acc_" + n for n in SCALARS] + \
+        ["rhs_" + n for n in SCALARS] + list(S_PRECIP) + [
+        "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
+        "difflux_nh3", "difflux_nh4sh", "prod", "tke_source", "dis_source"]
+    for n in extra:
+        src = fields.get(n)
+        if src is None and n.endswith("n") and n[:-1] in SCALARS:
+            src = fields.get(n[:-1])
+        keep[n] = np.zeros(shape) if src is None else np.ascontiguousarray(src, dtype=np.float64).reshape(shape).copy()
+    for n in ("nue", "Q_rad", "Q_precip"):
+        if o.f.get(n) is None:
+            o.f[n] = np.zeros(shape)
+            setattr(o.S, n, _dp(o.f[n]))
+    keep["vel_star"] = np.ascontiguousarray(fields["vel_star"], dtype=np.float64).reshape(shape[1:]).copy()
+    lh = np.ascontiguousarray(fields["layer_heights"], dtype=np.float32).copy()
+    X = OraPhys()
+    for s_, n in enumerate(SPECIES):
+        X.q[s_] = _dp(keep[n])
+        X.qn[s_] = _dp(keep[n + "n"])
+        X.acc_q[s_] = _dp(keep["acc_" + n])
+        X.rhs_q[s_] = _dp(keep["rhs_" + n])
+    for a in ("tke", "dis"):
+        setattr(X, a, _dp(keep[a]))
+        setattr(X, a + "n", _dp(keep[a + "n"]))
+        setattr(X, "acc_" + a, _dp(keep["acc_" + a]))
+        setattr(X, "rhs_" + a, _dp(keep["rhs_" + a]))
+    for s_, n in enumerate(S_PRECIP):
+        X.s_precip[s_] = _dp(keep[n])
+    for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "prod",
+              "tke_source", "dis_source", "vel_star"):
+        setattr(X, n, _dp(keep[n]))
+    for q, n in enumerate(("difflux_h2s", "difflux_nh3", "difflux_nh4sh")):
+        X.difflux[q] = _dp(keep[n])
+    X.nue_out = _dp(o.f["nue"])
+    X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    out = {}
+    for it in range(1, iters + 1):
+        o.lib.ora_iteration_phys(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(micro),
+                                 ctypes.byref(o.G), ctypes.byref(o.S), ctypes.byref(X),
+                                 ctypes.c_int(it), ctypes.c_int(1 if it == 1 else 0),
+                                 ctypes.c_int(sweeps))
+        if it in snapshots or it == iters:
+            snap = {n: a.copy() for n, a in o.f.items() if a is not None}
+            snap.update({n: a.copy() for n, a in keep.items()})
+            out[it] = snap
+    return out

@@ -225,6 +225,46 @@ def micro_case(ref, g, data, seed=SATADJ_SEED + 4):
             data[f"mc_{step}_{n}"] = ref.get(n)
 
 
+ITER_FIELDS = ("t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wall_nue", "aux_u",
+               "aux_v", "aux_w") + PHYS_FIELDS + tuple(n + "n" for n in PHYS_FIELDS) + (
+    "nue", "prod", "tke_source", "dis_source", "Q_rad", "Q_precip", "massflux_h2s",
+    "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s", "difflux_nh3",
+    "difflux_nh4sh", "S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+    "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4", "S_precip_ch4_cloud",
+    "S_precip_ch4_ice")
+
+
+def phys_iters_case(ref, g, data, iters):
+    """`iters` iterations of the loop with the physics on (closure, radiation, precipitation, the
+    NH4SH equilibrium, the saturation adjustments), from the reference's own moist initial state;
+    every field the iteration reads is recorded before, every field it writes after."""
+    shape = ref.shape
+    for n in ITER_FIELDS:
+        data["in_" + n] = ref.get(n)
+    if ref.scalar("has_p_baro") == 1.0:
+        data["in_p_baro"] = ref.get1("p_baro").reshape(shape)
+    data["in_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for c in MICRO_CONSTS:
+        data["micro_" + c] = np.array(ref.scalar(c))
+    for c in ("species_diff_scale", "sc_h2o", "sc_h2s", "sc_nh3", "sc_ch4", "sc_nh4sh",
+              "chemical_reaction", "r_p_nh4sh", "rg_nh4sh", "mue_mix", "re_turb"):
+        data["phys_" + c] = np.array(ref.scalar(c))
+    data["knobd_abl_height"] = np.array(ref.L.ref_knob_d(b"abl_height"))
+    for gas in GASES:
+        cst = np.zeros(14)
+        ref.L.ref_gas_consts(gas.encode(), cst.ctypes.data_as(ctypes.c_void_p))
+        data["gas_" + gas] = cst
+    for it in range(1, iters + 1):
+        rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 0)
+        if rc != 0:
+            raise SystemExit(f"ref_iteration rc={rc}")
+        if it in (1, iters):
+            for n in ITER_FIELDS:
+                data[f"it{it}_{n}"] = ref.get(n)
+            data[f"it{it}_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -238,17 +278,20 @@ def main():
     ap.add_argument("--turb", action="store_true")
     ap.add_argument("--bc", action="store_true")
     ap.add_argument("--micro", action="store_true")
+    ap.add_argument("--phys-iters", type=int, default=0)
+    ap.add_argument("--perturb-ulp", action="store_true",
+                    help="with --phys-iters: start from t one ulp above the model's own (fluid cells)")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
     env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
-    if a.micro:
+    if a.micro or a.phys_iters:
         env = dict(MOIST_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro or a.phys_iters))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -265,6 +308,11 @@ def main():
         bc_case(ref, g, data)
     elif a.micro:
         micro_case(ref, g, data)
+    elif a.phys_iters:
+        if a.perturb_ulp:
+            t = ref.get("t")
+            ref.set("t", np.where(g["solid"] == 0, np.nextafter(t, np.inf), t))
+        phys_iters_case(ref, g, data, a.phys_iters)
     elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
