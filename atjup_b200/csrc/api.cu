@@ -421,8 +421,14 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
         if (c->phys_on) {
             // species and closure first: they read the same stage input velocities, and the
             // dynamics stage 3 writes its result over the stage-0 input
-            Timed tm(c, TK_PHYS);
-            if ((rc = launch_phys_stage(c, s, ins[s]))) return rc;
+            if (c->phys.species_on) {
+                Timed tm(c, TK_SPECIES);
+                if ((rc = launch_phys_stage(c, s, ins[s], 0))) return rc;
+            }
+            if (c->phys.turb_on) {
+                Timed tm(c, TK_CLOSURE);
+                if ((rc = launch_phys_stage(c, s, ins[s], 1))) return rc;
+            }
         }
         Timed tm(c, TK_RK_STAGE);
         if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
@@ -495,7 +501,7 @@ int micro_call(AtjupCtx* c, int what, const char* name) {
         set_error(std::string(name) + ": set the physics and microphysics blocks first");
         return ATJUP_ERR_ARG;
     }
-    Timed tm(c, TK_PHYS);
+    Timed tm(c, TK_MICRO);
     return launch_micro(c, what);
 }
 }  // namespace
@@ -513,7 +519,7 @@ int atjup_gpu_turbulence(AtjupCtx* c) {
         set_error("turbulence: the closure is off (atjup_gpu_set_physics with turb_on = 1 first)");
         return ATJUP_ERR_ARG;
     }
-    Timed tm(c, TK_PHYS);
+    Timed tm(c, TK_TURB);
     return launch_turbulence(c);
 }
 
@@ -724,7 +730,7 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
     if ((rc = atjup_gpu_rk4_step(c, iter_n))) return rc;
     if ((rc = atjup_gpu_bc(c, ATJUP_BC_ALL))) return rc;
     if (ph && c->phys.turb_on) {                      // ATJUP_TURB_WALL_HOLD 1
-        Timed tm(c, TK_PHYS);
+        Timed tm(c, TK_TURB);
         if ((rc = launch_turb_wall_hold(c))) return rc;
     }
     if (P.shapiro_inloop > 0) {

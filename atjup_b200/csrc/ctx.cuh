@@ -123,7 +123,7 @@ void set_error(const std::string& msg);
 
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
-       TK_SOLVER, TK_SATADJ, TK_PHYS, TK_COUNT };
+       TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_COUNT };
 void timer_begin(AtjupCtx* c, int cls);
 void timer_end(AtjupCtx* c);
 int cuda_status(cudaError_t e, const char* what);
@@ -152,7 +152,7 @@ int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) 
 int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
-int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin);
+int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin, int what);
 int launch_turbulence(AtjupCtx* c);
 int launch_turb_wall_hold(AtjupCtx* c);
 enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP };

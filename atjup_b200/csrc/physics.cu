@@ -385,7 +385,8 @@ const int kScalarField[ATJUP_S_COUNT + 2] = {
     ATJUP_F_NH3_CLOUD, ATJUP_F_NH3_ICE, ATJUP_F_CH4, ATJUP_F_CH4_CLOUD, ATJUP_F_CH4_ICE,
     ATJUP_F_NH4SH, ATJUP_F_TKE, ATJUP_F_DIS};
 
-int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin) {
+namespace {
+PhysStage stage_args(AtjupCtx* c, int stage, const double* const* vin) {
     const AtjupParams& P = c->P;
     const AtjupPhysics& H = c->phys;
     PhysStage a{};
@@ -455,14 +456,21 @@ int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin) {
     a.has_nue = P.has_nue;
     a.turb_model = H.turb_model;
     a.turb_buoy = H.turb_buoy;
+    return a;
+}
+}  // namespace
+
+// species_stage_kernel of one RK stage (what = 0) or closure_stage_kernel (what = 1)
+int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin, int what) {
+    const AtjupParams& P = c->P;
+    const PhysStage a = stage_args(c, stage, vin);
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
-    if (H.species_on) {
+    if (what == 0) {
         species_stage_kernel<<<grid, block, 0, c->stream>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");
-    }
-    if (H.turb_on) {
+    } else {
         closure_stage_kernel<<<grid, block, 0, c->stream>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("closure_stage_kernel");

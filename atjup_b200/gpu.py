@@ -283,7 +283,7 @@ class GpuModel:
 
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
-                      "mixture", "solver", "satadj", "phys")
+                      "mixture", "solver", "satadj", "species", "closure", "turb", "micro")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

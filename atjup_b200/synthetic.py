@@ -186,6 +186,42 @@ def physics(s: dict, gases: dict, seed: int = 20261206, u_0: float = 100.0,
     return out
 
 
+def full_physics(s: dict, gases: dict, seed: int = 20261207, u_0: float = 100.0,
+                 L_atm: float = 140.0, h2s_fraction: float = 7.0e-4) -> dict:
+    """The full-physics benchmark state on a state from state(): vapour of H2O, NH3, CH4 at 90 % of
+    the liquid saturation density of the cell (the model's vapour-pressure fits) times seeded
+    U(0.95, 1.05), capped at 2 % of the mixture density, no condensate; H2S at h2s_fraction of the
+    mixture density, no NH4SH; k = 1e-4 m2/s2 x U(0.5, 1.5) and omega = 1e-3 1/s x U(0.5, 1.5) in
+    the model's units (k / u_0^2, omega L / u_0); the diagnostic and source fields zero (the
+    iteration computes them); the friction velocity 0.05 m/s and the level heights [km]."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    t, p, rho = s["t"], s["p_stat"], s["rho_mix"]
+    shape = t.shape
+    im = shape[0]
+    fluid = s["solid"] == 0
+    out = {}
+    for gas, cst in gases.items():
+        sat = saturation_density(t * 165.0, p, rho, cst)
+        sat = np.where(np.isfinite(sat), np.minimum(sat, 0.02 * rho), 0.0)
+        name = gas.lower()
+        out[name] = np.where(fluid, 0.9 * sat * rng.uniform(0.95, 1.05, shape), 0.0)
+        out[name + "_cloud"] = np.zeros(shape)
+        out[name + "_ice"] = np.zeros(shape)
+    out["h2s"] = np.where(fluid, h2s_fraction * rho, 0.0)
+    out["nh4sh"] = np.zeros(shape)
+    out["tke"] = np.where(fluid, 1e-4 / u_0 ** 2 * rng.uniform(0.5, 1.5, shape), 0.0)
+    out["dis"] = np.where(fluid, 1e-3 * (L_atm * 1e3 / u_0) * rng.uniform(0.5, 1.5, shape), 0.0)
+    for n in ("nue", "prod", "tke_source", "dis_source", "Q_rad", "Q_precip",
+              "S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
+              "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4", "S_precip_ch4_cloud",
+              "S_precip_ch4_ice", "massflux_h2s", "massflux_nh3", "massflux_nh4sh",
+              "fluxlim_nh4sh", "difflux_h2s", "difflux_nh3", "difflux_nh4sh"):
+        out[n] = np.zeros(shape)
+    out["vel_star"] = np.full(shape[1:], 0.05)
+    out["layer_heights"] = (np.arange(im) * (L_atm / (im - 1))).astype(np.float32)
+    return out
+
+
 def smooth121(f: np.ndarray, passes: int = 3) -> np.ndarray:
     """`passes` Shapiro 1-2-1 passes in k (ring of km-1 meridians, seam copy), then j (clamped at
     the poles), then i (clamped), no fluid floor -- damp_wiggles with i_surface = nullptr

@@ -1,14 +1,20 @@
 #!/usr/bin/env python
-"""Benchmark of ATJUP's time step on B200: one model iteration of the dry configuration.
+"""Benchmark of ATJUP's time step on B200: one model iteration with the full physics.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload phys|dry]
 
-Workload: the dry dynamics configuration on the 41 x 181 x 361 shell (2.68 M cells, FP64):
-each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381) -- the
-red-black pressure pass on even iterations, mixture density, the four RK4 stages, the boundary
-passes, the in-loop 4th-order Shapiro filter of u, v, w and the column balance of v. The state is
-a seeded synthetic one with the shapes and value ranges of the model's own initial state
-(atjup_b200/synthetic.py); it is device-resident when the timed region starts.
+Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 shell (2.68 M
+cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
+on even iterations the red-black pressure pass, mixture density, radiation, the saturation
+adjustment of H2O, NH3 and CH4, the NH4SH equilibrium, precipitation, the k-omega SST closure
+update and the chemistry fluxes; every iteration the four RK4 stages of t, u, v, w, the 11
+species and k*, omega*, the boundary passes, the in-loop 4th-order Shapiro filter of u, v, w, the
+column balance of v and the species clamp. The initial state follows the full-physics recipe
+(atjup_b200/synthetic.py: state + full_physics): vapour at 90 % of saturation with U(0.95, 1.05)
+noise, k = 1e-4 m2/s2 x U(0.5, 1.5), omega = 1e-3 1/s x U(0.5, 1.5), the dynamics perturbations of
+the dry recipe; it is device-resident when the timed region starts. `--workload dry` times the
+dry dynamics iteration instead (microphysics, radiation, closure off).
 
 Prints one JSON line. `value` is seconds per step for the whole job (N replicas: max-over-ranks
 device time / (N * K)); `e2e` is the same metric through the public C ABI with host buffers
@@ -34,30 +40,59 @@ sys.path.insert(0, str(ROOT))
 
 IM, JM, KM = 41, 181, 361
 N_CELLS = IM * JM * KM
-METRIC = "s per RK4 step (dry FP64 dynamics, 41x181x361: one model iteration incl. pressure pass)"
 UNIT = "s/step"
-CONFIG = {
-    "workload": "dry dynamics iteration on the 41x181x361 shell (BASELINE config 0 knobs): "
-                "pressure red-black pass on even iterations, RK4 (4 stages), BCs, 4th-order "
-                "Shapiro on u,v,w, column balance of v",
-    "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
-    "l2": "no flush: inputs larger than L2 (each RK stage streams ~0.47 GB)",
-    "parallelism": "replicas (the path does not shard)",
+METRICS = {
+    "phys": "s per RK4 step (full-physics FP64 iteration, 41x181x361: pressure pass, radiation, "
+            "saturation adjustment, NH4SH, precipitation, k-omega SST, chemistry, RK4 of 17 fields, "
+            "BCs, filters)",
+    "dry": "s per RK4 step (dry FP64 dynamics, 41x181x361: one model iteration incl. pressure pass)",
+}
+CONFIGS = {
+    "phys": {
+        "workload": "full-physics iteration on the 41x181x361 shell (full-physics knobs: closure, "
+                    "radiation, precipitation, saturation adjustment, NH4SH equilibrium on; moist "
+                    "convective adjustment off): the loop's schedule, pressure and physics on even "
+                    "iterations, RK4 of t, u, v, w, 11 species, k*, omega* every iteration",
+        "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
+        "l2": "no flush: inputs larger than L2 (each RK stage streams > 1.8 GB)",
+        "parallelism": "replicas (the path does not shard)",
+    },
+    "dry": {
+        "workload": "dry dynamics iteration on the 41x181x361 shell (BASELINE config 0 knobs): "
+                    "pressure red-black pass on even iterations, RK4 (4 stages), BCs, 4th-order "
+                    "Shapiro on u,v,w, column balance of v",
+        "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
+        "l2": "no flush: inputs larger than L2 (each RK stage streams ~0.47 GB)",
+        "parallelism": "replicas (the path does not shard)",
+    },
 }
 # Algorithmic bytes of one RK stage launch: N * b * (17 F + 4 A) / 4 + N bytes of mask, with
 # F = 4 prognostic fields (t, u, v, w) and A = 5 frozen inputs (p_dyn, p_hydro, p_stat, rho_mix,
 # wall_nue), b = 8 (FP64): one RK4 step of 1.89 GB over its four stage launches.
 RK_STEP_BYTES = N_CELLS * 8 * (17 * 4 + 4 * 5) + 4 * N_CELLS
 RK_STAGE_BYTES = RK_STEP_BYTES / 4
-# DRAM bytes (read + write) of one rk_stage_kernel launch from an ncu capture
-# (profiles/rk_stage_kernel_dry_41x181x361.md); None until captured.
-RK_STAGE_TRAFFIC = None
+# species_stage_kernel, per cell and stage: u, v, w, nue (32 B) and the flag byte, and per species
+# the stage input, the time-level-n value and the stage output (24 B) and the accumulator (12 B
+# averaged over the stages: written at stage 0, read and written at 1 and 2, read at 3), plus the
+# frozen sources: S_precip of 9 species, the mass flux of H2S and NH3, the flux limiter, mass flux
+# and mixture density of NH4SH (112 B): 541 B per cell.
+SPECIES_STAGE_BYTES = N_CELLS * (33 + 11 * 36 + 112)
+# closure_stage_kernel, per cell and stage: u, v, w (24 B), k*, omega* in, n and out (48 B), their
+# accumulators (24 B), nue (8 B), prod and the two sources written at stage 3 (6 B averaged), flags.
+CLOSURE_STAGE_BYTES = N_CELLS * (24 + 48 + 24 + 8 + 6 + 1)
+STAGE_KERNELS = {"rk_stage": ("rk_stage_kernel", RK_STAGE_BYTES),
+                 "species": ("species_stage_kernel", SPECIES_STAGE_BYTES),
+                 "closure": ("closure_stage_kernel", CLOSURE_STAGE_BYTES)}
+# DRAM bytes (read + write) per launch from ncu captures (profiles/); None until captured.
+STAGE_TRAFFIC = {"rk_stage_kernel": None, "species_stage_kernel": None, "closure_stage_kernel": None}
 
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
     "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
     "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
 }
+PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1", "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1",
+            "ATJUP_NH4SH_EQ": "1"}
 
 
 def measured_peak_hbm():
@@ -124,10 +159,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(steps=3, warmup=1):
+def cpu_baseline(workload, steps=3, warmup=1):
     """The reference's own CPU iteration (oracle/_ref) timed on this host's cores."""
     cmd = [sys.executable, str(ROOT / "oracle" / "ref_bench.py"), "--steps", str(steps),
-           "--warmup", str(warmup)]
+           "--warmup", str(warmup)] + (["--phys"] if workload == "phys" else [])
     try:
         out = subprocess.run(cmd, capture_output=True, text=True, timeout=600).stdout
         d = json.loads(out.strip().splitlines()[-1])
@@ -138,23 +173,24 @@ def cpu_baseline(steps=3, warmup=1):
         return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                 "sample": "unavailable: " + d["unavailable"]}
     return {"value": d["s_per_step"], "unit": UNIT, "cores": d["threads"], "kind": "reference",
-            "sample": f"{d['steps']} dry iterations of the reference (built at -O3 from its "
-                      f"sources, OpenMP {d['threads']} threads) after {warmup} warm-up, on its own "
-                      f"initial state"}
+            "sample": f"{d['steps']} {'full-physics' if workload == 'phys' else 'dry'} iterations "
+                      f"of the reference (built at -O3 from its sources, OpenMP {d['threads']} "
+                      f"threads) after {warmup} warm-up, on its own initial state"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cb = cpu_baseline(steps=args.steps, warmup=args.warmup)
+    cb = cpu_baseline(args.workload, steps=args.steps, warmup=args.warmup)
     if cb["value"] is None:
         print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
         return
     v = cb["value"]
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+    line = {"impl": "reference", "metric": METRICS[args.workload], "value": v, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "the reference's own initial state (dry knobs)", "config": CONFIG,
+            "data": f"the reference's own initial state ({args.workload} knobs)",
+            "config": CONFIGS[args.workload],
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -167,6 +203,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="phys", choices=["phys", "dry"])
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -181,7 +218,8 @@ def main():
 
     from atjup_b200 import synthetic
     from atjup_b200.gpu import GpuModel
-    from atjup_b200.params import resolve_params, FIELD_IDS
+    from atjup_b200.params import (DEFAULT_GASES, FIELD_IDS, SCALARS, resolve_micro, resolve_params,
+                                   resolve_physics)
     from atjup_b200.replicas import max_over_ranks, whole_job_seconds_per_step
 
     torch.cuda.set_device(local_rank)
@@ -192,11 +230,19 @@ def main():
         dist = dist_mod
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    P = resolve_params(DRY_ENV, im=IM, jm=JM, km=KM)
+    phys = args.workload == "phys"
+    P = resolve_params(PHYS_ENV if phys else DRY_ENV, im=IM, jm=JM, km=KM)
     s = synthetic.state(IM, JM, KM, seed=20261203 + rank)
     grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
     fields = {k: v for k, v in s.items() if k not in grid}
+    if phys:
+        P.has_nue = 1
+        P.has_heating = 1
+        fields.update(synthetic.full_physics(s, DEFAULT_GASES, seed=20261207 + rank))
     m = GpuModel(P, grid)
+    if phys:
+        m.set_physics(resolve_physics(PHYS_ENV), fields["layer_heights"])
+        m.set_micro(resolve_micro(PHYS_ENV))
     m.upload_state(fields)
     stream = torch.cuda.Stream()
     m.set_stream(stream.cuda_stream)
@@ -234,13 +280,17 @@ def main():
     barrier()
     t_ms = ev0.elapsed_time(ev1)
     launches = m.launch_count() - n0
-    st_ms, st_n = m.timing_read(0)          # rk_stage_kernel
+    per_class = {}
+    for ci, cname in enumerate(m.TIMING_CLASSES):
+        ms, n = m.timing_read(ci)
+        if n:
+            per_class[cname] = (ms, n)
     m.timing(False)
     t_ms = max_over_ranks(t_ms, device="cuda")
     value = whole_job_seconds_per_step(t_ms / 1e3, args.steps, world)
 
     # ---- end to end through the C ABI with pinned host buffers ----
-    names = ["t", "u", "v", "w", "p_dyn"]
+    names = ["t", "u", "v", "w", "p_dyn"] + (list(SCALARS) if phys else [])
     host_in = {n: torch.from_numpy(np.ascontiguousarray(fields[n])).pin_memory() for n in names}
     host_out = {n: torch.empty((IM, JM, KM), dtype=torch.float64).pin_memory() for n in names}
     import ctypes
@@ -266,19 +316,27 @@ def main():
     nbytes = len(names) * N_CELLS * 8
 
     peak, peak_kind = measured_peak_hbm()
-    achieved = (RK_STAGE_BYTES / (st_ms / st_n / 1e3)) / 1e9 if st_n else None
+    # the roofline of the stage kernel with the most device time in the timed region
+    cands = [c for c in STAGE_KERNELS if c in per_class]
+    top = max(cands, key=lambda c: per_class[c][0])
+    kname, kbytes = STAGE_KERNELS[top]
+    st_ms, st_n = per_class[top]
+    achieved = (kbytes / (st_ms / st_n / 1e3)) / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded; shapes and value ranges of the model's initial state)",
-        "config": CONFIG,
-        "roofline": {"kernel": "rk_stage_kernel", "bound": "hbm",
+        "metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; shapes and value ranges of the model's initial state"
+                + (", full-physics recipe" if phys else "") + ")",
+        "config": CONFIGS[args.workload],
+        "roofline": {"kernel": kname, "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None,
+                     "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
-                     "traffic": RK_STAGE_TRAFFIC, "algorithmic_bytes_per_launch": RK_STAGE_BYTES,
-                     "avg_launch_ms": st_ms / st_n if st_n else None, "launches": st_n},
+                     "traffic": STAGE_TRAFFIC[kname], "algorithmic_bytes_per_launch": kbytes,
+                     "avg_launch_ms": st_ms / st_n, "launches": st_n},
+        "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
+                                        sorted(per_class.items(), key=lambda kv: -kv[1][0])},
         "e2e": {"value": whole_job_seconds_per_step(e2e_s, e2e_steps, world), "unit": UNIT,
                 "steps": e2e_steps,
                 "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
@@ -289,7 +347,7 @@ def main():
         dist.barrier()
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(line))
     m.close()
     if dist is not None:

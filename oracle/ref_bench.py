@@ -1,12 +1,14 @@
-"""Time the reference's own CPU implementation of one dry model iteration.
+"""Time the reference's own CPU implementation of one model iteration (dry or full physics).
 
 TEST / BASELINE INFRASTRUCTURE: used only by bench.py's CPU legs (the reference arm and the
 cpu_baseline figure). Runs oracle/_ref/libatjup_ref.so -- the unmodified reference built from its
 sources -- in this process: the reference's initialisation (untimed), `warmup` iterations
-(untimed), then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule for the dry
-configuration, each timed by wall clock on the host. Prints one JSON line.
+(untimed), then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule -- the dry
+configuration, or with --phys the full physics (the closure, radiation, precipitation, the
+saturation adjustments, the NH4SH equilibrium and the chemistry block on; moist convective
+adjustment off) -- each timed by wall clock on the host. Prints one JSON line.
 
-    python oracle/ref_bench.py --steps K --warmup W [--threads T]
+    python oracle/ref_bench.py --steps K --warmup W [--threads T] [--phys]
 """
 from __future__ import annotations
 
@@ -30,16 +32,21 @@ DRY_ENV = {
 }
 
 
+PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1", "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1",
+            "ATJUP_NH4SH_EQ": "1"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--phys", action="store_true")
     a = ap.parse_args()
     if not LIB.exists():
         print(json.dumps({"unavailable": f"{LIB} not built"}))
         return
-    os.environ.update(DRY_ENV)
+    os.environ.update(PHYS_ENV if a.phys else DRY_ENV)
     threads = a.threads or os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
     L = ctypes.CDLL(str(LIB))
@@ -55,7 +62,7 @@ def main():
     times = []
     for it in range(1, a.warmup + a.steps + 1):
         t0 = time.perf_counter()
-        rc = L.ref_iteration(it, 1 if it == 1 else 0, 1)
+        rc = L.ref_iteration(it, 1 if it == 1 else 0, 0 if a.phys else 1)
         dt = time.perf_counter() - t0
         if rc != 0:
             break
