@@ -216,13 +216,22 @@ __device__ __forceinline__ bool cell_index(const MicroArgs& a, int& i, int& j, i
     return true;
 }
 
-// f(x) of ChemistryJup.h:297-300; K_p = 10^(14.82 - 4705 / T) through the correctly rounded
-// double-double exponential (dd_exp10.cuh), which agrees with the C library's pow in all but
-// ~0.1 % of arguments, so the bisection's last decisions fall the reference's way
+// The sign of f(x) of ChemistryJup.h:297-300, the only use the bisection makes of it. K_p =
+// 10^(14.82 - 4705 / T); the reference takes it from the C library's pow, which rounds (nearly
+// always) correctly. CUDA's exp10 is within 1 ulp of 10^y, so B = K_p atm^2 formed from it is
+// within about 4 ulp (1e-15 relative) of B formed from the correctly rounded K_p; when
+// |A - B| exceeds 1e-14 B, the sign of A - B is therefore the correctly rounded one. Only
+// within that margin of the root is K_p recomputed through the correctly rounded
+// double-double exponential (dd_exp10.cuh). Non-finite values fail the margin test and take
+// the double-double path too.
 __device__ __forceinline__ double nh4sh_f(double x, double a_, double b_, double T0, double heat) {
     const double R_univ = 8314.46, atm = 101325.0;
     const double T = T0 + heat * x, RT = R_univ * T;
-    return (a_ - x) * (b_ - x) * RT * RT - ddx::exp10(14.82 - 4705.0 / T) * atm * atm;
+    const double A = (a_ - x) * (b_ - x) * RT * RT;
+    const double y = 14.82 - 4705.0 / T;
+    const double B_fast = exp10(y) * atm * atm;
+    if (fabs(A - B_fast) > 1.0e-14 * B_fast) return A - B_fast;
+    return A - ddx::exp10(y) * atm * atm;
 }
 
 __global__ void nh4sh_kernel(MicroArgs a, double L_f) {

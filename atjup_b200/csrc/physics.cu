@@ -8,12 +8,11 @@
 // species floor at 0, the NaN-safe clamp of k* into [0, k_max], omega* >= 1e-10).
 //
 // A scalar's right-hand side needs its own 7-point stencil, the cell's velocities and nue, and
-// its frozen sources, and no other scalar. So one thread per cell (k fastest, coalesced) loops
-// over the species: per species it reads the stage input at the cell and its six neighbours (the
-// k neighbours come from the warp's own loads, the i and j neighbours mostly from L2, where the
-// three planes a block row touches stay resident), the time-level-n value and the accumulator,
-// and writes the next stage input and the accumulator -- 6 to 8 doubles of DRAM traffic per
-// species per cell per stage. The closure kernel adds the nine velocity gradients its production
+// its frozen sources, and no other scalar. So the species kernel is one thread per cell and
+// species (k fastest, coalesced): it reads the stage input at the cell and its six neighbours (the
+// k neighbours from the warp's own loads, the i and j neighbours mostly from L2), the
+// time-level-n value and the accumulator, and writes the next stage input and the accumulator --
+// 6 to 8 doubles of DRAM traffic per species per cell per stage. The closure kernel adds the nine velocity gradients its production
 // term needs. Both kernels read the same stage input velocities as the dynamics kernel of the
 // stage, and write only scalar buffers, so they are ordered freely against it.
 //
@@ -132,92 +131,139 @@ __device__ __forceinline__ int precip_slot(int s) {
     }
 }
 
-// blockIdx.z = i, blockIdx.y * blockDim.y + threadIdx.y = j, blockIdx.x * blockDim.x + threadIdx.x = k
+// One thread per (cell, species): blockIdx.z = i * ATJUP_S_COUNT + species, so the eleven species
+// blocks of one radial plane run back to back and the plane's u, v, w, nue come from DRAM once and
+// from L2 for the other ten; each species' stencil is its own coalesced stream.
+// blockIdx.y * blockDim.y + threadIdx.y = j, blockIdx.x * blockDim.x + threadIdx.x = k.
 __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
+    const int i = blockIdx.z / ATJUP_S_COUNT;
+    const int s = blockIdx.z - i * ATJUP_S_COUNT;
     if (k >= a.km || j >= a.jm) return;
-    const size_t c0 = ((size_t)i * a.jm + j) * a.KP + k;
-    const uint8_t fl = a.flags[c0];
+    // Every load is issued before the integrated-cell test (one memory round trip, not two):
+    // the neighbour addresses are clamped into the block, so the boundary cells that the test
+    // then sends to the copy below read only their own cell.
+    const size_t plane = (size_t)a.jm * a.KP, row = ((size_t)i * a.jm + j) * a.KP;
+    const size_t c = row + k;
+    const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
+    const size_t cip = (i < a.im - 1) ? c + plane : c, cim = (i > 0) ? c - plane : c;
+    const size_t cjp = (j < a.jm - 1) ? c + a.KP : c, cjm = (j > 0) ? c - a.KP : c;
+    const size_t ckp = row + ke, ckm = row + kw;
+    const double* F = a.q_in[s];
+    const uint8_t fl = a.flags[c];
+    const double f0 = F[c], fip = F[cip], fim = F[cim], fjp = F[cjp], fjm = F[cjm];
+    const double fkp = F[ckp], fkm = F[ckm];
+    const double u0 = a.u[c], v0 = a.v[c], w0 = a.w[c];
+    const double nv = a.has_nue ? a.nue[c] : 0.0;
+    const double qn = a.q_n[s][c];
+    const double acc_in = (a.stage == 0) ? 0.0 : a.acc[s][c];
+    double src0, src1 = 0.0, src2 = 0.0;
+    if (s == ATJUP_S_H2S) {
+        src0 = a.mf_h2s[c];
+    } else if (s == ATJUP_S_NH3) {
+        src0 = a.mf_nh3[c];
+        src1 = a.sprec[3][c];
+    } else if (s == ATJUP_S_NH4SH) {
+        src0 = a.fluxlim[c];
+        src1 = a.mf_nh4sh[c];
+        src2 = a.rho_mix[c];
+    } else {
+        src0 = a.sprec[precip_slot(s)][c];
+    }
     if (!(fl & NB_INT)) {
-        if (a.stage < 3)
-            for (int s = 0; s < ATJUP_S_COUNT; s++) a.q_out[s][c0] = a.q_live[s][c0];
+        if (a.stage < 3) a.q_out[s][c] = a.q_live[s][c];
         return;
     }
-    const Cell x = cell_of(a, i, j, k);
     const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
-    const double u0 = a.u[x.c], v0 = a.v[x.c], w0 = a.w[x.c];
     const double v_invrm = v0 * g.inv_rm;
     const double w_invrs = w0 * g.inv_rmsinthe;
     const double two_inv_rm = 2.0 * g.inv_rm;
     double nue_t = 0.0;
-    if (a.has_nue && a.turb_coupling != 0.0) {
-        const double nv = a.nue[x.c];
-        if (isfinite(nv)) nue_t = a.turb_coupling * dmax(0.0, nv);
-    }
+    if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t = a.turb_coupling * dmax(0.0, nv);
     const double nue_t_s = nue_t / 0.9;
-#pragma unroll 1
-    for (int s = 0; s < ATJUP_S_COUNT; s++) {
-        const double* F = a.q_in[s];
-        const double f0 = F[x.c];
-        const double fip = F[x.cip], fim = F[x.cim], fjp = F[x.cjp], fjm = F[x.cjm];
-        const double fkp = F[x.ckp], fkm = F[x.ckm];
-        const double d1r = (fip - fim) * a.inv_2dr;
-        const double d2r = (fip - 2.0 * f0 + fim) * a.inv_dr2;
-        const double d1t = (fjp - fjm) * a.inv_2dthe;
-        const double d2t = (fjp - 2.0 * f0 + fjm) * a.inv_dthe2;
-        const double d1p = (fkp - fkm) * a.inv_2dphi;
-        const double d2p = (fkp - 2.0 * f0 + fkm) * a.inv_dphi2;
-        const double transport = u0 * d1r + v_invrm * d1t + w_invrs * d1p;
-        const double diffusion = d2r + d1r * two_inv_rm + d2t * g.inv_rm2 +
-                                 d1t * g.costhe_inv_rm2sinthe + d2p * g.inv_rm2sinthe2;
-        const double coef = a.coef[s] + nue_t_s;
-        double r;
-        if (s == ATJUP_S_H2S) {
-            r = -transport + diffusion * coef + a.chemical_reaction * a.mf_h2s[x.c];
-        } else if (s == ATJUP_S_NH3) {
-            r = -transport + diffusion * coef + a.chemical_reaction * a.mf_nh3[x.c] +
-                a.precip_coupling * a.sprec[3][x.c];
-        } else if (s == ATJUP_S_NH4SH) {
-            const double v_stokes = a.stokes_pre * (a.rg_nh4sh - a.rho_mix[x.c]) * a.g / a.mue_mix;
-            r = -transport + a.fluxlim[x.c] + diffusion * coef +
-                a.chemical_reaction * a.mf_nh4sh[x.c] + (v_stokes / a.u_0) * d1r;
-        } else {
-            r = -transport + diffusion * coef + a.precip_coupling * a.sprec[precip_slot(s)][x.c];
-        }
-        rk_update(a, s, x.c, r);
+    const double d1r = (fip - fim) * a.inv_2dr;
+    const double d2r = (fip - 2.0 * f0 + fim) * a.inv_dr2;
+    const double d1t = (fjp - fjm) * a.inv_2dthe;
+    const double d2t = (fjp - 2.0 * f0 + fjm) * a.inv_dthe2;
+    const double d1p = (fkp - fkm) * a.inv_2dphi;
+    const double d2p = (fkp - 2.0 * f0 + fkm) * a.inv_dphi2;
+    const double transport = u0 * d1r + v_invrm * d1t + w_invrs * d1p;
+    const double diffusion = d2r + d1r * two_inv_rm + d2t * g.inv_rm2 +
+                             d1t * g.costhe_inv_rm2sinthe + d2p * g.inv_rm2sinthe2;
+    const double coef = a.coef[s] + nue_t_s;
+    double r;
+    if (s == ATJUP_S_H2S) {
+        r = -transport + diffusion * coef + a.chemical_reaction * src0;
+    } else if (s == ATJUP_S_NH3) {
+        r = -transport + diffusion * coef + a.chemical_reaction * src0 + a.precip_coupling * src1;
+    } else if (s == ATJUP_S_NH4SH) {
+        const double v_stokes = a.stokes_pre * (a.rg_nh4sh - src2) * a.g / a.mue_mix;
+        r = -transport + src0 + diffusion * coef + a.chemical_reaction * src1 +
+            (v_stokes / a.u_0) * d1r;
+    } else {
+        r = -transport + diffusion * coef + a.precip_coupling * src0;
+    }
+    // RK bookkeeping (RungeKutta_Jup_Turb.cpp:425-490, 493-568), the accumulator read above
+    const double accv = (a.stage == 0) ? a.wgt * r : acc_in + a.wgt * r;
+    if (a.stage < 3) {
+        a.acc[s][c] = accv;
+        a.q_out[s][c] = qn + a.c_in * r;
+    } else {
+        const double x = qn + a.dt * accv * a.one_sixth;
+        a.q_out[s][c] = (s == ATJUP_S_NH4SH) ? ((x < 0.0) ? 0.0 : x) : dmax(0.0, x);
     }
 }
 
 // k*, omega*: transport, diffusion with the model's coefficients, and the closure sources
+// one instantiation per closure model, so that each holds the registers of its own branch only
+template <int MODEL>
 __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
     if (k >= a.km || j >= a.jm) return;
     const int ST = ATJUP_S_COUNT, SD = ATJUP_S_COUNT + 1;
-    const size_t c0 = ((size_t)i * a.jm + j) * a.KP + k;
-    const uint8_t fl = a.flags[c0];
-    if (!(fl & NB_INT)) {
-        if (a.stage < 3) {
-            a.q_out[ST][c0] = a.q_live[ST][c0];
-            a.q_out[SD][c0] = a.q_live[SD][c0];
-        }
-        return;
-    }
-    const Cell x = cell_of(a, i, j, k);
-    const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
+    // Every load is issued before the integrated-cell test (one memory round trip): the
+    // neighbour addresses are clamped into the block, so boundary cells read only their own
+    // cell before the test sends them to the copy below.
+    Cell x = cell_of(a, i, j, k);
+    if (i == a.im - 1) x.cip = x.c;
+    if (i == 0) x.cim = x.c;
+    if (j == a.jm - 1) x.cjp = x.c;
+    if (j == 0) x.cjm = x.c;
+    const uint8_t fl = a.flags[x.c];
     const double* TK = a.q_in[ST];
     const double* DS = a.q_in[SD];
     const double tk0 = TK[x.c], ds0 = DS[x.c];
+    const double tip_ = TK[x.cip], tim_ = TK[x.cim], tjp_ = TK[x.cjp], tjm_ = TK[x.cjm];
+    const double tkp_ = TK[x.ckp], tkm_ = TK[x.ckm];
+    const double dip_ = DS[x.cip], dim_ = DS[x.cim], djp_ = DS[x.cjp], djm_ = DS[x.cjm];
+    const double dkp_ = DS[x.ckp], dkm_ = DS[x.ckm];
+    const double u0 = a.u[x.c], v0 = a.v[x.c], w0 = a.w[x.c];
+    const double uip = a.u[x.cip], uim = a.u[x.cim], vip = a.v[x.cip], vim = a.v[x.cim];
+    const double wip = a.w[x.cip], wim = a.w[x.cim];
+    const double ujp = a.u[x.cjp], ujm = a.u[x.cjm], vjp = a.v[x.cjp], vjm = a.v[x.cjm];
+    const double wjp = a.w[x.cjp], wjm = a.w[x.cjm];
+    const double ukp = a.u[x.ckp], ukm = a.u[x.ckm], vkp = a.v[x.ckp], vkm = a.v[x.ckm];
+    const double wkp = a.w[x.ckp], wkm = a.w[x.ckm];
+    const double nv = a.nue[x.c];
+    const int32_t topo = a.topo[(size_t)j * a.km + k];
+    if (!(fl & NB_INT)) {
+        if (a.stage < 3) {
+            a.q_out[ST][x.c] = a.q_live[ST][x.c];
+            a.q_out[SD][x.c] = a.q_live[SD][x.c];
+        }
+        return;
+    }
+    const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
     // the solid-face mirror (RHS_Jup_Turb.cpp:257-303): a solid neighbour reads as the cell
-    const double tip = (fl & NB_IP) ? tk0 : TK[x.cip], tim = (fl & NB_IM) ? tk0 : TK[x.cim];
-    const double tjp = (fl & NB_JP) ? tk0 : TK[x.cjp], tjm = (fl & NB_JM) ? tk0 : TK[x.cjm];
-    const double tkp = (fl & NB_KP) ? tk0 : TK[x.ckp], tkm = (fl & NB_KM) ? tk0 : TK[x.ckm];
-    const double dip = (fl & NB_IP) ? ds0 : DS[x.cip], dim = (fl & NB_IM) ? ds0 : DS[x.cim];
-    const double djp = (fl & NB_JP) ? ds0 : DS[x.cjp], djm = (fl & NB_JM) ? ds0 : DS[x.cjm];
-    const double dkp = (fl & NB_KP) ? ds0 : DS[x.ckp], dkm = (fl & NB_KM) ? ds0 : DS[x.ckm];
+    const double tip = (fl & NB_IP) ? tk0 : tip_, tim = (fl & NB_IM) ? tk0 : tim_;
+    const double tjp = (fl & NB_JP) ? tk0 : tjp_, tjm = (fl & NB_JM) ? tk0 : tjm_;
+    const double tkp = (fl & NB_KP) ? tk0 : tkp_, tkm = (fl & NB_KM) ? tk0 : tkm_;
+    const double dip = (fl & NB_IP) ? ds0 : dip_, dim = (fl & NB_IM) ? ds0 : dim_;
+    const double djp = (fl & NB_JP) ? ds0 : djp_, djm = (fl & NB_JM) ? ds0 : djm_;
+    const double dkp = (fl & NB_KP) ? ds0 : dkp_, dkm = (fl & NB_KM) ? ds0 : dkm_;
     const double dtkedr = (tip - tim) * a.inv_2dr, d2tkedr2 = (tip - 2.0 * tk0 + tim) * a.inv_dr2;
     const double ddisdr = (dip - dim) * a.inv_2dr, d2disdr2 = (dip - 2.0 * ds0 + dim) * a.inv_dr2;
     const double dtkedthe = (tjp - tjm) * a.inv_2dthe;
@@ -229,16 +275,15 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
     const double ddisdphi = (dkp - dkm) * a.inv_2dphi;
     const double d2disdphi2 = (dkp - 2.0 * ds0 + dkm) * a.inv_dphi2;
 
-    const double u0 = a.u[x.c], v0 = a.v[x.c], w0 = a.w[x.c];
-    const double dudr = (a.u[x.cip] - a.u[x.cim]) * a.inv_2dr;
-    const double dvdr = (a.v[x.cip] - a.v[x.cim]) * a.inv_2dr;
-    const double dwdr = (a.w[x.cip] - a.w[x.cim]) * a.inv_2dr;
-    const double dudthe = (a.u[x.cjp] - a.u[x.cjm]) * a.inv_2dthe;
-    const double dvdthe = (a.v[x.cjp] - a.v[x.cjm]) * a.inv_2dthe;
-    const double dwdthe = (a.w[x.cjp] - a.w[x.cjm]) * a.inv_2dthe;
-    const double dudphi = (a.u[x.ckp] - a.u[x.ckm]) * a.inv_2dphi;
-    const double dvdphi = (a.v[x.ckp] - a.v[x.ckm]) * a.inv_2dphi;
-    const double dwdphi = (a.w[x.ckp] - a.w[x.ckm]) * a.inv_2dphi;
+    const double dudr = (uip - uim) * a.inv_2dr;
+    const double dvdr = (vip - vim) * a.inv_2dr;
+    const double dwdr = (wip - wim) * a.inv_2dr;
+    const double dudthe = (ujp - ujm) * a.inv_2dthe;
+    const double dvdthe = (vjp - vjm) * a.inv_2dthe;
+    const double dwdthe = (wjp - wjm) * a.inv_2dthe;
+    const double dudphi = (ukp - ukm) * a.inv_2dphi;
+    const double dvdphi = (vkp - vkm) * a.inv_2dphi;
+    const double dwdphi = (wkp - wkm) * a.inv_2dphi;
     const double v_invrm = v0 * g.inv_rm;
     const double w_invrs = w0 * g.inv_rmsinthe;
     const double two_inv_rm = 2.0 * g.inv_rm;
@@ -251,7 +296,6 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
 
     const double C_nue = 0.028, dis_min = 1.0e-10, nue_gas_phys = 1.8e-5;
     const double L_m = a.L_m;
-    const double nv = a.nue[x.c];
     const double nue_here = isfinite(nv) ? dmax(0.0, nv) : 0.0;
     const double tke_s = dmax(tk0, dis_min);
     const double dis_s = dmax(ds0, dis_min);
@@ -263,7 +307,7 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
     const double dtkedthe_s = dtkedthe * g.inv_rm, ddisdthe_s = ddisdthe * g.inv_rm;
     const double dtkedphi_s = dtkedphi * g.inv_rmsinthe, ddisdphi_s = ddisdphi * g.inv_rmsinthe;
     const double grad_dot = dtkedr * ddisdr + dtkedthe_s * ddisdthe_s + dtkedphi_s * ddisdphi_s;
-    double cnue = (a.turb_model == ATJUP_TURB_K_EPSILON) ? C_nue * tke_s * tke_s / dis_s
+    double cnue = (MODEL == ATJUP_TURB_K_EPSILON) ? C_nue * tke_s * tke_s / dis_s
                                                          : tke_s / dis_s;
     cnue = dmin(cnue, a.nue_max);
     const double der = 0.66667 * (dudr_s + dvdthe_s + dwdphi_s);
@@ -278,13 +322,13 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
         + (cnue * (dwdr_s + dudphi_s)) * dwdr_s
         + (cnue * (dwdthe_s + dvdphi_s)) * dwdthe_s);
 
-    const double y_mount = layer_h(a, a.topo[(size_t)j * a.km + k]) * 1.0e3;
+    const double y_mount = layer_h(a, topo) * 1.0e3;
     const double dz_layer = dmax(1.0, layer_dz_m(a, i - 1 > 0 ? i - 1 : 0));
     const double y_phys = dmax(layer_h(a, i) * 1.0e3 - y_mount, dz_layer);
     const double y_star = y_phys / L_m;
 
     double dtre, ddre, tke_src, dis_src, c_w_prod;
-    if (a.turb_model == ATJUP_TURB_K_EPSILON) {               // Chien 1982
+    if (MODEL == ATJUP_TURB_K_EPSILON) {               // Chien 1982
         const double sig_k = 1.0, sig_w = 1.3, C_eps_1 = 1.35, C_eps_2 = 1.80;
         dtre = a.inv_re + nue_here / sig_k;
         ddre = a.inv_re + nue_here / sig_w;
@@ -299,7 +343,7 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
         tke_src = P_full - ds0 + L_k / a.re_turb;
         dis_src = P_w - Y_w + L_w / a.re_turb;
         c_w_prod = C_eps_1;
-    } else if (a.turb_model == ATJUP_TURB_K_OMEGA) {          // Wilcox
+    } else if (MODEL == ATJUP_TURB_K_OMEGA) {          // Wilcox
         const double sig_k = 0.6, sig_w = 0.5, bet_star = 0.09, gam = 0.52, bet_0 = 0.0708;
         dtre = a.inv_re + sig_k * nue_here;
         ddre = a.inv_re + sig_w * nue_here;
@@ -313,7 +357,8 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
         const double W13 = dudphi_s - dwdr_s;
         const double W23 = dvdphi_s - dwdthe_s;
         const double Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
-        const double chi_w = fabs(Omega * Omega * S_mag / pow(bet_star * dis_s, 3));
+        const double bd = bet_star * dis_s;
+        const double chi_w = fabs(Omega * Omega * S_mag / (bd * bd * bd));   // pow(bd, 3)
         const double f_bet = (1.0 + 85.0 * chi_w) / (1.0 + 100.0 * chi_w);
         const double bet_wc = bet_0 * f_bet;
         const double sig_d = (grad_dot <= 0.0) ? 0.0 : 0.125;
@@ -333,7 +378,8 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
         const double arg1 = dmin(dmax(sqrt(dmax(tk0, 0.0)) / (bet_star * dis_s * y_star),
                                       500.0 * nue_air_nd / (y_star * y_star * dis_s)),
                                  4.0 * sig_w2 * tke_s / (CD_kw * y_star * y_star));
-        const double F1 = tanh(pow(arg1, 4));
+        const double a2 = arg1 * arg1;
+        const double F1 = tanh(a2 * a2);                                     // pow(arg1, 4)
         const double sig_k = F1 * sig_k1 + (1.0 - F1) * sig_k2;
         const double sig_w = F1 * sig_w1 + (1.0 - F1) * sig_w2;
         dtre = a.inv_re + nue_here / sig_k;
@@ -467,11 +513,21 @@ int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin, int what
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
     if (what == 0) {
-        species_stage_kernel<<<grid, block, 0, c->stream>>>(a);
+        const dim3 sgrid(grid.x, grid.y, P.im * ATJUP_S_COUNT);
+        species_stage_kernel<<<sgrid, block, 0, c->stream>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");
     } else {
-        closure_stage_kernel<<<grid, block, 0, c->stream>>>(a);
+        switch (a.turb_model) {
+        case ATJUP_TURB_K_EPSILON:
+            closure_stage_kernel<ATJUP_TURB_K_EPSILON><<<grid, block, 0, c->stream>>>(a);
+            break;
+        case ATJUP_TURB_K_OMEGA:
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA><<<grid, block, 0, c->stream>>>(a);
+            break;
+        default:
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA_SST><<<grid, block, 0, c->stream>>>(a);
+        }
         c->launches++;
         ATJUP_CHECK_LAUNCH("closure_stage_kernel");
     }

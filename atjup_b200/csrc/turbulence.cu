@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(128) sources_kernel(TurbArgs a) {
                                              2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
             const double w_hat = dmax(ds0, C_lim * S_mag / sqrt(bet_star));
             const double sig_d = (grad_dot <= 0.0) ? 0.0 : 0.125;
-            const double chi_w = fabs(Omega * Omega * S_mag / pow(bet_star * dmax(ds0, 1.0e-20), 3));
+            const double bd = bet_star * dmax(ds0, 1.0e-20);
+            const double chi_w = fabs(Omega * Omega * S_mag / (bd * bd * bd));   // pow(bd, 3)
             const double f_bet = (1.0 + 85.0 * chi_w) / (1.0 + 100.0 * chi_w);
             const double bet_wc = bet_0 * f_bet;
             nue = tk0 / dmax(w_hat, 1.0e-20);
@@ -231,8 +232,9 @@ __global__ void __launch_bounds__(128) sources_kernel(TurbArgs a) {
                                      4.0 * sig_w2 * tk0 / (CD_kw * y_star * y_star));
             const double arg2 = dmax(2.0 * sqrt(tk0) / (bet_star * dis_safe * y_star),
                                      500.0 * nue_air_nd / (y_star * y_star * dis_safe));
-            const double F1 = tanh(pow(arg1, 4));
-            const double F2 = tanh(pow(arg2, 2));
+            const double a1sq = arg1 * arg1;
+            const double F1 = tanh(a1sq * a1sq);                                // pow(arg1, 4)
+            const double F2 = tanh(arg2 * arg2);                                // pow(arg2, 2)
             nue = a1 * tk0 / dmax(a1 * dis_safe, Omega * F2);
             const double tke_safe = dmax(tk0, 1.0e-20);
             const double P_k = dmin(prod, 20.0 * bet_star * tke_safe * dis_safe);

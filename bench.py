@@ -80,9 +80,10 @@ SPECIES_STAGE_BYTES = N_CELLS * (33 + 11 * 36 + 112)
 # closure_stage_kernel, per cell and stage: u, v, w (24 B), k*, omega* in, n and out (48 B), their
 # accumulators (24 B), nue (8 B), prod and the two sources written at stage 3 (6 B averaged), flags.
 CLOSURE_STAGE_BYTES = N_CELLS * (24 + 48 + 24 + 8 + 6 + 1)
-STAGE_KERNELS = {"rk_stage": ("rk_stage_kernel", RK_STAGE_BYTES),
-                 "species": ("species_stage_kernel", SPECIES_STAGE_BYTES),
-                 "closure": ("closure_stage_kernel", CLOSURE_STAGE_BYTES)}
+STAGE_KERNELS = {"rk_stage": ("rk_stage_kernel", RK_STAGE_BYTES / N_CELLS),
+                 "species": ("species_stage_kernel", SPECIES_STAGE_BYTES / N_CELLS),
+                 "closure": ("closure_stage_kernel", CLOSURE_STAGE_BYTES / N_CELLS)}
+# (algorithmic bytes per cell and launch; times the cells of the shell)
 # DRAM bytes (read + write) per launch from ncu captures (profiles/); None until captured.
 STAGE_TRAFFIC = {"rk_stage_kernel": None, "species_stage_kernel": None, "closure_stage_kernel": None}
 
@@ -204,6 +205,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="phys", choices=["phys", "dry"])
+    ap.add_argument("--grid", default=None,
+                    help="IMxJMxKM of a smaller shell, for profiling only (the metric is quoted "
+                         "on 41x181x361)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -231,7 +235,15 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     phys = args.workload == "phys"
+    global IM, JM, KM, N_CELLS
+    if args.grid:
+        import math
+        IM, JM, KM = (int(x) for x in args.grid.lower().split("x"))
+        N_CELLS = IM * JM * KM
     P = resolve_params(PHYS_ENV if phys else DRY_ENV, im=IM, jm=JM, km=KM)
+    if args.grid:
+        P.dthe = math.pi / (JM - 1)
+        P.dphi = 2.0 * math.pi / (KM - 1)
     s = synthetic.state(IM, JM, KM, seed=20261203 + rank)
     grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
     fields = {k: v for k, v in s.items() if k not in grid}
@@ -320,6 +332,7 @@ def main():
     cands = [c for c in STAGE_KERNELS if c in per_class]
     top = max(cands, key=lambda c: per_class[c][0])
     kname, kbytes = STAGE_KERNELS[top]
+    kbytes = kbytes * N_CELLS
     st_ms, st_n = per_class[top]
     achieved = (kbytes / (st_ms / st_n / 1e3)) / 1e9
     line = {
