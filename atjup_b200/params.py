@@ -399,6 +399,7 @@ _UNSUPPORTED = {
     "ATJUP_BC_POLE_COPY": ("1", "pole rows are copies"),
     "ATJUP_DAMP_PDYN": ("0", "no Shapiro pass on p_dyn in the loop"),
     "ATJUP_HYDRO_REF": ("0", "the hydrostatic integral runs upward from the base"),
+    "ATJUP_MCA": ("0", "the moist convective adjustment is not implemented (set ATJUP_MCA=0)"),
 }
 
 

@@ -355,10 +355,15 @@ int atjup_gpu_chemistry(AtjupCtx* ctx);
 /* cJupiterModel::clampNegativeSpecies (FileIO_Jup.cpp:494-548): species < 0 or NaN -> 0. */
 int atjup_gpu_clamp_species(AtjupCtx* ctx);
 
-/* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381) for the dry
- * configuration: pressure solve on even iterations (and when first != 0), mixture density,
- * RK4, boundary passes, in-loop Shapiro, column balance of v; restoreVar is implicit (the
- * device state is the time-level n copy). solve may be NULL (= params->press_sweeps sweeps). */
+/* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381). Dry: pressure
+ * solve on even iterations (and when first != 0), mixture density, RK4, boundary passes,
+ * in-loop Shapiro, column balance of v; restoreVar is implicit (the device state is the time
+ * level n copy). With atjup_gpu_set_physics and atjup_gpu_set_micro set, the full-physics
+ * schedule: on even iterations (and the first) also radiation, the H2O, NH3, CH4 saturation
+ * adjustments, the NH4SH equilibrium, precipitation, the n copies of the condensables, the
+ * turbulence update and the chemistry block; every iteration RK4 of the 17 fields, the boundary
+ * passes of every field list, the closure's wall hold, Shapiro, the column balance, the species
+ * clamp and restoreVar of the scalars. solve may be NULL (= params->press_sweeps sweeps). */
 int atjup_gpu_step(AtjupCtx* ctx, int32_t iter_n, int32_t first, const AtjupSolveOpts* solve);
 
 /* Count of non-finite values in the prognostic fields (NaN/Inf census; no device trap). */
