@@ -141,6 +141,10 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
         set_error("create: top_taper must be 0..3, pole_fill_rows 0..3");
         return ATJUP_ERR_UNSUPPORTED;
     }
+    if (P.precision != ATJUP_PREC_FP64 && P.precision != ATJUP_PREC_MIXED) {
+        set_error("create: precision must be ATJUP_PREC_FP64 or ATJUP_PREC_MIXED");
+        return ATJUP_ERR_ARG;
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { cuda_status(e, "cudaGetDevice"); return ATJUP_ERR_NO_DEVICE; }
@@ -155,6 +159,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     AtjupCtx* c = new AtjupCtx();
     c->P = P;
     c->device = dev;
+    c->step_prec = P.precision;
     c->KP = (P.km + 3 + 15) / 16 * 16;   // >= km + 3: 4-byte flag copies near the row end stay in the row
     c->NP = (size_t)P.im * P.jm * c->KP;
     int rc = ATJUP_OK;
@@ -412,11 +417,14 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
         if ((rc = launch_buoy_ref(c, Y[0]))) return rc;
         if ((rc = launch_hydrostatic(c, Y[2], Y[3]))) return rc;
     }
-    const double* in0[4] = {Y[0], Y[1], Y[2], Y[3]};
-    const double* in1[4] = {c->X1[0], c->X1[1], c->X1[2], c->X1[3]};
-    const double* in2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
-    const double* const* ins[4] = {in0, in1, in2, in1};
-    double* const* outs[4] = {c->X1, c->X2, c->X1, nullptr};
+    // stage buffers: doubles, or in the mixed step floats in the first half of each buffer
+    const void* in0[4] = {Y[0], Y[1], Y[2], Y[3]};
+    const void* in1[4] = {c->X1[0], c->X1[1], c->X1[2], c->X1[3]};
+    const void* in2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
+    void* out1[4] = {c->X1[0], c->X1[1], c->X1[2], c->X1[3]};
+    void* out2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
+    const void* const* ins[4] = {in0, in1, in2, in1};
+    void* const* outs[4] = {out1, out2, out1, nullptr};
     for (int s = 0; s < 4; s++) {
         if (c->phys_on) {
             // species and closure first: they read the same stage input velocities, and the
@@ -433,6 +441,17 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
         Timed tm(c, TK_RK_STAGE);
         if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
     }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_set_precision(AtjupCtx* c, int32_t prec) {
+    if (!c) { set_error("set_precision: null context"); return ATJUP_ERR_ARG; }
+    if (prec != ATJUP_PREC_FP64 && prec != ATJUP_PREC_MIXED) {
+        set_error("set_precision: precision must be ATJUP_PREC_FP64 or ATJUP_PREC_MIXED");
+        return ATJUP_ERR_ARG;
+    }
+    c->step_prec = prec;      // every stage buffer is rewritten by the next step's stage 0
+    c->P.precision = prec;
     return ATJUP_OK;
 }
 

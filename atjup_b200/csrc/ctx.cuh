@@ -64,6 +64,8 @@ struct AtjupCtx {
     double turb_taper_dz = 1.0;        // clamp_nue's taper depth (Turbulence.h:569-573) [m]
     // the loop's microphysics (atjup_gpu_set_micro)
     bool micro_on = false;
+    // storage of the RK stage buffers and accumulators: ATJUP_PREC_FP64, or ATJUP_PREC_MIXED (FP32)
+    int step_prec = ATJUP_PREC_FP64;
     AtjupMicro micro{};
     double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry
     // RK stage buffers and accumulators for t, u, v, w
@@ -135,7 +137,7 @@ inline size_t cell(const AtjupCtx* c, int i, int j, int k) {
 // launchers (return ATJUP_OK or an error code)
 int launch_buoy_ref(AtjupCtx* c, const double* t);
 int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w);
-int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* const* Xout);
+int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout);
 int launch_mixture_density(AtjupCtx* c);
 int launch_prepare_projection(AtjupCtx* c);
 int launch_pressure_source(AtjupCtx* c);
@@ -152,7 +154,7 @@ int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) 
 int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
-int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin, int what);
+int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what);
 int launch_turbulence(AtjupCtx* c);
 int launch_turb_wall_hold(AtjupCtx* c);
 enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP };

@@ -28,20 +28,19 @@ enum : uint8_t { NB_S = 1, NB_IP = 2, NB_IM = 4, NB_JP = 8, NB_JM = 16, NB_KP = 
                  NB_INT = 128 };
 
 struct PhysStage {
-    // stage input velocities
-    const double *u, *v, *w;
-    // scalars: stage input, next stage input (stage 3: the live field), time-level n,
-    // accumulator, live field (for the non-integrated copy)
-    const double* q_in[ATJUP_S_COUNT + 2];
-    double* q_out[ATJUP_S_COUNT + 2];
+    // Stage buffers, typed by the kernel's template arguments: the stage input (velocities,
+    // temperature, scalars), the next stage input (stage 3: the live field) and the accumulators.
+    const void *u, *v, *w, *t;
+    const void* q_in[ATJUP_S_COUNT + 2];
+    void* q_out[ATJUP_S_COUNT + 2];
+    void* acc[ATJUP_S_COUNT + 2];
+    // FP64: the time-level-n copies and the live fields (the non-integrated copy)
     const double* q_n[ATJUP_S_COUNT + 2];
-    double* acc[ATJUP_S_COUNT + 2];
     const double* q_live[ATJUP_S_COUNT + 2];
     // frozen inputs
     const double* sprec[9];
     const double *mf_h2s, *mf_nh3, *mf_nh4sh, *fluxlim;
     const double *nue, *rho_mix;
-    const double* t;                   // stage input temperature
     const double* vel_star;            // [jm][KP]
     const float* layer_h;              // [im]
     const int32_t* topo;               // [jm * km]
@@ -59,8 +58,8 @@ struct PhysStage {
     int has_nue, turb_model, turb_buoy;
 };
 
-__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }   // std::max
-__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }   // std::min
+template <typename R> __device__ __forceinline__ R dmax(R a, R b) { return a < b ? b : a; }   // std::max
+template <typename R> __device__ __forceinline__ R dmin(R a, R b) { return b < a ? b : a; }   // std::min
 
 __device__ __forceinline__ double safe_clamp(double v, double lo, double hi) {
     const unsigned long long b = (unsigned long long)__double_as_longlong(v);
@@ -82,37 +81,42 @@ struct Cell {
     size_t c, cip, cim, cjp, cjm, ckp, ckm;
 };
 
+// The cell and its six neighbours; the i and j neighbours of the block's faces are clamped to the
+// cell itself (those cells are never integrated: their loads only have to stay in bounds).
 __device__ __forceinline__ Cell cell_of(const PhysStage& a, int i, int j, int k) {
     Cell x;
-    const size_t row = ((size_t)i * a.jm + j) * a.KP;
+    const size_t row = ((size_t)i * a.jm + j) * a.KP, plane = (size_t)a.jm * a.KP;
     const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
     x.c = row + k;
-    x.cip = x.c + (size_t)a.jm * a.KP;
-    x.cim = x.c - (size_t)a.jm * a.KP;
-    x.cjp = x.c + a.KP;
-    x.cjm = x.c - a.KP;
+    x.cip = (i < a.im - 1) ? x.c + plane : x.c;
+    x.cim = (i > 0) ? x.c - plane : x.c;
+    x.cjp = (j < a.jm - 1) ? x.c + a.KP : x.c;
+    x.cjm = (j > 0) ? x.c - a.KP : x.c;
     x.ckp = row + ke;
     x.ckm = row + kw;
     return x;
 }
 
-// RK bookkeeping of one scalar at an integrated cell (RungeKutta_Jup_Turb.cpp:425-490, 493-568)
-__device__ __forceinline__ void rk_update(const PhysStage& a, int s, size_t c, double rhs) {
-    const double acc = (a.stage == 0) ? a.wgt * rhs : a.acc[s][c] + a.wgt * rhs;
-    const double qn = a.q_n[s][c];
+// RK bookkeeping of one scalar at an integrated cell (RungeKutta_Jup_Turb.cpp:425-490, 493-568).
+// The accumulator is summed in R and stored as TA; the next stage input and the final update are
+// formed in FP64 from the FP64 time-level-n value, then clamped, then stored as TO.
+template <typename TO, typename TA, typename R>
+__device__ __forceinline__ void rk_update(const PhysStage& a, int s, size_t c, R rhs, R acc_in,
+                                          double qn) {
+    const R acc = (a.stage == 0) ? (R)a.wgt * rhs : acc_in + (R)a.wgt * rhs;
     if (a.stage < 3) {
-        a.acc[s][c] = acc;
-        double x = qn + a.c_in * rhs;
+        static_cast<TA*>(a.acc[s])[c] = (TA)acc;
+        double x = qn + (double)((R)a.c_in * rhs);
         if (s == ATJUP_S_COUNT) x = safe_clamp(x, 0.0, a.tke_max_nd);          // k*
         else if (s == ATJUP_S_COUNT + 1) x = dmax(1.0e-10, x);                 // omega*
-        a.q_out[s][c] = x;
+        static_cast<TO*>(a.q_out[s])[c] = (TO)x;
     } else {
-        double x = qn + a.dt * acc * a.one_sixth;
+        double x = qn + a.dt * (double)acc * a.one_sixth;
         if (s == ATJUP_S_COUNT) x = safe_clamp(x, 0.0, a.tke_max_nd);
         else if (s == ATJUP_S_COUNT + 1) x = dmax(1.0e-10, x);
         else if (s == ATJUP_S_NH4SH) x = (x < 0.0) ? 0.0 : x;                  // keeps NaN, -0
         else x = dmax(0.0, x);
-        a.q_out[s][c] = x;
+        static_cast<TO*>(a.q_out[s])[c] = (TO)x;
     }
 }
 
@@ -131,10 +135,18 @@ __device__ __forceinline__ int precip_slot(int s) {
     }
 }
 
+// Template arguments of the stage kernels: TI the stage input's storage (velocities, temperature,
+// scalars), TO the next stage input's (stage 3: the live FP64 field), TA the accumulators', R the
+// arithmetic of the right-hand side. The FP64 step is <double, double, double, double>; the mixed
+// step keeps FP32 stage buffers and accumulators and FP32 arithmetic: stage 0 <double, float,
+// float, float> (it reads the live fields), stages 1-2 <float, float, float, float>, stage 3
+// <float, double, float, float>.
+
 // One thread per (cell, species): blockIdx.z = i * ATJUP_S_COUNT + species, so the eleven species
 // blocks of one radial plane run back to back and the plane's u, v, w, nue come from DRAM once and
 // from L2 for the other ten; each species' stencil is its own coalesced stream.
 // blockIdx.y * blockDim.y + threadIdx.y = j, blockIdx.x * blockDim.x + threadIdx.x = k.
+template <typename TI, typename TO, typename TA, typename R>
 __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -144,20 +156,18 @@ __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
     // Every load is issued before the integrated-cell test (one memory round trip, not two):
     // the neighbour addresses are clamped into the block, so the boundary cells that the test
     // then sends to the copy below read only their own cell.
-    const size_t plane = (size_t)a.jm * a.KP, row = ((size_t)i * a.jm + j) * a.KP;
-    const size_t c = row + k;
-    const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
-    const size_t cip = (i < a.im - 1) ? c + plane : c, cim = (i > 0) ? c - plane : c;
-    const size_t cjp = (j < a.jm - 1) ? c + a.KP : c, cjm = (j > 0) ? c - a.KP : c;
-    const size_t ckp = row + ke, ckm = row + kw;
-    const double* F = a.q_in[s];
+    const Cell x = cell_of(a, i, j, k);
+    const size_t c = x.c;
+    const TI* F = static_cast<const TI*>(a.q_in[s]);
     const uint8_t fl = a.flags[c];
-    const double f0 = F[c], fip = F[cip], fim = F[cim], fjp = F[cjp], fjm = F[cjm];
-    const double fkp = F[ckp], fkm = F[ckm];
-    const double u0 = a.u[c], v0 = a.v[c], w0 = a.w[c];
+    const R f0 = (R)F[c], fip = (R)F[x.cip], fim = (R)F[x.cim], fjp = (R)F[x.cjp];
+    const R fjm = (R)F[x.cjm], fkp = (R)F[x.ckp], fkm = (R)F[x.ckm];
+    const R u0 = (R)static_cast<const TI*>(a.u)[c];
+    const R v0 = (R)static_cast<const TI*>(a.v)[c];
+    const R w0 = (R)static_cast<const TI*>(a.w)[c];
     const double nv = a.has_nue ? a.nue[c] : 0.0;
     const double qn = a.q_n[s][c];
-    const double acc_in = (a.stage == 0) ? 0.0 : a.acc[s][c];
+    const R acc_in = (a.stage == 0) ? (R)0 : (R)static_cast<const TA*>(a.acc[s])[c];
     double src0, src1 = 0.0, src2 = 0.0;
     if (s == ATJUP_S_H2S) {
         src0 = a.mf_h2s[c];
@@ -172,53 +182,48 @@ __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
         src0 = a.sprec[precip_slot(s)][c];
     }
     if (!(fl & NB_INT)) {
-        if (a.stage < 3) a.q_out[s][c] = a.q_live[s][c];
+        if (a.stage < 3) static_cast<TO*>(a.q_out[s])[c] = (TO)a.q_live[s][c];
         return;
     }
     const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
-    const double v_invrm = v0 * g.inv_rm;
-    const double w_invrs = w0 * g.inv_rmsinthe;
-    const double two_inv_rm = 2.0 * g.inv_rm;
-    double nue_t = 0.0;
-    if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t = a.turb_coupling * dmax(0.0, nv);
-    const double nue_t_s = nue_t / 0.9;
-    const double d1r = (fip - fim) * a.inv_2dr;
-    const double d2r = (fip - 2.0 * f0 + fim) * a.inv_dr2;
-    const double d1t = (fjp - fjm) * a.inv_2dthe;
-    const double d2t = (fjp - 2.0 * f0 + fjm) * a.inv_dthe2;
-    const double d1p = (fkp - fkm) * a.inv_2dphi;
-    const double d2p = (fkp - 2.0 * f0 + fkm) * a.inv_dphi2;
-    const double transport = u0 * d1r + v_invrm * d1t + w_invrs * d1p;
-    const double diffusion = d2r + d1r * two_inv_rm + d2t * g.inv_rm2 +
-                             d1t * g.costhe_inv_rm2sinthe + d2p * g.inv_rm2sinthe2;
-    const double coef = a.coef[s] + nue_t_s;
-    double r;
+    const R v_invrm = v0 * (R)g.inv_rm;
+    const R w_invrs = w0 * (R)g.inv_rmsinthe;
+    const R two_inv_rm = (R)2 * (R)g.inv_rm;
+    double nue_t64 = 0.0;
+    if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t64 = a.turb_coupling * dmax(0.0, nv);
+    const R nue_t = (R)nue_t64;
+    const R nue_t_s = nue_t / (R)0.9;
+    const R d1r = (fip - fim) * (R)a.inv_2dr;
+    const R d2r = (fip - (R)2 * f0 + fim) * (R)a.inv_dr2;
+    const R d1t = (fjp - fjm) * (R)a.inv_2dthe;
+    const R d2t = (fjp - (R)2 * f0 + fjm) * (R)a.inv_dthe2;
+    const R d1p = (fkp - fkm) * (R)a.inv_2dphi;
+    const R d2p = (fkp - (R)2 * f0 + fkm) * (R)a.inv_dphi2;
+    const R transport = u0 * d1r + v_invrm * d1t + w_invrs * d1p;
+    const R diffusion = d2r + d1r * two_inv_rm + d2t * (R)g.inv_rm2 +
+                        d1t * (R)g.costhe_inv_rm2sinthe + d2p * (R)g.inv_rm2sinthe2;
+    const R coef = (R)a.coef[s] + nue_t_s;
+    R r;
     if (s == ATJUP_S_H2S) {
-        r = -transport + diffusion * coef + a.chemical_reaction * src0;
+        r = -transport + diffusion * coef + (R)(a.chemical_reaction * src0);
     } else if (s == ATJUP_S_NH3) {
-        r = -transport + diffusion * coef + a.chemical_reaction * src0 + a.precip_coupling * src1;
+        r = -transport + diffusion * coef + (R)(a.chemical_reaction * src0) +
+            (R)(a.precip_coupling * src1);
     } else if (s == ATJUP_S_NH4SH) {
         const double v_stokes = a.stokes_pre * (a.rg_nh4sh - src2) * a.g / a.mue_mix;
-        r = -transport + src0 + diffusion * coef + a.chemical_reaction * src1 +
-            (v_stokes / a.u_0) * d1r;
+        r = -transport + (R)src0 + diffusion * coef + (R)(a.chemical_reaction * src1) +
+            (R)(v_stokes / a.u_0) * d1r;
     } else {
-        r = -transport + diffusion * coef + a.precip_coupling * src0;
+        r = -transport + diffusion * coef + (R)(a.precip_coupling * src0);
     }
-    // RK bookkeeping (RungeKutta_Jup_Turb.cpp:425-490, 493-568), the accumulator read above
-    const double accv = (a.stage == 0) ? a.wgt * r : acc_in + a.wgt * r;
-    if (a.stage < 3) {
-        a.acc[s][c] = accv;
-        a.q_out[s][c] = qn + a.c_in * r;
-    } else {
-        const double x = qn + a.dt * accv * a.one_sixth;
-        a.q_out[s][c] = (s == ATJUP_S_NH4SH) ? ((x < 0.0) ? 0.0 : x) : dmax(0.0, x);
-    }
+    rk_update<TO, TA, R>(a, s, c, r, acc_in, qn);
 }
 
 // k*, omega*: transport, diffusion with the model's coefficients, and the closure sources
-// one instantiation per closure model, so that each holds the registers of its own branch only
-template <int MODEL>
-__global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
+// (RHS_Jup_Turb.cpp:257-303, 736-998, 1399-1452). One instantiation per closure model, so that
+// each holds the registers of its own branch only.
+template <int MODEL, typename TI, typename TO, typename TA, typename R>
+__global__ void __launch_bounds__(256, 3) closure_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
@@ -227,200 +232,216 @@ __global__ void __launch_bounds__(256) closure_stage_kernel(PhysStage a) {
     // Every load is issued before the integrated-cell test (one memory round trip): the
     // neighbour addresses are clamped into the block, so boundary cells read only their own
     // cell before the test sends them to the copy below.
-    Cell x = cell_of(a, i, j, k);
-    if (i == a.im - 1) x.cip = x.c;
-    if (i == 0) x.cim = x.c;
-    if (j == a.jm - 1) x.cjp = x.c;
-    if (j == 0) x.cjm = x.c;
+    const Cell x = cell_of(a, i, j, k);
     const uint8_t fl = a.flags[x.c];
-    const double* TK = a.q_in[ST];
-    const double* DS = a.q_in[SD];
-    const double tk0 = TK[x.c], ds0 = DS[x.c];
-    const double tip_ = TK[x.cip], tim_ = TK[x.cim], tjp_ = TK[x.cjp], tjm_ = TK[x.cjm];
-    const double tkp_ = TK[x.ckp], tkm_ = TK[x.ckm];
-    const double dip_ = DS[x.cip], dim_ = DS[x.cim], djp_ = DS[x.cjp], djm_ = DS[x.cjm];
-    const double dkp_ = DS[x.ckp], dkm_ = DS[x.ckm];
-    const double u0 = a.u[x.c], v0 = a.v[x.c], w0 = a.w[x.c];
-    const double uip = a.u[x.cip], uim = a.u[x.cim], vip = a.v[x.cip], vim = a.v[x.cim];
-    const double wip = a.w[x.cip], wim = a.w[x.cim];
-    const double ujp = a.u[x.cjp], ujm = a.u[x.cjm], vjp = a.v[x.cjp], vjm = a.v[x.cjm];
-    const double wjp = a.w[x.cjp], wjm = a.w[x.cjm];
-    const double ukp = a.u[x.ckp], ukm = a.u[x.ckm], vkp = a.v[x.ckp], vkm = a.v[x.ckm];
-    const double wkp = a.w[x.ckp], wkm = a.w[x.ckm];
+    const TI* TK = static_cast<const TI*>(a.q_in[ST]);
+    const TI* DS = static_cast<const TI*>(a.q_in[SD]);
+    const TI* Us = static_cast<const TI*>(a.u);
+    const TI* Vs = static_cast<const TI*>(a.v);
+    const TI* Ws = static_cast<const TI*>(a.w);
+    const R tk0 = (R)TK[x.c], ds0 = (R)DS[x.c];
+    const R tip_ = (R)TK[x.cip], tim_ = (R)TK[x.cim], tjp_ = (R)TK[x.cjp], tjm_ = (R)TK[x.cjm];
+    const R tkp_ = (R)TK[x.ckp], tkm_ = (R)TK[x.ckm];
+    const R dip_ = (R)DS[x.cip], dim_ = (R)DS[x.cim], djp_ = (R)DS[x.cjp], djm_ = (R)DS[x.cjm];
+    const R dkp_ = (R)DS[x.ckp], dkm_ = (R)DS[x.ckm];
+    const R u0 = (R)Us[x.c], v0 = (R)Vs[x.c], w0 = (R)Ws[x.c];
+    const R uip = (R)Us[x.cip], uim = (R)Us[x.cim], vip = (R)Vs[x.cip], vim = (R)Vs[x.cim];
+    const R wip = (R)Ws[x.cip], wim = (R)Ws[x.cim];
+    const R ujp = (R)Us[x.cjp], ujm = (R)Us[x.cjm], vjp = (R)Vs[x.cjp], vjm = (R)Vs[x.cjm];
+    const R wjp = (R)Ws[x.cjp], wjm = (R)Ws[x.cjm];
+    const R ukp = (R)Us[x.ckp], ukm = (R)Us[x.ckm], vkp = (R)Vs[x.ckp], vkm = (R)Vs[x.ckm];
+    const R wkp = (R)Ws[x.ckp], wkm = (R)Ws[x.ckm];
     const double nv = a.nue[x.c];
     const int32_t topo = a.topo[(size_t)j * a.km + k];
     if (!(fl & NB_INT)) {
         if (a.stage < 3) {
-            a.q_out[ST][x.c] = a.q_live[ST][x.c];
-            a.q_out[SD][x.c] = a.q_live[SD][x.c];
+            static_cast<TO*>(a.q_out[ST])[x.c] = (TO)a.q_live[ST][x.c];
+            static_cast<TO*>(a.q_out[SD])[x.c] = (TO)a.q_live[SD][x.c];
         }
         return;
     }
     const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
+    const R inv_rm = (R)g.inv_rm, inv_rmsinthe = (R)g.inv_rmsinthe;
     // the solid-face mirror (RHS_Jup_Turb.cpp:257-303): a solid neighbour reads as the cell
-    const double tip = (fl & NB_IP) ? tk0 : tip_, tim = (fl & NB_IM) ? tk0 : tim_;
-    const double tjp = (fl & NB_JP) ? tk0 : tjp_, tjm = (fl & NB_JM) ? tk0 : tjm_;
-    const double tkp = (fl & NB_KP) ? tk0 : tkp_, tkm = (fl & NB_KM) ? tk0 : tkm_;
-    const double dip = (fl & NB_IP) ? ds0 : dip_, dim = (fl & NB_IM) ? ds0 : dim_;
-    const double djp = (fl & NB_JP) ? ds0 : djp_, djm = (fl & NB_JM) ? ds0 : djm_;
-    const double dkp = (fl & NB_KP) ? ds0 : dkp_, dkm = (fl & NB_KM) ? ds0 : dkm_;
-    const double dtkedr = (tip - tim) * a.inv_2dr, d2tkedr2 = (tip - 2.0 * tk0 + tim) * a.inv_dr2;
-    const double ddisdr = (dip - dim) * a.inv_2dr, d2disdr2 = (dip - 2.0 * ds0 + dim) * a.inv_dr2;
-    const double dtkedthe = (tjp - tjm) * a.inv_2dthe;
-    const double d2tkedthe2 = (tjp - 2.0 * tk0 + tjm) * a.inv_dthe2;
-    const double ddisdthe = (djp - djm) * a.inv_2dthe;
-    const double d2disdthe2 = (djp - 2.0 * ds0 + djm) * a.inv_dthe2;
-    const double dtkedphi = (tkp - tkm) * a.inv_2dphi;
-    const double d2tkedphi2 = (tkp - 2.0 * tk0 + tkm) * a.inv_dphi2;
-    const double ddisdphi = (dkp - dkm) * a.inv_2dphi;
-    const double d2disdphi2 = (dkp - 2.0 * ds0 + dkm) * a.inv_dphi2;
+    const R tip = (fl & NB_IP) ? tk0 : tip_, tim = (fl & NB_IM) ? tk0 : tim_;
+    const R tjp = (fl & NB_JP) ? tk0 : tjp_, tjm = (fl & NB_JM) ? tk0 : tjm_;
+    const R tkp = (fl & NB_KP) ? tk0 : tkp_, tkm = (fl & NB_KM) ? tk0 : tkm_;
+    const R dip = (fl & NB_IP) ? ds0 : dip_, dim = (fl & NB_IM) ? ds0 : dim_;
+    const R djp = (fl & NB_JP) ? ds0 : djp_, djm = (fl & NB_JM) ? ds0 : djm_;
+    const R dkp = (fl & NB_KP) ? ds0 : dkp_, dkm = (fl & NB_KM) ? ds0 : dkm_;
+    const R i2r = (R)a.inv_2dr, i2t = (R)a.inv_2dthe, i2p = (R)a.inv_2dphi;
+    const R dtkedr = (tip - tim) * i2r, d2tkedr2 = (tip - (R)2 * tk0 + tim) * (R)a.inv_dr2;
+    const R ddisdr = (dip - dim) * i2r, d2disdr2 = (dip - (R)2 * ds0 + dim) * (R)a.inv_dr2;
+    const R dtkedthe = (tjp - tjm) * i2t;
+    const R d2tkedthe2 = (tjp - (R)2 * tk0 + tjm) * (R)a.inv_dthe2;
+    const R ddisdthe = (djp - djm) * i2t;
+    const R d2disdthe2 = (djp - (R)2 * ds0 + djm) * (R)a.inv_dthe2;
+    const R dtkedphi = (tkp - tkm) * i2p;
+    const R d2tkedphi2 = (tkp - (R)2 * tk0 + tkm) * (R)a.inv_dphi2;
+    const R ddisdphi = (dkp - dkm) * i2p;
+    const R d2disdphi2 = (dkp - (R)2 * ds0 + dkm) * (R)a.inv_dphi2;
 
-    const double dudr = (uip - uim) * a.inv_2dr;
-    const double dvdr = (vip - vim) * a.inv_2dr;
-    const double dwdr = (wip - wim) * a.inv_2dr;
-    const double dudthe = (ujp - ujm) * a.inv_2dthe;
-    const double dvdthe = (vjp - vjm) * a.inv_2dthe;
-    const double dwdthe = (wjp - wjm) * a.inv_2dthe;
-    const double dudphi = (ukp - ukm) * a.inv_2dphi;
-    const double dvdphi = (vkp - vkm) * a.inv_2dphi;
-    const double dwdphi = (wkp - wkm) * a.inv_2dphi;
-    const double v_invrm = v0 * g.inv_rm;
-    const double w_invrs = w0 * g.inv_rmsinthe;
-    const double two_inv_rm = 2.0 * g.inv_rm;
-    const double transport_tke = u0 * dtkedr + v_invrm * dtkedthe + w_invrs * dtkedphi;
-    const double transport_dis = u0 * ddisdr + v_invrm * ddisdthe + w_invrs * ddisdphi;
-    const double diffusion_tke = d2tkedr2 + dtkedr * two_inv_rm + d2tkedthe2 * g.inv_rm2 +
-                                 dtkedthe * g.costhe_inv_rm2sinthe + d2tkedphi2 * g.inv_rm2sinthe2;
-    const double diffusion_dis = d2disdr2 + ddisdr * two_inv_rm + d2disdthe2 * g.inv_rm2 +
-                                 ddisdthe * g.costhe_inv_rm2sinthe + d2disdphi2 * g.inv_rm2sinthe2;
+    const R dudr = (uip - uim) * i2r;
+    const R dvdr = (vip - vim) * i2r;
+    const R dwdr = (wip - wim) * i2r;
+    const R dudthe = (ujp - ujm) * i2t;
+    const R dvdthe = (vjp - vjm) * i2t;
+    const R dwdthe = (wjp - wjm) * i2t;
+    const R dudphi = (ukp - ukm) * i2p;
+    const R dvdphi = (vkp - vkm) * i2p;
+    const R dwdphi = (wkp - wkm) * i2p;
+    const R v_invrm = v0 * inv_rm;
+    const R w_invrs = w0 * inv_rmsinthe;
+    const R two_inv_rm = (R)2 * inv_rm;
+    const R transport_tke = u0 * dtkedr + v_invrm * dtkedthe + w_invrs * dtkedphi;
+    const R transport_dis = u0 * ddisdr + v_invrm * ddisdthe + w_invrs * ddisdphi;
+    const R diffusion_tke = d2tkedr2 + dtkedr * two_inv_rm + d2tkedthe2 * (R)g.inv_rm2 +
+                            dtkedthe * (R)g.costhe_inv_rm2sinthe + d2tkedphi2 * (R)g.inv_rm2sinthe2;
+    const R diffusion_dis = d2disdr2 + ddisdr * two_inv_rm + d2disdthe2 * (R)g.inv_rm2 +
+                            ddisdthe * (R)g.costhe_inv_rm2sinthe + d2disdphi2 * (R)g.inv_rm2sinthe2;
 
-    const double C_nue = 0.028, dis_min = 1.0e-10, nue_gas_phys = 1.8e-5;
+    const R C_nue = (R)0.028, dis_min = (R)1.0e-10;
+    const double nue_gas_phys = 1.8e-5;
     const double L_m = a.L_m;
-    const double nue_here = isfinite(nv) ? dmax(0.0, nv) : 0.0;
-    const double tke_s = dmax(tk0, dis_min);
-    const double dis_s = dmax(ds0, dis_min);
-    const double dudr_s = dudr, dvdr_s = dvdr, dwdr_s = dwdr;
-    const double dudthe_s = dudthe * g.inv_rm, dvdthe_s = dvdthe * g.inv_rm;
-    const double dwdthe_s = dwdthe * g.inv_rm;
-    const double dudphi_s = dudphi * g.inv_rmsinthe, dvdphi_s = dvdphi * g.inv_rmsinthe;
-    const double dwdphi_s = dwdphi * g.inv_rmsinthe;
-    const double dtkedthe_s = dtkedthe * g.inv_rm, ddisdthe_s = ddisdthe * g.inv_rm;
-    const double dtkedphi_s = dtkedphi * g.inv_rmsinthe, ddisdphi_s = ddisdphi * g.inv_rmsinthe;
-    const double grad_dot = dtkedr * ddisdr + dtkedthe_s * ddisdthe_s + dtkedphi_s * ddisdphi_s;
-    double cnue = (MODEL == ATJUP_TURB_K_EPSILON) ? C_nue * tke_s * tke_s / dis_s
-                                                         : tke_s / dis_s;
-    cnue = dmin(cnue, a.nue_max);
-    const double der = 0.66667 * (dudr_s + dvdthe_s + dwdphi_s);
-    const double P_full = dmax(0.0,
-          (cnue * (2.0 * dudr_s - der) - 0.66667 * tk0) * dudr_s
+    const R nue_here = isfinite(nv) ? (R)dmax(0.0, nv) : (R)0;
+    const R tke_s = dmax(tk0, dis_min);
+    const R dis_s = dmax(ds0, dis_min);
+    const R dudr_s = dudr, dvdr_s = dvdr, dwdr_s = dwdr;
+    const R dudthe_s = dudthe * inv_rm, dvdthe_s = dvdthe * inv_rm;
+    const R dwdthe_s = dwdthe * inv_rm;
+    const R dudphi_s = dudphi * inv_rmsinthe, dvdphi_s = dvdphi * inv_rmsinthe;
+    const R dwdphi_s = dwdphi * inv_rmsinthe;
+    const R dtkedthe_s = dtkedthe * inv_rm, ddisdthe_s = ddisdthe * inv_rm;
+    const R dtkedphi_s = dtkedphi * inv_rmsinthe, ddisdphi_s = ddisdphi * inv_rmsinthe;
+    const R grad_dot = dtkedr * ddisdr + dtkedthe_s * ddisdthe_s + dtkedphi_s * ddisdphi_s;
+    R cnue = (MODEL == ATJUP_TURB_K_EPSILON) ? C_nue * tke_s * tke_s / dis_s : tke_s / dis_s;
+    cnue = dmin(cnue, (R)a.nue_max);
+    const R c23 = (R)0.66667, two = (R)2;
+    const R der = c23 * (dudr_s + dvdthe_s + dwdphi_s);
+    const R P_full = dmax((R)0,
+          (cnue * (two * dudr_s - der) - c23 * tk0) * dudr_s
         + (cnue * (dudthe_s + dvdr_s)) * dudthe_s
         + (cnue * (dudphi_s + dwdr_s)) * dudphi_s
-        + (cnue * (2.0 * dvdthe_s - der) - 0.66667 * tk0) * dvdthe_s
+        + (cnue * (two * dvdthe_s - der) - c23 * tk0) * dvdthe_s
         + (cnue * (dvdr_s + dudthe_s)) * dvdr_s
         + (cnue * (dvdphi_s + dwdthe_s)) * dvdphi_s
-        + (cnue * (2.0 * dwdphi_s - der) - 0.66667 * tk0) * dwdphi_s
+        + (cnue * (two * dwdphi_s - der) - c23 * tk0) * dwdphi_s
         + (cnue * (dwdr_s + dudphi_s)) * dwdr_s
         + (cnue * (dwdthe_s + dvdphi_s)) * dwdthe_s);
 
     const double y_mount = layer_h(a, topo) * 1.0e3;
     const double dz_layer = dmax(1.0, layer_dz_m(a, i - 1 > 0 ? i - 1 : 0));
     const double y_phys = dmax(layer_h(a, i) * 1.0e3 - y_mount, dz_layer);
-    const double y_star = y_phys / L_m;
+    const R y_star = (R)(y_phys / L_m);
+    const R inv_re = (R)a.inv_re;
 
-    double dtre, ddre, tke_src, dis_src, c_w_prod;
-    if (MODEL == ATJUP_TURB_K_EPSILON) {               // Chien 1982
-        const double sig_k = 1.0, sig_w = 1.3, C_eps_1 = 1.35, C_eps_2 = 1.80;
-        dtre = a.inv_re + nue_here / sig_k;
-        ddre = a.inv_re + nue_here / sig_w;
+    R dtre, ddre, tke_src, dis_src, c_w_prod;
+    if (MODEL == ATJUP_TURB_K_EPSILON) {                      // Chien 1982
+        const R sig_k = (R)1.0, sig_w = (R)1.3, C_eps_1 = (R)1.35, C_eps_2 = (R)1.80;
+        dtre = inv_re + nue_here / sig_k;
+        ddre = inv_re + nue_here / sig_w;
+        // the wall-damping exponentials in FP64: their arguments overflow FP32 near dis_min
         const double d_plus = y_phys * a.vel_star[(size_t)j * a.KP + k] / nue_gas_phys;
-        const double Re_T = tke_s * tke_s * a.u_0 * L_m / (dis_s * nue_gas_phys);
-        const double f_2 = 1.0 - 0.4 / 1.8 * exp(-Re_T * Re_T / 36.0);
-        const double y_star2 = y_star * y_star;
-        const double L_k = -2.0 * tk0 / y_star2;
-        const double L_w = -2.0 * ds0 / y_star2 * exp(-0.5 * d_plus);
-        const double P_w = C_eps_1 * ds0 / tke_s * P_full;
-        const double Y_w = C_eps_2 * f_2 * ds0 * ds0 / tke_s;
-        tke_src = P_full - ds0 + L_k / a.re_turb;
-        dis_src = P_w - Y_w + L_w / a.re_turb;
+        const double tke_d = (double)tke_s, dis_d = (double)dis_s;
+        const double Re_T = tke_d * tke_d * a.u_0 * L_m / (dis_d * nue_gas_phys);
+        const R f_2 = (R)(1.0 - 0.4 / 1.8 * exp(-Re_T * Re_T / 36.0));
+        const R y_star2 = y_star * y_star;
+        const R L_k = -(R)2 * tk0 / y_star2;
+        const R L_w = (R)(-2.0 * (double)ds0 / (double)y_star2 * exp(-0.5 * d_plus));
+        const R P_w = C_eps_1 * ds0 / tke_s * P_full;
+        const R Y_w = C_eps_2 * f_2 * ds0 * ds0 / tke_s;
+        tke_src = P_full - ds0 + L_k / (R)a.re_turb;
+        dis_src = P_w - Y_w + L_w / (R)a.re_turb;
         c_w_prod = C_eps_1;
-    } else if (MODEL == ATJUP_TURB_K_OMEGA) {          // Wilcox
-        const double sig_k = 0.6, sig_w = 0.5, bet_star = 0.09, gam = 0.52, bet_0 = 0.0708;
-        dtre = a.inv_re + sig_k * nue_here;
-        ddre = a.inv_re + sig_w * nue_here;
-        const double S11 = dudr_s, S22 = dvdthe_s, S33 = dwdphi_s;
-        const double S12 = 0.5 * (dudthe_s + dvdr_s);
-        const double S13 = 0.5 * (dudphi_s + dwdr_s);
-        const double S23 = 0.5 * (dvdphi_s + dwdthe_s);
-        const double S_mag = sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 +
-                                         2.0 * (S12 * S12 + S13 * S13 + S23 * S23)));
-        const double W12 = dudthe_s - dvdr_s;
-        const double W13 = dudphi_s - dwdr_s;
-        const double W23 = dvdphi_s - dwdthe_s;
-        const double Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
-        const double bd = bet_star * dis_s;
-        const double chi_w = fabs(Omega * Omega * S_mag / (bd * bd * bd));   // pow(bd, 3)
+    } else if (MODEL == ATJUP_TURB_K_OMEGA) {                 // Wilcox
+        const R sig_k = (R)0.6, sig_w = (R)0.5, bet_star = (R)0.09, gam = (R)0.52;
+        const double bet_0 = 0.0708;
+        dtre = inv_re + sig_k * nue_here;
+        ddre = inv_re + sig_w * nue_here;
+        const R S11 = dudr_s, S22 = dvdthe_s, S33 = dwdphi_s;
+        const R S12 = (R)0.5 * (dudthe_s + dvdr_s);
+        const R S13 = (R)0.5 * (dudphi_s + dwdr_s);
+        const R S23 = (R)0.5 * (dvdphi_s + dwdthe_s);
+        const R S_mag = sqrt((R)2 * (S11 * S11 + S22 * S22 + S33 * S33 +
+                                     (R)2 * (S12 * S12 + S13 * S13 + S23 * S23)));
+        const R W12 = dudthe_s - dvdr_s;
+        const R W13 = dudphi_s - dwdr_s;
+        const R W23 = dvdphi_s - dwdthe_s;
+        const R Omega = sqrt(W12 * W12 + W13 * W13 + W23 * W23);
+        // the vortex-stretching ratio in FP64: (0.09 omega*)^3 underflows FP32 near dis_min
+        const double bd = 0.09 * (double)dis_s;
+        const double chi_w = fabs((double)Omega * (double)Omega * (double)S_mag / (bd * bd * bd));
         const double f_bet = (1.0 + 85.0 * chi_w) / (1.0 + 100.0 * chi_w);
-        const double bet_wc = bet_0 * f_bet;
-        const double sig_d = (grad_dot <= 0.0) ? 0.0 : 0.125;
-        const double P_k = dmin(P_full, 20.0 * bet_star * tke_s * dis_s);
-        const double Y_k = bet_star * tke_s * dis_s;
-        const double P_w = gam * dis_s / tke_s * P_k;
-        const double Y_w = bet_wc * dis_s * dis_s;
-        const double D_w = sig_d / dis_s * grad_dot;
+        const R bet_wc = (R)(bet_0 * f_bet);
+        const R sig_d = (grad_dot <= (R)0) ? (R)0 : (R)0.125;
+        const R P_k = dmin(P_full, (R)20 * bet_star * tke_s * dis_s);
+        const R Y_k = bet_star * tke_s * dis_s;
+        const R P_w = gam * dis_s / tke_s * P_k;
+        const R Y_w = bet_wc * dis_s * dis_s;
+        const R D_w = sig_d / dis_s * grad_dot;
         tke_src = P_k - Y_k;
         dis_src = P_w - Y_w + D_w;
         c_w_prod = gam;
     } else {                                                   // SST, Menter 1994
-        const double bet_star = 0.09, sig_k1 = 1.176, sig_k2 = 1.0, sig_w1 = 2.0, sig_w2 = 1.168;
-        const double bet1 = 0.0333, bet2 = 0.0368, gam1 = 0.413, gam2 = 0.2;
-        const double nue_air_nd = nue_gas_phys / (a.u_0 * L_m);
-        const double CD_kw = dmax(2.0 * sig_w2 / dis_s * grad_dot, 1.0e-20);
-        const double arg1 = dmin(dmax(sqrt(dmax(tk0, 0.0)) / (bet_star * dis_s * y_star),
-                                      500.0 * nue_air_nd / (y_star * y_star * dis_s)),
-                                 4.0 * sig_w2 * tke_s / (CD_kw * y_star * y_star));
-        const double a2 = arg1 * arg1;
-        const double F1 = tanh(a2 * a2);                                     // pow(arg1, 4)
-        const double sig_k = F1 * sig_k1 + (1.0 - F1) * sig_k2;
-        const double sig_w = F1 * sig_w1 + (1.0 - F1) * sig_w2;
-        dtre = a.inv_re + nue_here / sig_k;
-        ddre = a.inv_re + nue_here / sig_w;
-        const double P_k = dmin(P_full, 20.0 * bet_star * tke_s * dis_s);
-        const double Y_k = bet_star * tke_s * dis_s;
-        const double P_w = (F1 * gam1 + (1.0 - F1) * gam2) * P_k * dis_s / tke_s;
-        const double Y_w = (F1 * bet1 + (1.0 - F1) * bet2) * dis_s * dis_s;
-        const double D_w = 2.0 * (1.0 - F1) * sig_w2 / dis_s * grad_dot;
+        const R bet_star = (R)0.09, sig_k1 = (R)1.176, sig_k2 = (R)1.0, sig_w1 = (R)2.0;
+        const R sig_w2 = (R)1.168;
+        const R bet1 = (R)0.0333, bet2 = (R)0.0368, gam1 = (R)0.413, gam2 = (R)0.2;
+        const R nue_air_nd = (R)(nue_gas_phys / (a.u_0 * L_m));
+        const R CD_kw = dmax((R)2 * sig_w2 / dis_s * grad_dot, (R)1.0e-20);
+        const R arg1 = dmin(dmax(sqrt(dmax(tk0, (R)0)) / (bet_star * dis_s * y_star),
+                                 (R)500 * nue_air_nd / (y_star * y_star * dis_s)),
+                            (R)4 * sig_w2 * tke_s / (CD_kw * y_star * y_star));
+        const R a2 = arg1 * arg1;
+        const R F1 = tanh(a2 * a2);                                          // pow(arg1, 4)
+        const R one = (R)1;
+        const R sig_k = F1 * sig_k1 + (one - F1) * sig_k2;
+        const R sig_w = F1 * sig_w1 + (one - F1) * sig_w2;
+        dtre = inv_re + nue_here / sig_k;
+        ddre = inv_re + nue_here / sig_w;
+        const R P_k = dmin(P_full, (R)20 * bet_star * tke_s * dis_s);
+        const R Y_k = bet_star * tke_s * dis_s;
+        const R P_w = (F1 * gam1 + (one - F1) * gam2) * P_k * dis_s / tke_s;
+        const R Y_w = (F1 * bet1 + (one - F1) * bet2) * dis_s * dis_s;
+        const R D_w = (R)2 * (one - F1) * sig_w2 / dis_s * grad_dot;
         tke_src = P_k - Y_k;
         dis_src = P_w - Y_w + D_w;
-        c_w_prod = F1 * gam1 + (1.0 - F1) * gam2;
+        c_w_prod = F1 * gam1 + (one - F1) * gam2;
     }
     if (a.turb_buoy) {                                         // RHS_Jup_Turb.cpp:963-981
+        const TI* Ts = static_cast<const TI*>(a.t);
         const int ip = (i + 1 < a.im - 1) ? i + 1 : a.im - 1, imn = (i - 1 > 0) ? i - 1 : 0;
         const double dz_m = (layer_h(a, ip) - layer_h(a, imn)) * 1.0e3;
         const size_t rs = (size_t)a.jm * a.KP;
-        const double T_K = dmax(a.t[x.c] * a.t_ref, 1.0);
-        const double dTdz = (a.t[x.c + (ip - i) * rs] - a.t[x.c - (i - imn) * rs]) * a.t_ref /
-                            dmax(dz_m, 1.0);
+        const double T_K = dmax((double)Ts[x.c] * a.t_ref, 1.0);
+        const double dTdz = ((double)Ts[x.c + (ip - i) * rs] - (double)Ts[x.c - (i - imn) * rs]) *
+                            a.t_ref / dmax(dz_m, 1.0);
         const double N2 = a.g / T_K * (dTdz + a.g / a.cp_mix);
         const double tscale = L_m / a.u_0;
-        const double G_b = -(cnue / a.turb_buoy_prt) * N2 * tscale * tscale;
+        const double G_b = -((double)cnue / a.turb_buoy_prt) * N2 * tscale * tscale;
         if (isfinite(G_b)) {
-            tke_src += G_b;
-            dis_src += c_w_prod * dis_s / tke_s * dmax(G_b, 0.0);
+            tke_src += (R)G_b;
+            dis_src += c_w_prod * dis_s / tke_s * (R)dmax(G_b, 0.0);
         }
     }
-    const double tke_src_max = 20.0 * tke_s * dis_s;
-    const double dis_src_max = 20.0 * dis_s * dis_s;
-    if (!isfinite(tke_src)) tke_src = 0.0;
-    if (!isfinite(dis_src)) dis_src = 0.0;
+    const R tke_src_max = (R)20 * tke_s * dis_s;
+    const R dis_src_max = (R)20 * dis_s * dis_s;
+    if (!isfinite(tke_src)) tke_src = (R)0;
+    if (!isfinite(dis_src)) dis_src = (R)0;
     tke_src = dmax(-tke_src_max, dmin(tke_src_max, tke_src));
     dis_src = dmax(-dis_src_max, dmin(dis_src_max, dis_src));
     if (a.stage == 3) {
-        a.prod[x.c] = P_full;
-        a.tke_source[x.c] = tke_src;
-        a.dis_source[x.c] = dis_src;
+        a.prod[x.c] = (double)P_full;
+        a.tke_source[x.c] = (double)tke_src;
+        a.dis_source[x.c] = (double)dis_src;
     }
-    rk_update(a, ST, x.c, -transport_tke + diffusion_tke * dtre + tke_src);
-    rk_update(a, SD, x.c, -transport_dis + diffusion_dis * ddre + dis_src);
+    // the accumulators and n copies are read here, not with the stencil: read early they hold
+    // four more registers (8 in FP64) through the whole source computation
+    const R acc_t = (a.stage == 0) ? (R)0 : (R)static_cast<const TA*>(a.acc[ST])[x.c];
+    const R acc_d = (a.stage == 0) ? (R)0 : (R)static_cast<const TA*>(a.acc[SD])[x.c];
+    rk_update<TO, TA, R>(a, ST, x.c, -transport_tke + diffusion_tke * dtre + tke_src, acc_t,
+                         a.q_n[ST][x.c]);
+    rk_update<TO, TA, R>(a, SD, x.c, -transport_dis + diffusion_dis * ddre + dis_src, acc_d,
+                         a.q_n[SD][x.c]);
 }
 
 }  // namespace
@@ -432,7 +453,7 @@ const int kScalarField[ATJUP_S_COUNT + 2] = {
     ATJUP_F_NH4SH, ATJUP_F_TKE, ATJUP_F_DIS};
 
 namespace {
-PhysStage stage_args(AtjupCtx* c, int stage, const double* const* vin) {
+PhysStage stage_args(AtjupCtx* c, int stage, const void* const* vin) {
     const AtjupParams& P = c->P;
     const AtjupPhysics& H = c->phys;
     PhysStage a{};
@@ -442,8 +463,9 @@ PhysStage stage_args(AtjupCtx* c, int stage, const double* const* vin) {
     for (int s = 0; s < ATJUP_S_COUNT + 2; s++) {
         const int id = kScalarField[s];
         double* live = c->f[id];
-        const double* in[4] = {live, c->S1[s], c->S2[s], c->S1[s]};
-        double* out[4] = {c->S1[s], c->S2[s], c->S1[s], live};
+        // the stage buffers hold doubles, or floats in their first half in the mixed step
+        const void* in[4] = {live, c->S1[s], c->S2[s], c->S1[s]};
+        void* out[4] = {c->S1[s], c->S2[s], c->S1[s], live};
         a.q_in[s] = in[stage];
         a.q_out[s] = out[stage];
         a.q_n[s] = c->fn[id];
@@ -506,32 +528,41 @@ PhysStage stage_args(AtjupCtx* c, int stage, const double* const* vin) {
 }
 }  // namespace
 
-// species_stage_kernel of one RK stage (what = 0) or closure_stage_kernel (what = 1)
-int launch_phys_stage(AtjupCtx* c, int stage, const double* const* vin, int what) {
+template <typename TI, typename TO, typename TA, typename R>
+static int launch_typed(AtjupCtx* c, const PhysStage& a, int what) {
     const AtjupParams& P = c->P;
-    const PhysStage a = stage_args(c, stage, vin);
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
     if (what == 0) {
         const dim3 sgrid(grid.x, grid.y, P.im * ATJUP_S_COUNT);
-        species_stage_kernel<<<sgrid, block, 0, c->stream>>>(a);
+        species_stage_kernel<TI, TO, TA, R><<<sgrid, block, 0, c->stream>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");
     } else {
         switch (a.turb_model) {
         case ATJUP_TURB_K_EPSILON:
-            closure_stage_kernel<ATJUP_TURB_K_EPSILON><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_EPSILON, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
             break;
         case ATJUP_TURB_K_OMEGA:
-            closure_stage_kernel<ATJUP_TURB_K_OMEGA><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
             break;
         default:
-            closure_stage_kernel<ATJUP_TURB_K_OMEGA_SST><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA_SST, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
         }
         c->launches++;
         ATJUP_CHECK_LAUNCH("closure_stage_kernel");
     }
     return ATJUP_OK;
+}
+
+// species_stage_kernel of one RK stage (what = 0) or closure_stage_kernel (what = 1); vin are
+// the stage input's t, u, v, w (stage 0: the FP64 state; later stages: the stage buffers)
+int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what) {
+    const PhysStage a = stage_args(c, stage, vin);
+    if (c->step_prec != ATJUP_PREC_MIXED) return launch_typed<double, double, double, double>(c, a, what);
+    if (stage == 0) return launch_typed<double, float, float, float>(c, a, what);
+    if (stage < 3) return launch_typed<float, float, float, float>(c, a, what);
+    return launch_typed<float, double, float, float>(c, a, what);
 }
 
 }  // namespace atjup

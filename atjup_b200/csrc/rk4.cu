@@ -20,8 +20,7 @@ namespace {
 constexpr int TK = 36, TJ = 7, NT = 256, NL = TK * TJ;   // 252 live threads of 256
 constexpr int NCH = 3;                                   // radial chunks per column tile
 constexpr int HK = TK + 2, HJ = TJ + 2, HC = HK * HJ;   // halo tile of one plane
-constexpr int NF = 6;                                   // t, u, v, w, p_dyn, p_hydro
-constexpr int NX = 10;                                  // per-cell inputs: Y[4], acc[4], rho, wall_nue
+constexpr int NX = 5;    // FP64 per-cell inputs besides Y: rho, wall_nue, nue, Q_rad, Q_precip
 
 // Per-cell flags, precomputed from the static mask (atjup_gpu_set_grid): bit 0 solid, 1 solid i+1,
 // 2 solid i-1, 3 solid j+1, 4 solid j-1, 5 solid k+1 (ring), 6 solid k-1 (ring), 7 integrated
@@ -46,11 +45,14 @@ struct StageConst {
     int has_nue, has_heating, precip_local;
 };
 
+// The stage buffers X (stage input), Xo (next stage input) and acc are typed by the kernel's
+// template arguments (FP64, or FP32 in the mixed step); Y (time level n), the pressures and the
+// frozen inputs are FP64.
 struct StagePtrs {
-    const double* X[4];
-    double* Xo[4];
+    const void* X[4];
+    void* Xo[4];
     double* Y[4];
-    double* acc[4];
+    void* acc[4];
     const double *p_dyn, *p_hydro, *p_stat, *rho, *wall_nue, *nue, *Q_rad, *Q_precip;
     double *aux_u, *aux_v, *aux_w;
     const uint8_t* nb;
@@ -59,12 +61,16 @@ struct StagePtrs {
     const double *cell_vbar0, *cell_ubar0;
 };
 
+template <typename TI, typename TA>
 struct __align__(16) StageSmem {
-    double tile[3][NF][HC];   // planes i, i+1, i+2 (in flight) with a one-cell halo in j and k
+    double ptile[3][2][HC];   // p_dyn, p_hydro of planes i, i+1, i+2 (in flight), one-cell halo in j, k
     double ps[3][NT];         // p_stat at the cells of the same three planes
-    double ex[2][NX][NT];     // per-cell inputs of planes i and i+1
+    double Yx[2][4][NT];      // time-level-n t, u, v, w of planes i and i+1 (stages 1-3)
+    double ex[2][NX][NT];     // FP64 per-cell inputs of planes i and i+1
     GeoIJ geo[2][TJ];         // geometry rows of planes i and i+1
     double cm[2][2][TJ];      // cell-hold means (v, u) of planes i and i+1
+    TI tile[3][4][HC];        // stage input t, u, v, w of planes i, i+1, i+2, one-cell halo
+    TA ax[2][4][NT];          // accumulators of planes i and i+1 (stages 1-3)
     uint8_t nb[2][NT];        // per-cell flags of planes i and i+1
 };
 
@@ -76,25 +82,32 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+template <typename T>
+__device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
+    if constexpr (sizeof(T) == 8) cp_async8(smem, gmem);
+    else cp_async4(smem, gmem);
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 
-// Issue the asynchronous copies of plane i's halo tile and p_stat into ring slot i % 3.
-__device__ __forceinline__ void issue_tile(StageSmem& S, const StagePtrs& a, const StageConst& q,
-                                           int i, int j0, int k0, int tid) {
+// Issue the asynchronous copies of plane i's halo tiles and p_stat into ring slot i % 3.
+template <typename TI, typename TA>
+__device__ __forceinline__ void issue_tile(StageSmem<TI, TA>& S, const StagePtrs& a,
+                                           const StageConst& q, int i, int j0, int k0, int tid) {
     const int sl = i % 3;
     const size_t base = (size_t)i * q.jm * q.KP;
-    const double* src[NF] = {a.X[0], a.X[1], a.X[2], a.X[3], a.p_dyn, a.p_hydro};
-    for (int e = tid; e < NF * HC; e += NT) {
+    for (int e = tid; e < 6 * HC; e += NT) {
         const int f = e / HC, h = e - f * HC;
         const int hj = h / HK, hk = h - hj * HK;
         int j = j0 - 1 + hj;
         j = j < 0 ? 0 : (j > q.jm - 1 ? q.jm - 1 : j);
         int k = k0 - 1 + hk;          // the ring of km-1 meridians: k-1 of 0 is km-2, k+1 of km-2 is 0
         k = (k < 0) ? q.km - 2 : (k >= q.km - 1 ? 0 : k);   // (beyond km-1: unused lanes)
-        cp_async8(&S.tile[sl][f][h], src[f] + base + (size_t)j * q.KP + k);
+        const size_t o = base + (size_t)j * q.KP + k;
+        if (f < 4) cp_async(&S.tile[sl][f][h], static_cast<const TI*>(a.X[f]) + o);
+        else cp_async8(&S.ptile[sl][f - 4][h], (f == 4 ? a.p_dyn : a.p_hydro) + o);
     }
     if (tid < NL) {
         const int tx = tid % TK, ty = tid / TK;
@@ -104,8 +117,9 @@ __device__ __forceinline__ void issue_tile(StageSmem& S, const StagePtrs& a, con
 }
 
 // Issue the copies of plane i's per-cell inputs, geometry rows and cell means into slot i % 2.
-__device__ __forceinline__ void issue_extra(StageSmem& S, const StagePtrs& a, const StageConst& q,
-                                            int i, int j0, int k0, int tid) {
+template <typename TI, typename TA>
+__device__ __forceinline__ void issue_extra(StageSmem<TI, TA>& S, const StagePtrs& a,
+                                            const StageConst& q, int i, int j0, int k0, int tid) {
     const int sl = i & 1;
     if (tid < NL) {
         const int tx = tid % TK, ty = tid / TK;
@@ -114,12 +128,17 @@ __device__ __forceinline__ void issue_extra(StageSmem& S, const StagePtrs& a, co
         if (q.stage > 0) {
 #pragma unroll
             for (int f = 0; f < 4; f++) {
-                cp_async8(&S.ex[sl][f][tid], a.Y[f] + c);
-                cp_async8(&S.ex[sl][4 + f][tid], a.acc[f] + c);
+                cp_async8(&S.Yx[sl][f][tid], a.Y[f] + c);
+                cp_async(&S.ax[sl][f][tid], static_cast<const TA*>(a.acc[f]) + c);
             }
         }
-        cp_async8(&S.ex[sl][8][tid], a.rho + c);
-        cp_async8(&S.ex[sl][9][tid], a.wall_nue + c);
+        cp_async8(&S.ex[sl][0][tid], a.rho + c);
+        cp_async8(&S.ex[sl][1][tid], a.wall_nue + c);
+        if (q.has_nue) cp_async8(&S.ex[sl][2][tid], a.nue + c);
+        if (q.has_heating) {
+            cp_async8(&S.ex[sl][3][tid], a.Q_rad + c);
+            cp_async8(&S.ex[sl][4][tid], a.Q_precip + c);
+        }
     }
     // flags: 4 bytes per copy along a tile row (k0 and the row pitch are multiples of 4)
     if (tid < TJ * (TK / 4) && k0 + 4 * (tid % (TK / 4)) <= q.km - 2) {
@@ -142,11 +161,17 @@ __device__ __forceinline__ void issue_extra(StageSmem& S, const StagePtrs& a, co
     }
 }
 
-// One RK stage: every (j, k) column of the block's tile, plane by plane.
+// One RK stage: every (j, k) column of the block's tile, plane by plane. TI is the storage of the
+// stage input, TO of the next stage input, TA of the accumulators (all double in the FP64 step;
+// the mixed step stores them in FP32: stage 0 <double, float, float> reads the FP64 state, stages
+// 1-3 <float, float, float>). The right-hand side is evaluated in FP64 either way: the kernel's
+// residency is set by its shared memory, not its registers, and the final update y_n + dt/6 acc
+// is formed in FP64 from the FP64 time-level-n state.
+template <typename TI, typename TO, typename TA>
 __global__ void __launch_bounds__(NT, 2)
 rk_stage_kernel(StagePtrs a, StageConst q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StageSmem& S = *reinterpret_cast<StageSmem*>(smem_raw);
+    StageSmem<TI, TA>& S = *reinterpret_cast<StageSmem<TI, TA>*>(smem_raw);
     const int tid = threadIdx.x;
     const int tx = tid % TK, ty = tid / TK;
     const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
@@ -176,38 +201,39 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
         __syncthreads();
 
         const int cs = i % 3, ns = (i + 1) % 3, xs = i & 1;
-        const double* Tt = S.tile[cs][0];
-        const double* Ut = S.tile[cs][1];
-        const double* Vt = S.tile[cs][2];
-        const double* Wt = S.tile[cs][3];
-        const double* Pt = S.tile[cs][4];
-        const double* Ht = S.tile[cs][5];
+        const TI* Tt = S.tile[cs][0];
+        const TI* Ut = S.tile[cs][1];
+        const TI* Vt = S.tile[cs][2];
+        const TI* Wt = S.tile[cs][3];
+        const double* Pt = S.ptile[cs][0];
+        const double* Ht = S.ptile[cs][1];
         if (live && i >= i_lo) {
             const size_t c = (size_t)i * plane + (size_t)j * row + k;
             const uint8_t nbm = S.nb[xs][tid];
             if (!(nbm & NB_INT)) {
                 if (q.stage == 0) {
 #pragma unroll
-                    for (int f = 0; f < 4; f++) a.Xo[f][c] = ld(a.Y[f] + c);
+                    for (int f = 0; f < 4; f++) static_cast<TO*>(a.Xo[f])[c] = (TO)ld(a.Y[f] + c);
                 } else if (q.stage < 3) {
 #pragma unroll
-                    for (int f = 0; f < 4; f++) a.Xo[f][c] = S.ex[xs][f][tid];
+                    for (int f = 0; f < 4; f++) static_cast<TO*>(a.Xo[f])[c] = (TO)S.Yx[xs][f][tid];
                 }
             } else {
                 const GeoIJ& g = S.geo[xs][ty];
-                const double t0 = Tt[h], u0 = Ut[h], v0 = Vt[h], w0 = Wt[h];
-                const double* Tn = S.tile[ns][0];
-                const double* Un = S.tile[ns][1];
-                const double* Vn = S.tile[ns][2];
-                const double* Wn = S.tile[ns][3];
+                const double t0 = (double)Tt[h], u0 = (double)Ut[h], v0 = (double)Vt[h];
+                const double w0 = (double)Wt[h];
+                const TI* Tn = S.tile[ns][0];
+                const TI* Un = S.tile[ns][1];
+                const TI* Vn = S.tile[ns][2];
+                const TI* Wn = S.tile[ns][3];
                 // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
 #define DERIVS(F, FN, FM, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
-    const double d1r = (FN[h] - FM) * q.inv_2dr;                                      \
-    const double d2r = (FN[h] - 2.0 * f0 + FM) * q.inv_dr2;                           \
-    const double d1t = (F[h + HK] - F[h - HK]) * q.inv_2dthe;                         \
-    const double d2t = (F[h + HK] - 2.0 * f0 + F[h - HK]) * q.inv_dthe2;              \
-    const double d1p = (F[h + 1] - F[h - 1]) * q.inv_2dphi;                           \
-    const double d2p = (F[h + 1] - 2.0 * f0 + F[h - 1]) * q.inv_dphi2;
+    const double d1r = ((double)FN[h] - FM) * q.inv_2dr;                              \
+    const double d2r = ((double)FN[h] - 2.0 * f0 + FM) * q.inv_dr2;                   \
+    const double d1t = ((double)F[h + HK] - (double)F[h - HK]) * q.inv_2dthe;         \
+    const double d2t = ((double)F[h + HK] - 2.0 * f0 + (double)F[h - HK]) * q.inv_dthe2; \
+    const double d1p = ((double)F[h + 1] - (double)F[h - 1]) * q.inv_2dphi;           \
+    const double d2p = ((double)F[h + 1] - 2.0 * f0 + (double)F[h - 1]) * q.inv_dphi2;
                 DERIVS(Tt, Tn, m_t, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
                 DERIVS(Ut, Un, m_u, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
                 DERIVS(Vt, Vn, m_v, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
@@ -216,7 +242,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 // pressure gradients, solid faces mirrored to the local value (RHS_Jup_Turb.cpp:119-130)
                 const bool wall = q.pgrad_wall;
                 const double pc = Pt[h];
-                const double pip = (wall && (nbm & NB_IP)) ? pc : S.tile[ns][4][h];
+                const double pip = (wall && (nbm & NB_IP)) ? pc : S.ptile[ns][0][h];
                 const double pim = (wall && (nbm & NB_IM)) ? pc : m_pd;
                 const double pjp = (wall && (nbm & NB_JP)) ? pc : Pt[h + HK];
                 const double pjm = (wall && (nbm & NB_JM)) ? pc : Pt[h - HK];
@@ -239,7 +265,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 const double w_invrs = w0 * g.inv_rmsinthe;
 
                 // compression work with the hydrostatic part (RHS_Jup_Turb.cpp:459-482)
-                const double rho_l = S.ex[xs][8][tid];
+                const double rho_l = S.ex[xs][0][tid];
                 double dpstatdr = 0.0;
                 if (q.adiabatic) {
                     dpstatdr = (S.ps[ns][tid] - m_ps) * q.inv_2dr * q.to_nd;
@@ -295,7 +321,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                                                ? rho_l
                                                : ((T_phys > 1.0) ? P_phys / (q.R_mix * T_phys) : 0.0);
                         if (rho > 0.0 && q.cp_mix > 0.0) {
-                            radiation_t = q.rad_coupling * ld(a.Q_rad + c) * q.L_rad /
+                            radiation_t = q.rad_coupling * S.ex[xs][3][tid] * q.L_rad /
                                           (rho * q.cp_mix * q.u_0 * q.t_ref);
                             if (!isfinite(radiation_t)) radiation_t = 0.0;
                             else if (radiation_t > 0.5) radiation_t = 0.5;
@@ -306,7 +332,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                         double rho_p = q.r_mix;
                         if (q.precip_local) rho_p = (rho_l > 0.0 && isfinite(rho_l)) ? rho_l : q.r_mix;
                         if (rho_p > 0.0 && q.cp_mix > 0.0) {
-                            precip_t = q.precip_coupling * ld(a.Q_precip + c) * q.L_rad /
+                            precip_t = q.precip_coupling * S.ex[xs][4][tid] * q.L_rad /
                                        (rho_p * q.cp_mix * q.u_0 * q.t_ref);
                             if (!isfinite(precip_t)) precip_t = 0.0;
                             else if (precip_t > 0.5) precip_t = 0.5;
@@ -317,11 +343,11 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
 
                 double nue_t = 0.0;
                 if (q.has_nue) {
-                    const double nn = ld(a.nue + c);
+                    const double nn = S.ex[xs][2][tid];
                     if (q.turb_coupling != 0.0 && isfinite(nn)) nue_t = q.turb_coupling * fmax(0.0, nn);
                 }
                 const double nue_t_s = nue_t / 0.9;
-                const double visc = q.inv_re + nue_t + S.ex[xs][9][tid];
+                const double visc = q.inv_re + nue_t + S.ex[xs][1][tid];
 
                 const double rhs_t = +pressure_t - transport_t + diffusion_t * (q.t_visc + nue_t_s) +
                                      radiation_t + precip_t;
@@ -342,20 +368,20 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                     const double y0[4] = {t0, u0, v0, w0};
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        a.acc[f][c] = q.wgt * rhs[f];
-                        a.Xo[f][c] = y0[f] + q.c_in * rhs[f];
+                        static_cast<TA*>(a.acc[f])[c] = (TA)(q.wgt * rhs[f]);
+                        static_cast<TO*>(a.Xo[f])[c] = (TO)(y0[f] + q.c_in * rhs[f]);
                     }
                 } else if (q.stage < 3) {
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        a.acc[f][c] = S.ex[xs][4 + f][tid] + q.wgt * rhs[f];
-                        a.Xo[f][c] = S.ex[xs][f][tid] + q.c_in * rhs[f];
+                        static_cast<TA*>(a.acc[f])[c] = (TA)((double)S.ax[xs][f][tid] + q.wgt * rhs[f]);
+                        static_cast<TO*>(a.Xo[f])[c] = (TO)(S.Yx[xs][f][tid] + q.c_in * rhs[f]);
                     }
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        const double acc3 = S.ex[xs][4 + f][tid] + q.wgt * rhs[f];
-                        a.Y[f][c] = S.ex[xs][f][tid] + q.dt * acc3 * q.one_sixth;
+                        const double acc3 = (double)S.ax[xs][f][tid] + q.wgt * rhs[f];
+                        a.Y[f][c] = S.Yx[xs][f][tid] + q.dt * acc3 * q.one_sixth;
                     }
                     // the projection source the next pressure solve reads (the last stage's values)
                     a.aux_u[c] = rhs_u + dpdr_term;
@@ -365,7 +391,8 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
             }
         }
         if (live) {   // slide the radial window up one plane
-            m_t = Tt[h]; m_u = Ut[h]; m_v = Vt[h]; m_w = Wt[h]; m_pd = Pt[h];
+            m_t = (double)Tt[h]; m_u = (double)Ut[h]; m_v = (double)Vt[h]; m_w = (double)Wt[h];
+            m_pd = Pt[h];
             m_ps = S.ps[cs][tid];
         }
         __syncthreads();
@@ -496,7 +523,26 @@ int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w) {
     return ATJUP_OK;
 }
 
-int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* const* Xout) {
+template <typename TI, typename TO, typename TA>
+static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, const char* name) {
+    const AtjupParams& P = c->P;
+    static bool attr_set = false;       // one flag per instantiation
+    if (!attr_set) {
+        ATJUP_CUDA(cudaFuncSetAttribute(rk_stage_kernel<TI, TO, TA>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(StageSmem<TI, TA>)));
+        attr_set = true;
+    }
+    dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
+    c->launches++;
+    rk_stage_kernel<TI, TO, TA><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q);
+    ATJUP_CHECK_LAUNCH(name);
+    return ATJUP_OK;
+}
+
+// Xin / Xout: the stage input and the next stage input (stage 0 reads the FP64 state itself;
+// the other buffers are FP64 or, in the mixed step, FP32)
+int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout) {
     const AtjupParams& P = c->P;
     StagePtrs a{};
     for (int f = 0; f < 4; f++) {
@@ -567,17 +613,10 @@ int launch_rk_stage(AtjupCtx* c, int stage, const double* const* Xin, double* co
     q.has_heating = (P.has_heating && a.Q_rad && a.Q_precip) ? 1 : 0;
     q.precip_local = (P.precip_rho_local && P.local_rho) ? 1 : 0;
 
-    static bool attr_set = false;
-    if (!attr_set) {
-        ATJUP_CUDA(cudaFuncSetAttribute(rk_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(StageSmem)));
-        attr_set = true;
-    }
-    dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
-    c->launches++;
-    rk_stage_kernel<<<grid, NT, sizeof(StageSmem), c->stream>>>(a, q);
-    ATJUP_CHECK_LAUNCH("rk_stage");
-    return ATJUP_OK;
+    if (c->step_prec != ATJUP_PREC_MIXED)
+        return launch_stage_t<double, double, double>(c, a, q, "rk_stage");
+    if (stage == 0) return launch_stage_t<double, float, float>(c, a, q, "rk_stage (mixed)");
+    return launch_stage_t<float, float, float>(c, a, q, "rk_stage (mixed)");
 }
 
 int launch_mixture_density(AtjupCtx* c) {

@@ -69,6 +69,7 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_upload2d.argtypes = [vp, i32, vp]
     L.atjup_gpu_turbulence.argtypes = [vp]
     L.atjup_gpu_set_micro.argtypes = [vp, ctypes.POINTER(_p.AtjupMicro)]
+    L.atjup_gpu_set_precision.argtypes = [vp, i32]
     for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species"):
         getattr(L, "atjup_gpu_" + n).argtypes = [vp]
     L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
@@ -159,6 +160,11 @@ class GpuModel:
         assert lh.shape == (self.shape[0],)
         _check(self.L.atjup_gpu_set_physics(self.ctx, ctypes.byref(phys), _ptr(lh)))
         self._phys = True
+
+    def set_precision(self, precision: int) -> None:
+        """The RK step's precision: params.PREC_FP64, or params.PREC_MIXED (FP32 stage buffers and
+        accumulators, FP32 species and closure right-hand sides)."""
+        _check(self.L.atjup_gpu_set_precision(self.ctx, int(precision)))
 
     def upload_n(self, name: str, a) -> None:
         a = np.ascontiguousarray(a, np.float64).reshape(self.shape)

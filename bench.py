@@ -2,7 +2,7 @@
 """Benchmark of ATJUP's time step on B200: one model iteration with the full physics.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload phys|dry]
+                    [--workload phys|dry] [--precision fp64|mixed]
 
 Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 shell (2.68 M
 cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
@@ -14,13 +14,19 @@ column balance of v and the species clamp. The initial state follows the full-ph
 (atjup_b200/synthetic.py: state + full_physics): vapour at 90 % of saturation with U(0.95, 1.05)
 noise, k = 1e-4 m2/s2 x U(0.5, 1.5), omega = 1e-3 1/s x U(0.5, 1.5), the dynamics perturbations of
 the dry recipe; it is device-resident when the timed region starts. `--workload dry` times the
-dry dynamics iteration instead (microphysics, radiation, closure off).
+dry dynamics iteration instead (microphysics, radiation, closure off). `--precision mixed` runs
+the mixed-precision RK step (AtjupParams.precision = ATJUP_PREC_MIXED: FP32 stage inputs and
+accumulators of the 17 fields, FP32 species and closure right-hand sides; FP64 time-level-n state,
+final update, dynamics right-hand side, pressure, level means, column balance and the loop's
+physics).
 
 Prints one JSON line. `value` is seconds per step for the whole job (N replicas: max-over-ranks
 device time / (N * K)); `e2e` is the same metric through the public C ABI with host buffers
 (pinned), the host->device upload of the step's state and the device->host read of its result
-inside the timed region. With --impl reference the line times the reference's own CPU code of
-the same iteration (built from its sources into oracle/_ref) on this host's cores.
+inside the timed region. For the full-physics workload in FP64 the line also carries
+`mixed_precision`: the run continued for K more iterations in the mixed-precision RK step, timed
+the same way. With --impl reference the line times the reference's own CPU code of the same
+iteration (built from its sources into oracle/_ref) on this host's cores.
 """
 from __future__ import annotations
 
@@ -42,10 +48,17 @@ IM, JM, KM = 41, 181, 361
 N_CELLS = IM * JM * KM
 UNIT = "s/step"
 METRICS = {
-    "phys": "s per RK4 step (full-physics FP64 iteration, 41x181x361: pressure pass, radiation, "
+    "phys": "s per RK4 step (full-physics {prec} iteration, 41x181x361: pressure pass, radiation, "
             "saturation adjustment, NH4SH, precipitation, k-omega SST, chemistry, RK4 of 17 fields, "
             "BCs, filters)",
-    "dry": "s per RK4 step (dry FP64 dynamics, 41x181x361: one model iteration incl. pressure pass)",
+    "dry": "s per RK4 step (dry {prec} dynamics, 41x181x361: one model iteration incl. pressure pass)",
+}
+PREC_NAMES = {"fp64": "FP64", "mixed": "mixed FP32/FP64"}
+PREC_CONFIG = {
+    "fp64": "fp64",
+    "mixed": "mixed: FP32 stage inputs and accumulators of the RK step, FP32 species and closure "
+             "right-hand sides; FP64 state, final update, dynamics right-hand side, pressure, "
+             "level means, column balance and microphysics",
 }
 CONFIGS = {
     "phys": {
@@ -66,26 +79,50 @@ CONFIGS = {
         "parallelism": "replicas (the path does not shard)",
     },
 }
-# Algorithmic bytes of one RK stage launch: N * b * (17 F + 4 A) / 4 + N bytes of mask, with
-# F = 4 prognostic fields (t, u, v, w) and A = 5 frozen inputs (p_dyn, p_hydro, p_stat, rho_mix,
-# wall_nue), b = 8 (FP64): one RK4 step of 1.89 GB over its four stage launches.
-RK_STEP_BYTES = N_CELLS * 8 * (17 * 4 + 4 * 5) + 4 * N_CELLS
-RK_STAGE_BYTES = RK_STEP_BYTES / 4
-# species_stage_kernel, per cell and stage: u, v, w, nue (32 B) and the flag byte, and per species
-# the stage input, the time-level-n value and the stage output (24 B) and the accumulator (12 B
-# averaged over the stages: written at stage 0, read and written at 1 and 2, read at 3), plus the
-# frozen sources: S_precip of 9 species, the mass flux of H2S and NH3, the flux limiter, mass flux
-# and mixture density of NH4SH (112 B): 541 B per cell.
-SPECIES_STAGE_BYTES = N_CELLS * (33 + 11 * 36 + 112)
-# closure_stage_kernel, per cell and stage: u, v, w (24 B), k*, omega* in, n and out (48 B), their
-# accumulators (24 B), nue (8 B), prod and the two sources written at stage 3 (6 B averaged), flags.
-CLOSURE_STAGE_BYTES = N_CELLS * (24 + 48 + 24 + 8 + 6 + 1)
-STAGE_KERNELS = {"rk_stage": ("rk_stage_kernel", RK_STAGE_BYTES / N_CELLS),
-                 "species": ("species_stage_kernel", SPECIES_STAGE_BYTES / N_CELLS),
-                 "closure": ("closure_stage_kernel", CLOSURE_STAGE_BYTES / N_CELLS)}
+# Algorithmic bytes per cell of one RK stage launch, averaged over the four stages of a step.
+#
+# A field of the RK step costs, over the four stages: stage 0 reads its state Y and writes the
+# next stage input X and the accumulator; stages 1-2 read X, Y and the accumulator and write X
+# and the accumulator; stage 3 reads X, Y and the accumulator and writes Y. With FP64 everywhere
+# that is 17 x 8 = 136 B per field and step (the 17F of N b (17F + 4A)); with FP32 X and
+# accumulators (mixed) 16 + 24 + 24 + 24 = 88 B. Per stage: 34 B (FP64), 22 B (mixed).
+FIELD_STAGE_BYTES = {"fp64": 34.0, "mixed": 22.0}
+
+
+def rk_stage_bytes(prec, phys):
+    # t, u, v, w; A frozen FP64 inputs read every stage (p_dyn, p_hydro, p_stat, rho_mix, wall_nue,
+    # and with full physics nue, Q_rad, Q_precip); aux_u, aux_v, aux_w written at stage 3; flags
+    a = 8 if phys else 5
+    return 4 * FIELD_STAGE_BYTES[prec] + 8 * a + 3 * 8 / 4 + 1
+
+
+def species_stage_bytes(prec):
+    # u, v, w (FP64 at stage 0, the stage buffers' type after), nue and the flag byte; per species
+    # the stencil's stage input, the FP64 n copy, the output and the accumulator; the FP64 frozen
+    # sources (S_precip of 9 species, the mass fluxes of H2S and NH3, the NH4SH limiter, mass flux
+    # and mixture density: 112 B). FP64: 33 + 11 x 36 + 112 = 541 B.
+    uvw = 24.0 if prec == "fp64" else (24 + 3 * 12) / 4
+    per = 36.0 if prec == "fp64" else 5 + 8 + 5 + 6
+    return uvw + 8 + 1 + 11 * per + 112
+
+
+def closure_stage_bytes(prec):
+    # u, v, w; k*, omega*: stage input, n copy, output, accumulator; nue; prod and the two sources
+    # written at stage 3 (6 B averaged); flags. FP64: 24 + 48 + 24 + 8 + 6 + 1 = 111 B.
+    if prec == "fp64":
+        return 24 + 48 + 24 + 8 + 6 + 1
+    return (24 + 3 * 12) / 4 + 2 * (5 + 8 + 5) + 2 * 6 + 8 + 6 + 1
+
+
+def stage_kernels(prec, phys):
+    return {"rk_stage": ("rk_stage_kernel", rk_stage_bytes(prec, phys)),
+            "species": ("species_stage_kernel", species_stage_bytes(prec)),
+            "closure": ("closure_stage_kernel", closure_stage_bytes(prec))}
 # (algorithmic bytes per cell and launch; times the cells of the shell)
 # DRAM bytes (read + write) per launch from ncu captures (profiles/); None until captured.
-STAGE_TRAFFIC = {"rk_stage_kernel": None, "species_stage_kernel": None, "closure_stage_kernel": None}
+# DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step,
+# from ncu captures (profiles/); None where not captured.
+STAGE_TRAFFIC_PER_CELL = {}
 
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
@@ -187,7 +224,8 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
         return
     v = cb["value"]
-    line = {"impl": "reference", "metric": METRICS[args.workload], "value": v, "unit": UNIT,
+    line = {"impl": "reference", "metric": METRICS[args.workload].format(prec="FP64"),
+            "value": v, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": f"the reference's own initial state ({args.workload} knobs)",
@@ -205,6 +243,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="phys", choices=["phys", "dry"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None,
                     help="IMxJMxKM of a smaller shell, for profiling only (the metric is quoted "
                          "on 41x181x361)")
@@ -222,8 +261,8 @@ def main():
 
     from atjup_b200 import synthetic
     from atjup_b200.gpu import GpuModel
-    from atjup_b200.params import (DEFAULT_GASES, FIELD_IDS, SCALARS, resolve_micro, resolve_params,
-                                   resolve_physics)
+    from atjup_b200.params import (DEFAULT_GASES, FIELD_IDS, PREC_FP64, PREC_MIXED, SCALARS,
+                                   resolve_micro, resolve_params, resolve_physics)
     from atjup_b200.replicas import max_over_ranks, whole_job_seconds_per_step
 
     torch.cuda.set_device(local_rank)
@@ -255,6 +294,8 @@ def main():
     if phys:
         m.set_physics(resolve_physics(PHYS_ENV), fields["layer_heights"])
         m.set_micro(resolve_micro(PHYS_ENV))
+    if args.precision == "mixed":
+        m.set_precision(PREC_MIXED)
     m.upload_state(fields)
     stream = torch.cuda.Stream()
     m.set_stream(stream.cuda_stream)
@@ -277,29 +318,56 @@ def main():
         torch.cuda.synchronize()
 
     # ---- device-timed region ----
-    clocks = ClockSampler(local_rank)
-    n0 = m.launch_count()
-    m.timing(True)
-    barrier()
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    ev1.synchronize()
-    clk = clocks.stop()
-    barrier()
-    t_ms = ev0.elapsed_time(ev1)
-    launches = m.launch_count() - n0
-    per_class = {}
-    for ci, cname in enumerate(m.TIMING_CLASSES):
-        ms, n = m.timing_read(ci)
-        if n:
-            per_class[cname] = (ms, n)
-    m.timing(False)
-    t_ms = max_over_ranks(t_ms, device="cuda")
+    def timed_region(steps):
+        clocks = ClockSampler(local_rank)
+        n0 = m.launch_count()
+        m.timing(True)
+        barrier()
+        clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+        clk = clocks.stop()
+        barrier()
+        t_ms = ev0.elapsed_time(ev1)
+        launches = m.launch_count() - n0
+        per_class = {}
+        for ci, cname in enumerate(m.TIMING_CLASSES):
+            ms, n = m.timing_read(ci)
+            if n:
+                per_class[cname] = (ms, n)
+        m.timing(False)
+        return max_over_ranks(t_ms, device="cuda"), per_class, launches, clk
+
+    t_ms, per_class, launches, clk = timed_region(args.steps)
     value = whole_job_seconds_per_step(t_ms / 1e3, args.steps, world)
+
+    # ---- the same iterations in the mixed-precision RK step, continuing the run ----
+    mixed = None
+    if phys and args.precision == "fp64":
+        m.set_precision(PREC_MIXED)
+        for _ in range(2):
+            step()
+        mt_ms, mper, _, mclk = timed_region(args.steps)
+        m.set_precision(PREC_FP64)
+        mk = stage_kernels("mixed", phys)["species"][1] * N_CELLS
+        sms, sn = mper["species"]
+        mixed = {"value": whole_job_seconds_per_step(mt_ms / 1e3, args.steps, world),
+                 "unit": UNIT, "ms_per_step": mt_ms / args.steps, "dtype": "f32+f64",
+                 "precision": PREC_CONFIG["mixed"],
+                 "accuracy": "relative L2 vs the FP64 step after 200 iterations of this workload "
+                             "<= 1e-5 per prognostic field, except the condensates bounded by "
+                             "the FP64 step's own sensitivity to one FP32 rounding of its input "
+                             "(tests/test_mixed.py)",
+                 "species_stage_roofline": {"achieved": mk / (sms / sn / 1e3) / 1e9,
+                                            "algorithmic_bytes_per_launch": mk,
+                                            "avg_launch_ms": sms / sn},
+                 "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
+                                                 sorted(mper.items(), key=lambda kv: -kv[1][0])},
+                 "clocks": mclk}
 
     # ---- end to end through the C ABI with pinned host buffers ----
     names = ["t", "u", "v", "w", "p_dyn"] + (list(SCALARS) if phys else [])
@@ -329,24 +397,29 @@ def main():
 
     peak, peak_kind = measured_peak_hbm()
     # the roofline of the stage kernel with the most device time in the timed region
-    cands = [c for c in STAGE_KERNELS if c in per_class]
+    kernels = stage_kernels(args.precision, phys)
+    cands = [c for c in kernels if c in per_class]
     top = max(cands, key=lambda c: per_class[c][0])
-    kname, kbytes = STAGE_KERNELS[top]
+    kname, kbytes = kernels[top]
     kbytes = kbytes * N_CELLS
+    tpc = STAGE_TRAFFIC_PER_CELL.get((args.precision, kname))
+    traffic = None if tpc is None else tpc * N_CELLS
     st_ms, st_n = per_class[top]
     achieved = (kbytes / (st_ms / st_n / 1e3)) / 1e9
     line = {
-        "metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": world,
+        "metric": METRICS[args.workload].format(prec=PREC_NAMES[args.precision]),
+        "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded; shapes and value ranges of the model's initial state"
                 + (", full-physics recipe" if phys else "") + ")",
-        "config": CONFIGS[args.workload],
+        "config": {**CONFIGS[args.workload], "precision": PREC_CONFIG[args.precision]},
         "roofline": {"kernel": kname, "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
-                     "traffic": STAGE_TRAFFIC[kname], "algorithmic_bytes_per_launch": kbytes,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": kbytes,
                      "avg_launch_ms": st_ms / st_n, "launches": st_n},
         "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
                                         sorted(per_class.items(), key=lambda kv: -kv[1][0])},
@@ -356,6 +429,9 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if mixed is not None:
+        mixed["species_stage_roofline"]["frac"] = mixed["species_stage_roofline"]["achieved"] / peak
+        line["mixed_precision"] = mixed
     if dist is not None:
         dist.barrier()
     if rank == 0:

@@ -124,7 +124,12 @@ typedef struct AtjupParams {
     double shapiro_strength;           /* ATJUP_SHAPIRO_STRENGTH 1                              */
     int32_t v_massbal_stride;          /* ATJUP_V_MASSBAL_STRIDE 1                              */
     int32_t v_massbal_zonal;           /* ATJUP_V_MASSBAL_ZONAL (follows ATJUP_VORTEX), 1       */
-    int32_t precision;                 /* ATJUP_PREC_FP64 or ATJUP_PREC_MIXED                   */
+    int32_t precision;                 /* the RK step: ATJUP_PREC_FP64, or ATJUP_PREC_MIXED: the    */
+                                       /* stage inputs and accumulators of the 17 fields in FP32,  */
+                                       /* the species and closure right-hand sides in FP32; the    */
+                                       /* time-level-n state, the final update, the dynamics RHS,  */
+                                       /* the pressure, the level means, the column balance and    */
+                                       /* the loop's physics stay FP64                              */
 } AtjupParams;
 
 typedef struct AtjupSolveOpts {
@@ -261,6 +266,9 @@ typedef struct AtjupPhysics {
  * layer_heights_km[im] is m_layer_heights (float, km), the wall distance of the closure.
  * Allocates the scalar stage buffers on first use. phys = NULL switches back to dynamics only. */
 int atjup_gpu_set_physics(AtjupCtx* ctx, const AtjupPhysics* phys, const float* layer_heights_km);
+/* Switch the precision of the RK step (AtjupParams.precision) between steps. No reference
+ * counterpart: the reference computes in FP64 only. */
+int atjup_gpu_set_precision(AtjupCtx* ctx, int32_t precision);
 /* The time-level-n copy of a transported scalar (field ids ATJUP_F_H2O .. ATJUP_F_DIS). */
 int atjup_gpu_upload_n(AtjupCtx* ctx, int32_t field_id, const double* host);
 int atjup_gpu_download_n(AtjupCtx* ctx, int32_t field_id, double* host);
