@@ -72,6 +72,8 @@ __global__ void radiation_kernel(MicroArgs a) {
     const int i_top = a.im - 1;
     if (i_base >= i_top) return;
     double B[MAX_IM], eps[MAX_IM], Fd[MAX_IM + 1], Fu[MAX_IM + 1], Fsw[MAX_IM + 2];
+    // the levels are independent here: unrolled, the loads of four levels are in flight together
+#pragma unroll 4
     for (int i = i_base; i <= i_top; i++) {
         const size_t c = c0 + (size_t)i * plane;
         const double T = a.t[c] * a.t_ref;
@@ -120,46 +122,99 @@ __global__ void radiation_kernel(MicroArgs a) {
     for (int i = 0; i < i_base; i++) a.Q_rad[c0 + (size_t)i * plane] = 0.0;
 }
 
-__global__ void precip_kernel(MicroArgs a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
-    if (k >= a.km) return;
-    const size_t plane = (size_t)a.jm * a.KP, c0 = (size_t)j * a.KP + k;
-    for (int i = 0; i < a.im; i++) {
-        const size_t c = c0 + (size_t)i * plane;
-        a.Q_precip[c] = 0.0;
-        for (int q = 0; q < 9; q++) a.sprec[q][c] = 0.0;
+// The inputs of one level of a column sweep, loaded ahead of the level's computation.
+struct PrecipLevel {
+    double t, p, vap, cld, ice, rho;
+};
+
+__device__ __forceinline__ PrecipLevel precip_load(const MicroArgs& a, const double* vap,
+                                                   const double* cld, const double* ice, size_t c) {
+    PrecipLevel L;
+    L.t = a.t[c];
+    L.p = a.p_stat[c];
+    L.vap = vap[c];
+    L.cld = cld[c];
+    L.ice = ice[c];
+    L.rho = a.local_rho ? a.rho_mix[c] : 0.0;
+    return L;
+}
+
+// The three gases' sweeps of a column are independent except for Q_precip, the sum of their
+// latent heating. So a block is PR_COLS columns x 3 gases (threadIdx.y = gas: H2O, NH3, CH4), the
+// three threads of a column walk its levels in step, and at each level the H2O thread adds the
+// three contributions in the reference's order ((0 + H2O) + NH3) + CH4 from shared memory
+// (double-buffered by level parity, one barrier per level). Within a sweep the inputs of a level
+// depend only on the state before the sweep: each level's loads are issued two levels ahead of
+// its computation (and so ahead, in program order, of the stores of the level in between, which
+// touch other cells), so a column waits for one memory round trip per sweep, not one per level.
+constexpr int PRECIP_AHEAD = 2;
+constexpr int PR_COLS = 64;
+
+__global__ void __launch_bounds__(PR_COLS * 3, 4) precip_kernel(MicroArgs a) {
+    __shared__ double contrib[2][3][PR_COLS];
+    const int tx = threadIdx.x, gq = threadIdx.y;
+    const int k = blockIdx.x * PR_COLS + tx, j = blockIdx.y;
+    const bool col = k < a.km;
+    const size_t plane = (size_t)a.jm * a.KP, c0 = (size_t)j * a.KP + (col ? k : 0);
+    const AtjupGasParams& gs = a.mc.gas[gq];
+    const int sv = gq == 0 ? ATJUP_S_H2O : (gq == 1 ? ATJUP_S_NH3 : ATJUP_S_CH4);
+    double *vap = a.q[sv], *cld = a.q[sv + 1], *ice = a.q[sv + 2];
+    double *Sv = a.sprec[3 * gq], *Sc = a.sprec[3 * gq + 1], *Si = a.sprec[3 * gq + 2];
+    if (col) {
+        for (int i = 0; i < a.im; i++) {
+            const size_t c = c0 + (size_t)i * plane;
+            if (gq == 0) a.Q_precip[c] = 0.0;
+            Sv[c] = 0.0;
+            Sc[c] = 0.0;
+            Si[c] = 0.0;
+        }
     }
-    int i_base = a.topo[(size_t)j * a.km + k];
+    int i_base = col ? a.topo[(size_t)j * a.km + k] : a.im;
     if (i_base < 0) i_base = 0;
     const int i_top = a.im - 1;
-    if (i_base >= i_top) return;
+    const bool live = col && i_base < i_top;   // the column has levels to sweep
     const AtjupMicro& mc = a.mc;
     const double P_max_flux = 1.0e-4, dep_frac = 1.0, ratio_cap = 5.0, rs = mc.precip_rate_scale;
     const double c_c_au = 2.0e-8, c_i_au = 5.0e-8, q_c_crit = 5.0e-4, c_ac = 1.0e-7;
     const double c_rim = 1.0e-8, z_csg = 2.5e-8, a_ev = 2.76e-3, c_melt_K = 0.2, c_frz_K = 0.2;
     const double P_ref = 1.0e-4, v_fall = 2.0;
     const double nd = (a.L_atm * 1.0e3) / a.u_0;
-    for (int gq = 0; gq < 3; gq++) {
-        const AtjupGasParams& gs = mc.gas[gq];
-        const int sv = gq == 0 ? ATJUP_S_H2O : (gq == 1 ? ATJUP_S_NH3 : ATJUP_S_CH4);
-        double *vap = a.q[sv], *cld = a.q[sv + 1], *ice = a.q[sv + 2];
-        double *Sv = a.sprec[3 * gq], *Sc = a.sprec[3 * gq + 1], *Si = a.sprec[3 * gq + 2];
-        const double Lf = gs.ls - gs.lv;
-        double Pr = 0.0, Ps = 0.0, Pg = 0.0;
-        for (int i = i_top - 1; i >= i_base; i--) {
-            const size_t c = c0 + (size_t)i * plane;
-            const double T = a.t[c] * a.t_ref;
-            const double p_u = a.p_stat[c];
-            const double q_v = dmax(0.0, vap[c]), q_c = dmax(0.0, cld[c]), q_i = dmax(0.0, ice[c]);
+    const double Lf = gs.ls - gs.lv;
+    double Pr = 0.0, Ps = 0.0, Pg = 0.0;
+    // ring of the next PRECIP_AHEAD levels' inputs (level i - q in slot q - 1)
+    PrecipLevel ahead[PRECIP_AHEAD];
+#pragma unroll
+    for (int q = 0; q < PRECIP_AHEAD; q++) {
+        const int il = i_top - 1 - q;
+        if (live && il >= i_base) ahead[q] = precip_load(a, vap, cld, ice, c0 + (size_t)il * plane);
+    }
+    // every thread of the block walks the same levels (the barrier below is block-wide); a
+    // column takes part from its top level down to its base
+    for (int i = i_top - 1; i >= 0; i--) {
+        const bool act = live && i >= i_base;
+        const size_t c = c0 + (size_t)i * plane;
+        PrecipLevel L{};
+        if (act) {
+            L = ahead[0];
+#pragma unroll
+            for (int q = 0; q < PRECIP_AHEAD - 1; q++) ahead[q] = ahead[q + 1];
+            if (i - PRECIP_AHEAD >= i_base)
+                ahead[PRECIP_AHEAD - 1] = precip_load(a, vap, cld, ice, c - (size_t)PRECIP_AHEAD * plane);
+        }
+        const double dz = dmax(0.0, layer_dz_m(a, i));
+        if (dz <= 0.0) continue;          // the same for every thread: no barrier is skipped unevenly
+        double q_heat = 0.0;
+        if (act) {
+            const double T = L.t * a.t_ref;
+            const double p_u = L.p;
+            const double q_v = dmax(0.0, L.vap), q_c = dmax(0.0, L.cld), q_i = dmax(0.0, L.ice);
             const double E_r = svp(T, gs.C, gs.L0, gs.R, gs.del_alf, gs.del_bet);
             double rho = a.r_mix;
             if (a.local_rho) {
-                const double r = a.rho_mix[c];
+                const double r = L.rho;
                 if (r > 0.0 && isfinite(r)) rho = r;
             }
             const double q_sat = (p_u > E_r) ? rho * gs.ep * E_r / p_u : q_v;
-            const double dz = dmax(0.0, layer_dz_m(a, i));
-            if (dz <= 0.0) continue;
             const double F_r_in = Pr, F_s_in = Ps, F_g_in = Pg;
             const double Rain = dmin(ratio_cap, F_r_in / P_ref);
             const double Snow = dmin(ratio_cap, F_s_in / P_ref);
@@ -182,8 +237,8 @@ __global__ void precip_kernel(MicroArgs a) {
             const double F_ev_sat = dmax(0.0, q_sat - q_v) * v_fall;
             const double F_ev = dmin(dmin(S_ev_raw * dz, F_r_avail), F_ev_sat);
             const double S_ev = F_ev / dz;
-            a.Q_precip[c] += Lf * (S_s_rim + S_g_rim + S_csg) + Lf * (F_r_frz - F_s_melt - F_g_melt) / dz -
-                             gs.lv * F_ev / dz;
+            q_heat = Lf * (S_s_rim + S_g_rim + S_csg) + Lf * (F_r_frz - F_s_melt - F_g_melt) / dz -
+                     gs.lv * F_ev / dz;
             const double tau = dz / v_fall;
             const double d_c = dmin(dep_frac * q_c, (S_c_au + S_ac + S_s_rim + S_g_rim + S_csg) * tau);
             const double d_i = dmin(dep_frac * q_i, S_i_au * tau);
@@ -203,6 +258,11 @@ __global__ void precip_kernel(MicroArgs a) {
             Ps = dmin(P_max_flux, dmax(0.0, F_s));
             Pg = dmin(P_max_flux, dmax(0.0, F_g));
         }
+        const int b = i & 1;
+        contrib[b][gq][tx] = q_heat;
+        __syncthreads();
+        if (act && gq == 0)   // Q_precip += H2O, then NH3, then CH4 (Q_precip was zeroed above)
+            a.Q_precip[c] = ((0.0 + contrib[b][0][tx]) + contrib[b][1][tx]) + contrib[b][2][tx];
     }
 }
 
@@ -431,7 +491,7 @@ int launch_micro(AtjupCtx* c, int what) {
         c->launches++;
         break;
     case MICRO_PRECIP:
-        precip_kernel<<<gcol, TB, 0, c->stream>>>(a);
+        precip_kernel<<<dim3((P.km + PR_COLS - 1) / PR_COLS, P.jm), dim3(PR_COLS, 3), 0, c->stream>>>(a);
         c->launches++;
         break;
     case MICRO_NH4SH:

@@ -120,9 +120,15 @@ def stage_kernels(prec, phys):
             "closure": ("closure_stage_kernel", closure_stage_bytes(prec))}
 # (algorithmic bytes per cell and launch; times the cells of the shell)
 # DRAM bytes (read + write) per launch from ncu captures (profiles/); None until captured.
-# DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step,
-# from ncu captures (profiles/); None where not captured.
-STAGE_TRAFFIC_PER_CELL = {}
+# DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step:
+# dram__bytes_read.sum + dram__bytes_write.sum of each stage launch in one ncu capture of this
+# workload on the 41x181x361 shell (profiles/stage_traffic_phys_41x181x361.md).
+STAGE_TRAFFIC_PER_CELL = {
+    ("fp64", "species_stage_kernel"): 560.1, ("fp64", "closure_stage_kernel"): 100.1,
+    ("fp64", "rk_stage_kernel"): 199.4,
+    ("mixed", "species_stage_kernel"): 406.3, ("mixed", "closure_stage_kernel"): 68.4,
+    ("mixed", "rk_stage_kernel"): 153.4,
+}
 
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
@@ -364,6 +370,8 @@ def main():
                              "(tests/test_mixed.py)",
                  "species_stage_roofline": {"achieved": mk / (sms / sn / 1e3) / 1e9,
                                             "algorithmic_bytes_per_launch": mk,
+                                            "traffic": STAGE_TRAFFIC_PER_CELL.get(
+                                                ("mixed", "species_stage_kernel"), 0) * N_CELLS or None,
                                             "avg_launch_ms": sms / sn},
                  "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
                                                  sorted(mper.items(), key=lambda kv: -kv[1][0])},
