@@ -70,6 +70,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_turbulence.argtypes = [vp]
     L.atjup_gpu_set_micro.argtypes = [vp, ctypes.POINTER(_p.AtjupMicro)]
     L.atjup_gpu_set_precision.argtypes = [vp, i32]
+    L.atjup_gpu_save_state.argtypes = [vp, ctypes.c_char_p, i32, i32]
+    L.atjup_gpu_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i32)]
     for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species"):
         getattr(L, "atjup_gpu_" + n).argtypes = [vp]
     L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
@@ -165,6 +167,21 @@ class GpuModel:
         """The RK step's precision: params.PREC_FP64, or params.PREC_MIXED (FP32 stage buffers and
         accumulators, FP32 species and closure right-hand sides)."""
         _check(self.L.atjup_gpu_set_precision(self.ctx, int(precision)))
+
+    # ---- restart files ----
+    def save_state(self, path, iter_n: int, carried: int = 1) -> None:
+        """atjup_gpu_save_state: the reference's restart file of the state between steps -- JUP2
+        (carried = 1), JUP1 (0), or JUP2 with the trailer of the five arrays the reference's list
+        omits (2)."""
+        _check(self.L.atjup_gpu_save_state(self.ctx, str(path).encode(), int(iter_n), int(carried)))
+
+    def load_state(self, path) -> tuple[int, int]:
+        """atjup_gpu_load_state: (iteration in the header, carried: 0 JUP1, 1 JUP2, 2 JUP2 with
+        the trailer)."""
+        it, car = ctypes.c_int32(), ctypes.c_int32()
+        _check(self.L.atjup_gpu_load_state(self.ctx, str(path).encode(), ctypes.byref(it),
+                                           ctypes.byref(car)))
+        return it.value, car.value
 
     def upload_n(self, name: str, a) -> None:
         a = np.ascontiguousarray(a, np.float64).reshape(self.shape)

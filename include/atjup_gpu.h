@@ -377,6 +377,28 @@ int atjup_gpu_step(AtjupCtx* ctx, int32_t iter_n, int32_t first, const AtjupSolv
 /* Count of non-finite values in the prognostic fields (NaN/Inf census; no device trap). */
 int atjup_gpu_nonfinite_count(AtjupCtx* ctx, int64_t* count);
 
+/* ---- restart files (FileIO_Jup.cpp:261-683) ---- */
+
+/* cJupiterModel::save_state (FileIO_Jup.cpp:584-624): write the device state to `path` in the
+ * reference's restart format -- header {magic, im, jm, km, iter} (int32), then every array of
+ * restart_arrays() as im*jm rows of km doubles, and with carried != 0 (magic "JUP2") the arrays
+ * of restart_arrays_carried() and vel_star, else magic "JUP1". Call it between steps (after
+ * atjup_gpu_step), where every time-level-n copy equals its live field, as the reference does
+ * after restoreVar. thermalmassflux, a diagnostic this library does not compute, is written as
+ * zeros. carried = 2 also appends, after vel_star, a trailer ("ATJX", count, arrays) with the NH4SH
+ * mass flux and the NH3-cloud and CH4 precipitation sinks, which the next iterations read but the
+ * reference's list omits; the reference's loader does not read past vel_star. The reference names
+ * the file <output_path>/jup_restart_<iter>.bin. */
+int atjup_gpu_save_state(AtjupCtx* ctx, const char* path, int32_t iter, int32_t carried);
+/* cJupiterModel::load_state (FileIO_Jup.cpp:626-683): read a JUP1 or JUP2 file written by the
+ * reference or by atjup_gpu_save_state into the device state. The magic, the grid and the file
+ * size are checked before any device field is written (ATJUP_ERR_ARG and a message otherwise).
+ * iter receives the header's iteration, carried 0 for JUP1, 1 for JUP2, 2 for JUP2 with the
+ * trailer of atjup_gpu_save_state. Resume with
+ * atjup_gpu_step(iter + 1, first = !carried): the reference forces the physics block on the
+ * first resumed iteration only for a JUP1 file. */
+int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t* carried);
+
 /* Instrumentation (no reference counterpart: the reference prints wall-clock timers per routine,
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
  * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */

@@ -355,6 +355,23 @@ void ref_chem_fluxes() {
     JupiterUtils::damp_wiggles(m.fluxlim_nh4sh, &m.i_topography, true, true, true);
 }
 void ref_restore() { g_m->restoreVar(1.0); }
+
+// cJupiterModel::save_state / load_state (FileIO_Jup.cpp:584-683) with the model's output
+// directory pointed at dir for the call: the file is dir/jup_restart_<iter>.bin.
+int ref_save_state(const char* dir, int iter) {
+    const std::string keep = g_m->output_path;
+    g_m->output_path = dir;
+    g_m->save_state(iter);
+    g_m->output_path = keep;
+    return 0;
+}
+int ref_load_state(const char* dir, int iter) {
+    const std::string keep = g_m->output_path;
+    g_m->output_path = dir;
+    const bool ok = g_m->load_state(iter);
+    g_m->output_path = keep;
+    return ok ? 0 : 1;
+}
 void ref_mixture_density() { g_m->computeMixtureDensity(); }
 void ref_satadj(const char* gas) { gas_adjust(*g_m, gas); }
 

@@ -13,8 +13,8 @@ RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "al
 PROGNOSTIC = ("t", "u", "v", "w", "p_dyn") + SCALARS
 
 
-def ref_iters_case(iters=3):
-    d = ref_dump("--phys-iters", str(iters))
+def ref_iters_case(iters=3, *extra):
+    d = ref_dump("--phys-iters", str(iters), *extra)
     P = dump_params(d, env=MOIST_ENV)
     P.has_nue = 1
     P.has_heating = 1

@@ -234,7 +234,21 @@ ITER_FIELDS = ("t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wal
     "S_precip_ch4_ice")
 
 
-def phys_iters_case(ref, g, data, iters):
+# cJupiterModel::restart_arrays() and restart_arrays_carried() (FileIO_Jup.cpp:281-304), in file
+# order; vel_star follows them in a JUP2 file.
+RESTART_FIELDS = ("t", "u", "v", "w", "tn", "un", "vn", "wn",
+                  "h2o", "h2o_cloud", "h2o_ice", "h2on", "h2o_cloudn", "h2o_icen", "h2s", "h2sn",
+                  "nh3", "nh3_cloud", "nh3_ice", "nh3n", "nh3_cloudn", "nh3_icen",
+                  "ch4", "ch4_cloud", "ch4_ice", "ch4n", "ch4_cloudn", "ch4_icen",
+                  "nh4sh", "nh4shn", "p_dyn", "p_dynn", "p_stat", "tke", "dis", "tken", "disn",
+                  "nue")
+RESTART_CARRIED = ("aux_u", "aux_v", "aux_w", "difflux_h2s", "difflux_nh3", "massflux_h2s",
+                   "massflux_nh3", "fluxlim_nh4sh", "thermalmassflux", "Q_precip", "Q_rad",
+                   "rho_mix", "S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice",
+                   "S_precip_nh3", "S_precip_nh3_ice")
+
+
+def phys_iters_case(ref, g, data, iters, save_restart=None):
     """`iters` iterations of the loop with the physics on (closure, radiation, precipitation, the
     NH4SH equilibrium, the saturation adjustments), from the reference's own moist initial state;
     every field the iteration reads is recorded before, every field it writes after."""
@@ -263,6 +277,12 @@ def phys_iters_case(ref, g, data, iters):
             for n in ITER_FIELDS:
                 data[f"it{it}_{n}"] = ref.get(n)
             data[f"it{it}_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
+        if save_restart and it == save_restart[1]:
+            # the reference's restart file after this iteration, and every array it holds
+            ref.quiet(ref.L.ref_save_state, save_restart[0].encode(), it)
+            for n in RESTART_FIELDS + RESTART_CARRIED:
+                data[f"rs{it}_{n}"] = ref.get(n)
+            data[f"rs{it}_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
 
 
 def main():
@@ -281,17 +301,23 @@ def main():
     ap.add_argument("--phys-iters", type=int, default=0)
     ap.add_argument("--perturb-ulp", action="store_true",
                     help="with --phys-iters: start from t one ulp above the model's own (fluid cells)")
+    ap.add_argument("--save-restart", default=None, metavar="DIR:N",
+                    help="with --phys-iters: write the reference's restart file to DIR after "
+                         "iteration N (and record its arrays as rsN_*)")
+    ap.add_argument("--load-restart", default=None, metavar="DIR:N",
+                    help="load DIR/jup_restart_N.bin into the reference's moist model with its "
+                         "own load_state and record every restart array as rs_*")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
     env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
-    if a.micro or a.phys_iters:
+    if a.micro or a.phys_iters or a.load_restart:
         env = dict(MOIST_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro or a.phys_iters))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro or a.phys_iters or a.load_restart))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -312,7 +338,17 @@ def main():
         if a.perturb_ulp:
             t = ref.get("t")
             ref.set("t", np.where(g["solid"] == 0, np.nextafter(t, np.inf), t))
-        phys_iters_case(ref, g, data, a.phys_iters)
+        sr = None
+        if a.save_restart:
+            d_, n_ = a.save_restart.rsplit(":", 1)
+            sr = (d_, int(n_))
+        phys_iters_case(ref, g, data, a.phys_iters, sr)
+    elif a.load_restart:
+        d_, n_ = a.load_restart.rsplit(":", 1)
+        data["load_rc"] = np.array(ref.quiet(ref.L.ref_load_state, d_.encode(), int(n_)))
+        for n in RESTART_FIELDS + RESTART_CARRIED:
+            data["rs_" + n] = ref.get(n)
+        data["rs_vel_star"] = ref.get1("vel_star").reshape(ref.shape[1], ref.shape[2])
     elif a.satadj or a.satadj_synthetic:
         if a.satadj:
             f = perturb_moist({n: ref.get(n) for n in ("t",) + SPECIES}, g["solid"])
