@@ -25,7 +25,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-re
 # The microphysics decide branches on exact cancellations (a rain flux that evaporates completely
 # is 0, not +-1 ulp; a saturation test sits on its threshold): these files keep the reference's
 # rounding by being compiled without FMA contraction, as the reference is.
-PER_FILE = {"satadj.cu": ["-fmad=false"], "micro.cu": ["-fmad=false"]}
+PER_FILE = {"satadj.cu": ["-fmad=false"], "micro.cu": ["-fmad=false"], "mca.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

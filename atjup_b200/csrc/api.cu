@@ -72,6 +72,7 @@ void free_all(AtjupCtx* c) {
     for (auto& p : c->kf) { cudaFree(p); p = nullptr; }
     cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red); cudaFree(c->stage);
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
+    cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
     cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
@@ -455,6 +456,37 @@ int atjup_gpu_set_precision(AtjupCtx* c, int32_t prec) {
     return ATJUP_OK;
 }
 
+int atjup_gpu_set_mca(AtjupCtx* c, const AtjupMca* m) {
+    if (!c) { set_error("set_mca: null context"); return ATJUP_ERR_ARG; }
+    if (!m) { c->mca_on = false; return ATJUP_OK; }
+    if (!c->micro_on || !c->phys_on || !c->layer_h) {
+        set_error("set_mca: needs atjup_gpu_set_physics and atjup_gpu_set_micro first");
+        return ATJUP_ERR_ARG;
+    }
+    c->mca = *m;
+    c->mca_on = m->stride > 0;
+    return mca_setup(c);
+}
+
+int atjup_gpu_mca(AtjupCtx* c, AtjupMcaStats* st) {
+    if (!c || !c->mca_bounds || !c->micro_on) { set_error("mca: atjup_gpu_set_mca was not called"); return ATJUP_ERR_ARG; }
+    {
+        Timed tm(c, TK_MCA);
+        int rc = launch_mca(c);
+        if (rc) return rc;
+    }
+    if (st) {
+        unsigned long long h[8];
+        ATJUP_CUDA(cudaMemcpyAsync(h, c->mca_stats, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+        ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+        st->columns = (int64_t)h[0]; st->layers = (int64_t)h[1];
+        st->moist_triggers = (int64_t)h[2]; st->dry_triggers = (int64_t)h[3];
+        st->unstable_t = (int64_t)h[4]; st->held = (int64_t)h[5]; st->skipped = (int64_t)h[6];
+        st->max_passes = (int32_t)h[7]; st->pad = 0;
+    }
+    return ATJUP_OK;
+}
+
 int atjup_gpu_set_physics(AtjupCtx* c, const AtjupPhysics* ph, const float* layer_heights_km) {
     if (!c) { set_error("set_physics: null context"); return ATJUP_ERR_ARG; }
     if (!ph) { c->phys_on = false; return ATJUP_OK; }
@@ -751,6 +783,10 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
     if (ph && c->phys.turb_on) {                      // ATJUP_TURB_WALL_HOLD 1
         Timed tm(c, TK_TURB);
         if ((rc = launch_turb_wall_hold(c))) return rc;
+    }
+    if (ph && c->mca_on && iter_n % c->mca.stride == 0) {
+        Timed tm(c, TK_MCA);
+        if ((rc = launch_mca(c))) return rc;
     }
     if (P.shapiro_inloop > 0) {
         for (int f = ATJUP_F_U; f <= ATJUP_F_W; f++)

@@ -67,6 +67,13 @@ struct AtjupCtx {
     // storage of the RK stage buffers and accumulators: ATJUP_PREC_FP64, or ATJUP_PREC_MIXED (FP32)
     int step_prec = ATJUP_PREC_FP64;
     AtjupMicro micro{};
+    // moist convective adjustment (mca.cu)
+    bool mca_on = false;
+    AtjupMca mca{};
+    void* mca_bounds = nullptr;     // int2 [jm * km]: the column's (i0, i1)
+    void* mca_flags = nullptr;      // unsigned [2 * jm * km + 1]: flags, list, count
+    void* mca_slots = nullptr;      // per-thread column scratch of the column kernel
+    void* mca_stats = nullptr;      // unsigned long long [8]
     double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
@@ -125,7 +132,7 @@ void set_error(const std::string& msg);
 
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
-       TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_COUNT };
+       TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_MCA, TK_COUNT };
 void timer_begin(AtjupCtx* c, int cls);
 void timer_end(AtjupCtx* c);
 int cuda_status(cudaError_t e, const char* what);
@@ -138,6 +145,8 @@ inline size_t cell(const AtjupCtx* c, int i, int j, int k) {
 int launch_buoy_ref(AtjupCtx* c, const double* t);
 int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w);
 int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout);
+int mca_setup(AtjupCtx* c);
+int launch_mca(AtjupCtx* c);
 int launch_mixture_density(AtjupCtx* c);
 int launch_prepare_projection(AtjupCtx* c);
 int launch_pressure_source(AtjupCtx* c);

@@ -70,6 +70,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_turbulence.argtypes = [vp]
     L.atjup_gpu_set_micro.argtypes = [vp, ctypes.POINTER(_p.AtjupMicro)]
     L.atjup_gpu_set_precision.argtypes = [vp, i32]
+    L.atjup_gpu_set_mca.argtypes = [vp, ctypes.POINTER(_p.AtjupMca)]
+    L.atjup_gpu_mca.argtypes = [vp, ctypes.POINTER(_p.AtjupMcaStats)]
     L.atjup_gpu_save_state.argtypes = [vp, ctypes.c_char_p, i32, i32]
     L.atjup_gpu_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i32)]
     for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species"):
@@ -167,6 +169,16 @@ class GpuModel:
         """The RK step's precision: params.PREC_FP64, or params.PREC_MIXED (FP32 stage buffers and
         accumulators, FP32 species and closure right-hand sides)."""
         _check(self.L.atjup_gpu_set_precision(self.ctx, int(precision)))
+
+    def set_mca(self, mca: "_p.AtjupMca | None") -> None:
+        """atjup_gpu_set_mca: the moist convective adjustment of the iteration (None: off)."""
+        _check(self.L.atjup_gpu_set_mca(self.ctx, ctypes.byref(mca) if mca is not None else None))
+
+    def mca(self) -> dict:
+        """atjup_gpu_mca: one moist convective adjustment of the device state; its counters."""
+        st = _p.AtjupMcaStats()
+        _check(self.L.atjup_gpu_mca(self.ctx, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in st._fields_ if n != "pad"}
 
     # ---- restart files ----
     def save_state(self, path, iter_n: int, carried: int = 1) -> None:
@@ -306,7 +318,7 @@ class GpuModel:
 
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
-                      "mixture", "solver", "satadj", "species", "closure", "turb", "micro")
+                      "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

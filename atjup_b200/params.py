@@ -235,6 +235,43 @@ def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, 
     return mc
 
 
+class AtjupMca(ctypes.Structure):
+    """Mirror of AtjupMca (the moist convective adjustment)."""
+    _fields_ = [(n, ctypes.c_int32) for n in ("stride", "ledoux", "loading", "interior",
+                                               "max_pass", "pad")] + [
+        (n, ctypes.c_double) for n in ("relax", "ep_h2s", "L_nh4sh")]
+
+
+class AtjupMcaStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("columns", "layers", "moist_triggers",
+                                               "dry_triggers", "unstable_t", "held", "skipped")] + [
+        ("max_passes", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+# ChemistryJup::nh4sh_formation_heat (ChemistryJup.h:283): 4705 ln(10) R_univ / m_nh4sh [J/kg]
+NH4SH_FORMATION_HEAT = 4705.0 * math.log(10.0) * 8314.46 / 51.1114
+EP_H2S = 15.35                      # cJupiterModel.h:418
+
+
+def resolve_mca(env: Mapping[str, str] | None = None) -> AtjupMca:
+    """The moist convective adjustment with the reference's defaults (cJupiterModel.cpp:115-124,
+    ConvectiveAdjustment.h:403-420, cJupiterModel.h:1038-1042): ATJUP_MCA 1 (every iteration),
+    ATJUP_MCA_LEDOUX 1, ATJUP_MCA_LOADING 1, ATJUP_MCA_INTERIOR 1, ATJUP_MCA_PASSES 64,
+    ATJUP_MCA_RELAX 1; NH4SH carries its heat of formation when ATJUP_NH4SH_EQ is on."""
+    env = os.environ if env is None else env
+    m = AtjupMca()
+    m.stride = max(0, _env(env, "ATJUP_MCA", 1))
+    m.ledoux = int(_env(env, "ATJUP_MCA_LEDOUX", 1) != 0)
+    m.loading = int(_env(env, "ATJUP_MCA_LOADING", 1) != 0)
+    m.interior = int(_env(env, "ATJUP_MCA_INTERIOR", 1) != 0)
+    passes = _env(env, "ATJUP_MCA_PASSES", 64)
+    m.max_pass = passes if passes > 0 else 64
+    m.relax = min(1.0, max(0.0, _env(env, "ATJUP_MCA_RELAX", 1.0, float)))
+    m.ep_h2s = EP_H2S
+    m.L_nh4sh = NH4SH_FORMATION_HEAT if _env(env, "ATJUP_NH4SH_EQ", 1) != 0 else 0.0
+    return m
+
+
 class AtjupSatStats(ctypes.Structure):
     _fields_ = [("adjusted", ctypes.c_int64), ("not_converged", ctypes.c_int64),
                 ("dry_exits", ctypes.c_int64)]
@@ -399,7 +436,10 @@ _UNSUPPORTED = {
     "ATJUP_BC_POLE_COPY": ("1", "pole rows are copies"),
     "ATJUP_DAMP_PDYN": ("0", "no Shapiro pass on p_dyn in the loop"),
     "ATJUP_HYDRO_REF": ("0", "the hydrostatic integral runs upward from the base"),
-    "ATJUP_MCA": ("0", "the moist convective adjustment is not implemented (set ATJUP_MCA=0)"),
+    "ATJUP_MCA_SMOOTH": ("0", "the latitude-smoothed stability search is not implemented"),
+    "ATJUP_MCA_PHASE": ("0", "the temperature-split phase rule is not implemented"),
+    "ATJUP_CHROM": ("0", "the chromophore tracer is not implemented"),
+    "ATJUP_CONV_ADJ": ("0", "the dry convective adjustment is not implemented"),
 }
 
 
@@ -411,4 +451,8 @@ def check_supported(env: Mapping[str, str] | None = None) -> list[str]:
         v = env.get(name)
         if v is not None and str(int(float(v)) if v.strip().lstrip("-").replace(".", "", 1).isdigit() else v) != ok:
             bad.append(f"{name}={v}: {why}")
+    # the dry convective adjustment defaults to ATJUP_NONDIM (cJupiterModel.cpp:125-131)
+    if env.get("ATJUP_CONV_ADJ") is None and _env(env, "ATJUP_NONDIM", 0) != 0:
+        bad.append("ATJUP_NONDIM set without ATJUP_CONV_ADJ=0: the dry convective adjustment it "
+                   "switches on is not implemented")
     return bad

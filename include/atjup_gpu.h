@@ -363,6 +363,44 @@ int atjup_gpu_chemistry(AtjupCtx* ctx);
 /* cJupiterModel::clampNegativeSpecies (FileIO_Jup.cpp:494-548): species < 0 or NaN -> 0. */
 int atjup_gpu_clamp_species(AtjupCtx* ctx);
 
+/* ---- moist convective adjustment, Ledoux criterion (ConvectiveAdjustment.h:275-849) ---- */
+
+/* The knobs of MoistConvectiveAdjustment<cJupiterModel>::run (ConvectiveAdjustment.h:403-420) and
+ * the driver's tracer constants (cJupiterModel.cpp:1300-1320). The two gases are H2O and NH3 with
+ * the saturation constants of the micro block (AtjupMicro.gas[0], gas[1]); the tracers are H2S (a
+ * gas in the virtual temperature, ep_h2s) and NH4SH (a condensate carrying its heat of formation,
+ * L_nh4sh). The reference's chromophore tracer is zero unless ATJUP_CHROM is on, which this
+ * library does not provide. Latitude smoothing (MCA_SMOOTH > 0), the temperature-split phase rule
+ * (MCA_PHASE 1) and cp(T) (CP_H2, CP_GAS) are Jupiter's defaults off and not provided. */
+typedef struct AtjupMca {
+    int32_t stride;              /* ATJUP_MCA 1: every N iterations, after the boundary passes   */
+    int32_t ledoux;              /* ATJUP_MCA_LEDOUX 1: composition in the density test          */
+    int32_t loading;             /* ATJUP_MCA_LOADING 1: condensate weight in the density test   */
+    int32_t interior;            /* ATJUP_MCA_INTERIOR 1: radial boundary planes left out        */
+    int32_t max_pass;            /* ATJUP_MCA_PASSES 64: sweep cap per column                    */
+    int32_t pad;
+    double relax;                /* ATJUP_MCA_RELAX 1: fraction of the adjustment applied        */
+    double ep_h2s;               /* 15.35: H2S molar-mass ratio (cJupiterModel.h:418)            */
+    double L_nh4sh;              /* NH4SH heat of formation [J/kg] with ATJUP_NH4SH_EQ, else 0   */
+} AtjupMca;
+
+typedef struct AtjupMcaStats {
+    int64_t columns;             /* columns adjusted                                             */
+    int64_t layers;              /* cells mixed, summed over the segments                        */
+    int64_t moist_triggers, dry_triggers;   /* first-sweep segments started by a saturated /    */
+                                            /* unsaturated parcel                               */
+    int64_t unstable_t, held;    /* pairs unstable in T; of those, held by their composition    */
+    int64_t skipped;             /* columns left alone (no positive state, failed solve)         */
+    int32_t max_passes, pad;     /* the most sweeps a column used                                */
+} AtjupMcaStats;
+
+/* Set (or with NULL clear) the moist convective adjustment of the iteration; needs the micro
+ * block (the gases' constants) and the physics block (the species). */
+int atjup_gpu_set_mca(AtjupCtx* ctx, const AtjupMca* mca);
+/* MoistConvectiveAdjustment<cJupiterModel>::run on the device state: t and the H2O, NH3, H2S,
+ * NH4SH fields of every column that holds an unstable pair. stats may be NULL. */
+int atjup_gpu_mca(AtjupCtx* ctx, AtjupMcaStats* stats);
+
 /* One iteration of cJupiterModel::Run's loop (cJupiterModel.cpp:1032-1381). Dry: pressure
  * solve on even iterations (and when first != 0), mixture density, RK4, boundary passes,
  * in-loop Shapiro, column balance of v; restoreVar is implicit (the device state is the time
@@ -370,8 +408,8 @@ int atjup_gpu_clamp_species(AtjupCtx* ctx);
  * schedule: on even iterations (and the first) also radiation, the H2O, NH3, CH4 saturation
  * adjustments, the NH4SH equilibrium, precipitation, the n copies of the condensables, the
  * turbulence update and the chemistry block; every iteration RK4 of the 17 fields, the boundary
- * passes of every field list, the closure's wall hold, Shapiro, the column balance, the species
- * clamp and restoreVar of the scalars. solve may be NULL (= params->press_sweeps sweeps). */
+ * passes of every field list, the closure's wall hold, the moist convective adjustment (when set,
+ * on its stride), Shapiro, the column balance, the species clamp and restoreVar of the scalars. solve may be NULL (= params->press_sweeps sweeps). */
 int atjup_gpu_step(AtjupCtx* ctx, int32_t iter_n, int32_t first, const AtjupSolveOpts* solve);
 
 /* Count of non-finite values in the prognostic fields (NaN/Inf census; no device trap). */
@@ -404,7 +442,7 @@ int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t
  * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */
 enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
        ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_SPECIES,
-       ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_COUNT };
+       ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */

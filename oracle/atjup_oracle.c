@@ -2309,9 +2309,308 @@ void ora_clamp_species(const AtjupParams* P, ora_phys* X) {
  * ATJUP_RK_SCALAR_SYNC = 2, the closure update and the chemistry block; every iteration runs RK4,
  * the boundary passes, the closure's wall law again, the in-loop Shapiro filter, the column
  * balance of v, the species clamp and restoreVar). S->nue must be X->nue_out. */
+/* -------------------------------------------------------------------------------------------
+ * Moist convective adjustment with the Ledoux criterion (ConvectiveAdjustment.h:403-849, the
+ * driver's call at cJupiterModel.cpp:1300-1320) with Jupiter's defaults: no latitude smoothing,
+ * the t_0 phase rule, constant cp. Gases H2O and NH3 (MC->gas[0], gas[1]); tracers H2S (a gas in
+ * the virtual temperature) and NH4SH (a condensate carrying its heat of formation). The report
+ * counters go to stats[8] = {columns, layers, moist triggers, dry triggers, pairs unstable in T,
+ * of those held, skipped, most sweeps}; the conservation drift is print-only in the reference.
+ * ------------------------------------------------------------------------------------------- */
+enum { MCA_NG = 2, MCA_NT = 2, MCA_MAXI = 128, MCA_NITER = 60 };
+static const double MCA_TOL_K = 1.0e-7, MCA_TOL_T = 1.0e-10;
+
+typedef struct {
+    const AtjupGasParams* g[MCA_NG];
+    double tr_ep[MCA_NT], tr_L[MCA_NT];
+    int tr_cond[MCA_NT];
+    double cp, grav;
+    int ledoux, loading;
+} mca_ctx;
+
+/* mass fraction at saturation over the phase T selects (ConvectiveAdjustment.h:440-453) */
+static double mca_qsat(const mca_ctx* M, int g, double T, double p) {
+    const AtjupGasParams* s = M->g[g];
+    const double E = (T >= s->t_0) ? ora_svp(T, s->C, s->L0, s->R, s->del_alf, s->del_bet)
+                                   : ora_svp(T, s->C_i, s->L0_i, s->R, s->del_alf_i, s->del_bet_i);
+    const double q = s->ep * E / p;
+    return isfinite(q) ? q : 0.0;
+}
+static double mca_lat(const mca_ctx* M, int g, double T) {
+    return T >= M->g[g]->t_0 ? M->g[g]->lv : M->g[g]->ls;
+}
+static double mca_fof(const mca_ctx* M, double TT, double hL, const double* qt, double p, double z) {
+    double f = M->cp * TT + M->grav * z - hL;
+    for (int g = 0; g < MCA_NG; g++) f -= mca_lat(M, g, TT) * dmax(0.0, qt[g] - mca_qsat(M, g, TT, p));
+    return f;
+}
+/* equilibrium temperature of (h_L, q_t) at (p, z) by Illinois regula falsi in the bracket
+ * [all vapour, all condensed] (ConvectiveAdjustment.h:459-486) */
+static int mca_equil(const mca_ctx* M, double hL, const double* qt, double p, double z, double* T,
+                     double* cond) {
+    const double T_lo = (hL - M->grav * z) / M->cp;
+    if (!(T_lo > 0.0) || !(p > 0.0)) return 0;
+    int any = 0;
+    for (int g = 0; g < MCA_NG; g++) if (qt[g] > mca_qsat(M, g, T_lo, p)) { any = 1; break; }
+    if (!any) {
+        *T = T_lo;
+        for (int g = 0; g < MCA_NG; g++) cond[g] = 0.0;
+        return 1;
+    }
+    double span = 0.0;
+    for (int g = 0; g < MCA_NG; g++) span += dmax(M->g[g]->lv, M->g[g]->ls) * dmax(0.0, qt[g]);
+    double a = T_lo, b = T_lo + span / M->cp + 1.0e-9;
+    double fa = mca_fof(M, a, hL, qt, p, z), fb = mca_fof(M, b, hL, qt, p, z);
+    int side = 0;
+    for (int it = 0; it < MCA_NITER && b - a > MCA_TOL_T; it++) {
+        double c = (fb - fa != 0.0) ? b - fb * (b - a) / (fb - fa) : 0.5 * (a + b);
+        if (!(c > a && c < b)) c = 0.5 * (a + b);
+        const double fc = mca_fof(M, c, hL, qt, p, z);
+        if (fc < 0.0) { a = c; fa = fc; if (side == -1) fb *= 0.5; side = -1; }
+        else          { b = c; fb = fc; if (side == +1) fa *= 0.5; side = +1; }
+        if (fabs(fc) <= M->cp * MCA_TOL_T) { a = b = c; break; }
+    }
+    *T = b;
+    for (int g = 0; g < MCA_NG; g++) cond[g] = dmax(0.0, qt[g] - mca_qsat(M, g, *T, p));
+    return 1;
+}
+
+/* one column's state and the parcel test (ConvectiveAdjustment.h:524-675) */
+typedef struct {
+    double T[MCA_MAXI], p[MCA_MAXI], z[MCA_MAXI], rho[MCA_MAXI], w[MCA_MAXI], hL[MCA_MAXI];
+    double T0[MCA_MAXI], Teq[MCA_MAXI], hL0[MCA_MAXI];
+    double qt[MCA_MAXI * MCA_NG], qv[MCA_MAXI * MCA_NG], qc[MCA_MAXI * MCA_NG];
+    double qi[MCA_MAXI * MCA_NG], ceq[MCA_MAXI * MCA_NG], qt0[MCA_MAXI * MCA_NG];
+    double qr[MCA_MAXI * MCA_NT], qr0[MCA_MAXI * MCA_NT];
+    char eq_ok[MCA_MAXI], touched[MCA_MAXI], cen_u[MCA_MAXI], cen_m[MCA_MAXI];
+} mca_col;
+
+static double mca_trE(const mca_ctx* M, const mca_col* C, int i) {
+    double e = 0.0;
+    for (int r = 0; r < MCA_NT; r++) e += M->tr_L[r] * C->qr[i * MCA_NT + r];
+    return e;
+}
+static double mca_tv(const mca_ctx* M, const mca_col* C, double TT, const double* v,
+                     const double* cnd, int i) {
+    if (!M->ledoux) return TT;
+    double f = 1.0;
+    for (int g = 0; g < MCA_NG; g++) {
+        f += v[g] * (1.0 / M->g[g]->ep - 1.0);
+        if (M->loading) f -= cnd[g];
+    }
+    for (int r = 0; r < MCA_NT; r++) {
+        const double q = C->qr[i * MCA_NT + r];
+        if (M->tr_ep[r] > 0.0) f += q * (1.0 / M->tr_ep[r] - 1.0);
+        else if (M->tr_cond[r] && M->loading) f -= q;
+    }
+    return TT * f;
+}
+/* parcel from a lifted to b: unstable when lighter than the air at b in its own equilibrium */
+static int mca_unstable(const mca_ctx* M, mca_col* C, int a, int b, int* held, int* moist) {
+    double Tp, pc[MCA_NG], pv[MCA_NG], ec[MCA_NG], ev[MCA_NG];
+    if (!mca_equil(M, C->hL[a] + mca_trE(M, C, a), &C->qt[a * MCA_NG], C->p[b], C->z[b], &Tp, pc))
+        return 0;
+    if (!C->eq_ok[b]) {
+        if (!mca_equil(M, C->hL[b] + mca_trE(M, C, b), &C->qt[b * MCA_NG], C->p[b], C->z[b],
+                       &C->Teq[b], &C->ceq[b * MCA_NG]))
+            return 0;
+        C->eq_ok[b] = 1;
+    }
+    const double Tb = C->Teq[b];
+    int wet = 0;
+    for (int g = 0; g < MCA_NG; g++) {
+        ec[g] = C->ceq[b * MCA_NG + g];
+        pv[g] = C->qt[a * MCA_NG + g] - pc[g];
+        if (pc[g] > 0.0) wet = 1;
+        ev[g] = C->qt[b * MCA_NG + g] - ec[g];
+    }
+    const double dTv = mca_tv(M, C, Tp, pv, pc, a) - mca_tv(M, C, Tb, ev, ec, b);
+    if (held) *held = (Tp - Tb > MCA_TOL_K) && !(dTv > MCA_TOL_K);
+    if (moist) *moist = wet;
+    return dTv > MCA_TOL_K;
+}
+/* cell q to equilibrium from its h_L and q_t */
+static int mca_settle(const mca_ctx* M, mca_col* C, int q) {
+    double TT, pc[MCA_NG];
+    if (!mca_equil(M, C->hL[q] + mca_trE(M, C, q), &C->qt[q * MCA_NG], C->p[q], C->z[q], &TT, pc))
+        return 0;
+    C->T[q] = TT;
+    C->Teq[q] = TT;
+    C->eq_ok[q] = 1;
+    for (int g = 0; g < MCA_NG; g++) {
+        const int x = q * MCA_NG + g;
+        C->ceq[x] = pc[g];
+        C->qv[x] = C->qt[x] - pc[g];
+        if (TT >= M->g[g]->t_0) { C->qc[x] = pc[g]; C->qi[x] = 0.0; }
+        else { C->qi[x] = pc[g]; C->qc[x] = 0.0; }
+    }
+    C->touched[q] = 1;
+    return 1;
+}
+/* mix h_L, q_t and the tracers over [a, b], mass-weighted, and settle every cell */
+static int mca_mix(const mca_ctx* M, mca_col* C, int a, int b) {
+    double sw = 0.0, sh = 0.0, sq[MCA_NG] = {0.0}, sr[MCA_NT] = {0.0};
+    for (int q = a; q <= b; q++) {
+        sw += C->w[q];
+        sh += C->w[q] * C->hL[q];
+        for (int g = 0; g < MCA_NG; g++) sq[g] += C->w[q] * C->qt[q * MCA_NG + g];
+        for (int r = 0; r < MCA_NT; r++) sr[r] += C->w[q] * C->qr[q * MCA_NT + r];
+    }
+    for (int q = a; q <= b; q++) {
+        C->hL[q] = sh / sw;
+        for (int g = 0; g < MCA_NG; g++) C->qt[q * MCA_NG + g] = sq[g] / sw;
+        for (int r = 0; r < MCA_NT; r++) C->qr[q * MCA_NT + r] = sr[r] / sw;
+        if (!mca_settle(M, C, q)) return 0;
+    }
+    return 1;
+}
+
+void ora_mca(const AtjupParams* P, const AtjupMicro* MC, const AtjupMca* A, const ora_grid* G,
+             ora_state* S, ora_phys* X, int64_t* stats) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    mca_ctx M;
+    M.g[0] = &MC->gas[0];
+    M.g[1] = &MC->gas[1];
+    M.tr_ep[0] = A->ep_h2s; M.tr_cond[0] = 0; M.tr_L[0] = 0.0;     /* H2S   */
+    M.tr_ep[1] = 0.0;       M.tr_cond[1] = 1; M.tr_L[1] = A->L_nh4sh;   /* NH4SH */
+    M.cp = P->cp_mix;
+    M.grav = P->g;
+    M.ledoux = A->ledoux;
+    M.loading = A->loading;
+    const double relax = dmin(1.0, dmax(0.0, A->relax));
+    const int max_pass = A->max_pass > 0 ? A->max_pass : 64;
+    double* vap[MCA_NG] = {X->q[ATJUP_S_H2O], X->q[ATJUP_S_NH3]};
+    double* cld[MCA_NG] = {X->q[ATJUP_S_H2O_CLOUD], X->q[ATJUP_S_NH3_CLOUD]};
+    double* ice[MCA_NG] = {X->q[ATJUP_S_H2O_ICE], X->q[ATJUP_S_NH3_ICE]};
+    double* trf[MCA_NT] = {X->q[ATJUP_S_H2S], X->q[ATJUP_S_NH4SH]};
+    int64_t st[8] = {0};
+    mca_col* C = (mca_col*)malloc(sizeof(mca_col));
+    if (!C || im > MCA_MAXI) { free(C); return; }
+    for (int j = 0; j < jm; j++) {
+        for (int k = 0; k < km; k++) {
+            int i0 = 0;
+            while (i0 < im && G->solid[IDX(i0, j, k)] == 1) i0++;
+            int i1 = i0;
+            while (i1 + 1 < im && G->solid[IDX(i1 + 1, j, k)] != 1) i1++;
+            if (A->interior) { if (i0 == 0) i0 = 1; if (i1 == im - 1) i1 = im - 2; }
+            if (i1 - i0 < 1) continue;
+            memset(C->eq_ok, 0, sizeof C->eq_ok);
+            memset(C->touched, 0, sizeof C->touched);
+            int ok = 1;
+            for (int i = i0; i <= i1 && ok; i++) {
+                const size_t c = IDX(i, j, k);
+                C->T[i] = C->T0[i] = S->t[c] * P->t_ref;
+                C->p[i] = S->p_stat[c];
+                C->z[i] = (double)X->layer_heights[i] * 1.0e3;
+                double r = P->r_mix;
+                if (P->local_rho) { const double rr = S->rho_mix[c]; r = (rr > 0.0 && isfinite(rr)) ? rr : P->r_mix; }
+                C->rho[i] = r;
+                if (!(C->T[i] > 0.0) || !(C->p[i] > 0.0) || !(C->rho[i] > 0.0) ||
+                    !isfinite(C->T[i] + C->p[i] + C->rho[i]))
+                    ok = 0;
+            }
+            if (!ok) { st[6]++; continue; }
+            for (int i = i0; i <= i1 && ok; i++) {
+                const size_t c = IDX(i, j, k);
+                const double lo = (i > i0) ? 0.5 * (C->z[i - 1] + C->z[i]) : C->z[i0];
+                const double hi = (i < i1) ? 0.5 * (C->z[i] + C->z[i + 1]) : C->z[i1];
+                C->w[i] = C->rho[i] * (hi - lo);
+                if (!(C->w[i] > 0.0)) ok = 0;
+                double h = M.cp * C->T[i] + M.grav * C->z[i];
+                for (int g = 0; g < MCA_NG; g++) {
+                    const int x = i * MCA_NG + g;
+                    C->qv[x] = dmax(0.0, vap[g][c]) / C->rho[i];
+                    C->qc[x] = dmax(0.0, cld[g][c]) / C->rho[i];
+                    C->qi[x] = dmax(0.0, ice[g][c]) / C->rho[i];
+                    C->qt[x] = C->qv[x] + C->qc[x] + C->qi[x];
+                    h -= M.g[g]->lv * C->qc[x] + M.g[g]->ls * C->qi[x];
+                }
+                for (int r = 0; r < MCA_NT; r++) {
+                    C->qr[i * MCA_NT + r] = trf[r][c] / C->rho[i];
+                    h -= M.tr_L[r] * C->qr[i * MCA_NT + r];
+                }
+                C->hL[i] = h;
+            }
+            if (!ok) { st[6]++; continue; }
+            /* census of the unadjusted column */
+            for (int i = i0; i < i1; i++) {
+                int held = 0, moist = 0;
+                const int u = mca_unstable(&M, C, i, i + 1, &held, &moist);
+                C->cen_u[i] = (char)u;
+                C->cen_m[i] = (char)moist;
+                if (u || held) st[4]++;
+                if (held) st[5]++;
+            }
+            memcpy(C->hL0, C->hL, sizeof C->hL);
+            memcpy(C->qt0, C->qt, sizeof C->qt);
+            memcpy(C->qr0, C->qr, sizeof C->qr);
+            int passes = 0, changed = 1, fail = 0;
+            int64_t layers = 0;
+            while (changed && passes < max_pass && !fail) {
+                changed = 0;
+                passes++;
+                int i = i0;
+                while (i < i1 && !fail) {
+                    int moist = 0, uns;
+                    if (passes == 1 && !C->touched[i] && !C->touched[i + 1]) { uns = C->cen_u[i]; moist = C->cen_m[i]; }
+                    else uns = mca_unstable(&M, C, i, i + 1, NULL, &moist);
+                    if (!uns) { i++; continue; }
+                    if (passes == 1) { if (moist) st[2]++; else st[3]++; }
+                    int a = i, b = i + 1;
+                    for (;;) {
+                        if (!mca_mix(&M, C, a, b)) { fail = 1; break; }
+                        int ext = 0;
+                        if (a > i0 && mca_unstable(&M, C, a - 1, a, NULL, NULL)) { a--; ext = 1; }
+                        if (b < i1 && mca_unstable(&M, C, b, b + 1, NULL, NULL)) { b++; ext = 1; }
+                        if (!ext) break;
+                    }
+                    layers += b - a + 1;
+                    changed = 1;
+                    i = b;
+                }
+            }
+            if (fail) { st[6]++; continue; }
+            if (layers == 0) continue;
+            if (relax < 1.0) {
+                for (int q = i0; q <= i1 && !fail; q++) {
+                    if (!C->touched[q]) continue;
+                    C->hL[q] = C->hL0[q] + relax * (C->hL[q] - C->hL0[q]);
+                    for (int g = 0; g < MCA_NG; g++) {
+                        const int x = q * MCA_NG + g;
+                        C->qt[x] = C->qt0[x] + relax * (C->qt[x] - C->qt0[x]);
+                    }
+                    for (int r = 0; r < MCA_NT; r++) {
+                        const int x = q * MCA_NT + r;
+                        C->qr[x] = C->qr0[x] + relax * (C->qr[x] - C->qr0[x]);
+                    }
+                    if (!mca_settle(&M, C, q)) fail = 1;
+                }
+                if (fail) { st[6]++; continue; }
+            }
+            for (int q = i0; q <= i1; q++) {
+                if (!C->touched[q]) continue;
+                const size_t c = IDX(q, j, k);
+                S->t[c] = C->T[q] / P->t_ref;
+                for (int g = 0; g < MCA_NG; g++) {
+                    const int x = q * MCA_NG + g;
+                    vap[g][c] = C->qv[x] * C->rho[q];
+                    cld[g][c] = C->qc[x] * C->rho[q];
+                    ice[g][c] = C->qi[x] * C->rho[q];
+                }
+                for (int r = 0; r < MCA_NT; r++) trf[r][c] = C->qr[q * MCA_NT + r] * C->rho[q];
+            }
+            st[0]++;
+            st[1] += layers;
+            if (passes > st[7]) st[7] = passes;
+        }
+    }
+    free(C);
+    if (stats) memcpy(stats, st, sizeof st);
+}
+
 void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const AtjupMicro* MC,
-                        const ora_grid* G, ora_state* S, ora_phys* X, int iter_n, int first,
-                        int sweeps) {
+                        const AtjupMca* MCA, const ora_grid* G, ora_state* S, ora_phys* X,
+                        int iter_n, int first, int sweeps) {
     const size_t N = (size_t)P->im * P->jm * P->km;
     if (iter_n % 2 == 0 || first) {
         ora_pressure_sweeps(P, G, S, sweeps, 1.0, NULL);
@@ -2347,6 +2646,7 @@ void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const Atju
         ora_turb_wall_bc(P, PH, G, X);
         ora_turb_wall_omega(P, PH, G, X);
     }
+    if (MCA && MCA->stride > 0 && iter_n % MCA->stride == 0) ora_mca(P, MC, MCA, G, S, X, NULL);
     if (P->shapiro_inloop > 0) {
         ora_shapiro(P, G, S->u, 4, P->shapiro_strength, P->shapiro_inloop, 1);
         ora_shapiro(P, G, S->v, 4, P->shapiro_strength, P->shapiro_inloop, 1);

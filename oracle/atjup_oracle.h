@@ -131,10 +131,13 @@ void ora_clamp_species(const AtjupParams* P, ora_phys* X);
 /* Turbulence.h:383-422 apply_wall_bc and the driver's turbWallOmega (cJupiterModel.cpp:360-377) */
 void ora_turb_wall_bc(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X);
 void ora_turb_wall_omega(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* G, ora_phys* X);
-/* One iteration of cJupiterModel.cpp:1032-1381 with the physics on */
+/* MoistConvectiveAdjustment<cJupiterModel>::run (ConvectiveAdjustment.h:403-849); stats[8] */
+void ora_mca(const AtjupParams* P, const AtjupMicro* MC, const AtjupMca* A, const ora_grid* G,
+             ora_state* S, ora_phys* X, int64_t* stats);
+/* One iteration of cJupiterModel.cpp:1032-1381 with the physics on; MCA may be NULL (off) */
 void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const AtjupMicro* MC,
-                        const ora_grid* G, ora_state* S, ora_phys* X, int iter_n, int first,
-                        int sweeps);
+                        const AtjupMca* MCA, const ora_grid* G, ora_state* S, ora_phys* X,
+                        int iter_n, int first, int sweeps);
 /* One dry iteration of cJupiterModel.cpp:1032-1381 */
 void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
                        int first, int sweeps);

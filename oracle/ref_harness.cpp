@@ -138,6 +138,25 @@ void gas_adjust(cJupiterModel& m, const std::string& gas) {
             m.ch4, m.ch4_cloud, m.ch4_ice);
 }
 
+// MoistConvectiveAdjustmentJup with the gases and tracers of the loop's call
+// (cJupiterModel.cpp:1300-1320).
+void run_mca(cJupiterModel& m) {
+    typedef MoistConvectiveAdjustmentJup::Gas Gas_;
+    typedef MoistConvectiveAdjustmentJup::Tracer Tr_;
+    std::vector<Gas_> gases = {
+        {"H2O", &m.h2o, &m.h2o_cloud, &m.h2o_ice, m.ep_h2o, m.lv_h2o, m.ls_h2o, m.t_0_h2o,
+         m.C_h2o, m.L0_h2o, m.R_h2o, m.del_alf_h2o, m.del_bet_h2o, m.C_h2o_ice, m.L0_h2o_ice,
+         m.del_alf_h2o_ice, m.del_bet_h2o_ice, m.t_00_h2o},
+        {"NH3", &m.nh3, &m.nh3_cloud, &m.nh3_ice, m.ep_nh3, m.lv_nh3, m.ls_nh3, m.t_0_nh3,
+         m.C_nh3, m.L0_nh3, m.R_nh3, m.del_alf_nh3, m.del_bet_nh3, m.C_nh3_ice, m.L0_nh3_ice,
+         m.del_alf_nh3_ice, m.del_bet_nh3_ice, m.t_00_nh3}};
+    const double L_nh4sh = ChemistryJup::nh4sh_eq() ? ChemistryJup::nh4sh_formation_heat() : 0.0;
+    std::vector<Tr_> tracers = {{"H2S", &m.h2s, m.ep_h2s, false, 0.0},
+                                {"NH4SH", &m.nh4sh, 0.0, true, L_nh4sh},
+                                {"chrom", &m.chrom, 0.0, false, 0.0}};
+    MoistConvectiveAdjustmentJup(m, gases, tracers).run();
+}
+
 }  // namespace
 
 extern "C" {
@@ -240,6 +259,7 @@ double ref_scalar(const char* name) {
     if (n == "has_p_baro") return m.p_baro.empty() ? 0.0 : 1.0;
     if (n == "iter_n") return m.iter_n;
     if (n == "re_turb") return m.re_turb;
+    if (n == "ep_h2s") return m.ep_h2s;
     if (n == "sc_h2o") return m.sc_h2o;
     if (n == "sc_h2s") return m.sc_h2s;
     if (n == "sc_nh3") return m.sc_nh3;
@@ -355,6 +375,7 @@ void ref_chem_fluxes() {
     JupiterUtils::damp_wiggles(m.fluxlim_nh4sh, &m.i_topography, true, true, true);
 }
 void ref_restore() { g_m->restoreVar(1.0); }
+void ref_mca() { run_mca(*g_m); }
 
 // cJupiterModel::save_state / load_state (FileIO_Jup.cpp:584-683) with the model's output
 // directory pointed at dir for the call: the file is dir/jup_restart_<iter>.bin.
@@ -414,7 +435,6 @@ int ref_iteration(int iter_n, int first, int dry) {
     cJupiterModel& m = *g_m;
     m.iter_n = iter_n;
     if (k_conv_adj()) return 2;
-    if (k_mca_stride() > 0 && iter_n % k_mca_stride() == 0) return 3;
     if (iter_n % 2 == 0 || first) {
         PressureSolverJup(m).run();
         static const bool damp_pdyn = [](){ const char* e = getenv("ATJUP_DAMP_PDYN"); return e ? atoi(e) != 0 : !cJupiterModel::geo_balance(); }();
@@ -472,6 +492,7 @@ int ref_iteration(int iter_n, int first, int dry) {
     BC_Jup(m).bcSolidGround();
     static const int turb_wall_hold = [](){ const char* e = getenv("ATJUP_TURB_WALL_HOLD"); return e ? atoi(e) : 1; }();
     if (m.use_turbulence_model && turb_wall_hold != 0) { TurbulenceJup(m).apply_wall_bc(); turb_wall_omega(m); }
+    if (k_mca_stride() > 0 && iter_n % k_mca_stride() == 0) run_mca(m);
     if (k_shapiro_inloop() > 0) {
         const double s = k_shapiro_strength();
         JupiterUtils::damp_wiggles_ho(m.u, &m.i_topography, true, true, true, s, k_shapiro_inloop());

@@ -29,6 +29,8 @@ PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1"}
 # The full-physics iteration: the closure, radiation, precipitation and the NH4SH equilibrium on
 # (their reference defaults); moist convective adjustment and the cone projection stay off.
 MOIST_ENV = {**PHYS_ENV, "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1", "ATJUP_NH4SH_EQ": "1"}
+# the reference's default full physics: MOIST_ENV with the moist convective adjustment every iteration
+MCA_ENV = {**MOIST_ENV, "ATJUP_MCA": "1"}
 
 DYN_FIELDS = ["t", "u", "v", "w", "p_dyn", "p_hydro", "p_stat", "rho_mix", "wall_nue",
               "aux_u", "aux_v", "aux_w"]
@@ -405,8 +407,32 @@ def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
     return out
 
 
+def oracle_mca(params, micro, mca, grid: dict, fields: dict):
+    """ora_mca (one moist convective adjustment) on copies of fields; returns (fields, counters)
+    with counters {columns, layers, moist_triggers, dry_triggers, unstable_t, held, skipped,
+    max_passes}."""
+    from atjup_b200.params import SPECIES
+    o = Oracle(params, grid, fields)
+    shape = o.shape
+    keep = {n: np.ascontiguousarray(fields.get(n, np.zeros(shape)), dtype=np.float64).reshape(shape).copy()
+            for n in SPECIES}
+    X = OraPhys()
+    for s_, n in enumerate(SPECIES):
+        X.q[s_] = _dp(keep[n])
+    lh = np.ascontiguousarray(fields["layer_heights"], dtype=np.float32).copy()
+    X.layer_heights = lh.ctypes.data_as(_P(ctypes.c_float))
+    st = np.zeros(8, dtype=np.int64)
+    o.lib.ora_mca(ctypes.byref(params), ctypes.byref(micro), ctypes.byref(mca), ctypes.byref(o.G),
+                  ctypes.byref(o.S), ctypes.byref(X), st.ctypes.data_as(ctypes.c_void_p))
+    out = {"t": o.f["t"].copy()}
+    out.update(keep)
+    names = ("columns", "layers", "moist_triggers", "dry_triggers", "unstable_t", "held",
+             "skipped", "max_passes")
+    return out, dict(zip(names, (int(x) for x in st)))
+
+
 def oracle_iteration_phys(params, phys, micro, grid: dict, fields: dict, iters, sweeps=1,
-                          snapshots=()) -> dict:
+                          snapshots=(), mca=None) -> dict:
     """ora_iteration_phys for iterations 1..iters (the first with first = 1) on copies of fields;
     returns {iteration: {field: array}} for the iterations in snapshots (and the last)."""
     from atjup_b200.params import S_PRECIP, SCALARS, SPECIES
@@ -451,6 +477,7 @@ def oracle_iteration_phys(params, phys, micro, grid: dict, fields: dict, iters, 
     out = {}
     for it in range(1, iters + 1):
         o.lib.ora_iteration_phys(ctypes.byref(params), ctypes.byref(phys), ctypes.byref(micro),
+                                 ctypes.byref(mca) if mca is not None else None,
                                  ctypes.byref(o.G), ctypes.byref(o.S), ctypes.byref(X),
                                  ctypes.c_int(it), ctypes.c_int(1 if it == 1 else 0),
                                  ctypes.c_int(sweeps))

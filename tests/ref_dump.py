@@ -248,6 +248,59 @@ RESTART_CARRIED = ("aux_u", "aux_v", "aux_w", "difflux_h2s", "difflux_nh3", "mas
                    "S_precip_nh3", "S_precip_nh3_ice")
 
 
+MCA_SEED = 20261205
+MCA_FIELDS = ("t", "h2o", "h2o_cloud", "h2o_ice", "nh3", "nh3_cloud", "nh3_ice", "h2s", "nh4sh")
+
+
+def perturb_unstable(f: dict, solid: np.ndarray, layer_h: np.ndarray, seed: int = MCA_SEED) -> dict:
+    """Seeded perturbation that makes the moist convective adjustment fire: in 3 % of the columns
+    the lowest four fluid levels are warmed (4 K at the bottom, halving upwards), and in 2 % the
+    vapour of the lowest three levels is raised to 1.5 x itself (saturated parcels)."""
+    rng = np.random.default_rng(seed)
+    im, jm, km = f["t"].shape
+    t = f["t"].copy()
+    h2o, nh3 = f["h2o"].copy(), f["nh3"].copy()
+    fluid = solid == 0
+    warm = rng.random((jm, km)) < 0.03
+    wet = rng.random((jm, km)) < 0.02
+    for j, k in zip(*np.nonzero(warm | wet)):
+        col = np.nonzero(fluid[:, j, k])[0]
+        col = col[col >= 1]
+        if len(col) < 5:
+            continue
+        i0 = col[0]
+        for d in range(4):
+            if warm[j, k]:
+                t[i0 + d, j, k] += 4.0 / 2 ** d / 165.0
+            if wet[j, k] and d < 3:
+                h2o[i0 + d, j, k] *= 1.5
+                nh3[i0 + d, j, k] *= 1.5
+    out = dict(f)
+    out.update(t=t, h2o=h2o, nh3=nh3)
+    return out
+
+
+def mca_case(ref, g, data):
+    """One MoistConvectiveAdjustmentJup (the loop's gases and tracers) on the reference's moist
+    state perturbed by perturb_unstable; inputs as in_*, outputs as mca_*."""
+    f = perturb_unstable({n: ref.get(n) for n in MCA_FIELDS}, g["solid"],
+                         ref.get1("layer_heights"))
+    for n, v in f.items():
+        ref.set(n, v)
+        data["in_" + n] = v
+    data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
+    for c in MICRO_CONSTS:
+        data["micro_" + c] = np.array(ref.scalar(c))
+    for gas in GASES:
+        cst = np.zeros(14)
+        ref.L.ref_gas_consts(gas.encode(), cst.ctypes.data_as(ctypes.c_void_p))
+        data["gas_" + gas] = cst
+    data["ep_h2s"] = np.array(ref.scalar("ep_h2s"))
+    ref.quiet(ref.L.ref_mca)
+    for n in MCA_FIELDS:
+        data["mca_" + n] = ref.get(n)
+
+
 def phys_iters_case(ref, g, data, iters, save_restart=None):
     """`iters` iterations of the loop with the physics on (closure, radiation, precipitation, the
     NH4SH equilibrium, the saturation adjustments), from the reference's own moist initial state;
@@ -301,6 +354,8 @@ def main():
     ap.add_argument("--phys-iters", type=int, default=0)
     ap.add_argument("--perturb-ulp", action="store_true",
                     help="with --phys-iters: start from t one ulp above the model's own (fluid cells)")
+    ap.add_argument("--mca", action="store_true",
+                    help="one moist convective adjustment on the perturbed moist state")
     ap.add_argument("--save-restart", default=None, metavar="DIR:N",
                     help="with --phys-iters: write the reference's restart file to DIR after "
                          "iteration N (and record its arrays as rsN_*)")
@@ -313,11 +368,11 @@ def main():
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
     env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
-    if a.micro or a.phys_iters or a.load_restart:
+    if a.micro or a.phys_iters or a.load_restart or a.mca:
         env = dict(MOIST_ENV)
     env.update(dict(kv.split("=", 1) for kv in a.env))
     ref = Reference(env, out_dir + "/run", threads=a.threads,
-                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro or a.phys_iters or a.load_restart))
+                    zero_species=not (a.moist or a.satadj or a.satadj_synthetic or a.rk4_phys or a.turb or a.bc or a.micro or a.phys_iters or a.load_restart or a.mca))
     data = {}
     g = ref.grid()
     for k, v in g.items():
@@ -343,6 +398,8 @@ def main():
             d_, n_ = a.save_restart.rsplit(":", 1)
             sr = (d_, int(n_))
         phys_iters_case(ref, g, data, a.phys_iters, sr)
+    elif a.mca:
+        mca_case(ref, g, data)
     elif a.load_restart:
         d_, n_ = a.load_restart.rsplit(":", 1)
         data["load_rc"] = np.array(ref.quiet(ref.L.ref_load_state, d_.encode(), int(n_)))
