@@ -73,6 +73,7 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red); cudaFree(c->stage);
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
+    if (c->mca_count_host) cudaFreeHost(c->mca_count_host);
     cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
@@ -477,8 +478,8 @@ int atjup_gpu_mca(AtjupCtx* c, AtjupMcaStats* st) {
     }
     if (st) {
         unsigned long long h[8];
-        ATJUP_CUDA(cudaMemcpyAsync(h, c->mca_stats, sizeof h, cudaMemcpyDeviceToHost, c->stream));
-        ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+        int rc = mca_read_stats(c, h);
+        if (rc) return rc;
         st->columns = (int64_t)h[0]; st->layers = (int64_t)h[1];
         st->moist_triggers = (int64_t)h[2]; st->dry_triggers = (int64_t)h[3];
         st->unstable_t = (int64_t)h[4]; st->held = (int64_t)h[5]; st->skipped = (int64_t)h[6];

@@ -73,7 +73,8 @@ struct AtjupCtx {
     void* mca_bounds = nullptr;     // int2 [jm * km]: the column's (i0, i1)
     void* mca_flags = nullptr;      // unsigned [2 * jm * km + 1]: flags, list, count
     void* mca_slots = nullptr;      // per-thread column scratch of the column kernel
-    void* mca_stats = nullptr;      // unsigned long long [8]
+    void* mca_stats = nullptr;      // unsigned long long [8 + 2 * partials]
+    unsigned* mca_count_host = nullptr;   // pinned: the listed-column count read after the census
     double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
@@ -147,6 +148,7 @@ int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w);
 int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout);
 int mca_setup(AtjupCtx* c);
 int launch_mca(AtjupCtx* c);
+int mca_read_stats(AtjupCtx* c, unsigned long long* out);
 int launch_mixture_density(AtjupCtx* c);
 int launch_prepare_projection(AtjupCtx* c);
 int launch_pressure_source(AtjupCtx* c);

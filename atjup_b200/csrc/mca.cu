@@ -33,6 +33,7 @@ constexpr int MAXI = 64;               // levels a column slot holds (the refere
 constexpr int NITER = 60;              // cap of the equilibrium solve
 constexpr double TOL_K = 1.0e-7, TOL_T = 1.0e-10;
 constexpr int NSLOT = 4096;            // columns adjusted concurrently (per-thread scratch slots)
+constexpr int NPART = 256;             // partial census counters (spread so the adds do not contend)
 
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
 
@@ -51,20 +52,22 @@ struct McaArgs {
     int tr_cond[NT];
     double cp, grav, t_ref, r_mix, relax;
     int im, jm, km, KP, local_rho, ledoux, loading, max_pass;
-    unsigned long long* stats;         // [8]
+    unsigned long long* stats;         // [8], then NPART pairs of census partial counts
     unsigned* colflag;                 // [jm * km]
     unsigned* list;                    // [jm * km] listed columns
     unsigned* count;
 };
 
-// ATPhys.h:49-52 [bar]
-__device__ __forceinline__ double svp(double T, double C, double L0, double R, double da, double db) {
-    return exp(C + (-L0 / T + da * log(T) + db * T) / (1e-3 * R));
+// ATPhys.h:49-52 [bar], with log(T) passed in: both gases are evaluated at the same T, and the
+// logarithm (a pure function) is the same value whether computed once or per gas
+__device__ __forceinline__ double svp(double T, double lT, double C, double L0, double R, double da,
+                                      double db) {
+    return exp(C + (-L0 / T + da * lT + db * T) / (1e-3 * R));
 }
-__device__ __forceinline__ double qsat(const McaArgs& a, int g, double T, double p) {
+__device__ __forceinline__ double qsat(const McaArgs& a, int g, double T, double lT, double p) {
     const AtjupGasParams& s = a.gas[g];
-    const double E = (T >= s.t_0) ? svp(T, s.C, s.L0, s.R, s.del_alf, s.del_bet)
-                                  : svp(T, s.C_i, s.L0_i, s.R, s.del_alf_i, s.del_bet_i);
+    const double E = (T >= s.t_0) ? svp(T, lT, s.C, s.L0, s.R, s.del_alf, s.del_bet)
+                                  : svp(T, lT, s.C_i, s.L0_i, s.R, s.del_alf_i, s.del_bet_i);
     const double q = s.ep * E / p;
     return isfinite(q) ? q : 0.0;
 }
@@ -74,7 +77,8 @@ __device__ __forceinline__ double lat(const McaArgs& a, int g, double T) {
 __device__ __forceinline__ double fof(const McaArgs& a, double TT, double hL, const double* qt,
                                       double p, double z) {
     double f = a.cp * TT + a.grav * z - hL;
-    for (int g = 0; g < NG; g++) f -= lat(a, g, TT) * dmax(0.0, qt[g] - qsat(a, g, TT, p));
+    const double lT = log(TT);
+    for (int g = 0; g < NG; g++) f -= lat(a, g, TT) * dmax(0.0, qt[g] - qsat(a, g, TT, lT, p));
     return f;
 }
 // equilibrium temperature of (h_L, q_t) at (p, z): Illinois regula falsi in [all vapour, all
@@ -84,8 +88,9 @@ __device__ bool equil(const McaArgs& a, double hL, const double* qt, double p, d
     const double T_lo = (hL - a.grav * z) / a.cp;
     if (!(T_lo > 0.0) || !(p > 0.0)) return false;
     bool any = false;
+    const double lT_lo = log(T_lo);
     for (int g = 0; g < NG; g++)
-        if (qt[g] > qsat(a, g, T_lo, p)) { any = true; break; }
+        if (qt[g] > qsat(a, g, T_lo, lT_lo, p)) { any = true; break; }
     if (!any) {
         T = T_lo;
         for (int g = 0; g < NG; g++) cond[g] = 0.0;
@@ -105,7 +110,8 @@ __device__ bool equil(const McaArgs& a, double hL, const double* qt, double p, d
         if (fabs(fc) <= a.cp * TOL_T) { lo = hi = c; break; }
     }
     T = hi;
-    for (int g = 0; g < NG; g++) cond[g] = dmax(0.0, qt[g] - qsat(a, g, T, p));
+    const double lT = log(T);
+    for (int g = 0; g < NG; g++) cond[g] = dmax(0.0, qt[g] - qsat(a, g, T, lT, p));
     return true;
 }
 
@@ -219,14 +225,21 @@ __global__ void mca_census_kernel(McaArgs a) {
             }
         }
     }
-    // the census counters (a warp sum, one atomic per warp)
+    // the census counters: a block sum, added to one of NPART partial counters (summed on the
+    // host); adds from every warp to one address would serialise some 160k atomic operations
     for (int o = 16; o > 0; o >>= 1) {
         ut += __shfl_down_sync(0xffffffffu, ut, o);
         hd += __shfl_down_sync(0xffffffffu, hd, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        if (ut) atomicAdd(&a.stats[4], ut);
-        if (hd) atomicAdd(&a.stats[5], hd);
+    __shared__ unsigned long long sut[4], shd[4];
+    if ((threadIdx.x & 31) == 0) { sut[threadIdx.x >> 5] = ut; shd[threadIdx.x >> 5] = hd; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long bu = sut[0] + sut[1] + sut[2] + sut[3];
+        const unsigned long long bh = shd[0] + shd[1] + shd[2] + shd[3];
+        const unsigned part = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) % NPART;
+        if (bu) atomicAdd(&a.stats[8 + 2 * part], bu);
+        if (bh) atomicAdd(&a.stats[9 + 2 * part], bh);
     }
 }
 
@@ -281,11 +294,14 @@ __device__ bool col_mix(const McaArgs& a, Col& C, int lo, int up) {
     return true;
 }
 
-__global__ void __launch_bounds__(64) mca_column_kernel(McaArgs a, Col* slots) {
+// NSLOT threads in blocks of COL_BLOCK; listed column idx goes to lane idx / blocks of block
+// idx % blocks, so a few listed columns land on as many SMs, not on the lanes of one block
+constexpr int COL_BLOCK = 32;
+__global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* slots) {
     const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
     Col& C = slots[slot];
     const unsigned n = *a.count;
-    for (unsigned idx = slot; idx < n; idx += NSLOT) {
+    for (unsigned idx = threadIdx.x * gridDim.x + blockIdx.x; idx < n; idx += NSLOT) {
         const unsigned col = a.list[idx];
         const int j = (int)(col / (unsigned)a.km), k = (int)(col % (unsigned)a.km);
         const int2 b = a.bounds[col];
@@ -397,7 +413,8 @@ int mca_setup(AtjupCtx* c) {
     if (!c->mca_bounds) ATJUP_CUDA(cudaMalloc(&c->mca_bounds, sizeof(int2) * ncol));
     if (!c->mca_flags) ATJUP_CUDA(cudaMalloc(&c->mca_flags, sizeof(unsigned) * (2 * ncol + 1)));
     if (!c->mca_slots) ATJUP_CUDA(cudaMalloc(&c->mca_slots, sizeof(Col) * NSLOT));
-    if (!c->mca_stats) ATJUP_CUDA(cudaMalloc(&c->mca_stats, sizeof(unsigned long long) * 8));
+    if (!c->mca_count_host) ATJUP_CUDA(cudaMallocHost(&c->mca_count_host, sizeof(unsigned)));
+    if (!c->mca_stats) ATJUP_CUDA(cudaMalloc(&c->mca_stats, sizeof(unsigned long long) * (8 + 2 * NPART)));
     mca_bounds_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
         c->solid, static_cast<int2*>(c->mca_bounds), P.im, P.jm, P.km, c->KP, c->mca.interior);
     c->launches++;
@@ -438,15 +455,30 @@ int launch_mca(AtjupCtx* c) {
     a.colflag = static_cast<unsigned*>(c->mca_flags);
     a.list = a.colflag + ncol;
     a.count = a.colflag + 2 * ncol;
-    ATJUP_CUDA(cudaMemsetAsync(c->mca_stats, 0, sizeof(unsigned long long) * 8, c->stream));
+    ATJUP_CUDA(cudaMemsetAsync(c->mca_stats, 0, sizeof(unsigned long long) * (8 + 2 * NPART), c->stream));
     ATJUP_CUDA(cudaMemsetAsync(a.colflag, 0, sizeof(unsigned) * ncol, c->stream));
     ATJUP_CUDA(cudaMemsetAsync(a.count, 0, sizeof(unsigned), c->stream));
     mca_census_kernel<<<dim3((P.km + 127) / 128, P.jm, P.im - 1), 128, 0, c->stream>>>(a);
     c->launches++;
     ATJUP_CHECK_LAUNCH("mca_census");
-    mca_column_kernel<<<NSLOT / 64, 64, 0, c->stream>>>(a, static_cast<Col*>(c->mca_slots));
+    // the listed columns: almost always none, and then the column kernel is not launched
+    ATJUP_CUDA(cudaMemcpyAsync(c->mca_count_host, a.count, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    if (*c->mca_count_host == 0) return ATJUP_OK;
+    mca_column_kernel<<<NSLOT / COL_BLOCK, COL_BLOCK, 0, c->stream>>>(a, static_cast<Col*>(c->mca_slots));
     c->launches++;
     ATJUP_CHECK_LAUNCH("mca_column");
+    return ATJUP_OK;
+}
+
+// the counters of the last adjustment: [8], the census partials summed into [4] and [5]
+int mca_read_stats(AtjupCtx* c, unsigned long long* out) {
+    unsigned long long h[8 + 2 * NPART];
+    ATJUP_CUDA(cudaMemcpyAsync(h, c->mca_stats, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 8; q++) out[q] = h[q];
+    for (int q = 0; q < NPART; q++) { out[4] += h[8 + 2 * q]; out[5] += h[9 + 2 * q]; }
     return ATJUP_OK;
 }
 

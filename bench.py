@@ -9,8 +9,8 @@ cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.
 on even iterations the red-black pressure pass, mixture density, radiation, the saturation
 adjustment of H2O, NH3 and CH4, the NH4SH equilibrium, precipitation, the k-omega SST closure
 update and the chemistry fluxes; every iteration the four RK4 stages of t, u, v, w, the 11
-species and k*, omega*, the boundary passes, the in-loop 4th-order Shapiro filter of u, v, w, the
-column balance of v and the species clamp. The initial state follows the full-physics recipe
+species and k*, omega*, the boundary passes, the moist convective adjustment, the in-loop
+4th-order Shapiro filter of u, v, w, the column balance of v and the species clamp. The initial state follows the full-physics recipe
 (atjup_b200/synthetic.py: state + full_physics): vapour at 90 % of saturation with U(0.95, 1.05)
 noise, k = 1e-4 m2/s2 x U(0.5, 1.5), omega = 1e-3 1/s x U(0.5, 1.5), the dynamics perturbations of
 the dry recipe; it is device-resident when the timed region starts. `--workload dry` times the
@@ -50,7 +50,7 @@ UNIT = "s/step"
 METRICS = {
     "phys": "s per RK4 step (full-physics {prec} iteration, 41x181x361: pressure pass, radiation, "
             "saturation adjustment, NH4SH, precipitation, k-omega SST, chemistry, RK4 of 17 fields, "
-            "BCs, filters)",
+            "BCs, moist convective adjustment, filters)",
     "dry": "s per RK4 step (dry {prec} dynamics, 41x181x361: one model iteration incl. pressure pass)",
 }
 PREC_NAMES = {"fp64": "FP64", "mixed": "mixed FP32/FP64"}
@@ -62,10 +62,11 @@ PREC_CONFIG = {
 }
 CONFIGS = {
     "phys": {
-        "workload": "full-physics iteration on the 41x181x361 shell (full-physics knobs: closure, "
-                    "radiation, precipitation, saturation adjustment, NH4SH equilibrium on; moist "
-                    "convective adjustment off): the loop's schedule, pressure and physics on even "
-                    "iterations, RK4 of t, u, v, w, 11 species, k*, omega* every iteration",
+        "workload": "full-physics iteration on the 41x181x361 shell (the reference's default "
+                    "physics: closure, radiation, precipitation, saturation adjustment, NH4SH "
+                    "equilibrium, moist convective adjustment every iteration): the loop's "
+                    "schedule, pressure and physics on even iterations, RK4 of t, u, v, w, 11 "
+                    "species, k*, omega* every iteration",
         "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
         "l2": "no flush: inputs larger than L2 (each RK stage streams > 1.8 GB)",
         "parallelism": "replicas (the path does not shard)",
@@ -135,8 +136,10 @@ DRY_ENV = {
     "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
     "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
 }
+# the reference's default full physics: closure, radiation, precipitation, NH4SH equilibrium and
+# the moist convective adjustment every iteration
 PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1", "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1",
-            "ATJUP_NH4SH_EQ": "1"}
+            "ATJUP_NH4SH_EQ": "1", "ATJUP_MCA": "1"}
 
 
 def measured_peak_hbm():
@@ -268,7 +271,7 @@ def main():
     from atjup_b200 import synthetic
     from atjup_b200.gpu import GpuModel
     from atjup_b200.params import (DEFAULT_GASES, FIELD_IDS, PREC_FP64, PREC_MIXED, SCALARS,
-                                   resolve_micro, resolve_params, resolve_physics)
+                                   resolve_mca, resolve_micro, resolve_params, resolve_physics)
     from atjup_b200.replicas import max_over_ranks, whole_job_seconds_per_step
 
     torch.cuda.set_device(local_rank)
@@ -300,6 +303,7 @@ def main():
     if phys:
         m.set_physics(resolve_physics(PHYS_ENV), fields["layer_heights"])
         m.set_micro(resolve_micro(PHYS_ENV))
+        m.set_mca(resolve_mca(PHYS_ENV))
     if args.precision == "mixed":
         m.set_precision(PREC_MIXED)
     m.upload_state(fields)

@@ -32,8 +32,10 @@ DRY_ENV = {
 }
 
 
+# the reference's default full physics: closure, radiation, precipitation, NH4SH equilibrium and
+# the moist convective adjustment every iteration
 PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1", "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1",
-            "ATJUP_NH4SH_EQ": "1"}
+            "ATJUP_NH4SH_EQ": "1", "ATJUP_MCA": "1"}
 
 
 def main():

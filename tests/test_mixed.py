@@ -41,10 +41,11 @@ def bench_state():
 def model(P, grid, fields, precision):
     import bench
     from atjup_b200.gpu import GpuModel
-    from atjup_b200.params import resolve_micro, resolve_physics
+    from atjup_b200.params import resolve_mca, resolve_micro, resolve_physics
     m = GpuModel(P, grid)
     m.set_physics(resolve_physics(bench.PHYS_ENV), fields["layer_heights"])
     m.set_micro(resolve_micro(bench.PHYS_ENV))
+    m.set_mca(resolve_mca(bench.PHYS_ENV))
     m.set_precision(precision)
     m.upload_state(fields)
     return m
