@@ -73,6 +73,7 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->src); cudaFree(c->tmp); cudaFree(c->tmp2); cudaFree(c->red); cudaFree(c->stage);
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
+    cudaFree(c->mca_pairs);
     if (c->mca_count_host) cudaFreeHost(c->mca_count_host);
     cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);

@@ -73,6 +73,7 @@ struct AtjupCtx {
     void* mca_bounds = nullptr;     // int2 [jm * km]: the column's (i0, i1)
     void* mca_flags = nullptr;      // unsigned [2 * jm * km + 1]: flags, list, count
     void* mca_slots = nullptr;      // per-thread column scratch of the column kernel
+    void* mca_pairs = nullptr;      // uint8 [im * jm * km]: the census result of every pair
     void* mca_stats = nullptr;      // unsigned long long [8 + 2 * partials]
     unsigned* mca_count_host = nullptr;   // pinned: the listed-column count read after the census
     double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry

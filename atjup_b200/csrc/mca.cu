@@ -17,8 +17,9 @@
 //                       a column with an unstable pair, or with a cell the reference would refuse,
 //                       is appended to a list.
 //   mca_column_kernel   one thread per listed column: the reference's whole column algorithm
-//                       (its own census, the sweeps, the segment growth, the relaxation, the
-//                       write-back), with the column's state in a per-thread slot in global memory.
+//                       (starting from the census the census kernel recorded per pair, the sweeps,
+//                       the segment growth, the relaxation, the write-back), with the column's
+//                       state in a per-thread slot in global memory.
 // A column that is not listed is left alone by the reference too (no unstable pair: pass 1 mixes
 // nothing). The equilibrium solve and every expression keep the reference's operand order, and
 // the file is compiled without FMA contraction; the parcel test compares a virtual-temperature
@@ -56,6 +57,7 @@ struct McaArgs {
     unsigned* colflag;                 // [jm * km]
     unsigned* list;                    // [jm * km] listed columns
     unsigned* count;
+    uint8_t* pairs;                    // [im * jm * km] census of pair (i, i+1): bit 0 unstable, bit 1 moist
 };
 
 // ATPhys.h:49-52 [bar], with log(T) passed in: both gases are evaluated at the same T, and the
@@ -221,6 +223,7 @@ __global__ void mca_census_kernel(McaArgs a) {
                 if (ok) uns = pair_test(a, lo.hL, lo.qt, lo.qr, up.p, up.z, Tb, ecb, up.qt, up.qr, ok, &held, &moist);
                 if (uns || held) ut = 1;
                 if (held) hd = 1;
+                a.pairs[((size_t)i * a.jm + j) * a.km + k] = (uint8_t)((uns ? 1 : 0) | (moist ? 2 : 0));
                 if (uns) enqueue(a, col);
             }
         }
@@ -331,11 +334,12 @@ __global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* s
                 if (!(C.w[i] > 0.0)) ok = false;
             }
         if (!ok) { atomicAdd(&a.stats[6], 1ull); continue; }
-        // the census again, for the first sweep (its counters came from the census kernel)
+        // the census of the first sweep, as the census kernel found it (the same pair tests on the
+        // same state); every pair of a column that loads is written there
         for (int i = i0; i < i1; i++) {
-            bool moist = false;
-            C.cen_u[i] = col_unstable(a, C, i, i + 1, nullptr, &moist) ? 1 : 0;
-            C.cen_m[i] = moist ? 1 : 0;
+            const uint8_t f = a.pairs[((size_t)i * a.jm + j) * a.km + k];
+            C.cen_u[i] = f & 1;
+            C.cen_m[i] = (f >> 1) & 1;
         }
         for (int i = i0; i <= i1; i++) {
             C.hL0[i] = C.hL[i];
@@ -413,6 +417,7 @@ int mca_setup(AtjupCtx* c) {
     if (!c->mca_bounds) ATJUP_CUDA(cudaMalloc(&c->mca_bounds, sizeof(int2) * ncol));
     if (!c->mca_flags) ATJUP_CUDA(cudaMalloc(&c->mca_flags, sizeof(unsigned) * (2 * ncol + 1)));
     if (!c->mca_slots) ATJUP_CUDA(cudaMalloc(&c->mca_slots, sizeof(Col) * NSLOT));
+    if (!c->mca_pairs) ATJUP_CUDA(cudaMalloc(&c->mca_pairs, (size_t)P.im * P.jm * P.km));
     if (!c->mca_count_host) ATJUP_CUDA(cudaMallocHost(&c->mca_count_host, sizeof(unsigned)));
     if (!c->mca_stats) ATJUP_CUDA(cudaMalloc(&c->mca_stats, sizeof(unsigned long long) * (8 + 2 * NPART)));
     mca_bounds_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
@@ -455,6 +460,7 @@ int launch_mca(AtjupCtx* c) {
     a.colflag = static_cast<unsigned*>(c->mca_flags);
     a.list = a.colflag + ncol;
     a.count = a.colflag + 2 * ncol;
+    a.pairs = static_cast<uint8_t*>(c->mca_pairs);
     ATJUP_CUDA(cudaMemsetAsync(c->mca_stats, 0, sizeof(unsigned long long) * (8 + 2 * NPART), c->stream));
     ATJUP_CUDA(cudaMemsetAsync(a.colflag, 0, sizeof(unsigned) * ncol, c->stream));
     ATJUP_CUDA(cudaMemsetAsync(a.count, 0, sizeof(unsigned), c->stream));
