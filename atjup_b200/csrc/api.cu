@@ -55,6 +55,7 @@ int alloc(double** p, size_t n) {
 }
 
 void free_all(AtjupCtx* c) {
+    xfer_free(c);
     solver_free(c);
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
     for (auto& p : c->f2) { cudaFree(p); p = nullptr; }
@@ -74,7 +75,6 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
     cudaFree(c->mca_pairs);
-    if (c->mca_count_host) cudaFreeHost(c->mca_count_host);
     cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
@@ -859,6 +859,7 @@ int atjup_gpu_launch_count(AtjupCtx* c, int64_t* launches) {
 int atjup_gpu_synchronize(AtjupCtx* c) {
     if (!c) return ATJUP_ERR_ARG;
     ATJUP_CUDA(cudaStreamSynchronize(c->stream));
+    if (int rc = xfer_synchronize(c)) return rc;
     return ATJUP_OK;
 }
 

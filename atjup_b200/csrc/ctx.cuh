@@ -44,6 +44,15 @@ struct AtjupCtx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // asynchronous field exchange (xfer.cu): copy streams, double-buffered staging by round
+    bool xfer_on = false;
+    cudaStream_t x_h2d = nullptr, x_d2h = nullptr;
+    double* x_up[2][ATJUP_F_COUNT] = {};
+    double* x_out[2][ATJUP_F_COUNT] = {};
+    cudaEvent_t x_up_done[2] = {}, x_up_free[2][ATJUP_F_COUNT] = {}, x_out_free[2][ATJUP_F_COUNT] = {};
+    cudaEvent_t x_out_ready = nullptr;
+    unsigned long long x_pending[2] = {0, 0};
+    long long x_round = 0;
     int KP = 0;              // padded row pitch (elements)
     size_t NP = 0;           // im * jm * KP
     bool grid_set = false;
@@ -75,7 +84,6 @@ struct AtjupCtx {
     void* mca_slots = nullptr;      // per-thread column scratch of the column kernel
     void* mca_pairs = nullptr;      // uint8 [im * jm * km]: the census result of every pair
     void* mca_stats = nullptr;      // unsigned long long [8 + 2 * partials]
-    unsigned* mca_count_host = nullptr;   // pinned: the listed-column count read after the census
     double* cos_lat = nullptr;         // [jm] max(0, sin(pi j / (jm - 1))), the solar geometry
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
@@ -164,6 +172,8 @@ int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, 
 int launch_nonfinite(AtjupCtx* c, unsigned long long* d_count);
 int launch_pad(AtjupCtx* c, const double* flat, double* padded);     // (i,j,k) km -> KP rows
 int launch_unpad(AtjupCtx* c, const double* padded, double* flat);
+void xfer_free(AtjupCtx* c);
+int xfer_synchronize(AtjupCtx* c);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
 int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what);

@@ -418,7 +418,6 @@ int mca_setup(AtjupCtx* c) {
     if (!c->mca_flags) ATJUP_CUDA(cudaMalloc(&c->mca_flags, sizeof(unsigned) * (2 * ncol + 1)));
     if (!c->mca_slots) ATJUP_CUDA(cudaMalloc(&c->mca_slots, sizeof(Col) * NSLOT));
     if (!c->mca_pairs) ATJUP_CUDA(cudaMalloc(&c->mca_pairs, (size_t)P.im * P.jm * P.km));
-    if (!c->mca_count_host) ATJUP_CUDA(cudaMallocHost(&c->mca_count_host, sizeof(unsigned)));
     if (!c->mca_stats) ATJUP_CUDA(cudaMalloc(&c->mca_stats, sizeof(unsigned long long) * (8 + 2 * NPART)));
     mca_bounds_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
         c->solid, static_cast<int2*>(c->mca_bounds), P.im, P.jm, P.km, c->KP, c->mca.interior);
@@ -467,11 +466,8 @@ int launch_mca(AtjupCtx* c) {
     mca_census_kernel<<<dim3((P.km + 127) / 128, P.jm, P.im - 1), 128, 0, c->stream>>>(a);
     c->launches++;
     ATJUP_CHECK_LAUNCH("mca_census");
-    // the listed columns: almost always none, and then the column kernel is not launched
-    ATJUP_CUDA(cudaMemcpyAsync(c->mca_count_host, a.count, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                               c->stream));
-    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
-    if (*c->mca_count_host == 0) return ATJUP_OK;
+    // the listed columns (almost always none: the kernel then reads the count and returns; the
+    // host does not wait for the count, so the launches of the step stay queued ahead)
     mca_column_kernel<<<NSLOT / COL_BLOCK, COL_BLOCK, 0, c->stream>>>(a, static_cast<Col*>(c->mca_slots));
     c->launches++;
     ATJUP_CHECK_LAUNCH("mca_column");

@@ -70,6 +70,9 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_turbulence.argtypes = [vp]
     L.atjup_gpu_set_micro.argtypes = [vp, ctypes.POINTER(_p.AtjupMicro)]
     L.atjup_gpu_set_precision.argtypes = [vp, i32]
+    L.atjup_gpu_upload_async.argtypes = [vp, i32, vp]
+    L.atjup_gpu_apply_uploads.argtypes = [vp]
+    L.atjup_gpu_download_async.argtypes = [vp, i32, vp]
     L.atjup_gpu_set_mca.argtypes = [vp, ctypes.POINTER(_p.AtjupMca)]
     L.atjup_gpu_mca.argtypes = [vp, ctypes.POINTER(_p.AtjupMcaStats)]
     L.atjup_gpu_save_state.argtypes = [vp, ctypes.c_char_p, i32, i32]
@@ -137,6 +140,20 @@ class GpuModel:
         out = np.empty(self.shape)
         _check(self.L.atjup_gpu_download(self.ctx, _p.FIELD_IDS[name], _ptr(out)))
         return out
+
+    def upload_async(self, name: str, a) -> None:
+        """atjup_gpu_upload_async: queue a field's upload (a contiguous float64 array that must stay
+        alive and unchanged until synchronize())."""
+        assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == int(np.prod(self.shape))
+        _check(self.L.atjup_gpu_upload_async(self.ctx, _p.FIELD_IDS[name], _ptr(a)))
+
+    def apply_uploads(self) -> None:
+        _check(self.L.atjup_gpu_apply_uploads(self.ctx))
+
+    def download_async(self, name: str, out) -> None:
+        """atjup_gpu_download_async into out (contiguous float64; valid after synchronize())."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == int(np.prod(self.shape))
+        _check(self.L.atjup_gpu_download_async(self.ctx, _p.FIELD_IDS[name], _ptr(out)))
 
     def upload_state(self, fields: dict) -> None:
         """Upload every known field in fields; with physics set, also the time-level-n copies

@@ -10,8 +10,9 @@ on even iterations the red-black pressure pass, mixture density, radiation, the 
 adjustment of H2O, NH3 and CH4, the NH4SH equilibrium, precipitation, the k-omega SST closure
 update and the chemistry fluxes; every iteration the four RK4 stages of t, u, v, w, the 11
 species and k*, omega*, the boundary passes, the moist convective adjustment, the in-loop
-4th-order Shapiro filter of u, v, w, the column balance of v and the species clamp. The initial state follows the full-physics recipe
-(atjup_b200/synthetic.py: state + full_physics): vapour at 90 % of saturation with U(0.95, 1.05)
+4th-order Shapiro filter of u, v, w, the column balance of v and the species clamp. The initial
+state follows the full-physics recipe (atjup_b200/synthetic.py: state + full_physics): vapour at
+90 % of saturation with U(0.95, 1.05)
 noise, k = 1e-4 m2/s2 x U(0.5, 1.5), omega = 1e-3 1/s x U(0.5, 1.5), the dynamics perturbations of
 the dry recipe; it is device-resident when the timed region starts. `--workload dry` times the
 dry dynamics iteration instead (microphysics, radiation, closure off). `--precision mixed` runs
@@ -23,7 +24,9 @@ physics).
 Prints one JSON line. `value` is seconds per step for the whole job (N replicas: max-over-ranks
 device time / (N * K)); `e2e` is the same metric through the public C ABI with host buffers
 (pinned), the host->device upload of the step's state and the device->host read of its result
-inside the timed region. For the full-physics workload in FP64 the line also carries
+inside the timed region every step: through the asynchronous exchange (atjup_gpu_upload_async,
+atjup_gpu_apply_uploads, atjup_gpu_download_async), whose copies of consecutive steps overlap the
+compute, and (`e2e_serial`) through the synchronous atjup_gpu_upload / atjup_gpu_download. For the full-physics workload in FP64 the line also carries
 `mixed_precision`: the run continued for K more iterations in the mixed-precision RK step, timed
 the same way. With --impl reference the line times the reference's own CPU code of the same
 iteration (built from its sources into oracle/_ref) on this host's cores.
@@ -120,7 +123,7 @@ def stage_kernels(prec, phys):
             "species": ("species_stage_kernel", species_stage_bytes(prec)),
             "closure": ("closure_stage_kernel", closure_stage_bytes(prec))}
 # (algorithmic bytes per cell and launch; times the cells of the shell)
-# DRAM bytes (read + write) per launch from ncu captures (profiles/); None until captured.
+
 # DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step:
 # dram__bytes_read.sum + dram__bytes_write.sum of each stage launch in one ncu capture of this
 # workload on the 41x181x361 shell (profiles/stage_traffic_phys_41x181x361.md).
@@ -393,7 +396,35 @@ def main():
     def down(n):
         m._rc(m.L.atjup_gpu_download(m.ctx, FIELD_IDS[n], ctypes.c_void_p(host_out[n].data_ptr())))
 
+    def up_async(n):
+        m._rc(m.L.atjup_gpu_upload_async(m.ctx, FIELD_IDS[n], ctypes.c_void_p(host_in[n].data_ptr())))
+
+    def down_async(n):
+        m._rc(m.L.atjup_gpu_download_async(m.ctx, FIELD_IDS[n],
+                                           ctypes.c_void_p(host_out[n].data_ptr())))
+
+    def e2e_step_async():
+        for n in names:
+            up_async(n)
+        m._rc(m.L.atjup_gpu_apply_uploads(m.ctx))
+        step()
+        for n in names:
+            down_async(n)
+
     e2e_steps = max(3, min(args.steps, 10))
+    # the pipelined exchange (atjup_gpu_upload_async / apply_uploads / download_async): step n+1's
+    # uploads and step n's downloads overlap step n's compute; one untimed round allocates the
+    # staging buffers
+    e2e_step_async()
+    m.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step_async()
+    m.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, device="cuda")
+    # the same with the synchronous atjup_gpu_upload / atjup_gpu_download, for comparison
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -403,8 +434,7 @@ def main():
         for n in names:
             down(n)
     m.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, device="cuda")
+    e2e_serial_s = max_over_ranks(time.perf_counter() - t0, device="cuda")
     nbytes = len(names) * N_CELLS * 8
 
     peak, peak_kind = measured_peak_hbm()
@@ -437,7 +467,11 @@ def main():
                                         sorted(per_class.items(), key=lambda kv: -kv[1][0])},
         "e2e": {"value": whole_job_seconds_per_step(e2e_s, e2e_steps, world), "unit": UNIT,
                 "steps": e2e_steps,
-                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "api": "atjup_gpu_upload_async, atjup_gpu_apply_uploads, atjup_gpu_step, "
+                       "atjup_gpu_download_async (copies of consecutive steps overlap the compute)"},
+        "e2e_serial": {"value": whole_job_seconds_per_step(e2e_serial_s, e2e_steps, world),
+                       "unit": UNIT, "api": "atjup_gpu_upload, atjup_gpu_step, atjup_gpu_download"},
         "gpu_launches": launches,
         "clocks": clk,
     }

@@ -187,6 +187,24 @@ int atjup_gpu_download_array(AtjupCtx* ctx, int32_t field_id, double*** x);
 /* Device pointer of a field (row pitch in elements via *pitch) for zero-copy interop (DLPack). */
 int atjup_gpu_field_ptr(AtjupCtx* ctx, int32_t field_id, void** dev_ptr, int32_t* pitch);
 
+/* Asynchronous exchange of whole fields, for a caller that keeps the state on the host and hands it
+ * to the library every step (no counterpart in the reference, which has no device). The copies run
+ * on two copy streams of the library's own, so step n+1's uploads and step n's downloads overlap
+ * step n's compute:
+ *   atjup_gpu_upload_async(ctx, id, host)    queue the copy of host (contiguous (i, j, k), pinned
+ *                                            for overlap) into a device staging buffer;
+ *   atjup_gpu_apply_uploads(ctx)             make the fields queued since the last call live, in
+ *                                            the order of the library's compute stream;
+ *   atjup_gpu_download_async(ctx, id, host)  snapshot the field in the compute stream's order and
+ *                                            queue its copy to host.
+ * Host buffers must stay untouched until atjup_gpu_synchronize, which waits for the copy streams
+ * too. A field takes effect only through atjup_gpu_apply_uploads; the time-level-n copies of the
+ * scalars are not touched (as with atjup_gpu_upload). Staging: two device copies of each field
+ * used, allocated on first use. */
+int atjup_gpu_upload_async(AtjupCtx* ctx, int32_t field_id, const double* host);
+int atjup_gpu_apply_uploads(AtjupCtx* ctx);
+int atjup_gpu_download_async(AtjupCtx* ctx, int32_t field_id, double* host);
+
 /* cJupiterModel::RungeKuttaJup (RungeKutta_Jup_Turb.cpp:261-583): buoyancy level mean,
  * hydrostatic pressure, four fused RK stages (RHSJup per cell, RHS_Jup_Turb.cpp:31-1457). */
 int atjup_gpu_rk4_step(AtjupCtx* ctx, int32_t iter_n);
