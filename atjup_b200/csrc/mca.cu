@@ -228,21 +228,20 @@ __global__ void mca_census_kernel(McaArgs a) {
             }
         }
     }
-    // the census counters: a block sum, added to one of NPART partial counters (summed on the
-    // host); adds from every warp to one address would serialise some 160k atomic operations
+    // the census counters: a warp sum, added by lane 0 to one of NPART partial counters (summed on
+    // the host). No block barrier: a warp whose pairs took no iterative solve leaves at once
+    // instead of waiting for the slowest warp of its block, and the partials keep the adds from
+    // contending on one address.
     for (int o = 16; o > 0; o >>= 1) {
         ut += __shfl_down_sync(0xffffffffu, ut, o);
         hd += __shfl_down_sync(0xffffffffu, hd, o);
     }
-    __shared__ unsigned long long sut[4], shd[4];
-    if ((threadIdx.x & 31) == 0) { sut[threadIdx.x >> 5] = ut; shd[threadIdx.x >> 5] = hd; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned long long bu = sut[0] + sut[1] + sut[2] + sut[3];
-        const unsigned long long bh = shd[0] + shd[1] + shd[2] + shd[3];
-        const unsigned part = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) % NPART;
-        if (bu) atomicAdd(&a.stats[8 + 2 * part], bu);
-        if (bh) atomicAdd(&a.stats[9 + 2 * part], bh);
+    if ((threadIdx.x & 31) == 0 && (ut | hd)) {
+        const unsigned warp = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) *
+                              (blockDim.x >> 5) + (threadIdx.x >> 5);
+        const unsigned part = warp % NPART;
+        if (ut) atomicAdd(&a.stats[8 + 2 * part], ut);
+        if (hd) atomicAdd(&a.stats[9 + 2 * part], hd);
     }
 }
 

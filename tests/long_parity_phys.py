@@ -3,7 +3,10 @@
 printing the relative L2 difference of every prognostic field. A measurement, not collected by
 pytest (the 200-iteration reference run takes several minutes on the host cores).
 
-    python tests/long_parity_phys.py [--iters 200]
+    python tests/long_parity_phys.py [--iters 200] [--mca]
+
+--mca runs both sides with the moist convective adjustment every iteration (the reference's
+default).
 
 Test infrastructure only (reads the reference through oracle/_ref like the other parity tests).
 """
@@ -25,14 +28,19 @@ from oracle_bridge import rel_l2  # noqa: E402
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--mca", action="store_true")
     args = ap.parse_args()
-    from atjup_b200.params import PREC_FP64, PREC_MIXED
+    from atjup_b200.params import PREC_FP64, PREC_MIXED, resolve_mca
+    from oracle_bridge import MCA_ENV
     t0 = time.time()
-    d, P, PH, MC, g, f = ref_iters_case(args.iters)
+    extra = ("--env", "ATJUP_MCA=1") if args.mca else ()
+    d, P, PH, MC, g, f = ref_iters_case(args.iters, *extra)
     t_ref = time.time() - t0
-    out = {"iterations": args.iters, "reference_seconds": round(t_ref, 1)}
+    out = {"iterations": args.iters, "mca": args.mca, "reference_seconds": round(t_ref, 1)}
     for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
         m = gpu_moist_model(P, PH, MC, g, f)
+        if args.mca:
+            m.set_mca(resolve_mca(MCA_ENV))
         m.set_precision(prec)
         for it in range(1, args.iters + 1):
             m.step(it, first=(it == 1))
