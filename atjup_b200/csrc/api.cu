@@ -528,10 +528,6 @@ int atjup_gpu_set_physics(AtjupCtx* c, const AtjupPhysics* ph, const float* laye
 int atjup_gpu_set_micro(AtjupCtx* c, const AtjupMicro* mc) {
     if (!c) { set_error("set_micro: null context"); return ATJUP_ERR_ARG; }
     if (!mc) { c->micro_on = false; return ATJUP_OK; }
-    if (!mc->nh4sh_eq) {
-        set_error("set_micro: ATJUP_NH4SH_EQ=0 (NH4SH by reaction rates) is not implemented");
-        return ATJUP_ERR_UNSUPPORTED;
-    }
     const int jm = c->P.jm;
     std::vector<double> cl(jm);
     const double pi_ = 3.14159265358979323846;

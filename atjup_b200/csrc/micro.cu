@@ -5,7 +5,7 @@
 //   precip_kernel         Precipitation<cJupiterModel>::run / column (Precipitation.h:191-445)
 //   nh4sh_kernel          ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373)
 //   difflux_kernel        the diffusive fluxes of DiffMassFluxJup (ChemistryJup.h:375-538, 756-780)
-//   massflux_kernel       ChemMassRateJup with the equilibrium on (ChemistryJup.h:59-281)
+//   massflux_kernel       ChemMassRateJup: reaction rate + diffusive flux (ChemistryJup.h:59-281)
 //   fluxlim_kernel        FluxLimiter<cJupiterModel>::nh4sh (FluxLimiter.h)
 //   clamp_species_kernel  clampNegativeSpecies (FileIO_Jup.cpp:494-548)
 //
@@ -380,7 +380,31 @@ __global__ void massflux_kernel(MicroArgs a) {
         for (int q = 0; q < 3; q++) a.massflux[q][c] = 0.0;
         return;
     }
-    for (int q = 0; q < 3; q++) a.massflux[q][c] = 0.0 + a.difflux[q][c];
+    // the reaction rates in kg/(m3 s), ordered like massflux (H2S, NH3, NH4SH); 0 with the
+    // equilibrium on and outside the 200..230 K formation window (the gate-zero default)
+    double w[3] = {0.0, 0.0, 0.0};
+    if (!a.mc.nh4sh_eq) {
+        const AtjupMicro& m = a.mc;
+        const double t_u = a.t[c] * a.t_ref;
+        if (t_u <= m.t_0_nh4sh && t_u >= m.t_00_nh4sh) {
+            const double keq = m.m_nh4sh / (m.m_nh3 * m.m_h2s);
+            const double kf = 15000.0 * pow(t_u, -0.5) * exp(-3020.0 / t_u);
+            const double kb = kf / keq;
+            const double nh3 = a.q[ATJUP_S_NH3][c], h2s = a.q[ATJUP_S_H2S][c], nh4sh = a.q[ATJUP_S_NH4SH][c];
+            // the concentrations normalised to carry r_mix together (the molar-concentration
+            // form is the non-default alternative)
+            const double sum_c = nh3 / m.m_nh3 + h2s / m.m_h2s + nh4sh / m.m_nh4sh;
+            const double denom = (sum_c == 0.0) ? 0.0 : a.r_mix / sum_c;
+            const double c_nh3 = nh3 / m.m_nh3 * denom;
+            const double c_h2s = h2s / m.m_h2s * denom;
+            const double c_nh4sh = nh4sh / m.m_nh4sh * denom;
+            const double R_diff = kf * c_nh3 * c_h2s - kb * c_nh4sh;
+            w[0] = -m.m_h2s * R_diff;
+            w[1] = -m.m_nh3 * R_diff;
+            w[2] = m.m_nh4sh * R_diff;
+        }
+    }
+    for (int q = 0; q < 3; q++) a.massflux[q][c] = w[q] + a.difflux[q][c];
 }
 
 __device__ __forceinline__ double superbee_phi(double r) {

@@ -190,7 +190,8 @@ class AtjupMicro(ctypes.Structure):
                                        "cia_strength", "opacity_strength", "solar_strength",
                                        "sw_tau_per_bar", "precip_rate_scale", "m_nh3", "m_h2s",
                                        "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh",
-                                       "polar_divisor_floor")] + [("gas", AtjupGasParams * 3)]
+                                       "polar_divisor_floor", "t_0_nh4sh", "t_00_nh4sh")] + [
+        ("gas", AtjupGasParams * 3)]
 
 
 # cJupiterModel's radiation constants (cJupiterModel.h:1109-1118), molar masses (255-270) and the
@@ -199,7 +200,8 @@ class AtjupMicro(ctypes.Structure):
 DEFAULT_MICRO = {"F_int": 5.4, "S_solar": 50.5, "albedo_bond": 0.343, "x_H2": 0.863,
                  "x_He": 0.134, "m_nh3": 17.03052, "m_h2s": 34.08088, "m_nh4sh": 51.1114,
                  "D_nh3": 0.92e-5 / (817.0 * 0.61), "D_h2s": 1.3e-5 / (949.0 * 0.94),
-                 "D_nh4sh": 0.0, "polar_divisor_floor": 0.4}
+                 "D_nh4sh": 0.0, "polar_divisor_floor": 0.4, "t_0_nh4sh": 230.0,
+                 "t_00_nh4sh": 200.0}
 
 
 def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, float] | None = None,
@@ -227,7 +229,7 @@ def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, 
     mc.sw_tau_per_bar = _env(env, "ATJUP_SW_TAU_PER_BAR", 1.0, float)
     mc.precip_rate_scale = _env(env, "ATJUP_PRECIP_SCALE", 1.0, float)
     for n in ("F_int", "S_solar", "albedo_bond", "x_H2", "x_He", "m_nh3", "m_h2s", "m_nh4sh",
-              "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor"):
+              "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor", "t_0_nh4sh", "t_00_nh4sh"):
         setattr(mc, n, c[n])
     gases = gases or DEFAULT_GASES
     for q, g in enumerate(("H2O", "NH3", "CH4")):
@@ -437,6 +439,8 @@ _UNSUPPORTED = {
     "ATJUP_DAMP_PDYN": ("0", "no Shapiro pass on p_dyn in the loop"),
     "ATJUP_HYDRO_REF": ("0", "the hydrostatic integral runs upward from the base"),
     "ATJUP_MCA_SMOOTH": ("0", "the latitude-smoothed stability search is not implemented"),
+    "ATJUP_CHEM_MOLAR_CONC": ("0", "the rate law's molar-concentration form is not implemented"),
+    "ATJUP_CHEM_GATE_ZERO": ("1", "the rate law keeps its last rate outside the window only with 1"),
     "ATJUP_MCA_PHASE": ("0", "the temperature-split phase rule is not implemented"),
     "ATJUP_CHROM": ("0", "the chromophore tracer is not implemented"),
     "ATJUP_CONV_ADJ": ("0", "the dry convective adjustment is not implemented"),

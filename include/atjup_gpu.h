@@ -341,7 +341,8 @@ int atjup_gpu_satadj(AtjupCtx* ctx, int32_t gas, const AtjupGasParams* gp, Atjup
 typedef struct AtjupMicro {
     int32_t radiation_on;        /* ATJUP_RADIATION 1                                             */
     int32_t precip_on;           /* ATJUP_PRECIP 1                                                */
-    int32_t nh4sh_eq;            /* ATJUP_NH4SH_EQ 1: NH4SH by equilibrium (ChemistryJup.h:285)    */
+    int32_t nh4sh_eq;            /* ATJUP_NH4SH_EQ 1: NH4SH by equilibrium (ChemistryJup.h:285);  */
+                                 /* 0: by the reaction-rate law (ChemistryJup.h:135-235)          */
     int32_t satadj_on;           /* the three gas adjustments (always on in the reference)        */
     int32_t solar_on;            /* ATJUP_SOLAR 1                                                 */
     int32_t rad_bottom;          /* ATJUP_RAD_BOTTOM 0: lower boundary of the thermal stream      */
@@ -359,6 +360,8 @@ typedef struct AtjupMicro {
     double m_nh3, m_h2s, m_nh4sh;          /* molar masses [kg/kmol]                              */
     double D_nh3, D_h2s, D_nh4sh;          /* mue / (rg sc): diffusivities of the mass fluxes     */
     double polar_divisor_floor;            /* 0.4 (ATPhys.h:104-108)                              */
+    double t_0_nh4sh, t_00_nh4sh;          /* 230, 200 K: the rate law's NH4SH formation window   */
+                                           /* (cJupiterModel.h:194-195; nh4sh_eq = 0)             */
     AtjupGasParams gas[3];                 /* H2O, NH3, CH4                                        */
 } AtjupMicro;
 
@@ -374,7 +377,8 @@ int atjup_gpu_precipitation(AtjupCtx* ctx);
  * equilibrium per cell by bisection, with its latent heat. */
 int atjup_gpu_nh4sh_equilibrium(AtjupCtx* ctx);
 /* The chemistry block of the loop: DiffMassFluxJup's diffusive fluxes (ChemistryJup.h:375-538),
- * their 1-2-1 smoothing, ChemMassRateJup (59-281; with the equilibrium on, massflux = difflux),
+ * their 1-2-1 smoothing, ChemMassRateJup (59-281; massflux = reaction rate + difflux, the rate
+ * zero with the equilibrium on),
  * FluxLimiterNH4SH (FluxLimiter.h) and the smoothing of the mass fluxes (cJupiterModel.cpp:
  * 1144-1162). */
 int atjup_gpu_chemistry(AtjupCtx* ctx);

@@ -2230,7 +2230,8 @@ void ora_chemistry(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G
                 for (int q = 0; q < 3; q++) X->difflux[q][c] = D[q] * chem_laplacian(P, MC, G, spec[q], i, j, k);
             }
     for (int q = 0; q < 3; q++) ora_shapiro(P, G, X->difflux[q], 2, 1.0, 1, 1);
-    /* ChemMassRateJup (59-281) with the equilibrium on: the reaction rates are 0 */
+    /* ChemMassRateJup (59-281): massflux = reaction rate + difflux; the rate is 0 with the
+     * equilibrium on (ATJUP_NH4SH_EQ=1) and outside the [t_00_nh4sh, t_0_nh4sh] window */
     for (int i = 0; i < im; i++)
         for (int k = 0; k < km; k++) {
             for (int j = 0; j < 3; j++)
@@ -2248,7 +2249,27 @@ void ora_chemistry(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G
                     for (int q = 0; q < 3; q++) mf[q][c] = 0.0;
                     continue;
                 }
-                for (int q = 0; q < 3; q++) mf[q][c] = 0.0 + X->difflux[q][c];
+                double w[3] = {0.0, 0.0, 0.0};    /* H2S, NH3, NH4SH */
+                const double t_u = S->t[c] * P->t_ref;
+                if (!MC->nh4sh_eq && t_u <= MC->t_0_nh4sh && t_u >= MC->t_00_nh4sh) {
+                    /* kf = A T^B exp(-T_d / T), A 15000, B -0.5, T_d 3020 (react_rate_const);
+                     * kb = kf / keq, keq = m_nh4sh / (m_nh3 m_h2s) */
+                    const double keq = MC->m_nh4sh / (MC->m_nh3 * MC->m_h2s);
+                    const double kf = 15000.0 * pow(t_u, -0.5) * exp(-3020.0 / t_u);
+                    const double kb = kf / keq;
+                    const double nh3 = spec[1][c], h2s = spec[0][c], nh4sh = spec[2][c];
+                    /* concentrations scaled so that they sum to r_mix (the default normalisation) */
+                    const double sum_c = nh3 / MC->m_nh3 + h2s / MC->m_h2s + nh4sh / MC->m_nh4sh;
+                    const double denom = (sum_c == 0.0) ? 0.0 : P->r_mix / sum_c;
+                    const double c_nh3 = nh3 / MC->m_nh3 * denom;
+                    const double c_h2s = h2s / MC->m_h2s * denom;
+                    const double c_nh4sh = nh4sh / MC->m_nh4sh * denom;
+                    const double R_diff = kf * c_nh3 * c_h2s - kb * c_nh4sh;
+                    w[0] = -MC->m_h2s * R_diff;
+                    w[1] = -MC->m_nh3 * R_diff;
+                    w[2] = MC->m_nh4sh * R_diff;
+                }
+                for (int q = 0; q < 3; q++) mf[q][c] = w[q] + X->difflux[q][c];
             }
     /* FluxLimiter<cJupiterModel>::nh4sh (FluxLimiter.h): superbee anti-diffusion of NH4SH */
     const double* Q = X->q[ATJUP_S_NH4SH];

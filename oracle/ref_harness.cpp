@@ -274,6 +274,8 @@ double ref_scalar(const char* name) {
     if (n == "D_h2s") return m.mue_h2s / (m.rg_h2s * m.sc_h2s);
     if (n == "D_nh4sh") return m.mue_nh4sh / (m.rg_nh4sh * m.sc_nh4sh);
     if (n == "polar_divisor_floor") return ATPhys::polar_divisor_floor<cJupiterModel>();
+    if (n == "t_0_nh4sh") return m.t_0_nh4sh;
+    if (n == "t_00_nh4sh") return m.t_00_nh4sh;
     if (n == "rad_F_int") return cJupiterModel::rad_F_int();
     if (n == "rad_S_solar") return cJupiterModel::rad_S_solar();
     if (n == "rad_albedo_bond") return cJupiterModel::rad_albedo_bond();

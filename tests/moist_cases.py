@@ -13,21 +13,33 @@ RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "al
 PROGNOSTIC = ("t", "u", "v", "w", "p_dyn") + SCALARS
 
 
+def env_of(extra) -> dict:
+    """MOIST_ENV with the "--env KEY=VALUE" pairs of a ref_dump flag list applied"""
+    env = dict(MOIST_ENV)
+    for flag, kv in zip(extra, extra[1:]):
+        if flag == "--env":
+            k, v = kv.split("=", 1)
+            env[k] = v
+    return env
+
+
 def ref_iters_case(iters=3, *extra):
     d = ref_dump("--phys-iters", str(iters), *extra)
-    P = dump_params(d, env=MOIST_ENV)
+    env = env_of(extra)
+    P = dump_params(d, env=env)
     P.has_nue = 1
     P.has_heating = 1
-    MC = resolve_micro(MOIST_ENV, {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items()
-                                   if k.startswith("micro_")},
+    MC = resolve_micro(env, {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items()
+                             if k.startswith("micro_")},
                        {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
     consts = {k[5:]: float(v) for k, v in d.items() if k.startswith("phys_")}
     consts["abl_height"] = float(d["knobd_abl_height"])
-    return d, P, resolve_physics(MOIST_ENV, consts), MC, dump_grid(d), dump_fields(d)
+    return d, P, resolve_physics(env, consts), MC, dump_grid(d), dump_fields(d)
 
 
-def synthetic_moist_case(im, jm, km, seed=41):
-    P, g, f = synthetic_case(im, jm, km, seed=seed, env=MOIST_ENV)
+def synthetic_moist_case(im, jm, km, seed=41, env=None):
+    env = MOIST_ENV if env is None else env
+    P, g, f = synthetic_case(im, jm, km, seed=seed, env=env)
     P.has_nue = 1
     P.has_heating = 1
     s = dict(f)
@@ -36,7 +48,7 @@ def synthetic_moist_case(im, jm, km, seed=41):
     shape = f["t"].shape
     for n in ("difflux_h2s", "difflux_nh3", "difflux_nh4sh"):
         f[n] = np.zeros(shape)
-    return P, resolve_physics(MOIST_ENV), resolve_micro(MOIST_ENV), g, f
+    return P, resolve_physics(env), resolve_micro(env), g, f
 
 
 def gpu_moist_model(P, PH, MC, g, f):

@@ -180,6 +180,7 @@ def bc_case(ref, g, data, seed=SATADJ_SEED + 3):
 
 
 MICRO_CONSTS = ("m_nh3", "m_h2s", "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor",
+                "t_0_nh4sh", "t_00_nh4sh",
                 "rad_F_int", "rad_S_solar", "rad_albedo_bond", "rad_x_H2", "rad_x_He",
                 "rad_cia_strength", "rad_opacity_strength", "rad_solar", "rad_solar_strength",
                 "rad_sw_tau_per_bar", "rad_bottom", "precip_rate_scale", "precip_coupling_on")

@@ -80,6 +80,13 @@ def test_unsupported_knobs_are_named():
     assert P.check_supported({}) == []
     bad = P.check_supported({"ATJUP_PRESS_LINE": "1", "ATJUP_T_LIMITER": "0"})
     assert len(bad) == 1 and bad[0].startswith("ATJUP_PRESS_LINE=1")
+    # NH4SH by the rate law is implemented in its default form only
+    assert P.check_supported({"ATJUP_NH4SH_EQ": "0"}) == []
+    bad = P.check_supported({"ATJUP_NH4SH_EQ": "0", "ATJUP_CHEM_MOLAR_CONC": "1",
+                             "ATJUP_CHEM_GATE_ZERO": "0"})
+    assert sorted(b.split("=")[0] for b in bad) == ["ATJUP_CHEM_GATE_ZERO", "ATJUP_CHEM_MOLAR_CONC"]
+    mc = P.resolve_micro({"ATJUP_NH4SH_EQ": "0"})
+    assert mc.nh4sh_eq == 0 and (mc.t_0_nh4sh, mc.t_00_nh4sh) == (230.0, 200.0)
 
 
 def _rank_main(rank, world, port, out):

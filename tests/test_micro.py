@@ -14,7 +14,12 @@ precipitation outputs (Q_precip, S_precip_*) are therefore held to a column-wise
 of the columns hold a cell that differs by more than 1e-12 of the field's maximum, every other cell
 agrees to relative L2 <= 1e-12, the grid totals agree to 1e-4, and no cell is off by more than half
 the field's maximum. Measured: 0.24 % of the columns flip on the reference's own state (totals to
-4e-7), up to 0.9 % on the synthetic 41x61x97 case (totals to 6e-5)."""
+4e-7), up to 0.9 % on the synthetic 41x61x97 case (totals to 6e-5).
+
+With ATJUP_NH4SH_EQ=0 NH4SH forms by the reaction-rate law of ChemMassRateJup
+(ChemistryJup.h:135-235) inside the 200..230 K window instead of the equilibrium: the same
+routines run with the rate law in the chemistry block, against the reference (oracle bit-exact,
+GPU to the bars above) and against the oracle on the synthetic shells."""
 import numpy as np
 import pytest
 
@@ -29,11 +34,16 @@ RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "al
           "rad_x_H2": "x_H2", "rad_x_He": "x_He"}
 
 
-def ref_micro_case():
-    d = ref_dump("--micro")
-    P = dump_params(d, env=MOIST_ENV)
+RATE_ENV = {**MOIST_ENV, "ATJUP_NH4SH_EQ": "0"}
+
+
+def ref_micro_case(env=MOIST_ENV):
+    flags = ("--micro",) + tuple(x for k, v in sorted(env.items()) if MOIST_ENV.get(k) != v
+                                 for x in ("--env", f"{k}={v}"))
+    d = ref_dump(*flags)
+    P = dump_params(d, env=env)
     consts = {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items() if k.startswith("micro_")}
-    MC = resolve_micro(MOIST_ENV, consts, {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
+    MC = resolve_micro(env, consts, {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
     return d, P, MC
 
 
@@ -52,6 +62,22 @@ def test_oracle_micro_bit_exact(ref_required):
     assert (d["mc_chemistry_fluxlim_nh4sh"] != 0).sum() > 10000
 
 
+@pytest.mark.slow
+def test_oracle_micro_rate_law_bit_exact(ref_required):
+    d, P, MC = ref_micro_case(RATE_ENV)
+    assert MC.nh4sh_eq == 0
+    out = oracle_micro(P, MC, dump_grid(d), dump_fields(d), STEPS)
+    for step in STEPS:
+        for n in MICRO_FIELDS + SPECIES:
+            assert np.array_equal(out[step][n], d[f"mc_{step}_{n}"], equal_nan=True), \
+                f"after {step}: {n} differs from the reference (rate law)"
+    # the rate acts: the mass fluxes differ from the equilibrium-on chemistry in many cells
+    MC.nh4sh_eq = 1
+    eq = oracle_micro(P, MC, dump_grid(d), dump_fields(d), STEPS)
+    for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh"):
+        assert (out["chemistry"][n] != eq["chemistry"][n]).sum() > 100000, n
+
+
 def test_resolve_micro_defaults():
     mc = resolve_micro({})
     assert (mc.radiation_on, mc.precip_on, mc.nh4sh_eq, mc.solar_on, mc.rad_bottom,
@@ -61,8 +87,8 @@ def test_resolve_micro_defaults():
     assert resolve_micro({"ATJUP_PRECIP_COUPLING": "0"}).precip_coupling_on == 0
 
 
-def micro_case(im, jm, km, seed=31):
-    P, g, f = synthetic_case(im, jm, km, seed=seed, env=MOIST_ENV)
+def micro_case(im, jm, km, seed=31, env=MOIST_ENV):
+    P, g, f = synthetic_case(im, jm, km, seed=seed, env=env)
     s = dict(f)
     s["solid"] = g["solid"]
     f.update(synthetic.physics(s, DEFAULT_GASES, seed=seed + 1))
@@ -75,7 +101,7 @@ def micro_case(im, jm, km, seed=31):
         f[n] = np.where(fluid & (rng.uniform(size=shape) < 0.005), -np.abs(f[n]) - 1e-9, f[n])
     for n in ("difflux_h2s", "difflux_nh3", "difflux_nh4sh"):
         f[n] = np.zeros(shape)
-    return P, resolve_physics(MOIST_ENV), resolve_micro(MOIST_ENV), g, f
+    return P, resolve_physics(env), resolve_micro(env), g, f
 
 
 def gpu_micro(P, PH, MC, g, f, steps=STEPS):
@@ -130,16 +156,18 @@ def check(got, want, where=""):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("env", [MOIST_ENV, RATE_ENV], ids=["equilibrium", "rate_law"])
 @pytest.mark.parametrize("shape", [(13, 37, 49), (41, 61, 97)])
-def test_gpu_micro_matches_oracle(shape):
-    P, PH, MC, g, f = micro_case(*shape)
+def test_gpu_micro_matches_oracle(shape, env):
+    P, PH, MC, g, f = micro_case(*shape, env=env)
     check(gpu_micro(P, PH, MC, g, f), oracle_micro(P, MC, g, f, STEPS), f"{shape}: ")
 
 
 @pytest.mark.gpu
-def test_gpu_micro_matches_reference_full_grid(ref_required):
-    d, P, MC = ref_micro_case()
+@pytest.mark.parametrize("env", [MOIST_ENV, RATE_ENV], ids=["equilibrium", "rate_law"])
+def test_gpu_micro_matches_reference_full_grid(ref_required, env):
+    d, P, MC = ref_micro_case(env)
     f = dump_fields(d)
-    got = gpu_micro(P, resolve_physics(MOIST_ENV), MC, dump_grid(d), f)
+    got = gpu_micro(P, resolve_physics(env), MC, dump_grid(d), f)
     flips = check(got, {s: {n: d[f"mc_{s}_{n}"] for n in MICRO_FIELDS + SPECIES} for s in STEPS}, "full grid: ")
     print("full-grid microphysics vs reference: flipped columns per precipitation field", flips)

@@ -15,6 +15,11 @@ it: started from its own state with t one ulp higher (relative 1.5e-16, `tests/r
 times that self-sensitivity: h2s and nh3 <= 1e-8, nh4sh <= 1e-7 (measured on the GPU 3.6e-9,
 7.4e-10, 2.9e-8).
 
+With ATJUP_NH4SH_EQ=0 NH4SH forms by the reaction-rate law of ChemMassRateJup
+(ChemistryJup.h:135-235) instead of the equilibrium (which is then skipped, and H2S and NH4SH
+leave the scalar sync): the oracle is bit-exact with the reference after 3 such iterations, and
+the GPU is held to the same bars after 3 and 20.
+
 On the synthetic shell the NH4SH flux limiter (a superbee switch and sign tests on NH4SH
 differences) and the precipitation's rain-evaporation switch can flip on a last-bit difference of
 exp/log/pow in a rare cell, which then shows in nh4sh: every other prognostic field is held to
@@ -28,16 +33,23 @@ import ref_dump as R
 
 REF_TOL = 1e-10
 NH4SH_FAMILY_TOL = {"h2s": 1e-8, "nh3": 1e-8, "nh4sh": 1e-7}
+RATE_LAW = ("--env", "ATJUP_NH4SH_EQ=0")
+CHEMISTRY = {"equilibrium": (), "rate_law": RATE_LAW}
 
 
 @pytest.mark.slow
-def test_oracle_moist_iterations_bit_exact(ref_required):
-    d, P, PH, MC, g, f = ref_iters_case(3)
+@pytest.mark.parametrize("chem", sorted(CHEMISTRY))
+def test_oracle_moist_iterations_bit_exact(ref_required, chem):
+    d, P, PH, MC, g, f = ref_iters_case(3, *CHEMISTRY[chem])
+    assert MC.nh4sh_eq == (chem == "equilibrium")
     out = oracle_iteration_phys(P, PH, MC, g, f, 3, snapshots=(1,))
     for it in (1, 3):
         for n in R.ITER_FIELDS:
             assert np.array_equal(out[it][n], d[f"it{it}_{n}"], equal_nan=True), \
                 f"iteration {it}: {n} differs from the reference"
+    if chem == "rate_law":
+        # no NH4SH in the initial state without the equilibrium: the rate law forms it
+        assert not f["nh4sh"].any() and (d["it3_nh4sh"] > 0).sum() > 10000
 
 
 def run_gpu(P, PH, MC, g, f, iters, snaps, names):
@@ -52,8 +64,13 @@ def run_gpu(P, PH, MC, g, f, iters, snaps, names):
 
 
 @pytest.mark.gpu
-def test_gpu_moist_step_matches_oracle_synthetic():
+@pytest.mark.parametrize("chem", sorted(CHEMISTRY))
+def test_gpu_moist_step_matches_oracle_synthetic(chem):
+    from atjup_b200.params import resolve_micro
+    from oracle_bridge import MOIST_ENV
     P, PH, MC, g, f = synthetic_moist_case(13, 37, 49)
+    if chem == "rate_law":
+        MC = resolve_micro({**MOIST_ENV, "ATJUP_NH4SH_EQ": "0"})
     want = oracle_iteration_phys(P, PH, MC, g, f, 3, snapshots=(1,))
     got = run_gpu(P, PH, MC, g, f, 3, (1, 3), PROGNOSTIC)
     for it in (1, 3):
@@ -64,13 +81,14 @@ def test_gpu_moist_step_matches_oracle_synthetic():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("chem", sorted(CHEMISTRY))
 @pytest.mark.parametrize("iters", [3, 20])
-def test_gpu_moist_step_matches_reference(ref_required, iters):
-    d, P, PH, MC, g, f = ref_iters_case(iters)
+def test_gpu_moist_step_matches_reference(ref_required, iters, chem):
+    d, P, PH, MC, g, f = ref_iters_case(iters, *CHEMISTRY[chem])
     got = run_gpu(P, PH, MC, g, f, iters, (iters,), PROGNOSTIC)[iters]
     worst = {n: rel_l2(got[n], d[f"it{iters}_{n}"]) for n in PROGNOSTIC}
     report = {k: f"{v:.1e}" for k, v in worst.items()}
-    print(f"full physics, {iters} iterations vs reference:", report)
+    print(f"full physics ({chem}), {iters} iterations vs reference:", report)
     for n in PROGNOSTIC:
         assert np.isfinite(got[n]).all(), f"{n}: non-finite"
         assert worst[n] <= NH4SH_FAMILY_TOL.get(n, REF_TOL), f"after {iters} iterations: {n} relative L2 {worst[n]:.3e} ({report})"
