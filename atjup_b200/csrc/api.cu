@@ -20,7 +20,7 @@ int cuda_status(cudaError_t e, const char* what) {
     return ATJUP_ERR_CUDA;
 }
 
-void timer_begin(AtjupCtx* c, int cls) {
+void timer_begin(AtjupCtx* c, int cls, cudaStream_t st) {
     if (!c->timing) return;
     if ((size_t)(2 * c->tn + 2) > c->tev.size()) {
         for (int q = 0; q < 512; q++) {
@@ -31,21 +31,24 @@ void timer_begin(AtjupCtx* c, int cls) {
     }
     c->tcls.resize(c->tn + 1);
     c->tcls[c->tn] = cls;
-    cudaEventRecord(c->tev[2 * c->tn], c->stream);
+    cudaEventRecord(c->tev[2 * c->tn], st);
 }
 
-void timer_end(AtjupCtx* c) {
+void timer_end(AtjupCtx* c, cudaStream_t st) {
     if (!c->timing) return;
-    cudaEventRecord(c->tev[2 * c->tn + 1], c->stream);
+    cudaEventRecord(c->tev[2 * c->tn + 1], st);
     c->tn++;
 }
 
 namespace {
 
+// brackets the launches of one timing class with events on the compute stream (or on st)
 struct Timed {
     AtjupCtx* c;
-    Timed(AtjupCtx* c_, int cls) : c(c_) { timer_begin(c, cls); }
-    ~Timed() { timer_end(c); }
+    cudaStream_t st;
+    Timed(AtjupCtx* c_, int cls) : c(c_), st(c_->stream) { timer_begin(c, cls, st); }
+    Timed(AtjupCtx* c_, int cls, cudaStream_t s) : c(c_), st(s) { timer_begin(c, cls, st); }
+    ~Timed() { timer_end(c, st); }
 };
 
 int alloc(double** p, size_t n) {
@@ -56,6 +59,13 @@ int alloc(double** p, size_t n) {
 
 void free_all(AtjupCtx* c) {
     xfer_free(c);
+    if (c->side) {
+        cudaStreamSynchronize(c->side);
+        cudaEventDestroy(c->side_fork);
+        cudaEventDestroy(c->side_join);
+        cudaStreamDestroy(c->side);
+        c->side = nullptr;
+    }
     solver_free(c);
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
     for (auto& p : c->f2) { cudaFree(p); p = nullptr; }
@@ -207,6 +217,12 @@ int atjup_gpu_set_stream(AtjupCtx* c, void* stream) {
         ATJUP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         c->own_stream = true;
     }
+    return ATJUP_OK;
+}
+
+int atjup_gpu_stream(AtjupCtx* c, void** stream) {
+    if (!c || !stream) { set_error("stream: null argument"); return ATJUP_ERR_ARG; }
+    *stream = (void*)c->stream;
     return ATJUP_OK;
 }
 
@@ -428,21 +444,36 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
     void* out2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
     const void* const* ins[4] = {in0, in1, in2, in1};
     void* const* outs[4] = {out1, out2, out1, nullptr};
+    // The species and closure kernels of stage s read the stage input ins[s] and write only scalar
+    // buffers; the dynamics kernel of stage s reads ins[s] too and writes outs[s], which is the
+    // input the scalars of stage s - 1 read (X1 for stage 2, the FP64 state for stage 3). So the
+    // scalars of stage s run on the side stream beside the dynamics of stage s: they start after
+    // the dynamics of stage s - 1 (fork), and the dynamics of stage s + 1 starts after them (join).
+    const bool fork = c->phys_on && (c->phys.species_on || c->phys.turb_on);
+    if (fork && !c->side) {
+        ATJUP_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming));
+        ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming));
+    }
     for (int s = 0; s < 4; s++) {
-        if (c->phys_on) {
-            // species and closure first: they read the same stage input velocities, and the
-            // dynamics stage 3 writes its result over the stage-0 input
+        if (fork) {
+            ATJUP_CUDA(cudaEventRecord(c->side_fork, c->stream));
+            ATJUP_CUDA(cudaStreamWaitEvent(c->side, c->side_fork, 0));
             if (c->phys.species_on) {
-                Timed tm(c, TK_SPECIES);
-                if ((rc = launch_phys_stage(c, s, ins[s], 0))) return rc;
+                Timed tm(c, TK_SPECIES, c->side);
+                if ((rc = launch_phys_stage(c, s, ins[s], 0, c->side))) return rc;
             }
             if (c->phys.turb_on) {
-                Timed tm(c, TK_CLOSURE);
-                if ((rc = launch_phys_stage(c, s, ins[s], 1))) return rc;
+                Timed tm(c, TK_CLOSURE, c->side);
+                if ((rc = launch_phys_stage(c, s, ins[s], 1, c->side))) return rc;
             }
+            ATJUP_CUDA(cudaEventRecord(c->side_join, c->side));
         }
-        Timed tm(c, TK_RK_STAGE);
-        if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
+        {
+            Timed tm(c, TK_RK_STAGE);
+            if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
+        }
+        if (fork) ATJUP_CUDA(cudaStreamWaitEvent(c->stream, c->side_join, 0));
     }
     return ATJUP_OK;
 }

@@ -53,6 +53,10 @@ struct AtjupCtx {
     cudaEvent_t x_out_ready = nullptr;
     unsigned long long x_pending[2] = {0, 0};
     long long x_round = 0;
+    // a second compute stream: the species and closure kernels of an RK stage run on it beside
+    // the dynamics kernel of the same stage (one fork and one join per stage)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
     int KP = 0;              // padded row pitch (elements)
     size_t NP = 0;           // im * jm * KP
     bool grid_set = false;
@@ -143,8 +147,8 @@ void set_error(const std::string& msg);
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
        TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_MCA, TK_COUNT };
-void timer_begin(AtjupCtx* c, int cls);
-void timer_end(AtjupCtx* c);
+void timer_begin(AtjupCtx* c, int cls, cudaStream_t st);
+void timer_end(AtjupCtx* c, cudaStream_t st);
 int cuda_status(cudaError_t e, const char* what);
 
 inline size_t cell(const AtjupCtx* c, int i, int j, int k) {
@@ -176,7 +180,7 @@ void xfer_free(AtjupCtx* c);
 int xfer_synchronize(AtjupCtx* c);
 int launch_satadj(AtjupCtx* c, int gas, const AtjupGasParams& gp);
 extern const int kScalarField[ATJUP_S_COUNT + 2];
-int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what);
+int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what, cudaStream_t st);
 int launch_turbulence(AtjupCtx* c);
 int launch_turb_wall_hold(AtjupCtx* c);
 enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP };

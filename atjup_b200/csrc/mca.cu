@@ -66,10 +66,13 @@ __device__ __forceinline__ double svp(double T, double lT, double C, double L0, 
                                       double db) {
     return exp(C + (-L0 / T + da * lT + db * T) / (1e-3 * R));
 }
+// the phase's coefficients are selected first, so the saturation curve is one exp in the code
+// (the liquid and ice curves are the same expression on different constants)
 __device__ __forceinline__ double qsat(const McaArgs& a, int g, double T, double lT, double p) {
     const AtjupGasParams& s = a.gas[g];
-    const double E = (T >= s.t_0) ? svp(T, lT, s.C, s.L0, s.R, s.del_alf, s.del_bet)
-                                  : svp(T, lT, s.C_i, s.L0_i, s.R, s.del_alf_i, s.del_bet_i);
+    const bool liq = T >= s.t_0;
+    const double E = svp(T, lT, liq ? s.C : s.C_i, liq ? s.L0 : s.L0_i, s.R,
+                         liq ? s.del_alf : s.del_alf_i, liq ? s.del_bet : s.del_bet_i);
     const double q = s.ep * E / p;
     return isfinite(q) ? q : 0.0;
 }
@@ -203,8 +206,10 @@ __global__ void mca_bounds_kernel(const uint8_t* solid, int2* bounds, int im, in
     bounds[(size_t)j * km + k] = make_int2(i0, i1);
 }
 
-// one thread per pair (i, i+1): the census of the unadjusted column
-__global__ void mca_census_kernel(McaArgs a) {
+// one thread per pair (i, i+1): the census of the unadjusted column. Capped at 64 registers
+// (eight blocks per SM): the solve is a chain of dependent FP64 exp/log, and the extra warps hide
+// more of it than the few spilled values cost.
+__global__ void __launch_bounds__(128, 8) mca_census_kernel(McaArgs a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
     unsigned long long ut = 0, hd = 0;
     if (k < a.km) {

@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
 // (RHS_Jup_Turb.cpp:257-303, 736-998, 1399-1452). One instantiation per closure model, so that
 // each holds the registers of its own branch only.
 template <int MODEL, typename TI, typename TO, typename TA, typename R>
-__global__ void __launch_bounds__(256, 3) closure_stage_kernel(PhysStage a) {
+__global__ void __launch_bounds__(256, 4) closure_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
@@ -529,25 +529,25 @@ PhysStage stage_args(AtjupCtx* c, int stage, const void* const* vin) {
 }  // namespace
 
 template <typename TI, typename TO, typename TA, typename R>
-static int launch_typed(AtjupCtx* c, const PhysStage& a, int what) {
+static int launch_typed(AtjupCtx* c, const PhysStage& a, int what, cudaStream_t st) {
     const AtjupParams& P = c->P;
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
     if (what == 0) {
         const dim3 sgrid(grid.x, grid.y, P.im * ATJUP_S_COUNT);
-        species_stage_kernel<TI, TO, TA, R><<<sgrid, block, 0, c->stream>>>(a);
+        species_stage_kernel<TI, TO, TA, R><<<sgrid, block, 0, st>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");
     } else {
         switch (a.turb_model) {
         case ATJUP_TURB_K_EPSILON:
-            closure_stage_kernel<ATJUP_TURB_K_EPSILON, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_EPSILON, TI, TO, TA, R><<<grid, block, 0, st>>>(a);
             break;
         case ATJUP_TURB_K_OMEGA:
-            closure_stage_kernel<ATJUP_TURB_K_OMEGA, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA, TI, TO, TA, R><<<grid, block, 0, st>>>(a);
             break;
         default:
-            closure_stage_kernel<ATJUP_TURB_K_OMEGA_SST, TI, TO, TA, R><<<grid, block, 0, c->stream>>>(a);
+            closure_stage_kernel<ATJUP_TURB_K_OMEGA_SST, TI, TO, TA, R><<<grid, block, 0, st>>>(a);
         }
         c->launches++;
         ATJUP_CHECK_LAUNCH("closure_stage_kernel");
@@ -555,14 +555,15 @@ static int launch_typed(AtjupCtx* c, const PhysStage& a, int what) {
     return ATJUP_OK;
 }
 
-// species_stage_kernel of one RK stage (what = 0) or closure_stage_kernel (what = 1); vin are
-// the stage input's t, u, v, w (stage 0: the FP64 state; later stages: the stage buffers)
-int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what) {
+// species_stage_kernel of one RK stage (what = 0) or closure_stage_kernel (what = 1) on stream
+// st; vin are the stage input's t, u, v, w (stage 0: the FP64 state; later stages: the stage
+// buffers)
+int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what, cudaStream_t st) {
     const PhysStage a = stage_args(c, stage, vin);
-    if (c->step_prec != ATJUP_PREC_MIXED) return launch_typed<double, double, double, double>(c, a, what);
-    if (stage == 0) return launch_typed<double, float, float, float>(c, a, what);
-    if (stage < 3) return launch_typed<float, float, float, float>(c, a, what);
-    return launch_typed<float, double, float, float>(c, a, what);
+    if (c->step_prec != ATJUP_PREC_MIXED) return launch_typed<double, double, double, double>(c, a, what, st);
+    if (stage == 0) return launch_typed<double, float, float, float>(c, a, what, st);
+    if (stage < 3) return launch_typed<float, float, float, float>(c, a, what, st);
+    return launch_typed<float, double, float, float>(c, a, what, st);
 }
 
 }  // namespace atjup

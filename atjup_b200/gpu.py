@@ -41,6 +41,7 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_create.argtypes = [ctypes.POINTER(_p.AtjupParams), ctypes.POINTER(vp)]
     L.atjup_gpu_destroy.argtypes = [vp]
     L.atjup_gpu_set_stream.argtypes = [vp, vp]
+    L.atjup_gpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.atjup_gpu_upload.argtypes = [vp, i32, vp]
     L.atjup_gpu_download.argtypes = [vp, i32, vp]
@@ -271,6 +272,12 @@ class GpuModel:
 
     def set_stream(self, stream_handle: int | None):
         _check(self.L.atjup_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
+
+    def stream_handle(self) -> int:
+        """the cudaStream_t the context issues its work on, as an integer"""
+        s = ctypes.c_void_p()
+        _check(self.L.atjup_gpu_stream(self.ctx, ctypes.byref(s)))
+        return s.value or 0
 
     # ---- the hot path, by the reference's routine names ----
     def runge_kutta(self, iter_n: int = 0):

@@ -310,8 +310,9 @@ def main():
     if args.precision == "mixed":
         m.set_precision(PREC_MIXED)
     m.upload_state(fields)
-    stream = torch.cuda.Stream()
-    m.set_stream(stream.cuda_stream)
+    # events are recorded on the library's own stream; no torch stream is created, so the process
+    # holds only the library's streams and each gets a hardware queue of its own
+    stream = torch.cuda.ExternalStream(m.stream_handle())
 
     it = [0]
 

@@ -165,6 +165,13 @@ int atjup_gpu_destroy(AtjupCtx* ctx);
 
 /* Use a caller-owned cudaStream_t (passed as void*); NULL = the context's own stream. */
 int atjup_gpu_set_stream(AtjupCtx* ctx, void* stream);
+/* The cudaStream_t (as void*) the context issues its work on, its own or the one set above, for
+ * a caller that records events on it or orders its own work after the library's. Besides it the
+ * library uses up to three streams of its own (the scalar stages of the RK step, and the two copy
+ * streams of the asynchronous exchange). A process whose streams outnumber
+ * CUDA_DEVICE_MAX_CONNECTIONS (8 by default) shares hardware queues between streams, which can
+ * order an asynchronous copy behind unrelated compute. (No reference counterpart.) */
+int atjup_gpu_stream(AtjupCtx* ctx, void** stream);
 
 /* Geometry and frozen per-(i,j) inputs:
  *   rad[im]      metric radius rad.z (cJupiterModel.cpp:441-468 shifts it to R/L_atm + i dr)

@@ -6,7 +6,8 @@ copies run on the library's copy streams and overlap the compute of neighbouring
 * Three full-physics steps, each with its own inputs (so a stale or early copy would show), the
   results of every step downloaded: bit-identical to the synchronous path.
 * Two downloads of one field around a step, with no upload in between (the same staging buffer
-  reused): the first holds the state before the step, the second after it."""
+  reused): the first holds the state before the step, the second after it.
+* atjup_gpu_stream returns the stream the context issues on, before and after atjup_gpu_set_stream."""
 import numpy as np
 import pytest
 
@@ -75,3 +76,21 @@ def test_async_download_reuses_its_buffer_in_order():
     m.close()
     assert np.array_equal(a, before)
     assert np.array_equal(b, after)
+
+
+@pytest.mark.gpu
+def test_stream_handle_follows_set_stream():
+    import torch
+    P, PH, MC, g, f = synthetic_moist_case(13, 37, 49, seed=63)
+    m = gpu_moist_model(P, PH, MC, g, f)
+    own = m.stream_handle()
+    assert own != 0
+    s = torch.cuda.Stream()
+    m.set_stream(s.cuda_stream)
+    assert m.stream_handle() == s.cuda_stream
+    m.step(1, first=True)
+    m.synchronize()
+    m.set_stream(None)                     # back to a stream of the context's own
+    assert m.stream_handle() not in (0, s.cuda_stream)
+    assert m.nonfinite_count() == 0
+    m.close()
