@@ -20,24 +20,25 @@ int cuda_status(cudaError_t e, const char* what) {
     return ATJUP_ERR_CUDA;
 }
 
-void timer_begin(AtjupCtx* c, int cls, cudaStream_t st) {
-    if (!c->timing) return;
+int timer_begin(AtjupCtx* c, int cls, cudaStream_t st) {
+    if (!c->timing) return -1;
     if ((size_t)(2 * c->tn + 2) > c->tev.size()) {
         for (int q = 0; q < 512; q++) {
             cudaEvent_t e;
-            if (cudaEventCreate(&e) != cudaSuccess) { c->timing = false; return; }
+            if (cudaEventCreate(&e) != cudaSuccess) { c->timing = false; return -1; }
             c->tev.push_back(e);
         }
     }
-    c->tcls.resize(c->tn + 1);
-    c->tcls[c->tn] = cls;
-    cudaEventRecord(c->tev[2 * c->tn], st);
+    const int n = c->tn++;
+    c->tcls.resize(c->tn);
+    c->tcls[n] = cls;
+    cudaEventRecord(c->tev[2 * n], st);
+    return n;
 }
 
-void timer_end(AtjupCtx* c, cudaStream_t st) {
-    if (!c->timing) return;
-    cudaEventRecord(c->tev[2 * c->tn + 1], st);
-    c->tn++;
+void timer_end(AtjupCtx* c, int slot, cudaStream_t st) {
+    if (slot < 0) return;
+    cudaEventRecord(c->tev[2 * slot + 1], st);
 }
 
 namespace {
@@ -46,9 +47,41 @@ namespace {
 struct Timed {
     AtjupCtx* c;
     cudaStream_t st;
-    Timed(AtjupCtx* c_, int cls) : c(c_), st(c_->stream) { timer_begin(c, cls, st); }
-    Timed(AtjupCtx* c_, int cls, cudaStream_t s) : c(c_), st(s) { timer_begin(c, cls, st); }
-    ~Timed() { timer_end(c, st); }
+    int slot;
+    Timed(AtjupCtx* c_, int cls) : c(c_), st(c_->stream), slot(timer_begin(c_, cls, c_->stream)) {}
+    Timed(AtjupCtx* c_, int cls, cudaStream_t s) : c(c_), st(s), slot(timer_begin(c_, cls, s)) {}
+    ~Timed() { timer_end(c, slot, st); }
+};
+
+// The side stream: work that is independent of the compute stream's next launches runs on it
+// (the scalar RK stages beside the dynamics stage, precipitation beside the closure update and
+// the chemistry, the moist convective adjustment beside the velocity filters). fork_side orders
+// the side stream after everything issued so far on the compute stream; join_side orders the
+// compute stream after everything issued so far on the side stream.
+int side_init(AtjupCtx* c) {
+    if (c->side) return ATJUP_OK;
+    ATJUP_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming));
+    ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming));
+    return ATJUP_OK;
+}
+int fork_side(AtjupCtx* c) {
+    if (int rc = side_init(c)) return rc;
+    ATJUP_CUDA(cudaEventRecord(c->side_fork, c->stream));
+    ATJUP_CUDA(cudaStreamWaitEvent(c->side, c->side_fork, 0));
+    return ATJUP_OK;
+}
+int join_side(AtjupCtx* c) {
+    ATJUP_CUDA(cudaEventRecord(c->side_join, c->side));
+    ATJUP_CUDA(cudaStreamWaitEvent(c->stream, c->side_join, 0));
+    return ATJUP_OK;
+}
+// issues the enclosed entry points on the side stream (they launch on c->stream)
+struct OnSide {
+    AtjupCtx* c;
+    cudaStream_t main;
+    explicit OnSide(AtjupCtx* c_) : c(c_), main(c_->stream) { c->stream = c->side; }
+    ~OnSide() { c->stream = main; }
 };
 
 int alloc(double** p, size_t n) {
@@ -450,30 +483,36 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
     // scalars of stage s run on the side stream beside the dynamics of stage s: they start after
     // the dynamics of stage s - 1 (fork), and the dynamics of stage s + 1 starts after them (join).
     const bool fork = c->phys_on && (c->phys.species_on || c->phys.turb_on);
-    if (fork && !c->side) {
-        ATJUP_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-        ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming));
-        ATJUP_CUDA(cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming));
-    }
     for (int s = 0; s < 4; s++) {
+        // timing slots of the stage: the dynamics kernel's, the side stream's first and last (the
+        // stage's span is read from them; an event of its own here would change how the two
+        // streams' kernels share the GPU)
+        int side_first = -1, side_last = -1, dyn = -1;
         if (fork) {
-            ATJUP_CUDA(cudaEventRecord(c->side_fork, c->stream));
-            ATJUP_CUDA(cudaStreamWaitEvent(c->side, c->side_fork, 0));
+            if ((rc = fork_side(c))) return rc;
             if (c->phys.species_on) {
                 Timed tm(c, TK_SPECIES, c->side);
+                side_first = side_last = tm.slot;
                 if ((rc = launch_phys_stage(c, s, ins[s], 0, c->side))) return rc;
             }
             if (c->phys.turb_on) {
                 Timed tm(c, TK_CLOSURE, c->side);
+                if (side_first < 0) side_first = tm.slot;
+                side_last = tm.slot;
                 if ((rc = launch_phys_stage(c, s, ins[s], 1, c->side))) return rc;
             }
-            ATJUP_CUDA(cudaEventRecord(c->side_join, c->side));
         }
         {
             Timed tm(c, TK_RK_STAGE);
+            dyn = tm.slot;
             if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
         }
-        if (fork) ATJUP_CUDA(cudaStreamWaitEvent(c->stream, c->side_join, 0));
+        if (fork && (rc = join_side(c))) return rc;
+        if (dyn >= 0) {
+            c->tgrp.push_back(dyn);
+            c->tgrp.push_back(side_first);
+            c->tgrp.push_back(side_last);
+        }
     }
     return ATJUP_OK;
 }
@@ -777,6 +816,7 @@ int copy_to_n(AtjupCtx* c, const int* idx, int n) {
 // device), the closure update and the chemistry block.
 int physics_block(AtjupCtx* c) {
     int rc;
+    bool side_precip = false;
     const AtjupMicro& mc = c->micro;
     if (c->micro_on) {
         if (mc.radiation_on && (rc = atjup_gpu_radiation(c))) return rc;
@@ -785,7 +825,18 @@ int physics_block(AtjupCtx* c) {
                 if ((rc = atjup_gpu_satadj(c, g, &mc.gas[g], nullptr))) return rc;
         }
         if (mc.nh4sh_eq && (rc = atjup_gpu_nh4sh_equilibrium(c))) return rc;
-        if (mc.precip_on && (rc = atjup_gpu_precipitation(c))) return rc;
+        // Coupled precipitation writes only its sources (S_precip_*, Q_precip), which nothing
+        // before the RK step reads, and reads t and the species, which nothing before the RK step
+        // writes: it runs on the side stream beside the n copies, the closure update and the
+        // chemistry. Uncoupled, it writes the species, and stays in order.
+        side_precip = mc.precip_on && mc.precip_coupling_on;
+        if (side_precip) {
+            if ((rc = fork_side(c))) return rc;
+            OnSide on(c);
+            if ((rc = atjup_gpu_precipitation(c))) return rc;
+        } else if (mc.precip_on && (rc = atjup_gpu_precipitation(c))) {
+            return rc;
+        }
         const int sync[11] = {ATJUP_S_H2O, ATJUP_S_H2O_CLOUD, ATJUP_S_H2O_ICE, ATJUP_S_NH3,
                               ATJUP_S_NH3_CLOUD, ATJUP_S_NH3_ICE, ATJUP_S_CH4, ATJUP_S_CH4_CLOUD,
                               ATJUP_S_CH4_ICE, ATJUP_S_H2S, ATJUP_S_NH4SH};
@@ -793,6 +844,7 @@ int physics_block(AtjupCtx* c) {
     }
     if (c->phys.turb_on && (rc = atjup_gpu_turbulence(c))) return rc;
     if (c->micro_on && (rc = atjup_gpu_chemistry(c))) return rc;
+    if (side_precip && (rc = join_side(c))) return rc;
     return ATJUP_OK;
 }
 }  // namespace
@@ -813,7 +865,13 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
         Timed tm(c, TK_TURB);
         if ((rc = launch_turb_wall_hold(c))) return rc;
     }
-    if (ph && c->mca_on && iter_n % c->mca.stride == 0) {
+    // The moist convective adjustment reads and writes t, the vapours, condensates and tracers;
+    // the velocity filters and the column balance only u, v, w: the adjustment runs on the side
+    // stream beside them, joined before the species clamp.
+    const bool mca_now = ph && c->mca_on && iter_n % c->mca.stride == 0;
+    if (mca_now) {
+        if ((rc = fork_side(c))) return rc;
+        OnSide on(c);
         Timed tm(c, TK_MCA);
         if ((rc = launch_mca(c))) return rc;
     }
@@ -825,6 +883,7 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
         Timed tm(c, TK_BALANCE_V);
         if ((rc = launch_balance_v(c))) return rc;
     }
+    if (mca_now && (rc = join_side(c))) return rc;
     if (ph) {
         // clampNegativeSpecies, then restoreVar of the scalars (the dynamics need none)
         if (c->micro_on && (rc = atjup_gpu_clamp_species(c))) return rc;
@@ -856,6 +915,7 @@ int atjup_gpu_timing(AtjupCtx* c, int32_t enable) {
     ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     c->tn = 0;
     c->tcls.clear();
+    c->tgrp.clear();
     c->timing = enable != 0;
     return ATJUP_OK;
 }
@@ -864,6 +924,30 @@ int atjup_gpu_timing_read(AtjupCtx* c, int32_t cls, double* total_ms, int64_t* c
     if (!c || cls < 0 || cls >= TK_COUNT) return ATJUP_ERR_ARG;
     double tot = 0.0;
     int64_t n = 0;
+    if (cls == TK_RK_GROUP) {
+        // per RK stage: from the earlier start to the later end of the dynamics kernel (slot 0)
+        // and the second stream's kernels (first slot 1, last slot 2); the largest elapsed time
+        // over the start and end pairs is that span
+        for (size_t g = 0; g + 2 < c->tgrp.size(); g += 3) {
+            const int starts[2] = {c->tgrp[g], c->tgrp[g + 1]}, ends[2] = {c->tgrp[g], c->tgrp[g + 2]};
+            double span = 0.0;
+            for (int en : ends) {
+                if (en < 0) continue;
+                ATJUP_CUDA(cudaEventSynchronize(c->tev[2 * en + 1]));
+                for (int st : starts) {
+                    if (st < 0) continue;
+                    float ms = 0.f;
+                    ATJUP_CUDA(cudaEventElapsedTime(&ms, c->tev[2 * st], c->tev[2 * en + 1]));
+                    span = std::max(span, (double)ms);
+                }
+            }
+            tot += span;
+            n++;
+        }
+        if (total_ms) *total_ms = tot;
+        if (count) *count = n;
+        return ATJUP_OK;
+    }
     for (int q = 0; q < c->tn; q++) {
         if (c->tcls[q] != cls) continue;
         ATJUP_CUDA(cudaEventSynchronize(c->tev[2 * q + 1]));

@@ -137,6 +137,9 @@ struct AtjupCtx {
     bool timing = false;
     std::vector<cudaEvent_t> tev;     // event pool, two per timed launch
     std::vector<int> tcls;            // class of each timed launch
+    // the RK stages run on two streams: per stage the slot whose start opens it and the slots
+    // whose ends close it (class TK_RK_GROUP is read from these, without events of its own)
+    std::vector<int> tgrp;            // three slots per stage: start, end, end (-1: none)
     int tn = 0;                       // timed launches recorded
 };
 
@@ -146,9 +149,12 @@ void set_error(const std::string& msg);
 
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
-       TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_MCA, TK_COUNT };
-void timer_begin(AtjupCtx* c, int cls, cudaStream_t st);
-void timer_end(AtjupCtx* c, cudaStream_t st);
+       TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_MCA, TK_RK_GROUP,
+       TK_COUNT };
+// an event pair per timed region: timer_begin records the start on st and returns the region's
+// slot (-1 with timing off), timer_end records the end of that slot; regions may nest
+int timer_begin(AtjupCtx* c, int cls, cudaStream_t st);
+void timer_end(AtjupCtx* c, int slot, cudaStream_t st);
 int cuda_status(cudaError_t e, const char* what);
 
 inline size_t cell(const AtjupCtx* c, int i, int j, int k) {

@@ -32,10 +32,12 @@ int xfer_init(AtjupCtx* c) {
     return ATJUP_OK;
 }
 
-int stage_buffer(AtjupCtx* c, double** p) {
-    if (*p) return ATJUP_OK;
+// both rounds' staging buffers of a field (pair[0], pair[1]) are allocated at its first exchange,
+// so a steady exchange allocates nothing (a cudaMalloc in a later round would wait for the device)
+int stage_buffer(AtjupCtx* c, double** pair0, double** pair1) {
     const AtjupParams& P = c->P;
-    ATJUP_CUDA(cudaMalloc(p, sizeof(double) * (size_t)P.im * P.jm * P.km));
+    for (double** p : {pair0, pair1})
+        if (!*p) ATJUP_CUDA(cudaMalloc(p, sizeof(double) * (size_t)P.im * P.jm * P.km));
     return ATJUP_OK;
 }
 
@@ -82,7 +84,7 @@ int atjup_gpu_upload_async(AtjupCtx* c, int32_t id, const double* host) {
     int rc = xfer_init(c);
     if (rc) return rc;
     const int s = c->x_round & 1;
-    if ((rc = stage_buffer(c, &c->x_up[s][id]))) return rc;
+    if ((rc = stage_buffer(c, &c->x_up[0][id], &c->x_up[1][id]))) return rc;
     // the buffer's last reader (the apply of the round before last) must be done with it
     ATJUP_CUDA(cudaStreamWaitEvent(c->x_h2d, c->x_up_free[s][id], 0));
     const AtjupParams& P = c->P;
@@ -116,7 +118,7 @@ int atjup_gpu_download_async(AtjupCtx* c, int32_t id, double* host) {
     int rc = xfer_init(c);
     if (rc) return rc;
     const int s = c->x_round & 1;
-    if ((rc = stage_buffer(c, &c->x_out[s][id]))) return rc;
+    if ((rc = stage_buffer(c, &c->x_out[0][id], &c->x_out[1][id]))) return rc;
     // the buffer's last reader (an earlier copy to the host) must be done with it
     ATJUP_CUDA(cudaStreamWaitEvent(c->stream, c->x_out_free[s][id], 0));
     if ((rc = launch_unpad(c, c->f[id], c->x_out[s][id]))) return rc;

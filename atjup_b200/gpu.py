@@ -342,7 +342,8 @@ class GpuModel:
 
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
-                      "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca")
+                      "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca",
+                      "rk_group")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

@@ -468,10 +468,15 @@ int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t
 
 /* Instrumentation (no reference counterpart: the reference prints wall-clock timers per routine,
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
- * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. */
+ * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. Launches
+ * that run on the library's second stream (the scalar RK stages, coupled precipitation, the moist
+ * convective adjustment) are timed on it, so their times include the share of the GPU that the
+ * concurrent work on the other stream takes. ATJUP_TK_RK_GROUP is one RK stage as a whole (the
+ * scalar and dynamics kernels together), read from those events' first start and last end. */
 enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
        ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_SPECIES,
-       ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_COUNT };
+       ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_RK_GROUP,
+       ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */

@@ -94,3 +94,23 @@ def test_stream_handle_follows_set_stream():
     assert m.stream_handle() not in (0, s.cuda_stream)
     assert m.nonfinite_count() == 0
     m.close()
+
+
+@pytest.mark.gpu
+def test_stage_group_timing():
+    """ATJUP_TK_RK_GROUP: one entry per RK stage, each spanning the stage's scalar kernels (second
+    stream) and its dynamics kernel; so it is at least the longer of the two streams' work and at
+    most their sum, plus the launch gaps between them (50 us per stage allowed)."""
+    P, PH, MC, g, f = synthetic_moist_case(13, 37, 49, seed=64)
+    m = gpu_moist_model(P, PH, MC, g, f)
+    m.timing(True)
+    for it in (1, 2):
+        m.step(it, first=(it == 1))
+    m.synchronize()
+    cls = {n: m.timing_read(i) for i, n in enumerate(m.TIMING_CLASSES)}
+    m.timing(False)
+    m.close()
+    grp_ms, grp_n = cls["rk_group"]
+    assert grp_n == 8 and cls["rk_stage"][1] == 8 and cls["species"][1] == 8 and cls["closure"][1] == 8
+    side = cls["species"][0] + cls["closure"][0]
+    assert max(side, cls["rk_stage"][0]) * 0.999 <= grp_ms <= side + cls["rk_stage"][0] + 8 * 0.05
