@@ -100,6 +100,8 @@ void free_all(AtjupCtx* c) {
         c->side = nullptr;
     }
     solver_free(c);
+    cudaFree(c->lin);
+    c->lin = nullptr;
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
     for (auto& p : c->f2) { cudaFree(p); p = nullptr; }
     for (auto& p : c->fn) { cudaFree(p); p = nullptr; }

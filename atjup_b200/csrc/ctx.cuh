@@ -110,6 +110,7 @@ struct AtjupCtx {
     double* dsum = nullptr;      // [ATJUP_MAX_SOLVE_PARTIALS * 4] dot-product partials
     double* hsum = nullptr;      // pinned host copy of the final dot products
     unsigned long long* counters = nullptr;  // [8] event counters of the last satadj call
+    double* lin = nullptr;       // scratch of the RK4 tangent-linear / adjoint (adjoint.cu)
 
     // static grid
     uint8_t* solid = nullptr;

@@ -42,6 +42,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_destroy.argtypes = [vp]
     L.atjup_gpu_set_stream.argtypes = [vp, vp]
     L.atjup_gpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.atjup_gpu_rk4_tlm.argtypes = [vp, ctypes.POINTER(vp)]
+    L.atjup_gpu_rk4_adjoint.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.atjup_gpu_upload.argtypes = [vp, i32, vp]
     L.atjup_gpu_download.argtypes = [vp, i32, vp]
@@ -272,6 +274,36 @@ class GpuModel:
 
     def set_stream(self, stream_handle: int | None):
         _check(self.L.atjup_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
+
+    def _four(self, tensors):
+        """device pointers of four float64 CUDA tensors of shape (im, jm, pitch), contiguous"""
+        shape = (self.P.im, self.P.jm, self.field_ptr("t")[1])
+        ptrs = (ctypes.c_void_p * 4)()
+        for q, x in enumerate(tensors):
+            if (not x.is_cuda or str(x.dtype) != "torch.float64" or tuple(x.shape) != shape
+                    or not x.is_contiguous()):
+                raise ValueError(f"expected contiguous float64 CUDA tensors of shape {shape}")
+            ptrs[q] = x.data_ptr()
+        return ptrs
+
+    def _on_tensors(self, fn, tensors):
+        # the library issues on its own stream: torch's writes of the inputs must be done before
+        # it reads them, and its results before torch reads them
+        import torch
+        ptrs = self._four(tensors)
+        torch.cuda.current_stream().synchronize()
+        _check(fn(self.ctx, ptrs))
+        self.synchronize()
+
+    def rk4_tlm(self, dt, du, dv, dw):
+        """tangent-linear of one RK4 step of the dry dynamics about the current state, in place
+        on four (im, jm, pitch) float64 CUDA tensors (t, u, v, w)"""
+        self._on_tensors(self.L.atjup_gpu_rk4_tlm, (dt, du, dv, dw))
+
+    def rk4_adjoint(self, at, au, av, aw):
+        """adjoint of one RK4 step of the dry dynamics about the current state, in place: the
+        adjoint of the step's result in, of its input out"""
+        self._on_tensors(self.L.atjup_gpu_rk4_adjoint, (at, au, av, aw))
 
     def stream_handle(self) -> int:
         """the cudaStream_t the context issues its work on, as an integer"""

@@ -466,6 +466,22 @@ int atjup_gpu_save_state(AtjupCtx* ctx, const char* path, int32_t iter, int32_t 
  * first resumed iteration only for a JUP1 file. */
 int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t* carried);
 
+/* Tangent-linear and adjoint of one RK4 step of the dry dynamics: RungeKuttaJup
+ * (RungeKutta_Jup_Turb.cpp:261-583) with the t, u, v, w right-hand sides of RHSJup
+ * (RHS_Jup_Turb.cpp:31-1457), the buoyancy level mean (47-69) and the hydrostatic integral
+ * (119-259), linearised about the context's current t, u, v, w. p_dyn, p_stat, rho_mix, wall_nue
+ * and the cell-hold means are inputs of the step and held fixed; the state is not advanced.
+ * d / a are four device buffers (t, u, v, w) in the context's padded layout (atjup_gpu_field_ptr
+ * gives the row pitch; lanes k >= km are ignored):
+ *   atjup_gpu_rk4_tlm      d in: a perturbation of the time-level-n state; out: the step's
+ *                          response (lanes k >= km set to 0)
+ *   atjup_gpu_rk4_adjoint  a in: the adjoint of the step's result; out: of its input
+ * Dry dynamics in FP64 only (ATJUP_ERR_UNSUPPORTED with the physics block, nue or heating on, or
+ * the mixed step). The adjoint adds with FP64 atomics, so its last bits depend on their order.
+ * (The reference has no derivative code.) */
+int atjup_gpu_rk4_tlm(AtjupCtx* ctx, double* const d[4]);
+int atjup_gpu_rk4_adjoint(AtjupCtx* ctx, double* const a[4]);
+
 /* Instrumentation (no reference counterpart: the reference prints wall-clock timers per routine,
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair
  * on its stream around every kernel launch of a class; atjup_gpu_timing_read sums them. Launches

@@ -363,6 +363,10 @@ def main():
     ap.add_argument("--load-restart", default=None, metavar="DIR:N",
                     help="load DIR/jup_restart_N.bin into the reference's moist model with its "
                          "own load_state and record every restart array as rs_*")
+    ap.add_argument("--rk4-fd", default=None, metavar="NDIR:EPS",
+                    help="central differences of one RungeKuttaJup: for NDIR seeded directions d "
+                         "(tests/adjoint_cases.py), the top level's zonal mean of w after one "
+                         "step from the initial state +- EPS d (t, u, v, w and their n copies)")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
     ap.add_argument("--threads", type=int, default=0)
@@ -434,6 +438,23 @@ def main():
             for n in SPECIES:
                 if n.startswith(gas.lower()):
                     data[f"sat_{gas}_{n}"] = ref.get(n)
+    elif a.rk4_fd:
+        import adjoint_cases as AC
+        ndir, eps = a.rk4_fd.split(":")
+        ndir, eps = int(ndir), float(eps)
+        base = {f: ref.get(f) for f in AC.FIELDS}
+        ref.quiet(ref.L.ref_rk4)
+        data["fd_zm0"] = AC.zonal_mean_top(ref.get("w"))
+        for k in range(ndir):
+            d = AC.direction(k, ref.shape)
+            for sgn, tag in ((1.0, "p"), (-1.0, "m")):
+                for f in AC.FIELDS:
+                    x = base[f] + sgn * eps * d[f]
+                    ref.set(f, x)
+                    ref.set(f + "n", x)
+                ref.quiet(ref.L.ref_rk4)
+                data[f"fd_zm{tag}_{k}"] = AC.zonal_mean_top(ref.get("w"))
+        data["fd_eps"] = np.array(eps)
     elif a.rk4:
         ref.quiet(ref.L.ref_rk4)
         for n in DYN_FIELDS:
