@@ -249,8 +249,9 @@ __global__ void tl_stage_kernel(TlArgs A, LinConst q) {
 struct AdArgs {
     LinPtrs a;
     const double* lYn[4];      // adjoint of the step's result
-    const double* lXn[4];      // adjoint of the next stage input (stages 0-2)
-    double* lX[4];             // adjoint of this stage's input (accumulated)
+    double* lXn[4];            // adjoint of the next stage input (stages 0-2); cleared here
+    double* lX[4];             // adjoint of this stage's input (accumulated; zero on entry)
+    double* lY[4];             // adjoint of the step's input (accumulated)
     double* lph;               // adjoint of p_hydro (accumulated)
     double* lb;                // adjoint of the level means (accumulated)
     int stage;
@@ -275,14 +276,22 @@ __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
     if (k < q.km) {
         const Nbr n = nbr_of(q, i, j, k);
         const uint8_t nbm = A.a.nb[n.c];
+        // every cell: the next stage input is Y + c_in rhs, so its adjoint (complete once the
+        // next stage's scatter is done) adds to the input's; its buffer is then cleared for the
+        // scatter of the stage below (stage 3 has none to read and only clears)
+        double lxn[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int f = 0; f < 4; f++) {
+            if (A.stage < 3) {
+                lxn[f] = A.lXn[f][n.c];
+                A.lY[f][n.c] += lxn[f];
+            }
+            A.lXn[f][n.c] = 0.0;
+        }
         if (nbm & NB_INT) {
             // the adjoint of the cell's right-hand sides: from the final update (dt/6 wgt) and,
             // for stages 0-2, from the next stage input (c_in)
             double lr[4];
-            for (int f = 0; f < 4; f++) {
-                lr[f] = q.dt * (1.0 / 6.0) * A.wgt * A.lYn[f][n.c];
-                if (A.stage < 3) lr[f] += A.c_in * A.lXn[f][n.c];
-            }
+            for (int f = 0; f < 4; f++) lr[f] = q.dt * (1.0 / 6.0) * A.wgt * A.lYn[f][n.c] + A.c_in * lxn[f];
             const double at = lr[0], au = lr[1], av = lr[2], aw = lr[3];
             const GeoIJ& g = A.a.geo[(size_t)i * q.jm + j];
             const Der T = der_of(q, A.a.X[0], n), U = der_of(q, A.a.X[1], n);
@@ -381,16 +390,19 @@ __global__ void add_kernel(double* __restrict__ y, const double* __restrict__ x,
 }
 
 // ---- level mean: per level i, W_i = sum of sin(the_j) over the cells the forward mean counts
-// (fluid, t > 0, finite buoyancy) and, given dt, S_i = sum of sin(the_j) d(b)/dt dt; one block
-// per level in a fixed order (deterministic)
+// (fluid, t > 0, finite buoyancy) and, given dt, S_i = sum of sin(the_j) d(b)/dt dt / W_i, the
+// perturbation of the level mean. Two fixed-order levels (deterministic): LB_PARTS blocks per
+// level over interleaved rows, then one thread per level
+constexpr int LB_PARTS = 16;
+
 __global__ void __launch_bounds__(LB_THREADS)
-lin_level_kernel(const double* __restrict__ t, const double* __restrict__ dt,
-                 const double* __restrict__ p_stat, const uint8_t* __restrict__ solid,
-                 const double* __restrict__ sin_the, double* __restrict__ W, double* __restrict__ S,
-                 int jm, int km, int KP, double g, double rR, double t_ref) {
-    const int i = blockIdx.x;
+lin_level_partial(const double* __restrict__ t, const double* __restrict__ dt,
+                  const double* __restrict__ p_stat, const uint8_t* __restrict__ solid,
+                  const double* __restrict__ sin_the, double* __restrict__ part, int jm, int km,
+                  int KP, double g, double rR, double t_ref) {
+    const int i = blockIdx.y, b = blockIdx.x;
     double s = 0.0, ws = 0.0;
-    for (int j = 0; j < jm; j++) {
+    for (int j = b; j < jm; j += LB_PARTS) {
         const double wgt = sin_the[j];
         const size_t row = ((size_t)i * jm + j) * KP;
         for (int k = threadIdx.x; k < km; k += LB_THREADS) {
@@ -413,9 +425,22 @@ lin_level_kernel(const double* __restrict__ t, const double* __restrict__ dt,
     if (threadIdx.x == 0) {
         double ts = 0.0, tw = 0.0;
         for (int q = 0; q < LB_THREADS / 32; q++) { ts += sh_s[q]; tw += sh_w[q]; }
-        W[i] = tw;
-        S[i] = (tw > 0.0) ? ts / tw : 0.0;     // the perturbation of the level mean
+        part[(i * LB_PARTS + b) * 2 + 0] = ts;
+        part[(i * LB_PARTS + b) * 2 + 1] = tw;
     }
+}
+
+__global__ void lin_level_final(const double* __restrict__ part, double* __restrict__ W,
+                                double* __restrict__ S, int im) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= im) return;
+    double ts = 0.0, tw = 0.0;
+    for (int b = 0; b < LB_PARTS; b++) {
+        ts += part[(i * LB_PARTS + b) * 2 + 0];
+        tw += part[(i * LB_PARTS + b) * 2 + 1];
+    }
+    W[i] = tw;
+    S[i] = (tw > 0.0) ? ts / tw : 0.0;
 }
 
 // the level mean's transpose: lt += lb_i sin(the_j) / W_i d(b)/dt over the counted cells
@@ -503,6 +528,7 @@ struct Lin {
     double* ph;          // tangent or adjoint of p_hydro
     double* ph_save;     // the context's p_hydro, put back after the recompute
     double* lv;          // [4 * im]: W, the level means' tangent or adjoint, the saved means
+    double* part;        // [2 * LB_PARTS * im]: partial sums of the level means
 };
 
 int lin_setup(AtjupCtx* c, Lin& L) {
@@ -521,7 +547,7 @@ int lin_setup(AtjupCtx* c, Lin& L) {
     }
     const size_t NF = 30;
     if (!c->lin) {
-        ATJUP_CUDA(cudaMalloc(&c->lin, sizeof(double) * (NF * c->NP + 4 * (size_t)P.im)));
+        ATJUP_CUDA(cudaMalloc(&c->lin, sizeof(double) * (NF * c->NP + (4 + 2 * LB_PARTS) * (size_t)P.im)));
     }
     double* p = c->lin;
     for (int s = 0; s < 3; s++) for (int f = 0; f < 4; f++) { L.S[s][f] = p; p += c->NP; }
@@ -531,6 +557,7 @@ int lin_setup(AtjupCtx* c, Lin& L) {
     L.ph = p; p += c->NP;
     L.ph_save = p; p += c->NP;
     L.lv = p;
+    L.part = p + 4 * (size_t)P.im;
     return ATJUP_OK;
 }
 
@@ -603,9 +630,11 @@ int atjup_gpu_rk4_tlm(AtjupCtx* c, double* const d[4]) {
     const LinConst q = lin_const(c);
     double* W = L.lv;
     double* db = L.lv + P.im;
-    lin_level_kernel<<<P.im, LB_THREADS, 0, c->stream>>>(
-        c->f[ATJUP_F_T], d[0], c->f[ATJUP_F_P_STAT], c->solid, c->sin_the, W, db, P.jm, P.km,
+    lin_level_partial<<<dim3(LB_PARTS, P.im), LB_THREADS, 0, c->stream>>>(
+        c->f[ATJUP_F_T], d[0], c->f[ATJUP_F_P_STAT], c->solid, c->sin_the, L.part, P.jm, P.km,
         c->KP, q.g, q.rR, q.t_ref);
+    lin_level_final<<<(P.im + 63) / 64, 64, 0, c->stream>>>(L.part, W, db, P.im);
+    c->launches++;
     tl_hydro_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
         c->f[ATJUP_F_V], c->f[ATJUP_F_W], d[2], d[3], c->solid, c->rad, c->cor_col, L.ph, P.im,
         P.jm, P.km, c->KP, P.dr);
@@ -657,16 +686,18 @@ int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
     ATJUP_CUDA(cudaMemsetAsync(lb, 0, sizeof(double) * P.im, c->stream));
     const dim3 grid((P.km + 127) / 128, P.jm, P.im);
     const unsigned nblk = (unsigned)((c->NP + 255) / 256);
+    // stage 3 scatters into A[1]; every later stage's target was cleared by the stage before it
+    for (int f = 0; f < 4; f++) ATJUP_CUDA(cudaMemsetAsync(L.A[1][f], 0, bytes, c->stream));
     for (int s = 3; s >= 0; s--) {
         double* const* cur = L.A[s & 1];
         double* const* nxt = L.A[(s + 1) & 1];
-        for (int f = 0; f < 4; f++) ATJUP_CUDA(cudaMemsetAsync(cur[f], 0, bytes, c->stream));
         AdArgs A{};
         A.a = lin_ptrs(c, L, s);
         for (int f = 0; f < 4; f++) {
             A.lYn[f] = L.B[f];
             A.lXn[f] = nxt[f];
             A.lX[f] = cur[f];
+            A.lY[f] = a[f];
         }
         A.lph = L.ph;
         A.lb = lb;
@@ -674,17 +705,21 @@ int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
         A.c_in = stage_c_in(P, s);
         A.wgt = stage_wgt(s);
         ad_stage_kernel<<<grid, 128, 0, c->stream>>>(A, q);
-        for (int f = 0; f < 4; f++) add_kernel<<<nblk, 256, 0, c->stream>>>(a[f], cur[f], c->NP);
-        c->launches += 5;
+        c->launches++;
         ATJUP_CHECK_LAUNCH("rk4_adjoint: stage");
     }
+    // the adjoint of stage 0's input, which is Y itself
+    for (int f = 0; f < 4; f++) add_kernel<<<nblk, 256, 0, c->stream>>>(a[f], L.A[0][f], c->NP);
+    c->launches += 4;
     // the column integral onto v, w and the level mean onto t
     ad_hydro_kernel<<<dim3((P.km + 127) / 128, P.jm), 128, 0, c->stream>>>(
         c->f[ATJUP_F_V], c->f[ATJUP_F_W], L.ph, c->solid, c->rad, c->cor_col, a[2], a[3], P.im,
         P.jm, P.km, c->KP, P.dr);
-    lin_level_kernel<<<P.im, LB_THREADS, 0, c->stream>>>(
-        c->f[ATJUP_F_T], nullptr, c->f[ATJUP_F_P_STAT], c->solid, c->sin_the, W, L.lv + 2 * P.im,
-        P.jm, P.km, c->KP, q.g, q.rR, q.t_ref);
+    lin_level_partial<<<dim3(LB_PARTS, P.im), LB_THREADS, 0, c->stream>>>(
+        c->f[ATJUP_F_T], nullptr, c->f[ATJUP_F_P_STAT], c->solid, c->sin_the, L.part, P.jm, P.km,
+        c->KP, q.g, q.rR, q.t_ref);
+    lin_level_final<<<(P.im + 63) / 64, 64, 0, c->stream>>>(L.part, W, L.lv + 2 * P.im, P.im);
+    c->launches++;
     ad_level_kernel<<<grid, 128, 0, c->stream>>>(c->f[ATJUP_F_T], c->f[ATJUP_F_P_STAT], c->solid,
                                                  c->sin_the, W, lb, a[0], P.jm, P.km, c->KP, q.g,
                                                  q.rR, q.t_ref);

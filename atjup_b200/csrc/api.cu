@@ -255,6 +255,14 @@ int atjup_gpu_set_stream(AtjupCtx* c, void* stream) {
     return ATJUP_OK;
 }
 
+int atjup_gpu_copy_field(AtjupCtx* c, int32_t id, double* buf, int32_t to_field) {
+    if (!c || !buf || !valid_field(id)) { set_error("copy_field: bad argument"); return ATJUP_ERR_ARG; }
+    const size_t bytes = sizeof(double) * c->NP;
+    if (to_field) ATJUP_CUDA(cudaMemcpyAsync(c->f[id], buf, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    else ATJUP_CUDA(cudaMemcpyAsync(buf, c->f[id], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return ATJUP_OK;
+}
+
 int atjup_gpu_stream(AtjupCtx* c, void** stream) {
     if (!c || !stream) { set_error("stream: null argument"); return ATJUP_ERR_ARG; }
     *stream = (void*)c->stream;

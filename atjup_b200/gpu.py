@@ -43,6 +43,7 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_set_stream.argtypes = [vp, vp]
     L.atjup_gpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_rk4_tlm.argtypes = [vp, ctypes.POINTER(vp)]
+    L.atjup_gpu_copy_field.argtypes = [vp, i32, vp, i32]
     L.atjup_gpu_rk4_adjoint.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.atjup_gpu_upload.argtypes = [vp, i32, vp]
@@ -275,10 +276,10 @@ class GpuModel:
     def set_stream(self, stream_handle: int | None):
         _check(self.L.atjup_gpu_set_stream(self.ctx, ctypes.c_void_p(stream_handle or 0)))
 
-    def _four(self, tensors):
-        """device pointers of four float64 CUDA tensors of shape (im, jm, pitch), contiguous"""
+    def _ptrs(self, tensors):
+        """device pointers of float64 CUDA tensors of shape (im, jm, pitch), contiguous"""
         shape = (self.P.im, self.P.jm, self.field_ptr("t")[1])
-        ptrs = (ctypes.c_void_p * 4)()
+        ptrs = (ctypes.c_void_p * len(tensors))()
         for q, x in enumerate(tensors):
             if (not x.is_cuda or str(x.dtype) != "torch.float64" or tuple(x.shape) != shape
                     or not x.is_contiguous()):
@@ -286,11 +287,35 @@ class GpuModel:
             ptrs[q] = x.data_ptr()
         return ptrs
 
+    def set_state_tensors(self, tensors, names=("t", "u", "v", "w"), wait=True):
+        """copy (im, jm, pitch) float64 CUDA tensors into the named fields; with wait False the
+        call returns once the copies are queued (the library's later work is ordered after them,
+        but the tensors must not be rewritten before the next synchronize)"""
+        import torch
+        ptrs = self._ptrs(tensors)
+        torch.cuda.current_stream().synchronize()
+        for q, n in enumerate(names):
+            _check(self.L.atjup_gpu_copy_field(self.ctx, _p.FIELD_IDS[n], ptrs[q], 1))
+        if wait:
+            self.synchronize()
+
+    def state_tensors(self, names=("t", "u", "v", "w")):
+        """the named fields as new (im, jm, pitch) float64 CUDA tensors"""
+        import torch
+        out = [torch.empty((self.P.im, self.P.jm, self.field_ptr("t")[1]), dtype=torch.float64,
+                           device="cuda") for _ in names]
+        ptrs = self._ptrs(out)
+        torch.cuda.current_stream().synchronize()
+        for q, n in enumerate(names):
+            _check(self.L.atjup_gpu_copy_field(self.ctx, _p.FIELD_IDS[n], ptrs[q], 0))
+        self.synchronize()
+        return out
+
     def _on_tensors(self, fn, tensors):
         # the library issues on its own stream: torch's writes of the inputs must be done before
         # it reads them, and its results before torch reads them
         import torch
-        ptrs = self._four(tensors)
+        ptrs = self._ptrs(tensors)
         torch.cuda.current_stream().synchronize()
         _check(fn(self.ctx, ptrs))
         self.synchronize()

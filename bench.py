@@ -273,6 +273,82 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_adjoint(args):
+    """K dry RK4 steps forward and their adjoint through the torch.autograd binding (each step
+    keeps its input as the checkpoint and the adjoint recomputes its stages), on the 41x181x361
+    shell: the time of forward with checkpoints + backward over the time of K plain forward steps,
+    and the device memory the chain holds. One GPU."""
+    import numpy as np
+    import torch
+
+    from atjup_b200 import synthetic
+    from atjup_b200.autograd import rk4_steps
+    from atjup_b200.gpu import GpuModel
+    from atjup_b200.params import resolve_params
+
+    K = args.steps
+    P = resolve_params(DRY_ENV, im=IM, jm=JM, km=KM)
+    s = synthetic.state(IM, JM, KM, seed=20261203)
+    grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
+    m = GpuModel(P, grid)
+    m.upload_state({k: v for k, v in s.items() if k not in grid})
+    y0 = m.state_tensors()
+    stream = torch.cuda.ExternalStream(m.stream_handle())
+    the = torch.tensor(grid["the"], device="cuda")
+    a = np.random.Generator(np.random.Philox(key=20261204)).uniform(-50.0, 150.0, 8) / P.u_0
+    uref = sum(float(a[n - 1]) * torch.sin(n * the) for n in range(1, 9))
+
+    def forward_plain():
+        m.set_state_tensors(y0)
+        for _ in range(K):
+            m.runge_kutta()
+
+    def chain():
+        x = [t.clone().requires_grad_() for t in y0]
+        out = rk4_steps(m, *x, steps=K)
+        zm = out[3][IM - 2, :, : KM - 1].mean(dim=1)
+        J = (torch.sin(the) * (zm - uref) ** 2).sum()
+        J.backward()
+        return J
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, e0.elapsed_time(e1) / 1e3
+
+    for _ in range(2):                      # warm-up: library scratch, torch allocator
+        forward_plain()
+        chain()
+    fwd_wall, fwd_dev = timed(forward_plain)
+    torch.cuda.reset_peak_memory_stats()
+    free0 = torch.cuda.mem_get_info()[0]
+    ad_wall, _ = timed(chain)
+    torch_peak = torch.cuda.max_memory_allocated()
+    lib_scratch = 30 * IM * JM * m.field_ptr("t")[1] * 8
+    m.close()
+    line = {
+        "metric": f"adjoint+forward / forward time, {K} dry RK4 steps (41x181x361, FP64)",
+        "value": ad_wall / fwd_wall, "unit": "x", "n_gpus": 1, "steps": K, "warmup": 2,
+        "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded dry state)",
+        "config": {"workload": "rk4-adjoint: K RK4 steps of the dry dynamics through "
+                               "atjup_b200.autograd.RK4Step, loss = sin-weighted squared error of "
+                               "the top level's zonal-mean w against a seeded 8-mode jet",
+                   "grid": "41x181x361", "checkpoints": "each step's input (t, u, v, w)"},
+        "forward_ms_per_step": fwd_wall / K * 1e3,
+        "forward_device_ms_per_step": fwd_dev / K * 1e3,
+        "adjoint_and_forward_ms_per_step": ad_wall / K * 1e3,
+        "peak_bytes": {"torch_tensors": torch_peak, "library_scratch": lib_scratch,
+                       "device_free_at_start": free0},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -280,7 +356,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="phys", choices=["phys", "dry"])
+    ap.add_argument("--workload", default="phys", choices=["phys", "dry", "rk4-adjoint"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None,
                     help="IMxJMxKM of a smaller shell, for profiling only (the metric is quoted "
@@ -293,6 +369,9 @@ def main():
         run_reference(args, rank, world)
         return
     args.warmup = max(args.warmup, 3)
+    if args.workload == "rk4-adjoint":
+        run_adjoint(args)
+        return
 
     import numpy as np
     import torch

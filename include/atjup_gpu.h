@@ -481,6 +481,11 @@ int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t
  * (The reference has no derivative code.) */
 int atjup_gpu_rk4_tlm(AtjupCtx* ctx, double* const d[4]);
 int atjup_gpu_rk4_adjoint(AtjupCtx* ctx, double* const a[4]);
+/* Device-to-device copy between a field and a caller's device buffer in the padded layout
+ * (im * jm * pitch doubles), in the context's stream order: to_field 1 copies buf into the field,
+ * 0 the field into buf. For callers that hold the state in their own device tensors (the torch
+ * binding of the RK4 step). (No reference counterpart.) */
+int atjup_gpu_copy_field(AtjupCtx* ctx, int32_t field_id, double* buf, int32_t to_field);
 
 /* Instrumentation (no reference counterpart: the reference prints wall-clock timers per routine,
  * e.g. RungeKutta_Jup_Turb.cpp:577-579). With timing on, the library records a CUDA event pair

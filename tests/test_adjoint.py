@@ -10,7 +10,7 @@ buoyancy level mean and the hydrostatic integral, linearised about the current s
   from the adjoint, against central differences (eps = 1e-6) of the reference's own
   RungeKuttaJup (oracle/_ref) on its dry initial state, along 16 seeded directions: each
   directional derivative within 1e-6 relative plus the central difference's own rounding,
-  100 ulp of J over 2 eps (measured: within 1e-7 relative, 2e-8 absolute, on derivatives of
+  10 ulp of J over 2 eps (measured: within 1e-7 relative, 2e-8 absolute, on derivatives of
   order 1; the reference's central differences equal the GPU's to 12 digits).
 """
 import numpy as np
@@ -119,7 +119,7 @@ def test_adjoint_gradient_matches_reference_differences(ref_required):
     lam["w"] = AC.loss_adjoint_w(y1["w"], the, uref)
     grad = adjoint(m, lam)
     j0 = AC.loss(y1["w"], the, uref)
-    floor = 100.0 * np.finfo(float).eps * abs(j0) / (2.0 * EPS)
+    floor = 10.0 * np.finfo(float).eps * abs(j0) / (2.0 * EPS)
     worst = 0.0
     for k in range(NDIR):
         dk = AC.direction(k, m.shape)
@@ -160,3 +160,40 @@ def test_refused_outside_the_dry_fp64_step():
     with pytest.raises(AtjupError):
         m.rk4_tlm(*x)
     m.close()
+
+
+def test_autograd_three_steps_match_differences():
+    """Three RK4 steps through the torch.autograd binding (atjup_b200.autograd.RK4Step, each step
+    its own checkpoint) and the loss of the last step's w: the gradient along a seeded direction
+    against central differences of three GPU steps, within 1e-6 relative plus the rounding floor."""
+    import torch
+    from atjup_b200.autograd import rk4_steps
+    p, g, f = synthetic_case(41, 61, 97, seed=74)
+    m = gpu_from(p, g, f)
+    im, jm, km = m.shape
+    the = g["the"]
+    uref = AC.u_ref(the, p.u_0)
+    y0 = {n: m.download(n) for n in AC.FIELDS}
+    x = [t.requires_grad_() for t in padded(m, [y0[n] for n in AC.FIELDS])]
+    out = rk4_steps(m, *x, steps=3)
+    zm = out[3][im - 2, :, : km - 1].mean(dim=1)
+    th = torch.tensor(the, device="cuda")
+    ur = torch.tensor(uref, device="cuda")
+    J = (torch.sin(th) * (zm - ur) ** 2).sum()
+    J.backward()
+    grad = {n: x[q].grad[:, :, :km].cpu().numpy() for q, n in enumerate(AC.FIELDS)}
+    d = AC.direction(11, m.shape)
+
+    def J_of(sign):
+        y = {n: y0[n] + sign * EPS * d[n] for n in AC.FIELDS}
+        for _ in range(3):
+            y = rk4_from(m, y)
+        return AC.loss(y["w"], the, uref)
+
+    ad = dot(grad, d)
+    fd = (J_of(1.0) - J_of(-1.0)) / (2.0 * EPS)
+    m.close()
+    floor = 10.0 * np.finfo(float).eps * abs(float(J)) / (2.0 * EPS)
+    print(f"autograd, 3 steps: adjoint {ad:.12e}  central difference {fd:.12e}  "
+          f"rel {abs(ad - fd) / abs(fd):.2e}  floor {floor:.1e}")
+    assert abs(ad - fd) <= 1e-6 * abs(fd) + floor
