@@ -82,7 +82,7 @@ CONFIGS = {
         "parallelism": "replicas (the path does not shard)",
     },
     "dry": {
-        "workload": "dry dynamics iteration on the 41x181x361 shell (BASELINE config 0 knobs): "
+        "workload": "dry dynamics iteration on the 41x181x361 shell (dry knobs: obstacle on, no physics, 4th-order in-loop Shapiro): "
                     "pressure red-black pass on even iterations, RK4 (4 stages), BCs, 4th-order "
                     "Shapiro on u,v,w, column balance of v",
         "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",

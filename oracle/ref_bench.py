@@ -1,6 +1,6 @@
 """Time the reference's own CPU implementation of one model iteration (dry or full physics).
 
-TEST / BASELINE INFRASTRUCTURE: used only by bench.py's CPU legs (the reference arm and the
+TEST AND CPU-BASELINE INFRASTRUCTURE: used only by bench.py's CPU legs (the reference arm and the
 cpu_baseline figure). Runs oracle/_ref/libatjup_ref.so -- the unmodified reference built from its
 sources -- in this process: the reference's initialisation (untimed), `warmup` iterations
 (untimed), then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule -- the dry

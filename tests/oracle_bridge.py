@@ -16,7 +16,7 @@ ORACLE_SO = ROOT / "oracle" / "liboracle.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libatjup_ref.so"
 
 # The dry configuration: obstacle on, microphysics / radiation / turbulence / MCA / cone
-# projection off, in-loop 4th-order Shapiro on u, v, w (BASELINE config 0 knobs).
+# projection off, in-loop 4th-order Shapiro on u, v, w (the dry configuration's knobs).
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
     "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",

@@ -108,7 +108,7 @@ def test_full_grid_rk4_reference_state(ref_required):
 
 @pytest.mark.slow
 def test_full_grid_20_dry_iterations(ref_required):
-    """20 dry iterations, GPU FP64 vs the reference <= 1e-10 per field."""
+    """The dry configuration: 20 iterations, GPU FP64 vs the reference <= 1e-10 per field."""
     d = ref_dump("--iters", "20")
     p, g, f = dump_params(d), dump_grid(d), dump_fields(d)
     m = gpu_from(p, g, f)

@@ -56,7 +56,8 @@ def test_residual_solve_small(shape, prec):
 @pytest.mark.slow
 @pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED], ids=["fp64", "mixed"])
 def test_residual_solve_full_grid(prec):
-    """BASELINE config 1 on the 41x181x361 shell with the obstacle, to 1e-10."""
+    """The isolated Poisson solve (seeded smoothed right-hand side) on the 41x181x361 shell with the
+    obstacle, to 1e-10."""
     p, g, f = synthetic_case(41, 181, 361)
     b = synthetic.poisson_rhs(41, 181, 361)
     o = oracle_from(p, g, f)
