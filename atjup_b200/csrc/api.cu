@@ -638,6 +638,7 @@ int micro_call(AtjupCtx* c, int what, const char* name) {
 int atjup_gpu_radiation(AtjupCtx* c) { return micro_call(c, MICRO_RADIATION, "radiation"); }
 int atjup_gpu_precipitation(AtjupCtx* c) { return micro_call(c, MICRO_PRECIP, "precipitation"); }
 int atjup_gpu_nh4sh_equilibrium(AtjupCtx* c) { return micro_call(c, MICRO_NH4SH, "nh4sh_equilibrium"); }
+int atjup_gpu_diagnostics(AtjupCtx* c) { return micro_call(c, MICRO_DIAG, "diagnostics"); }
 int atjup_gpu_chemistry(AtjupCtx* c) { return micro_call(c, MICRO_CHEMISTRY, "chemistry"); }
 int atjup_gpu_clamp_species(AtjupCtx* c) { return micro_call(c, MICRO_CLAMP, "clamp_species"); }
 
@@ -855,6 +856,8 @@ int physics_block(AtjupCtx* c) {
     if (c->phys.turb_on && (rc = atjup_gpu_turbulence(c))) return rc;
     if (c->micro_on && (rc = atjup_gpu_chemistry(c))) return rc;
     if (side_precip && (rc = join_side(c))) return rc;
+    // Forces and Latent_Heat close the block (cJupiterModel.cpp:1163-1164): outputs only
+    if (c->micro_on && mc.diagnostics_on && (rc = atjup_gpu_diagnostics(c))) return rc;
     return ATJUP_OK;
 }
 }  // namespace

@@ -190,7 +190,7 @@ extern const int kScalarField[ATJUP_S_COUNT + 2];
 int launch_phys_stage(AtjupCtx* c, int stage, const void* const* vin, int what, cudaStream_t st);
 int launch_turbulence(AtjupCtx* c);
 int launch_turb_wall_hold(AtjupCtx* c);
-enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP };
+enum { MICRO_RADIATION = 0, MICRO_PRECIP, MICRO_NH4SH, MICRO_CHEMISTRY, MICRO_CLAMP, MICRO_DIAG };
 int launch_micro(AtjupCtx* c, int what);
 int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStats* st);
 void solver_free(AtjupCtx* c);

@@ -8,6 +8,8 @@
 //   massflux_kernel       ChemMassRateJup: reaction rate + diffusive flux (ChemistryJup.h:59-281)
 //   fluxlim_kernel        FluxLimiter<cJupiterModel>::nh4sh (FluxLimiter.h)
 //   clamp_species_kernel  clampNegativeSpecies (FileIO_Jup.cpp:494-548)
+//   diagnostics_kernel    cJupiterModel::Forces (InitValues_Jup.cpp:742-812) and Latent_Heat
+//                         (Thermo_Jup.cpp:89-232): output fields only
 //
 // Radiation and precipitation are vertical sweeps through a column (the thermal fluxes down then
 // up, the falling hydrometeor fluxes top-down), so each is one thread per (j, k) column, k fastest
@@ -460,6 +462,124 @@ __global__ void clamp_species_kernel(MicroArgs a) {
         if (!(a.q[s][c] >= 0.0)) a.q[s][c] = 0.0;
 }
 
+// The output diagnostics: the force densities of Forces and the latent and sensible heating of
+// Latent_Heat. One thread per cell; both routines fill i 1..im-2, j 1..jm-2 and the phi ring
+// k 0..km-2, Latent_Heat also zeroes its fields at i = 0; other cells keep their values. The
+// sine and cosine of the colatitude are the host's (the reference's sin and cos of the.z), and
+// every expression keeps the reference's operand order (this file has no FMA contraction), so
+// only CUDA's exp differs in its last bit; it feeds the saturation tests of Latent_Heat.
+struct DiagArgs {
+    const double *t, *u, *v, *w, *p_dyn, *p_stat, *h2o, *nh3;
+    const uint8_t* solid;
+    const double *rad, *sin_the;
+    const GeoIJ* geo;
+    double *cor, *cen, *buo, *pgf, *ql, *qs;
+    double cc[8];
+    double ep_w, lv_w, ls_w, ep_a, lv_a, ls_a, fix_lat, fix_sen;
+    double omega, Coriolis, centrifugal, buoyancy, r_mix, R_mix, g, t_ref, p_dyn_to_bar, L_atm;
+    double u_0, cp_mix, dr, dthe, dphi;
+    int im, jm, km, KP, costhe_abs;
+};
+
+__global__ void diagnostics_kernel(DiagArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
+    if (k >= a.km) return;
+    const size_t plane = (size_t)a.jm * a.KP, row = ((size_t)i * a.jm + j) * a.KP, c = row + k;
+    if (i == 0) {
+        a.ql[c] = 0.0;
+        a.qs[c] = 0.0;
+        return;
+    }
+    if (i > a.im - 2 || j < 1 || j > a.jm - 2 || k > a.km - 2) return;
+    const int ke = (k >= a.km - 2) ? 0 : k + 1, kw = (k == 0) ? a.km - 2 : k - 1;
+    const size_t cp = c + plane, cm = c - plane, cjp = c + a.KP, cjm = c - a.KP;
+    const size_t ckp = row + ke, ckm = row + kw;
+    const double rm = a.rad[i];
+    const double sinthe = a.sin_the[j];
+    double costhe = a.geo[(size_t)i * a.jm + j].costhe;
+    if (a.costhe_abs && j > 90) costhe = -costhe;
+    const double rmsinthe = rm * sinthe;
+    // Forces
+    const double omega = a.omega;
+    const double Cor_r = -2.0 * omega * sinthe * a.w[c];
+    const double Cor_the = +2.0 * omega * costhe * a.w[c];
+    const double Cor_phi = +2.0 * omega * (-costhe * a.v[c] + sinthe * a.u[c]);
+    const double dpdr = (a.p_dyn[cp] - a.p_dyn[cm]) / (2.0 * a.dr);
+    const double dpdthe = (a.p_dyn[cjp] - a.p_dyn[cjm]) / (2.0 * a.dthe);
+    const double dpdphi = (a.p_dyn[ckp] - a.p_dyn[ckm]) / (2.0 * a.dphi);
+    a.cor[c] = a.Coriolis * a.r_mix * sqrt((Cor_r * Cor_r + Cor_the * Cor_the + Cor_phi * Cor_phi) / 3.0);
+    a.cen[c] = a.centrifugal * a.r_mix * omega * omega * rm * (1.0 + fabs(sinthe));
+    const double tc = a.t[c];
+    a.buo[c] = (tc > 0.0) ? a.buoyancy * a.r_mix * a.g * (a.p_stat[c] + a.p_dyn[c] * a.p_dyn_to_bar) /
+                                (a.r_mix * a.R_mix * tc * a.t_ref) * 1e5
+                          : 0.0;
+    const double gth = dpdthe / rm, gph = dpdphi / rmsinthe;
+    a.pgf[c] = -sqrt((dpdr * dpdr + gth * gth + gph * gph) / 3.0) * a.p_dyn_to_bar * 1.0e5 /
+               (a.L_atm * 1.0e3);
+    // Latent_Heat
+    const double t_u = tc * a.t_ref;
+    const double p_u = a.p_stat[c];
+    const double E_Rain = exp(a.cc[0] / t_u + a.cc[1]);
+    const double E_Ice = exp(a.cc[2] / t_u + a.cc[3]);
+    const double q_Rain = a.ep_w * E_Rain / dmax(p_u - E_Rain, 1.0e-12);
+    const double q_Ice = a.ep_w * E_Ice / dmax(p_u - E_Ice, 1.0e-12);
+    const double E_Rain_nh3 = exp(a.cc[4] / t_u + a.cc[5]);
+    const double E_Ice_nh3 = exp(a.cc[6] / t_u + a.cc[7]);
+    const double q_Rain_nh3 = a.ep_a * E_Rain_nh3 / dmax(p_u - E_Rain_nh3, 1.0e-12);
+    const double q_Ice_nh3 = a.ep_a * E_Ice_nh3 / dmax(p_u - E_Ice_nh3, 1.0e-12);
+    const double u_av = 0.5 * (a.u[cp] + a.u[cm]);
+    const double v_av = 0.5 * (a.v[cp] + a.v[cm]);
+    const double w_av = 0.5 * (a.w[cp] + a.w[cm]);
+    const double velocity_av = -sqrt((u_av * u_av + v_av * v_av + w_av * w_av) / 3.0);
+    const double dtdr = (a.t[cp] - a.t[cm]) / (2.0 * a.dr) * 1.0;
+    const double dtdthe = (a.t[cjp] - a.t[cjm]) / (2.0 * rm * a.dthe);
+    const double dtdphi = (a.t[ckp] - a.t[ckm]) / (2.0 * rmsinthe * a.dphi);
+    const double dh2odr = (a.h2o[cp] - a.h2o[cm]) / (2.0 * a.dr) * 1.0;
+    const double dh2odthe = (a.h2o[cjp] - a.h2o[cjm]) / (2.0 * rm * a.dthe);
+    const double dh2odphi = (a.h2o[ckp] - a.h2o[ckm]) / (2.0 * rmsinthe * a.dphi);
+    const double dnh3dr = (a.nh3[cp] - a.nh3[cm]) / (2.0 * a.dr) * 1.0;
+    const double dnh3dthe = (a.nh3[cjp] - a.nh3[cjm]) / (2.0 * rm * a.dthe);
+    const double dnh3dphi = (a.nh3[ckp] - a.nh3[ckm]) / (2.0 * rmsinthe * a.dphi);
+    const double dtemp = dtdr + dtdthe + dtdphi;
+    const double dh2o = dh2odr + dh2odthe + dh2odphi;
+    const double dnh3 = dnh3dr + dnh3dthe + dnh3dphi;
+    const double Lr = a.L_atm * (a.im - 1);
+    const double h = a.h2o[c], nn = a.nh3[c];
+    double ql = (h >= q_Rain) ? a.lv_w * velocity_av * dh2o * a.u_0 / Lr * a.fix_lat : 0.0;
+    double ice = (h >= q_Ice) ? a.ls_w * velocity_av * dh2o * a.u_0 / Lr * a.fix_lat : 0.0;
+    if (nn >= q_Rain_nh3) ql = ql + a.lv_a * velocity_av * dnh3 * a.u_0 / Lr * a.fix_lat;
+    if (nn >= q_Ice_nh3) ice = ice + a.ls_a * velocity_av * dnh3 * a.u_0 / Lr * a.fix_lat;
+    ql = ql + ice;
+    double qs = a.r_mix * a.cp_mix * velocity_av * a.u_0 * dtemp * a.t_ref / (Lr * Lr) * a.fix_sen;
+    if (a.solid[c] == 1) { ql = 0.0; qs = 0.0; }
+    a.ql[c] = ql;
+    a.qs[c] = qs;
+}
+
+DiagArgs diag_args(AtjupCtx* c) {
+    const AtjupParams& P = c->P;
+    const AtjupMicro& mc = c->micro;
+    DiagArgs a{};
+    a.t = c->f[ATJUP_F_T]; a.u = c->f[ATJUP_F_U]; a.v = c->f[ATJUP_F_V]; a.w = c->f[ATJUP_F_W];
+    a.p_dyn = c->f[ATJUP_F_P_DYN]; a.p_stat = c->f[ATJUP_F_P_STAT];
+    a.h2o = c->f[ATJUP_F_H2O]; a.nh3 = c->f[ATJUP_F_NH3];
+    a.solid = c->solid; a.rad = c->rad; a.sin_the = c->sin_the; a.geo = c->geo;
+    a.cor = c->f[ATJUP_F_CORIOLIS_FORCE]; a.cen = c->f[ATJUP_F_CENTRIFUGAL_FORCE];
+    a.buo = c->f[ATJUP_F_BUOYANCY_FORCE]; a.pgf = c->f[ATJUP_F_PRESGRAD_FORCE];
+    a.ql = c->f[ATJUP_F_Q_LATENT]; a.qs = c->f[ATJUP_F_Q_SENSIBLE];
+    for (int q = 0; q < 8; q++) a.cc[q] = mc.cc[q];
+    a.ep_w = mc.gas[ATJUP_GAS_H2O].ep; a.lv_w = mc.gas[ATJUP_GAS_H2O].lv; a.ls_w = mc.gas[ATJUP_GAS_H2O].ls;
+    a.ep_a = mc.gas[ATJUP_GAS_NH3].ep; a.lv_a = mc.gas[ATJUP_GAS_NH3].lv; a.ls_a = mc.gas[ATJUP_GAS_NH3].ls;
+    a.fix_lat = mc.qheat_scale ? (P.im - 1) / 1.0e3 : 1.0;
+    a.fix_sen = mc.qheat_scale ? P.L_atm * (P.im - 1) * (P.im - 1) / 1.0e3 : 1.0;
+    a.omega = P.omega; a.Coriolis = P.Coriolis; a.centrifugal = P.centrifugal;
+    a.buoyancy = P.buoyancy; a.r_mix = P.r_mix; a.R_mix = P.R_mix; a.g = P.g; a.t_ref = P.t_ref;
+    a.p_dyn_to_bar = P.p_dyn_to_bar; a.L_atm = P.L_atm; a.u_0 = P.u_0; a.cp_mix = P.cp_mix;
+    a.dr = P.dr; a.dthe = P.dthe; a.dphi = P.dphi;
+    a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP; a.costhe_abs = mc.costhe_abs;
+    return a;
+}
+
 MicroArgs make_args(AtjupCtx* c) {
     const AtjupParams& P = c->P;
     MicroArgs a{};
@@ -540,6 +660,10 @@ int launch_micro(AtjupCtx* c, int what) {
     }
     case MICRO_CLAMP:
         clamp_species_kernel<<<gcell, TB, 0, c->stream>>>(a);
+        c->launches++;
+        break;
+    case MICRO_DIAG:
+        diagnostics_kernel<<<gcell, TB, 0, c->stream>>>(diag_args(c));
         c->launches++;
         break;
     default:

@@ -81,7 +81,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_mca.argtypes = [vp, ctypes.POINTER(_p.AtjupMcaStats)]
     L.atjup_gpu_save_state.argtypes = [vp, ctypes.c_char_p, i32, i32]
     L.atjup_gpu_load_state.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i32)]
-    for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species"):
+    for n in ("radiation", "precipitation", "nh4sh_equilibrium", "chemistry", "clamp_species",
+              "diagnostics"):
         getattr(L, "atjup_gpu_" + n).argtypes = [vp]
     L.atjup_gpu_download2d.argtypes = [vp, i32, vp]
     _lib = L
@@ -241,6 +242,11 @@ class GpuModel:
     def precipitation(self) -> None:
         """Precipitation<cJupiterModel>::run (Precipitation.h:191-445)."""
         _check(self.L.atjup_gpu_precipitation(self.ctx))
+
+    def diagnostics(self) -> None:
+        """cJupiterModel::Forces and Latent_Heat: the force densities and the latent and sensible
+        heating (output fields)"""
+        _check(self.L.atjup_gpu_diagnostics(self.ctx))
 
     def nh4sh_eq(self) -> None:
         """ChemistryJup::EquilibriumNH4SH("loop") (ChemistryJup.h:291-373)."""

@@ -25,7 +25,9 @@ F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, 
     F_S_PRECIP_NH3, F_S_PRECIP_NH3_CLOUD, F_S_PRECIP_NH3_ICE, \
     F_S_PRECIP_CH4, F_S_PRECIP_CH4_CLOUD, F_S_PRECIP_CH4_ICE, \
     F_MASSFLUX_H2S, F_MASSFLUX_NH3, F_MASSFLUX_NH4SH, F_FLUXLIM_NH4SH, \
-    F_PROD, F_TKE_SOURCE, F_DIS_SOURCE, F_DIFFLUX_H2S, F_DIFFLUX_NH3, F_DIFFLUX_NH4SH = range(48)
+    F_PROD, F_TKE_SOURCE, F_DIS_SOURCE, F_DIFFLUX_H2S, F_DIFFLUX_NH3, F_DIFFLUX_NH4SH, \
+    F_CORIOLIS_FORCE, F_CENTRIFUGAL_FORCE, F_BUOYANCY_FORCE, F_PRESGRAD_FORCE, F_Q_LATENT, \
+    F_Q_SENSIBLE = range(54)
 F2_VEL_STAR = 0
 FIELD_IDS = {
     "t": F_T, "u": F_U, "v": F_V, "w": F_W, "p_dyn": F_P_DYN, "p_hydro": F_P_HYDRO,
@@ -45,7 +47,13 @@ FIELD_IDS = {
     "massflux_nh4sh": F_MASSFLUX_NH4SH, "fluxlim_nh4sh": F_FLUXLIM_NH4SH,
     "prod": F_PROD, "tke_source": F_TKE_SOURCE, "dis_source": F_DIS_SOURCE,
     "difflux_h2s": F_DIFFLUX_H2S, "difflux_nh3": F_DIFFLUX_NH3, "difflux_nh4sh": F_DIFFLUX_NH4SH,
+    "CoriolisForce": F_CORIOLIS_FORCE, "CentrifugalForce": F_CENTRIFUGAL_FORCE,
+    "BuoyancyForce": F_BUOYANCY_FORCE, "PresGradForce": F_PRESGRAD_FORCE,
+    "Q_Latent": F_Q_LATENT, "Q_Sensible": F_Q_SENSIBLE,
 }
+# the output diagnostics of Forces and Latent_Heat
+DIAGNOSTICS = ("CoriolisForce", "CentrifugalForce", "BuoyancyForce", "PresGradForce", "Q_Latent",
+               "Q_Sensible")
 
 # transported scalars in the order of the physics block (ATJUP_S_*), and the fields whose
 # time-level-n copies the RK step keeps (the species, then k*, omega*)
@@ -185,13 +193,15 @@ def resolve_physics(env: Mapping[str, str] | None = None, constants: Mapping[str
 class AtjupMicro(ctypes.Structure):
     """Mirror of AtjupMicro (the loop's radiation, precipitation and chemistry)."""
     _fields_ = [(n, ctypes.c_int32) for n in ("radiation_on", "precip_on", "nh4sh_eq", "satadj_on",
-                                               "solar_on", "rad_bottom", "precip_coupling_on", "pad")] + [
+                                               "solar_on", "rad_bottom", "precip_coupling_on",
+                                               "diagnostics_on", "costhe_abs", "qheat_scale",
+                                               "pad")] + [
         (n, ctypes.c_double) for n in ("F_int", "S_solar", "albedo_bond", "x_H2", "x_He",
                                        "cia_strength", "opacity_strength", "solar_strength",
                                        "sw_tau_per_bar", "precip_rate_scale", "m_nh3", "m_h2s",
                                        "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh",
                                        "polar_divisor_floor", "t_0_nh4sh", "t_00_nh4sh")] + [
-        ("gas", AtjupGasParams * 3)]
+        ("cc", ctypes.c_double * 8), ("gas", AtjupGasParams * 3)]
 
 
 # cJupiterModel's radiation constants (cJupiterModel.h:1109-1118), molar masses (255-270) and the
@@ -201,7 +211,13 @@ DEFAULT_MICRO = {"F_int": 5.4, "S_solar": 50.5, "albedo_bond": 0.343, "x_H2": 0.
                  "x_He": 0.134, "m_nh3": 17.03052, "m_h2s": 34.08088, "m_nh4sh": 51.1114,
                  "D_nh3": 0.92e-5 / (817.0 * 0.61), "D_h2s": 1.3e-5 / (949.0 * 0.94),
                  "D_nh4sh": 0.0, "polar_divisor_floor": 0.4, "t_0_nh4sh": 230.0,
-                 "t_00_nh4sh": 200.0}
+                 "t_00_nh4sh": 200.0,
+                 # Latent_Heat's Clausius-Clapeyron pairs (cJupiterModel.h:222-240)
+                 "coeff_h2o_A": -4961.04, "coeff_h2o_B": 13.0662, "coeff_h2o_A_i": -4961.04,
+                 "coeff_h2o_B_i": 13.0662, "coeff_nh3_A": -2836.56, "coeff_nh3_B": 11.7271,
+                 "coeff_nh3_A_i": -2836.56, "coeff_nh3_B_i": 11.7271}
+CC_NAMES = ("coeff_h2o_A", "coeff_h2o_B", "coeff_h2o_A_i", "coeff_h2o_B_i", "coeff_nh3_A",
+            "coeff_nh3_B", "coeff_nh3_A_i", "coeff_nh3_B_i")
 
 
 def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, float] | None = None,
@@ -209,7 +225,8 @@ def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, 
     """Microphysics block from the environment with the reference's defaults (ATJUP_RADIATION 1,
     ATJUP_PRECIP 1, ATJUP_NH4SH_EQ 1, ATJUP_SOLAR 1, ATJUP_RAD_BOTTOM 0, ATJUP_PRECIP_COUPLING 1,
     ATJUP_CIA_STRENGTH 3.9, ATJUP_OPACITY_STRENGTH 1, ATJUP_SOLAR_STRENGTH 1,
-    ATJUP_SW_TAU_PER_BAR 1, ATJUP_PRECIP_SCALE 1); constants override DEFAULT_MICRO, gases
+    ATJUP_SW_TAU_PER_BAR 1, ATJUP_PRECIP_SCALE 1, ATJUP_COSTHE_ABS 0, ATJUP_QHEAT_SCALE 0, the
+    Forces / Latent_Heat diagnostics on); constants override DEFAULT_MICRO, gases
     the three gas constant sets (DEFAULT_GASES)."""
     env = os.environ if env is None else env
     c = dict(DEFAULT_MICRO)
@@ -228,6 +245,11 @@ def resolve_micro(env: Mapping[str, str] | None = None, constants: Mapping[str, 
     mc.solar_strength = _env(env, "ATJUP_SOLAR_STRENGTH", 1.0, float)
     mc.sw_tau_per_bar = _env(env, "ATJUP_SW_TAU_PER_BAR", 1.0, float)
     mc.precip_rate_scale = _env(env, "ATJUP_PRECIP_SCALE", 1.0, float)
+    mc.diagnostics_on = 1
+    mc.costhe_abs = int(_env(env, "ATJUP_COSTHE_ABS", 0) != 0)
+    mc.qheat_scale = int(_env(env, "ATJUP_QHEAT_SCALE", 0) != 0)
+    for q, n in enumerate(CC_NAMES):
+        mc.cc[q] = c[n]
     for n in ("F_int", "S_solar", "albedo_bond", "x_H2", "x_He", "m_nh3", "m_h2s", "m_nh4sh",
               "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor", "t_0_nh4sh", "t_00_nh4sh"):
         setattr(mc, n, c[n])

@@ -61,6 +61,9 @@ enum {
     ATJUP_F_PROD, ATJUP_F_TKE_SOURCE, ATJUP_F_DIS_SOURCE,     /* closure diagnostics (out)     */
     ATJUP_F_DIFFLUX_H2S, ATJUP_F_DIFFLUX_NH3, ATJUP_F_DIFFLUX_NH4SH,
                                                               /* diffusive chemistry fluxes    */
+    ATJUP_F_CORIOLIS_FORCE, ATJUP_F_CENTRIFUGAL_FORCE, ATJUP_F_BUOYANCY_FORCE,
+    ATJUP_F_PRESGRAD_FORCE, ATJUP_F_Q_LATENT, ATJUP_F_Q_SENSIBLE,
+                                                              /* output diagnostics (out)      */
     ATJUP_F_COUNT
 };
 
@@ -354,6 +357,10 @@ typedef struct AtjupMicro {
     int32_t solar_on;            /* ATJUP_SOLAR 1                                                 */
     int32_t rad_bottom;          /* ATJUP_RAD_BOTTOM 0: lower boundary of the thermal stream      */
     int32_t precip_coupling_on;  /* ATJUP_PRECIP_COUPLING != 0: sources, not in-place removal     */
+    int32_t diagnostics_on;      /* 1: Forces and Latent_Heat close the physics block, as in the  */
+                                 /* loop (cJupiterModel.cpp:1163-1164)                             */
+    int32_t costhe_abs;          /* ATJUP_COSTHE_ABS 0 (cJupiterModel.h:1131-1134)                 */
+    int32_t qheat_scale;         /* ATJUP_QHEAT_SCALE 0 (cJupiterModel.h:963-970)                  */
     int32_t pad;
     /* radiation (Radiation.h:166-487, cJupiterModel.h:1109-1118)                                 */
     double F_int, S_solar, albedo_bond, x_H2, x_He;
@@ -369,12 +376,20 @@ typedef struct AtjupMicro {
     double polar_divisor_floor;            /* 0.4 (ATPhys.h:104-108)                              */
     double t_0_nh4sh, t_00_nh4sh;          /* 230, 200 K: the rate law's NH4SH formation window   */
                                            /* (cJupiterModel.h:194-195; nh4sh_eq = 0)             */
+    double cc[8];                          /* Latent_Heat's Clausius-Clapeyron E = exp(A/T + B):  */
+                                           /* A, B, A_i, B_i of H2O, then of NH3                  */
+                                           /* (cJupiterModel.h:222-240)                            */
     AtjupGasParams gas[3];                 /* H2O, NH3, CH4                                        */
 } AtjupMicro;
 
 /* Set (or with NULL clear) the microphysics of the iteration; with it and the physics block set,
  * atjup_gpu_step runs the full-physics schedule of the loop. */
 int atjup_gpu_set_micro(AtjupCtx* ctx, const AtjupMicro* micro);
+/* cJupiterModel::Forces (InitValues_Jup.cpp:742-812) and Latent_Heat (Thermo_Jup.cpp:89-232):
+ * the Coriolis, centrifugal, buoyancy and pressure-gradient force densities and the latent and
+ * sensible heating, output fields that nothing in the step reads. atjup_gpu_step runs it at the
+ * end of the physics block when AtjupMicro.diagnostics_on is set. */
+int atjup_gpu_diagnostics(AtjupCtx* ctx);
 /* Radiation<cJupiterModel>::run (Radiation.h:251-487): grey two-stream fluxes per column -> Q_rad. */
 int atjup_gpu_radiation(AtjupCtx* ctx);
 /* Precipitation<cJupiterModel>::run (Precipitation.h:191-445): the three-category column scheme of

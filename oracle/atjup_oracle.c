@@ -1043,6 +1043,7 @@ void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, in
 
 /* Size of the parameter block as compiled here, for binding checks. */
 size_t ora_params_sizeof(void) { return sizeof(AtjupParams); }
+size_t ora_micro_sizeof(void) { return sizeof(AtjupMicro); }
 size_t ora_gas_params_sizeof(void) { return sizeof(AtjupGasParams); }
 size_t ora_sat_stats_sizeof(void) { return sizeof(AtjupSatStats); }
 
@@ -2679,4 +2680,107 @@ void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const Atju
     for (int q = 0; q < ATJUP_S_COUNT; q++) memcpy(X->qn[q], X->q[q], sizeof(double) * N);
     memcpy(X->tken, X->tke, sizeof(double) * N);
     memcpy(X->disn, X->dis, sizeof(double) * N);
+}
+
+
+/* cJupiterModel::Forces (InitValues_Jup.cpp:742-812) and cJupiterModel::Latent_Heat
+ * (Thermo_Jup.cpp:89-232): out[0..5] = CoriolisForce, CentrifugalForce, BuoyancyForce,
+ * PresGradForce, Q_Latent, Q_Sensible. Forces fills i 1..im-2, j 1..jm-2, k 0..km-2 (the phi
+ * ring); Latent_Heat zeroes its two fields at i = 0 and fills the same interior, i downwards.
+ * Cells outside keep their values. coord_stretching is off (exp_rm = 1). */
+static double ora_max(double a, double b) { return (a < b) ? b : a; }   /* std::max */
+
+void ora_diagnostics(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                     const double* t, const double* u, const double* v, const double* w,
+                     const double* p_dyn, const double* p_stat, const double* h2o,
+                     const double* nh3, double* const* out) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    double *cor = out[0], *cen = out[1], *buo = out[2], *pgf = out[3], *ql = out[4], *qs = out[5];
+    const double omega = P->omega;
+    for (int i = 1; i < im - 1; i++)
+        for (int j = 1; j < jm - 1; j++) {
+            const double rm = G->rad[i];
+            const double sinthe = sin(G->the[j]);
+            double costhe = cos(G->the[j]);
+            if (MC->costhe_abs && j > 90) costhe = -costhe;
+            const double rmsinthe = rm * sinthe;
+            for (int k = 0; k < km - 1; k++) {
+                const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+                const size_t c = IDX(i, j, k);
+                const double Cor_r = -2.0 * omega * sinthe * w[c];
+                const double Cor_the = +2.0 * omega * costhe * w[c];
+                const double Cor_phi = +2.0 * omega * (-costhe * v[c] + sinthe * u[c]);
+                const double dpdr = (p_dyn[IDX(i + 1, j, k)] - p_dyn[IDX(i - 1, j, k)]) / (2.0 * P->dr);
+                const double dpdthe = (p_dyn[IDX(i, j + 1, k)] - p_dyn[IDX(i, j - 1, k)]) / (2.0 * P->dthe);
+                const double dpdphi = (p_dyn[IDX(i, j, ke)] - p_dyn[IDX(i, j, kw)]) / (2.0 * P->dphi);
+                cor[c] = P->Coriolis * P->r_mix *
+                         sqrt((pow(Cor_r, 2) + pow(Cor_the, 2) + pow(Cor_phi, 2)) / 3.0);
+                cen[c] = P->centrifugal * P->r_mix * omega * omega * rm * (1.0 + fabs(sinthe));
+                buo[c] = (t[c] > 0.0)
+                             ? P->buoyancy * P->r_mix * P->g * (p_stat[c] + p_dyn[c] * P->p_dyn_to_bar) /
+                                   (P->r_mix * P->R_mix * t[c] * P->t_ref) * 1e5
+                             : 0.0;
+                pgf[c] = -sqrt((pow(dpdr, 2) + pow(dpdthe / rm, 2) + pow(dpdphi / rmsinthe, 2)) / 3.0) *
+                         P->p_dyn_to_bar * 1.0e5 / (P->L_atm * 1.0e3);
+            }
+        }
+    for (int j = 0; j < jm; j++)
+        for (int k = 0; k < km; k++) { ql[IDX(0, j, k)] = 0.0; qs[IDX(0, j, k)] = 0.0; }
+    const double fix_lat = MC->qheat_scale ? (im - 1) / 1.0e3 : 1.0;
+    const double fix_sen = MC->qheat_scale ? P->L_atm * (im - 1) * (im - 1) / 1.0e3 : 1.0;
+    const AtjupGasParams *gw = &MC->gas[0], *ga = &MC->gas[1];
+    for (int j = 1; j < jm - 1; j++) {
+        const double sinthe = sin(G->the[j]);
+        for (int k = 0; k < km - 1; k++) {
+            const int kw = phi_wrap(1, k - 1, km), ke = phi_wrap(1, k + 1, km);
+            for (int i = im - 2; i >= 1; i--) {
+                const size_t c = IDX(i, j, k), cp = IDX(i + 1, j, k), cm = IDX(i - 1, j, k);
+                const size_t cjp = IDX(i, j + 1, k), cjm = IDX(i, j - 1, k);
+                const size_t ckp = IDX(i, j, ke), ckm = IDX(i, j, kw);
+                const double rm = G->rad[i];
+                const double rmsinthe = rm * sinthe;
+                const double exp_rm = 1.0;
+                double Latency_Ice = 0.0;
+                const double t_u = t[c] * P->t_ref;
+                const double p_u = p_stat[c];
+                const double E_Rain = exp(MC->cc[0] / t_u + MC->cc[1]);
+                const double E_Ice = exp(MC->cc[2] / t_u + MC->cc[3]);
+                const double q_Rain = gw->ep * E_Rain / ora_max(p_u - E_Rain, 1.0e-12);
+                const double q_Ice = gw->ep * E_Ice / ora_max(p_u - E_Ice, 1.0e-12);
+                const double E_Rain_nh3 = exp(MC->cc[4] / t_u + MC->cc[5]);
+                const double E_Ice_nh3 = exp(MC->cc[6] / t_u + MC->cc[7]);
+                const double q_Rain_nh3 = ga->ep * E_Rain_nh3 / ora_max(p_u - E_Rain_nh3, 1.0e-12);
+                const double q_Ice_nh3 = ga->ep * E_Ice_nh3 / ora_max(p_u - E_Ice_nh3, 1.0e-12);
+                const double u_av = 0.5 * (u[cp] + u[cm]);
+                const double v_av = 0.5 * (v[cp] + v[cm]);
+                const double w_av = 0.5 * (w[cp] + w[cm]);
+                const double velocity_av = -sqrt((pow(u_av, 2) + pow(v_av, 2) + pow(w_av, 2)) / 3.0);
+                const double dtdr = (t[cp] - t[cm]) / (2.0 * P->dr) * exp_rm;
+                const double dtdthe = (t[cjp] - t[cjm]) / (2.0 * rm * P->dthe);
+                const double dtdphi = (t[ckp] - t[ckm]) / (2.0 * rmsinthe * P->dphi);
+                const double dh2odr = (h2o[cp] - h2o[cm]) / (2.0 * P->dr) * exp_rm;
+                const double dh2odthe = (h2o[cjp] - h2o[cjm]) / (2.0 * rm * P->dthe);
+                const double dh2odphi = (h2o[ckp] - h2o[ckm]) / (2.0 * rmsinthe * P->dphi);
+                const double dnh3dr = (nh3[cp] - nh3[cm]) / (2.0 * P->dr) * exp_rm;
+                const double dnh3dthe = (nh3[cjp] - nh3[cjm]) / (2.0 * rm * P->dthe);
+                const double dnh3dphi = (nh3[ckp] - nh3[ckm]) / (2.0 * rmsinthe * P->dphi);
+                const double dtemp = dtdr + dtdthe + dtdphi;
+                const double dh2o = dh2odr + dh2odthe + dh2odphi;
+                const double dnh3 = dnh3dr + dnh3dthe + dnh3dphi;
+                const double Lr = P->L_atm * (im - 1);
+                if (h2o[c] >= q_Rain) ql[c] = gw->lv * velocity_av * dh2o * P->u_0 / Lr * fix_lat;
+                else ql[c] = 0.0;
+                if (h2o[c] >= q_Ice) Latency_Ice = gw->ls * velocity_av * dh2o * P->u_0 / Lr * fix_lat;
+                else Latency_Ice = 0.0;
+                if (nh3[c] >= q_Rain_nh3)
+                    ql[c] = ql[c] + ga->lv * velocity_av * dnh3 * P->u_0 / Lr * fix_lat;
+                if (nh3[c] >= q_Ice_nh3)
+                    Latency_Ice = Latency_Ice + ga->ls * velocity_av * dnh3 * P->u_0 / Lr * fix_lat;
+                ql[c] = ql[c] + Latency_Ice;
+                qs[c] = P->r_mix * P->cp_mix * velocity_av * P->u_0 * dtemp * P->t_ref /
+                        pow(P->L_atm * (im - 1), 2) * fix_sen;
+                if (G->solid[c] == 1) { ql[c] = 0.0; qs[c] = 0.0; }
+            }
+        }
+    }
 }

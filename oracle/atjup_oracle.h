@@ -142,6 +142,14 @@ void ora_iteration_phys(const AtjupParams* P, const AtjupPhysics* PH, const Atju
 void ora_iteration_dry(const AtjupParams* P, const ora_grid* G, ora_state* S, int iter_n,
                        int first, int sweeps);
 
+/* cJupiterModel::Forces (InitValues_Jup.cpp:742-812) and Latent_Heat (Thermo_Jup.cpp:89-232):
+ * out = CoriolisForce, CentrifugalForce, BuoyancyForce, PresGradForce, Q_Latent, Q_Sensible */
+void ora_diagnostics(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
+                     const double* t, const double* u, const double* v, const double* w,
+                     const double* p_dyn, const double* p_stat, const double* h2o,
+                     const double* nh3, double* const* out);
+size_t ora_micro_sizeof(void);
+
 #ifdef __cplusplus
 }
 #endif

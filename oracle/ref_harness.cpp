@@ -83,6 +83,8 @@ Array* field_by_name(const std::string& n) {
         F(nh3_cloudn), F(nh3_icen), F(ch4n), F(ch4_cloudn), F(ch4_icen), F(nh4shn), F(chromn),
         F(massflux_h2s), F(massflux_nh3), F(massflux_nh4sh), F(difflux_h2s), F(difflux_nh3),
         F(difflux_nh4sh), F(thermalmassflux), F(p_hydro), F(p_dyn), F(p_dynn), F(p_stat),
+        F(CoriolisForce), F(CentrifugalForce), F(BuoyancyForce), F(PresGradForce), F(Q_Latent),
+        F(Q_Sensible),
         F(rhs_t), F(rhs_u), F(rhs_v), F(rhs_w), F(rhs_h2o), F(rhs_h2o_cloud), F(rhs_h2o_ice),
         F(rhs_h2s), F(rhs_nh3), F(rhs_nh3_cloud), F(rhs_nh3_ice), F(rhs_ch4), F(rhs_ch4_cloud),
         F(rhs_ch4_ice), F(rhs_nh4sh), F(rhs_tke), F(rhs_dis), F(acc_t), F(acc_u), F(acc_v),
@@ -274,6 +276,14 @@ double ref_scalar(const char* name) {
     if (n == "D_h2s") return m.mue_h2s / (m.rg_h2s * m.sc_h2s);
     if (n == "D_nh4sh") return m.mue_nh4sh / (m.rg_nh4sh * m.sc_nh4sh);
     if (n == "polar_divisor_floor") return ATPhys::polar_divisor_floor<cJupiterModel>();
+    if (n == "coeff_h2o_A") return m.coeff_h2o_A;
+    if (n == "coeff_h2o_B") return m.coeff_h2o_B;
+    if (n == "coeff_h2o_A_i") return m.coeff_h2o_A_i;
+    if (n == "coeff_h2o_B_i") return m.coeff_h2o_B_i;
+    if (n == "coeff_nh3_A") return m.coeff_nh3_A;
+    if (n == "coeff_nh3_B") return m.coeff_nh3_B;
+    if (n == "coeff_nh3_A_i") return m.coeff_nh3_A_i;
+    if (n == "coeff_nh3_B_i") return m.coeff_nh3_B_i;
     if (n == "t_0_nh4sh") return m.t_0_nh4sh;
     if (n == "t_00_nh4sh") return m.t_00_nh4sh;
     if (n == "rad_F_int") return cJupiterModel::rad_F_int();
@@ -359,6 +369,8 @@ void ref_clamp_species() { g_m->clampNegativeSpecies(); }
 void ref_radiation() { RadiationJup(*g_m).run(); }
 void ref_precipitation() { PrecipitationJup(*g_m).run(); }
 void ref_nh4sh_eq() { ChemistryJup(*g_m).EquilibriumNH4SH("loop"); }
+// the output diagnostics that close the physics block (cJupiterModel.cpp:1163-1164)
+void ref_diagnostics() { g_m->Forces(); g_m->Latent_Heat(); }
 // The chemistry block of the loop (cJupiterModel.cpp:1144-1162 in the order ref_iteration runs
 // it): diffusive fluxes, their 1-2-1 smoothing, the mass rate, the NH4SH flux limiter and the
 // smoothing of the mass fluxes.

@@ -362,14 +362,17 @@ def oracle_bc(params, grid: dict, fields: dict, steps=("radius", "theta", "phi",
 MICRO_SPECIES_SOURCES = ("S_precip_h2o", "S_precip_h2o_cloud", "S_precip_h2o_ice", "S_precip_nh3",
                          "S_precip_nh3_cloud", "S_precip_nh3_ice", "S_precip_ch4",
                          "S_precip_ch4_cloud", "S_precip_ch4_ice")
+MICRO_DIAGNOSTICS = ("CoriolisForce", "CentrifugalForce", "BuoyancyForce", "PresGradForce",
+                     "Q_Latent", "Q_Sensible")
 MICRO_FIELDS = ("t", "Q_rad", "Q_precip") + MICRO_SPECIES_SOURCES + (
     "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
-    "difflux_nh3", "difflux_nh4sh")
+    "difflux_nh3", "difflux_nh4sh") + MICRO_DIAGNOSTICS
 
 
 def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
     """The microphysics routines in order on copies of fields (steps from radiation,
-    precipitation, nh4sh_eq, chemistry, clamp_species); returns {step: {field: array}}."""
+    precipitation, nh4sh_eq, chemistry, diagnostics, clamp_species); returns
+    {step: {field: array}}."""
     from atjup_b200.params import SPECIES
     f = dict(fields)
     f.setdefault("Q_rad", np.zeros(np.shape(fields["t"])))
@@ -379,7 +382,7 @@ def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
     keep = {}
     names = list(SPECIES) + list(MICRO_SPECIES_SOURCES) + [
         "massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
-        "difflux_nh3", "difflux_nh4sh"]
+        "difflux_nh3", "difflux_nh4sh"] + list(MICRO_DIAGNOSTICS)
     for n in names:
         keep[n] = np.ascontiguousarray(fields.get(n, np.zeros(shape)), dtype=np.float64).reshape(shape).copy()
     X = OraPhys()
@@ -398,6 +401,11 @@ def oracle_micro(params, micro, grid: dict, fields: dict, steps) -> dict:
         fn = getattr(o.lib, "ora_" + step)
         if step == "clamp_species":
             fn(ctypes.byref(params), ctypes.byref(X))
+        elif step == "diagnostics":
+            outs = (_P(ctypes.c_double) * 6)(*[_dp(keep[n]) for n in MICRO_DIAGNOSTICS])
+            fn(ctypes.byref(params), ctypes.byref(micro), ctypes.byref(o.G),
+               *[_dp(o.f[n]) for n in ("t", "u", "v", "w", "p_dyn", "p_stat")],
+               _dp(keep["h2o"]), _dp(keep["nh3"]), outs)
         else:
             fn(ctypes.byref(params), ctypes.byref(micro), ctypes.byref(o.G), ctypes.byref(o.S),
                ctypes.byref(X))

@@ -24,7 +24,8 @@ import numpy as np
 sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 
-from oracle_bridge import DRY_ENV, DYN_FIELDS, MICRO_FIELDS, MOIST_ENV, PHYS_ENV, Reference  # noqa: E402
+from oracle_bridge import (DRY_ENV, DYN_FIELDS, MICRO_DIAGNOSTICS, MICRO_FIELDS, MOIST_ENV,  # noqa: E402
+                           PHYS_ENV, Reference)
 
 SPECIES = ("h2o", "h2o_cloud", "h2o_ice", "nh3", "nh3_cloud", "nh3_ice",
            "ch4", "ch4_cloud", "ch4_ice")
@@ -180,7 +181,8 @@ def bc_case(ref, g, data, seed=SATADJ_SEED + 3):
 
 
 MICRO_CONSTS = ("m_nh3", "m_h2s", "m_nh4sh", "D_nh3", "D_h2s", "D_nh4sh", "polar_divisor_floor",
-                "t_0_nh4sh", "t_00_nh4sh",
+                "t_0_nh4sh", "t_00_nh4sh", "coeff_h2o_A", "coeff_h2o_B", "coeff_h2o_A_i",
+                "coeff_h2o_B_i", "coeff_nh3_A", "coeff_nh3_B", "coeff_nh3_A_i", "coeff_nh3_B_i",
                 "rad_F_int", "rad_S_solar", "rad_albedo_bond", "rad_x_H2", "rad_x_He",
                 "rad_cia_strength", "rad_opacity_strength", "rad_solar", "rad_solar_strength",
                 "rad_sw_tau_per_bar", "rad_bottom", "precip_rate_scale", "precip_coupling_on")
@@ -209,7 +211,7 @@ def micro_case(ref, g, data, seed=SATADJ_SEED + 4):
     for n in ("u", "v", "w"):
         data["in_" + n] = ref.get(n)
     for n in ("massflux_h2s", "massflux_nh3", "massflux_nh4sh", "fluxlim_nh4sh", "difflux_h2s",
-              "difflux_nh3", "difflux_nh4sh"):
+              "difflux_nh3", "difflux_nh4sh") + MICRO_DIAGNOSTICS:
         data["in_" + n] = ref.get(n)
     data["in_layer_heights"] = ref.get1("layer_heights").astype(np.float32)
     for c in MICRO_CONSTS:
@@ -220,6 +222,7 @@ def micro_case(ref, g, data, seed=SATADJ_SEED + 4):
         data["gas_" + gas] = cst
     for step, fn in (("radiation", ref.L.ref_radiation), ("precipitation", ref.L.ref_precipitation),
                      ("nh4sh_eq", ref.L.ref_nh4sh_eq), ("chemistry", ref.L.ref_chem_fluxes),
+                     ("diagnostics", ref.L.ref_diagnostics),
                      ("clamp_species", ref.L.ref_clamp_species)):
         ref.quiet(fn)
         for n in MICRO_FIELDS + PHYS_FIELDS[:11]:

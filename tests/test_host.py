@@ -49,6 +49,8 @@ def test_params_struct_size_matches_oracle():
     assert so.ora_params_sizeof() == ctypes.sizeof(P.AtjupParams)
     so.ora_gas_params_sizeof.restype = ctypes.c_size_t
     assert so.ora_gas_params_sizeof() == ctypes.sizeof(P.AtjupGasParams)
+    so.ora_micro_sizeof.restype = ctypes.c_size_t
+    assert so.ora_micro_sizeof() == ctypes.sizeof(P.AtjupMicro)
     so.ora_sat_stats_sizeof.restype = ctypes.c_size_t
     assert so.ora_sat_stats_sizeof() == ctypes.sizeof(P.AtjupSatStats)
 
@@ -115,13 +117,14 @@ def test_replica_timing_is_max_over_ranks():
 
 
 def test_field_ids_match_the_header():
-    """The Python field ids (atjup_b200.params) are the header's enum, in order."""
+    """The Python field ids (atjup_b200.params) are the header's enum, in order (the Python names
+    are the reference's array names: compared without case and underscores)."""
     src = (ROOT / "include" / "atjup_gpu.h").read_text()
     body = src[src.index("ATJUP_F_T = 0"):src.index("ATJUP_F_COUNT")]
     names = re.findall(r"ATJUP_F_(\w+)", body)
     py = {v: k for k, v in P.FIELD_IDS.items()}
     assert len(names) == len(P.FIELD_IDS)
     for i, n in enumerate(names):
-        assert py[i].lower() == n.lower(), (i, n, py[i])
+        assert py[i].lower().replace("_", "") == n.lower().replace("_", ""), (i, n, py[i])
     s_body = src[src.index("ATJUP_S_H2O = 0"):src.index("ATJUP_S_COUNT")]
     assert [x.lower() for x in re.findall(r"ATJUP_S_(\w+)", s_body)] == list(P.SPECIES)

@@ -16,6 +16,11 @@ agrees to relative L2 <= 1e-12, the grid totals agree to 1e-4, and no cell is of
 the field's maximum. Measured: 0.24 % of the columns flip on the reference's own state (totals to
 4e-7), up to 0.9 % on the synthetic 41x61x97 case (totals to 6e-5).
 
+The output diagnostics (cJupiterModel::Forces, InitValues_Jup.cpp:742-812, and Latent_Heat,
+Thermo_Jup.cpp:89-232) run after the chemistry block as in the loop. Latent_Heat switches each
+gas's contribution on where the vapour reaches saturation, a test on CUDA's exp, so Q_Latent is
+held to the precipitation's column-wise bar; the force densities and Q_Sensible to 1e-12.
+
 With ATJUP_NH4SH_EQ=0 NH4SH forms by the reaction-rate law of ChemMassRateJup
 (ChemistryJup.h:135-235) inside the 200..230 K window instead of the equilibrium: the same
 routines run with the rate law in the chemistry block, against the reference (oracle bit-exact,
@@ -29,7 +34,7 @@ from helpers import dump_fields, dump_grid, dump_params, ref_dump, synthetic_cas
 from oracle_bridge import MICRO_FIELDS, MOIST_ENV, oracle_micro, rel_l2
 
 MICRO_TOL = 1e-12
-STEPS = ("radiation", "precipitation", "nh4sh_eq", "chemistry", "clamp_species")
+STEPS = ("radiation", "precipitation", "nh4sh_eq", "chemistry", "diagnostics", "clamp_species")
 RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "albedo_bond",
           "rad_x_H2": "x_H2", "rad_x_He": "x_He"}
 
@@ -118,7 +123,7 @@ def gpu_micro(P, PH, MC, g, f, steps=STEPS):
     return out
 
 
-FLIP_FIELDS = ("Q_precip",) + tuple(n for n in MICRO_FIELDS if n.startswith("S_precip"))
+FLIP_FIELDS = ("Q_precip", "Q_Latent") + tuple(n for n in MICRO_FIELDS if n.startswith("S_precip"))
 FLIP_COLUMNS = 0.02
 
 
