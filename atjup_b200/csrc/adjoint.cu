@@ -258,21 +258,28 @@ struct AdArgs {
     double c_in, wgt;
 };
 
+// the transposed differences of one field at one cell: the four i and j neighbours are added at
+// once; the centre and the two phi neighbours are returned (cc, cp, cm) and combined across the
+// warp below, where the phi neighbours are the adjacent lanes
 __device__ __forceinline__ void scatter_field(const LinConst& q, double* L, const Nbr& n,
                                               double a0, double a1r, double a2r, double a1t,
-                                              double a2t, double a1p, double a2p) {
+                                              double a2t, double a1p, double a2p, double& cc,
+                                              double& cp, double& cm) {
     atomicAdd(L + n.ip, a1r * q.inv_2dr + a2r * q.inv_dr2);
     atomicAdd(L + n.im, -a1r * q.inv_2dr + a2r * q.inv_dr2);
     atomicAdd(L + n.jp, a1t * q.inv_2dthe + a2t * q.inv_dthe2);
     atomicAdd(L + n.jm, -a1t * q.inv_2dthe + a2t * q.inv_dthe2);
-    atomicAdd(L + n.kp, a1p * q.inv_2dphi + a2p * q.inv_dphi2);
-    atomicAdd(L + n.km, -a1p * q.inv_2dphi + a2p * q.inv_dphi2);
-    atomicAdd(L + n.c, a0 - 2.0 * (a2r * q.inv_dr2 + a2t * q.inv_dthe2 + a2p * q.inv_dphi2));
+    cp = a1p * q.inv_2dphi + a2p * q.inv_dphi2;
+    cm = -a1p * q.inv_2dphi + a2p * q.inv_dphi2;
+    cc = a0 - 2.0 * (a2r * q.inv_dr2 + a2t * q.inv_dthe2 + a2p * q.inv_dphi2);
 }
 
 __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
     double lb_cell = 0.0;
+    // per field: the adjoint added at the cell itself and at its phi+ and phi- neighbours
+    double cc[4] = {0.0, 0.0, 0.0, 0.0}, cp[4] = {0.0, 0.0, 0.0, 0.0}, cm[4] = {0.0, 0.0, 0.0, 0.0};
+    size_t at_c = 0, at_kp = 0, at_km = 0;
     if (k < q.km) {
         const Nbr n = nbr_of(q, i, j, k);
         const uint8_t nbm = A.a.nb[n.c];
@@ -364,10 +371,10 @@ __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
             Av0 -= aw * q.Coriolis * q.cor_phi_f * g.costhe;
             Au0 -= aw * q.Coriolis * q.cor_phi_f * g.sinthe_true;
 
-            scatter_field(q, A.lX[0], n, At0, Tr1, Tr2, Tt1, Tt2, Tp1, Tp2);
-            scatter_field(q, A.lX[1], n, Au0, Ur1, Ur2, Ut1, Ut2, Up1, Up2);
-            scatter_field(q, A.lX[2], n, Av0, Vr1, Vr2, Vt1, Vt2, Vp1, Vp2);
-            scatter_field(q, A.lX[3], n, Aw0, Wr1, Wr2, Wt1, Wt2, Wp1, Wp2);
+            scatter_field(q, A.lX[0], n, At0, Tr1, Tr2, Tt1, Tt2, Tp1, Tp2, cc[0], cp[0], cm[0]);
+            scatter_field(q, A.lX[1], n, Au0, Ur1, Ur2, Ut1, Ut2, Up1, Up2, cc[1], cp[1], cm[1]);
+            scatter_field(q, A.lX[2], n, Av0, Vr1, Vr2, Vt1, Vt2, Vp1, Vp2, cc[2], cp[2], cm[2]);
+            scatter_field(q, A.lX[3], n, Aw0, Wr1, Wr2, Wt1, Wt2, Wp1, Wp2, cc[3], cp[3], cm[3]);
             if (q.use_hp) {
                 size_t jp, jm, kp, km;
                 ph_nbrs(q, n, nbm, jp, jm, kp, km);
@@ -376,6 +383,34 @@ __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
                 atomicAdd(A.lph + kp, Ahkp);
                 atomicAdd(A.lph + km, Ahkm);
             }
+        }
+    }
+    // The phi neighbours across the warp: a warp is 32 consecutive k of one (i, j) row, so lane l's
+    // phi+ cell is lane l+1's and its phi- cell lane l-1's, unless the neighbour is across the
+    // warp's edge or the ring's seam (k = km-2 -> 0, 0 -> km-2); those are added by atomics.
+    {
+        const int lane = threadIdx.x & 31;
+        const bool own = k < q.km;
+        if (own) {
+            const size_t row = ((size_t)i * q.jm + j) * q.KP;
+            at_c = row + k;
+            at_kp = row + ((k >= q.km - 2) ? 0 : k + 1);
+            at_km = row + ((k == 0) ? q.km - 2 : k - 1);
+        }
+        const bool send_p = lane == 31 || k >= q.km - 2;        // phi+ not taken by lane l+1
+        const bool send_m = lane == 0 || k == 0;                 // phi- not taken by lane l-1
+        const bool take_l = lane > 0 && k - 1 < q.km - 2;        // lane l-1's phi+ is this cell
+        const bool take_r = lane < 31;                           // lane l+1's phi- is this cell
+        for (int f = 0; f < 4; f++) {
+            const double from_l = __shfl_up_sync(0xffffffffu, cp[f], 1);
+            const double from_r = __shfl_down_sync(0xffffffffu, cm[f], 1);
+            if (!own) continue;
+            double tot = cc[f];
+            if (take_l) tot += from_l;
+            if (take_r) tot += from_r;
+            if (tot != 0.0) atomicAdd(A.lX[f] + at_c, tot);
+            if (send_p && cp[f] != 0.0) atomicAdd(A.lX[f] + at_kp, cp[f]);
+            if (send_m && cm[f] != 0.0) atomicAdd(A.lX[f] + at_km, cm[f]);
         }
     }
     // the level mean's adjoint: a warp sum, one add per warp (a block lies in one level)

@@ -193,7 +193,7 @@ def test_autograd_three_steps_match_differences():
     ad = dot(grad, d)
     fd = (J_of(1.0) - J_of(-1.0)) / (2.0 * EPS)
     m.close()
-    floor = 10.0 * np.finfo(float).eps * abs(float(J)) / (2.0 * EPS)
+    floor = 10.0 * np.finfo(float).eps * abs(float(J.detach())) / (2.0 * EPS)
     print(f"autograd, 3 steps: adjoint {ad:.12e}  central difference {fd:.12e}  "
           f"rel {abs(ad - fd) / abs(fd):.2e}  floor {floor:.1e}")
     assert abs(ad - fd) <= 1e-6 * abs(fd) + floor
