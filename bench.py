@@ -8,7 +8,7 @@ Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 
 cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
 on even iterations the red-black pressure pass, mixture density, radiation, the saturation
 adjustment of H2O, NH3 and CH4, the NH4SH equilibrium, precipitation, the k-omega SST closure
-update and the chemistry fluxes; every iteration the four RK4 stages of t, u, v, w, the 11
+update, the chemistry fluxes and the output diagnostics (Forces, Latent_Heat); every iteration the four RK4 stages of t, u, v, w, the 11
 species and k*, omega*, the boundary passes, the moist convective adjustment, the in-loop
 4th-order Shapiro filter of u, v, w, the column balance of v and the species clamp. The initial
 state follows the full-physics recipe (atjup_b200/synthetic.py: state + full_physics): vapour at
@@ -75,8 +75,9 @@ CONFIGS = {
         "workload": "full-physics iteration on the 41x181x361 shell (the reference's default "
                     "physics: closure, radiation, precipitation, saturation adjustment, NH4SH "
                     "equilibrium, moist convective adjustment every iteration): the loop's "
-                    "schedule, pressure and physics on even iterations, RK4 of t, u, v, w, 11 "
-                    "species, k*, omega* every iteration",
+                    "schedule, pressure and physics on even iterations (with the Forces and "
+                    "Latent_Heat output diagnostics), RK4 of t, u, v, w, 11 species, k*, omega* "
+                    "every iteration",
         "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
         "l2": "no flush: inputs larger than L2 (each RK stage streams > 1.8 GB)",
         "parallelism": "replicas (the path does not shard)",
