@@ -3,10 +3,10 @@
 printing the relative L2 difference of every prognostic field. A measurement, not collected by
 pytest (the 200-iteration reference run takes several minutes on the host cores).
 
-    python tests/long_parity_phys.py [--iters 200] [--mca]
+    python tests/long_parity_phys.py [--iters 200] [--mca] [--rate-law]
 
 --mca runs both sides with the moist convective adjustment every iteration (the reference's
-default).
+default); --rate-law forms NH4SH by the reaction-rate law (ATJUP_NH4SH_EQ=0) on both sides.
 
 Test infrastructure only (reads the reference through oracle/_ref like the other parity tests).
 """
@@ -29,14 +29,18 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iters", type=int, default=200)
     ap.add_argument("--mca", action="store_true")
+    ap.add_argument("--rate-law", action="store_true")
     args = ap.parse_args()
     from atjup_b200.params import PREC_FP64, PREC_MIXED, resolve_mca
     from oracle_bridge import MCA_ENV
     t0 = time.time()
     extra = ("--env", "ATJUP_MCA=1") if args.mca else ()
+    if args.rate_law:
+        extra = extra + ("--env", "ATJUP_NH4SH_EQ=0")
     d, P, PH, MC, g, f = ref_iters_case(args.iters, *extra)
     t_ref = time.time() - t0
-    out = {"iterations": args.iters, "mca": args.mca, "reference_seconds": round(t_ref, 1)}
+    out = {"iterations": args.iters, "mca": args.mca, "rate_law": args.rate_law,
+           "reference_seconds": round(t_ref, 1)}
     for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
         m = gpu_moist_model(P, PH, MC, g, f)
         if args.mca:
