@@ -90,6 +90,12 @@ def test_resolve_micro_defaults():
     assert mc.cia_strength == 3.9 and mc.D_nh4sh == 0.0 and mc.polar_divisor_floor == 0.4
     assert mc.gas[2].t_0 == DEFAULT_GASES["CH4"][0]
     assert resolve_micro({"ATJUP_PRECIP_COUPLING": "0"}).precip_coupling_on == 0
+    # the output diagnostics: on, with the reference's Clausius-Clapeyron pairs and knobs off
+    assert (mc.diagnostics_on, mc.costhe_abs, mc.qheat_scale) == (1, 0, 0)
+    assert list(mc.cc) == [-4961.04, 13.0662, -4961.04, 13.0662, -2836.56, 11.7271, -2836.56, 11.7271]
+    k = resolve_micro({"ATJUP_COSTHE_ABS": "1", "ATJUP_QHEAT_SCALE": "1"})
+    assert (k.costhe_abs, k.qheat_scale) == (1, 1)
+    assert resolve_micro({}, {"coeff_nh3_B": 12.0}).cc[5] == 12.0
 
 
 def micro_case(im, jm, km, seed=31, env=MOIST_ENV):
