@@ -1,7 +1,8 @@
 """Transposes of the linear passes of the dry iteration, in numpy: the in-loop 4th-order Shapiro
 filter (lib/Utils.cpp:334-453, one pass), the zonal column balance of v
-(InitValues_Jup.cpp:1500-1538) and the boundary passes on t, u, v, w (BC_Jup.h:185-658,
-BoundaryConditions.h:253-360). Test infrastructure only: the specification, checked by
+(InitValues_Jup.cpp:1500-1538), the boundary passes on t, u, v, w (BC_Jup.h:185-658,
+BoundaryConditions.h:253-360) and the pressure pass (PressureSolver.h:144-766 with the radial walls
+of its source, cJupiterModel.cpp:1842-1864). Test infrastructure only: the specification, checked by
 dot-product tests against the oracle's forward passes, that GPU transposes of the whole
 iteration follow. Arrays are (im, jm, km) C-ordered; topo is the (jm, km) fluid floor.
 
@@ -9,7 +10,10 @@ Each forward pass maps an input field x to an output y cell by cell from a copy 
 transpose scatters each output's adjoint back through the same stencil: a 4th-order cell
 (y = x - c4 d4 x) gives 1 - 6 c4 to itself, 4 c4 to its first and -c4 to its second neighbours, a
 2nd-order cell (y = x + c2 d2 x) 1 - 2 c2 and c2, a copied cell 1. The passes are applied in
-reverse order.
+reverse order. The pressure pass updates p in place, one colour at a time; no cell of a colour
+reads another of the same colour (the ring of km-1 meridians is even), so each colour's transpose
+is a scatter of lam / den to the six neighbours and of -lam / den to the source, the colours
+taken black then red and the folds first within each sweep.
 """
 from __future__ import annotations
 
@@ -219,3 +223,172 @@ def bc_T(lam, solid, lid_u=1, top_taper=3, pole_fill_rows=2, mount_t_ambient=1):
             x[im - 3, :, :kn] += (g3 / kn)[:, None]
             x[im - 2, :, :kn] += (g2 / kn)[:, None]
     return L
+
+
+def _press_weights(P, grid):
+    """per interior cell the six neighbour weights of the red-black sweep (PressureSolver.h:
+    354-357, 461-479) and their sum den; the k neighbours wrap on the ring of km-1 meridians"""
+    im, jm, km = P.im, P.jm, P.km
+    sol = np.asarray(grid["solid"]).reshape(im, jm, km).astype(bool)
+    rad = np.asarray(grid["rad"], dtype=np.float64)
+    the = np.asarray(grid["the"], dtype=np.float64)
+    sinthe = np.maximum(P.sinthe_min, np.abs(np.sin(the)))
+    inv_rm2 = 1.0 / (rad * rad)
+    n1 = np.full((im, jm), 1.0 / (P.dr * P.dr))
+    n2 = inv_rm2[:, None] * np.full(jm, 1.0 / (P.dthe * P.dthe))[None, :]
+    n3 = (inv_rm2[:, None] / (sinthe * sinthe)[None, :]) * (1.0 / (P.dphi * P.dphi))
+    n = km - 1
+    ke = np.r_[(np.arange(n) + 1) % n, 0]
+    kw = np.r_[(np.arange(n) - 1) % n, 0]
+    interior = np.zeros((im, jm, km), bool)
+    interior[1:-1, 1:-1, :n] = True
+    fl = ~sol
+    nb_fluid = (_shift(fl, -1, 0), _shift(fl, 1, 0), _shift(fl, -1, 1), _shift(fl, 1, 1),
+                fl[:, :, ke], fl[:, :, kw])                                # +i, -i, +j, -j, +k, -k
+    full = ~(bool(P.press_wall) & fl)                                     # every face kept
+    W = []
+    for d, nn in enumerate((n1, n1, n2, n2, n3, n3)):
+        w = np.where(full | nb_fluid[d], nn[:, :, None], 0.0)
+        W.append(np.where(interior, w, 0.0))
+    den = np.where(interior, W[0] + W[1] + W[2] + W[3] + W[4] + W[5], 0.0)
+    return W, den, interior, ke, kw
+
+
+def _fold_T(lam):
+    """transpose of the folds after each sweep: 2-point Neumann in r over the whole shell, then
+    in theta, then the seam copy k = km-1 <- k = 0"""
+    im, jm, km = lam.shape
+    lam[:, :, 0] += lam[:, :, km - 1]
+    lam[:, :, km - 1] = 0.0
+    for ax, n in ((1, jm), (0, im)):
+        for edge, in1, in2 in ((0, 1, 2), (n - 1, n - 2, n - 3)):
+            sl = [slice(None)] * 3
+            sl[ax] = edge
+            g = lam[tuple(sl)].copy()
+            lam[tuple(sl)] = 0.0
+            sl[ax] = in1
+            lam[tuple(sl)] += C43 * g
+            sl[ax] = in2
+            lam[tuple(sl)] -= C13 * g
+
+
+def _div_terms(P, grid, i, j, k):
+    """the terms (field 0/1/2 = aux_u/v/w, (i, j, k), coefficient) of one cell's divergence
+    source (PressureSolver.h:370-459): one-sided at solid cells, the later theta and phi cases
+    overriding the earlier as in the reference"""
+    im, jm, km = P.im, P.jm, P.km
+    sol = grid["_sol3"]
+    n = km - 1
+    kw, ke = (k - 1) % n, (k + 1) % n
+    rm = float(grid["rad"][i])
+    sinthe = max(P.sinthe_min, abs(np.sin(grid["the"][j])))
+    i2dr, i2dt, i2dp = 1.0 / (2.0 * P.dr), 1.0 / (2.0 * P.dthe), 1.0 / (2.0 * P.dphi)
+    idt, idp = 1.0 / P.dthe, 1.0 / P.dphi
+    inv_rm, inv_rms = 1.0 / rm, 1.0 / (rm * sinthe)
+    sld = sol[i, j, k]
+    if i < im - 2 and sld and not sol[i + 1, j, k]:
+        du = [((i, j, k), -3.0 * i2dr), ((i + 1, j, k), 4.0 * i2dr), ((i + 2, j, k), -i2dr)]
+    else:
+        du = [((i + 1, j, k), i2dr), ((i - 1, j, k), -i2dr)]
+    dv = [((i, j + 1, k), i2dt), ((i, j - 1, k), -i2dt)]
+    if 2 < j < jm - 2:
+        ajp, ajm = not sol[i, j + 1, k], not sol[i, j - 1, k]
+        if sld and ajp and not sol[i, j + 2, k]:
+            dv = [((i, j, k), -3.0 * i2dt), ((i, j + 1, k), 4.0 * i2dt), ((i, j + 2, k), -i2dt)]
+        if sld and ajm and not sol[i, j - 2, k]:
+            dv = [((i, j, k), 3.0 * i2dt), ((i, j - 1, k), -4.0 * i2dt), ((i, j - 2, k), i2dt)]
+        if (sld and ajp and sol[i, j + 2, k]) or (j == jm - 2 and not sld and sol[i, j + 1, k]):
+            dv = [((i, j + 1, k), idt), ((i, j, k), -idt)]
+        if (sld and ajm and sol[i, j - 2, k]) or (j == 1 and sld and ajm):
+            dv = [((i, j - 1, k), idt), ((i, j, k), -idt)]
+    dw = [((i, j, ke), i2dp), ((i, j, kw), -i2dp)]
+    if 2 < k < km - 2:
+        akp, akm = not sol[i, j, ke], not sol[i, j, kw]
+        skp2 = sol[i, j, k + 2] if k < km - 2 else False
+        skm2 = sol[i, j, k - 2] if k > 2 else False
+        if sld and akp and not skp2:
+            dw = [((i, j, k), -3.0 * i2dp), ((i, j, k + 1), 4.0 * i2dp), ((i, j, k + 2), -i2dp)]
+        if sld and akm and not skm2:
+            dw = [((i, j, k), 3.0 * i2dp), ((i, j, k - 1), -4.0 * i2dp), ((i, j, k - 2), i2dp)]
+        if (sld and akp and skp2) or (k == km - 2 and not sld and sol[i, j, ke]):
+            dw = [((i, j, k + 1), idp), ((i, j, k), -idp)]
+        if (sld and akm and skm2) or (k == 1 and sld and akm):
+            dw = [((i, j, k - 1), idp), ((i, j, k), -idp)]
+    return ([(0, c, a) for c, a in du] + [(1, c, a * inv_rm) for c, a in dv]
+            + [(2, c, a * inv_rms) for c, a in dw])
+
+
+def _with_sol3(P, grid):
+    g = dict(grid)
+    g["_sol3"] = np.asarray(grid["solid"]).reshape(P.im, P.jm, P.km).astype(bool)
+    return g
+
+
+def pressure_source(P, grid, aux):
+    """the unclamped divergence source of (aux_u, aux_v, aux_w) after the radial walls of the
+    projection (cJupiterModel.cpp:1842-1864) at the cells the sweep updates (den > 0)"""
+    g = _with_sol3(P, grid)
+    a = [np.array(x, dtype=np.float64) for x in aux]
+    im, jm, km = a[0].shape
+    for j in range(1, jm - 1):
+        for k in range(km - 1):
+            if P.rigid_lid:
+                a[0][0, j, k] = a[0][im - 1, j, k] = 0.0
+            else:
+                a[0][0, j, k] = C43 * a[0][1, j, k] - C13 * a[0][2, j, k]
+                a[0][im - 1, j, k] = C43 * a[0][im - 2, j, k] - C13 * a[0][im - 3, j, k]
+            for q in (1, 2):
+                a[q][0, j, k] = C43 * a[q][1, j, k] - C13 * a[q][2, j, k]
+                a[q][im - 1, j, k] = C43 * a[q][im - 2, j, k] - C13 * a[q][im - 3, j, k]
+    _, den, interior, _, _ = _press_weights(P, grid)
+    src = np.zeros_like(a[0])
+    for i, j, k in zip(*np.nonzero(interior & (den > 0))):
+        src[i, j, k] = sum(coef * a[q][c] for q, c, coef in _div_terms(P, g, i, j, k))
+    return src
+
+
+def pressure_T(lam, P, grid, sweeps, pass_mask=None):
+    """the transpose of the pressure pass (PressureSolver.h:144-766, pointwise branch, omega 1):
+    `sweeps` red-black Gauss-Seidel sweeps of p_dyn with the folds after each, the source the
+    clamped divergence of aux_u, aux_v, aux_w after their radial walls. The clamp is linearised
+    by pass_mask (1 where |div| < cap den, default everywhere). Returns the adjoints of p_dyn
+    and of aux_u, aux_v, aux_w before the pass."""
+    lp = np.array(lam, dtype=np.float64)
+    im, jm, km = lp.shape
+    W, den, interior, ke, kw = _press_weights(P, grid)
+    n = km - 1
+    ii, jj, kk = np.meshgrid(np.arange(im), np.arange(jm), np.arange(km), indexing="ij")
+    parity = (ii + jj + kk) & 1
+    lsrc = np.zeros_like(lp)
+    for _ in range(sweeps):
+        _fold_T(lp)
+        for colour in (1, 0):
+            act = interior & (den > 0) & (parity == colour)
+            G = np.where(act, lp, 0.0) / np.where(act, den, 1.0)
+            lp[act] = 0.0
+            lsrc -= G
+            lp += _shift(W[0] * G, 1, 0) + _shift(W[1] * G, -1, 0)
+            lp += _shift(W[2] * G, 1, 1) + _shift(W[3] * G, -1, 1)
+            lp[:, :, :n] += np.roll((W[4] * G)[:, :, :n], 1, axis=2)
+            lp[:, :, :n] += np.roll((W[5] * G)[:, :, :n], -1, axis=2)
+    if pass_mask is not None:
+        lsrc = lsrc * pass_mask
+    g = _with_sol3(P, grid)
+    la = [np.zeros_like(lp) for _ in range(3)]
+    for i, j, k in zip(*np.nonzero(lsrc)):
+        s = lsrc[i, j, k]
+        for q, c, coef in _div_terms(P, g, i, j, k):
+            la[q][c] += coef * s
+    for j in range(1, jm - 1):
+        for k in range(km - 1):
+            if P.rigid_lid:
+                la[0][0, j, k] = la[0][im - 1, j, k] = 0.0
+            qs = (1, 2) if P.rigid_lid else (0, 1, 2)
+            for q in qs:
+                g0, g1 = la[q][0, j, k], la[q][im - 1, j, k]
+                la[q][0, j, k] = la[q][im - 1, j, k] = 0.0
+                la[q][1, j, k] += C43 * g0
+                la[q][2, j, k] -= C13 * g0
+                la[q][im - 2, j, k] += C43 * g1
+                la[q][im - 3, j, k] -= C13 * g1
+    return lp, la

@@ -1,8 +1,10 @@
 """The numpy transposes of the dry iteration's linear passes (tests/adjoint_linear.py) against
 the oracle's forward passes, by the dot-product test <F d, l> = <d, F^T l> on seeded random d
 and l: one pass of the in-loop 4th-order Shapiro filter (lib/Utils.cpp:334-453), the zonal
-column balance of v (InitValues_Jup.cpp:1500-1538) and the boundary passes on t, u, v, w
-(BC_Jup.h:185-658, BoundaryConditions.h:253-360) with each of their knobs. These transposes
+column balance of v (InitValues_Jup.cpp:1500-1538), the boundary passes on t, u, v, w
+(BC_Jup.h:185-658, BoundaryConditions.h:253-360) with each of their knobs, and the pressure pass
+(PressureSolver.h:144-766: two red-black sweeps of p_dyn and the one-sided divergence source of
+aux_u, aux_v, aux_w), with its clamp off and with a fixed clamp mask. These transposes
 are the specification that GPU transposes of the whole dry iteration follow; the bar is
 roundoff (1e-13 relative)."""
 import ctypes
@@ -67,4 +69,73 @@ def test_boundary_transpose(shape, knobs):
     LT = AL.bc_T(lam, g["solid"], lid_u=p.lid_u, top_taper=p.top_taper,
                  pole_fill_rows=p.pole_fill_rows, mount_t_ambient=p.mount_t_ambient)
     rhs = sum(float(np.vdot(d[n], LT[n])) for n in NAMES)
+    assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
+
+
+NO_CLAMP = 1e200      # the source clamp cap * den never binds, so the pass is linear
+
+
+def aux_case(shape, knobs, seed):
+    p, g, f = synthetic_case(*shape, seed=81)
+    p.p_dyn_cap = NO_CLAMP
+    for k, v in knobs.items():
+        setattr(p, k, v)
+    rng = np.random.default_rng(seed)
+    sh = f["t"].shape
+    return p, g, f, rng.standard_normal(sh), [rng.standard_normal(sh) for _ in range(3)], \
+        rng.standard_normal(sh)
+
+
+def set_aux(o, d_a):
+    o.f["aux_u"][...], o.f["aux_v"][...], o.f["aux_w"][...] = d_a
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_pressure_source_matches_oracle(shape):
+    p, g, f, _, d_a, _ = aux_case(shape, {}, 6)
+    o = oracle_from(p, g, f)
+    set_aux(o, d_a)
+    o.call("ora_prepare_projection")
+    want = o.source()
+    got = AL.pressure_source(p, g, d_a)
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    # the one-sided stencils at the obstacle are exercised
+    gg = AL._with_sol3(p, g)
+    one_sided = sum(1 for i, j, k in zip(*np.nonzero(gg["_sol3"]))
+                    if 0 < i < p.im - 1 and 0 < j < p.jm - 1 and k < p.km - 1
+                    and len(AL._div_terms(p, gg, i, j, k)) > 6)
+    assert one_sided > 0
+
+
+@pytest.mark.parametrize("knobs", [{}, {"press_wall": 0}, {"rigid_lid": 0}],
+                         ids=["default", "no_press_wall", "free_lid"])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_pressure_transpose(shape, knobs):
+    p, g, f, d_p, d_a, lam = aux_case(shape, knobs, 6)
+    o = oracle_from(p, g, f)
+    o.f["p_dyn"][...] = d_p
+    set_aux(o, d_a)
+    o.pressure(sweeps=2)
+    lhs = float(np.vdot(o.f["p_dyn"], lam))
+    lp, la = AL.pressure_T(lam, p, g, 2)
+    rhs = float(np.vdot(d_p, lp)) + sum(float(np.vdot(d_a[q], la[q])) for q in range(3))
+    assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_pressure_transpose_clamp_mask(shape):
+    """the clamp linearised at a base state passes the source's derivative only where it does
+    not bind: the forward runs the sweeps on b = mask * source through the oracle's b argument"""
+    p, g, f, d_p, d_a, lam = aux_case(shape, {}, 7)
+    mask = (np.random.default_rng(8).uniform(size=d_p.shape) < 0.7).astype(np.float64)
+    o = oracle_from(p, g, f)
+    set_aux(o, d_a)
+    o.call("ora_prepare_projection")
+    b = mask * o.source()
+    o = oracle_from(p, g, f)
+    o.f["p_dyn"][...] = d_p
+    o.pressure(sweeps=2, b=np.ascontiguousarray(b))
+    lhs = float(np.vdot(o.f["p_dyn"], lam))
+    lp, la = AL.pressure_T(lam, p, g, 2, pass_mask=mask)
+    rhs = float(np.vdot(d_p, lp)) + sum(float(np.vdot(d_a[q], la[q])) for q in range(3))
     assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
