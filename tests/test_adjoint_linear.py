@@ -139,3 +139,31 @@ def test_pressure_transpose_clamp_mask(shape):
     lp, la = AL.pressure_T(lam, p, g, 2, pass_mask=mask)
     rhs = float(np.vdot(d_p, lp)) + sum(float(np.vdot(d_a[q], la[q])) for q in range(3))
     assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_iteration_tail_transpose(shape):
+    """the dry iteration after the RK step, in the loop's order (cJupiterModel.cpp:1032-1381):
+    the boundary passes, two in-loop Shapiro passes of u, v, w (ATJUP_VEL_SHAPIRO_INLOOP=2; the
+    default is 0), the column balance of v; its transpose is the transposes in reverse order"""
+    p, g, f = synthetic_case(*shape, seed=81)
+    passes = p.shapiro_inloop = 2
+    rng = np.random.default_rng(9)
+    d = {n: rng.standard_normal(f["t"].shape) for n in NAMES}
+    lam = {n: rng.standard_normal(f["t"].shape) for n in NAMES}
+    o = oracle_from(p, g, {**f, **d})
+    for step in ("radius", "theta", "phi", "solid"):
+        o.call(f"ora_bc_{step}")
+    for n in ("u", "v", "w"):
+        o.shapiro(n, 4, p.shapiro_strength, passes, 1)
+    o.lib.ora_balance_column_v(ctypes.byref(o.P), ctypes.byref(o.G), ctypes.byref(o.S))
+    lhs = sum(float(np.vdot(o.f[n], lam[n])) for n in NAMES)
+    L = {n: lam[n].copy() for n in NAMES}
+    L["v"] = AL.balance_v_T(L["v"], g["topo"], g["rad"], p.dr)
+    for n in ("u", "v", "w"):
+        for _ in range(passes):
+            L[n] = AL.shapiro4_T(L[n], g["topo"], p.shapiro_strength)
+    L = AL.bc_T(L, g["solid"], lid_u=p.lid_u, top_taper=p.top_taper,
+                pole_fill_rows=p.pole_fill_rows, mount_t_ambient=p.mount_t_ambient)
+    rhs = sum(float(np.vdot(d[n], L[n])) for n in NAMES)
+    assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
