@@ -2,7 +2,8 @@
 filter (lib/Utils.cpp:334-453, one pass), the zonal column balance of v
 (InitValues_Jup.cpp:1500-1538), the boundary passes on t, u, v, w (BC_Jup.h:185-658,
 BoundaryConditions.h:253-360) and the pressure pass (PressureSolver.h:144-766 with the radial walls
-of its source, cJupiterModel.cpp:1842-1864). Test infrastructure only: the specification, checked by
+of its source, cJupiterModel.cpp:1842-1864), and the tangent-linear and transpose of the
+mixture density between them and the RK step (computeMixtureDensity). Test infrastructure only: the specification, checked by
 dot-product tests against the oracle's forward passes, that GPU transposes of the whole
 iteration follow. Arrays are (im, jm, km) C-ordered; topo is the (jm, km) fluid floor.
 
@@ -392,3 +393,33 @@ def pressure_T(lam, P, grid, sweeps, pass_mask=None):
                 la[q][im - 2, j, k] += C43 * g1
                 la[q][im - 3, j, k] -= C13 * g1
     return lp, la
+
+
+def _rho_base(P, t, p_stat, p_dyn):
+    w = 1.0 if P.rho_pdyn else 0.0
+    T = np.asarray(t) * P.t_ref
+    p_pa = (np.asarray(p_stat) + w * np.asarray(p_dyn) * P.p_dyn_to_bar) * 1.0e5
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rho = p_pa / (P.R_mix * T)
+    live = (T > 0.0) & np.isfinite(rho)
+    return w, T, np.where(live, rho, 0.0), live
+
+
+def mixture_density_tl(P, t, p_stat, p_dyn, dt, dp_stat, dp_dyn):
+    """the tangent-linear of the mixture density (rho = (p_stat + p_dyn c) 1e5 / (R_mix t t_ref),
+    0 where t <= 0) about (t, p_stat, p_dyn)"""
+    w, T, rho, live = _rho_base(P, t, p_stat, p_dyn)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d = (1.0e5 * (dp_stat + w * P.p_dyn_to_bar * dp_dyn) / (P.R_mix * T)
+             - rho * dt / np.asarray(t))
+    return np.where(live, d, 0.0)
+
+
+def mixture_density_T(P, t, p_stat, p_dyn, lam):
+    """its transpose: the adjoints of t, p_stat, p_dyn from that of rho_mix"""
+    w, T, rho, live = _rho_base(P, t, p_stat, p_dyn)
+    lam = np.where(live, lam, 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a_p = np.where(live, 1.0e5 * lam / (P.R_mix * T), 0.0)
+        a_t = np.where(live, -rho * lam / np.asarray(t), 0.0)
+    return a_t, a_p, w * P.p_dyn_to_bar * a_p

@@ -4,7 +4,9 @@ and l: one pass of the in-loop 4th-order Shapiro filter (lib/Utils.cpp:334-453),
 column balance of v (InitValues_Jup.cpp:1500-1538), the boundary passes on t, u, v, w
 (BC_Jup.h:185-658, BoundaryConditions.h:253-360) with each of their knobs, and the pressure pass
 (PressureSolver.h:144-766: two red-black sweeps of p_dyn and the one-sided divergence source of
-aux_u, aux_v, aux_w), with its clamp off and with a fixed clamp mask. These transposes
+aux_u, aux_v, aux_w), with its clamp off and with a fixed clamp mask; the iteration's tail after
+the RK step composed in the loop's order; and the mixture density's tangent-linear against central
+differences of the oracle. These transposes
 are the specification that GPU transposes of the whole dry iteration follow; the bar is
 roundoff (1e-13 relative)."""
 import ctypes
@@ -166,4 +168,32 @@ def test_iteration_tail_transpose(shape):
     L = AL.bc_T(L, g["solid"], lid_u=p.lid_u, top_taper=p.top_taper,
                 pole_fill_rows=p.pole_fill_rows, mount_t_ambient=p.mount_t_ambient)
     rhs = sum(float(np.vdot(d[n], L[n])) for n in NAMES)
+    assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
+
+
+def test_mixture_density_tl_and_transpose():
+    """the tangent-linear against central differences of the oracle's mixture density
+    (computeMixtureDensity), then the transpose against the tangent-linear by the dot product"""
+    p, g, f = synthetic_case(9, 21, 33, seed=81)
+    p.rho_pdyn = 1
+    rng = np.random.default_rng(10)
+    sh = f["t"].shape
+    dirs = [rng.standard_normal(sh) * s for s in (np.abs(f["t"]).mean(), np.abs(f["p_stat"]).mean(),
+                                                  np.abs(f["p_stat"]).mean() / p.p_dyn_to_bar)]
+
+    def rho(eps):
+        o = oracle_from(p, g, {**f, "t": f["t"] + eps * dirs[0], "p_stat": f["p_stat"] + eps * dirs[1],
+                               "p_dyn": f["p_dyn"] + eps * dirs[2]})
+        o.call("ora_mixture_density")
+        return o.f["rho_mix"].copy()
+
+    eps = 1e-6
+    fd = (rho(eps) - rho(-eps)) / (2.0 * eps)
+    tl = AL.mixture_density_tl(p, f["t"], f["p_stat"], f["p_dyn"], *dirs)
+    assert (tl != 0).sum() > 0.5 * tl.size
+    assert np.linalg.norm(fd - tl) <= 1e-7 * np.linalg.norm(tl)
+    lam = rng.standard_normal(sh)
+    lhs = float(np.vdot(tl, lam))
+    adj = AL.mixture_density_T(p, f["t"], f["p_stat"], f["p_dyn"], lam)
+    rhs = sum(float(np.vdot(d, a)) for d, a in zip(dirs, adj))
     assert rel(lhs, rhs) <= DOT_TOL, (lhs, rhs)
