@@ -330,12 +330,14 @@ void ora_rk4(const AtjupParams* P, const ora_grid* G, ora_state* S) {
     for (int stage = 0; stage < 4; stage++) {
         const double c_in = (stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0);
         const double wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+        #pragma omp parallel for schedule(static)
         for (int i = 1; i < im - 1; i++)
             for (int j = 3; j < jm - 3; j++)
                 for (int k = 0; k < km - 1; k++) {
                     if (G->solid[IDX(i, j, k)]) continue;
                     ora_rhs_cell(P, G, S, i, j, k);
                 }
+        #pragma omp parallel for schedule(static)
         for (int i = 1; i < im - 1; i++)
             for (int j = 3; j < jm - 3; j++)
                 for (int k = 0; k < km - 1; k++) {
@@ -354,6 +356,7 @@ void ora_rk4(const AtjupParams* P, const ora_grid* G, ora_state* S) {
                 }
     }
     const double one_sixth = 1.0 / 6.0;
+    #pragma omp parallel for schedule(static)
     for (int i = 1; i < im - 1; i++)
         for (int j = 3; j < jm - 3; j++)
             for (int k = 0; k < km - 1; k++) {
@@ -1561,6 +1564,9 @@ void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* 
     for (int stage = 0; stage < 4; stage++) {
         const double c_in = (stage == 0 || stage == 1) ? 0.5 * dt : (stage == 2 ? dt : 0.0);
         const double wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
+        /* each cell writes only its own right-hand sides and reads no other cell's: the loops
+         * run in parallel with the same result to the bit */
+        #pragma omp parallel for schedule(static)
         for (int i = 1; i < im - 1; i++)
             for (int j = 3; j < jm - 3; j++)
                 for (int k = 0; k < km - 1; k++) {
@@ -1568,6 +1574,7 @@ void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* 
                     ora_rhs_cell(P, G, S, i, j, k);
                     ora_rhs_phys_cell(P, PH, G, S, X, i, j, k);
                 }
+        #pragma omp parallel for schedule(static)
         for (int i = 1; i < im - 1; i++)
             for (int j = 3; j < jm - 3; j++)
                 for (int k = 0; k < km - 1; k++) {
@@ -1595,6 +1602,7 @@ void ora_rk4_phys(const AtjupParams* P, const AtjupPhysics* PH, const ora_grid* 
                 }
     }
     const double one_sixth = 1.0 / 6.0;
+    #pragma omp parallel for schedule(static)
     for (int i = 1; i < im - 1; i++)
         for (int j = 3; j < jm - 3; j++)
             for (int k = 0; k < km - 1; k++) {
