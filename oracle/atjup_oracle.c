@@ -2155,6 +2155,8 @@ void ora_nh4sh_eq(const AtjupParams* P, const AtjupMicro* MC, const ora_grid* G,
     const double R_univ = 8314.46, atm = 101325.0;
     const double L_f = 4705.0 * log(10.0) * 8314.46 / 51.1114;
     double *nh3 = X->q[ATJUP_S_NH3], *h2s = X->q[ATJUP_S_H2S], *nh4sh = X->q[ATJUP_S_NH4SH];
+    /* each cell reads and writes only itself: parallel, bit-identical to one thread */
+    #pragma omp parallel for schedule(dynamic, 1)
     for (int j = 0; j < jm; j++)
         for (int k = 0; k < km; k++)
             for (int i = 0; i < im; i++) {
