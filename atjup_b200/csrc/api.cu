@@ -722,7 +722,7 @@ int atjup_gpu_pressure_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveSta
     def.sweeps = c->P.press_sweeps;
     def.omega = 1.0;
     if (!o) o = &def;
-    if (o->mode == ATJUP_SOLVE_RESIDUAL) {
+    if (o->mode == ATJUP_SOLVE_RESIDUAL || o->mode == ATJUP_SOLVE_SOR) {
         Timed tm(c, TK_SOLVER);
         return pressure_residual_solve(c, o, st);
     }

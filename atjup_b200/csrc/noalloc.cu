@@ -1,11 +1,10 @@
 // Column balance of v with no device allocation (atjup_gpu_balance_column_v_noalloc).
 //
 // Some callers cannot call cudaMalloc at all: a host model that hands the GPU layer one
-// preallocated memory pool and forbids allocations after start-up, code running while a CUDA
-// stream is being captured (an allocation there invalidates the capture), or an embedding that
-// must never fail mid-run on an out-of-memory allocation. This entry point takes the caller's
-// device buffers for inputs and output and keeps its own scratch -- the per-column means of r v
-// and the per-row means -- in a fixed-size file-scope device array, so it allocates nothing.
+// preallocated memory pool and forbids allocations after start-up, or an embedding that must
+// never fail mid-run on an out-of-memory allocation. This entry point takes the caller's device
+// buffers for inputs and output and keeps its own scratch -- the per-column means of r v and the
+// per-row means -- in a fixed-size file-scope device array, so it allocates nothing.
 //
 // Limits: jm <= ATJUP_NOALLOC_MAX_J and pitch <= ATJUP_NOALLOC_MAX_PITCH (larger sizes are
 // rejected with ATJUP_ERR_ARG). The array (~1.05 MB) is resident on every GPU that loads this
@@ -13,6 +12,12 @@
 // every value a call reads is written earlier in that same call, so nothing needs clearing.
 // Calls that overlap on the GPU (different streams, or different host threads without ordering)
 // race on the array: order them on one stream.
+//
+// Set-up: the first call on each device, with that device current, looks up the array's device
+// address with cudaGetSymbolAddress and keeps it for the rest of the process; that first call
+// should come before any stream capture. A cudaDeviceReset ends the module the address belongs
+// to, so the kept address is stale afterwards: a process that resets a device must not call this
+// entry point on it again.
 #include "ctx.cuh"
 
 #include <atomic>

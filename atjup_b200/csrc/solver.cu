@@ -19,8 +19,8 @@
 //     discrete Fourier transform over the meridian ring and one tridiagonal system in theta per
 //     wavenumber (the reference's PRESS_BAROTROPIC idea, PressureSolver.h:49-67, 573-708, used
 //     here as a preconditioner, so the obstacle need not be obstacle-free).
-// Mixed precision: FP32 PCG as the inner solver of an FP64 iterative-refinement loop whose
-// residual b - A p is formed in FP64.
+// Mixed precision: the Krylov vectors, the residual b - A p and the update of p stay FP64; the
+// preconditioner (the radial line solves and the column-mode solve) runs in FP32.
 #include "ctx.cuh"
 
 #include <cmath>
@@ -369,6 +369,54 @@ residual_kernel(const double* __restrict__ b, const double* __restrict__ x, doub
         for (int w = 0; w < RB / 32; w++) { tr += sh[0][w]; tv += sh[1][w]; }
         part[blockIdx.x] = tr;
         part[NRED + blockIdx.x] = tv;
+    }
+}
+
+// One colour of point red-black SOR on A x = b (the same folded operator as apply_kernel and
+// residual_kernel): x_c <- x_c + omega ((b_c - sum_off a_cf x_f) / a_cc - x_c) for the fluid
+// interior cells with (i + j + k) % 2 == colour. A folded boundary face contributes +w/3 to a_cc
+// and -w/3 to the inward neighbour's coefficient; a plain face -w to a_cc and +w to the
+// neighbour's. Within one colour every cell reads only cells of the other colour (the phi ring
+// has an even number of meridians), so the parallel pass equals the sequential one.
+__global__ void __launch_bounds__(RB)
+sor_kernel(const double* __restrict__ b, double* __restrict__ x, const uint8_t* __restrict__ s,
+           const GeoIJ* __restrict__ geo, const double* __restrict__ yw, OpC q, int colour,
+           double omega) {
+    const size_t plane = (size_t)q.jm * q.KP, row = q.KP;
+    const size_t NP = (size_t)q.im * plane;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < NP;
+         c += (size_t)gridDim.x * blockDim.x) {
+        if (!(yw[c] > 0.0)) continue;
+        const int k = (int)(c % row);
+        const int j = (int)((c / row) % q.jm);
+        const int i = (int)(c / plane);
+        if (((i + j + k) & 1) != colour) continue;
+        const GeoIJ& g = geo[i * q.jm + j];
+        const double n1 = q.n1, n2 = g.num2, n3 = g.num3;
+        const int kw = (k == 0) ? q.km - 2 : k - 1;
+        const int ke = (k == q.km - 2) ? 0 : k + 1;
+        double diag = 0.0, off = 0.0;
+        if (!s[c + plane]) {
+            if (i + 1 == q.im - 1) { diag += n1 * kC13; off -= n1 * kC13 * x[c - plane]; }
+            else { diag -= n1; off += n1 * x[c + plane]; }
+        }
+        if (!s[c - plane]) {
+            if (i - 1 == 0) { diag += n1 * kC13; off -= n1 * kC13 * x[c + plane]; }
+            else { diag -= n1; off += n1 * x[c - plane]; }
+        }
+        if (!s[c + row]) {
+            if (j + 1 == q.jm - 1) { diag += n2 * kC13; off -= n2 * kC13 * x[c - row]; }
+            else { diag -= n2; off += n2 * x[c + row]; }
+        }
+        if (!s[c - row]) {
+            if (j - 1 == 0) { diag += n2 * kC13; off -= n2 * kC13 * x[c + row]; }
+            else { diag -= n2; off += n2 * x[c - row]; }
+        }
+        if (!s[c - k + ke]) { diag -= n3; off += n3 * x[c - k + ke]; }
+        if (!s[c - k + kw]) { diag -= n3; off += n3 * x[c - k + kw]; }
+        if (diag == 0.0) continue;
+        const double xc = x[c];
+        x[c] = xc + omega * ((b[c] - off) / diag - xc);
     }
 }
 
@@ -733,7 +781,33 @@ int pressure_residual_solve(AtjupCtx* c, const AtjupSolveOpts* o, AtjupSolveStat
     // radial-line and column-mode systems have condition numbers ~1e5 -- but not the residual);
     // p += e. Stops at the tolerance, or when the residual no longer falls (it has reached the
     // rounding floor of an FP64 p, which is reported).
-    const int max_outer = 8;
+    if (o->mode == ATJUP_SOLVE_SOR) {
+        // point red-black SOR with omega, the residual checked every `check` sweeps
+        const double omega = (o->omega > 0.0 && o->omega < 2.0) ? o->omega : 1.0;
+        const int check = 50;
+        int sweeps = 0;
+        for (;;) {
+            residual_kernel<<<nb, RB, 0, stm>>>(b64, p64, V.b, c->solid, c->geo, S->yw, q, S->part);
+            finalize_kernel<<<1, 1, 0, stm>>>(S->part, nb, S->scal, 10, 0);
+            finalize_kernel<<<1, 1, 0, stm>>>(S->part + NRED, nb, S->scal, 12, 0);
+            c->launches += 3;
+            ATJUP_CUDA(cudaMemcpyAsync(S->hs, S->scal, sizeof(double) * 16, cudaMemcpyDeviceToHost, stm));
+            ATJUP_CUDA(cudaStreamSynchronize(stm));
+            rel = (bnorm > 0.0) ? std::sqrt(S->hs[10]) / bnorm : 0.0;
+            floor_rel = (bnorm > 0.0) ? 2.220446049250313e-16 * std::sqrt(S->hs[12]) / bnorm : 0.0;
+            if (!std::isfinite(rel)) { set_error("pressure_solve: non-finite residual"); return ATJUP_ERR_NONFINITE; }
+            if (rel <= o->rel_tol || sweeps >= o->max_iter) break;
+            const int n = std::min(check, o->max_iter - sweeps);
+            for (int t = 0; t < n; t++) {
+                sor_kernel<<<nb, RB, 0, stm>>>(b64, p64, c->solid, c->geo, S->yw, q, 0, omega);
+                sor_kernel<<<nb, RB, 0, stm>>>(b64, p64, c->solid, c->geo, S->yw, q, 1, omega);
+            }
+            c->launches += 2 * n;
+            sweeps += n;
+        }
+        total_it = sweeps;
+    }
+    const int max_outer = (o->mode == ATJUP_SOLVE_SOR) ? -1 : 8;
     for (int outer = 0; outer <= max_outer; outer++) {
         residual_kernel<<<nb, RB, 0, stm>>>(b64, p64, V.b, c->solid, c->geo, S->yw, q, S->part);
         finalize_kernel<<<1, 1, 0, stm>>>(S->part, nb, S->scal, 10, 0);

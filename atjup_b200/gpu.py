@@ -348,12 +348,17 @@ class GpuModel:
         _check(self.L.atjup_gpu_rk4_step(self.ctx, iter_n))
 
     def pressure_solver(self, mode=_p.SOLVE_SWEEPS, sweeps=None, omega=1.0, rel_tol=1e-10,
-                        max_iter=2000, precision=_p.PREC_FP64, external_rhs=False):
-        """PressureSolverJup::run (PressureSolver.h:144-766); returns AtjupSolveStats."""
+                        max_iter=2000, precision=_p.PREC_FP64, external_rhs=False,
+                        allow_not_converged=False):
+        """PressureSolverJup::run (PressureSolver.h:144-766); returns AtjupSolveStats. With
+        allow_not_converged an iteration cap reached (ATJUP_ERR_NOT_CONVERGED) returns the stats
+        instead of raising."""
         o = _p.AtjupSolveOpts(mode, sweeps if sweeps is not None else self.P.press_sweeps,
                               max_iter, precision, rel_tol, omega, int(external_rhs))
         st = _p.AtjupSolveStats()
-        _check(self.L.atjup_gpu_pressure_solve(self.ctx, ctypes.byref(o), ctypes.byref(st)))
+        rc = self.L.atjup_gpu_pressure_solve(self.ctx, ctypes.byref(o), ctypes.byref(st))
+        if not (allow_not_converged and rc == 4):
+            _check(rc)
         return st
 
     def set_solve_rhs(self, b) -> None:

@@ -69,7 +69,7 @@ TURB_K_EPSILON, TURB_K_OMEGA, TURB_K_OMEGA_SST = 0, 1, 2
 GAS_H2O, GAS_NH3, GAS_CH4 = 0, 1, 2
 GAS_IDS = {"H2O": GAS_H2O, "NH3": GAS_NH3, "CH4": GAS_CH4}
 
-SOLVE_SWEEPS, SOLVE_RESIDUAL = 0, 1
+SOLVE_SWEEPS, SOLVE_RESIDUAL, SOLVE_SOR = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 BC_RADIUS, BC_THETA, BC_PHI, BC_SOLID, BC_ALL = 1, 2, 4, 8, 15
 

@@ -2,34 +2,47 @@
 """Benchmark of ATJUP's time step on B200: one model iteration with the full physics.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload phys|dry] [--precision fp64|mixed]
+                    [--workload phys|dry|rk4-adjoint] [--precision fp64|mixed] [--no-extras]
 
 Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 shell (2.68 M
 cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
 on even iterations the red-black pressure pass, mixture density, radiation, the saturation
 adjustment of H2O, NH3 and CH4, the NH4SH equilibrium, precipitation, the k-omega SST closure
-update, the chemistry fluxes and the output diagnostics (Forces, Latent_Heat); every iteration the four RK4 stages of t, u, v, w, the 11
-species and k*, omega*, the boundary passes, the moist convective adjustment, the in-loop
-4th-order Shapiro filter of u, v, w, the column balance of v and the species clamp. The initial
-state follows the full-physics recipe (atjup_b200/synthetic.py: state + full_physics): vapour at
-90 % of saturation with U(0.95, 1.05)
-noise, k = 1e-4 m2/s2 x U(0.5, 1.5), omega = 1e-3 1/s x U(0.5, 1.5), the dynamics perturbations of
-the dry recipe; it is device-resident when the timed region starts. `--workload dry` times the
-dry dynamics iteration instead (microphysics, radiation, closure off). `--precision mixed` runs
-the mixed-precision RK step (AtjupParams.precision = ATJUP_PREC_MIXED: FP32 stage inputs and
-accumulators of the 17 fields, FP32 species and closure right-hand sides; FP64 time-level-n state,
-final update, dynamics right-hand side, pressure, level means, column balance and the loop's
-physics).
+update, the chemistry fluxes and the output diagnostics (Forces, Latent_Heat); every iteration
+the four RK4 stages of t, u, v, w, the 11 species and k*, omega*, the boundary passes, the moist
+convective adjustment, the in-loop 4th-order Shapiro filter of u, v, w, the column balance of v
+and the species clamp. `--workload dry` times the dry dynamics iteration instead (microphysics,
+radiation, closure off). `--precision mixed` runs the mixed-precision RK step
+(AtjupParams.precision = ATJUP_PREC_MIXED: FP32 stage inputs and accumulators of the 17 fields,
+FP32 species and closure right-hand sides; FP64 time-level-n state, final update, dynamics
+right-hand side, pressure, level means, column balance and the loop's physics).
+
+Initial state: the reference's own initial state with the configuration's seeded recipe applied
+(oracle/baseline_state.py: Gaussian noise on t, u, v, w; for full physics vapour at 90 % of
+saturation x U(0.95, 1.05), no condensate, seeded k and omega), produced once per run, untimed, by
+the reference built from its sources, and handed to this arm byte for byte; the reference arm
+and the CPU baseline start from the same bytes. It is device-resident when the timed region
+starts. Without the reference library the synthetic state of atjup_b200/synthetic.py stands in
+(the line's `data` says which).
 
 Prints one JSON line. `value` is seconds per step for the whole job (N replicas: max-over-ranks
 device time / (N * K)); `e2e` is the same metric through the public C ABI with host buffers
 (pinned), the host->device upload of the step's state and the device->host read of its result
 inside the timed region every step: through the asynchronous exchange (atjup_gpu_upload_async,
 atjup_gpu_apply_uploads, atjup_gpu_download_async), whose copies of consecutive steps overlap the
-compute, and (`e2e_serial`) through the synchronous atjup_gpu_upload / atjup_gpu_download. For the full-physics workload in FP64 the line also carries
-`mixed_precision`: the run continued for K more iterations in the mixed-precision RK step, timed
-the same way. With --impl reference the line times the reference's own CPU code of the same
-iteration (built from its sources into oracle/_ref) on this host's cores.
+compute, and (`e2e_serial`) through the synchronous atjup_gpu_upload / atjup_gpu_download. With
+--impl reference the line times the reference's own CPU code of the same iteration (built from
+its sources into oracle/_ref) on this host's cores.
+
+Sections of the default line besides the headline (N = 1; --no-extras drops them):
+* `mixed_precision`: the same K iterations from the same state in the mixed-precision RK step,
+  and the relative L2 per prognostic field of 200 mixed iterations against 200 FP64 iterations
+  from that state.
+* `poisson`: the isolated Poisson solve on the shell (seeded smoothed N(0, 1) right-hand side):
+  FP64 PCG, mixed PCG (FP32 preconditioner) and point red-black SOR with omega = 1.7 --
+  iterations, seconds per solve, relative residual, its FP64 rounding floor, HBM GB/s.
+* `adjoint`: adjoint+forward over forward time of 50 dry RK4 steps through the torch.autograd
+  binding, from the dry configuration's state, with the memory it holds.
 
 `roofline` is that of one RK stage. With full physics the species and closure kernels of a stage
 run on a second stream beside the dynamics kernel, so the stage (timing class `rk_group`: from the
@@ -153,7 +166,7 @@ def stage_roofline(prec, phys, per_class, peak):
 
 # DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step:
 # dram__bytes_read.sum + dram__bytes_write.sum of each stage launch in one ncu capture of this
-# workload on the 41x181x361 shell (profiles/stage_traffic_phys_41x181x361.md).
+# workload on the 41x181x361 shell.
 STAGE_TRAFFIC_PER_CELL = {
     ("fp64", "species_stage_kernel"): 560.1, ("fp64", "closure_stage_kernel"): 100.1,
     ("fp64", "rk_stage_kernel"): 199.4,
@@ -236,12 +249,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(workload, steps=3, warmup=1):
-    """The reference's own CPU iteration (oracle/_ref) timed on this host's cores."""
+REF_LIB = ROOT / "oracle" / "_ref" / "libatjup_ref.so"
+STATE_RECIPE = {
+    "phys": "the reference's own initial state (its initialisation, phys knobs) with the "
+            "full-physics recipe: Philox(20261203) noise on w, v, u, t; Philox(20261207) vapour at "
+            "90 % of saturation x U(0.95, 1.05), k, omega (oracle/baseline_state.py)",
+    "dry": "the reference's own initial state (its initialisation, dry knobs) with the dry "
+           "recipe: Philox(20261203) noise on w, v, u, t (oracle/baseline_state.py)",
+}
+
+
+def cpu_baseline(workload, steps=8, warmup=2):
+    """The reference's own CPU iteration (oracle/_ref) timed on this host's cores, from the same
+    seeded initial state as the GPU arm."""
     cmd = [sys.executable, str(ROOT / "oracle" / "ref_bench.py"), "--steps", str(steps),
            "--warmup", str(warmup)] + (["--phys"] if workload == "phys" else [])
     try:
-        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600).stdout
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=900).stdout
         d = json.loads(out.strip().splitlines()[-1])
     except Exception as e:
         return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
@@ -252,7 +276,8 @@ def cpu_baseline(workload, steps=3, warmup=1):
     return {"value": d["s_per_step"], "unit": UNIT, "cores": d["threads"], "kind": "reference",
             "sample": f"{d['steps']} {'full-physics' if workload == 'phys' else 'dry'} iterations "
                       f"of the reference (built at -O3 from its sources, OpenMP {d['threads']} "
-                      f"threads) after {warmup} warm-up, on its own initial state"}
+                      f"threads) after {warmup} warm-up, from {d['state']}",
+            "state": d["state"]}
 
 
 def run_reference(args, rank, world):
@@ -267,32 +292,189 @@ def run_reference(args, rank, world):
             "value": v, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": f"the reference's own initial state ({args.workload} knobs)",
+            "data": cb["state"],
             "config": CONFIGS[args.workload],
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def run_adjoint(args):
-    """K dry RK4 steps forward and their adjoint through the torch.autograd binding (each step
-    keeps its input as the checkpoint and the adjoint recomputes its stages), on the 41x181x361
-    shell: the time of forward with checkpoints + backward over the time of K plain forward steps,
-    and the device memory the chain holds. One GPU."""
+# ---- the benchmark state ---------------------------------------------------------------------
+
+MICRO_RENAME = {"rad_F_int": "F_int", "rad_S_solar": "S_solar", "rad_albedo_bond": "albedo_bond",
+                "rad_x_H2": "x_H2", "rad_x_He": "x_He"}
+
+
+def reference_state(workload, rank, dist):
+    """The configuration's seeded initial state as a dict of arrays: the reference's own
+    initialisation with the seeded recipe applied, produced once per run, untimed, by
+    oracle/baseline_state.py (rank 0 writes it, every rank reads it), so that this arm and the
+    reference arm start from the same bytes. None when the reference library is not built."""
     import numpy as np
+    path = Path(tempfile.gettempdir()) / f"atjup_bench_state_{workload}_{os.getpid() if dist is None else 'dist'}.npz"
+    ok = [REF_LIB.exists()]
+    if rank == 0 and ok[0]:
+        cmd = [sys.executable, str(ROOT / "oracle" / "baseline_state.py"), str(path),
+               "--config", workload]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        ok[0] = r.returncode == 0 and path.exists()
+    if dist is not None:
+        dist.barrier()
+    if not ok[0] and rank == 0:
+        return None
+    if not path.exists():
+        return None
+    with np.load(path) as z:
+        d = {k: z[k] for k in z.files}
+    if dist is not None:
+        dist.barrier()
+    if rank == 0:
+        path.unlink(missing_ok=True)
+    return d
+
+
+def model_inputs(d, workload):
+    """(params, physics, micro, mca, grid, fields) of a state dict written by
+    oracle/baseline_state.py."""
+    from atjup_b200.params import resolve_mca, resolve_micro, resolve_params, resolve_physics
+    env = PHYS_ENV if workload == "phys" else DRY_ENV
+    consts = {k[6:]: float(v) for k, v in d.items() if k.startswith("const_")}
+    im, jm, km = d["in_t"].shape
+    P = resolve_params(env, im=im, jm=jm, km=km, constants=consts)
+    grid = {k[5:]: v for k, v in d.items() if k.startswith("grid_")}
+    fields = {k[3:]: v for k, v in d.items() if k.startswith("in_")}
+    if workload != "phys":
+        return P, None, None, None, grid, fields
+    P.has_nue = 1
+    P.has_heating = 1
+    MC = resolve_micro(env, {MICRO_RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items()
+                             if k.startswith("micro_")},
+                       {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
+    pc = {k[5:]: float(v) for k, v in d.items() if k.startswith("phys_")}
+    pc["abl_height"] = float(d["knobd_abl_height"])
+    return P, resolve_physics(env, pc), MC, resolve_mca(env), grid, fields
+
+
+def synthetic_inputs(workload, rank):
+    """Fallback when the reference is not built: the synthetic state of atjup_b200.synthetic
+    (the reference's grid shapes and value ranges, the same seeded recipes)."""
+    from atjup_b200 import synthetic
+    from atjup_b200.params import (DEFAULT_GASES, resolve_mca, resolve_micro, resolve_params,
+                                   resolve_physics)
+    phys = workload == "phys"
+    P = resolve_params(PHYS_ENV if phys else DRY_ENV, im=IM, jm=JM, km=KM)
+    if (IM, JM, KM) != (41, 181, 361):
+        import math
+        P.dthe = math.pi / (JM - 1)
+        P.dphi = 2.0 * math.pi / (KM - 1)
+    s = synthetic.state(IM, JM, KM, seed=20261203 + rank)
+    grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
+    fields = {k: v for k, v in s.items() if k not in grid}
+    if not phys:
+        return P, None, None, None, grid, fields
+    P.has_nue = 1
+    P.has_heating = 1
+    fields.update(synthetic.full_physics(s, DEFAULT_GASES, seed=20261207 + rank))
+    return (P, resolve_physics(PHYS_ENV), resolve_micro(PHYS_ENV), resolve_mca(PHYS_ENV), grid,
+            fields)
+
+
+def build_model(P, PH, MC, MCA, grid, fields):
+    from atjup_b200.gpu import GpuModel
+    m = GpuModel(P, grid)
+    if PH is not None:
+        m.set_physics(PH, fields["layer_heights"])
+        m.set_micro(MC)
+        m.set_mca(MCA)
+    m.upload_state(fields)
+    return m
+
+
+# ---- config 1: the isolated Poisson solve ----------------------------------------------------
+
+def poisson_section(m, stream):
+    """The isolated Poisson solve on the model's shell (seeded N(0, 1) right-hand side smoothed by
+    3 passes of the 1-2-1 filter per direction, its incompatible part removed by the solver):
+    FP64 PCG, mixed PCG (FP32 preconditioner) and point red-black SOR with omega = 1.7, each
+    timed with CUDA events on the library's stream."""
     import torch
 
     from atjup_b200 import synthetic
+    from atjup_b200.params import PREC_FP64, PREC_MIXED, SOLVE_RESIDUAL, SOLVE_SOR
+    im, jm, km = m.shape
+    b = synthetic.poisson_rhs(im, jm, km)
+    m.set_solve_rhs(b)
+    n = im * jm * km
+    peak, kind = measured_peak_hbm()
+
+    def timed(**kw):
+        m.pressure_solver(**kw)                      # warm: set-up and first-touch
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m.synchronize()
+        ev0.record(stream)
+        st = m.pressure_solver(**kw)
+        ev1.record(stream)
+        ev1.synchronize()
+        return st, ev0.elapsed_time(ev1) / 1e3
+
+    out = {"problem": "A p = b on the 41x181x361 shell with the obstacle: the reference's folded "
+                      "all-Neumann operator (PressureSolver.h:144-766); b seeded N(0, 1) smoothed "
+                      "by 3 passes of 1-2-1 per direction, made compatible by removing its "
+                      "component along the operator's left null vector",
+           "target": "relative residual 1e-10, or <= 8 x the rounding floor of an FP64 p "
+                     "(rel_floor) where that is above 1e-10"}
+    # PCG: per iteration the operator, the update, the radial line solve, the inverse DFT and the
+    # direction touch N (23 b + 1) bytes in FP64 (b = 8); the mixed form keeps z and the line
+    # factors in FP32: N (153 + 1) bytes
+    for name, prec, bpc in (("fp64", PREC_FP64, 23 * 8 + 1), ("mixed", PREC_MIXED, 154)):
+        st, t = timed(mode=SOLVE_RESIDUAL, rel_tol=1e-10, max_iter=5000, precision=prec,
+                      external_rhs=True, allow_not_converged=True)
+        gbs = st.iterations * n * bpc / t / 1e9 if t > 0 else None
+        out[name] = {"s_per_solve": t, "iterations": st.iterations,
+                     "refinement_steps": st.inner_solves, "rel_residual": st.rel_residual,
+                     "rel_floor": st.rel_floor,
+                     "converged": bool(st.rel_residual <= max(1e-10, 8 * st.rel_floor)),
+                     "hbm_gbs": gbs, "hbm_frac": gbs / peak if gbs else None,
+                     "algorithmic_bytes_per_iteration": n * bpc}
+    # point SOR, omega = 1.7: two sweep caps give the contraction per sweep, hence the sweeps
+    # 1e-10 would take; each sweep moves N (3 b + 1) bytes
+    res = {}
+    for cap in (500, 1000):
+        st, t = timed(mode=SOLVE_SOR, omega=1.7, rel_tol=1e-10, max_iter=cap,
+                      external_rhs=True, allow_not_converged=True)
+        res[cap] = (st, t)
+    (s1, _), (s2, t2) = res[500], res[1000]
+    import math
+    rate = (s2.rel_residual / s1.rel_residual) ** (1.0 / 500) if s1.rel_residual > 0 else None
+    proj = (1000 + math.log(1e-10 / s2.rel_residual) / math.log(rate)
+            if rate is not None and 0 < rate < 1 else None)
+    gbs = s2.iterations * n * 25 / t2 / 1e9
+    out["sor_omega_1.7"] = {"sweeps": s2.iterations, "s": t2, "s_per_sweep": t2 / s2.iterations,
+                            "rel_residual": s2.rel_residual, "rel_residual_at_500": s1.rel_residual,
+                            "contraction_per_sweep": rate, "projected_sweeps_to_1e-10": proj,
+                            "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                            "algorithmic_bytes_per_sweep": n * 25}
+    out["peak"] = {"hbm_gbs": peak, "kind": kind}
+    return out
+
+
+# ---- config 4: the adjoint -------------------------------------------------------------------
+
+def adjoint_section(P, grid, fields, K):
+    """K RK4 steps of the dry dynamics forward and their adjoint through the torch.autograd
+    binding (each step keeps its input as the checkpoint and the adjoint recomputes its stages):
+    the time of forward with checkpoints + backward over the time of K plain forward steps, and
+    the device memory the chain holds. Loss J = sum_theta sin(colatitude) (zonal-mean w at the top
+    integrated level - u_ref)^2, u_ref = sum_{n=1..8} a_n sin(n theta), a_n seeded U(-50, 150) m/s."""
+    import numpy as np
+    import torch
+
     from atjup_b200.autograd import rk4_steps
     from atjup_b200.gpu import GpuModel
-    from atjup_b200.params import resolve_params
 
-    K = args.steps
-    P = resolve_params(DRY_ENV, im=IM, jm=JM, km=KM)
-    s = synthetic.state(IM, JM, KM, seed=20261203)
-    grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
     m = GpuModel(P, grid)
-    m.upload_state({k: v for k, v in s.items() if k not in grid})
+    m.upload_state(fields)
+    im, jm, km = m.shape
     y0 = m.state_tensors()
     stream = torch.cuda.ExternalStream(m.stream_handle())
     the = torch.tensor(grid["the"], device="cuda")
@@ -307,7 +489,7 @@ def run_adjoint(args):
     def chain():
         x = [t.clone().requires_grad_() for t in y0]
         out = rk4_steps(m, *x, steps=K)
-        zm = out[3][IM - 2, :, : KM - 1].mean(dim=1)
+        zm = out[3][im - 2, :, : km - 1].mean(dim=1)
         J = (torch.sin(the) * (zm - uref) ** 2).sum()
         J.backward()
         return J
@@ -328,26 +510,42 @@ def run_adjoint(args):
         chain()
     fwd_wall, fwd_dev = timed(forward_plain)
     torch.cuda.reset_peak_memory_stats()
-    free0 = torch.cuda.mem_get_info()[0]
+    base = torch.cuda.memory_allocated()
     ad_wall, _ = timed(chain)
-    torch_peak = torch.cuda.max_memory_allocated()
-    lib_scratch = 30 * IM * JM * m.field_ptr("t")[1] * 8
+    torch_peak = torch.cuda.max_memory_allocated() - base
+    lib_scratch = 30 * im * jm * m.field_ptr("t")[1] * 8
     m.close()
-    line = {
-        "metric": f"adjoint+forward / forward time, {K} dry RK4 steps (41x181x361, FP64)",
-        "value": ad_wall / fwd_wall, "unit": "x", "n_gpus": 1, "steps": K, "warmup": 2,
-        "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded dry state)",
-        "config": {"workload": "rk4-adjoint: K RK4 steps of the dry dynamics through "
-                               "atjup_b200.autograd.RK4Step, loss = sin-weighted squared error of "
-                               "the top level's zonal-mean w against a seeded 8-mode jet",
-                   "grid": "41x181x361", "checkpoints": "each step's input (t, u, v, w)"},
+    return {
+        "metric": f"adjoint+forward / forward time, {K} dry RK4 steps",
+        "ratio": ad_wall / fwd_wall, "steps": K,
+        "what": "the RK4 step of the dry dynamics (t, u, v, w right-hand sides, level mean, "
+                "hydrostatic integral) through atjup_b200.autograd.RK4Step; checkpoints: each "
+                "step's input",
         "forward_ms_per_step": fwd_wall / K * 1e3,
         "forward_device_ms_per_step": fwd_dev / K * 1e3,
         "adjoint_and_forward_ms_per_step": ad_wall / K * 1e3,
-        "peak_bytes": {"torch_tensors": torch_peak, "library_scratch": lib_scratch,
-                       "device_free_at_start": free0},
+        "peak_bytes": {"torch_tensors_above_start": torch_peak, "library_scratch": lib_scratch},
     }
+
+
+def run_adjoint(args):
+    """--workload rk4-adjoint: the adjoint section alone, as its own JSON line."""
+    d = reference_state("dry", 0, None)
+    if d is not None:
+        P, _, _, _, grid, fields = model_inputs(d, "dry")
+        data = STATE_RECIPE["dry"]
+    else:
+        P, _, _, _, grid, fields = synthetic_inputs("dry", 0)
+        data = "synthetic (seeded dry state; the reference is not built here)"
+    a = adjoint_section(P, grid, fields, args.steps)
+    line = {"metric": a.pop("metric"), "value": a.pop("ratio"), "unit": "x", "n_gpus": 1,
+            "steps": args.steps, "warmup": 2, "higher_is_better": False, "dtype": "f64",
+            "data": data, "config": {"workload": "rk4-adjoint", "grid": "41x181x361"}, **a}
     print(json.dumps(line))
+
+
+PROGNOSTIC = ("t", "u", "v", "w", "p_dyn", "h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3",
+              "nh3_cloud", "nh3_ice", "ch4", "ch4_cloud", "ch4_ice", "nh4sh", "tke", "dis")
 
 
 def main():
@@ -357,11 +555,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the Poisson, adjoint and mixed-precision accuracy sections")
     ap.add_argument("--workload", default="phys", choices=["phys", "dry", "rk4-adjoint"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None,
-                    help="IMxJMxKM of a smaller shell, for profiling only (the metric is quoted "
-                         "on 41x181x361)")
+                    help="IMxJMxKM of a smaller synthetic shell, for profiling only (the metric "
+                         "is quoted on 41x181x361)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -377,10 +577,7 @@ def main():
     import numpy as np
     import torch
 
-    from atjup_b200 import synthetic
-    from atjup_b200.gpu import GpuModel
-    from atjup_b200.params import (DEFAULT_GASES, FIELD_IDS, PREC_FP64, PREC_MIXED, SCALARS,
-                                   resolve_mca, resolve_micro, resolve_params, resolve_physics)
+    from atjup_b200.params import FIELD_IDS, PREC_FP64, PREC_MIXED, SCALARS
     from atjup_b200.replicas import max_over_ranks, whole_job_seconds_per_step
 
     torch.cuda.set_device(local_rank)
@@ -389,33 +586,24 @@ def main():
         import torch.distributed as dist_mod
         from datetime import timedelta
         dist = dist_mod
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     phys = args.workload == "phys"
     global IM, JM, KM, N_CELLS
     if args.grid:
-        import math
         IM, JM, KM = (int(x) for x in args.grid.lower().split("x"))
         N_CELLS = IM * JM * KM
-    P = resolve_params(PHYS_ENV if phys else DRY_ENV, im=IM, jm=JM, km=KM)
-    if args.grid:
-        P.dthe = math.pi / (JM - 1)
-        P.dphi = 2.0 * math.pi / (KM - 1)
-    s = synthetic.state(IM, JM, KM, seed=20261203 + rank)
-    grid = {k: s[k] for k in ("rad", "the", "solid", "topo", "cell_vbar0", "cell_ubar0")}
-    fields = {k: v for k, v in s.items() if k not in grid}
-    if phys:
-        P.has_nue = 1
-        P.has_heating = 1
-        fields.update(synthetic.full_physics(s, DEFAULT_GASES, seed=20261207 + rank))
-    m = GpuModel(P, grid)
-    if phys:
-        m.set_physics(resolve_physics(PHYS_ENV), fields["layer_heights"])
-        m.set_micro(resolve_micro(PHYS_ENV))
-        m.set_mca(resolve_mca(PHYS_ENV))
-    if args.precision == "mixed":
-        m.set_precision(PREC_MIXED)
-    m.upload_state(fields)
+    d = None if args.grid else reference_state(args.workload, rank, dist)
+    if d is not None:
+        P, PH, MC, MCA, grid, fields = model_inputs(d, args.workload)
+        data = STATE_RECIPE[args.workload]
+    else:
+        P, PH, MC, MCA, grid, fields = synthetic_inputs(args.workload, rank)
+        data = ("synthetic (seeded; shapes and value ranges of the model's initial state"
+                + (", full-physics recipe" if phys else "") + "; the reference is not built here)")
+    m = build_model(P, PH, MC, MCA, grid, fields)
+    prec0 = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    m.set_precision(prec0)
     # events are recorded on the library's own stream; no torch stream is created, so the process
     # holds only the library's streams and each gets a hardware queue of its own
     stream = torch.cuda.ExternalStream(m.stream_handle())
@@ -426,11 +614,11 @@ def main():
         it[0] += 1
         m.step(it[0], it[0] == 1)
 
-    for _ in range(args.warmup):
-        step()
-    m.synchronize()
-    if m.nonfinite_count() != 0:
-        raise SystemExit("non-finite state after warm-up")
+    def restart(prec):
+        """the state back to the configuration's initial state, iteration 1 next"""
+        m.set_precision(prec)
+        m.upload_state(fields)
+        it[0] = 0
 
     def barrier():
         if dist is not None:
@@ -462,30 +650,49 @@ def main():
         m.timing(False)
         return max_over_ranks(t_ms, device="cuda"), per_class, launches, clk
 
-    t_ms, per_class, launches, clk = timed_region(args.steps)
+    def warm_and_time(prec):
+        restart(prec)
+        for _ in range(args.warmup):
+            step()
+        m.synchronize()
+        if m.nonfinite_count() != 0:
+            raise SystemExit("non-finite state after warm-up")
+        return timed_region(args.steps)
+
+    t_ms, per_class, launches, clk = warm_and_time(prec0)
     value = whole_job_seconds_per_step(t_ms / 1e3, args.steps, world)
 
-    # ---- the same iterations in the mixed-precision RK step, continuing the run ----
+    # ---- the same iterations in the mixed-precision RK step, from the same state ----
     mixed = None
     if phys and args.precision == "fp64":
-        m.set_precision(PREC_MIXED)
-        for _ in range(2):
-            step()
-        mt_ms, mper, _, mclk = timed_region(args.steps)
-        m.set_precision(PREC_FP64)
+        mt_ms, mper, _, mclk = warm_and_time(PREC_MIXED)
         mixed = {"value": whole_job_seconds_per_step(mt_ms / 1e3, args.steps, world),
                  "unit": UNIT, "ms_per_step": mt_ms / args.steps, "dtype": "f32+f64",
                  "precision": PREC_CONFIG["mixed"],
-                 "accuracy": "relative L2 vs the FP64 step after 200 iterations of this workload "
-                             "<= 1e-5 per prognostic field, except the condensates bounded by "
-                             "the FP64 step's own sensitivity to one FP32 rounding of its input "
-                             "(tests/test_mixed.py)",
                  "stage_roofline": mper,
                  "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
                                                  sorted(mper.items(), key=lambda kv: -kv[1][0])},
                  "clocks": mclk}
+        if not args.no_extras:
+            # accuracy: 200 iterations of each from the configuration's state, relative L2 per
+            # field of the mixed run against the FP64 run
+            n_acc = 200
+            snaps = {}
+            for prec in (PREC_FP64, PREC_MIXED):
+                restart(prec)
+                for _ in range(n_acc):
+                    step()
+                snaps[prec] = {n: m.download(n) for n in PROGNOSTIC}
+            rel = {}
+            for n in PROGNOSTIC:
+                a, b = snaps[PREC_FP64][n], snaps[PREC_MIXED][n]
+                nb = float(np.linalg.norm(a))
+                rel[n] = float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(b))
+            mixed["rel_l2_vs_fp64_after_200"] = rel
+            mixed["fields_above_1e-5"] = sorted(k for k, v in rel.items() if v > 1e-5)
 
     # ---- end to end through the C ABI with pinned host buffers ----
+    restart(prec0)
     names = ["t", "u", "v", "w", "p_dyn"] + (list(SCALARS) if phys else [])
     host_in = {n: torch.from_numpy(np.ascontiguousarray(fields[n])).pin_memory() for n in names}
     host_out = {n: torch.empty((IM, JM, KM), dtype=torch.float64).pin_memory() for n in names}
@@ -548,8 +755,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-        "data": "synthetic (seeded; shapes and value ranges of the model's initial state"
-                + (", full-physics recipe" if phys else "") + ")",
+        "data": data,
         "config": {**CONFIGS[args.workload], "precision": PREC_CONFIG[args.precision]},
         "roofline": roof,
         "device_ms_per_step_by_class": {k: round(v[0] / args.steps, 4) for k, v in
@@ -567,13 +773,22 @@ def main():
     if mixed is not None:
         mixed["stage_roofline"] = stage_roofline("mixed", phys, mixed["stage_roofline"], peak)
         line["mixed_precision"] = mixed
+    if world == 1 and not args.no_extras and not args.grid:
+        line["poisson"] = poisson_section(m, stream)
+    m.close()
+    if world == 1 and not args.no_extras and not args.grid:
+        dd = reference_state("dry", 0, None) if d is not None else None
+        if dd is not None:
+            Pd, _, _, _, gd, fd = model_inputs(dd, "dry")
+        else:
+            Pd, _, _, _, gd, fd = synthetic_inputs("dry", 0)
+        line["adjoint"] = adjoint_section(Pd, gd, fd, 50)
     if dist is not None:
         dist.barrier()
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and not args.grid:
             line["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(line))
-    m.close()
     if dist is not None:
         dist.destroy_process_group()
 

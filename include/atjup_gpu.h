@@ -73,7 +73,10 @@ enum { ATJUP_F2_VEL_STAR = 0, ATJUP_F2_COUNT };
 /* ---- solver modes for atjup_gpu_pressure_solve ---- */
 enum {
     ATJUP_SOLVE_SWEEPS = 0,    /* the reference: n red-black Gauss-Seidel sweeps, no residual   */
-    ATJUP_SOLVE_RESIDUAL = 1   /* same discrete operator, iterated to a relative residual       */
+    ATJUP_SOLVE_RESIDUAL = 1,  /* same discrete operator, iterated to a relative residual       */
+    ATJUP_SOLVE_SOR = 2        /* same operator by point red-black SOR with opts->omega, up to   */
+                               /* max_iter sweeps, the residual checked every 50 sweeps; returns */
+                               /* ATJUP_ERR_NOT_CONVERGED (stats filled) at the sweep cap        */
 };
 enum { ATJUP_PREC_FP64 = 0, ATJUP_PREC_MIXED = 1 };
 
@@ -246,11 +249,15 @@ int atjup_gpu_balance_column_v(AtjupCtx* ctx, double* vshift);
 /* The column balance of v for callers that cannot allocate device memory. No counterpart in the
  * reference: it computes what atjup_gpu_balance_column_v computes, on the caller's own device
  * buffers -- v (in/out, [im][jm][pitch] doubles), i_topo ([jm * km] int32), rad ([im]) -- and keeps
- * its scratch in a fixed file-scope device array instead of allocating. For hosts whose memory is
- * preallocated, code inside stream capture, or embeddings that must not fail on an allocation.
+ * its scratch in a fixed file-scope device array instead of allocating. For host models that hand
+ * the GPU layer one memory pool sized at start-up and allow no allocation after it, and for
+ * embeddings that must not fail part-way through a run on an out-of-memory allocation.
  * Limits: jm <= ATJUP_NOALLOC_MAX_J, pitch <= ATJUP_NOALLOC_MAX_PITCH, else ATJUP_ERR_ARG. The
- * first call on each device looks up the array's address (make it before any stream capture).
- * Calls share the array: calls that overlap on the GPU race. stream: a cudaStream_t or NULL. */
+ * first call on each device looks up the array's device address (cudaGetSymbolAddress) and keeps
+ * it for the life of the process; make that first call before any stream capture. The kept
+ * address does not survive cudaDeviceReset: after a reset, do not call this entry point again in
+ * the same process. Calls share the array: calls that overlap on the GPU race.
+ * stream: a cudaStream_t or NULL. */
 #define ATJUP_NOALLOC_MAX_J 256
 #define ATJUP_NOALLOC_MAX_PITCH 512
 int atjup_gpu_balance_column_v_noalloc(double* v, const int32_t* i_topo, const double* rad,

@@ -2,18 +2,19 @@
 
 TEST AND CPU-BASELINE INFRASTRUCTURE: used only by bench.py's CPU legs (the reference arm and the
 cpu_baseline figure). Runs oracle/_ref/libatjup_ref.so -- the unmodified reference built from its
-sources -- in this process: the reference's initialisation (untimed), `warmup` iterations
-(untimed), then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule -- the dry
-configuration, or with --phys the full physics (the closure, radiation, precipitation, the
-saturation adjustments, the NH4SH equilibrium and the chemistry block on; moist convective
-adjustment off) -- each timed by wall clock on the host. Prints one JSON line.
+sources -- in this process: the reference's initialisation with the benchmark configuration's
+seeded initial state applied (oracle/baseline_state.py; untimed), `warmup` iterations (untimed),
+then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule -- the dry configuration, or
+with --phys the reference's default full physics (the k-omega SST closure, radiation,
+precipitation, the saturation adjustments, the NH4SH equilibrium, the chemistry block and the
+moist convective adjustment every iteration, as baseline_state.PHYS_ENV sets) -- each timed by
+wall clock on the host. Prints one JSON line.
 
     python oracle/ref_bench.py --steps K --warmup W [--threads T] [--phys]
 """
 from __future__ import annotations
 
 import argparse
-import ctypes
 import json
 import os
 import sys
@@ -22,20 +23,8 @@ import time
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
 LIB = HERE / "_ref" / "libatjup_ref.so"
-
-DRY_ENV = {
-    "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
-    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
-    "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
-    "ATJUP_RESTART_STRIDE": "0", "ATJUP_VTK_STRIDE": "100000", "ATJUP_PANORAMA_STRIDE": "100000",
-}
-
-
-# the reference's default full physics: closure, radiation, precipitation, NH4SH equilibrium and
-# the moist convective adjustment every iteration
-PHYS_ENV = {**DRY_ENV, "ATJUP_TURB": "1", "ATJUP_PRECIP": "1", "ATJUP_RADIATION": "1",
-            "ATJUP_NH4SH_EQ": "1", "ATJUP_MCA": "1"}
 
 
 def main():
@@ -48,20 +37,22 @@ def main():
     if not LIB.exists():
         print(json.dumps({"unavailable": f"{LIB} not built"}))
         return
-    os.environ.update(PHYS_ENV if a.phys else DRY_ENV)
+    import baseline_state as BS
+    config = "phys" if a.phys else "dry"
     threads = a.threads or os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    L = ctypes.CDLL(str(LIB))
     out_dir = tempfile.mkdtemp(prefix="atjup_refbench_")
-    L.ref_quiet(1)
     t0 = time.perf_counter()
-    rc = L.ref_create((out_dir + "/run").encode(), threads)
-    t_init = time.perf_counter() - t0
-    if rc != 0:
-        L.ref_quiet(0)
-        print(json.dumps({"unavailable": f"ref_create rc={rc}"}))
+    try:
+        ref = BS.make(config, out_dir + "/run", threads=threads)
+    except Exception as e:   # noqa: BLE001 -- reported as the arm's unavailability
+        print(json.dumps({"unavailable": f"reference initialisation failed: {e}"}))
         return
+    t_init = time.perf_counter() - t0
+    L = ref.L
     times = []
+    rc = 0
+    L.ref_quiet(1)
     for it in range(1, a.warmup + a.steps + 1):
         t0 = time.perf_counter()
         rc = L.ref_iteration(it, 1 if it == 1 else 0, 0 if a.phys else 1)
@@ -75,7 +66,8 @@ def main():
         print(json.dumps({"unavailable": f"ref_iteration rc={rc}"}))
     else:
         print(json.dumps({"s_per_step": sum(times) / len(times), "steps": len(times),
-                          "step_times": times, "threads": threads, "init_s": t_init}))
+                          "step_times": times, "threads": threads, "init_s": t_init,
+                          "state": BS.describe(config)}))
     sys.stdout.flush()
     os._exit(0)
 

@@ -58,3 +58,37 @@ def gpu_moist_model(P, PH, MC, g, f):
     m.set_micro(MC)
     m.upload_state(f)
     return m
+
+
+def baseline_case(config: str, iters: int):
+    """The reference from a benchmark configuration's seeded initial state
+    (oracle/baseline_state.py), run `iters` iterations: (dump, params, physics, micro, mca, grid,
+    fields). physics, micro and mca are None for the dry configuration."""
+    import baseline_state as BS
+    from atjup_b200.params import resolve_mca
+    env = BS.ENVS[config]
+    if config == "dry":
+        d = ref_dump("--baseline", "dry", "--iters", str(iters))
+        return d, dump_params(d, env=env), None, None, None, dump_grid(d), dump_fields(d)
+    d = ref_dump("--baseline", "phys", "--phys-iters", str(iters))
+    P = dump_params(d, env=env)
+    P.has_nue = 1
+    P.has_heating = 1
+    MC = resolve_micro(env, {RENAME.get(k[6:], k[6:]): float(v) for k, v in d.items()
+                             if k.startswith("micro_")},
+                       {g: tuple(d["gas_" + g]) for g in ("H2O", "NH3", "CH4")})
+    consts = {k[5:]: float(v) for k, v in d.items() if k.startswith("phys_")}
+    consts["abl_height"] = float(d["knobd_abl_height"])
+    return (d, P, resolve_physics(env, consts), MC, resolve_mca(env), dump_grid(d),
+            dump_fields(d))
+
+
+def gpu_baseline_model(P, PH, MC, MCA, g, f):
+    from atjup_b200.gpu import GpuModel
+    m = GpuModel(P, g)
+    if PH is not None:
+        m.set_physics(PH, f["layer_heights"])
+        m.set_micro(MC)
+        m.set_mca(MCA)
+    m.upload_state(f)
+    return m

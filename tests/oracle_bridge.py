@@ -11,6 +11,10 @@ import numpy as np
 
 from atjup_b200.params import AtjupParams, resolve_params
 
+import sys as _sys
+_sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+from ref_model import RefModel  # noqa: E402
+
 ROOT = Path(__file__).resolve().parents[1]
 ORACLE_SO = ROOT / "oracle" / "liboracle.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libatjup_ref.so"
@@ -129,67 +133,9 @@ class Oracle:
         return out
 
 
-class Reference:
-    """The unmodified reference (oracle/_ref/libatjup_ref.so), one model per process."""
-
-    def __init__(self, env: dict, out_dir: str, threads: int = 0, zero_species: bool = True):
-        os.environ.update(env)
-        if not REF_SO.exists():
-            raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref)")
-        L = ctypes.CDLL(str(REF_SO))
-        L.ref_scalar.restype = ctypes.c_double
-        L.ref_knob_d.restype = ctypes.c_double
-        L.ref_balance_v.restype = ctypes.c_double
-        self.L = L
-        L.ref_quiet(1)
-        rc = L.ref_create(out_dir.encode(), threads)
-        L.ref_quiet(0)
-        if rc != 0:
-            raise RuntimeError(f"ref_create failed rc={rc}")
-        im, jm, km = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        L.ref_dims(ctypes.byref(im), ctypes.byref(jm), ctypes.byref(km))
-        self.shape = (im.value, jm.value, km.value)
-        if zero_species:
-            z = np.zeros(self.shape)
-            for n in ("h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3", "nh3_cloud", "nh3_ice",
-                      "ch4", "ch4_cloud", "ch4_ice", "nh4sh", "h2on", "h2o_cloudn", "h2o_icen",
-                      "h2sn", "nh3n", "nh3_cloudn", "nh3_icen", "ch4n", "ch4_cloudn", "ch4_icen",
-                      "nh4shn"):
-                self.set(n, z)
-
-    def scalar(self, n):
-        return self.L.ref_scalar(n.encode())
-
-    def get(self, n):
-        a = np.empty(self.shape)
-        if self.L.ref_get3(n.encode(), a.ctypes.data_as(ctypes.c_void_p)) != 0:
-            raise KeyError(n)
-        return a
-
-    def set(self, n, a):
-        a = np.ascontiguousarray(a, dtype=np.float64)
-        if self.L.ref_set3(n.encode(), a.ctypes.data_as(ctypes.c_void_p)) != 0:
-            raise KeyError(n)
-
-    def get1(self, n):
-        cap = self.shape[0] * self.shape[1] * self.shape[2]
-        a = np.empty(cap)
-        m = self.L.ref_get1(n.encode(), a.ctypes.data_as(ctypes.c_void_p), cap)
-        if m < 0:
-            raise KeyError(n)
-        return a[:m].copy()
-
-    def topo(self):
-        a = np.empty(self.shape[1] * self.shape[2], dtype=np.int32)
-        self.L.ref_get_topo(a.ctypes.data_as(ctypes.c_void_p))
-        return a.reshape(self.shape[1], self.shape[2])
-
-    def quiet(self, fn, *args):
-        self.L.ref_quiet(1)
-        try:
-            return fn(*args)
-        finally:
-            self.L.ref_quiet(0)
+class Reference(RefModel):
+    """The unmodified reference (oracle/_ref/libatjup_ref.so), one model per process, with the
+    conversions the tests need (AtjupParams, grid and field dicts)."""
 
     def params(self, env: dict | None = None) -> AtjupParams:
         """AtjupParams with the model's own constants (the knobs resolved from env)."""

@@ -372,9 +372,38 @@ def main():
                          "step from the initial state +- EPS d (t, u, v, w and their n copies)")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
+    ap.add_argument("--baseline", default=None, choices=("dry", "phys"),
+                    help="start from the benchmark configuration's seeded initial state "
+                         "(oracle/baseline_state.py) with its knobs: dry with --iters, "
+                         "phys (the reference's default physics) with --phys-iters")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
+    if a.baseline:
+        import baseline_state as BS
+        ref = BS.make(a.baseline, out_dir + "/run", threads=a.threads, cls=Reference,
+                      env_extra=dict(kv.split("=", 1) for kv in a.env))
+        data = {}
+        BS.record(ref, data, moist=(a.baseline == "phys"))
+        if a.baseline == "phys":
+            iters = a.phys_iters
+            for it in range(1, iters + 1):
+                rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 0)
+                if rc != 0:
+                    raise SystemExit(f"ref_iteration rc={rc}")
+                if it in (1, iters):
+                    for n in ITER_FIELDS:
+                        data[f"it{it}_{n}"] = ref.get(n)
+        else:
+            for it in range(1, a.iters + 1):
+                rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 1)
+                if rc != 0:
+                    raise SystemExit(f"ref_iteration rc={rc}")
+            for n in DYN_FIELDS:
+                data["out_" + n] = ref.get(n)
+        np.savez(a.out, **data)
+        sys.stdout.flush()
+        os._exit(0)
     env = dict(PHYS_ENV) if (a.rk4_phys or a.turb or a.bc) else dict(DRY_ENV)
     if a.micro or a.phys_iters or a.load_restart or a.mca:
         env = dict(MOIST_ENV)

@@ -1,0 +1,86 @@
+"""The two benchmark configurations from their own seeded initial states, against the reference.
+
+Each state is the reference's own initial state with the configuration's seeded recipe applied
+on the reference side (oracle/baseline_state.py): the dry configuration's Gaussian noise on
+t, u, v, w (none inside the obstacle), and for full physics also vapour at 90 % of saturation
+times U(0.95, 1.05), no condensate, seeded k* and omega*. The GPU starts from the same bytes.
+
+* dry, 20 iterations: GPU FP64 vs the reference <= 1e-10 relative L2 per field (t, u, v, w,
+  p_dyn, p_hydro, rho_mix), the bar for the FP64 GPU path.
+* full physics (the reference's default physics: k-omega SST, radiation, precipitation, the
+  saturation adjustments, the NH4SH equilibrium, the moist convective adjustment every
+  iteration), 20 and 200 iterations: <= 1e-10 per prognostic field, except the NH4SH family
+  (h2s, nh3 <= 1e-8, nh4sh <= 1e-7): the equilibrium's bisection stops at a width of 1e-15 of the
+  cell's largest concentration, so a last-bit difference of its inputs moves its output by that
+  width; the reference moves that far itself when its state is perturbed by one ulp
+  (tests/test_moist_step.py), and the bar is ten times that self-sensitivity.
+* CPU: the C oracle is bit-identical to the reference over three dry iterations from the dry
+  configuration's state (np.array_equal), so the oracle is pinned on this input as well.
+"""
+import numpy as np
+import pytest
+
+from helpers import DYN_FIELDS, oracle_from, rel_l2
+from moist_cases import PROGNOSTIC, baseline_case, gpu_baseline_model
+
+REF_TOL = 1e-10
+NH4SH_FAMILY_TOL = {"h2s": 1e-8, "nh3": 1e-8, "nh4sh": 1e-7}
+DRY_COMPARED = ("t", "u", "v", "w", "p_dyn", "p_hydro", "rho_mix")
+
+
+@pytest.mark.slow
+def test_dry_state_recipe_and_oracle_bit_exact(ref_required):
+    d, P, _, _, _, g, f = baseline_case("dry", 3)
+    fluid = g["solid"] == 0
+    # the recipe's noise is there and has the stated size: the reference's initial fields are
+    # smooth along phi, so neighbour differences along phi of i.i.d. noise of deviation s have
+    # deviation s sqrt(2)
+    pair = fluid[:, :, 1:] & fluid[:, :, :-1]
+    for n, s in (("u", 0.01 / 100.0), ("w", 0.1 / 100.0), ("t", 0.05 / 165.0)):
+        dk = np.diff(f[n], axis=2)[pair]
+        est = np.median(np.abs(dk - np.median(dk))) * 1.4826 / np.sqrt(2.0)
+        assert 0.9 * s < est < 1.1 * s, f"{n}: noise deviation {est:.3e}, recipe {s:.3e}"
+    assert np.array_equal(f["u"][:, :, -1], f["u"][:, :, 0])
+    assert not np.any(f["u"][~fluid])
+    o = oracle_from(P, g, f)
+    for it in range(1, 4):
+        o.iteration(it, it == 1)
+    for n in DRY_COMPARED:
+        assert np.array_equal(o.f[n], d["out_" + n]), f"oracle {n} differs from the reference"
+
+
+def _run(P, PH, MC, MCA, g, f, iters, names):
+    m = gpu_baseline_model(P, PH, MC, MCA, g, f)
+    for it in range(1, iters + 1):
+        m.step(it, it == 1)
+    out = {n: m.download(n) for n in names}
+    assert m.nonfinite_count() == 0
+    m.close()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+def test_gpu_dry_config_20_iterations(ref_required):
+    d, P, PH, MC, MCA, g, f = baseline_case("dry", 20)
+    got = _run(P, PH, MC, MCA, g, f, 20, DRY_COMPARED)
+    worst = {n: rel_l2(got[n], d["out_" + n]) for n in DRY_COMPARED}
+    print("dry configuration, 20 iterations vs reference:",
+          {k: f"{v:.1e}" for k, v in worst.items()})
+    for n in DRY_COMPARED:
+        assert worst[n] <= REF_TOL, f"{n}: relative L2 {worst[n]:.3e} after 20 iterations"
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+@pytest.mark.parametrize("iters", [20, 200])
+def test_gpu_full_physics_config(ref_required, iters):
+    d, P, PH, MC, MCA, g, f = baseline_case("phys", iters)
+    got = _run(P, PH, MC, MCA, g, f, iters, PROGNOSTIC)
+    worst = {n: rel_l2(got[n], d[f"it{iters}_{n}"]) for n in PROGNOSTIC}
+    report = {k: f"{v:.1e}" for k, v in worst.items()}
+    print(f"full-physics configuration, {iters} iterations vs reference:", report)
+    for n in PROGNOSTIC:
+        assert np.isfinite(got[n]).all(), f"{n}: non-finite"
+        assert worst[n] <= NH4SH_FAMILY_TOL.get(n, REF_TOL), \
+            f"after {iters} iterations: {n} relative L2 {worst[n]:.3e} ({report})"

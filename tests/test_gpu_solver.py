@@ -82,3 +82,26 @@ def test_residual_solve_in_loop_source():
     tol = max(1e-10, 8 * st.rel_floor)
     e = _rel_residual(o, m.download("p_dyn"), src)
     assert e <= 2 * tol, f"oracle residual {e:.3e} (floor {st.rel_floor:.2e}, {st.iterations} it)"
+
+
+@pytest.mark.parametrize("omega", [1.0, 1.7])
+def test_sor_arm_small(omega):
+    """Point red-black SOR (ATJUP_SOLVE_SOR) on the same operator: the relative residual it reports
+    is the oracle's residual of the p it returns, and more sweeps lower it (the slow column modes
+    of this operator keep it far from 1e-10 within any practical number of sweeps)."""
+    from atjup_b200.params import SOLVE_SOR
+    shape = (13, 37, 49)
+    p, g, f = synthetic_case(*shape)
+    b = synthetic.poisson_rhs(*shape, seed=5)
+    o = oracle_from(p, g, f)
+    m = gpu_from(p, g, f)
+    m.set_solve_rhs(b)
+    rels = []
+    for cap in (100, 400):
+        st = m.pressure_solver(mode=SOLVE_SOR, omega=omega, rel_tol=1e-10, max_iter=cap,
+                               external_rhs=True, allow_not_converged=True)
+        assert st.iterations == cap
+        e = _rel_residual(o, m.download("p_dyn"), b)
+        assert abs(e - st.rel_residual) <= 1e-6 * e + 1e-12, (e, st.rel_residual)
+        rels.append(e)
+    assert rels[1] < rels[0] < 1.0, rels
