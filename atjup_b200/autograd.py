@@ -42,3 +42,43 @@ def rk4_steps(model, t, u, v, w, steps: int):
     for _ in range(steps):
         y = RK4Step.apply(model, *y)
     return y
+
+
+class IterationStep(torch.autograd.Function):
+    """One whole dry iteration of the reference's loop (atjup_gpu_step: the pressure pass and the
+    mixture density on even iterations and the first, RK4, the boundary passes, the in-loop
+    Shapiro filter and the column balance of v) on the nine fields one iteration hands the next
+    (atjup_b200.params.LIN_FIELDS: t, u, v, w, p_dyn, aux_u, aux_v, aux_w, rho_mix). Its backward is
+    atjup_gpu_iteration_adjoint about the iteration's input, which the step keeps as its
+    checkpoint; the adjoint recomputes the pressure pass and the RK stages from it."""
+
+    @staticmethod
+    def forward(ctx, model, iter_n, first, *x):
+        from .params import LIN_FIELDS
+        y = tuple(t.detach().contiguous() for t in x)
+        model.set_state_tensors(y, names=LIN_FIELDS, wait=False)
+        model.step(iter_n, first)
+        out = model.state_tensors(LIN_FIELDS)
+        ctx.model, ctx.iter_n, ctx.first = model, iter_n, first
+        ctx.save_for_backward(*y)
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        from .params import LIN_FIELDS
+        y = ctx.saved_tensors
+        model = ctx.model
+        model.set_state_tensors(y, names=LIN_FIELDS, wait=False)   # the linearisation point
+        g = [torch.zeros_like(r) if gr is None else gr.detach().clone().contiguous()
+             for gr, r in zip(grads, y)]
+        model.iteration_adjoint(g, ctx.iter_n, ctx.first)
+        return (None, None, None, *g)
+
+
+def iterations(model, x, steps: int, start: int = 1):
+    """`steps` differentiable dry iterations from the nine tensors x (LIN_FIELDS order), numbered
+    start, start + 1, ... (the first of a run has first = True)"""
+    y = tuple(x)
+    for n in range(start, start + steps):
+        y = IterationStep.apply(model, n, n == 1, *y)
+    return y

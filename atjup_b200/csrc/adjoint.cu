@@ -34,7 +34,7 @@ struct LinConst {
     double dt, dr;
     double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
     double cor_phi_f, coeff_energy_p, to_nd, r_mix, rR, g, t_ref;
-    double t_visc, inv_re, buoy_k, metric_on, cor_rad_on, Coriolis;
+    double t_visc, inv_re, buoy_k, metric_on, cor_rad_on, Coriolis, pgrad_scale;
     int pgrad_wall, adiabatic, adiabatic_rho, hydro_split, use_hp;
 };
 
@@ -63,6 +63,7 @@ LinConst lin_const(const AtjupCtx* c) {
     q.metric_on = P.metric_split ? 0.0 : 1.0;
     q.cor_rad_on = P.coriolis_split ? 0.0 : 1.0;
     q.Coriolis = P.Coriolis;
+    q.pgrad_scale = P.pgrad_scale;
     q.pgrad_wall = P.pgrad_wall;
     q.adiabatic = P.adiabatic;
     q.adiabatic_rho = P.adiabatic_rho;
@@ -152,6 +153,24 @@ __device__ __forceinline__ Frozen frozen_of(const LinConst& q, const LinPtrs& a,
     return z;
 }
 
+// the six p_dyn neighbours of the pressure gradients, a solid face mirrored to the cell itself
+// (RHS_Jup_Turb.cpp:119-130): i+, i-, j+, j-, k+, k-
+__device__ __forceinline__ void p_nbrs(const LinConst& q, const Nbr& n, uint8_t nbm, size_t* o) {
+    const bool wall = q.pgrad_wall;
+    o[0] = (wall && (nbm & NB_IP)) ? n.c : n.ip;
+    o[1] = (wall && (nbm & NB_IM)) ? n.c : n.im;
+    o[2] = (wall && (nbm & NB_JP)) ? n.c : n.jp;
+    o[3] = (wall && (nbm & NB_JM)) ? n.c : n.jm;
+    o[4] = (wall && (nbm & NB_KP)) ? n.c : n.kp;
+    o[5] = (wall && (nbm & NB_KM)) ? n.c : n.km;
+}
+
+// d(dpstatdr)/d(rho) / dpstatdr of the compression work with ATJUP_ADIABATIC_RHO: -1/rho where
+// the forward divides by rho, else 0
+__device__ __forceinline__ double dpstat_rho_factor(const LinConst& q, double rho_l) {
+    return (q.adiabatic && q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) ? -1.0 / rho_l : 0.0;
+}
+
 // the mirrored p_hydro neighbours of the v and w equations: the cell itself at a solid face
 __device__ __forceinline__ void ph_nbrs(const LinConst& q, const Nbr& n, uint8_t nbm, size_t& jp,
                                         size_t& jm, size_t& kp, size_t& km) {
@@ -173,6 +192,9 @@ struct TlArgs {
     double* dacc[4];
     const double* dph;
     const double* db;
+    const double* dp;          // perturbation of p_dyn (null: held fixed)
+    const double* drho;        // perturbation of rho_mix (null: held fixed)
+    double* daux[3];           // stage 3: aux_u, aux_v, aux_w, written at integrated cells (null: none)
     int stage;
     double c_in, wgt;
 };
@@ -226,14 +248,35 @@ __global__ void tl_stage_kernel(TlArgs A, LinConst q) {
         d_dph_phi = (A.dph[kp] - A.dph[km]) * q.inv_2dphi * irs;
     }
     const double d_buoy = z.buoy ? q.buoy_k * (z.dbdt0 * dT.f0 - A.db[i]) : 0.0;
+    // the pressure gradients of a perturbed p_dyn and the compression work of a perturbed rho
+    double ddpdr = 0.0, ddpdthe = 0.0, ddpdphi = 0.0, ddpstat = 0.0;
+    if (A.dp) {
+        size_t o[6];
+        p_nbrs(q, n, nbm, o);
+        ddpdr = (A.dp[o[0]] - A.dp[o[1]]) * q.inv_2dr;
+        ddpdthe = (A.dp[o[2]] - A.dp[o[3]]) * q.inv_2dthe;
+        ddpdphi = (A.dp[o[4]] - A.dp[o[5]]) * q.inv_2dphi;
+    }
+    if (A.drho) ddpstat = z.dpstatdr * dpstat_rho_factor(q, A.a.rho[n.c]) * A.drho[n.c];
+    const double d_pressure_p = q.coeff_energy_p *
+        (u0 * (ddpdr + ddpstat) + v0 * irm * ddpdthe + w0 * irs * ddpdphi);
+    const double gp_u = q.pgrad_scale * ddpdr;
+    const double gp_v = q.pgrad_scale * ddpdthe * irm;
+    const double gp_w = q.pgrad_scale * ddpdphi * irs;
 
-    const double dr_t = d_pressure_t - d_transport_t + d_diff_t * q.t_visc;
-    const double dr_u = (q.hydro_split ? 0.0 : d_buoy) - d_transport_u + d_diff_u * z.visc -
+    const double dr_t = d_pressure_t + d_pressure_p - d_transport_t + d_diff_t * q.t_visc;
+    const double dr_u = -gp_u + (q.hydro_split ? 0.0 : d_buoy) - d_transport_u + d_diff_u * z.visc -
                         q.cor_rad_on * q.Coriolis * g.cor_rad * dw0;
-    const double dr_v = -d_dph_the - d_transport_v + d_diff_v * z.visc - q.Coriolis * g.cor_the * dw0;
-    const double dr_w = -d_dph_phi - d_transport_w + d_diff_w * z.visc -
+    const double dr_v = -gp_v - d_dph_the - d_transport_v + d_diff_v * z.visc -
+                        q.Coriolis * g.cor_the * dw0;
+    const double dr_w = -gp_w - d_dph_phi - d_transport_w + d_diff_w * z.visc -
                         q.Coriolis * q.cor_phi_f * (g.costhe * dv0 + g.sinthe_true * du0);
     const double drhs[4] = {dr_t, dr_u, dr_v, dr_w};
+    if (A.stage == 3 && A.daux[0]) {   // aux = rhs + the p_dyn gradient term (rk4.cu)
+        A.daux[0][n.c] = dr_u + gp_u;
+        A.daux[1][n.c] = dr_v + gp_v;
+        A.daux[2][n.c] = dr_w + gp_w;
+    }
     for (int f = 0; f < 4; f++) {
         const double acc = (A.stage == 0) ? A.wgt * drhs[f] : A.dacc[f][n.c] + A.wgt * drhs[f];
         if (A.stage < 3) {
@@ -254,6 +297,10 @@ struct AdArgs {
     double* lY[4];             // adjoint of the step's input (accumulated)
     double* lph;               // adjoint of p_hydro (accumulated)
     double* lb;                // adjoint of the level means (accumulated)
+    double* lp;                // adjoint of p_dyn (accumulated; null: p_dyn held fixed)
+    double* lrho;              // adjoint of rho_mix (accumulated; null: held fixed)
+    double* laux[3];           // stage 3: adjoint of aux_u, aux_v, aux_w, read and cleared at the
+                               // integrated cells (null: aux not an output)
     int stage;
     double c_in, wgt;
 };
@@ -299,7 +346,14 @@ __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
             // for stages 0-2, from the next stage input (c_in)
             double lr[4];
             for (int f = 0; f < 4; f++) lr[f] = q.dt * (1.0 / 6.0) * A.wgt * A.lYn[f][n.c] + A.c_in * lxn[f];
-            const double at = lr[0], au = lr[1], av = lr[2], aw = lr[3];
+            // stage 3 also writes aux = rhs + the p_dyn gradient term of u, v, w: its adjoint adds
+            // to the right-hand sides' adjoints everywhere but in the p_dyn gradients
+            double lax = 0.0, lay = 0.0, law = 0.0;
+            if (A.stage == 3 && A.laux[0]) {
+                lax = A.laux[0][n.c]; lay = A.laux[1][n.c]; law = A.laux[2][n.c];
+                A.laux[0][n.c] = 0.0; A.laux[1][n.c] = 0.0; A.laux[2][n.c] = 0.0;
+            }
+            const double at = lr[0], au = lr[1] + lax, av = lr[2] + lay, aw = lr[3] + law;
             const GeoIJ& g = A.a.geo[(size_t)i * q.jm + j];
             const Der T = der_of(q, A.a.X[0], n), U = der_of(q, A.a.X[1], n);
             const Der V = der_of(q, A.a.X[2], n), W = der_of(q, A.a.X[3], n);
@@ -371,6 +425,24 @@ __global__ void ad_stage_kernel(AdArgs A, LinConst q) {
             Av0 -= aw * q.Coriolis * q.cor_phi_f * g.costhe;
             Au0 -= aw * q.Coriolis * q.cor_phi_f * g.sinthe_true;
 
+            if (A.lp) {
+                // the p_dyn gradients: of the compression work (rhs_t) and of the momentum
+                // equations (without the aux part, which cancels them)
+                const double Gr = at * q.coeff_energy_p * u0 - q.pgrad_scale * lr[1];
+                const double Gt = (at * q.coeff_energy_p * v0 - q.pgrad_scale * lr[2]) * irm;
+                const double Gp = (at * q.coeff_energy_p * w0 - q.pgrad_scale * lr[3]) * irs;
+                size_t o[6];
+                p_nbrs(q, n, nbm, o);
+                atomicAdd(A.lp + o[0], Gr * q.inv_2dr);
+                atomicAdd(A.lp + o[1], -Gr * q.inv_2dr);
+                atomicAdd(A.lp + o[2], Gt * q.inv_2dthe);
+                atomicAdd(A.lp + o[3], -Gt * q.inv_2dthe);
+                atomicAdd(A.lp + o[4], Gp * q.inv_2dphi);
+                atomicAdd(A.lp + o[5], -Gp * q.inv_2dphi);
+            }
+            if (A.lrho)
+                A.lrho[n.c] += at * q.coeff_energy_p * u0 * z.dpstatdr *
+                               dpstat_rho_factor(q, A.a.rho[n.c]);
             scatter_field(q, A.lX[0], n, At0, Tr1, Tr2, Tt1, Tt2, Tp1, Tp2, cc[0], cp[0], cm[0]);
             scatter_field(q, A.lX[1], n, Au0, Ur1, Ur2, Ut1, Ut2, Up1, Up2, cc[1], cp[1], cm[1]);
             scatter_field(q, A.lX[2], n, Av0, Vr1, Vr2, Vt1, Vt2, Vp1, Vp2, cc[2], cp[2], cm[2]);
@@ -657,6 +729,21 @@ extern "C" {
 int atjup_gpu_rk4_tlm(AtjupCtx* c, double* const d[4]) {
     if (!c || !d || !d[0] || !d[1] || !d[2] || !d[3]) { set_error("rk4_tlm: null argument"); return ATJUP_ERR_ARG; }
     if (!c->grid_set) { set_error("rk4_tlm: atjup_gpu_set_grid was not called"); return ATJUP_ERR_ARG; }
+    return rk4_tlm_ext(c, d, nullptr, nullptr, nullptr);
+}
+
+int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
+    if (!c || !a || !a[0] || !a[1] || !a[2] || !a[3]) { set_error("rk4_adjoint: null argument"); return ATJUP_ERR_ARG; }
+    if (!c->grid_set) { set_error("rk4_adjoint: atjup_gpu_set_grid was not called"); return ATJUP_ERR_ARG; }
+    return rk4_adjoint_ext(c, a, nullptr, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+namespace atjup {
+
+int rk4_tlm_ext(AtjupCtx* c, double* const d[4], const double* dp, const double* drho,
+                double* const daux[3]) {
     Lin L;
     int rc;
     if ((rc = lin_setup(c, L))) return rc;
@@ -689,6 +776,9 @@ int atjup_gpu_rk4_tlm(AtjupCtx* c, double* const d[4]) {
         }
         A.dph = L.ph;
         A.db = db;
+        A.dp = dp;
+        A.drho = drho;
+        for (int f = 0; f < 3; f++) A.daux[f] = daux ? daux[f] : nullptr;
         A.stage = s;
         A.c_in = stage_c_in(P, s);
         A.wgt = stage_wgt(s);
@@ -702,9 +792,8 @@ int atjup_gpu_rk4_tlm(AtjupCtx* c, double* const d[4]) {
     return lin_restore(c, L);
 }
 
-int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
-    if (!c || !a || !a[0] || !a[1] || !a[2] || !a[3]) { set_error("rk4_adjoint: null argument"); return ATJUP_ERR_ARG; }
-    if (!c->grid_set) { set_error("rk4_adjoint: atjup_gpu_set_grid was not called"); return ATJUP_ERR_ARG; }
+int rk4_adjoint_ext(AtjupCtx* c, double* const a[4], double* lp, double* lrho,
+                    double* const laux[3]) {
     Lin L;
     int rc;
     if ((rc = lin_setup(c, L))) return rc;
@@ -736,6 +825,9 @@ int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
         }
         A.lph = L.ph;
         A.lb = lb;
+        A.lp = lp;
+        A.lrho = lrho;
+        for (int f = 0; f < 3; f++) A.laux[f] = laux ? laux[f] : nullptr;
         A.stage = s;
         A.c_in = stage_c_in(P, s);
         A.wgt = stage_wgt(s);
@@ -763,4 +855,4 @@ int atjup_gpu_rk4_adjoint(AtjupCtx* c, double* const a[4]) {
     return lin_restore(c, L);
 }
 
-}  // extern "C"
+}  // namespace atjup

@@ -102,6 +102,8 @@ void free_all(AtjupCtx* c) {
     solver_free(c);
     cudaFree(c->lin);
     c->lin = nullptr;
+    cudaFree(c->itlin);
+    c->itlin = nullptr;
     for (auto& p : c->f) { cudaFree(p); p = nullptr; }
     for (auto& p : c->f2) { cudaFree(p); p = nullptr; }
     for (auto& p : c->fn) { cudaFree(p); p = nullptr; }

@@ -210,12 +210,16 @@ __global__ void ambient_kernel(const int32_t* __restrict__ rows, const uint8_t* 
 }  // namespace
 
 int launch_bc(AtjupCtx* c, int which) {
+    return launch_bc_ptrs(c, which, c->f[ATJUP_F_T], c->f[ATJUP_F_U], c->f[ATJUP_F_V],
+                          c->f[ATJUP_F_W], c->f[ATJUP_F_P_DYN], c->f[ATJUP_F_P_STAT], c->phys_on);
+}
+
+// The passes on the given t, u, v, w, p_dyn, p_stat (the dry lists unless phys, which takes the
+// context's other fields as well): the tangent-linear of the dry passes is this on perturbations.
+int launch_bc_ptrs(AtjupCtx* c, int which, double* t, double* u, double* v, double* w,
+                   double* p_dyn, double* p_stat, bool phys) {
     const AtjupParams& P = c->P;
-    double* t = c->f[ATJUP_F_T];
-    double* u = c->f[ATJUP_F_U];
-    double* v = c->f[ATJUP_F_V];
-    double* w = c->f[ATJUP_F_W];
-    const bool ph = c->phys_on;
+    const bool ph = phys;
     // the field lists of the passes (BC_Jup.h:275-350) over the fields the device holds
     auto add = [](FieldList& L, double* x) { L.f[L.n++] = x; };
     auto add_species = [&](FieldList& L) {
@@ -267,7 +271,7 @@ int launch_bc(AtjupCtx* c, int which) {
     if (which & ATJUP_BC_SOLID) {
         if (c->n_solid > 0) {
             FieldList S{};
-            add(S, t); add(S, c->f[ATJUP_F_P_STAT]); add(S, c->f[ATJUP_F_P_DYN]);
+            add(S, t); add(S, p_stat); add(S, p_dyn);
             if (ph) { add_species(S); add_massflux(S, true); }
             c->launches++;
             solid_kernel<<<(c->n_solid + 127) / 128, 128, 0, c->stream>>>(c->solid_list, c->n_solid,

@@ -111,6 +111,7 @@ struct AtjupCtx {
     double* hsum = nullptr;      // pinned host copy of the final dot products
     unsigned long long* counters = nullptr;  // [8] event counters of the last satadj call
     double* lin = nullptr;       // scratch of the RK4 tangent-linear / adjoint (adjoint.cu)
+    double* itlin = nullptr;     // scratch of the iteration's tangent-linear / adjoint (iteration_lin.cu)
 
     // static grid
     uint8_t* solid = nullptr;
@@ -173,8 +174,18 @@ int launch_mixture_density(AtjupCtx* c);
 int launch_prepare_projection(AtjupCtx* c);
 int launch_pressure_source(AtjupCtx* c);
 int launch_pressure_sweep(AtjupCtx* c, int colour, double omega);
+int launch_prepare_projection_ptr(AtjupCtx* c, double* au, double* av, double* aw);
+int launch_pressure_source_ptr(AtjupCtx* c, const double* au, const double* av, const double* aw,
+                               double* src, const uint8_t* mask_in, uint8_t* mask_out);
+int launch_pressure_sweep_ptr(AtjupCtx* c, double* p, const double* src, int colour, double omega);
 int launch_pressure_fold(AtjupCtx* c, double* p);
 int launch_bc(AtjupCtx* c, int which);
+int launch_bc_ptrs(AtjupCtx* c, int which, double* t, double* u, double* v, double* w,
+                   double* p_dyn, double* p_stat, bool phys);
+int rk4_tlm_ext(AtjupCtx* c, double* const d[4], const double* dp, const double* drho,
+                double* const daux[3]);
+int rk4_adjoint_ext(AtjupCtx* c, double* const a[4], double* lp, double* lrho,
+                    double* const laux[3]);
 int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passes, int use_topo);
 int launch_balance_v(AtjupCtx* c);
 int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, double* dvc,

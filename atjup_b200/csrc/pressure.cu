@@ -51,10 +51,14 @@ __device__ __forceinline__ double gather(const double* __restrict__ p,
 }
 
 // Divergence source of one cell (PressureSolver.h:370-459), clamped (484-487).
+// mask_out (optional): 1 where the clamp passes the divergence (finite, |div| <= cap den), else 0.
+// mask_in (optional, the tangent-linear of the clamp about a base state): the divergence times
+// mask_in, unclamped.
 __global__ void source_kernel(const double* __restrict__ Su, const double* __restrict__ Sv,
                               const double* __restrict__ Sw, const uint8_t* __restrict__ s,
                               const GeoIJ* __restrict__ geo, double* __restrict__ src,
-                              PressConst q) {
+                              PressConst q, const uint8_t* __restrict__ mask_in,
+                              uint8_t* __restrict__ mask_out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y + 1;
     const int i = blockIdx.z + 1;
@@ -132,6 +136,8 @@ __global__ void source_kernel(const double* __restrict__ Su, const double* __res
     if (!pf) dw_dphi = (Sw[ckp] - Sw[ckm]) * q.inv_2dphi;
     double div_src = du_dr * 1.0 + dv_dthe * g.inv_rm + dw_dphi * g.inv_rmsinthe;
     const double src_max = den * q.cap;
+    if (mask_out) mask_out[c] = (isfinite(div_src) && fabs(div_src) <= src_max) ? 1 : 0;
+    if (mask_in) { src[c] = mask_in[c] ? div_src : 0.0; return; }
     if (!isfinite(div_src)) div_src = 0.0;
     else if (div_src > src_max) div_src = src_max;
     else if (div_src < -src_max) div_src = -src_max;
@@ -227,38 +233,50 @@ PressConst make_const(const AtjupCtx* c) {
 
 }  // namespace
 
-int launch_prepare_projection(AtjupCtx* c) {
+int launch_prepare_projection_ptr(AtjupCtx* c, double* au, double* av, double* aw) {
     const AtjupParams& P = c->P;
     dim3 grid((P.km - 1 + 127) / 128, P.jm - 2);
     c->launches++;
-    prepare_kernel<<<grid, 128, 0, c->stream>>>(c->f[ATJUP_F_AUX_U], c->f[ATJUP_F_AUX_V],
-                                               c->f[ATJUP_F_AUX_W], P.im, P.jm, P.km, c->KP,
-                                               P.rigid_lid);
+    prepare_kernel<<<grid, 128, 0, c->stream>>>(au, av, aw, P.im, P.jm, P.km, c->KP, P.rigid_lid);
     ATJUP_CHECK_LAUNCH("prepare_projection");
     return ATJUP_OK;
 }
 
-int launch_pressure_source(AtjupCtx* c) {
+int launch_prepare_projection(AtjupCtx* c) {
+    return launch_prepare_projection_ptr(c, c->f[ATJUP_F_AUX_U], c->f[ATJUP_F_AUX_V],
+                                         c->f[ATJUP_F_AUX_W]);
+}
+
+int launch_pressure_source_ptr(AtjupCtx* c, const double* au, const double* av, const double* aw,
+                               double* src, const uint8_t* mask_in, uint8_t* mask_out) {
     const AtjupParams& P = c->P;
     const PressConst q = make_const(c);
     dim3 grid((P.km - 1 + 127) / 128, P.jm - 2, P.im - 2);
     c->launches++;
-    source_kernel<<<grid, 128, 0, c->stream>>>(c->f[ATJUP_F_AUX_U], c->f[ATJUP_F_AUX_V],
-                                              c->f[ATJUP_F_AUX_W], c->solid, c->geo, c->src, q);
+    source_kernel<<<grid, 128, 0, c->stream>>>(au, av, aw, c->solid, c->geo, src, q, mask_in,
+                                              mask_out);
     ATJUP_CHECK_LAUNCH("pressure_source");
     return ATJUP_OK;
 }
 
-int launch_pressure_sweep(AtjupCtx* c, int colour, double omega) {
+int launch_pressure_source(AtjupCtx* c) {
+    return launch_pressure_source_ptr(c, c->f[ATJUP_F_AUX_U], c->f[ATJUP_F_AUX_V],
+                                      c->f[ATJUP_F_AUX_W], c->src, nullptr, nullptr);
+}
+
+int launch_pressure_sweep_ptr(AtjupCtx* c, double* p, const double* src, int colour, double omega) {
     const AtjupParams& P = c->P;
     const PressConst q = make_const(c);
     const int nx = (P.km - 1 + 1) / 2;
     dim3 grid((nx + 127) / 128, P.jm - 2, P.im - 2);
     c->launches++;
-    sweep_kernel<<<grid, 128, 0, c->stream>>>(c->f[ATJUP_F_P_DYN], c->solid, c->src, c->geo, q,
-                                             colour, omega);
+    sweep_kernel<<<grid, 128, 0, c->stream>>>(p, c->solid, src, c->geo, q, colour, omega);
     ATJUP_CHECK_LAUNCH("pressure_sweep");
     return ATJUP_OK;
+}
+
+int launch_pressure_sweep(AtjupCtx* c, int colour, double omega) {
+    return launch_pressure_sweep_ptr(c, c->f[ATJUP_F_P_DYN], c->src, colour, omega);
 }
 
 int launch_pressure_fold(AtjupCtx* c, double* p) {

@@ -162,12 +162,14 @@ __device__ __forceinline__ void issue_extra(StageSmem<TI, TA>& S, const StagePtr
 }
 
 // One RK stage: every (j, k) column of the block's tile, plane by plane. TI is the storage of the
-// stage input, TO of the next stage input, TA of the accumulators (all double in the FP64 step;
-// the mixed step stores them in FP32: stage 0 <double, float, float> reads the FP64 state, stages
-// 1-3 <float, float, float>). The right-hand side is evaluated in FP64 either way: the kernel's
-// residency is set by its shared memory, not its registers, and the final update y_n + dt/6 acc
-// is formed in FP64 from the FP64 time-level-n state.
-template <typename TI, typename TO, typename TA>
+// stage input, TO of the next stage input, TA of the accumulators, R the arithmetic of the
+// right-hand side (all double in the FP64 step; the mixed step stores the buffers in FP32 --
+// stage 0 <double, float, float> reads the FP64 state, stages 1-3 <float, float, float> -- and
+// evaluates the stencils in FP32). Kept in FP64 in both: the differences of the FP64 pressures
+// p_dyn, p_hydro and p_stat (then rounded to R), the buoyancy anomaly against the FP64 level
+// mean, the heating rates of the FP64 sources, the next stage input y_n + c_in rhs and the final
+// update y_n + dt/6 acc from the FP64 time-level-n state, and the projection source aux.
+template <typename TI, typename TO, typename TA, typename R>
 __global__ void __launch_bounds__(NT, 2)
 rk_stage_kernel(StagePtrs a, StageConst q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -220,20 +222,20 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 }
             } else {
                 const GeoIJ& g = S.geo[xs][ty];
-                const double t0 = (double)Tt[h], u0 = (double)Ut[h], v0 = (double)Vt[h];
-                const double w0 = (double)Wt[h];
+                const R t0 = (R)Tt[h], u0 = (R)Ut[h], v0 = (R)Vt[h];
+                const R w0 = (R)Wt[h];
                 const TI* Tn = S.tile[ns][0];
                 const TI* Un = S.tile[ns][1];
                 const TI* Vn = S.tile[ns][2];
                 const TI* Wn = S.tile[ns][3];
                 // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
 #define DERIVS(F, FN, FM, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
-    const double d1r = ((double)FN[h] - FM) * q.inv_2dr;                              \
-    const double d2r = ((double)FN[h] - 2.0 * f0 + FM) * q.inv_dr2;                   \
-    const double d1t = ((double)F[h + HK] - (double)F[h - HK]) * q.inv_2dthe;         \
-    const double d2t = ((double)F[h + HK] - 2.0 * f0 + (double)F[h - HK]) * q.inv_dthe2; \
-    const double d1p = ((double)F[h + 1] - (double)F[h - 1]) * q.inv_2dphi;           \
-    const double d2p = ((double)F[h + 1] - 2.0 * f0 + (double)F[h - 1]) * q.inv_dphi2;
+    const R d1r = ((R)FN[h] - (R)FM) * (R)q.inv_2dr;                                  \
+    const R d2r = ((R)FN[h] - (R)2.0 * f0 + (R)FM) * (R)q.inv_dr2;                    \
+    const R d1t = ((R)F[h + HK] - (R)F[h - HK]) * (R)q.inv_2dthe;                     \
+    const R d2t = ((R)F[h + HK] - (R)2.0 * f0 + (R)F[h - HK]) * (R)q.inv_dthe2;       \
+    const R d1p = ((R)F[h + 1] - (R)F[h - 1]) * (R)q.inv_2dphi;                       \
+    const R d2p = ((R)F[h + 1] - (R)2.0 * f0 + (R)F[h - 1]) * (R)q.inv_dphi2;
                 DERIVS(Tt, Tn, m_t, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
                 DERIVS(Ut, Un, m_u, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
                 DERIVS(Vt, Vn, m_v, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
@@ -248,74 +250,77 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 const double pjm = (wall && (nbm & NB_JM)) ? pc : Pt[h - HK];
                 const double pkp = (wall && (nbm & NB_KP)) ? pc : Pt[h + 1];
                 const double pkm = (wall && (nbm & NB_KM)) ? pc : Pt[h - 1];
-                const double dpdr = (pip - pim) * q.inv_2dr;
-                const double dpdthe = (pjp - pjm) * q.inv_2dthe;
-                const double dpdphi = (pkp - pkm) * q.inv_2dphi;
+                const R dpdr = (R)((pip - pim) * q.inv_2dr);
+                const R dpdthe = (R)((pjp - pjm) * q.inv_2dthe);
+                const R dpdphi = (R)((pkp - pkm) * q.inv_2dphi);
 
                 // body forces (RHS_Jup_Turb.cpp:384-423)
-                const double Coriolis_rad = g.cor_rad * w0;
-                const double Coriolis_the = g.cor_the * w0;
-                double v_cor = v0, u_cor = u0;
+                const R Coriolis_rad = (R)g.cor_rad * w0;
+                const R Coriolis_the = (R)g.cor_the * w0;
+                R v_cor = v0, u_cor = u0;
                 if (q.cell_hold) {
-                    v_cor -= S.cm[xs][0][ty];
-                    u_cor -= S.cm[xs][1][ty];
+                    v_cor -= (R)S.cm[xs][0][ty];
+                    u_cor -= (R)S.cm[xs][1][ty];
                 }
-                const double Coriolis_phi = q.cor_phi_f * (+g.costhe * v_cor + g.sinthe_true * u_cor);
-                const double v_invrm = v0 * g.inv_rm;
-                const double w_invrs = w0 * g.inv_rmsinthe;
+                const R Coriolis_phi = (R)q.cor_phi_f * (+(R)g.costhe * v_cor + (R)g.sinthe_true * u_cor);
+                const R v_invrm = v0 * (R)g.inv_rm;
+                const R w_invrs = w0 * (R)g.inv_rmsinthe;
 
                 // compression work with the hydrostatic part (RHS_Jup_Turb.cpp:459-482)
                 const double rho_l = S.ex[xs][0][tid];
-                double dpstatdr = 0.0;
+                double dpstatdr64 = 0.0;
                 if (q.adiabatic) {
-                    dpstatdr = (S.ps[ns][tid] - m_ps) * q.inv_2dr * q.to_nd;
-                    if (q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr *= q.r_mix / rho_l;
+                    dpstatdr64 = (S.ps[ns][tid] - m_ps) * q.inv_2dr * q.to_nd;
+                    if (q.adiabatic_rho && rho_l > 0.0 && isfinite(rho_l)) dpstatdr64 *= q.r_mix / rho_l;
                 }
-                const double pressure_t = q.coeff_energy_p *
+                const R dpstatdr = (R)dpstatdr64;
+                const R pressure_t = (R)q.coeff_energy_p *
                     (u0 * (dpdr + dpstatdr) + v_invrm * dpdthe + w_invrs * dpdphi);
-                const double transport_t = u0 * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
-                const double transport_u = u0 * dudr + v_invrm * dudthe + w_invrs * dudphi -
-                                           q.metric_on * (v0 * v0 + w0 * w0) * g.inv_rm;
-                const double transport_v = u0 * dvdr + v_invrm * dvdthe + w_invrs * dvdphi +
-                                           (u0 * v0 - w0 * w0 * g.cotanthe) * g.inv_rm;
-                const double transport_w = u0 * dwdr + v_invrm * dwdthe + w_invrs * dwdphi +
-                                           (w0 * u0 + v0 * w0 * g.cotanthe) * g.inv_rm;
+                const R transport_t = u0 * dtdr + v_invrm * dtdthe + w_invrs * dtdphi;
+                const R transport_u = u0 * dudr + v_invrm * dudthe + w_invrs * dudphi -
+                                      (R)q.metric_on * (v0 * v0 + w0 * w0) * (R)g.inv_rm;
+                const R transport_v = u0 * dvdr + v_invrm * dvdthe + w_invrs * dvdphi +
+                                      (u0 * v0 - w0 * w0 * (R)g.cotanthe) * (R)g.inv_rm;
+                const R transport_w = u0 * dwdr + v_invrm * dwdthe + w_invrs * dwdphi +
+                                      (w0 * u0 + v0 * w0 * (R)g.cotanthe) * (R)g.inv_rm;
 
                 // diffusion (RHS_Jup_Turb.cpp:521-545)
-                const double two_inv_rm = 2.0 * g.inv_rm;
-                const double diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * g.inv_rm2 +
-                                           dtdthe * g.costhe_inv_rm2sinthe + d2tdphi2 * g.inv_rm2sinthe2;
-                const double diffusion_u = d2udr2 + 2.0 * u0 * g.inv_rm2 + d2udthe2 * g.inv_rm2 +
-                                           4.0 * dudr * g.inv_rm + dudthe * g.costhe_inv_rm2sinthe +
-                                           d2udphi2 * g.inv_rm2sinthe2;
-                const double diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * g.inv_rm2 +
-                                           dvdthe * g.costhe_inv_rm2sinthe - g.v_metric * v0 +
-                                           d2vdphi2 * g.inv_rm2sinthe2 + 2.0 * dudthe * g.inv_rm2 -
-                                           dwdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
-                const double diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * g.inv_rm2 +
-                                           dwdthe * g.costhe_inv_rm2sinthe - g.v_metric * w0 +
-                                           d2wdphi2 * g.inv_rm2sinthe2 + 2.0 * dudphi * g.inv_rm2sinthe +
-                                           dvdphi * 2.0 * g.costhe * g.inv_rm2sinthe2;
+#define G_(x) ((R)g.x)
+                const R two_inv_rm = (R)2.0 * G_(inv_rm);
+                const R diffusion_t = d2tdr2 + dtdr * two_inv_rm + d2tdthe2 * G_(inv_rm2) +
+                                      dtdthe * G_(costhe_inv_rm2sinthe) + d2tdphi2 * G_(inv_rm2sinthe2);
+                const R diffusion_u = d2udr2 + (R)2.0 * u0 * G_(inv_rm2) + d2udthe2 * G_(inv_rm2) +
+                                      (R)4.0 * dudr * G_(inv_rm) + dudthe * G_(costhe_inv_rm2sinthe) +
+                                      d2udphi2 * G_(inv_rm2sinthe2);
+                const R diffusion_v = d2vdr2 + dvdr * two_inv_rm + d2vdthe2 * G_(inv_rm2) +
+                                      dvdthe * G_(costhe_inv_rm2sinthe) - G_(v_metric) * v0 +
+                                      d2vdphi2 * G_(inv_rm2sinthe2) + (R)2.0 * dudthe * G_(inv_rm2) -
+                                      dwdphi * (R)2.0 * G_(costhe) * G_(inv_rm2sinthe2);
+                const R diffusion_w = d2wdr2 + dwdr * two_inv_rm + d2wdthe2 * G_(inv_rm2) +
+                                      dwdthe * G_(costhe_inv_rm2sinthe) - G_(v_metric) * w0 +
+                                      d2wdphi2 * G_(inv_rm2sinthe2) + (R)2.0 * dudphi * G_(inv_rm2sinthe) +
+                                      dvdphi * (R)2.0 * G_(costhe) * G_(inv_rm2sinthe2);
+#undef G_
 
-                const double dpdr_term = q.pgrad_scale * dpdr;
-                const double dpdthe_term = q.pgrad_scale * dpdthe * g.inv_rm;
-                const double dpdphi_term = q.pgrad_scale * dpdphi * g.inv_rmsinthe;
-                double dphdthe_term = 0.0, dphdphi_term = 0.0;
+                const R dpdr_term = (R)q.pgrad_scale * dpdr;
+                const R dpdthe_term = (R)q.pgrad_scale * dpdthe * (R)g.inv_rm;
+                const R dpdphi_term = (R)q.pgrad_scale * dpdphi * (R)g.inv_rmsinthe;
+                R dphdthe_term = (R)0.0, dphdphi_term = (R)0.0;
                 if (q.use_hp) {
                     const double hc = Ht[h];
                     const double hjp = (wall && (nbm & NB_JP)) ? hc : Ht[h + HK];
                     const double hjm = (wall && (nbm & NB_JM)) ? hc : Ht[h - HK];
                     const double hkp = (wall && (nbm & NB_KP)) ? hc : Ht[h + 1];
                     const double hkm = (wall && (nbm & NB_KM)) ? hc : Ht[h - 1];
-                    dphdthe_term = (hjp - hjm) * q.inv_2dthe * g.inv_rm;
-                    dphdphi_term = (hkp - hkm) * q.inv_2dphi * g.inv_rmsinthe;
+                    dphdthe_term = (R)((hjp - hjm) * q.inv_2dthe) * (R)g.inv_rm;
+                    dphdphi_term = (R)((hkp - hkm) * q.inv_2dphi) * (R)g.inv_rmsinthe;
                 }
 
                 // radiative and latent heating (RHS_Jup_Turb.cpp:646-718)
                 double radiation_t = 0.0, precip_t = 0.0;
                 if (q.has_heating) {
                     if (q.rad_coupling != 0.0) {
-                        const double T_phys = t0 * q.t_ref;
+                        const double T_phys = (double)t0 * q.t_ref;
                         const double P_phys = S.ps[cs][tid] * 1.0e5;
                         const double rho = (rho_l > 0.0 && isfinite(rho_l))
                                                ? rho_l
@@ -347,46 +352,48 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                     if (q.turb_coupling != 0.0 && isfinite(nn)) nue_t = q.turb_coupling * fmax(0.0, nn);
                 }
                 const double nue_t_s = nue_t / 0.9;
-                const double visc = q.inv_re + nue_t + S.ex[xs][1][tid];
+                const R visc = (R)(q.inv_re + nue_t + S.ex[xs][1][tid]);
 
-                const double rhs_t = +pressure_t - transport_t + diffusion_t * (q.t_visc + nue_t_s) +
-                                     radiation_t + precip_t;
+                const R rhs_t = +pressure_t - transport_t + diffusion_t * (R)(q.t_visc + nue_t_s) +
+                                (R)radiation_t + (R)precip_t;
+                // the buoyancy anomaly against the level mean, in FP64 (the mean is FP64)
+                const double t0d = (double)t0;
                 const double buoyancy_u =
-                    (t0 > 0.0) ? q.buoy_k * (q.g * S.ps[cs][tid] / (q.rR * t0 * q.t_ref) - a.buoy_ref[i])
-                               : 0.0;
-                const double rhs_u = -dpdr_term + (q.hydro_split ? 0.0 : buoyancy_u) - transport_u +
-                                     diffusion_u * visc - q.cor_rad_on * q.Coriolis * Coriolis_rad +
-                                     q.centrifugal * g.cent_rad;
-                const double rhs_v = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc -
-                                     q.Coriolis * Coriolis_the + q.centrifugal * g.cent_the;
-                const double rhs_w = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc -
-                                     q.Coriolis * Coriolis_phi;
+                    (t0d > 0.0) ? q.buoy_k * (q.g * S.ps[cs][tid] / (q.rR * t0d * q.t_ref) - a.buoy_ref[i])
+                                : 0.0;
+                const R rhs_u = -dpdr_term + (q.hydro_split ? (R)0.0 : (R)buoyancy_u) - transport_u +
+                                diffusion_u * visc - (R)(q.cor_rad_on * q.Coriolis) * Coriolis_rad +
+                                (R)(q.centrifugal * g.cent_rad);
+                const R rhs_v = -dpdthe_term - dphdthe_term - transport_v + diffusion_v * visc -
+                                (R)q.Coriolis * Coriolis_the + (R)(q.centrifugal * g.cent_the);
+                const R rhs_w = -dpdphi_term - dphdphi_term - transport_w + diffusion_w * visc -
+                                (R)q.Coriolis * Coriolis_phi;
 
                 // accumulate (RungeKutta_Jup_Turb.cpp:419-490), form the next stage input / result
-                const double rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
+                const R rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
                 if (q.stage == 0) {
-                    const double y0[4] = {t0, u0, v0, w0};
+                    const double y0[4] = {(double)Tt[h], (double)Ut[h], (double)Vt[h], (double)Wt[h]};
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        static_cast<TA*>(a.acc[f])[c] = (TA)(q.wgt * rhs[f]);
-                        static_cast<TO*>(a.Xo[f])[c] = (TO)(y0[f] + q.c_in * rhs[f]);
+                        static_cast<TA*>(a.acc[f])[c] = (TA)((R)q.wgt * rhs[f]);
+                        static_cast<TO*>(a.Xo[f])[c] = (TO)(y0[f] + q.c_in * (double)rhs[f]);
                     }
                 } else if (q.stage < 3) {
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        static_cast<TA*>(a.acc[f])[c] = (TA)((double)S.ax[xs][f][tid] + q.wgt * rhs[f]);
-                        static_cast<TO*>(a.Xo[f])[c] = (TO)(S.Yx[xs][f][tid] + q.c_in * rhs[f]);
+                        static_cast<TA*>(a.acc[f])[c] = (TA)((R)S.ax[xs][f][tid] + (R)q.wgt * rhs[f]);
+                        static_cast<TO*>(a.Xo[f])[c] = (TO)(S.Yx[xs][f][tid] + q.c_in * (double)rhs[f]);
                     }
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        const double acc3 = (double)S.ax[xs][f][tid] + q.wgt * rhs[f];
+                        const double acc3 = (double)S.ax[xs][f][tid] + q.wgt * (double)rhs[f];
                         a.Y[f][c] = S.Yx[xs][f][tid] + q.dt * acc3 * q.one_sixth;
                     }
                     // the projection source the next pressure solve reads (the last stage's values)
-                    a.aux_u[c] = rhs_u + dpdr_term;
-                    a.aux_v[c] = rhs_v + dpdthe_term;
-                    a.aux_w[c] = rhs_w + dpdphi_term;
+                    a.aux_u[c] = (double)rhs_u + (double)dpdr_term;
+                    a.aux_v[c] = (double)rhs_v + (double)dpdthe_term;
+                    a.aux_w[c] = (double)rhs_w + (double)dpdphi_term;
                 }
             }
         }
@@ -523,19 +530,19 @@ int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w) {
     return ATJUP_OK;
 }
 
-template <typename TI, typename TO, typename TA>
+template <typename TI, typename TO, typename TA, typename R>
 static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, const char* name) {
     const AtjupParams& P = c->P;
     static bool attr_set = false;       // one flag per instantiation
     if (!attr_set) {
-        ATJUP_CUDA(cudaFuncSetAttribute(rk_stage_kernel<TI, TO, TA>,
+        ATJUP_CUDA(cudaFuncSetAttribute(rk_stage_kernel<TI, TO, TA, R>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)sizeof(StageSmem<TI, TA>)));
         attr_set = true;
     }
     dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
     c->launches++;
-    rk_stage_kernel<TI, TO, TA><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q);
+    rk_stage_kernel<TI, TO, TA, R><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q);
     ATJUP_CHECK_LAUNCH(name);
     return ATJUP_OK;
 }
@@ -614,9 +621,9 @@ int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const*
     q.precip_local = (P.precip_rho_local && P.local_rho) ? 1 : 0;
 
     if (c->step_prec != ATJUP_PREC_MIXED)
-        return launch_stage_t<double, double, double>(c, a, q, "rk_stage");
-    if (stage == 0) return launch_stage_t<double, float, float>(c, a, q, "rk_stage (mixed)");
-    return launch_stage_t<float, float, float>(c, a, q, "rk_stage (mixed)");
+        return launch_stage_t<double, double, double, double>(c, a, q, "rk_stage");
+    if (stage == 0) return launch_stage_t<double, float, float, float>(c, a, q, "rk_stage (mixed)");
+    return launch_stage_t<float, float, float, float>(c, a, q, "rk_stage (mixed)");
 }
 
 int launch_mixture_density(AtjupCtx* c) {

@@ -45,6 +45,8 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_rk4_tlm.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_copy_field.argtypes = [vp, i32, vp, i32]
     L.atjup_gpu_rk4_adjoint.argtypes = [vp, ctypes.POINTER(vp)]
+    L.atjup_gpu_iteration_tlm.argtypes = [vp, i32, i32, i32, ctypes.POINTER(vp)]
+    L.atjup_gpu_iteration_adjoint.argtypes = [vp, i32, i32, i32, ctypes.POINTER(vp)]
     L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.atjup_gpu_upload.argtypes = [vp, i32, vp]
     L.atjup_gpu_download.argtypes = [vp, i32, vp]
@@ -335,6 +337,19 @@ class GpuModel:
         """adjoint of one RK4 step of the dry dynamics about the current state, in place: the
         adjoint of the step's result in, of its input out"""
         self._on_tensors(self.L.atjup_gpu_rk4_adjoint, (at, au, av, aw))
+
+    def iteration_tlm(self, tensors, iter_n: int, first: bool = False, parts: int = _p.LIN_ALL):
+        """tangent-linear of one dry iteration (atjup_gpu_iteration_tlm) about the current state,
+        in place on nine (im, jm, pitch) float64 CUDA tensors in the order of LIN_FIELDS"""
+        self._on_tensors(lambda ctx, ptrs: self.L.atjup_gpu_iteration_tlm(
+            ctx, int(iter_n), int(first), int(parts), ptrs), tensors)
+
+    def iteration_adjoint(self, tensors, iter_n: int, first: bool = False,
+                          parts: int = _p.LIN_ALL):
+        """adjoint of one dry iteration (atjup_gpu_iteration_adjoint) about the current state, in
+        place: the adjoint of the iteration's output in, of its input out (LIN_FIELDS order)"""
+        self._on_tensors(lambda ctx, ptrs: self.L.atjup_gpu_iteration_adjoint(
+            ctx, int(iter_n), int(first), int(parts), ptrs), tensors)
 
     def stream_handle(self) -> int:
         """the cudaStream_t the context issues its work on, as an integer"""

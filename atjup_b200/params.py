@@ -72,6 +72,10 @@ GAS_IDS = {"H2O": GAS_H2O, "NH3": GAS_NH3, "CH4": GAS_CH4}
 SOLVE_SWEEPS, SOLVE_RESIDUAL, SOLVE_SOR = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 BC_RADIUS, BC_THETA, BC_PHI, BC_SOLID, BC_ALL = 1, 2, 4, 8, 15
+# the passes of atjup_gpu_iteration_tlm / atjup_gpu_iteration_adjoint, and their nine fields
+LIN_PRESSURE, LIN_MIXTURE, LIN_RK4, LIN_BC, LIN_SHAPIRO, LIN_BALANCE = 1, 2, 4, 8, 16, 32
+LIN_ALL = 63
+LIN_FIELDS = ("t", "u", "v", "w", "p_dyn", "aux_u", "aux_v", "aux_w", "rho_mix")
 
 GAS_CONST_NAMES = ("t_0", "t_00", "ep", "lv", "ls", "C", "L0", "R", "del_alf", "del_bet",
                    "C_i", "L0_i", "del_alf_i", "del_bet_i")

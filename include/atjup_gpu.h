@@ -503,6 +503,30 @@ int atjup_gpu_load_state(AtjupCtx* ctx, const char* path, int32_t* iter, int32_t
  * (The reference has no derivative code.) */
 int atjup_gpu_rk4_tlm(AtjupCtx* ctx, double* const d[4]);
 int atjup_gpu_rk4_adjoint(AtjupCtx* ctx, double* const a[4]);
+
+/* Tangent-linear and adjoint of one whole dry iteration of cJupiterModel::Run's loop
+ * (cJupiterModel.cpp:1032-1381 with the dry knobs): on even iterations (and when first != 0) the
+ * pressure pass (PressureSolver.h:144-766, prepareProjectionBoundaries cJupiterModel.cpp:
+ * 1842-1864; ATJUP_SOLVE_SWEEPS with press_sweeps sweeps, omega 1) and the mixture density
+ * (InitValues_Jup.cpp:717-740); every iteration RungeKuttaJup, the boundary passes
+ * (BC_Jup.h:185-658), the in-loop 4th-order Shapiro filter of u, v, w (lib/Utils.cpp:334-453)
+ * and the column balance of v (InitValues_Jup.cpp:1500-1538). The linear state is nine device
+ * buffers in the context's padded layout: t, u, v, w, p_dyn, aux_u, aux_v, aux_w, rho_mix (what
+ * an iteration reads from the one before). Both linearise about the context's current state,
+ * taken as the iteration's input, and leave that state as they found it. The source clamp of the
+ * pressure pass is linearised as its derivative at the base state (the perturbation passes where
+ * the base divergence is not clamped).
+ *   atjup_gpu_iteration_tlm      d in: a perturbation of the iteration's input; out: its response
+ *   atjup_gpu_iteration_adjoint  a in: the adjoint of the iteration's output; out: of its input
+ * parts selects the passes in the linear map (ATJUP_LIN_ALL: the whole iteration; a pass left out
+ * is the identity), for checking them one at a time. Dry dynamics in FP64 only, as
+ * atjup_gpu_rk4_tlm. (The reference has no derivative code.) */
+enum { ATJUP_LIN_PRESSURE = 1, ATJUP_LIN_MIXTURE = 2, ATJUP_LIN_RK4 = 4, ATJUP_LIN_BC = 8,
+       ATJUP_LIN_SHAPIRO = 16, ATJUP_LIN_BALANCE = 32, ATJUP_LIN_ALL = 63 };
+int atjup_gpu_iteration_tlm(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_t parts,
+                            double* const d[9]);
+int atjup_gpu_iteration_adjoint(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_t parts,
+                                double* const a[9]);
 /* Device-to-device copy between a field and a caller's device buffer in the padded layout
  * (im * jm * pitch doubles), in the context's stream order: to_field 1 copies buf into the field,
  * 0 the field into buf. For callers that hold the state in their own device tensors (the torch

@@ -372,6 +372,9 @@ def main():
                          "step from the initial state +- EPS d (t, u, v, w and their n copies)")
     ap.add_argument("--env", action="append", default=[],
                     help="KEY=VALUE set before the model is built (knobs are read once)")
+    ap.add_argument("--iter-fd", default=None, metavar="NDIR:EPS:K",
+                    help="with --baseline dry: central differences of K dry iterations along NDIR "
+                         "seeded directions (the top level's zonal mean of w)")
     ap.add_argument("--baseline", default=None, choices=("dry", "phys"),
                     help="start from the benchmark configuration's seeded initial state "
                          "(oracle/baseline_state.py) with its knobs: dry with --iters, "
@@ -385,6 +388,12 @@ def main():
                       env_extra=dict(kv.split("=", 1) for kv in a.env))
         data = {}
         BS.record(ref, data, moist=(a.baseline == "phys"))
+        if a.perturb_ulp:
+            # the reference's own sensitivity: t one ulp higher in the fluid cells
+            t = ref.get("t")
+            t = np.where(ref.solid() == 0, np.nextafter(t, np.inf), t)
+            ref.set("t", t)
+            ref.set("tn", t)
         if a.baseline == "phys":
             iters = a.phys_iters
             for it in range(1, iters + 1):
@@ -394,6 +403,40 @@ def main():
                 if it in (1, iters):
                     for n in ITER_FIELDS:
                         data[f"it{it}_{n}"] = ref.get(n)
+        elif a.iter_fd:
+            # central differences of K dry iterations: for NDIR seeded directions d
+            # (tests/adjoint_cases.py) on t, u, v, w and their n copies, the top level's zonal mean
+            # of w after K iterations from the state +- EPS d; the model is put back to the
+            # state before each run (every field the dry iteration reads or writes)
+            import adjoint_cases as AC
+            ndir, eps, K = a.iter_fd.split(":")
+            ndir, eps, K = int(ndir), float(eps), int(K)
+            keep = ("t", "u", "v", "w", "tn", "un", "vn", "wn", "p_dyn", "p_dynn", "p_hydro",
+                    "p_stat", "rho_mix", "wall_nue", "aux_u", "aux_v", "aux_w", "acc_t", "acc_u",
+                    "acc_v", "acc_w", "rhs_t", "rhs_u", "rhs_v", "rhs_w")
+            snap = {n: ref.get(n) for n in keep}
+
+            def run(x):
+                for n in keep:
+                    ref.set(n, snap[n])
+                if x is not None:
+                    for f in AC.FIELDS:
+                        ref.set(f, x[f])
+                        ref.set(f + "n", x[f])
+                for it in range(1, K + 1):
+                    rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 1)
+                    if rc != 0:
+                        raise SystemExit(f"ref_iteration rc={rc}")
+                return AC.zonal_mean_top(ref.get("w"))
+
+            data["fd_zm0"] = run(None)
+            data["fd_zm0_again"] = run(None)
+            for k in range(ndir):
+                d = AC.direction(k, ref.shape)
+                for sgn, tag in ((1.0, "p"), (-1.0, "m")):
+                    data[f"fd_zm{tag}_{k}"] = run({f: snap[f] + sgn * eps * d[f] for f in AC.FIELDS})
+            data["fd_eps"] = np.array(eps)
+            data["fd_iters"] = np.array(K)
         else:
             for it in range(1, a.iters + 1):
                 rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 1)
