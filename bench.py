@@ -2,7 +2,7 @@
 """Benchmark of ATJUP's time step on B200: one model iteration with the full physics.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload phys|dry|rk4-adjoint] [--precision fp64|mixed] [--no-extras]
+                    [--workload phys|dry|adjoint] [--precision fp64|mixed] [--no-extras]
 
 Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 shell (2.68 M
 cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
@@ -41,8 +41,9 @@ Sections of the default line besides the headline (N = 1; --no-extras drops them
 * `poisson`: the isolated Poisson solve on the shell (seeded smoothed N(0, 1) right-hand side):
   FP64 PCG, mixed PCG (FP32 preconditioner) and point red-black SOR with omega = 1.7 --
   iterations, seconds per solve, relative residual, its FP64 rounding floor, HBM GB/s.
-* `adjoint`: adjoint+forward over forward time of 50 dry RK4 steps through the torch.autograd
-  binding, from the dry configuration's state, with the memory it holds.
+* `adjoint`: adjoint+forward over forward time of 50 whole dry iterations through the
+  torch.autograd binding (IterationStep), from the dry configuration's state, with the memory it
+  holds.
 
 `roofline` is that of one RK stage. With full physics the species and closure kernels of a stage
 run on a second stream beside the dynamics kernel, so the stage (timing class `rk_group`: from the
@@ -461,34 +462,39 @@ def poisson_section(m, stream):
 # ---- config 4: the adjoint -------------------------------------------------------------------
 
 def adjoint_section(P, grid, fields, K):
-    """K RK4 steps of the dry dynamics forward and their adjoint through the torch.autograd
-    binding (each step keeps its input as the checkpoint and the adjoint recomputes its stages):
-    the time of forward with checkpoints + backward over the time of K plain forward steps, and
-    the device memory the chain holds. Loss J = sum_theta sin(colatitude) (zonal-mean w at the top
-    integrated level - u_ref)^2, u_ref = sum_{n=1..8} a_n sin(n theta), a_n seeded U(-50, 150) m/s."""
+    """The dry configuration's adjoint: K whole dry iterations of the reference's loop (the
+    pressure pass and mixture density on even iterations, RK4, the boundary passes, the in-loop
+    Shapiro filter, the column balance) forward, and their adjoint through the torch.autograd
+    binding (atjup_b200.autograd.IterationStep: each iteration's input, the nine fields it reads,
+    is its checkpoint; the adjoint recomputes the pressure pass and the RK stages from it). The
+    loss is J = sum_theta sin(colatitude) (zonal-mean w at the top integrated level -
+    u_ref)^2, u_ref = sum_{n=1..8} a_n sin(n theta), a_n seeded U(-50, 150) m/s. Reports the time
+    of forward with checkpoints + backward over the time of K plain forward iterations, and the
+    device memory the chain holds."""
     import numpy as np
     import torch
 
-    from atjup_b200.autograd import rk4_steps
+    from atjup_b200.autograd import iterations
     from atjup_b200.gpu import GpuModel
+    from atjup_b200.params import LIN_FIELDS
 
     m = GpuModel(P, grid)
     m.upload_state(fields)
     im, jm, km = m.shape
-    y0 = m.state_tensors()
+    x0 = m.state_tensors(LIN_FIELDS)
     stream = torch.cuda.ExternalStream(m.stream_handle())
     the = torch.tensor(grid["the"], device="cuda")
     a = np.random.Generator(np.random.Philox(key=20261204)).uniform(-50.0, 150.0, 8) / P.u_0
     uref = sum(float(a[n - 1]) * torch.sin(n * the) for n in range(1, 9))
 
     def forward_plain():
-        m.set_state_tensors(y0)
-        for _ in range(K):
-            m.runge_kutta()
+        m.set_state_tensors(x0, names=LIN_FIELDS)
+        for n in range(1, K + 1):
+            m.step(n, n == 1)
 
     def chain():
-        x = [t.clone().requires_grad_() for t in y0]
-        out = rk4_steps(m, *x, steps=K)
+        x = [t.clone().requires_grad_() for t in x0]
+        out = iterations(m, x, K)
         zm = out[3][im - 2, :, : km - 1].mean(dim=1)
         J = (torch.sin(the) * (zm - uref) ** 2).sum()
         J.backward()
@@ -513,23 +519,28 @@ def adjoint_section(P, grid, fields, K):
     base = torch.cuda.memory_allocated()
     ad_wall, _ = timed(chain)
     torch_peak = torch.cuda.max_memory_allocated() - base
-    lib_scratch = 30 * im * jm * m.field_ptr("t")[1] * 8
+    pitch = m.field_ptr("t")[1]
+    lib_scratch = (30 + 8) * im * jm * pitch * 8
     m.close()
     return {
-        "metric": f"adjoint+forward / forward time, {K} dry RK4 steps",
+        "metric": f"adjoint+forward / forward time, {K} dry iterations",
         "ratio": ad_wall / fwd_wall, "steps": K,
-        "what": "the RK4 step of the dry dynamics (t, u, v, w right-hand sides, level mean, "
-                "hydrostatic integral) through atjup_b200.autograd.RK4Step; checkpoints: each "
-                "step's input",
-        "forward_ms_per_step": fwd_wall / K * 1e3,
-        "forward_device_ms_per_step": fwd_dev / K * 1e3,
-        "adjoint_and_forward_ms_per_step": ad_wall / K * 1e3,
-        "peak_bytes": {"torch_tensors_above_start": torch_peak, "library_scratch": lib_scratch},
+        "what": "whole dry iterations (pressure pass and mixture density on even iterations, "
+                "RK4, boundary passes, 4th-order Shapiro of u, v, w, column balance of v) "
+                "through atjup_b200.autograd.IterationStep (atjup_gpu_iteration_adjoint); "
+                "checkpoints: each iteration's input, t, u, v, w, p_dyn, aux_u, aux_v, aux_w, "
+                "rho_mix",
+        "forward_ms_per_iteration": fwd_wall / K * 1e3,
+        "forward_device_ms_per_iteration": fwd_dev / K * 1e3,
+        "adjoint_and_forward_ms_per_iteration": ad_wall / K * 1e3,
+        "peak_bytes": {"torch_tensors_above_start": torch_peak,
+                       "checkpoints": K * len(LIN_FIELDS) * im * jm * pitch * 8,
+                       "library_scratch": lib_scratch},
     }
 
 
 def run_adjoint(args):
-    """--workload rk4-adjoint: the adjoint section alone, as its own JSON line."""
+    """--workload adjoint: the adjoint section alone, as its own JSON line."""
     d = reference_state("dry", 0, None)
     if d is not None:
         P, _, _, _, grid, fields = model_inputs(d, "dry")
@@ -540,7 +551,7 @@ def run_adjoint(args):
     a = adjoint_section(P, grid, fields, args.steps)
     line = {"metric": a.pop("metric"), "value": a.pop("ratio"), "unit": "x", "n_gpus": 1,
             "steps": args.steps, "warmup": 2, "higher_is_better": False, "dtype": "f64",
-            "data": data, "config": {"workload": "rk4-adjoint", "grid": "41x181x361"}, **a}
+            "data": data, "config": {"workload": "adjoint of whole dry iterations", "grid": "41x181x361"}, **a}
     print(json.dumps(line))
 
 
@@ -557,7 +568,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the Poisson, adjoint and mixed-precision accuracy sections")
-    ap.add_argument("--workload", default="phys", choices=["phys", "dry", "rk4-adjoint"])
+    ap.add_argument("--workload", default="phys", choices=["phys", "dry", "adjoint"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None,
                     help="IMxJMxKM of a smaller synthetic shell, for profiling only (the metric "
@@ -570,7 +581,7 @@ def main():
         run_reference(args, rank, world)
         return
     args.warmup = max(args.warmup, 3)
-    if args.workload == "rk4-adjoint":
+    if args.workload == "adjoint":
         run_adjoint(args)
         return
 

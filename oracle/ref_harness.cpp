@@ -353,6 +353,8 @@ int ref_get_topo(int* out) {
 }
 
 void ref_set_iter(int iter_n) { g_m->iter_n = iter_n; }
+// the model object, for the drop-in harness compiled beside this one (gpu_dropin.cpp)
+void* ref_model_ptr(void) { return g_m; }
 
 // ---- single hot-path routines ----
 void ref_rk4() { g_m->RungeKuttaJup(); }
