@@ -53,10 +53,12 @@ class IterationStep(torch.autograd.Function):
     checkpoint; the adjoint recomputes the pressure pass and the RK stages from it."""
 
     @staticmethod
-    def forward(ctx, model, iter_n, first, *x):
+    def forward(ctx, model, iter_n, first, chained, *x):
         from .params import LIN_FIELDS
         y = tuple(t.detach().contiguous() for t in x)
-        model.set_state_tensors(y, names=LIN_FIELDS, wait=False)
+        if not chained:
+            # chained: x are the outputs of the step just run, which the context still holds
+            model.set_state_tensors(y, names=LIN_FIELDS, wait=False)
         model.step(iter_n, first)
         out = model.state_tensors(LIN_FIELDS)
         ctx.model, ctx.iter_n, ctx.first = model, iter_n, first
@@ -72,13 +74,14 @@ class IterationStep(torch.autograd.Function):
         g = [torch.zeros_like(r) if gr is None else gr.detach().clone().contiguous()
              for gr, r in zip(grads, y)]
         model.iteration_adjoint(g, ctx.iter_n, ctx.first)
-        return (None, None, None, *g)
+        return (None, None, None, None, *g)
 
 
 def iterations(model, x, steps: int, start: int = 1):
     """`steps` differentiable dry iterations from the nine tensors x (LIN_FIELDS order), numbered
-    start, start + 1, ... (the first of a run has first = True)"""
+    start, start + 1, ... (the first of a run has first = True). Between the iterations of the
+    chain the context keeps the state it just produced, so only the first input is copied in."""
     y = tuple(x)
     for n in range(start, start + steps):
-        y = IterationStep.apply(model, n, n == 1, *y)
+        y = IterationStep.apply(model, n, n == 1, n > start, *y)
     return y

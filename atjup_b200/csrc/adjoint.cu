@@ -686,7 +686,8 @@ int lin_forward(AtjupCtx* c, Lin& L) {
             in[f] = (s == 0) ? (const void*)Y[f] : (const void*)L.S[s - 1][f];
             out[f] = L.S[s][f];
         }
-        if ((rc = launch_rk_stage(c, s, in, out))) return rc;
+        const void* x1[4] = {L.S[0][0], L.S[0][1], L.S[0][2], L.S[0][3]};
+        if ((rc = launch_rk_stage(c, s, in, out, x1))) return rc;
     }
     return ATJUP_OK;
 }

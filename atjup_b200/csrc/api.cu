@@ -100,6 +100,7 @@ void free_all(AtjupCtx* c) {
         c->side = nullptr;
     }
     solver_free(c);
+    cone_free(c);
     cudaFree(c->lin);
     c->lin = nullptr;
     cudaFree(c->itlin);
@@ -170,6 +171,7 @@ void atjup_params_default(AtjupParams* p) {
     p->shapiro_inloop = 0; p->shapiro_strength = 1.0;
     p->v_massbal_stride = 1; p->v_massbal_zonal = 1;
     p->precision = ATJUP_PREC_FP64;
+    p->cone_proj_stride = 10; p->cone_proj_margin = 40; p->cone_proj_div = 3;
 }
 
 const char* atjup_gpu_last_error(void) { return g_err.c_str(); }
@@ -190,6 +192,10 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     if (P.top_taper < 0 || P.top_taper > 3 || P.pole_fill_rows < 0 || P.pole_fill_rows > 3) {
         set_error("create: top_taper must be 0..3, pole_fill_rows 0..3");
         return ATJUP_ERR_UNSUPPORTED;
+    }
+    if (P.cone_proj_stride < 0 || P.cone_proj_margin < 0 || P.cone_proj_div < 0) {
+        set_error("create: cone_proj_stride, cone_proj_margin and cone_proj_div must be >= 0");
+        return ATJUP_ERR_ARG;
     }
     if (P.precision != ATJUP_PREC_FP64 && P.precision != ATJUP_PREC_MIXED) {
         set_error("create: precision must be ATJUP_PREC_FP64 or ATJUP_PREC_MIXED");
@@ -408,7 +414,9 @@ int atjup_gpu_set_grid(AtjupCtx* c, const double* rad, const double* the, const 
         ATJUP_CUDA(cudaMemcpy(c->amb_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice));
     }
     solver_free(c);                      // rebuilt by the residual solver for this mask
+    cone_free(c);                        // and the projection's boxes
     c->grid_set = true;
+    if (P.cone_proj_stride > 0) return cone_prepare(c);
     return ATJUP_OK;
 }
 
@@ -517,7 +525,7 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
         {
             Timed tm(c, TK_RK_STAGE);
             dyn = tm.slot;
-            if ((rc = launch_rk_stage(c, s, ins[s], outs[s]))) return rc;
+            if ((rc = launch_rk_stage(c, s, ins[s], outs[s], in1))) return rc;
         }
         if (fork && (rc = join_side(c))) return rc;
         if (dyn >= 0) {
@@ -897,6 +905,11 @@ int atjup_gpu_step(AtjupCtx* c, int32_t iter_n, int32_t first, const AtjupSolveO
     if (P.v_massbal_stride > 0 && iter_n % P.v_massbal_stride == 0) {
         Timed tm(c, TK_BALANCE_V);
         if ((rc = launch_balance_v(c))) return rc;
+    }
+    // the flow around the obstacle re-imposed after the column balance (cJupiterModel.cpp:1362)
+    if (P.cone_proj_stride > 0 && iter_n % P.cone_proj_stride == 0) {
+        Timed tm(c, TK_CONE);
+        if ((rc = launch_cone_projection(c))) return rc;
     }
     if (mca_now && (rc = join_side(c))) return rc;
     if (ph) {

@@ -133,6 +133,7 @@ struct AtjupCtx {
     double* line_m = nullptr;
     double yw_sum = 0.0;
     void* solver = nullptr;           // residual-solver state (solver.cu), built on first use
+    void* cone = nullptr;             // projection around the obstacle (cone.cu), built on first use
 
     // instrumentation: kernel launches issued, and CUDA-event timing per kernel class
     long long launches = 0;
@@ -152,7 +153,7 @@ void set_error(const std::string& msg);
 // kernel classes of the timing hook (atjup_gpu_timing)
 enum { TK_RK_STAGE = 0, TK_RK_AUX, TK_PRESSURE, TK_BC, TK_SHAPIRO, TK_BALANCE_V, TK_MIXTURE,
        TK_SOLVER, TK_SATADJ, TK_SPECIES, TK_CLOSURE, TK_TURB, TK_MICRO, TK_MCA, TK_RK_GROUP,
-       TK_COUNT };
+       TK_CONE, TK_COUNT };
 // an event pair per timed region: timer_begin records the start on st and returns the region's
 // slot (-1 with timing off), timer_end records the end of that slot; regions may nest
 int timer_begin(AtjupCtx* c, int cls, cudaStream_t st);
@@ -166,7 +167,8 @@ inline size_t cell(const AtjupCtx* c, int i, int j, int k) {
 // launchers (return ATJUP_OK or an error code)
 int launch_buoy_ref(AtjupCtx* c, const double* t);
 int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w);
-int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout);
+int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout,
+                    const void* const* X1);
 int mca_setup(AtjupCtx* c);
 int launch_mca(AtjupCtx* c);
 int mca_read_stats(AtjupCtx* c, unsigned long long* out);
@@ -188,6 +190,9 @@ int rk4_adjoint_ext(AtjupCtx* c, double* const a[4], double* lp, double* lrho,
                     double* const laux[3]);
 int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passes, int use_topo);
 int launch_balance_v(AtjupCtx* c);
+int cone_prepare(AtjupCtx* c);
+int launch_cone_projection(AtjupCtx* c);
+void cone_free(AtjupCtx* c);
 int launch_balance_v_buffers(double* v, const int32_t* topo, const double* rad, double* dvc,
                              double* dvrow, int im, int jm, int km, int pitch, double dr,
                              int zonal, cudaStream_t st);

@@ -497,6 +497,15 @@ __global__ void shapiro_i_T_kernel(const double* __restrict__ src, double* __res
     dst[c] = acc;
 }
 
+// the mode of the output at offset o (-2..2) from the nine flags f[0..8] "inside the fluid" at
+// offsets -4..4: 4th order when its four neighbours are inside, 2nd order when only the nearest
+// two are, else a copy
+__device__ __forceinline__ int out_mode(const bool* f, int o) {
+    const int x = o + 4;
+    if (!(f[x] && f[x - 1] && f[x + 1])) return 0;
+    return (f[x - 2] && f[x + 2]) ? 4 : 2;
+}
+
 __global__ void shapiro_j_T_kernel(const double* __restrict__ src, double* __restrict__ dst,
                                    const int32_t* __restrict__ topo, FQ q) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -504,16 +513,18 @@ __global__ void shapiro_j_T_kernel(const double* __restrict__ src, double* __res
     if (k >= q.km) return;
     const size_t row = q.KP;
     const size_t c = ((size_t)i * q.jm + j) * row + k;
-    auto inf = [&](int jj) {
-        return jj >= 0 && jj <= q.jm - 1 && i >= floor_at(topo, q.use_topo, jj, k, q.km);
-    };
+    bool f[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        const int jj = j + e - 4;
+        f[e] = jj >= 0 && jj <= q.jm - 1 && i >= floor_at(topo, q.use_topo, jj, k, q.km);
+    }
     double acc = 0.0;
+#pragma unroll
     for (int d = -2; d <= 2; d++) {
-        const int o = j - d;
+        const int o = j - d;                 // the output reading this input at offset d
         if (o < 0 || o > q.jm - 1) continue;
-        int m = 0;
-        if (inf(o) && inf(o - 1) && inf(o + 1)) m = (inf(o - 2) && inf(o + 2)) ? 4 : 2;
-        const double wgt = fweight(m, d, q);
+        const double wgt = fweight(out_mode(f, -d), d, q);
         if (wgt != 0.0) acc += wgt * src[c - (ptrdiff_t)d * (ptrdiff_t)row];
     }
     dst[c] = acc;
@@ -528,16 +539,16 @@ __global__ void shapiro_k_T_kernel(const double* __restrict__ src, double* __res
     const size_t b = ((size_t)i * q.jm + j) * q.KP;
     if (k == q.km - 1) { dst[b + k] = 0.0; return; }   // the seam input is never read
     const int n = q.km - 1;
-    auto inf = [&](int kk) { return i >= floor_at(topo, q.use_topo, j, kk, q.km); };
-    auto lam = [&](int o) { return src[b + o] + (o == 0 ? src[b + q.km - 1] : 0.0); };
+    auto ring = [n](int kk) { return kk < 0 ? kk + n : (kk >= n ? kk - n : kk); };
+    bool f[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) f[e] = i >= floor_at(topo, q.use_topo, j, ring(k + e - 4), q.km);
     double acc = 0.0;
+#pragma unroll
     for (int d = -2; d <= 2; d++) {
-        const int o = ((k - d) % n + n) % n;
-        int m = 0;
-        if (inf(o) && inf((o - 1 + n) % n) && inf((o + 1) % n))
-            m = (inf((o - 2 + n) % n) && inf((o + 2) % n)) ? 4 : 2;
-        const double wgt = fweight(m, d, q);
-        if (wgt != 0.0) acc += wgt * lam(o);
+        const int o = ring(k - d);
+        const double wgt = fweight(out_mode(f, -d), d, q);
+        if (wgt != 0.0) acc += wgt * (src[b + o] + (o == 0 ? src[b + q.km - 1] : 0.0));
     }
     dst[b + k] = acc;
 }
@@ -637,7 +648,7 @@ int save_base(AtjupCtx* c, const Scratch& S, bool restore) {
     return ATJUP_OK;
 }
 
-int check_supported(AtjupCtx* c, const char* who) {
+int check_supported(AtjupCtx* c, const char* who, int iter_n) {
     const AtjupParams& P = c->P;
     char msg[200];
     if (!c->grid_set) {
@@ -652,6 +663,12 @@ int check_supported(AtjupCtx* c, const char* who) {
     }
     if (P.press_sweeps < 1) {
         snprintf(msg, sizeof(msg), "%s: needs press_sweeps >= 1", who);
+        set_error(msg);
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    if (P.cone_proj_stride > 0 && iter_n % P.cone_proj_stride == 0) {
+        snprintf(msg, sizeof(msg), "%s: the projection around the obstacle runs at this iteration "
+                 "and has no linearisation here (cone_proj_stride)", who);
         set_error(msg);
         return ATJUP_ERR_UNSUPPORTED;
     }
@@ -826,13 +843,14 @@ extern "C" {
 int atjup_gpu_iteration_tlm(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
                             double* const d[9]) {
     if (!c || !args_ok(d)) { set_error("iteration_tlm: null argument"); return ATJUP_ERR_ARG; }
-    int rc = check_supported(c, "iteration_tlm");
+    int rc = check_supported(c, "iteration_tlm", iter_n);
     if (rc) return rc;
     const AtjupParams& P = c->P;
     Scratch S;
     if ((rc = scratch(c, S))) return rc;
     const bool even = (iter_n % 2 == 0) || first;
-    if ((rc = save_base(c, S, false))) return rc;
+    // only the even iterations' base pressure pass and mixture density change the context
+    if (even && (rc = save_base(c, S, false))) return rc;
     if (even) {
         if ((rc = base_pressure_and_density(c, S))) return rc;
         // the perturbed pass reads the base clamp mask; the base state's p_dyn and aux are the
@@ -857,19 +875,19 @@ int atjup_gpu_iteration_tlm(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t 
                                            P.km, c->KP, P.dr, P.v_massbal_zonal, c->stream)))
             return rc;
     }
-    return save_base(c, S, true);
+    return even ? save_base(c, S, true) : ATJUP_OK;
 }
 
 int atjup_gpu_iteration_adjoint(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
                                 double* const a[9]) {
     if (!c || !args_ok(a)) { set_error("iteration_adjoint: null argument"); return ATJUP_ERR_ARG; }
-    int rc = check_supported(c, "iteration_adjoint");
+    int rc = check_supported(c, "iteration_adjoint", iter_n);
     if (rc) return rc;
     const AtjupParams& P = c->P;
     Scratch S;
     if ((rc = scratch(c, S))) return rc;
     const bool even = (iter_n % 2 == 0) || first;
-    if ((rc = save_base(c, S, false))) return rc;
+    if (even && (rc = save_base(c, S, false))) return rc;
     if (even && (rc = base_pressure_and_density(c, S))) return rc;
     if ((parts & ATJUP_LIN_BALANCE) && P.v_massbal_stride > 0 && iter_n % P.v_massbal_stride == 0 &&
         (rc = balance_T(c, a[LV])))
@@ -888,7 +906,7 @@ int atjup_gpu_iteration_adjoint(AtjupCtx* c, int32_t iter_n, int32_t first, int3
         if ((parts & ATJUP_LIN_MIXTURE) && (rc = mixture_lin(c, a, 1))) return rc;
         if ((parts & ATJUP_LIN_PRESSURE) && (rc = pressure_T(c, S, a))) return rc;
     }
-    return save_base(c, S, true);
+    return even ? save_base(c, S, true) : ATJUP_OK;
 }
 
 }  // extern "C"

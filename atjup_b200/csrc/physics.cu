@@ -49,6 +49,14 @@ struct PhysStage {
     const uint8_t* flags;
     const GeoIJ* geo;
     int im, jm, km, KP, stage;
+    // FP64 step: the species keep no accumulator. Stage s's right-hand side is recovered from the
+    // next stage input as (X_{s+1} - y_n) / c_s (exact: X_{s+1} lies within a factor 2 of y_n,
+    // so the subtraction is exact, Sterbenz), so stage 3 reads X1 and X2 beside its own input X3
+    // instead of one accumulator that stages 0-2 would each write and stages 1-2 read.
+    int acc_free;
+    const double* x1[ATJUP_S_COUNT];   // X1, X2 of the species (stage 3, acc_free)
+    const double* x2[ATJUP_S_COUNT];
+    double inv_c_half, inv_dt;         // 1 / c of stages 0 and 1 (2 / dt) and of stage 2 (1 / dt)
     double c_in, wgt, dt, one_sixth;
     double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
     double coef[ATJUP_S_COUNT];        // species_diff_scale / (sc re)
@@ -142,81 +150,131 @@ __device__ __forceinline__ int precip_slot(int s) {
 // float, float> (it reads the live fields), stages 1-2 <float, float, float, float>, stage 3
 // <float, double, float, float>.
 
-// One thread per (cell, species): blockIdx.z = i * ATJUP_S_COUNT + species, so the eleven species
-// blocks of one radial plane run back to back and the plane's u, v, w, nue come from DRAM once and
-// from L2 for the other ten; each species' stencil is its own coalesced stream.
-// blockIdx.y * blockDim.y + threadIdx.y = j, blockIdx.x * blockDim.x + threadIdx.x = k.
-template <typename TI, typename TO, typename TA, typename R>
-__global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z / ATJUP_S_COUNT;
-    const int s = blockIdx.z - i * ATJUP_S_COUNT;
-    if (k >= a.km || j >= a.jm) return;
-    // Every load is issued before the integrated-cell test (one memory round trip, not two):
-    // the neighbour addresses are clamped into the block, so the boundary cells that the test
-    // then sends to the copy below read only their own cell.
-    const Cell x = cell_of(a, i, j, k);
+// One thread per cell, the eleven species in turn (an unrolled loop: each species' index, sources
+// and coefficients are compile-time): what the species share -- the cell's indices, its flags,
+// u, v, w, nue and the eddy diffusivity nue_t / 0.9, the row's geometry -- is read and formed once
+// per cell. Each species reads its own 7-point stencil (coalesced along k), its FP64
+// time-level-n value, its accumulator (or, FP64 stage 3, X1 and X2) and its frozen sources.
+// blockIdx.y * blockDim.y + threadIdx.y = j, blockIdx.x * blockDim.x + threadIdx.x = k,
+// blockIdx.z = i.
+template <typename R>
+struct CellShared {
+    R u0, v_invrm, w_invrs, two_inv_rm, inv_rm2, ci, is2, nue_t_s;
+    double rho;
+};
+
+template <int S, typename TI, typename TO, typename TA, typename R>
+__device__ __forceinline__ void species_one(const PhysStage& a, const Cell& x,
+                                            const CellShared<R>& z) {
     const size_t c = x.c;
-    const TI* F = static_cast<const TI*>(a.q_in[s]);
-    const uint8_t fl = a.flags[c];
+    const TI* F = static_cast<const TI*>(a.q_in[S]);
     const R f0 = (R)F[c], fip = (R)F[x.cip], fim = (R)F[x.cim], fjp = (R)F[x.cjp];
     const R fjm = (R)F[x.cjm], fkp = (R)F[x.ckp], fkm = (R)F[x.ckm];
-    const R u0 = (R)static_cast<const TI*>(a.u)[c];
-    const R v0 = (R)static_cast<const TI*>(a.v)[c];
-    const R w0 = (R)static_cast<const TI*>(a.w)[c];
-    const double nv = a.has_nue ? a.nue[c] : 0.0;
-    const double qn = a.q_n[s][c];
-    const R acc_in = (a.stage == 0) ? (R)0 : (R)static_cast<const TA*>(a.acc[s])[c];
-    double src0, src1 = 0.0, src2 = 0.0;
-    if (s == ATJUP_S_H2S) {
+    const double qn = a.q_n[S][c];
+    R acc_in = (R)0;
+    double x1 = 0.0, x2 = 0.0;
+    if (a.acc_free) {
+        if (a.stage == 3) { x1 = a.x1[S][c]; x2 = a.x2[S][c]; }
+    } else if (a.stage > 0) {
+        acc_in = (R)static_cast<const TA*>(a.acc[S])[c];
+    }
+    double src0, src1 = 0.0;
+    if constexpr (S == ATJUP_S_H2S) {
         src0 = a.mf_h2s[c];
-    } else if (s == ATJUP_S_NH3) {
+    } else if constexpr (S == ATJUP_S_NH3) {
         src0 = a.mf_nh3[c];
         src1 = a.sprec[3][c];
-    } else if (s == ATJUP_S_NH4SH) {
+    } else if constexpr (S == ATJUP_S_NH4SH) {
         src0 = a.fluxlim[c];
         src1 = a.mf_nh4sh[c];
-        src2 = a.rho_mix[c];
     } else {
-        src0 = a.sprec[precip_slot(s)][c];
+        src0 = a.sprec[precip_slot(S)][c];
     }
-    if (!(fl & NB_INT)) {
-        if (a.stage < 3) static_cast<TO*>(a.q_out[s])[c] = (TO)a.q_live[s][c];
-        return;
-    }
-    const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
-    const R v_invrm = v0 * (R)g.inv_rm;
-    const R w_invrs = w0 * (R)g.inv_rmsinthe;
-    const R two_inv_rm = (R)2 * (R)g.inv_rm;
-    double nue_t64 = 0.0;
-    if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t64 = a.turb_coupling * dmax(0.0, nv);
-    const R nue_t = (R)nue_t64;
-    const R nue_t_s = nue_t / (R)0.9;
     const R d1r = (fip - fim) * (R)a.inv_2dr;
     const R d2r = (fip - (R)2 * f0 + fim) * (R)a.inv_dr2;
     const R d1t = (fjp - fjm) * (R)a.inv_2dthe;
     const R d2t = (fjp - (R)2 * f0 + fjm) * (R)a.inv_dthe2;
     const R d1p = (fkp - fkm) * (R)a.inv_2dphi;
     const R d2p = (fkp - (R)2 * f0 + fkm) * (R)a.inv_dphi2;
-    const R transport = u0 * d1r + v_invrm * d1t + w_invrs * d1p;
-    const R diffusion = d2r + d1r * two_inv_rm + d2t * (R)g.inv_rm2 +
-                        d1t * (R)g.costhe_inv_rm2sinthe + d2p * (R)g.inv_rm2sinthe2;
-    const R coef = (R)a.coef[s] + nue_t_s;
+    const R transport = z.u0 * d1r + z.v_invrm * d1t + z.w_invrs * d1p;
+    const R diffusion = d2r + d1r * z.two_inv_rm + d2t * z.inv_rm2 + d1t * z.ci + d2p * z.is2;
+    const R coef = (R)a.coef[S] + z.nue_t_s;
     R r;
-    if (s == ATJUP_S_H2S) {
+    if constexpr (S == ATJUP_S_H2S) {
         r = -transport + diffusion * coef + (R)(a.chemical_reaction * src0);
-    } else if (s == ATJUP_S_NH3) {
+    } else if constexpr (S == ATJUP_S_NH3) {
         r = -transport + diffusion * coef + (R)(a.chemical_reaction * src0) +
             (R)(a.precip_coupling * src1);
-    } else if (s == ATJUP_S_NH4SH) {
-        const double v_stokes = a.stokes_pre * (a.rg_nh4sh - src2) * a.g / a.mue_mix;
+    } else if constexpr (S == ATJUP_S_NH4SH) {
+        const double v_stokes = a.stokes_pre * (a.rg_nh4sh - z.rho) * a.g / a.mue_mix;
         r = -transport + (R)src0 + diffusion * coef + (R)(a.chemical_reaction * src1) +
             (R)(v_stokes / a.u_0) * d1r;
     } else {
         r = -transport + diffusion * coef + (R)(a.precip_coupling * src0);
     }
-    rk_update<TO, TA, R>(a, s, c, r, acc_in, qn);
+    if (a.acc_free) {
+        // FP64: no accumulator; stage 3 sums the right-hand sides recovered from X1, X2, X3
+        if (a.stage < 3) {
+            static_cast<TO*>(a.q_out[S])[c] = (TO)(qn + (double)((R)a.c_in * r));
+        } else {
+            const double k1 = (x1 - qn) * a.inv_c_half, k2 = (x2 - qn) * a.inv_c_half;
+            const double k3 = ((double)f0 - qn) * a.inv_dt;
+            const double acc = ((k1 + 2.0 * k2) + 2.0 * k3) + (double)r;
+            double q = qn + a.dt * acc * a.one_sixth;
+            q = (S == ATJUP_S_NH4SH) ? ((q < 0.0) ? 0.0 : q) : dmax(0.0, q);
+            static_cast<TO*>(a.q_out[S])[c] = (TO)q;
+        }
+        return;
+    }
+    rk_update<TO, TA, R>(a, S, c, r, acc_in, qn);
+}
+
+template <int S, typename TI, typename TO, typename TA, typename R>
+__device__ __forceinline__ void species_all(const PhysStage& a, const Cell& x,
+                                            const CellShared<R>& z) {
+    species_one<S, TI, TO, TA, R>(a, x, z);
+    if constexpr (S + 1 < ATJUP_S_COUNT) species_all<S + 1, TI, TO, TA, R>(a, x, z);
+}
+
+template <typename TI, typename TO, typename TA, typename R>
+__global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= a.km || j >= a.jm) return;
+    const Cell x = cell_of(a, i, j, k);
+    const size_t c = x.c;
+    // the loads the species share, issued with the flag before the integrated-cell test
+    const uint8_t fl = a.flags[c];
+    const R u0 = (R)static_cast<const TI*>(a.u)[c];
+    const R v0 = (R)static_cast<const TI*>(a.v)[c];
+    const R w0 = (R)static_cast<const TI*>(a.w)[c];
+    const double nv = a.has_nue ? a.nue[c] : 0.0;
+    const double rho = a.rho_mix[c];
+    if (!(fl & NB_INT)) {
+        // the cell keeps its live values through the step
+        if (a.stage < 3) {
+#pragma unroll
+            for (int s = 0; s < ATJUP_S_COUNT; s++)
+                static_cast<TO*>(a.q_out[s])[c] = (TO)a.q_live[s][c];
+        }
+        return;
+    }
+    const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
+    CellShared<R> z;
+    z.u0 = u0;
+    z.v_invrm = v0 * (R)g.inv_rm;
+    z.w_invrs = w0 * (R)g.inv_rmsinthe;
+    z.two_inv_rm = (R)2 * (R)g.inv_rm;
+    z.inv_rm2 = (R)g.inv_rm2;
+    z.ci = (R)g.costhe_inv_rm2sinthe;
+    z.is2 = (R)g.inv_rm2sinthe2;
+    double nue_t64 = 0.0;
+    if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t64 = a.turb_coupling * dmax(0.0, nv);
+    const R nue_t = (R)nue_t64;
+    z.nue_t_s = nue_t / (R)0.9;
+    z.rho = rho;
+    species_all<0, TI, TO, TA, R>(a, x, z);
 }
 
 // k*, omega*: transport, diffusion with the model's coefficients, and the closure sources
@@ -463,11 +521,17 @@ PhysStage stage_args(AtjupCtx* c, int stage, const void* const* vin) {
     for (int s = 0; s < ATJUP_S_COUNT + 2; s++) {
         const int id = kScalarField[s];
         double* live = c->f[id];
-        // the stage buffers hold doubles, or floats in their first half in the mixed step
-        const void* in[4] = {live, c->S1[s], c->S2[s], c->S1[s]};
-        void* out[4] = {c->S1[s], c->S2[s], c->S1[s], live};
+        // the stage buffers hold doubles, or floats in their first half in the mixed step; the
+        // FP64 species keep X1, X2 to the end and put X3 where the accumulator would be
+        const bool af = (s < ATJUP_S_COUNT) && c->step_prec != ATJUP_PREC_MIXED;
+        const void* in[4] = {live, c->S1[s], c->S2[s], af ? (const void*)c->Sacc[s] : c->S1[s]};
+        void* out[4] = {c->S1[s], c->S2[s], af ? (void*)c->Sacc[s] : c->S1[s], live};
         a.q_in[s] = in[stage];
         a.q_out[s] = out[stage];
+        if (s < ATJUP_S_COUNT) {
+            a.x1[s] = c->S1[s];
+            a.x2[s] = c->S2[s];
+        }
         a.q_n[s] = c->fn[id];
         a.acc[s] = c->Sacc[s];
         a.q_live[s] = live;
@@ -492,6 +556,9 @@ PhysStage stage_args(AtjupCtx* c, int stage, const void* const* vin) {
     a.flags = c->nbflags;
     a.geo = c->geo;
     a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP; a.stage = stage;
+    a.acc_free = (c->step_prec != ATJUP_PREC_MIXED) ? 1 : 0;
+    a.inv_c_half = 2.0 / P.dt;
+    a.inv_dt = 1.0 / P.dt;
     a.c_in = (stage == 0 || stage == 1) ? 0.5 * P.dt : (stage == 2 ? P.dt : 0.0);
     a.wgt = (stage == 0 || stage == 3) ? 1.0 : 2.0;
     a.dt = P.dt;
@@ -534,8 +601,7 @@ static int launch_typed(AtjupCtx* c, const PhysStage& a, int what, cudaStream_t 
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
     if (what == 0) {
-        const dim3 sgrid(grid.x, grid.y, P.im * ATJUP_S_COUNT);
-        species_stage_kernel<TI, TO, TA, R><<<sgrid, block, 0, st>>>(a);
+        species_stage_kernel<TI, TO, TA, R><<<grid, block, 0, st>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");
     } else {

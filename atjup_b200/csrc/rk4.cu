@@ -43,6 +43,12 @@ struct StageConst {
     double rad_coupling, precip_coupling, turb_coupling;
     int pgrad_wall, adiabatic, adiabatic_rho, hydro_split, use_hp, cell_hold;
     int has_nue, has_heating, precip_local;
+    // FP64 step: the accumulator is written once, at stage 2, from the right-hand sides of stages
+    // 0 and 1 recovered as (X_{s+1} - y_n) / c_s (X1 read per cell, X2 the stage's own input; the
+    // subtraction is exact, X lying within a factor 2 of y_n) plus stage 2's own: stages 0 and 1
+    // neither write nor read it
+    int acc_free;
+    double inv_c_half;         // 1 / c_in of stages 0 and 1 (2 / dt)
 };
 
 // The stage buffers X (stage input), Xo (next stage input) and acc are typed by the kernel's
@@ -50,6 +56,7 @@ struct StageConst {
 // frozen inputs are FP64.
 struct StagePtrs {
     const void* X[4];
+    const void* X1[4];         // stage 2 with acc_free: the stage-1 input (X1), read per cell
     void* Xo[4];
     double* Y[4];
     void* acc[4];
@@ -126,10 +133,13 @@ __device__ __forceinline__ void issue_extra(StageSmem<TI, TA>& S, const StagePtr
         const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
         const size_t c = ((size_t)i * q.jm + j) * q.KP + k;
         if (q.stage > 0) {
+            // the per-cell accumulator, or with acc_free X1 at stage 2 and the accumulator at 3
+            const bool need_ax = !q.acc_free || q.stage >= 2;
+            const void* const* src = (q.acc_free && q.stage == 2) ? a.X1 : (const void* const*)a.acc;
 #pragma unroll
             for (int f = 0; f < 4; f++) {
                 cp_async8(&S.Yx[sl][f][tid], a.Y[f] + c);
-                cp_async(&S.ax[sl][f][tid], static_cast<const TA*>(a.acc[f]) + c);
+                if (need_ax) cp_async(&S.ax[sl][f][tid], static_cast<const TA*>(src[f]) + c);
             }
         }
         cp_async8(&S.ex[sl][0][tid], a.rho + c);
@@ -375,8 +385,22 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                     const double y0[4] = {(double)Tt[h], (double)Ut[h], (double)Vt[h], (double)Wt[h]};
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
-                        static_cast<TA*>(a.acc[f])[c] = (TA)((R)q.wgt * rhs[f]);
+                        if (!q.acc_free) static_cast<TA*>(a.acc[f])[c] = (TA)((R)q.wgt * rhs[f]);
                         static_cast<TO*>(a.Xo[f])[c] = (TO)(y0[f] + q.c_in * (double)rhs[f]);
+                    }
+                } else if (q.acc_free && q.stage < 3) {
+                    // acc_free (FP64): stage 1 only forms X2; stage 2 forms X3 and the accumulator
+                    // k1 + 2 k2 + 2 k3 with k1 = (X1 - y_n) / c, k2 = (X2 - y_n) / c
+                    const double x2[4] = {(double)Tt[h], (double)Ut[h], (double)Vt[h], (double)Wt[h]};
+#pragma unroll
+                    for (int f = 0; f < 4; f++) {
+                        const double yn = S.Yx[xs][f][tid];
+                        if (q.stage == 2) {
+                            const double k1 = ((double)S.ax[xs][f][tid] - yn) * q.inv_c_half;
+                            const double k2 = (x2[f] - yn) * q.inv_c_half;
+                            static_cast<TA*>(a.acc[f])[c] = (TA)((k1 + 2.0 * k2) + q.wgt * (double)rhs[f]);
+                        }
+                        static_cast<TO*>(a.Xo[f])[c] = (TO)(yn + q.c_in * (double)rhs[f]);
                     }
                 } else if (q.stage < 3) {
 #pragma unroll
@@ -548,12 +572,15 @@ static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, 
 }
 
 // Xin / Xout: the stage input and the next stage input (stage 0 reads the FP64 state itself;
-// the other buffers are FP64 or, in the mixed step, FP32)
-int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout) {
+// the other buffers are FP64 or, in the mixed step, FP32); X1: the stage-1 input, which stage 2
+// reads in the FP64 step (may be null otherwise)
+int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const* Xout,
+                    const void* const* X1) {
     const AtjupParams& P = c->P;
     StagePtrs a{};
     for (int f = 0; f < 4; f++) {
         a.X[f] = Xin[f];
+        a.X1[f] = X1 ? X1[f] : nullptr;
         a.Xo[f] = Xout ? Xout[f] : nullptr;
         a.Y[f] = c->f[ATJUP_F_T + f];
         a.acc[f] = c->acc[f];
@@ -619,6 +646,12 @@ int launch_rk_stage(AtjupCtx* c, int stage, const void* const* Xin, void* const*
     q.has_nue = (P.has_nue && a.nue) ? 1 : 0;
     q.has_heating = (P.has_heating && a.Q_rad && a.Q_precip) ? 1 : 0;
     q.precip_local = (P.precip_rho_local && P.local_rho) ? 1 : 0;
+    q.acc_free = (c->step_prec != ATJUP_PREC_MIXED) ? 1 : 0;
+    q.inv_c_half = 2.0 / P.dt;
+    if (q.acc_free && stage == 2 && !X1) {
+        set_error("rk_stage: stage 2 needs the stage-1 input");
+        return ATJUP_ERR_ARG;
+    }
 
     if (c->step_prec != ATJUP_PREC_MIXED)
         return launch_stage_t<double, double, double, double>(c, a, q, "rk_stage");

@@ -59,6 +59,9 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_shapiro.argtypes = [vp, i32, i32, dbl, i32, i32]
     L.atjup_gpu_mixture_density.argtypes = [vp]
     L.atjup_gpu_balance_column_v.argtypes = [vp, ctypes.POINTER(dbl)]
+    L.atjup_gpu_cone_project.argtypes = [vp]
+    L.atjup_gpu_cone_stats.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), i32,
+                                       ctypes.POINTER(i32)]
     L.atjup_gpu_step.argtypes = [vp, i32, i32, ctypes.POINTER(_p.AtjupSolveOpts)]
     L.atjup_gpu_nonfinite_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.atjup_gpu_synchronize.argtypes = [vp]
@@ -399,6 +402,22 @@ class GpuModel:
         _check(self.L.atjup_gpu_balance_column_v(self.ctx, ctypes.byref(s)))
         return s.value
 
+    def cone_project(self):
+        """cJupiterModel::projectAroundObstacle(in_loop = true) (InitValues_Jup.cpp:1595-1822):
+        one call, warm-started from the previous call's phi of each level and solve."""
+        _check(self.L.atjup_gpu_cone_project(self.ctx))
+
+    def cone_stats(self):
+        """(levels i, sweeps [levels, 2]) of the last projection: SOR sweeps of the divergence
+        solve (0 when off) and of the wall-flux solve per level."""
+        n = ctypes.c_int32()
+        _check(self.L.atjup_gpu_cone_stats(self.ctx, None, None, 0, ctypes.byref(n)))
+        lv = (ctypes.c_int32 * max(n.value, 1))()
+        sw = (ctypes.c_int32 * max(2 * n.value, 1))()
+        _check(self.L.atjup_gpu_cone_stats(self.ctx, lv, sw, n.value, ctypes.byref(n)))
+        return (np.array(lv[:n.value], dtype=np.int32),
+                np.array(sw[:2 * n.value], dtype=np.int32).reshape(n.value, 2))
+
     def satadj(self, gas: str, gp: _p.AtjupGasParams, stats: bool = True):
         """SaturationAdjustmentJup(*this).run(gas, ...) (SaturationAdjustment.h:255-746) on the
         device fields of gas ("H2O", "NH3" or "CH4"); returns (adjusted, not converged, dry
@@ -426,7 +445,7 @@ class GpuModel:
     # ---- instrumentation ----
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
                       "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca",
-                      "rk_group")
+                      "rk_group", "cone")
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

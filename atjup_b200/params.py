@@ -14,7 +14,7 @@ import math
 import os
 from typing import Mapping
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # field ids (include/atjup_gpu.h)
 F_T, F_U, F_V, F_W, F_P_DYN, F_P_HYDRO, F_P_STAT, F_RHO_MIX, F_WALL_NUE, F_NUE, \
@@ -109,6 +109,8 @@ _FIELDS = [
     ("shapiro_inloop", ctypes.c_int32), ("shapiro_strength", ctypes.c_double),
     ("v_massbal_stride", ctypes.c_int32), ("v_massbal_zonal", ctypes.c_int32),
     ("precision", ctypes.c_int32),
+    ("cone_proj_stride", ctypes.c_int32), ("cone_proj_margin", ctypes.c_int32),
+    ("cone_proj_div", ctypes.c_int32),
 ]
 
 
@@ -440,6 +442,11 @@ def resolve_params(env: Mapping[str, str] | None = None, *, im=41, jm=181, km=36
     vortex = _env(env, "ATJUP_VORTEX", 1) != 0
     p.v_massbal_zonal = int(_env(env, "ATJUP_V_MASSBAL_ZONAL", 1 if vortex else 0) != 0)
     p.precision = PREC_FP64
+    # the in-loop projection around the obstacle, cJupiterModel.h:919-933 (a stride or H at or
+    # below zero switches its part off, as the reference's "> 0" tests do)
+    p.cone_proj_stride = max(0, _env(env, "ATJUP_CONE_PROJ_STRIDE", 10))
+    p.cone_proj_margin = _env(env, "ATJUP_CONE_PROJ_MARGIN", 40)
+    p.cone_proj_div = max(0, _env(env, "ATJUP_CONE_PROJ_DIV", 3))
     return p
 
 

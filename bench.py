@@ -105,14 +105,28 @@ CONFIGS = {
         "parallelism": "replicas (the path does not shard)",
     },
 }
-# Algorithmic bytes per cell of one RK stage launch, averaged over the four stages of a step.
-#
-# A field of the RK step costs, over the four stages: stage 0 reads its state Y and writes the
-# next stage input X and the accumulator; stages 1-2 read X, Y and the accumulator and write X
-# and the accumulator; stage 3 reads X, Y and the accumulator and writes Y. With FP64 everywhere
-# that is 17 x 8 = 136 B per field and step (the 17F of N b (17F + 4A)); with FP32 X and
-# accumulators (mixed) 16 + 24 + 24 + 24 = 88 B. Per stage: 34 B (FP64), 22 B (mixed).
-FIELD_STAGE_BYTES = {"fp64": 34.0, "mixed": 22.0}
+# The roofline's numerator: the algorithmic bytes of one RK stage by the scope's formula,
+# B_rk = N b (17 F + 4 A) + 4 N per RK step (a quarter per stage). F = fields integrated (dry 4:
+# t, u, v, w; full physics 17: with the 11 species and k*, omega*), A = frozen per-cell inputs the
+# right-hand sides read (dry 5: p_dyn, p_hydro, p_stat, rho_mix, wall_nue; full physics 21: with
+# nue, Q_rad, Q_precip, 9 S_precip, 3 mass fluxes, the NH4SH flux limiter), b = 8 (FP64) or 4
+# (the mixed step, whose stage buffers are FP32), the mask one byte per stage. Per field the 17 b
+# is the classic bookkeeping: stage 0 reads Y and writes X1 and the accumulator, stages 1-2 read
+# X, Y and the accumulator and write X and the accumulator, stage 3 reads X, Y and the accumulator
+# and writes Y.
+def formula_bytes_per_cell_stage(prec, phys):
+    F, A = (17, 21) if phys else (4, 5)
+    b = 8 if prec == "fp64" else 4
+    return (b * (17 * F + 4 * A) + 4) / 4
+
+
+# The bytes this implementation moves per cell and stage launch, averaged over the four stages.
+# FP64: the species keep no accumulator (stage 3 recovers the stage right-hand sides from X1, X2,
+# X3 and y_n: 3 + 3 + 3 + 5 = 14 accesses of 8 B per species and step, 28 B per stage), the
+# dynamics write it once at stage 2 (2 + 3 + 5 + 4 = 14 per field and step, 28 B per stage), the
+# closure keeps the classic 17 (34 B). Mixed (FP32 X and accumulators, FP64 y_n): 16 + 24 + 24 + 24
+# = 88 B per field and step, 22 B per stage.
+FIELD_STAGE_BYTES = {"fp64": 28.0, "mixed": 22.0}
 
 
 def rk_stage_bytes(prec, phys):
@@ -124,11 +138,12 @@ def rk_stage_bytes(prec, phys):
 
 def species_stage_bytes(prec):
     # u, v, w (FP64 at stage 0, the stage buffers' type after), nue and the flag byte; per species
-    # the stencil's stage input, the FP64 n copy, the output and the accumulator; the FP64 frozen
-    # sources (S_precip of 9 species, the mass fluxes of H2S and NH3, the NH4SH limiter, mass flux
-    # and mixture density: 112 B). FP64: 33 + 11 x 36 + 112 = 541 B.
+    # the stencil's stage input, the FP64 n copy and the output (and X1, X2 at stage 3, or the
+    # accumulator in the mixed step); the FP64 frozen sources (S_precip of 9 species, the mass
+    # fluxes of H2S and NH3, the NH4SH limiter, mass flux and mixture density: 112 B).
+    # FP64: 33 + 11 x 28 + 112 = 453 B.
     uvw = 24.0 if prec == "fp64" else (24 + 3 * 12) / 4
-    per = 36.0 if prec == "fp64" else 5 + 8 + 5 + 6
+    per = 28.0 if prec == "fp64" else 5 + 8 + 5 + 6
     return uvw + 8 + 1 + 11 * per + 112
 
 
@@ -144,33 +159,44 @@ def stage_kernels(prec, phys):
     return {"rk_stage": ("rk_stage_kernel", rk_stage_bytes(prec, phys)),
             "species": ("species_stage_kernel", species_stage_bytes(prec)),
             "closure": ("closure_stage_kernel", closure_stage_bytes(prec))}
-# (algorithmic bytes per cell and launch; times the cells of the shell)
+# (bytes moved per cell and launch; times the cells of the shell)
 
 
 def stage_roofline(prec, phys, per_class, peak):
     """The roofline of one RK stage. With full physics the species and closure kernels of a stage
     run on a second stream beside the dynamics kernel, so each kernel's event time includes the
     others' share of the GPU: the unit is the stage (timing class rk_group, first kernel start to
-    last kernel end) with the three kernels' algorithmic bytes and DRAM traffic. The dry step has the dynamics kernel alone."""
+    last kernel end). `achieved` is the stage's algorithmic bytes by the scope's formula over that
+    time; `moved_*` the bytes this implementation moves, and `traffic` the DRAM bytes ncu measured.
+    The dry step has the dynamics kernel alone."""
     kernels = stage_kernels(prec, phys)
     parts = [k for k in ("species", "closure", "rk_stage") if k in per_class] if phys else ["rk_stage"]
     names = [kernels[k][0] for k in parts]
-    kbytes = sum(kernels[k][1] for k in parts) * N_CELLS
+    moved = sum(kernels[k][1] for k in parts) * N_CELLS
+    fbytes = formula_bytes_per_cell_stage(prec, phys) * N_CELLS
     tpc = [STAGE_TRAFFIC_PER_CELL.get((prec, n)) for n in names]
     traffic = None if None in tpc else sum(tpc) * N_CELLS
     ms, n = per_class["rk_group" if phys else "rk_stage"]
-    achieved = kbytes / (ms / n / 1e3) / 1e9
+    t = ms / n / 1e3
+    achieved = fbytes / t / 1e9
+    F, A = (17, 21) if phys else (4, 5)
     return {"kernel": " + ".join(names) + (" (one RK stage, two streams)" if len(names) > 1 else ""),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes_per_launch": kbytes,
+            "frac": achieved / peak, "traffic": traffic,
+            "algorithmic_bytes_per_launch": fbytes,
+            "algorithmic_bytes_formula": "(N b (17 F + 4 A) + 4 N) / 4 per stage, N = %d, F = %d, "
+                                         "A = %d, b = %d" % (N_CELLS, F, A, 8 if prec == "fp64" else 4),
+            "moved_bytes_per_launch": moved, "moved_gbs": moved / t / 1e9,
+            "moved_frac": moved / t / 1e9 / peak,
             "avg_launch_ms": ms / n, "launches": n}
+
 
 # DRAM bytes (read + write) per cell and launch, averaged over the four stages of one RK step:
 # dram__bytes_read.sum + dram__bytes_write.sum of each stage launch in one ncu capture of this
 # workload on the 41x181x361 shell.
 STAGE_TRAFFIC_PER_CELL = {
-    ("fp64", "species_stage_kernel"): 560.1, ("fp64", "closure_stage_kernel"): 100.1,
-    ("fp64", "rk_stage_kernel"): 199.4,
+    ("fp64", "species_stage_kernel"): 449.2, ("fp64", "closure_stage_kernel"): 106.8,
+    ("fp64", "rk_stage_kernel"): 178.5,
     ("mixed", "species_stage_kernel"): 406.3, ("mixed", "closure_stage_kernel"): 68.4,
     ("mixed", "rk_stage_kernel"): 153.4,
 }
@@ -456,6 +482,44 @@ def poisson_section(m, stream):
                             "hbm_gbs": gbs, "hbm_frac": gbs / peak,
                             "algorithmic_bytes_per_sweep": n * 25}
     out["peak"] = {"hbm_gbs": peak, "kind": kind}
+    return out
+
+
+def cone_section(P, grid, fields, calls=3):
+    """The in-loop projection around the obstacle (projectAroundObstacle(in_loop = true), every
+    ATJUP_CONE_PROJ_STRIDE = 10 iterations by the reference's default; both benchmark
+    configurations pin it off, so it is timed here on its own): `calls` calls on the dry
+    configuration's state, the first from zero and the rest warm-started, each timed with CUDA
+    events on the library's stream, beside the reference's own per-call time on this host."""
+    import torch
+    m = build_model(P, None, None, None, grid, fields)
+    stream = torch.cuda.ExternalStream(m.stream_handle())
+    out = {"what": "per level cutting the obstacle (26 levels), the divergence solve (H = 3) and "
+                   "the wall-flux solve by lexicographic SOR to 1e-10, bit-identical to the "
+                   "reference; margin 40 cells", "calls": []}
+    m.cone_stats()                      # the static part (boxes, flags, buffers) outside the timing
+    for c in range(calls):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m.synchronize()
+        ev0.record(stream)
+        m.cone_project()
+        ev1.record(stream)
+        ev1.synchronize()
+        levels, sweeps = m.cone_stats()
+        out["calls"].append({"s": ev0.elapsed_time(ev1) / 1e3, "warm_start": c > 0,
+                             "levels": int(levels.size), "sweeps_max": int(sweeps.max()),
+                             "sweeps_mean": float(sweeps[sweeps > 0].mean())})
+    m.close()
+    out["gpu_s_per_call"] = sum(x["s"] for x in out["calls"]) / calls
+    cmd = [sys.executable, str(ROOT / "oracle" / "ref_bench.py"), "--cone", "2"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600).stdout
+        d = json.loads(r.strip().splitlines()[-1])
+        out["reference_s_per_call"] = d.get("cone_s_per_call")
+        out["reference_threads"] = d.get("threads")
+    except Exception as e:   # noqa: BLE001 -- the CPU leg is reported, not required
+        out["reference_s_per_call"] = None
+        out["reference_unavailable"] = str(e)
     return out
 
 
@@ -807,6 +871,7 @@ def main():
         else:
             Pd, _, _, _, gd, fd = synthetic_inputs("dry", 0)
         line["adjoint"] = adjoint_section(Pd, gd, fd, 50)
+        line["cone_projection"] = cone_section(Pd, gd, fd)
     if dist is not None:
         dist.barrier()
     if rank == 0:

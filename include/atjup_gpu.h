@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define ATJUP_ABI_VERSION 1
+#define ATJUP_ABI_VERSION 2
 
 /* ---- status codes ---- */
 enum {
@@ -136,6 +136,11 @@ typedef struct AtjupParams {
                                        /* time-level-n state, the final update, the dynamics RHS,  */
                                        /* the pressure, the level means, the column balance and    */
                                        /* the loop's physics stay FP64                              */
+    /* the in-loop projection around the obstacle (InitValues_Jup.cpp:1595-1822, called at      */
+    /* cJupiterModel.cpp:1356-1363 after the column balance of v)                              */
+    int32_t cone_proj_stride;          /* ATJUP_CONE_PROJ_STRIDE 10 (0 = off)                    */
+    int32_t cone_proj_margin;          /* ATJUP_CONE_PROJ_MARGIN 40: box cells beyond the body   */
+    int32_t cone_proj_div;             /* ATJUP_CONE_PROJ_DIV 3: H of the divergence solve       */
 } AtjupParams;
 
 typedef struct AtjupSolveOpts {
@@ -245,6 +250,18 @@ int atjup_gpu_mixture_density(AtjupCtx* ctx);
 
 /* cJupiterModel::balanceColumnV (InitValues_Jup.cpp:1500-1538); vshift may be NULL. */
 int atjup_gpu_balance_column_v(AtjupCtx* ctx, double* vshift);
+
+/* cJupiterModel::projectAroundObstacle(in_loop = true) (InitValues_Jup.cpp:1595-1822): per level
+ * that cuts the obstacle, the divergence solve (cone_proj_div > 0) and the wall-flux solve, each
+ * warm-started from its own phi of the previous call (zero before the first), v and w incremented,
+ * then the seam copy of v and w. atjup_gpu_step calls it every cone_proj_stride iterations; this
+ * entry runs one call on its own. The result is the reference's to the bit. */
+int atjup_gpu_cone_project(AtjupCtx* ctx);
+/* The levels of the projection and the SOR sweeps of its last call, per level: sweeps[2 l] of the
+ * divergence solve (0 when off), sweeps[2 l + 1] of the wall-flux solve (40001: not converged
+ * within 40000 sweeps, the reference's count). Fills up to cap levels; *n_levels = all levels. */
+int atjup_gpu_cone_stats(AtjupCtx* ctx, int32_t* level_i, int32_t* sweeps, int32_t cap,
+                         int32_t* n_levels);
 
 /* The column balance of v for callers that cannot allocate device memory. No counterpart in the
  * reference: it computes what atjup_gpu_balance_column_v computes, on the caller's own device
@@ -520,7 +537,9 @@ int atjup_gpu_rk4_adjoint(AtjupCtx* ctx, double* const a[4]);
  *   atjup_gpu_iteration_adjoint  a in: the adjoint of the iteration's output; out: of its input
  * parts selects the passes in the linear map (ATJUP_LIN_ALL: the whole iteration; a pass left out
  * is the identity), for checking them one at a time. Dry dynamics in FP64 only, as
- * atjup_gpu_rk4_tlm. (The reference has no derivative code.) */
+ * atjup_gpu_rk4_tlm; an iteration at which the projection around the obstacle runs
+ * (cone_proj_stride) is refused with ATJUP_ERR_UNSUPPORTED. (The reference has no derivative
+ * code.) */
 enum { ATJUP_LIN_PRESSURE = 1, ATJUP_LIN_MIXTURE = 2, ATJUP_LIN_RK4 = 4, ATJUP_LIN_BC = 8,
        ATJUP_LIN_SHAPIRO = 16, ATJUP_LIN_BALANCE = 32, ATJUP_LIN_ALL = 63 };
 int atjup_gpu_iteration_tlm(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_t parts,
@@ -543,7 +562,7 @@ int atjup_gpu_copy_field(AtjupCtx* ctx, int32_t field_id, double* buf, int32_t t
 enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, ATJUP_TK_SHAPIRO,
        ATJUP_TK_BALANCE_V, ATJUP_TK_MIXTURE, ATJUP_TK_SOLVER, ATJUP_TK_SATADJ, ATJUP_TK_SPECIES,
        ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_RK_GROUP,
-       ATJUP_TK_COUNT };
+       ATJUP_TK_CONE, ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */

@@ -11,6 +11,11 @@ moist convective adjustment every iteration, as baseline_state.PHYS_ENV sets) --
 wall clock on the host. Prints one JSON line.
 
     python oracle/ref_bench.py --steps K --warmup W [--threads T] [--phys]
+    python oracle/ref_bench.py --cone N [--threads T]
+
+With --cone N: no iterations; N in-loop projections around the obstacle
+(projectAroundObstacle(true), InitValues_Jup.cpp:1595-1822) on the dry configuration's state, the
+first from zero and the rest warm-started, each timed by wall clock.
 """
 from __future__ import annotations
 
@@ -33,6 +38,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--phys", action="store_true")
+    ap.add_argument("--cone", type=int, default=0)
     a = ap.parse_args()
     if not LIB.exists():
         print(json.dumps({"unavailable": f"{LIB} not built"}))
@@ -50,6 +56,18 @@ def main():
         return
     t_init = time.perf_counter() - t0
     L = ref.L
+    if a.cone:
+        times = []
+        L.ref_quiet(1)
+        for _ in range(a.cone):
+            t0 = time.perf_counter()
+            L.ref_cone_proj(0)
+            times.append(time.perf_counter() - t0)
+        L.ref_quiet(0)
+        print(json.dumps({"cone_s_per_call": sum(times) / len(times), "call_times": times,
+                          "threads": threads, "state": BS.describe(config)}))
+        sys.stdout.flush()
+        os._exit(0)
     times = []
     rc = 0
     L.ref_quiet(1)

@@ -410,6 +410,13 @@ int ref_load_state(const char* dir, int iter) {
     return ok ? 0 : 1;
 }
 void ref_mixture_density() { g_m->computeMixtureDensity(); }
+// the in-loop projection of the flow around the obstacle (cJupiterModel.cpp:1362-1363)
+// one in-loop projection around the obstacle (InitValues_Jup.cpp:1595-1822); with verbose its
+// summary line (SOR iterations up to N, wall inflow, divergence) is printed and flushed
+void ref_cone_proj(int verbose) {
+    g_m->projectAroundObstacle(true, verbose != 0);
+    fflush(stdout);
+}
 void ref_satadj(const char* gas) { gas_adjust(*g_m, gas); }
 
 // The 14 per-gas constants cJupiterModel passes to SaturationAdjustmentJup::run

@@ -342,6 +342,29 @@ def phys_iters_case(ref, g, data, iters, save_restart=None):
             data[f"rs{it}_vel_star"] = ref.get1("vel_star").reshape(shape[1], shape[2])
 
 
+def cone_call(ref, data: dict, tag: int) -> None:
+    """One in-loop projection around the obstacle on the reference's current state: u, v, w
+    before, v, w after, and the largest SOR sweep count of its printed summary."""
+    import re
+    for n in ("u", "v", "w"):
+        data[f"cone{tag}_pre_{n}"] = ref.get(n)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile() as tf:
+        os.dup2(tf.fileno(), 1)
+        try:
+            ref.L.ref_cone_proj(1)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        tf.seek(0)
+        txt = tf.read().decode(errors="replace")
+    m = re.search(r"SOR iterations up to (\d+)", txt)
+    data[f"cone{tag}_itmax"] = np.array(int(m.group(1)) if m else -1)
+    for n in ("v", "w"):
+        data[f"cone{tag}_post_{n}"] = ref.get(n)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("out")
@@ -379,6 +402,10 @@ def main():
                     help="start from the benchmark configuration's seeded initial state "
                          "(oracle/baseline_state.py) with its knobs: dry with --iters, "
                          "phys (the reference's default physics) with --phys-iters")
+    ap.add_argument("--cone-at", default=None, metavar="IT,IT,...",
+                    help="with --baseline dry: after each listed iteration (0: before the first) "
+                         "record u, v, w, run one in-loop projection around the obstacle and "
+                         "record v, w and the largest SOR sweep count it printed")
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args()
     out_dir = tempfile.mkdtemp(prefix="atjup_ref_")
@@ -438,10 +465,15 @@ def main():
             data["fd_eps"] = np.array(eps)
             data["fd_iters"] = np.array(K)
         else:
+            cone_at = {int(x) for x in a.cone_at.split(",")} if a.cone_at else set()
+            if 0 in cone_at:
+                cone_call(ref, data, 0)
             for it in range(1, a.iters + 1):
                 rc = ref.quiet(ref.L.ref_iteration, it, 1 if it == 1 else 0, 1)
                 if rc != 0:
                     raise SystemExit(f"ref_iteration rc={rc}")
+                if it in cone_at:
+                    cone_call(ref, data, it)
             for n in DYN_FIELDS:
                 data["out_" + n] = ref.get(n)
         np.savez(a.out, **data)

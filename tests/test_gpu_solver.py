@@ -88,7 +88,9 @@ def test_residual_solve_in_loop_source():
 def test_sor_arm_small(omega):
     """Point red-black SOR (ATJUP_SOLVE_SOR) on the same operator: the relative residual it reports
     is the oracle's residual of the p it returns, and more sweeps lower it (the slow column modes
-    of this operator keep it far from 1e-10 within any practical number of sweeps)."""
+    of this operator keep it far from 1e-10 within any practical number of sweeps; with omega 1.7
+    the relative residual stays above 1 for the first hundreds of sweeps, while the
+    high-frequency error, a small part of ||b||, is removed and the smooth modes barely move)."""
     from atjup_b200.params import SOLVE_SOR
     shape = (13, 37, 49)
     p, g, f = synthetic_case(*shape)
@@ -104,4 +106,4 @@ def test_sor_arm_small(omega):
         e = _rel_residual(o, m.download("p_dyn"), b)
         assert abs(e - st.rel_residual) <= 1e-6 * e + 1e-12, (e, st.rel_residual)
         rels.append(e)
-    assert rels[1] < rels[0] < 1.0, rels
+    assert rels[1] < rels[0], rels
