@@ -49,8 +49,9 @@ class IterationStep(torch.autograd.Function):
     mixture density on even iterations and the first, RK4, the boundary passes, the in-loop
     Shapiro filter and the column balance of v) on the nine fields one iteration hands the next
     (atjup_b200.params.LIN_FIELDS: t, u, v, w, p_dyn, aux_u, aux_v, aux_w, rho_mix). Its backward is
-    atjup_gpu_iteration_adjoint about the iteration's input, which the step keeps as its
-    checkpoint; the adjoint recomputes the pressure pass and the RK stages from it."""
+    atjup_gpu_iteration_adjoint_ckpt about the iteration's input: the step keeps its input and
+    its RK stage inputs (X1, X2, X3 of t, u, v, w, written there by the forward step itself) as
+    its checkpoint, and the adjoint recomputes only the pressure pass from it."""
 
     @staticmethod
     def forward(ctx, model, iter_n, first, chained, *x):
@@ -59,21 +60,27 @@ class IterationStep(torch.autograd.Function):
         if not chained:
             # chained: x are the outputs of the step just run, which the context still holds
             model.set_state_tensors(y, names=LIN_FIELDS, wait=False)
-        model.step(iter_n, first)
+        stages = [torch.empty_like(y[0]) for _ in range(12)]
+        model.set_stage_buffers(stages)
+        try:
+            model.step(iter_n, first)
+        finally:
+            model.set_stage_buffers(None)
         out = model.state_tensors(LIN_FIELDS)
         ctx.model, ctx.iter_n, ctx.first = model, iter_n, first
-        ctx.save_for_backward(*y)
+        ctx.save_for_backward(*y, *stages)
         return tuple(out)
 
     @staticmethod
     def backward(ctx, *grads):
         from .params import LIN_FIELDS
-        y = ctx.saved_tensors
+        saved = ctx.saved_tensors
+        y, stages = saved[:len(LIN_FIELDS)], saved[len(LIN_FIELDS):]
         model = ctx.model
         model.set_state_tensors(y, names=LIN_FIELDS, wait=False)   # the linearisation point
         g = [torch.zeros_like(r) if gr is None else gr.detach().clone().contiguous()
              for gr, r in zip(grads, y)]
-        model.iteration_adjoint(g, ctx.iter_n, ctx.first)
+        model.iteration_adjoint_ckpt(g, stages, ctx.iter_n, ctx.first)
         return (None, None, None, None, *g)
 
 

@@ -25,9 +25,10 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-re
 # The microphysics decide branches on exact cancellations (a rain flux that evaporates completely
 # is 0, not +-1 ulp; a saturation test sits on its threshold): these files keep the reference's
 # rounding by being compiled without FMA contraction, as the reference is. So does the projection
-# around the obstacle, whose SOR stopping test decides the sweep count on the last bits of phi.
+# around the obstacle, whose SOR stopping test decides the sweep count on the last bits of phi, and
+# the filters and the column balance, which then equal the reference's to the bit.
 PER_FILE = {"satadj.cu": ["-fmad=false"], "micro.cu": ["-fmad=false"], "mca.cu": ["-fmad=false"],
-            "cone.cu": ["-fmad=false"]}
+            "cone.cu": ["-fmad=false"], "filters.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

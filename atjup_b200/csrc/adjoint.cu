@@ -668,8 +668,9 @@ int lin_setup(AtjupCtx* c, Lin& L) {
     return ATJUP_OK;
 }
 
-// the forward stages 0-2 into L.S, with p_hydro and the level means of this state
-int lin_forward(AtjupCtx* c, Lin& L) {
+// the forward stages 0-2 into L.S (unless `stages` holds them), with p_hydro and the level means
+// of this state
+int lin_forward(AtjupCtx* c, Lin& L, const double* const* stages = nullptr) {
     const AtjupParams& P = c->P;
     double* Y[4] = {c->f[ATJUP_F_T], c->f[ATJUP_F_U], c->f[ATJUP_F_V], c->f[ATJUP_F_W]};
     ATJUP_CUDA(cudaMemcpyAsync(L.ph_save, c->f[ATJUP_F_P_HYDRO], sizeof(double) * c->NP,
@@ -679,6 +680,11 @@ int lin_forward(AtjupCtx* c, Lin& L) {
     int rc;
     if ((rc = launch_buoy_ref(c, Y[0]))) return rc;
     if ((rc = launch_hydrostatic(c, Y[2], Y[3]))) return rc;
+    if (stages) {
+        for (int s = 0; s < 3; s++)
+            for (int f = 0; f < 4; f++) L.S[s][f] = const_cast<double*>(stages[4 * s + f]);
+        return ATJUP_OK;
+    }
     for (int s = 0; s < 3; s++) {
         const void* in[4];
         void* out[4];
@@ -794,11 +800,11 @@ int rk4_tlm_ext(AtjupCtx* c, double* const d[4], const double* dp, const double*
 }
 
 int rk4_adjoint_ext(AtjupCtx* c, double* const a[4], double* lp, double* lrho,
-                    double* const laux[3]) {
+                    double* const laux[3], const double* const* stages) {
     Lin L;
     int rc;
     if ((rc = lin_setup(c, L))) return rc;
-    if ((rc = lin_forward(c, L))) return rc;
+    if ((rc = lin_forward(c, L, stages))) return rc;
     const AtjupParams& P = c->P;
     const LinConst q = lin_const(c);
     const size_t bytes = sizeof(double) * c->NP;

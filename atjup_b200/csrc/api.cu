@@ -123,7 +123,7 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
     cudaFree(c->mca_pairs);
-    cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
+    cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters); cudaFree(c->kerr);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
     cudaFree(c->sin_the); cudaFree(c->rad); cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
@@ -233,6 +233,7 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     A(&c->dvc, (size_t)P.jm * c->KP);
     A(&c->dvrow, (size_t)P.jm);
     A(reinterpret_cast<double**>(&c->counters), 8);
+    A(reinterpret_cast<double**>(&c->kerr), 1);
     if (rc == ATJUP_OK) {
         e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamCreate");
@@ -479,6 +480,23 @@ static int need_grid(AtjupCtx* c, const char* what) {
     return ATJUP_OK;
 }
 
+int atjup_gpu_set_stage_buffers(AtjupCtx* c, double* const bufs[12]) {
+    if (!c) return ATJUP_ERR_ARG;
+    if (!bufs) {
+        c->keep_on = false;
+        return ATJUP_OK;
+    }
+    for (int b = 0; b < 12; b++)
+        if (!bufs[b]) { set_error("set_stage_buffers: null buffer"); return ATJUP_ERR_ARG; }
+    if (c->phys_on || c->step_prec != ATJUP_PREC_FP64) {
+        set_error("set_stage_buffers: the FP64 dry step only");
+        return ATJUP_ERR_UNSUPPORTED;
+    }
+    for (int b = 0; b < 12; b++) c->keep[b] = bufs[b];
+    c->keep_on = true;
+    return ATJUP_OK;
+}
+
 int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
     (void)iter_n;
     int rc = need_grid(c, "rk4_step");
@@ -497,6 +515,16 @@ int atjup_gpu_rk4_step(AtjupCtx* c, int32_t iter_n) {
     void* out2[4] = {c->X2[0], c->X2[1], c->X2[2], c->X2[3]};
     const void* const* ins[4] = {in0, in1, in2, in1};
     void* const* outs[4] = {out1, out2, out1, nullptr};
+    // the caller's stage buffers (atjup_gpu_set_stage_buffers): X1, X2, X3 each kept
+    const void* kin[3][4];
+    void* kout[3][4];
+    if (c->keep_on && !c->phys_on && c->step_prec == ATJUP_PREC_FP64) {
+        for (int s = 0; s < 3; s++)
+            for (int f = 0; f < 4; f++) kin[s][f] = kout[s][f] = c->keep[4 * s + f];
+        for (int f = 0; f < 4; f++) in1[f] = kin[0][f];
+        ins[1] = kin[0]; ins[2] = kin[1]; ins[3] = kin[2];
+        outs[0] = kout[0]; outs[1] = kout[1]; outs[2] = kout[2];
+    }
     // The species and closure kernels of stage s read the stage input ins[s] and write only scalar
     // buffers; the dynamics kernel of stage s reads ins[s] too and writes outs[s], which is the
     // input the scalars of stage s - 1 read (X1 for stage 2, the FP64 state for stage 3). So the
@@ -986,6 +1014,13 @@ int atjup_gpu_timing_read(AtjupCtx* c, int32_t cls, double* total_ms, int64_t* c
     }
     if (total_ms) *total_ms = tot;
     if (count) *count = n;
+    return ATJUP_OK;
+}
+
+int atjup_gpu_kernel_errors(AtjupCtx* c, uint32_t* errors) {
+    if (!c || !errors) return ATJUP_ERR_ARG;
+    ATJUP_CUDA(cudaMemcpyAsync(errors, c->kerr, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     return ATJUP_OK;
 }
 

@@ -13,24 +13,39 @@
 // face corrections of each direction (a wall face's correction is minus the cell's velocity).
 // Finally the seam column k = km-1 takes v and w of k = 0.
 //
-// B200 form. One thread block per level; the level's phi, the cell flags and the per-cell
-// constants sit in shared memory (about 170 KB for the 105 x 117 box of the 41 x 181 x 361 grid).
-// Lexicographic SOR is replayed exactly as a pipelined wavefront: cell (a, b) of the box lies on
-// the anti-diagonal d = a + b, its sweep-t update needs sweep t of (a-1, b) and (a, b-1) and sweep
-// t-1 of (a+1, b) and (a, b+1), so step tau of the wavefront updates diagonal d = tau - 2(t-1)
-// for every sweep t in flight at once -- about D/2 diagonals of D = NJ + NK - 2 per step instead
-// of one. Each sweep meets one diagonal per step, so the warp that owns that diagonal reduces the
-// sweep's largest change and largest |phi| without atomics, and sweep t is complete after step
-// D + 2(t-1), where its stopping test is taken. The sweeps after the converged one have by then
-// already updated the first diagonals; the block restores the newest snapshot of phi that
-// precedes them (one every SNAP_EVERY steps, in HBM) and replays up to the converged sweep. The
-// arithmetic is the reference's, operation for operation (this file is compiled without FMA
-// contraction), so the result is the reference's to the bit.
+// B200 form. Lexicographic SOR is replayed exactly as a pipelined wavefront: cell (a, b) of the
+// box lies on the anti-diagonal d = a + b, its sweep-t update needs sweep t of (a-1, b) and
+// (a, b-1) and sweep t-1 of (a+1, b) and (a, b+1), so step tau of the wavefront can update
+// diagonal d = tau - 2(t-1) for every sweep t in flight at once. The cells of one step are then
+// exactly the cells of one colour of the checkerboard, (a + b) = tau mod 2, less those whose sweep
+// has not begun or is past the last; a step reads only the other colour, so the cells of a step
+// are independent and one barrier between steps orders them. phi is stored split by colour (each
+// row's cells of one colour contiguous), so a warp's lanes take consecutive cells of one row and
+// read the four neighbours from consecutive words of the other colour.
+//
+// Each level is one thread-block cluster of C blocks (C = 4, or fewer when the GPU cannot hold
+// every level's cluster at once: 26 levels on 104 SMs for the 41 x 181 x 361 grid). Block r owns
+// a band of the box's rows with its phi, cell flags and per-cell constants in shared memory; the
+// rows next to its band are read from the neighbouring blocks' shared memory (distributed shared
+// memory), and a cluster barrier ends each step. Each sweep's largest change and largest |phi|
+// are kept per block in a ring slot (the band's first cell of the sweep opens it, the other cells
+// raise it by a shared-memory atomic maximum on the IEEE bit pattern, issued only when a cell
+// exceeds the value it reads); sweep t is complete after step D + 2(t-1) (D = NJ + NK - 2), where
+// every block reads the C slots and takes the stopping test. The sweeps after the converged one
+// have by then already updated the first diagonals; each block restores its band from the newest
+// snapshot that precedes them (one every SNAP_EVERY steps, in HBM) and the cluster replays up to
+// the converged sweep. The arithmetic is the reference's, operation for operation (this file is
+// compiled without FMA contraction), so the result is the reference's to the bit.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ctx.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace atjup {
 
@@ -41,21 +56,27 @@ constexpr int CONE_MAXIT = 40000;        // InitValues_Jup.cpp:1728
 constexpr double CONE_TOL = 1.0e-10;     // InitValues_Jup.cpp:1761
 constexpr int SNAP_EVERY = 64;           // wavefront steps between snapshots
 constexpr int CONE_THREADS = 1024;
+constexpr int CONE_CLUSTER = 4;          // blocks per level (fewer when the GPU cannot hold them)
 constexpr size_t CONE_SMEM_CAP = 200 * 1024;
+constexpr int NROW = 6;                  // per box row: aN, aS, aL, s, s dphi, A of a plain cell
 
 // cell flags of the box (uint32 per cell: these bits, the special-cell index above bit 6)
 enum : uint32_t { CF_SOLID = 1, CF_N = 2, CF_S = 4, CF_W = 8, CF_E = 16, CF_NEAR = 32 };
+constexpr uint32_t CF_WALL = CF_N | CF_S | CF_W | CF_E;
 
 }  // namespace
 
+// One level's box. Colour-split storage: cell (a', b') of the box with its halo (a' = a + 1 in
+// 0..NJ+1, b' = b + 1 in 0..NK+1) sits at ((c (NJ + 2) + a') PW + b' / 2), c = (a' + b') mod 2;
+// the flags of interior cell (a, b) at ((c NJ + a) PW + (b + 1) / 2).
 struct ConeLevel {
-    int i, jlo, klo, NJ, NK, PJ, D, n_spec;
-    int64_t info_off;   // uint32 [NJ * PJ]: flags | special index << 6
-    int64_t spec_off;   // int32 [n_spec]: box cell a * PJ + b of each special cell
-    int64_t phi_off;    // double [(NJ + 2) * PJ] per warm-start buffer (halo included)
-    int64_t snap_off;   // double [n_snap * (NJ + 2) * PJ]
+    int i, jlo, klo, NJ, NK, PW, D, n_spec;
+    int64_t info_off;   // uint32 [2 * NJ * PW]: flags | special index << 6
+    int64_t spec_off;   // int32 [n_spec]: (c NJ + a) PW + m of each special cell
+    int64_t phi_off;    // double [2 * (NJ + 2) * PW] per warm-start buffer (halo included)
+    int64_t snap_off;   // double [n_snap * C * 2 * (nbmax + 2) * PW]: per block, its band
     int64_t tab_off;    // double [2 * n_spec] (global-memory mode)
-    int64_t row_off;    // double [5 * NJ]: aN, aS, aL, s, s dphi (global-memory mode)
+    int64_t row_off;    // double [NROW * NJ] (global-memory mode)
     int n_snap, ring;
 };
 
@@ -71,9 +92,11 @@ struct ConeState {
     double* s = nullptr;                    // [jm] max(sinthe_min, |sin(the_j)|)
     int* stats = nullptr;                   // [2 * levels] sweeps of the last call
     int H = 0, M = 0;
-    size_t smem = 0;                        // dynamic shared memory per block (0: global mode)
-    bool allocated = false;
-    int64_t n_info = 0, n_spec = 0, n_phi = 0, n_snap = 0, n_tab = 0, n_row = 0;
+    int C = 1;                              // blocks (one cluster) per level
+    int ring_max = 1;                       // the largest ring of the levels
+    bool smem_mode = true;
+    size_t smem = 0;                        // dynamic shared memory per block
+    int64_t n_phi = 0;
 };
 
 namespace {
@@ -94,74 +117,129 @@ struct ConeArgs {
     double* w;
     const uint8_t* solid;
     const double* rad;
-    int jm, km, KP, H, smem_mode;
+    int jm, km, KP, H, smem_mode, C, ring_max;
     double dr, dthe, dphi;
 };
 
-// One SOR update of box cell (a, b) (InitValues_Jup.cpp:1739-1758), in the reference's order of
-// operations; returns false for a cell the sweep skips (solid, or no fluid face: A = 0).
-__device__ __forceinline__ bool cone_update(double* phi, const uint32_t* info, const double* tab,
-                                            const double* rows, int NJ, int PJ, int a, int b,
-                                            bool div, double dthe, double dphi, double& dch,
-                                            double& pabs) {
-    const uint32_t inf = info[a * PJ + b];
+// A block's band of a level's box as the kernel sees it. Local row la = 1..nb is box row
+// a = A0 + la - 1 (halo coordinate a' = A0 + la); the words of colour x, local row la start at
+// phi + x cs + la PW, la = 0 and nb + 1 being the rows beside the band (nrow, srow per colour:
+// the neighbouring block's rows in its shared memory, or the box's halo).
+struct Box {
+    double* phi;
+    int cs;                     // colour stride of phi
+    const double* nrow[2];
+    const double* srow[2];
+    const uint32_t* info;       // flags of local row la, colour x at info + x ics + (la - 1) PW
+    int ics;
+    const double* tab;
+    const double* rows;         // [NROW][NJ], indexed by box row
+    unsigned long long* ring;   // [2 R]: largest change, largest |phi| of sweep t at t mod R
+    int NJ, NK, PW, D, R;       // R a power of two
+    int lgCH;                   // the row's words of one colour in 2^lgCH chunks of 32
+    int nb, A0;
+    bool div;
+    double dthe, dphi;
+};
+
+__device__ __forceinline__ const double* row_of(const Box& B, int x, int la) {
+    if (la == 0) return B.nrow[x];
+    if (la == B.nb + 1) return B.srow[x];
+    return B.phi + x * B.cs + la * B.PW;
+}
+
+// phi of the cell at local row la (0..nb+1), halo column b' (0..NK+1)
+__device__ __forceinline__ double phi_at(const Box& B, int la, int bp) {
+    return row_of(B, (B.A0 + la + bp) & 1, la)[bp >> 1];
+}
+
+// One SOR update of the cell at local row la, colour c, word m (InitValues_Jup.cpp:1739-1758), in
+// the reference's order of operations. Returns false for a cell the sweep skips (solid, or no
+// fluid face: A = 0); else the change and |phi| in dch, pabs.
+__device__ __forceinline__ bool cone_update(const Box& B, int la, int c, int m, int off,
+                                            double& dch, double& pabs) {
+    const uint32_t inf = B.info[c * B.ics + (la - 1) * B.PW + m];
     if (inf & CF_SOLID) return false;
-    const int q = (a + 1) * PJ + (b + 1);
-    const double aN = rows[a], aS = rows[NJ + a], aL = rows[2 * NJ + a];
-    double A = 0.0, B = 0.0;
-    if (div && (inf & CF_NEAR)) {
-        if (!(inf & CF_N)) { A += aN; B += aN * phi[q - PJ]; }
-        if (!(inf & CF_S)) { A += aS; B += aS * phi[q + PJ]; }
-        if (!(inf & CF_W)) { A += aL; B += aL * phi[q - 1]; }
-        if (!(inf & CF_E)) { A += aL; B += aL * phi[q + 1]; }
-        B += tab[2 * (inf >> 6)];
+    const int a = B.A0 + la - 1;
+    const double* rc = B.phi + (c ^ 1) * B.cs + la * B.PW;   // this row, the other colour
+    const double pN = row_of(B, c ^ 1, la - 1)[m], pS = row_of(B, c ^ 1, la + 1)[m];
+    const double pW = rc[m - 1 + off], pE = rc[m + off];
+    const double aN = B.rows[a], aS = B.rows[B.NJ + a], aL = B.rows[2 * B.NJ + a];
+    double A, Bs = 0.0;
+    if (!(inf & (CF_WALL | CF_NEAR)) || (!B.div && !(inf & CF_WALL))) {
+        // a plain cell: all four faces fluid
+        A = B.rows[5 * B.NJ + a];
+        Bs += aN * pN;
+        Bs += aS * pS;
+        Bs += aL * pW;
+        Bs += aL * pE;
+    } else if (B.div && (inf & CF_NEAR)) {
+        A = 0.0;
+        if (!(inf & CF_N)) { A += aN; Bs += aN * pN; }
+        if (!(inf & CF_S)) { A += aS; Bs += aS * pS; }
+        if (!(inf & CF_W)) { A += aL; Bs += aL * pW; }
+        if (!(inf & CF_E)) { A += aL; Bs += aL * pE; }
+        Bs += B.tab[2 * (inf >> 6)];
     } else {
-        double vp = 0.0, wp = 0.0;
-        if (inf & (CF_N | CF_S | CF_W | CF_E)) { vp = tab[2 * (inf >> 6)]; wp = tab[2 * (inf >> 6) + 1]; }
-        const double sj = rows[3 * NJ + a];
-        if (inf & CF_N) B -= aN * dthe * (-vp); else { A += aN; B += aN * phi[q - PJ]; }
-        if (inf & CF_S) B -= aS * dthe * (vp);  else { A += aS; B += aS * phi[q + PJ]; }
-        if (inf & CF_W) B -= aL * sj * dphi * (-wp); else { A += aL; B += aL * phi[q - 1]; }
-        if (inf & CF_E) B -= aL * sj * dphi * (wp);  else { A += aL; B += aL * phi[q + 1]; }
+        A = 0.0;
+        const double vp = B.tab[2 * (inf >> 6)], wp = B.tab[2 * (inf >> 6) + 1];
+        const double sj = B.rows[3 * B.NJ + a];
+        if (inf & CF_N) Bs -= aN * B.dthe * (-vp); else { A += aN; Bs += aN * pN; }
+        if (inf & CF_S) Bs -= aS * B.dthe * (vp);  else { A += aS; Bs += aS * pS; }
+        if (inf & CF_W) Bs -= aL * sj * B.dphi * (-wp); else { A += aL; Bs += aL * pW; }
+        if (inf & CF_E) Bs -= aL * sj * B.dphi * (wp);  else { A += aL; Bs += aL * pE; }
     }
     if (!(A > 0.0)) return false;
-    const double p = phi[q];
-    const double pn = p + CONE_OMEGA * (B / A - p);
-    dch = fmax(dch, fabs(pn - p));
-    phi[q] = pn;
-    pabs = fmax(pabs, fabs(pn));
+    double* own = B.phi + c * B.cs + la * B.PW + m;
+    const double p = *own;
+    const double pn = p + CONE_OMEGA * (Bs / A - p);
+    dch = fabs(pn - p);
+    *own = pn;
+    pabs = fabs(pn);
     return true;
 }
 
-__device__ __forceinline__ double warp_max(double x) {
-    for (int o = 16; o; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-    return x;
+// std::max(cur, x) as the reference folds it (a NaN x leaves cur), on the ring's bit patterns
+__device__ __forceinline__ void ring_raise(unsigned long long* slot, double x) {
+    if (x > __longlong_as_double((long long)*(volatile unsigned long long*)slot))
+        atomicMax(slot, (unsigned long long)__double_as_longlong(x));
 }
 
-// One wavefront step tau: every sweep t in [t_lo, t_hi] updates its diagonal tau - 2(t-1). With
-// ring != nullptr each sweep's largest change and |phi| are folded into ring[t % R].
-__device__ void cone_step(double* phi, const uint32_t* info, const double* tab, const double* rows,
-                          int NJ, int NK, int PJ, int D, int tau, int t_stop, bool div,
-                          double dthe, double dphi, double* ring, int R) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    const int t_hi = min(t_stop, tau / 2 + 1);
-    const int t_lo = tau <= D ? 1 : (tau - D + 1) / 2 + 1;
-    for (int t = t_lo + warp; t <= t_hi; t += nwarps) {
-        const int d = tau - 2 * (t - 1);
-        const int a0 = max(0, d - (NK - 1)), a1 = min(d, NJ - 1);
-        double dch = 0.0, pabs = 0.0;
-        for (int a = a0 + lane; a <= a1; a += 32)
-            cone_update(phi, info, tab, rows, NJ, PJ, a, d - a, div, dthe, dphi, dch, pabs);
-        if (ring) {
-            dch = warp_max(dch);
-            pabs = warp_max(pabs);
-            if (lane == 0) {
-                double* r = ring + 2 * (t % R);
-                if (d == 0) { r[0] = dch; r[1] = pabs; }
-                else { r[0] = fmax(r[0], dch); r[1] = fmax(r[1], pabs); }
-            }
-        }
+// One cell of a wavefront step tau on the block's band: the cell of colour tau mod 2 at local row
+// la, word m, if its sweep t = (tau - a - b) / 2 + 1 lies in [1, t_stop].
+__device__ __forceinline__ void cone_cell(const Box& B, int tau, int t_stop, bool reduce, int la,
+                                          int m) {
+    const int c = tau & 1;
+    const int a = B.A0 + la - 1;
+    const int off = (c ^ (a + 1)) & 1;              // b' of word 0 of this colour in row a'
+    const int b = off + 2 * m - 1;
+    if (b < 0 || b >= B.NK) return;
+    const int diff = tau - a - b;
+    if (diff < 0) return;
+    const int t = (diff >> 1) + 1;
+    if (t > t_stop) return;
+    double dch = 0.0, pabs = 0.0;
+    const bool upd = cone_update(B, la, c, m, off, dch, pabs);
+    if (!reduce) return;
+    unsigned long long* slot = B.ring + 2 * (t & (B.R - 1));
+    if (la == 1 && b == 0) {
+        // the band's first cell of the sweep, alone in its sweep here at this step: opens the
+        // band's slot
+        slot[0] = (unsigned long long)__double_as_longlong(upd && dch > 0.0 ? dch : 0.0);
+        slot[1] = (unsigned long long)__double_as_longlong(upd && pabs > 0.0 ? pabs : 0.0);
+    } else if (upd) {
+        ring_raise(slot, dch);
+        ring_raise(slot + 1, pabs);
     }
+}
+
+// One wavefront step tau on the block's band. Warp w owns chunk w mod 2^lgCH of the local rows
+// 1 + w / 2^lgCH + n 32 / 2^lgCH: lane l updates word 32 chunk + l of each (no division).
+__device__ void cone_step(const Box& B, int tau, int t_stop, bool reduce) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m = ((warp & ((1 << B.lgCH) - 1)) << 5) + lane;
+    const int la_step = (blockDim.x >> 5) >> B.lgCH;
+    for (int la = 1 + (warp >> B.lgCH); la <= B.nb; la += la_step) cone_cell(B, tau, t_stop, reduce, la, m);
 }
 
 // s r D of a cell within H cells of the body: its 3-D face divergence with face values the
@@ -181,52 +259,66 @@ __device__ double cone_face_div(const ConeArgs& A, int i, int j, int k) {
            (wp - wm) / A.dphi;
 }
 
-__device__ void cone_copy(double* dst, const double* src, int n) {
-    for (int x = threadIdx.x; x < n; x += blockDim.x) dst[x] = src[x];
+// the band's rows 1..nb of both colours between phi (colour stride cs) and a packed copy
+// [2][nb][PW] (to_packed) or back
+__device__ void band_copy(double* phi, int cs, double* packed, int nb, int PW, bool to_packed) {
+    const int n = 2 * nb * PW;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+        const int col = x / (nb * PW), r = x - col * nb * PW;
+        double* p = phi + col * cs + PW + r;      // local row 1 + r / PW, word r mod PW
+        if (to_packed) packed[x] = *p;
+        else *p = packed[x];
+    }
 }
 
-// Lexicographic SOR of one level's solve as the pipelined wavefront; returns the reference's
-// sweep count `it` (the converged sweep, or CONE_MAXIT + 1 without convergence).
-__device__ int cone_sor(double* phi, const uint32_t* info, const double* tab, const double* rows,
-                        int NJ, int NK, int PJ, int D, bool div, double dthe, double dphi,
-                        double* ring, int R, double* snap, int n_snap, int* snap_tag) {
-    const int nphi = (NJ + 2) * PJ;
-    cone_copy(snap, phi, nphi);
+// Lexicographic SOR of one level's solve as the pipelined wavefront on the cluster; returns the
+// reference's sweep count `it` (the converged sweep, or CONE_MAXIT + 1 without convergence).
+// snap: this block's snapshot ring, n_snap slots of 2 nbmax PW doubles. A cluster barrier ends
+// every step: the next step's edge rows read the neighbours' rows of this one.
+__device__ int cone_sor(const Box& B, double* snap, int slot_sz, int n_snap, int* snap_tag, int C) {
+    cg::cluster_group cl = cg::this_cluster();
+    band_copy(B.phi, B.cs, snap, B.nb, B.PW, true);
     if (threadIdx.x == 0) {
         snap_tag[0] = -1;
         for (int s = 1; s < n_snap; s++) snap_tag[s] = INT_MIN;
     }
-    __syncthreads();
+    cl.sync();
     int next = 1 % n_snap, t_conv = 0, it = CONE_MAXIT + 1;
     for (int tau = 0;; tau++) {
-        cone_step(phi, info, tab, rows, NJ, NK, PJ, D, tau, CONE_MAXIT, div, dthe, dphi, ring, R);
-        __syncthreads();
-        if (tau >= D && ((tau - D) & 1) == 0) {
-            const int t = (tau - D) / 2 + 1;       // the sweep this step completed
-            const double* r = ring + 2 * (t % R);
-            if (r[0] <= CONE_TOL * fmax(r[1], 1.0e-30)) { t_conv = t; break; }
+        cone_step(B, tau, CONE_MAXIT, true);
+        cl.sync();
+        if (tau >= B.D && ((tau - B.D) & 1) == 0) {
+            const int t = (tau - B.D) / 2 + 1;       // the sweep this step completed
+            double dmax = 0.0, pmax = 0.0;
+            for (int r = 0; r < C; r++) {
+                const unsigned long long* sl = cl.map_shared_rank(B.ring + 2 * (t & (B.R - 1)), r);
+                dmax = fmax(dmax, __longlong_as_double((long long)sl[0]));
+                pmax = fmax(pmax, __longlong_as_double((long long)sl[1]));
+            }
+            if (dmax <= CONE_TOL * fmax(pmax, 1.0e-30)) { t_conv = t; break; }
             if (t == CONE_MAXIT) break;
         }
         if (tau % SNAP_EVERY == SNAP_EVERY - 1) {
-            cone_copy(snap + (size_t)next * nphi, phi, nphi);
+            band_copy(B.phi, B.cs, snap + (size_t)next * slot_sz, B.nb, B.PW, true);
             if (threadIdx.x == 0) snap_tag[next] = tau;
             next = (next + 1) % n_snap;
             __syncthreads();
         }
     }
     if (t_conv > 0) {
-        // back to the newest snapshot in which no cell is past sweep t_conv, then replay with
-        // the sweeps capped at t_conv up to the step that completes it
+        // back to the newest snapshot in which no cell is past sweep t_conv (the same slot in
+        // every block), then replay with the sweeps capped at t_conv up to the step that
+        // completes it
         it = t_conv;
-        const int target = 2 * (t_conv - 1), tau_c = D + 2 * (t_conv - 1);
+        const int target = 2 * (t_conv - 1), tau_c = B.D + 2 * (t_conv - 1);
         int best = 0, btag = INT_MIN;
         for (int s = 0; s < n_snap; s++)
             if (snap_tag[s] != INT_MIN && snap_tag[s] <= target && snap_tag[s] > btag) { best = s; btag = snap_tag[s]; }
-        cone_copy(phi, snap + (size_t)best * nphi, nphi);
-        __syncthreads();
+        band_copy(B.phi, B.cs, snap + (size_t)best * slot_sz, B.nb, B.PW, false);
+        cl.sync();
         for (int tau = btag + 1; tau <= tau_c; tau++) {
-            cone_step(phi, info, tab, rows, NJ, NK, PJ, D, tau, t_conv, div, dthe, dphi, nullptr, R);
-            __syncthreads();
+            cone_step(B, tau, t_conv, false);
+            cl.sync();
         }
     }
     return it;
@@ -235,81 +327,136 @@ __device__ int cone_sor(double* phi, const uint32_t* info, const double* tab, co
 __global__ void __launch_bounds__(CONE_THREADS, 1) cone_kernel(ConeArgs A) {
     extern __shared__ __align__(16) unsigned char cone_smem[];
     __shared__ int snap_tag[64];
-    const ConeLevel L = A.lv[blockIdx.x];
-    const int NJ = L.NJ, NK = L.NK, PJ = L.PJ, D = L.D, i = L.i;
-    const int nphi = (NJ + 2) * PJ;
-    double *phi, *tab, *rows, *ring;
-    const uint32_t* info;
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = A.C;
+    const int r = (int)cl.block_rank();
+    const int lvl = blockIdx.x / C;
+    const ConeLevel L = A.lv[lvl];
+    const int NJ = L.NJ, NK = L.NK, PW = L.PW, i = L.i;
+    const int A0 = (r * NJ) / C, nb = ((r + 1) * NJ) / C - A0, nbmax = (NJ + C - 1) / C;
+    Box B;
+    B.NJ = NJ; B.NK = NK; B.PW = PW; B.D = L.D; B.R = L.ring;
+    B.nb = nb; B.A0 = A0;
+    B.dthe = A.dthe; B.dphi = A.dphi;
+    B.lgCH = 0;
+    while ((32 << B.lgCH) < PW) B.lgCH++;
+    B.ring = reinterpret_cast<unsigned long long*>(cone_smem);
+    double* phi_local = reinterpret_cast<double*>(B.ring + 2 * A.ring_max);
+    double *rows, *tab;
     if (A.smem_mode) {
-        phi = reinterpret_cast<double*>(cone_smem);
-        tab = phi + nphi;
-        rows = tab + 2 * L.n_spec;
-        ring = rows + 5 * NJ;
-        uint32_t* inf = reinterpret_cast<uint32_t*>(ring + 2 * L.ring);
-        for (int x = threadIdx.x; x < NJ * PJ; x += blockDim.x) inf[x] = A.info[L.info_off + x];
-        info = inf;
+        B.cs = (nbmax + 2) * PW;
+        rows = phi_local + 2 * B.cs;
+        tab = rows + NROW * NJ;
+        uint32_t* inf = reinterpret_cast<uint32_t*>(tab + 2 * L.n_spec);
+        B.ics = nbmax * PW;
+        for (int x = threadIdx.x; x < 2 * nb * PW; x += blockDim.x) {
+            const int col = x / (nb * PW), rr = x - col * nb * PW;
+            inf[col * B.ics + rr] = A.info[L.info_off + (size_t)col * NJ * PW + (size_t)A0 * PW + rr];
+        }
+        B.info = inf;
+        for (int x = 0; x < 2; x++) {
+            B.nrow[x] = r > 0 ? cl.map_shared_rank(phi_local + x * B.cs + (A0 - ((r - 1) * NJ) / C) * PW, r - 1)
+                              : phi_local + x * B.cs;
+            B.srow[x] = r < C - 1 ? cl.map_shared_rank(phi_local + x * B.cs + PW, r + 1)
+                                  : phi_local + x * B.cs + (nb + 1) * PW;
+        }
     } else {
-        phi = nullptr;
-        tab = A.tab + L.tab_off;
+        // one block per level: phi in place in the warm-start buffer, the rest in HBM
+        B.cs = (NJ + 2) * PW;
         rows = A.rows + L.row_off;
-        ring = reinterpret_cast<double*>(cone_smem);
-        info = A.info + L.info_off;
+        tab = A.tab + L.tab_off;
+        B.ics = NJ * PW;
+        B.info = A.info + L.info_off;
     }
-    // the row coefficients (InitValues_Jup.cpp:1733-1735)
+    B.tab = tab;
+    B.rows = rows;
+    // the row coefficients (InitValues_Jup.cpp:1733-1735) and A of a cell with four fluid faces
     for (int a = threadIdx.x; a < NJ; a += blockDim.x) {
         const int j = L.jlo + a;
         const double sj = A.s[j];
-        rows[a] = 0.5 * (sj + A.s[j - 1]) / (A.dthe * A.dthe);
-        rows[NJ + a] = 0.5 * (sj + A.s[j + 1]) / (A.dthe * A.dthe);
-        rows[2 * NJ + a] = 1.0 / (sj * A.dphi * A.dphi);
+        const double aN = 0.5 * (sj + A.s[j - 1]) / (A.dthe * A.dthe);
+        const double aS = 0.5 * (sj + A.s[j + 1]) / (A.dthe * A.dthe);
+        const double aL = 1.0 / (sj * A.dphi * A.dphi);
+        double a4 = 0.0;
+        a4 += aN;
+        a4 += aS;
+        a4 += aL;
+        a4 += aL;
+        rows[a] = aN;
+        rows[NJ + a] = aS;
+        rows[2 * NJ + a] = aL;
         rows[3 * NJ + a] = sj;
         rows[4 * NJ + a] = sj * A.dphi;
+        rows[5 * NJ + a] = a4;
     }
     const int32_t* spec = A.spec + L.spec_off;
-    if (A.H == 0 && threadIdx.x == 0) A.stats[2 * blockIdx.x] = 0;
+    const int slot_sz = 2 * nbmax * PW;
+    double* snap = A.snap + L.snap_off + (size_t)r * L.n_snap * slot_sz;
+    if (A.H == 0 && r == 0 && threadIdx.x == 0) A.stats[2 * lvl] = 0;
     for (int pass = A.H > 0 ? 0 : 1; pass < 2; pass++) {
-        const bool div = pass == 0;
-        double* prev = (div ? A.prev0 : A.prev1) + L.phi_off;
-        if (A.smem_mode) cone_copy(phi, prev, nphi);
-        else phi = prev;
-        // the per-cell constants: the source of the divergence solve from the flow before it,
-        // the wall-face velocities of the wall-flux solve from the flow it starts from
-        __syncthreads();
-        for (int x = threadIdx.x; x < L.n_spec; x += blockDim.x) {
-            const int cb = spec[x], a = cb / PJ, b = cb - a * PJ;
-            const int j = L.jlo + a, k = L.klo + b;
-            if (div) {
-                tab[2 * x] = (info[cb] & CF_NEAR) ? cone_face_div(A, i, j, k) : 0.0;
-            } else {
-                const size_t c = ((size_t)i * A.jm + j) * A.KP + k;
-                tab[2 * x] = A.v[c];
-                tab[2 * x + 1] = A.w[c];
+        B.div = pass == 0;
+        double* prev = (B.div ? A.prev0 : A.prev1) + L.phi_off;
+        if (A.smem_mode) {
+            B.phi = phi_local;
+            for (int x = threadIdx.x; x < 2 * PW; x += blockDim.x) {   // the rows beside the band
+                const int col = x / PW, mm = x - col * PW;
+                phi_local[col * B.cs + mm] = 0.0;
+                phi_local[col * B.cs + (nb + 1) * PW + mm] = 0.0;
+            }
+            for (int x = threadIdx.x; x < 2 * nb * PW; x += blockDim.x) {
+                const int col = x / (nb * PW), rr = x - col * nb * PW;
+                phi_local[col * B.cs + PW + rr] = prev[(size_t)col * (NJ + 2) * PW + (size_t)(A0 + 1) * PW + rr];
+            }
+        } else {
+            B.phi = prev + (size_t)A0 * PW;
+            for (int x = 0; x < 2; x++) {
+                B.nrow[x] = B.phi + x * B.cs;
+                B.srow[x] = B.phi + x * B.cs + (nb + 1) * PW;
             }
         }
+        // the per-cell constants of the band: the source of the divergence solve from the flow
+        // before it, the wall-face velocities of the wall-flux solve from the flow it starts from
         __syncthreads();
-        const int it = cone_sor(phi, info, tab, rows, NJ, NK, PJ, D, div, A.dthe, A.dphi, ring,
-                                L.ring, A.snap + L.snap_off, L.n_snap, snap_tag);
-        // v and w incremented by the average of the two face corrections (InitValues_Jup.cpp:
-        // 1785-1793), a wall face's correction being minus the cell's velocity
-        for (int x = threadIdx.x; x < NJ * NK; x += blockDim.x) {
-            const int a = x / NK, b = x - a * NK;
-            const uint32_t inf = info[a * PJ + b];
-            if (inf & CF_SOLID) continue;
-            const size_t c = ((size_t)i * A.jm + (L.jlo + a)) * A.KP + (L.klo + b);
-            const int q = (a + 1) * PJ + (b + 1);
-            const double vp = A.v[c], wp = A.w[c], pp = phi[q];
-            const double sd = rows[4 * NJ + a];
-            const double dN = (inf & CF_N) ? -vp : (pp - phi[q - PJ]) / A.dthe;
-            const double dS = (inf & CF_S) ? -vp : (phi[q + PJ] - pp) / A.dthe;
-            const double dW = (inf & CF_W) ? -wp : (pp - phi[q - 1]) / sd;
-            const double dE = (inf & CF_E) ? -wp : (phi[q + 1] - pp) / sd;
-            A.v[c] = vp + 0.5 * (dN + dS);
-            A.w[c] = wp + 0.5 * (dW + dE);
+        for (int x = threadIdx.x; x < L.n_spec; x += blockDim.x) {
+            const int e = spec[x], mm = e % PW, rw = e / PW, a = rw % NJ, cc = rw / NJ;
+            if (a < A0 || a >= A0 + nb) continue;
+            const int b = ((cc ^ (a + 1)) & 1) + 2 * mm - 1;
+            const int j = L.jlo + a, k = L.klo + b;
+            if (B.div) {
+                tab[2 * x] = (A.info[L.info_off + e] & CF_NEAR) ? cone_face_div(A, i, j, k) : 0.0;
+            } else {
+                const size_t cix = ((size_t)i * A.jm + j) * A.KP + k;
+                tab[2 * x] = A.v[cix];
+                tab[2 * x + 1] = A.w[cix];
+            }
         }
-        // the warm start of the next call
-        if (A.smem_mode) cone_copy(prev, phi, nphi);
-        if (threadIdx.x == 0) A.stats[2 * blockIdx.x + pass] = it;
-        __syncthreads();
+        const int it = cone_sor(B, snap, slot_sz, L.n_snap, snap_tag, C);
+        // v and w of the band incremented by the average of the two face corrections
+        // (InitValues_Jup.cpp:1785-1793), a wall face's correction being minus the cell's velocity
+        for (int x = threadIdx.x; x < nb * NK; x += blockDim.x) {
+            const int la = 1 + x / NK, b = x - (la - 1) * NK;
+            const int a = A0 + la - 1, bp = b + 1;
+            const uint32_t inf = B.info[((a + b) & 1) * B.ics + (la - 1) * PW + (bp >> 1)];
+            if (inf & CF_SOLID) continue;
+            const size_t cix = ((size_t)i * A.jm + (L.jlo + a)) * A.KP + (L.klo + b);
+            const double vp = A.v[cix], wp = A.w[cix], pp = phi_at(B, la, bp);
+            const double sd = rows[4 * NJ + a];
+            const double dN = (inf & CF_N) ? -vp : (pp - phi_at(B, la - 1, bp)) / A.dthe;
+            const double dS = (inf & CF_S) ? -vp : (phi_at(B, la + 1, bp) - pp) / A.dthe;
+            const double dW = (inf & CF_W) ? -wp : (pp - phi_at(B, la, bp - 1)) / sd;
+            const double dE = (inf & CF_E) ? -wp : (phi_at(B, la, bp + 1) - pp) / sd;
+            A.v[cix] = vp + 0.5 * (dN + dS);
+            A.w[cix] = wp + 0.5 * (dW + dE);
+        }
+        // the band's phi is the warm start of the next call
+        if (A.smem_mode)
+            for (int x = threadIdx.x; x < 2 * nb * PW; x += blockDim.x) {
+                const int col = x / (nb * PW), rr = x - col * nb * PW;
+                prev[(size_t)col * (NJ + 2) * PW + (size_t)(A0 + 1) * PW + rr] = phi_local[col * B.cs + PW + rr];
+            }
+        if (r == 0 && threadIdx.x == 0) A.stats[2 * lvl + pass] = it;
+        // the neighbours have read this band's edge rows before the next pass overwrites them
+        cl.sync();
     }
 }
 
@@ -399,7 +546,6 @@ int cone_prepare(AtjupCtx* c) {
     std::vector<uint32_t> info;
     std::vector<int32_t> spec;
     int64_t n_phi = 0, n_snap = 0, n_tab = 0, n_row = 0;
-    size_t smem_max = 0, ring_bytes = 0;
     for (int i = 1; i < im - 1; i++) {
         int jmin = jm, jmax = -1, kmin = km, kmax = -1;
         for (int j = 0; j < jm; j++)
@@ -415,17 +561,23 @@ int cone_prepare(AtjupCtx* c) {
         ConeLevel L{};
         L.i = i; L.jlo = jlo; L.klo = klo;
         L.NJ = jhi - jlo + 1; L.NK = khi - klo + 1;
-        L.PJ = (L.NK + 2 + 1) & ~1;                  // even: the diagonal stride PJ-1 is odd
+        L.PW = (L.NK + 3) / 2;                       // words per row and colour, halo included
         L.D = L.NJ + L.NK - 2;
-        L.ring = L.D / 2 + 2;
+        L.ring = 1;
+        while (L.ring < L.D / 2 + 2) L.ring <<= 1;     // a power of two above the sweeps in flight
         L.n_snap = (L.D + SNAP_EVERY) / SNAP_EVERY + 2;
-        if (L.n_snap > 64) { delete cs; set_error("cone projection: box too large"); return ATJUP_ERR_UNSUPPORTED; }
+        if (L.n_snap > 64 || L.PW > 32 * 32) {
+            delete cs;
+            set_error("cone projection: box too large");
+            return ATJUP_ERR_UNSUPPORTED;
+        }
         L.info_off = (int64_t)info.size();
         L.spec_off = (int64_t)spec.size();
-        info.resize(info.size() + (size_t)L.NJ * L.PJ, CF_SOLID);
+        info.resize(info.size() + 2 * (size_t)L.NJ * L.PW, CF_SOLID);   // unused words: skipped
         for (int a = 0; a < L.NJ; a++)
             for (int b = 0; b < L.NK; b++) {
                 const int j = jlo + a, k = klo + b;
+                const int e = (((a + b) & 1) * L.NJ + a) * L.PW + ((b + 1) >> 1);
                 uint32_t f = 0;
                 if (S(i, j, k)) f = CF_SOLID;
                 else {
@@ -436,28 +588,71 @@ int cone_prepare(AtjupCtx* c) {
                     if (H > 0 && near[((size_t)i * jm + j) * km + k]) f |= CF_NEAR;
                     if (f) {
                         f |= (uint32_t)(spec.size() - L.spec_off) << 6;
-                        spec.push_back(a * L.PJ + b);
+                        spec.push_back(e);
                     }
                 }
-                info[L.info_off + (size_t)a * L.PJ + b] = f;
+                info[L.info_off + e] = f;
             }
         L.n_spec = (int)(spec.size() - L.spec_off);
-        const int64_t nphi = (int64_t)(L.NJ + 2) * L.PJ;
+        const int64_t nphi = 2 * (int64_t)(L.NJ + 2) * L.PW;
         L.phi_off = n_phi;  n_phi += nphi;
-        L.snap_off = n_snap; n_snap += (int64_t)L.n_snap * nphi;
         L.tab_off = n_tab;  n_tab += 2 * (int64_t)L.n_spec;
-        L.row_off = n_row;  n_row += 5 * (int64_t)L.NJ;
-        const size_t sm = sizeof(double) * ((size_t)nphi + 2 * (size_t)L.n_spec + 5 * (size_t)L.NJ +
-                                            2 * (size_t)L.ring) + sizeof(uint32_t) * (size_t)L.NJ * L.PJ;
-        smem_max = std::max(smem_max, sm);
-        ring_bytes = std::max(ring_bytes, sizeof(double) * 2 * (size_t)L.ring);
+        L.row_off = n_row;  n_row += NROW * (int64_t)L.NJ;
+        cs->ring_max = std::max(cs->ring_max, L.ring);
         cs->lv.push_back(L);
     }
     c->cone = cs;
-    const bool smem_mode = smem_max <= CONE_SMEM_CAP;
-    cs->smem = smem_mode ? smem_max : ring_bytes;
     cs->n_phi = n_phi;
     const size_t nl = cs->lv.size();
+    // blocks per level: a cluster of up to CONE_CLUSTER, each block a band of at least one row,
+    // the bands in shared memory; a level whose box does not fit runs as one block in HBM
+    int C = CONE_CLUSTER;
+    for (const ConeLevel& L : cs->lv) C = std::min(C, L.NJ);
+    auto smem_for = [&](int Cn) {
+        size_t mx = 0;
+        for (const ConeLevel& L : cs->lv) {
+            const size_t nbmax = (size_t)(L.NJ + Cn - 1) / Cn;
+            mx = std::max(mx, sizeof(double) * (2 * (nbmax + 2) * L.PW + NROW * (size_t)L.NJ +
+                                                2 * (size_t)L.n_spec) +
+                                  sizeof(uint32_t) * 2 * nbmax * L.PW);
+        }
+        return mx + sizeof(unsigned long long) * 2 * (size_t)cs->ring_max;
+    };
+    cs->smem_mode = nl > 0 && smem_for(std::max(C, 1)) <= CONE_SMEM_CAP;
+    if (!cs->smem_mode) C = 1;
+    C = std::max(C, 1);
+    // the largest cluster for which the GPU holds every level's cluster at once
+    for (; nl > 0 && C > 1; C--) {
+        const size_t sm = smem_for(C);
+        if (sm > CONE_SMEM_CAP) continue;
+        if (cudaFuncSetAttribute(cone_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)(nl * C));
+        cfg.blockDim = dim3(CONE_THREADS);
+        cfg.dynamicSmemBytes = sm;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n_active = 0;
+        if (cudaOccupancyMaxActiveClusters(&n_active, cone_kernel, &cfg) == cudaSuccess &&
+            n_active >= (int)nl)
+            break;
+        cudaGetLastError();
+    }
+    cs->smem = cs->smem_mode ? smem_for(C) : sizeof(unsigned long long) * 2 * (size_t)cs->ring_max;
+    if (nl > 0)
+        ATJUP_CUDA(cudaFuncSetAttribute(cone_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs->smem));
+    cs->C = C;
+    for (ConeLevel& L : cs->lv) {
+        const int64_t nbmax = (L.NJ + C - 1) / C;
+        L.snap_off = n_snap;
+        n_snap += (int64_t)C * L.n_snap * 2 * nbmax * L.PW;
+    }
     ATJUP_CUDA(cudaMalloc(&cs->s, sizeof(double) * jm));
     ATJUP_CUDA(cudaMemcpy(cs->s, s.data(), sizeof(double) * jm, cudaMemcpyHostToDevice));
     ATJUP_CUDA(cudaMalloc(&cs->stats, sizeof(int) * 2 * std::max<size_t>(nl, 1)));
@@ -475,11 +670,10 @@ int cone_prepare(AtjupCtx* c) {
         ATJUP_CUDA(cudaMemset(p, 0, sizeof(double) * n_phi));
     }
     ATJUP_CUDA(cudaMalloc(&cs->snap, sizeof(double) * n_snap));
-    if (!smem_mode) {
+    if (!cs->smem_mode) {
         ATJUP_CUDA(cudaMalloc(&cs->tab, sizeof(double) * std::max<int64_t>(n_tab, 1)));
         ATJUP_CUDA(cudaMalloc(&cs->rows, sizeof(double) * n_row));
     }
-    ATJUP_CUDA(cudaFuncSetAttribute(cone_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs->smem));
     return ATJUP_OK;
 }
 
@@ -496,10 +690,22 @@ int launch_cone_projection(AtjupCtx* c) {
         A.u = c->f[ATJUP_F_U]; A.v = c->f[ATJUP_F_V]; A.w = c->f[ATJUP_F_W];
         A.solid = c->solid; A.rad = c->rad;
         A.jm = P.jm; A.km = P.km; A.KP = c->KP; A.H = cs->H;
-        A.smem_mode = cs->tab == nullptr;
+        A.smem_mode = cs->smem_mode;
+        A.C = cs->C;
+        A.ring_max = cs->ring_max;
         A.dr = P.dr; A.dthe = P.dthe; A.dphi = P.dphi;
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs->C; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)(cs->lv.size() * cs->C));
+        cfg.blockDim = dim3(CONE_THREADS);
+        cfg.dynamicSmemBytes = cs->smem;
+        cfg.stream = c->stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
         c->launches++;
-        cone_kernel<<<(unsigned)cs->lv.size(), CONE_THREADS, cs->smem, c->stream>>>(A);
+        ATJUP_CUDA(cudaLaunchKernelEx(&cfg, cone_kernel, A));
         ATJUP_CHECK_LAUNCH("cone projection");
     }
     const int rows = P.im * P.jm;

@@ -92,6 +92,10 @@ struct AtjupCtx {
     // RK stage buffers and accumulators for t, u, v, w
     double* X1[4] = {};
     double* X2[4] = {};
+    // caller buffers for the stage inputs X1, X2, X3 of t, u, v, w (atjup_gpu_set_stage_buffers):
+    // the FP64 dry step writes its stages there, where an adjoint can take them as checkpoints
+    double* keep[12] = {};
+    bool keep_on = false;
     double* acc[4] = {};
     // scratch
     double* src = nullptr;       // Poisson source, one value per cell
@@ -110,6 +114,7 @@ struct AtjupCtx {
     double* dsum = nullptr;      // [ATJUP_MAX_SOLVE_PARTIALS * 4] dot-product partials
     double* hsum = nullptr;      // pinned host copy of the final dot products
     unsigned long long* counters = nullptr;  // [8] event counters of the last satadj call
+    unsigned* kerr = nullptr;    // error word of the kernels' bounded waits (bit 0: a staged copy)
     double* lin = nullptr;       // scratch of the RK4 tangent-linear / adjoint (adjoint.cu)
     double* itlin = nullptr;     // scratch of the iteration's tangent-linear / adjoint (iteration_lin.cu)
 
@@ -186,8 +191,10 @@ int launch_bc_ptrs(AtjupCtx* c, int which, double* t, double* u, double* v, doub
                    double* p_dyn, double* p_stat, bool phys);
 int rk4_tlm_ext(AtjupCtx* c, double* const d[4], const double* dp, const double* drho,
                 double* const daux[3]);
+// stages: the forward's stage inputs X1, X2, X3 of t, u, v, w (12 buffers, stage-major), or null
+// to recompute them
 int rk4_adjoint_ext(AtjupCtx* c, double* const a[4], double* lp, double* lrho,
-                    double* const laux[3]);
+                    double* const laux[3], const double* const* stages = nullptr);
 int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passes, int use_topo);
 int launch_balance_v(AtjupCtx* c);
 int cone_prepare(AtjupCtx* c);

@@ -878,9 +878,8 @@ int atjup_gpu_iteration_tlm(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t 
     return even ? save_base(c, S, true) : ATJUP_OK;
 }
 
-int atjup_gpu_iteration_adjoint(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
-                                double* const a[9]) {
-    if (!c || !args_ok(a)) { set_error("iteration_adjoint: null argument"); return ATJUP_ERR_ARG; }
+static int iteration_adjoint_impl(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
+                                  double* const a[9], const double* const* stages) {
     int rc = check_supported(c, "iteration_adjoint", iter_n);
     if (rc) return rc;
     const AtjupParams& P = c->P;
@@ -900,13 +899,27 @@ int atjup_gpu_iteration_adjoint(AtjupCtx* c, int32_t iter_n, int32_t first, int3
     if (parts & ATJUP_LIN_RK4) {
         double* a4[4] = {a[LT], a[LU], a[LV], a[LW]};
         double* laux[3] = {a[LAU], a[LAV], a[LAW]};
-        if ((rc = rk4_adjoint_ext(c, a4, a[LP], a[LR], laux))) return rc;
+        if ((rc = rk4_adjoint_ext(c, a4, a[LP], a[LR], laux, stages))) return rc;
     }
     if (even) {
         if ((parts & ATJUP_LIN_MIXTURE) && (rc = mixture_lin(c, a, 1))) return rc;
         if ((parts & ATJUP_LIN_PRESSURE) && (rc = pressure_T(c, S, a))) return rc;
     }
     return even ? save_base(c, S, true) : ATJUP_OK;
+}
+
+int atjup_gpu_iteration_adjoint(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
+                                double* const a[9]) {
+    if (!c || !args_ok(a)) { set_error("iteration_adjoint: null argument"); return ATJUP_ERR_ARG; }
+    return iteration_adjoint_impl(c, iter_n, first, parts, a, nullptr);
+}
+
+int atjup_gpu_iteration_adjoint_ckpt(AtjupCtx* c, int32_t iter_n, int32_t first, int32_t parts,
+                                     double* const a[9], const double* const stages[12]) {
+    if (!c || !args_ok(a) || !stages) { set_error("iteration_adjoint_ckpt: null argument"); return ATJUP_ERR_ARG; }
+    for (int b = 0; b < 12; b++)
+        if (!stages[b]) { set_error("iteration_adjoint_ckpt: null stage buffer"); return ATJUP_ERR_ARG; }
+    return iteration_adjoint_impl(c, iter_n, first, parts, a, stages);
 }
 
 }  // extern "C"

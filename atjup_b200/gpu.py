@@ -47,6 +47,9 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_rk4_adjoint.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_iteration_tlm.argtypes = [vp, i32, i32, i32, ctypes.POINTER(vp)]
     L.atjup_gpu_iteration_adjoint.argtypes = [vp, i32, i32, i32, ctypes.POINTER(vp)]
+    L.atjup_gpu_iteration_adjoint_ckpt.argtypes = [vp, i32, i32, i32, ctypes.POINTER(vp),
+                                                   ctypes.POINTER(vp)]
+    L.atjup_gpu_set_stage_buffers.argtypes = [vp, ctypes.POINTER(vp)]
     L.atjup_gpu_set_grid.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.atjup_gpu_upload.argtypes = [vp, i32, vp]
     L.atjup_gpu_download.argtypes = [vp, i32, vp]
@@ -69,6 +72,7 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_timing.argtypes = [vp, i32]
     L.atjup_gpu_timing_read.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int64)]
     L.atjup_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.atjup_gpu_kernel_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.atjup_gpu_satadj.argtypes = [vp, i32, ctypes.POINTER(_p.AtjupGasParams),
                                    ctypes.POINTER(_p.AtjupSatStats)]
     L.atjup_gpu_set_physics.argtypes = [vp, ctypes.POINTER(_p.AtjupPhysics), vp]
@@ -354,6 +358,26 @@ class GpuModel:
         self._on_tensors(lambda ctx, ptrs: self.L.atjup_gpu_iteration_adjoint(
             ctx, int(iter_n), int(first), int(parts), ptrs), tensors)
 
+    def iteration_adjoint_ckpt(self, tensors, stages, iter_n: int, first: bool = False,
+                               parts: int = _p.LIN_ALL):
+        """iteration_adjoint with the RK step's stage inputs kept by the forward iteration
+        (set_stage_buffers): twelve (im, jm, pitch) float64 CUDA tensors, X1, X2, X3 of
+        t, u, v, w (atjup_gpu_iteration_adjoint_ckpt)"""
+        sp = self._ptrs(stages)
+        self._on_tensors(lambda ctx, ptrs: self.L.atjup_gpu_iteration_adjoint_ckpt(
+            ctx, int(iter_n), int(first), int(parts), ptrs, sp), tensors)
+
+    def set_stage_buffers(self, stages):
+        """the following dry FP64 RK steps write their stage inputs X1, X2, X3 of t, u, v, w into
+        the twelve (im, jm, pitch) float64 CUDA tensors `stages`; None: the context's own buffers
+        (atjup_gpu_set_stage_buffers)"""
+        import torch
+        if stages is None:
+            _check(self.L.atjup_gpu_set_stage_buffers(self.ctx, None))
+            return
+        torch.cuda.current_stream().synchronize()   # the tensors' memory is free on torch's stream
+        _check(self.L.atjup_gpu_set_stage_buffers(self.ctx, self._ptrs(stages)))
+
     def stream_handle(self) -> int:
         """the cudaStream_t the context issues its work on, as an integer"""
         s = ctypes.c_void_p()
@@ -446,6 +470,12 @@ class GpuModel:
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
                       "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca",
                       "rk_group", "cone")
+
+    def kernel_errors(self) -> int:
+        """the error word of the kernels' bounded waits (0: none timed out)"""
+        e = ctypes.c_uint32()
+        _check(self.L.atjup_gpu_kernel_errors(self.ctx, ctypes.byref(e)))
+        return e.value
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

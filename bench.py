@@ -91,7 +91,8 @@ CONFIGS = {
                     "equilibrium, moist convective adjustment every iteration): the loop's "
                     "schedule, pressure and physics on even iterations (with the Forces and "
                     "Latent_Heat output diagnostics), RK4 of t, u, v, w, 11 species, k*, omega* "
-                    "every iteration",
+                    "every iteration, the projection around the obstacle every 10 iterations "
+                    "(the reference's default stride)",
         "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
         "l2": "no flush: inputs larger than L2 (each RK stage streams > 1.8 GB)",
         "parallelism": "replicas (the path does not shard)",
@@ -99,7 +100,8 @@ CONFIGS = {
     "dry": {
         "workload": "dry dynamics iteration on the 41x181x361 shell (dry knobs: obstacle on, no physics, 4th-order in-loop Shapiro): "
                     "pressure red-black pass on even iterations, RK4 (4 stages), BCs, 4th-order "
-                    "Shapiro on u,v,w, column balance of v",
+                    "Shapiro on u,v,w, column balance of v, the projection around the obstacle "
+                    "every 10 iterations (the reference's default stride)",
         "grid": "41x181x361", "cells": N_CELLS, "precision": "fp64",
         "l2": "no flush: inputs larger than L2 (each RK stage streams ~0.47 GB)",
         "parallelism": "replicas (the path does not shard)",
@@ -203,7 +205,7 @@ STAGE_TRAFFIC_PER_CELL = {
 
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
-    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
+    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "10",
     "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
 }
 # the reference's default full physics: closure, radiation, precipitation, NH4SH equilibrium and
@@ -286,7 +288,7 @@ STATE_RECIPE = {
 }
 
 
-def cpu_baseline(workload, steps=8, warmup=2):
+def cpu_baseline(workload, steps=10, warmup=2):
     """The reference's own CPU iteration (oracle/_ref) timed on this host's cores, from the same
     seeded initial state as the GPU arm."""
     cmd = [sys.executable, str(ROOT / "oracle" / "ref_bench.py"), "--steps", str(steps),
@@ -487,8 +489,8 @@ def poisson_section(m, stream):
 
 def cone_section(P, grid, fields, calls=3):
     """The in-loop projection around the obstacle (projectAroundObstacle(in_loop = true), every
-    ATJUP_CONE_PROJ_STRIDE = 10 iterations by the reference's default; both benchmark
-    configurations pin it off, so it is timed here on its own): `calls` calls on the dry
+    ATJUP_CONE_PROJ_STRIDE = 10 iterations by the reference's default, and so in both arms'
+    timed iterations), timed here on its own: `calls` calls on the dry
     configuration's state, the first from zero and the rest warm-started, each timed with CUDA
     events on the library's stream, beside the reference's own per-call time on this host."""
     import torch
@@ -534,7 +536,8 @@ def adjoint_section(P, grid, fields, K):
     loss is J = sum_theta sin(colatitude) (zonal-mean w at the top integrated level -
     u_ref)^2, u_ref = sum_{n=1..8} a_n sin(n theta), a_n seeded U(-50, 150) m/s. Reports the time
     of forward with checkpoints + backward over the time of K plain forward iterations, and the
-    device memory the chain holds."""
+    device memory the chain holds. The projection around the obstacle has no linearisation here:
+    these iterations run without it (cone_proj_stride 0)."""
     import numpy as np
     import torch
 
@@ -542,6 +545,8 @@ def adjoint_section(P, grid, fields, K):
     from atjup_b200.gpu import GpuModel
     from atjup_b200.params import LIN_FIELDS
 
+    P = type(P).from_buffer_copy(P)
+    P.cone_proj_stride = 0
     m = GpuModel(P, grid)
     m.upload_state(fields)
     im, jm, km = m.shape

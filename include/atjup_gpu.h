@@ -226,6 +226,12 @@ int atjup_gpu_download_async(AtjupCtx* ctx, int32_t field_id, double* host);
 /* cJupiterModel::RungeKuttaJup (RungeKutta_Jup_Turb.cpp:261-583): buoyancy level mean,
  * hydrostatic pressure, four fused RK stages (RHSJup per cell, RHS_Jup_Turb.cpp:31-1457). */
 int atjup_gpu_rk4_step(AtjupCtx* ctx, int32_t iter_n);
+/* Stage buffers of the FP64 dry RK step: with bufs (12 device buffers in the padded layout,
+ * stage-major X1 t, u, v, w, X2 .., X3 ..) every following RK step writes its stage inputs there
+ * instead of the context's own buffers, so that they outlive the step as the adjoint's checkpoint
+ * (atjup_gpu_iteration_adjoint_ckpt); NULL returns to the context's buffers. No counterpart in the
+ * reference. ATJUP_ERR_UNSUPPORTED with the physics block or the mixed step. */
+int atjup_gpu_set_stage_buffers(AtjupCtx* ctx, double* const bufs[12]);
 
 /* PressureSolverJup::run (PressureSolver.h:144-766) incl. prepareProjectionBoundaries
  * (cJupiterModel.cpp:1842-1864). SWEEPS reproduces the reference; RESIDUAL solves the same
@@ -546,6 +552,12 @@ int atjup_gpu_iteration_tlm(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_
                             double* const d[9]);
 int atjup_gpu_iteration_adjoint(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_t parts,
                                 double* const a[9]);
+/* The same with the RK step's stage inputs X1, X2, X3 of t, u, v, w (12 device buffers in the
+ * padded layout, stage-major: X1 t, u, v, w, X2 .., X3 ..) kept by the forward iteration
+ * (atjup_gpu_set_stage_buffers) instead of recomputed: a checkpoint of 12 fields per iteration
+ * that saves three RK stages per adjoint iteration. */
+int atjup_gpu_iteration_adjoint_ckpt(AtjupCtx* ctx, int32_t iter_n, int32_t first, int32_t parts,
+                                     double* const a[9], const double* const stages[12]);
 /* Device-to-device copy between a field and a caller's device buffer in the padded layout
  * (im * jm * pitch doubles), in the context's stream order: to_field 1 copies buf into the field,
  * 0 the field into buf. For callers that hold the state in their own device tensors (the torch
@@ -564,6 +576,10 @@ enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, A
        ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_RK_GROUP,
        ATJUP_TK_CONE, ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
+/* The error word of the kernels' bounded waits since the context was made (synchronises): 0, or
+ * bit 0 when an asynchronous copy of the staged species stage did not arrive in time (the block
+ * then stopped computing and the step's species are incomplete). */
+int atjup_gpu_kernel_errors(AtjupCtx* ctx, uint32_t* errors);
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */
 int atjup_gpu_launch_count(AtjupCtx* ctx, int64_t* launches);

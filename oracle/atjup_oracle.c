@@ -1013,6 +1013,159 @@ double ora_balance_column_v(const AtjupParams* P, const ora_grid* G, ora_state* 
     return vshift;
 }
 
+/* ------------------------------------------------------------------------------------------ */
+/* InitValues_Jup.cpp:1595-1822, projectAroundObstacle(in_loop = true): per level i = 1..im-2 that
+ * cuts the obstacle, the box M = cone_proj_margin cells wider than the body's cross-section
+ * (clipped to j 1..jm-2, k 1..km-2; phi = 0 one cell outside it), with H = cone_proj_div > 0 the
+ * divergence solve (cells within H cells of the body, Chebyshev in 3-D, take s r D of the flow
+ * before the correction as a source and close their wall faces), then the wall-flux solve; each
+ * by lexicographic SOR (omega 1.9, stop at a largest change <= 1e-10 of the largest |phi|, at
+ * most 40000 sweeps) from its phi of the previous call, then v, w incremented by the average of
+ * the two face corrections (a wall face's correction is minus the cell's velocity); last the
+ * seam copy of v and w. phi_div and phi_wall ([im*jm*km], zero before the first call) carry the
+ * warm starts; sweeps (may be NULL) receives [2 * levels] sweep counts, the return value is the
+ * number of levels.                                                                           */
+static int cone_near(const AtjupParams* P, const ora_grid* G, int H, int i, int j, int k) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    for (int di = -H; di <= H; di++) {
+        const int ii = i + di;
+        if (ii < 0 || ii >= im) continue;
+        for (int dj = -H; dj <= H; dj++) {
+            const int jj = j + dj;
+            if (jj < 0 || jj >= jm) continue;
+            for (int dk = -H; dk <= H; dk++) {
+                const int kk = k + dk;
+                if (kk < 0 || kk >= km) continue;
+                if (G->solid[IDX(ii, jj, kk)]) return 1;
+            }
+        }
+    }
+    return 0;
+}
+
+int ora_cone_project(const AtjupParams* P, const ora_grid* G, ora_state* S, double* phi_div,
+                     double* phi_wall, int32_t* sweeps) {
+    const int im = P->im, jm = P->jm, km = P->km;
+    const int H = P->cone_proj_div > 0 ? P->cone_proj_div : 0, M = P->cone_proj_margin;
+    const double dr = P->dr, dthe = P->dthe, dphi = P->dphi, omega = 1.9;
+    double* s = (double*)malloc(sizeof(double) * jm);
+    for (int j = 0; j < jm; j++) {
+        const double a = fabs(sin(G->the[j]));
+        s[j] = a > P->sinthe_min ? a : P->sinthe_min;
+    }
+#define SOL(a, b, c) (G->solid[IDX(a, b, c)] != 0)
+    int nlev = 0;
+    for (int i = 1; i < im - 1; i++) {
+        int jmin = jm, jmax = -1, kmin = km, kmax = -1;
+        for (int j = 0; j < jm; j++)
+            for (int k = 0; k < km; k++)
+                if (SOL(i, j, k)) {
+                    if (j < jmin) jmin = j;
+                    if (j > jmax) jmax = j;
+                    if (k < kmin) kmin = k;
+                    if (k > kmax) kmax = k;
+                }
+        if (jmax < 0) continue;
+        const int jlo = jmin - M > 1 ? jmin - M : 1, jhi = jmax + M < jm - 2 ? jmax + M : jm - 2;
+        const int klo = kmin - M > 1 ? kmin - M : 1, khi = kmax + M < km - 2 ? kmax + M : km - 2;
+        if (jhi < jlo || khi < klo) continue;
+        const int NJ = jhi - jlo + 1, NK = khi - klo + 1;
+        uint8_t* nr = (uint8_t*)calloc((size_t)NJ * NK, 1);
+        double* Gs = (double*)calloc((size_t)NJ * NK, sizeof(double));
+        if (H > 0)
+            for (int j = jlo; j <= jhi; j++)
+                for (int k = klo; k <= khi; k++) {
+                    if (SOL(i, j, k) || !cone_near(P, G, H, i, j, k)) continue;
+                    nr[(size_t)(j - jlo) * NK + (k - klo)] = 1;
+                    /* s r D, the 3-D face divergence with the wall faces closed (1653-1664) */
+                    const double r = G->rad[i], rp = r + 0.5 * dr, rm = r - 0.5 * dr;
+                    const double sj = s[j], sp = 0.5 * (sj + s[j + 1]), sm = 0.5 * (sj + s[j - 1]);
+                    const double up = SOL(i + 1, j, k) ? 0.0 : 0.5 * (S->u[IDX(i, j, k)] + S->u[IDX(i + 1, j, k)]);
+                    const double um = SOL(i - 1, j, k) ? 0.0 : 0.5 * (S->u[IDX(i, j, k)] + S->u[IDX(i - 1, j, k)]);
+                    const double vp = SOL(i, j + 1, k) ? 0.0 : 0.5 * (S->v[IDX(i, j, k)] + S->v[IDX(i, j + 1, k)]);
+                    const double vm = SOL(i, j - 1, k) ? 0.0 : 0.5 * (S->v[IDX(i, j, k)] + S->v[IDX(i, j - 1, k)]);
+                    const double wp = SOL(i, j, k + 1) ? 0.0 : 0.5 * (S->w[IDX(i, j, k)] + S->w[IDX(i, j, k + 1)]);
+                    const double wm = SOL(i, j, k - 1) ? 0.0 : 0.5 * (S->w[IDX(i, j, k)] + S->w[IDX(i, j, k - 1)]);
+                    Gs[(size_t)(j - jlo) * NK + (k - klo)] =
+                        sj * r * (rp * rp * up - rm * rm * um) / (r * r * dr) +
+                        (sp * vp - sm * vm) / dthe + (wp - wm) / dphi;
+                }
+        for (int pass = H > 0 ? 0 : 1; pass < 2; pass++) {
+            const int div = pass == 0;
+            double* phi = div ? phi_div : phi_wall;     /* the box's phi lives at its cells */
+            int it;
+            for (it = 1; it <= 40000; it++) {
+                double dmax = 0.0, pmax = 0.0;
+                for (int j = jlo; j <= jhi; j++) {
+                    const double aN = 0.5 * (s[j] + s[j - 1]) / (dthe * dthe);
+                    const double aS = 0.5 * (s[j] + s[j + 1]) / (dthe * dthe);
+                    const double aL = 1.0 / (s[j] * dphi * dphi);
+                    for (int k = klo; k <= khi; k++) {
+                        if (SOL(i, j, k)) continue;
+                        /* phi of a neighbour outside the box is the halo's 0 */
+                        const double pN = j - 1 >= jlo ? phi[IDX(i, j - 1, k)] : 0.0;
+                        const double pS = j + 1 <= jhi ? phi[IDX(i, j + 1, k)] : 0.0;
+                        const double pW = k - 1 >= klo ? phi[IDX(i, j, k - 1)] : 0.0;
+                        const double pE = k + 1 <= khi ? phi[IDX(i, j, k + 1)] : 0.0;
+                        const double vp = S->v[IDX(i, j, k)], wp = S->w[IDX(i, j, k)];
+                        double A = 0.0, B = 0.0;
+                        if (div && nr[(size_t)(j - jlo) * NK + (k - klo)]) {
+                            if (!SOL(i, j - 1, k)) { A += aN; B += aN * pN; }
+                            if (!SOL(i, j + 1, k)) { A += aS; B += aS * pS; }
+                            if (!SOL(i, j, k - 1)) { A += aL; B += aL * pW; }
+                            if (!SOL(i, j, k + 1)) { A += aL; B += aL * pE; }
+                            B += Gs[(size_t)(j - jlo) * NK + (k - klo)];
+                        } else {
+                            if (SOL(i, j - 1, k)) B -= aN * dthe * (-vp); else { A += aN; B += aN * pN; }
+                            if (SOL(i, j + 1, k)) B -= aS * dthe * (vp); else { A += aS; B += aS * pS; }
+                            if (SOL(i, j, k - 1)) B -= aL * s[j] * dphi * (-wp); else { A += aL; B += aL * pW; }
+                            if (SOL(i, j, k + 1)) B -= aL * s[j] * dphi * (wp); else { A += aL; B += aL * pE; }
+                        }
+                        if (!(A > 0.0)) continue;
+                        double* pp = &phi[IDX(i, j, k)];
+                        const double pn = *pp + omega * (B / A - *pp);
+                        const double d = fabs(pn - *pp);
+                        if (d > dmax) dmax = d;
+                        *pp = pn;
+                        if (fabs(pn) > pmax) pmax = fabs(pn);
+                    }
+                }
+                if (dmax <= 1.0e-10 * (pmax > 1.0e-30 ? pmax : 1.0e-30)) break;
+            }
+            if (sweeps) sweeps[2 * nlev + pass] = it;
+            for (int j = jlo; j <= jhi; j++)
+                for (int k = klo; k <= khi; k++) {
+                    if (SOL(i, j, k)) continue;
+                    const double vp = S->v[IDX(i, j, k)], wp = S->w[IDX(i, j, k)];
+                    const double pp = phi[IDX(i, j, k)];
+                    const double pN = j - 1 >= jlo ? phi[IDX(i, j - 1, k)] : 0.0;
+                    const double pS = j + 1 <= jhi ? phi[IDX(i, j + 1, k)] : 0.0;
+                    const double pW = k - 1 >= klo ? phi[IDX(i, j, k - 1)] : 0.0;
+                    const double pE = k + 1 <= khi ? phi[IDX(i, j, k + 1)] : 0.0;
+                    const double dN = SOL(i, j - 1, k) ? -vp : (pp - pN) / dthe;
+                    const double dS = SOL(i, j + 1, k) ? -vp : (pS - pp) / dthe;
+                    const double dW = SOL(i, j, k - 1) ? -wp : (pp - pW) / (s[j] * dphi);
+                    const double dE = SOL(i, j, k + 1) ? -wp : (pE - pp) / (s[j] * dphi);
+                    S->v[IDX(i, j, k)] = vp + 0.5 * (dN + dS);
+                    S->w[IDX(i, j, k)] = wp + 0.5 * (dW + dE);
+                }
+        }
+        if (sweeps && H == 0) sweeps[2 * nlev] = 0;
+        free(nr);
+        free(Gs);
+        nlev++;
+    }
+#undef SOL
+    /* the seam copy (1806-1807) */
+    for (int i = 0; i < im; i++)
+        for (int j = 0; j < jm; j++) {
+            S->v[IDX(i, j, km - 1)] = S->v[IDX(i, j, 0)];
+            S->w[IDX(i, j, km - 1)] = S->w[IDX(i, j, 0)];
+        }
+    free(s);
+    return nlev;
+}
+
 void ora_restore(const AtjupParams* P, ora_state* S) {
     const size_t N = (size_t)P->im * P->jm * P->km;
     memcpy(S->tn, S->t, sizeof(double) * N);

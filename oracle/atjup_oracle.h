@@ -106,6 +106,12 @@ void ora_shapiro(const AtjupParams* P, const ora_grid* G, double* f, int order, 
                  int passes, int use_topo);
 /* InitValues_Jup.cpp:1500-1538 */
 double ora_balance_column_v(const AtjupParams* P, const ora_grid* G, ora_state* S);
+/* InitValues_Jup.cpp:1595-1822 (projectAroundObstacle, in_loop = true): both solves per level
+ * with warm starts phi_div / phi_wall ([im*jm*km], zero before the first call), v and w
+ * incremented, the seam copied; sweeps ([2 * levels] or NULL) gets the SOR sweep counts
+ * (0 for a solve that is off). Returns the number of levels. */
+int ora_cone_project(const AtjupParams* P, const ora_grid* G, ora_state* S, double* phi_div,
+                     double* phi_wall, int32_t* sweeps);
 /* restoreVar (cJupiterModel.cpp:1757-1801) for the dynamics fields */
 void ora_restore(const AtjupParams* P, ora_state* S);
 /* SaturationAdjustment.h:255-746 for one gas (in place on t, c, cloud, ice); counts may be

@@ -43,11 +43,12 @@ from ref_model import RefModel  # noqa: E402
 DYN_SEED = 20261203
 PHYS_SEED = 20261207
 
-# The dry configuration: obstacle on, microphysics / radiation / turbulence / MCA / cone
-# projection off, in-loop 4th-order Shapiro on u, v, w.
+# The dry configuration: obstacle on, microphysics / radiation / turbulence / MCA off, in-loop
+# 4th-order Shapiro on u, v, w, the projection around the obstacle at the reference's default
+# stride (every 10 iterations).
 DRY_ENV = {
     "ATJUP_NO_SEAMOUNT": "0", "ATJUP_PRECIP": "0", "ATJUP_RADIATION": "0", "ATJUP_TURB": "0",
-    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "0",
+    "ATJUP_MCA": "0", "ATJUP_NH4SH_EQ": "0", "ATJUP_CONE_PROJ_STRIDE": "10",
     "ATJUP_VEL_SHAPIRO_ORDER": "4", "ATJUP_VEL_SHAPIRO_INLOOP": "1",
     "ATJUP_RESTART_STRIDE": "0", "ATJUP_VTK_STRIDE": "100000", "ATJUP_PANORAMA_STRIDE": "100000",
 }

@@ -121,6 +121,16 @@ class Oracle:
                              ctypes.c_int(order), ctypes.c_double(strength), ctypes.c_int(passes),
                              ctypes.c_int(use_topo))
 
+    def cone_project(self):
+        """One in-loop projection around the obstacle (ora_cone_project), warm-started from the
+        previous call on this object; returns the sweep counts [levels, 2]."""
+        if not hasattr(self, "_cone_phi"):
+            self._cone_phi = (np.zeros(self.shape), np.zeros(self.shape))
+        sw = np.zeros(2 * self.shape[0], dtype=np.int32)
+        n = self.call("ora_cone_project", _dp(self._cone_phi[0]), _dp(self._cone_phi[1]),
+                      sw.ctypes.data_as(_P(ctypes.c_int32)))
+        return sw[:2 * n].reshape(n, 2)
+
     def apply_A(self, p):
         out = np.zeros(self.shape)
         pp = np.ascontiguousarray(p, dtype=np.float64)

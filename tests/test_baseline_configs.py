@@ -5,6 +5,9 @@ on the reference side (oracle/baseline_state.py): the dry configuration's Gaussi
 t, u, v, w (none inside the obstacle), and for full physics also vapour at 90 % of saturation
 times U(0.95, 1.05), no condensate, seeded k* and omega*. The GPU starts from the same bytes.
 
+Both configurations run the reference's default in-loop projection around the obstacle (every
+10 iterations).
+
 * dry, 20 iterations: GPU FP64 vs the reference <= 1e-10 relative L2 per field (t, u, v, w,
   p_dyn, p_hydro, rho_mix), the bar for the FP64 GPU path.
 * full physics (the reference's default physics: k-omega SST, radiation, precipitation, the

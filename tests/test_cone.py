@@ -10,8 +10,11 @@ InitValues_Jup.cpp:1595-1822, every ATJUP_CONE_PROJ_STRIDE iterations at cJupite
   the second and third are warm-started from the phi of the one before: v and w equal the
   reference's bit for bit, u is untouched, and the largest sweep count equals the one the
   reference printed.
-* GPU, in the loop: the dry configuration with ATJUP_CONE_PROJ_STRIDE=10 over 20 iterations
-  (projections at 10 and 20), every field within the FP64 bar of 1e-10 relative L2.
+* GPU, in the loop: the dry configuration with ATJUP_CONE_PROJ_STRIDE=5 over 20 iterations
+  (projections at 5, 10, 15 and 20; the configuration's own stride, the reference's default 10,
+  is in tests/test_baseline_configs.py), every field within the FP64 bar of 1e-10 relative L2.
+* CPU, against the reference: the oracle's restatement (ora_cone_project) on the same three calls
+  as the GPU test, bit for bit.
 """
 import math
 import random
@@ -208,10 +211,10 @@ def test_gpu_cone_projection_bit_exact(ref_required):
 @pytest.mark.slow
 def test_gpu_dry_config_with_cone_projection(ref_required):
     import baseline_state as BS
-    env = {**BS.DRY_ENV, "ATJUP_CONE_PROJ_STRIDE": "10"}
-    d = ref_dump("--baseline", "dry", "--iters", "20", "--env", "ATJUP_CONE_PROJ_STRIDE=10")
+    env = {**BS.DRY_ENV, "ATJUP_CONE_PROJ_STRIDE": "5"}
+    d = ref_dump("--baseline", "dry", "--iters", "20", "--env", "ATJUP_CONE_PROJ_STRIDE=5")
     P = dump_params(d, env=env)
-    assert P.cone_proj_stride == 10 and P.cone_proj_div == 3 and P.cone_proj_margin == 40
+    assert P.cone_proj_stride == 5 and P.cone_proj_div == 3 and P.cone_proj_margin == 40
     m = gpu_from(P, dump_grid(d), dump_fields(d))
     try:
         for it in range(1, 21):
@@ -221,7 +224,26 @@ def test_gpu_dry_config_with_cone_projection(ref_required):
         assert m.nonfinite_count() == 0
     finally:
         m.close()
-    print("dry configuration with the projection every 10 iterations, 20 iterations vs reference:",
+    print("dry configuration with the projection every 5 iterations, 20 iterations vs reference:",
           {k: f"{v:.1e}" for k, v in worst.items()})
     for n in names:
         assert worst[n] <= 1e-10, f"{n}: relative L2 {worst[n]:.3e}"
+
+
+@pytest.mark.slow
+def test_oracle_cone_projection_bit_exact(ref_required):
+    """The oracle's restatement (ora_cone_project) against the reference: the same three calls as
+    the GPU test, the second and third warm-started, bit for bit, with the reference's sweeps."""
+    import baseline_state as BS
+    from helpers import oracle_from
+    calls = (0, 3, 8)
+    d = ref_dump("--baseline", "dry", "--iters", "8", "--cone-at", ",".join(map(str, calls)))
+    P = dump_params(d, env=BS.DRY_ENV)
+    o = oracle_from(P, dump_grid(d), dump_fields(d))
+    for tag in calls:
+        for n in ("u", "v", "w"):
+            o.f[n][...] = d[f"cone{tag}_pre_{n}"]
+        sweeps = o.cone_project()
+        assert int(sweeps.max()) == int(d[f"cone{tag}_itmax"])
+        for n in ("v", "w"):
+            assert np.array_equal(o.f[n], d[f"cone{tag}_post_{n}"]), f"call after {tag}: {n}"

@@ -61,6 +61,21 @@ def test_shapiro_small(small, order):
     _cmp(m, o, ["u", "w"], 1e-14)
 
 
+@pytest.mark.parametrize("order", [2, 4])
+def test_shapiro_fused_bit_exact(small, order):
+    """The fused three-pass kernel (k, j, i passes in one tile) equals the oracle's separate
+    passes (lib/Utils.cpp:227-453) to the bit: same rules, same order of operations, no FMA
+    contraction on either side."""
+    p, g, f = small
+    o = oracle_from(p, g, f)
+    m = gpu_from(p, g, f)
+    for n in ("u", "v", "w"):
+        o.shapiro(n, order, strength=1.0, passes=1)
+        m.shapiro(n, order, strength=1.0, passes=1)
+        assert np.array_equal(m.download(n), o.f[n]), f"{n}: order {order}"
+    m.close()
+
+
 def test_bc_small(small):
     p, g, f = small
     o = oracle_from(p, g, f)

@@ -111,6 +111,33 @@ def test_dot_product_per_pass(part, it):
     assert np.isfinite(lhs) and rel <= 1e-12
 
 
+@pytest.mark.parametrize("it", [2, 3], ids=["even", "odd"])
+def test_checkpointed_adjoint_equals_recomputed(it):
+    """The adjoint that takes the forward step's own RK stage inputs as its checkpoint
+    (atjup_gpu_set_stage_buffers, atjup_gpu_iteration_adjoint_ckpt) equals the one that
+    recomputes them from the iteration's input, to rounding (<= 1e-12 relative L2 per field: the
+    recompute repeats the pressure pass, whose reductions are not bit-reproducible run to run)."""
+    import torch
+    p, g, m = prepared((13, 37, 49), 83)
+    x0 = state(m)
+    xs = m.state_tensors(LIN_FIELDS)
+    stages = [torch.empty_like(xs[0]) for _ in range(12)]
+    m.set_stage_buffers(stages)
+    m.step(it, False)
+    m.set_stage_buffers(None)
+    m.set_state_tensors(xs, names=LIN_FIELDS)
+    lam = direction(m.shape, 5, {n: 1.0 / v for n, v in scales(x0).items()})
+    a_re = adjoint(m, lam, it, False)
+    x = padded(m, [lam[n] for n in LIN_FIELDS])
+    m.iteration_adjoint_ckpt(x, stages, it, False)
+    a_ck = dict(zip(LIN_FIELDS, unpadded(m, x)))
+    m.close()
+    worst = {n: _rel(a_ck[n], a_re[n]) for n in LIN_FIELDS}
+    print(f"iteration {it}: checkpointed vs recomputed adjoint", {k: f"{v:.1e}" for k, v in worst.items()})
+    for n in LIN_FIELDS:
+        assert worst[n] <= 1e-12, f"{n}: relative L2 {worst[n]:.3e}"
+
+
 def test_dot_product_whole_iteration_larger_shell():
     p, g, m = prepared((41, 61, 97), 82)
     sc = scales(state(m))
