@@ -123,7 +123,7 @@ void free_all(AtjupCtx* c) {
     cudaFree(c->buoy_ref); cudaFree(c->zm); cudaFree(c->dvc); cudaFree(c->dvrow);
     cudaFree(c->mca_bounds); cudaFree(c->mca_flags); cudaFree(c->mca_slots); cudaFree(c->mca_stats);
     cudaFree(c->mca_pairs);
-    cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters); cudaFree(c->kerr);
+    cudaFree(c->solve_b); cudaFree(c->dsum); cudaFree(c->counters);
     if (c->hsum) cudaFreeHost(c->hsum);
     cudaFree(c->solid); cudaFree(c->nbflags); cudaFree(c->topo); cudaFree(c->geo); cudaFree(c->cor_col);
     cudaFree(c->sin_the); cudaFree(c->rad); cudaFree(c->cell_vbar0); cudaFree(c->cell_ubar0);
@@ -233,7 +233,6 @@ int atjup_gpu_create(const AtjupParams* params, AtjupCtx** out) {
     A(&c->dvc, (size_t)P.jm * c->KP);
     A(&c->dvrow, (size_t)P.jm);
     A(reinterpret_cast<double**>(&c->counters), 8);
-    A(reinterpret_cast<double**>(&c->kerr), 1);
     if (rc == ATJUP_OK) {
         e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamCreate");
@@ -1014,13 +1013,6 @@ int atjup_gpu_timing_read(AtjupCtx* c, int32_t cls, double* total_ms, int64_t* c
     }
     if (total_ms) *total_ms = tot;
     if (count) *count = n;
-    return ATJUP_OK;
-}
-
-int atjup_gpu_kernel_errors(AtjupCtx* c, uint32_t* errors) {
-    if (!c || !errors) return ATJUP_ERR_ARG;
-    ATJUP_CUDA(cudaMemcpyAsync(errors, c->kerr, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-    ATJUP_CUDA(cudaStreamSynchronize(c->stream));
     return ATJUP_OK;
 }
 

@@ -114,7 +114,6 @@ struct AtjupCtx {
     double* dsum = nullptr;      // [ATJUP_MAX_SOLVE_PARTIALS * 4] dot-product partials
     double* hsum = nullptr;      // pinned host copy of the final dot products
     unsigned long long* counters = nullptr;  // [8] event counters of the last satadj call
-    unsigned* kerr = nullptr;    // error word of the kernels' bounded waits (bit 0: a staged copy)
     double* lin = nullptr;       // scratch of the RK4 tangent-linear / adjoint (adjoint.cu)
     double* itlin = nullptr;     // scratch of the iteration's tangent-linear / adjoint (iteration_lin.cu)
 

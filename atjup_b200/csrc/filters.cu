@@ -3,8 +3,9 @@
 // Reference: JupiterUtils::damp_wiggles (lib/Utils.cpp:227-323, order 2) and damp_wiggles_ho
 // (lib/Utils.cpp:334-453, order 4): direction-split passes k (periodic ring of km-1 meridians,
 // k = km-1 written as the copy of k = 0), then j (clamped at the poles), then i (clamped at the
-// fluid floor i_topography), each pass reading a full copy of the field. Here the three passes
-// are one kernel over tiles (shapiro3_kernel), written to tmp and copied back.
+// fluid floor i_topography), each pass reading a full copy of the field. Here each pass is an
+// out-of-place kernel that writes every cell (filtered, or copied where the reference skips),
+// chained field -> tmp -> tmp2 -> field.
 //
 // cJupiterModel::balanceColumnV (InitValues_Jup.cpp:1500-1538): trapezoid column mean of r v
 // over columns off the obstacle, then (zonal form) the row mean of those removed from every
@@ -25,121 +26,107 @@ __device__ __forceinline__ int floor_of(const int32_t* topo, int use_topo, int j
     return t > 0 ? t : 0;
 }
 
-// The three passes fused: one block owns an output tile of ST_I x ST_J x 32 cells and computes
-// the k pass over the tile widened by two cells in i and j (reading the field, its k neighbours
-// from L1), the j pass over the tile widened in i (from the k pass in shared memory), and the
-// i pass (from the j pass in shared memory), each with the reference's per-cell rules of that
-// pass and in its order of operations (this file is compiled without FMA contraction), so the
-// result is the three separate passes' to the bit. The field is read once from DRAM and the
-// result written once, to dst (the caller copies it back), where three separate passes move it
-// six times.
-constexpr int ST_I = 4, ST_J = 8, ST_K = 32;
-constexpr int SH_I = ST_I + 4, SH_J = ST_J + 4;
-
-__global__ void __launch_bounds__(256) shapiro3_kernel(const double* __restrict__ src,
-                                                       double* __restrict__ dst,
-                                                       const int32_t* __restrict__ topo,
-                                                       FiltConst q) {
-    __shared__ double K[SH_I][SH_J][ST_K];   // the k pass, tile widened by 2 in i and j
-    __shared__ double J[SH_I][ST_J][ST_K];   // the j pass, tile widened by 2 in i
-    const int k0 = blockIdx.x * ST_K, j0 = blockIdx.y * ST_J, i0 = blockIdx.z * ST_I;
+__global__ void shapiro_k_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                 const int32_t* __restrict__ topo, FiltConst q) {
+    const int k_out = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k_out >= q.km) return;
+    const size_t b = ((size_t)i * q.jm + j) * q.KP;
+    const int k = (k_out == q.km - 1) ? 0 : k_out;   // the seam copy takes k = 0's result
     const int n = q.km - 1;
+    const double cc = src[b + k];
+    double out = cc;
+    auto inf = [&](int kk) { return i >= floor_of(topo, q.use_topo, j, kk, q.km); };
+    if (inf(k)) {
+        if (q.order == 4) {
+            const int km1 = (k - 1 + n) % n, kp1 = (k + 1) % n;
+            const int km2 = (k - 2 + n) % n, kp2 = (k + 2) % n;
+            if (inf(km1) && inf(kp1)) {
+                if (inf(km2) && inf(kp2)) {
+                    const double d4 = src[b + kp2] - 4.0 * src[b + kp1] + 6.0 * cc -
+                                      4.0 * src[b + km1] + src[b + km2];
+                    out = cc - q.c4 * d4;
+                } else {
+                    out = cc + q.c2 * (src[b + km1] - 2.0 * cc + src[b + kp1]);
+                }
+            }
+        } else {
+            const int km1 = (k == 0) ? q.km - 2 : k - 1;
+            const int kp1 = (k == q.km - 2) ? 0 : k + 1;
+            const double vm = inf(km1) ? src[b + km1] : cc;
+            const double vp = inf(kp1) ? src[b + kp1] : cc;
+            out = cc + q.c2 * (vm - 2.0 * cc + vp);
+        }
+    }
+    dst[b + k_out] = out;
+}
+
+__global__ void shapiro_j_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                 const int32_t* __restrict__ topo, FiltConst q) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k >= q.km) return;
+    const size_t row = q.KP;
+    const size_t c = ((size_t)i * q.jm + j) * row + k;
+    const double cc = src[c];
+    double out = cc;
+    auto inf = [&](int jj) { return i >= floor_of(topo, q.use_topo, jj, k, q.km); };
+    if (inf(j)) {
+        if (q.order == 4) {
+            const bool fm1 = (j - 1 >= 0) && inf(j - 1);
+            const bool fp1 = (j + 1 <= q.jm - 1) && inf(j + 1);
+            if (fm1 && fp1) {
+                const bool fm2 = (j - 2 >= 0) && inf(j - 2);
+                const bool fp2 = (j + 2 <= q.jm - 1) && inf(j + 2);
+                if (fm2 && fp2) {
+                    const double d4 = src[c + 2 * row] - 4.0 * src[c + row] + 6.0 * cc -
+                                      4.0 * src[c - row] + src[c - 2 * row];
+                    out = cc - q.c4 * d4;
+                } else {
+                    out = cc + q.c2 * (src[c - row] - 2.0 * cc + src[c + row]);
+                }
+            }
+        } else {
+            const int jm1 = j - 1 > 0 ? j - 1 : 0, jp1 = j + 1 < q.jm - 1 ? j + 1 : q.jm - 1;
+            const size_t cm = c - (size_t)(j - jm1) * row, cp = c + (size_t)(jp1 - j) * row;
+            const double vm = inf(jm1) ? src[cm] : cc;
+            const double vp = inf(jp1) ? src[cp] : cc;
+            out = cc + q.c2 * (vm - 2.0 * cc + vp);
+        }
+    }
+    dst[c] = out;
+}
+
+__global__ void shapiro_i_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                 const int32_t* __restrict__ topo, FiltConst q) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, i = blockIdx.z;
+    if (k >= q.km) return;
     const size_t plane = (size_t)q.jm * q.KP;
-    // k pass: the ring of km-1 meridians, k = km-1 the copy of k = 0
-    for (int e = threadIdx.x; e < SH_I * SH_J * ST_K; e += blockDim.x) {
-        const int kc = e % ST_K, jj = (e / ST_K) % SH_J, ii = e / (ST_K * SH_J);
-        const int i = i0 - 2 + ii, j = j0 - 2 + jj, k_out = k0 + kc;
-        if (i < 0 || i >= q.im || j < 0 || j >= q.jm || k_out >= q.km) continue;
-        const size_t b = (size_t)i * plane + (size_t)j * q.KP;
-        const int k = (k_out == q.km - 1) ? 0 : k_out;
-        const double cc = src[b + k];
-        double out = cc;
-        auto inf = [&](int kk) { return i >= floor_of(topo, q.use_topo, j, kk, q.km); };
-        if (inf(k)) {
-            if (q.order == 4) {
-                const int km1 = (k - 1 + n) % n, kp1 = (k + 1) % n;
-                const int km2 = (k - 2 + n) % n, kp2 = (k + 2) % n;
-                if (inf(km1) && inf(kp1)) {
-                    if (inf(km2) && inf(kp2)) {
-                        const double d4 = src[b + kp2] - 4.0 * src[b + kp1] + 6.0 * cc -
-                                          4.0 * src[b + km1] + src[b + km2];
-                        out = cc - q.c4 * d4;
-                    } else {
-                        out = cc + q.c2 * (src[b + km1] - 2.0 * cc + src[b + kp1]);
-                    }
+    const size_t c = (size_t)i * plane + (size_t)j * q.KP + k;
+    const int is = floor_of(topo, q.use_topo, j, k, q.km);
+    const double cc = src[c];
+    double out = cc;
+    if (i >= is) {
+        if (q.order == 4) {
+            const bool fm1 = (i - 1 >= is), fp1 = (i + 1 <= q.im - 1);
+            if (fm1 && fp1) {
+                const bool fm2 = (i - 2 >= is), fp2 = (i + 2 <= q.im - 1);
+                if (fm2 && fp2) {
+                    const double d4 = src[c + 2 * plane] - 4.0 * src[c + plane] + 6.0 * cc -
+                                      4.0 * src[c - plane] + src[c - 2 * plane];
+                    out = cc - q.c4 * d4;
+                } else {
+                    out = cc + q.c2 * (src[c - plane] - 2.0 * cc + src[c + plane]);
                 }
-            } else {
-                const int km1 = (k == 0) ? q.km - 2 : k - 1;
-                const int kp1 = (k == q.km - 2) ? 0 : k + 1;
-                const double vm = inf(km1) ? src[b + km1] : cc;
-                const double vp = inf(kp1) ? src[b + kp1] : cc;
-                out = cc + q.c2 * (vm - 2.0 * cc + vp);
             }
+        } else {
+            const int im1 = i - 1 > is ? i - 1 : is, ip1 = i + 1 < q.im - 1 ? i + 1 : q.im - 1;
+            out = cc + q.c2 * (src[c - (size_t)(i - im1) * plane] - 2.0 * cc +
+                               src[c + (size_t)(ip1 - i) * plane]);
         }
-        K[ii][jj][kc] = out;
     }
-    __syncthreads();
-    // j pass on the k pass: clamped at the poles
-    for (int e = threadIdx.x; e < SH_I * ST_J * ST_K; e += blockDim.x) {
-        const int kc = e % ST_K, jj = (e / ST_K) % ST_J, ii = e / (ST_K * ST_J);
-        const int i = i0 - 2 + ii, j = j0 + jj, k = k0 + kc;
-        if (i < 0 || i >= q.im || j >= q.jm || k >= q.km) continue;
-        auto S = [&](int dj) { return K[ii][jj + 2 + dj][kc]; };
-        const double cc = S(0);
-        double out = cc;
-        auto inf = [&](int jx) { return i >= floor_of(topo, q.use_topo, jx, k, q.km); };
-        if (inf(j)) {
-            if (q.order == 4) {
-                const bool fm1 = (j - 1 >= 0) && inf(j - 1);
-                const bool fp1 = (j + 1 <= q.jm - 1) && inf(j + 1);
-                if (fm1 && fp1) {
-                    const bool fm2 = (j - 2 >= 0) && inf(j - 2);
-                    const bool fp2 = (j + 2 <= q.jm - 1) && inf(j + 2);
-                    if (fm2 && fp2) {
-                        const double d4 = S(2) - 4.0 * S(1) + 6.0 * cc - 4.0 * S(-1) + S(-2);
-                        out = cc - q.c4 * d4;
-                    } else {
-                        out = cc + q.c2 * (S(-1) - 2.0 * cc + S(1));
-                    }
-                }
-            } else {
-                const int jm1 = j - 1 > 0 ? j - 1 : 0, jp1 = j + 1 < q.jm - 1 ? j + 1 : q.jm - 1;
-                const double vm = inf(jm1) ? S(jm1 - j) : cc;
-                const double vp = inf(jp1) ? S(jp1 - j) : cc;
-                out = cc + q.c2 * (vm - 2.0 * cc + vp);
-            }
-        }
-        J[ii][jj][kc] = out;
-    }
-    __syncthreads();
-    // i pass on the j pass, from the fluid floor i_topography up; written to dst
-    for (int e = threadIdx.x; e < ST_I * ST_J * ST_K; e += blockDim.x) {
-        const int kc = e % ST_K, jj = (e / ST_K) % ST_J, ii = e / (ST_K * ST_J);
-        const int i = i0 + ii, j = j0 + jj, k = k0 + kc;
-        if (i >= q.im || j >= q.jm || k >= q.km) continue;
-        auto S = [&](int di) { return J[ii + 2 + di][jj][kc]; };
-        const int is = floor_of(topo, q.use_topo, j, k, q.km);
-        const double cc = S(0);
-        double out = cc;
-        if (i >= is) {
-            if (q.order == 4) {
-                const bool fm1 = (i - 1 >= is), fp1 = (i + 1 <= q.im - 1);
-                if (fm1 && fp1) {
-                    const bool fm2 = (i - 2 >= is), fp2 = (i + 2 <= q.im - 1);
-                    if (fm2 && fp2) {
-                        const double d4 = S(2) - 4.0 * S(1) + 6.0 * cc - 4.0 * S(-1) + S(-2);
-                        out = cc - q.c4 * d4;
-                    } else {
-                        out = cc + q.c2 * (S(-1) - 2.0 * cc + S(1));
-                    }
-                }
-            } else {
-                const int im1 = i - 1 > is ? i - 1 : is, ip1 = i + 1 < q.im - 1 ? i + 1 : q.im - 1;
-                out = cc + q.c2 * (S(im1 - i) - 2.0 * cc + S(ip1 - i));
-            }
-        }
-        dst[(size_t)i * plane + (size_t)j * q.KP + k] = out;
-    }
+    dst[c] = out;
 }
 
 // balanceColumnV: column means (one thread per column, the reference's summation order)
@@ -199,12 +186,15 @@ int launch_shapiro(AtjupCtx* c, double* f, int order, double strength, int passe
     q.use_topo = use_topo;
     q.c4 = strength / 16.0;
     q.c2 = strength * 0.25;
-    const dim3 g3((P.km + ST_K - 1) / ST_K, (P.jm + ST_J - 1) / ST_J, (P.im + ST_I - 1) / ST_I);
+    double* tmp2 = c->tmp2;
+    dim3 grid((P.km + 127) / 128, P.jm, P.im);
     for (int p = 0; p < passes; p++) {
         c->launches++;
-        shapiro3_kernel<<<g3, 256, 0, c->stream>>>(f, c->tmp, c->topo, q);
-        ATJUP_CUDA(cudaMemcpyAsync(f, c->tmp, sizeof(double) * c->NP, cudaMemcpyDeviceToDevice,
-                                   c->stream));
+        shapiro_k_kernel<<<grid, 128, 0, c->stream>>>(f, c->tmp, c->topo, q);
+        c->launches++;
+        shapiro_j_kernel<<<grid, 128, 0, c->stream>>>(c->tmp, tmp2, c->topo, q);
+        c->launches++;
+        shapiro_i_kernel<<<grid, 128, 0, c->stream>>>(tmp2, f, c->topo, q);
     }
     ATJUP_CHECK_LAUNCH("shapiro");
     return ATJUP_OK;

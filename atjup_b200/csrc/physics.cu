@@ -57,7 +57,6 @@ struct PhysStage {
     const double* x1[ATJUP_S_COUNT];   // X1, X2 of the species (stage 3, acc_free)
     const double* x2[ATJUP_S_COUNT];
     double inv_c_half, inv_dt;         // 1 / c of stages 0 and 1 (2 / dt) and of stage 2 (1 / dt)
-    unsigned* kerr;                    // error word: bit 0, a staged copy did not arrive
     double c_in, wgt, dt, one_sixth;
     double inv_2dr, inv_2dthe, inv_2dphi, inv_dr2, inv_dthe2, inv_dphi2;
     double coef[ATJUP_S_COUNT];        // species_diff_scale / (sc re)
@@ -294,183 +293,6 @@ __global__ void __launch_bounds__(256) species_stage_kernel(PhysStage a) {
     z.nue_t_s = nue_t / (R)0.9;
     z.rho = rho;
     species_all<0, TI, TO, TA, R>(a, x, z);
-}
-
-// ---- the FP64 species stage with its rows staged by the bulk-copy engine ----
-//
-// The same cell rule as species_stage_kernel, but each species' rows come into shared memory by
-// asynchronous bulk copies (cp.async.bulk on an mbarrier, this GPU's memory only) issued by one
-// thread two species ahead of the block's arithmetic: the bytes in flight are the copies', not
-// the threads' registers. A block owns 128 meridians x 2 colatitude rows of one radial level;
-// per species its slot holds the stage input's rows j0-1 .. j0+2 of level i with a two-cell halo
-// in k, its rows j0, j0+1 of levels i-1 and i+1, and the time-level-n value and the sources (at
-// stage 3 also X1 and X2) of rows j0, j0+1, each row at smem word (k - k0 + 2). The ring's
-// wrap-around (k = 0 and k >= km-2) reads those neighbours from global memory.
-constexpr int SP_ROWS = 18, SP_ROW = 132, SP_SLOTS = 2;
-constexpr int SP_MAX_SPIN = 1 << 26;
-
-struct SpSlot {
-    double r[SP_ROWS][SP_ROW];
-};
-enum { SR_C = 0, SR_IM = 4, SR_IP = 6, SR_QN = 8, SR_S0 = 10, SR_S1 = 12, SR_X1 = 14, SR_X2 = 16 };
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"((unsigned)__cvta_generic_to_shared(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
-                 ::"r"((unsigned)__cvta_generic_to_shared(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                 " selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(ok) : "r"((unsigned)__cvta_generic_to_shared(bar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src), "r"(bytes),
-                   "r"((unsigned)__cvta_generic_to_shared(bar)) : "memory");
-}
-
-// The rows of species S into a slot (one thread): the row copies and their byte count on bar.
-template <int S>
-__device__ void sp_issue(const PhysStage& a, SpSlot& sl, uint64_t* bar, int i, int j0, int k0) {
-    const int jm = a.jm, KP = a.KP;
-    // k range of the halo rows (two cells each side, clipped to the row) and of the others
-    const int ks = k0 == 0 ? 0 : k0 - 2;
-    const int nc = min(k0 + 130, KP) - ks;
-    const int nr = min(k0 + 128, KP) - k0;
-    const int oc = ks - (k0 - 2);                  // smem word of ks
-    const double* F = static_cast<const double*>(a.q_in[S]);
-    const double* src1 = species_src1<S>(a);
-    const bool st3 = a.stage == 3;
-    // per row j0, j0 + 1: levels i-1 and i+1, the time-level-n value, src0 (+ src1, + X1, X2)
-    const unsigned rows_other = 2 * (4 + (src1 ? 1 : 0) + (st3 ? 2 : 0));
-    mbar_expect(bar, (unsigned)(4 * nc * 8) + rows_other * (unsigned)(nr * 8));
-    auto row = [&](int ii, int jj) { return ((size_t)ii * jm + jj) * KP; };
-    auto cj = [&](int jj) { return jj < 0 ? 0 : (jj > jm - 1 ? jm - 1 : jj); };
-    const int im_ = i > 0 ? i - 1 : i, ip_ = i < a.im - 1 ? i + 1 : i;
-    for (int r = 0; r < 4; r++)
-        bulk_copy(&sl.r[SR_C + r][oc], F + row(i, cj(j0 - 1 + r)) + ks, nc * 8, bar);
-    for (int r = 0; r < 2; r++) {
-        const int jj = cj(j0 + r);
-        bulk_copy(&sl.r[SR_IM + r][2], F + row(im_, jj) + k0, nr * 8, bar);
-        bulk_copy(&sl.r[SR_IP + r][2], F + row(ip_, jj) + k0, nr * 8, bar);
-        bulk_copy(&sl.r[SR_QN + r][2], a.q_n[S] + row(i, jj) + k0, nr * 8, bar);
-        bulk_copy(&sl.r[SR_S0 + r][2], species_src0<S>(a) + row(i, jj) + k0, nr * 8, bar);
-        if (src1) bulk_copy(&sl.r[SR_S1 + r][2], src1 + row(i, jj) + k0, nr * 8, bar);
-        if (st3) {
-            bulk_copy(&sl.r[SR_X1 + r][2], a.x1[S] + row(i, jj) + k0, nr * 8, bar);
-            bulk_copy(&sl.r[SR_X2 + r][2], a.x2[S] + row(i, jj) + k0, nr * 8, bar);
-        }
-    }
-}
-
-// wait for a slot's copies; false (and the error word set) if they did not arrive
-__device__ __forceinline__ bool sp_wait(const PhysStage& a, uint64_t* bar, unsigned parity) {
-    for (int n = 0; n < SP_MAX_SPIN; n++)
-        if (mbar_try(bar, parity)) return true;
-    atomicOr(a.kerr, 1u);
-    return false;
-}
-
-template <int S>
-__device__ __forceinline__ void sp_cell(const PhysStage& a, const SpSlot& sl,
-                                        const CellShared<double>& z, int ty, int tx, size_t c,
-                                        size_t rowc, int k) {
-    const int w = tx + 2;
-    const double* F = static_cast<const double*>(a.q_in[S]);
-    const double f0 = sl.r[SR_C + 1 + ty][w];
-    const double fjm = sl.r[SR_C + ty][w], fjp = sl.r[SR_C + 2 + ty][w];
-    // the ring of km-1 meridians: k-1 of 0 is km-2, k+1 of km-2 (and of the seam copy) is 0
-    const double fkm = k == 0 ? F[rowc + a.km - 2] : sl.r[SR_C + 1 + ty][w - 1];
-    const double fkp = k >= a.km - 2 ? F[rowc] : sl.r[SR_C + 1 + ty][w + 1];
-    const double fim = sl.r[SR_IM + ty][w], fip = sl.r[SR_IP + ty][w];
-    const double qn = sl.r[SR_QN + ty][w];
-    const double src0 = sl.r[SR_S0 + ty][w];
-    const double src1 = species_src1<S>(a) ? sl.r[SR_S1 + ty][w] : 0.0;
-    double x1 = 0.0, x2 = 0.0;
-    if (a.stage == 3) { x1 = sl.r[SR_X1 + ty][w]; x2 = sl.r[SR_X2 + ty][w]; }
-    const double r = species_rhs<S, double>(a, z, f0, fip, fim, fjp, fjm, fkp, fkm, src0, src1);
-    static_cast<double*>(a.q_out[S])[c] = species_acc_free_out<S>(a, r, f0, qn, x1, x2);
-}
-
-// Species S: wait for its slot (every thread, bounded), compute, release the slot to species
-// S + SP_SLOTS. After a copy that did not arrive (the error word set) the block computes nothing
-// more and issues no more copies; it still waits (bounded) for the copies it has issued, then
-// returns.
-template <int S>
-__device__ __forceinline__ void sp_all(const PhysStage& a, SpSlot* slots, uint64_t* bars,
-                                       const CellShared<double>& z, bool work, bool producer,
-                                       int ty, int tx, size_t c, size_t rowc, int i, int j0, int k0,
-                                       int k) {
-    const int sl = S % SP_SLOTS;
-    const bool here = sp_wait(a, &bars[sl], (S / SP_SLOTS) & 1);
-    if (__syncthreads_or(!here)) {
-        for (int q = 1; q < SP_SLOTS && S + q < ATJUP_S_COUNT; q++)
-            sp_wait(a, &bars[(S + q) % SP_SLOTS], ((S + q) / SP_SLOTS) & 1);
-        return;
-    }
-    if (work) sp_cell<S>(a, slots[sl], z, ty, tx, c, rowc, k);
-    __syncthreads();
-    if constexpr (S + SP_SLOTS < ATJUP_S_COUNT) {
-        if (producer) sp_issue<S + SP_SLOTS>(a, slots[sl], &bars[sl], i, j0, k0);
-    }
-    if constexpr (S + 1 < ATJUP_S_COUNT) sp_all<S + 1>(a, slots, bars, z, work, producer, ty, tx, c, rowc, i, j0, k0, k);
-}
-
-__global__ void __launch_bounds__(256) species_staged_kernel(PhysStage a) {
-    extern __shared__ __align__(128) unsigned char sp_smem[];
-    SpSlot* slots = reinterpret_cast<SpSlot*>(sp_smem);
-    __shared__ __align__(8) uint64_t bars[SP_SLOTS];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int k0 = blockIdx.x * blockDim.x, j0 = blockIdx.y * blockDim.y, i = blockIdx.z;
-    const int k = k0 + tx, j = j0 + ty;
-    const bool producer = tx == 0 && ty == 0;
-    if (producer) {
-        for (int s = 0; s < SP_SLOTS; s++) mbar_init(&bars[s]);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-    if (producer) {
-        sp_issue<0>(a, slots[0], &bars[0], i, j0, k0);
-        sp_issue<1>(a, slots[1], &bars[1], i, j0, k0);
-    }
-    const bool in = k < a.km && j < a.jm;
-    const size_t rowc = ((size_t)i * a.jm + (in ? j : 0)) * a.KP;
-    const size_t c = rowc + (in ? k : 0);
-    bool work = false;
-    CellShared<double> z{};
-    if (in) {
-        const uint8_t fl = a.flags[c];
-        if (fl & NB_INT) {
-            work = true;
-            const double u0 = static_cast<const double*>(a.u)[c];
-            const double v0 = static_cast<const double*>(a.v)[c];
-            const double w0 = static_cast<const double*>(a.w)[c];
-            const double nv = a.has_nue ? a.nue[c] : 0.0;
-            const GeoIJ& g = a.geo[(size_t)i * a.jm + j];
-            z.u0 = u0;
-            z.v_invrm = v0 * g.inv_rm;
-            z.w_invrs = w0 * g.inv_rmsinthe;
-            z.two_inv_rm = 2.0 * g.inv_rm;
-            z.inv_rm2 = g.inv_rm2;
-            z.ci = g.costhe_inv_rm2sinthe;
-            z.is2 = g.inv_rm2sinthe2;
-            double nue_t64 = 0.0;
-            if (a.has_nue && a.turb_coupling != 0.0 && isfinite(nv)) nue_t64 = a.turb_coupling * dmax(0.0, nv);
-            z.nue_t_s = nue_t64 / 0.9;
-            z.rho = a.rho_mix[c];
-        } else if (a.stage < 3) {
-            // the cell keeps its live values through the step
-#pragma unroll
-            for (int s = 0; s < ATJUP_S_COUNT; s++)
-                static_cast<double*>(a.q_out[s])[c] = a.q_live[s][c];
-        }
-    }
-    sp_all<0>(a, slots, bars, z, work, producer, ty, tx, c, rowc, i, j0, k0, k);
 }
 
 // k*, omega*: transport, diffusion with the model's coefficients, and the closure sources
@@ -753,7 +575,6 @@ PhysStage stage_args(AtjupCtx* c, int stage, const void* const* vin) {
     a.geo = c->geo;
     a.im = P.im; a.jm = P.jm; a.km = P.km; a.KP = c->KP; a.stage = stage;
     a.acc_free = (c->step_prec != ATJUP_PREC_MIXED) ? 1 : 0;
-    a.kerr = c->kerr;
     a.inv_c_half = 2.0 / P.dt;
     a.inv_dt = 1.0 / P.dt;
     a.c_in = (stage == 0 || stage == 1) ? 0.5 * P.dt : (stage == 2 ? P.dt : 0.0);
@@ -798,14 +619,6 @@ static int launch_typed(AtjupCtx* c, const PhysStage& a, int what, cudaStream_t 
     const dim3 block(128, 2);
     const dim3 grid((P.km + 127) / 128, (P.jm + 1) / 2, P.im);
     if (what == 0) {
-        if constexpr (sizeof(TI) == 8 && sizeof(TO) == 8) {
-            if (a.acc_free) {
-                species_staged_kernel<<<grid, block, SP_SLOTS * sizeof(SpSlot), st>>>(a);
-                c->launches++;
-                ATJUP_CHECK_LAUNCH("species_staged_kernel");
-                return ATJUP_OK;
-            }
-        }
         species_stage_kernel<TI, TO, TA, R><<<grid, block, 0, st>>>(a);
         c->launches++;
         ATJUP_CHECK_LAUNCH("species_stage_kernel");

@@ -72,7 +72,6 @@ def load_library() -> ctypes.CDLL:
     L.atjup_gpu_timing.argtypes = [vp, i32]
     L.atjup_gpu_timing_read.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(ctypes.c_int64)]
     L.atjup_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
-    L.atjup_gpu_kernel_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
     L.atjup_gpu_satadj.argtypes = [vp, i32, ctypes.POINTER(_p.AtjupGasParams),
                                    ctypes.POINTER(_p.AtjupSatStats)]
     L.atjup_gpu_set_physics.argtypes = [vp, ctypes.POINTER(_p.AtjupPhysics), vp]
@@ -470,12 +469,6 @@ class GpuModel:
     TIMING_CLASSES = ("rk_stage", "rk_aux", "pressure", "bc", "shapiro", "balance_v",
                       "mixture", "solver", "satadj", "species", "closure", "turb", "micro", "mca",
                       "rk_group", "cone")
-
-    def kernel_errors(self) -> int:
-        """the error word of the kernels' bounded waits (0: none timed out)"""
-        e = ctypes.c_uint32()
-        _check(self.L.atjup_gpu_kernel_errors(self.ctx, ctypes.byref(e)))
-        return e.value
 
     def timing(self, on: bool):
         """Start (reset) or stop CUDA-event timing of the library's kernel launches."""

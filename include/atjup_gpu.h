@@ -576,10 +576,6 @@ enum { ATJUP_TK_RK_STAGE = 0, ATJUP_TK_RK_AUX, ATJUP_TK_PRESSURE, ATJUP_TK_BC, A
        ATJUP_TK_CLOSURE, ATJUP_TK_TURB, ATJUP_TK_MICRO, ATJUP_TK_MCA, ATJUP_TK_RK_GROUP,
        ATJUP_TK_CONE, ATJUP_TK_COUNT };
 int atjup_gpu_timing(AtjupCtx* ctx, int32_t enable);   /* 1: reset and record; 0: stop */
-/* The error word of the kernels' bounded waits since the context was made (synchronises): 0, or
- * bit 0 when an asynchronous copy of the staged species stage did not arrive in time (the block
- * then stopped computing and the step's species are incomplete). */
-int atjup_gpu_kernel_errors(AtjupCtx* ctx, uint32_t* errors);
 int atjup_gpu_timing_read(AtjupCtx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Number of kernels this context has launched since creation. */
 int atjup_gpu_launch_count(AtjupCtx* ctx, int64_t* launches);

@@ -62,10 +62,9 @@ def test_shapiro_small(small, order):
 
 
 @pytest.mark.parametrize("order", [2, 4])
-def test_shapiro_fused_bit_exact(small, order):
-    """The fused three-pass kernel (k, j, i passes in one tile) equals the oracle's separate
-    passes (lib/Utils.cpp:227-453) to the bit: same rules, same order of operations, no FMA
-    contraction on either side."""
+def test_shapiro_bit_exact(small, order):
+    """The filter's k, j and i passes equal the oracle's (lib/Utils.cpp:227-453) to the bit:
+    same rules, same order of operations, no FMA contraction on either side."""
     p, g, f = small
     o = oracle_from(p, g, f)
     m = gpu_from(p, g, f)
