@@ -2,7 +2,7 @@
 """Benchmark of ATJUP's time step on B200: one model iteration with the full physics.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload phys|dry|adjoint] [--precision fp64|mixed] [--no-extras]
+                    [--workload phys|dry|adjoint|cone] [--precision fp64|mixed] [--no-extras]
 
 Workload (default `phys`): the full-physics configuration on the 41 x 181 x 361 shell (2.68 M
 cells, FP64). Each step is one iteration of the reference's loop (cJupiterModel.cpp:1032-1381):
@@ -624,6 +624,23 @@ def run_adjoint(args):
     print(json.dumps(line))
 
 
+def run_cone(args):
+    """--workload cone: the projection around the obstacle alone (cone_section, `steps` calls),
+    as its own JSON line."""
+    d = reference_state("dry", 0, None)
+    if d is None:
+        print(json.dumps({"workload": "cone", "unavailable": "needs the reference's initial state"}))
+        return
+    P, _, _, _, grid, fields = model_inputs(d, "dry")
+    c = cone_section(P, grid, fields, calls=max(args.steps, 1))
+    line = {"metric": "s per call of the in-loop projection around the obstacle (26 levels, two "
+                      "solves each)", "value": c.pop("gpu_s_per_call"), "unit": "s/call",
+            "n_gpus": 1, "steps": args.steps, "warmup": 0, "higher_is_better": False,
+            "dtype": "f64", "data": STATE_RECIPE["dry"],
+            "config": {"workload": "projection around the obstacle", "grid": "41x181x361"}, **c}
+    print(json.dumps(line))
+
+
 PROGNOSTIC = ("t", "u", "v", "w", "p_dyn", "h2o", "h2o_cloud", "h2o_ice", "h2s", "nh3",
               "nh3_cloud", "nh3_ice", "ch4", "ch4_cloud", "ch4_ice", "nh4sh", "tke", "dis")
 
@@ -637,7 +654,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the Poisson, adjoint and mixed-precision accuracy sections")
-    ap.add_argument("--workload", default="phys", choices=["phys", "dry", "adjoint"])
+    ap.add_argument("--workload", default="phys", choices=["phys", "dry", "adjoint", "cone"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None,
                     help="IMxJMxKM of a smaller synthetic shell, for profiling only (the metric "
@@ -652,6 +669,9 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.workload == "adjoint":
         run_adjoint(args)
+        return
+    if args.workload == "cone":
+        run_cone(args)
         return
 
     import numpy as np

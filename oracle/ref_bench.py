@@ -7,7 +7,8 @@ seeded initial state applied (oracle/baseline_state.py; untimed), `warmup` itera
 then `steps` iterations of the cJupiterModel.cpp:1032-1381 schedule -- the dry configuration, or
 with --phys the reference's default full physics (the k-omega SST closure, radiation,
 precipitation, the saturation adjustments, the NH4SH equilibrium, the chemistry block and the
-moist convective adjustment every iteration, as baseline_state.PHYS_ENV sets) -- each timed by
+moist convective adjustment every iteration, as baseline_state.PHYS_ENV sets), both with the
+projection around the obstacle every 10 iterations (the reference's default) -- each timed by
 wall clock on the host. Prints one JSON line.
 
     python oracle/ref_bench.py --steps K --warmup W [--threads T] [--phys]
