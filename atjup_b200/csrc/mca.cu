@@ -16,10 +16,11 @@
 //                       the unadjusted column (the pair test, the "held by composition" count);
 //                       a column with an unstable pair, or with a cell the reference would refuse,
 //                       is appended to a list.
-//   mca_column_kernel   one thread per listed column: the reference's whole column algorithm
+//   mca_column_kernel   one warp per listed column: the reference's whole column algorithm
 //                       (starting from the census the census kernel recorded per pair, the sweeps,
 //                       the segment growth, the relaxation, the write-back), with the column's
-//                       state in a per-thread slot in global memory.
+//                       state in a per-warp slot in global memory and its independent parts (the
+//                       settles of a mixed segment, the pair tests of a sweep) on the lanes.
 // A column that is not listed is left alone by the reference too (no unstable pair: pass 1 mixes
 // nothing). The equilibrium solve and every expression keep the reference's operand order, and
 // the file is compiled without FMA contraction; the parcel test compares a virtual-temperature
@@ -33,7 +34,7 @@ constexpr int NG = 2, NT = 2;          // gases H2O, NH3; tracers H2S, NH4SH
 constexpr int MAXI = 64;               // levels a column slot holds (the reference grid has 41)
 constexpr int NITER = 60;              // cap of the equilibrium solve
 constexpr double TOL_K = 1.0e-7, TOL_T = 1.0e-10;
-constexpr int NSLOT = 4096;            // columns adjusted concurrently (per-thread scratch slots)
+constexpr int NSLOT = 4096;            // columns adjusted concurrently (per-warp scratch slots)
 constexpr int NPART = 256;             // partial census counters (spread so the adds do not contend)
 
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
@@ -256,6 +257,8 @@ struct Col {
     double qt[MAXI][NG], qv[MAXI][NG], qc[MAXI][NG], qi[MAXI][NG], ceq[MAXI][NG], qt0[MAXI][NG];
     double qr[MAXI][NT], qr0[MAXI][NT];
     char eq_ok[MAXI], touched[MAXI], cen_u[MAXI], cen_m[MAXI];
+    char pt_u[MAXI];           // the pair tests of a sweep on the state it starts from
+    char dirty[MAXI];          // mixed since those tests
 };
 
 __device__ bool col_unstable(const McaArgs& a, Col& C, int lo, int up, bool* held, bool* moist) {
@@ -284,7 +287,39 @@ __device__ bool col_settle(const McaArgs& a, Col& C, int q) {
     C.touched[q] = 1;
     return true;
 }
-__device__ bool col_mix(const McaArgs& a, Col& C, int lo, int up) {
+// One warp per listed column: NSLOT warps, COL_WARPS per block; listed column idx goes to warp
+// idx / blocks of block idx % blocks, so a few listed columns land on as many SMs. The
+// reference's algorithm walks the column in order, but most of its work is independent: the
+// loads, the settles of a mixed segment (one equilibrium solve per level), the two edge tests of
+// a growing segment, and, from the second sweep on, the pair tests of the sweep on the state it
+// starts from (a pair whose two levels no mix of the sweep has touched yet tests the same then as
+// when the walk reaches it: the test is a pure function of the two levels). The lanes take those;
+// the walk itself (the next pair, the segment's bounds, a mix's sums in the reference's order)
+// runs in step on every lane, and a lone test on lane 0. Every value comes from the same
+// expression as in the sequential algorithm, so the result is the same.
+constexpr int COL_WARPS = 4;
+constexpr unsigned FULL_WARP = 0xffffffffu;
+
+// the pair test (lo, up) on lane 0 (it may fill the equilibrium cache of up), its result on every
+// lane
+__device__ bool warp_unstable(const McaArgs& a, Col& C, int lo, int up, bool* moist, unsigned lane) {
+    int u = 0, m = 0;
+    if (lane == 0) {
+        bool mm = false;
+        u = col_unstable(a, C, lo, up, nullptr, &mm) ? 1 : 0;
+        m = mm ? 1 : 0;
+    }
+    __syncwarp();
+    u = __shfl_sync(FULL_WARP, u, 0);
+    m = __shfl_sync(FULL_WARP, m, 0);
+    if (moist) *moist = m != 0;
+    return u != 0;
+}
+
+// col_mix with the levels' settles spread over the lanes: the sums on every lane in the
+// reference's order, then each lane sets and settles its levels. A failed settle abandons the
+// column, so the levels set after it do not matter.
+__device__ bool warp_mix(const McaArgs& a, Col& C, int lo, int up, unsigned lane) {
     double sw = 0.0, sh = 0.0, sq[NG] = {0.0, 0.0}, sr[NT] = {0.0, 0.0};
     for (int q = lo; q <= up; q++) {
         sw += C.w[q];
@@ -292,34 +327,38 @@ __device__ bool col_mix(const McaArgs& a, Col& C, int lo, int up) {
         for (int g = 0; g < NG; g++) sq[g] += C.w[q] * C.qt[q][g];
         for (int r = 0; r < NT; r++) sr[r] += C.w[q] * C.qr[q][r];
     }
-    for (int q = lo; q <= up; q++) {
+    __syncwarp();
+    bool ok = true;
+    for (int q = lo + (int)lane; q <= up; q += 32) {
         C.hL[q] = sh / sw;
         for (int g = 0; g < NG; g++) C.qt[q][g] = sq[g] / sw;
         for (int r = 0; r < NT; r++) C.qr[q][r] = sr[r] / sw;
-        if (!col_settle(a, C, q)) return false;
+        C.dirty[q] = 1;
+        if (ok && !col_settle(a, C, q)) ok = false;
     }
-    return true;
+    ok = __all_sync(FULL_WARP, ok) != 0;
+    __syncwarp();
+    return ok;
 }
 
-// NSLOT threads in blocks of COL_BLOCK; listed column idx goes to lane idx / blocks of block
-// idx % blocks, so a few listed columns land on as many SMs, not on the lanes of one block
-constexpr int COL_BLOCK = 32;
-__global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* slots) {
-    const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
-    Col& C = slots[slot];
+__global__ void __launch_bounds__(32 * COL_WARPS) mca_column_kernel(McaArgs a, Col* slots) {
+    const unsigned lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    Col& C = slots[blockIdx.x * COL_WARPS + wi];
     const unsigned n = *a.count;
-    for (unsigned idx = threadIdx.x * gridDim.x + blockIdx.x; idx < n; idx += NSLOT) {
+    for (unsigned idx = wi * gridDim.x + blockIdx.x; idx < n; idx += NSLOT) {
         const unsigned col = a.list[idx];
         const int j = (int)(col / (unsigned)a.km), k = (int)(col % (unsigned)a.km);
         const int2 b = a.bounds[col];
         const int i0 = b.x, i1 = b.y;
         const size_t plane = (size_t)a.jm * a.KP, c0 = (size_t)j * a.KP + k;
+        // the column's cells (the reference refuses the whole column for any one of them)
         bool ok = true;
-        for (int i = i0; i <= i1; i++) { C.eq_ok[i] = 0; C.touched[i] = 0; }
-        for (int i = i0; i <= i1 && ok; i++) {
+        for (int i = i0 + (int)lane; i <= i1; i += 32) {
+            C.eq_ok[i] = 0;
+            C.touched[i] = 0;
+            C.dirty[i] = 0;
             Cell x;
-            ok = load_cell(a, i, c0 + (size_t)i * plane, x);
-            if (!ok) break;
+            if (!load_cell(a, i, c0 + (size_t)i * plane, x)) { ok = false; continue; }
             C.T[i] = C.T0[i] = x.T;
             C.p[i] = x.p;
             C.z[i] = x.z;
@@ -330,45 +369,70 @@ __global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* s
             }
             for (int r = 0; r < NT; r++) C.qr[i][r] = x.qr[r];
         }
-        if (ok)
-            for (int i = i0; i <= i1 && ok; i++) {
+        ok = __all_sync(FULL_WARP, ok) != 0;
+        __syncwarp();
+        if (ok) {
+            for (int i = i0 + (int)lane; i <= i1; i += 32) {
                 const double lo = (i > i0) ? 0.5 * (C.z[i - 1] + C.z[i]) : C.z[i0];
                 const double hi = (i < i1) ? 0.5 * (C.z[i] + C.z[i + 1]) : C.z[i1];
                 C.w[i] = C.rho[i] * (hi - lo);
                 if (!(C.w[i] > 0.0)) ok = false;
             }
-        if (!ok) { atomicAdd(&a.stats[6], 1ull); continue; }
+            ok = __all_sync(FULL_WARP, ok) != 0;
+        }
+        if (!ok) {
+            if (lane == 0) atomicAdd(&a.stats[6], 1ull);
+            __syncwarp();
+            continue;
+        }
         // the census of the first sweep, as the census kernel found it (the same pair tests on the
         // same state); every pair of a column that loads is written there
-        for (int i = i0; i < i1; i++) {
+        for (int i = i0 + (int)lane; i < i1; i += 32) {
             const uint8_t f = a.pairs[((size_t)i * a.jm + j) * a.km + k];
             C.cen_u[i] = f & 1;
             C.cen_m[i] = (f >> 1) & 1;
         }
-        for (int i = i0; i <= i1; i++) {
+        for (int i = i0 + (int)lane; i <= i1; i += 32) {
             C.hL0[i] = C.hL[i];
             for (int g = 0; g < NG; g++) C.qt0[i][g] = C.qt[i][g];
             for (int r = 0; r < NT; r++) C.qr0[i][r] = C.qr[i][r];
         }
+        __syncwarp();
         int passes = 0;
         long long layers = 0, moist_t = 0, dry_t = 0;
         bool changed = true, fail = false;
         while (changed && passes < a.max_pass && !fail) {
             changed = false;
             passes++;
+            if (passes >= 2) {
+                for (int i = i0 + (int)lane; i < i1; i += 32) {
+                    bool m = false;
+                    C.pt_u[i] = col_unstable(a, C, i, i + 1, nullptr, &m) ? 1 : 0;
+                }
+                for (int i = i0 + (int)lane; i <= i1; i += 32) C.dirty[i] = 0;
+                __syncwarp();
+            }
             int i = i0;
             while (i < i1 && !fail) {
                 bool moist = false, uns;
                 if (passes == 1 && !C.touched[i] && !C.touched[i + 1]) { uns = C.cen_u[i]; moist = C.cen_m[i]; }
-                else uns = col_unstable(a, C, i, i + 1, nullptr, &moist);
+                else if (passes >= 2 && !C.dirty[i] && !C.dirty[i + 1]) uns = C.pt_u[i];
+                else uns = warp_unstable(a, C, i, i + 1, &moist, lane);
                 if (!uns) { i++; continue; }
                 if (passes == 1) { if (moist) moist_t++; else dry_t++; }
                 int lo = i, up = i + 1;
                 for (;;) {
-                    if (!col_mix(a, C, lo, up)) { fail = true; break; }
+                    if (!warp_mix(a, C, lo, up, lane)) { fail = true; break; }
+                    // the two edge tests, independent of each other, on lanes 0 and 1
+                    int e0 = 0, e1 = 0;
+                    if (lane == 0 && lo > i0) e0 = col_unstable(a, C, lo - 1, lo, nullptr, nullptr) ? 1 : 0;
+                    if (lane == 1 && up < i1) e1 = col_unstable(a, C, up, up + 1, nullptr, nullptr) ? 1 : 0;
+                    __syncwarp();
+                    e0 = __shfl_sync(FULL_WARP, e0, 0);
+                    e1 = __shfl_sync(FULL_WARP, e1, 1);
                     bool ext = false;
-                    if (lo > i0 && col_unstable(a, C, lo - 1, lo, nullptr, nullptr)) { lo--; ext = true; }
-                    if (up < i1 && col_unstable(a, C, up, up + 1, nullptr, nullptr)) { up++; ext = true; }
+                    if (e0) { lo--; ext = true; }
+                    if (e1) { up++; ext = true; }
                     if (!ext) break;
                 }
                 layers += up - lo + 1;
@@ -376,23 +440,34 @@ __global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* s
                 i = up;
             }
         }
-        if (passes >= 1 && (moist_t || dry_t)) {
+        if (lane == 0 && passes >= 1 && (moist_t || dry_t)) {
             atomicAdd(&a.stats[2], (unsigned long long)moist_t);
             atomicAdd(&a.stats[3], (unsigned long long)dry_t);
         }
-        if (fail) { atomicAdd(&a.stats[6], 1ull); continue; }
+        if (fail) {
+            if (lane == 0) atomicAdd(&a.stats[6], 1ull);
+            __syncwarp();
+            continue;
+        }
         if (layers == 0) continue;
         if (a.relax < 1.0) {
-            for (int q = i0; q <= i1 && !fail; q++) {
-                if (!C.touched[q]) continue;
+            bool rok = true;
+            for (int q = i0 + (int)lane; q <= i1; q += 32) {
+                if (!C.touched[q] || !rok) continue;
                 C.hL[q] = C.hL0[q] + a.relax * (C.hL[q] - C.hL0[q]);
                 for (int g = 0; g < NG; g++) C.qt[q][g] = C.qt0[q][g] + a.relax * (C.qt[q][g] - C.qt0[q][g]);
                 for (int r = 0; r < NT; r++) C.qr[q][r] = C.qr0[q][r] + a.relax * (C.qr[q][r] - C.qr0[q][r]);
-                if (!col_settle(a, C, q)) fail = true;
+                if (!col_settle(a, C, q)) rok = false;
             }
-            if (fail) { atomicAdd(&a.stats[6], 1ull); continue; }
+            rok = __all_sync(FULL_WARP, rok) != 0;
+            __syncwarp();
+            if (!rok) {
+                if (lane == 0) atomicAdd(&a.stats[6], 1ull);
+                __syncwarp();
+                continue;
+            }
         }
-        for (int q = i0; q <= i1; q++) {
+        for (int q = i0 + (int)lane; q <= i1; q += 32) {
             if (!C.touched[q]) continue;
             const size_t c = c0 + (size_t)q * plane;
             a.t[c] = C.T[q] / a.t_ref;
@@ -403,9 +478,12 @@ __global__ void __launch_bounds__(COL_BLOCK) mca_column_kernel(McaArgs a, Col* s
             }
             for (int r = 0; r < NT; r++) a.trf[r][c] = C.qr[q][r] * C.rho[q];
         }
-        atomicAdd(&a.stats[0], 1ull);
-        atomicAdd(&a.stats[1], (unsigned long long)layers);
-        atomicMax(&a.stats[7], (unsigned long long)passes);
+        if (lane == 0) {
+            atomicAdd(&a.stats[0], 1ull);
+            atomicAdd(&a.stats[1], (unsigned long long)layers);
+            atomicMax(&a.stats[7], (unsigned long long)passes);
+        }
+        __syncwarp();
     }
 }
 
@@ -472,7 +550,7 @@ int launch_mca(AtjupCtx* c) {
     ATJUP_CHECK_LAUNCH("mca_census");
     // the listed columns (almost always none: the kernel then reads the count and returns; the
     // host does not wait for the count, so the launches of the step stay queued ahead)
-    mca_column_kernel<<<NSLOT / COL_BLOCK, COL_BLOCK, 0, c->stream>>>(a, static_cast<Col*>(c->mca_slots));
+    mca_column_kernel<<<NSLOT / COL_WARPS, 32 * COL_WARPS, 0, c->stream>>>(a, static_cast<Col*>(c->mca_slots));
     c->launches++;
     ATJUP_CHECK_LAUNCH("mca_column");
     return ATJUP_OK;
