@@ -102,6 +102,24 @@ def test_gpu_mca_matches_oracle():
 
 
 @pytest.mark.gpu
+def test_gpu_mca_warp_form_matches_oracle():
+    """With at most 2048 listed columns the column kernel runs one warp per column (the settles of
+    a mixed segment and a sweep's pair tests on the lanes); the shell above lists nearly all of its
+    5,917 columns and so runs one thread per column. This smaller shell (1,519 columns) takes the
+    warp form, against the oracle with the same bars."""
+    P, PH, MC, g, f = synthetic_moist_case(41, 31, 49, seed=53)
+    f = R.perturb_unstable(f, g["solid"], f["layer_heights"], seed=54)
+    M = resolve_mca(MCA_ENV)
+    want, wst = oracle_mca(P, MC, M, g, f)
+    got, gst = gpu_mca(P, PH, MC, M, g, f)
+    assert 50 < wst["columns"] <= 2048, wst
+    frac = check_columns(got, want, "synthetic 41x31x49")
+    assert abs(gst["columns"] - wst["columns"]) <= COL_FLIP * wst["columns"] + 1, (gst, wst)
+    assert gst["max_passes"] == wst["max_passes"], (gst, wst)
+    print("mca (warp form) GPU vs oracle: differing columns", frac, "counters GPU", gst, "oracle", wst)
+
+
+@pytest.mark.gpu
 def test_gpu_mca_matches_reference(ref_required):
     d, P, MC, M, g, f = mca_ref_case()
     from atjup_b200.params import resolve_physics
