@@ -322,9 +322,11 @@ __global__ void __launch_bounds__(256, 3) species_stage_kernel(PhysStage a) {
 
 // k*, omega*: transport, diffusion with the model's coefficients, and the closure sources
 // (RHS_Jup_Turb.cpp:257-303, 736-998, 1399-1452). One instantiation per closure model, so that
-// each holds the registers of its own branch only.
+// each holds the registers of its own branch only. Three blocks per SM (at most 80 registers: the
+// k-omega SST form spilled 172 bytes at 64; the step measured 6.70 ms against 6.72 at 64 and 6.82
+// at 128).
 template <int MODEL, typename TI, typename TO, typename TA, typename R>
-__global__ void __launch_bounds__(256, 4) closure_stage_kernel(PhysStage a) {
+__global__ void __launch_bounds__(256, 3) closure_stage_kernel(PhysStage a) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
