@@ -485,8 +485,14 @@ int atjup_gpu_set_stage_buffers(AtjupCtx* c, double* const bufs[12]) {
         c->keep_on = false;
         return ATJUP_OK;
     }
-    for (int b = 0; b < 12; b++)
+    for (int b = 0; b < 12; b++) {
         if (!bufs[b]) { set_error("set_stage_buffers: null buffer"); return ATJUP_ERR_ARG; }
+        // the stage kernel reads its input through tensor maps, whose base must be 16-byte aligned
+        if (reinterpret_cast<uintptr_t>(bufs[b]) % 16) {
+            set_error("set_stage_buffers: buffers must be 16-byte aligned");
+            return ATJUP_ERR_ARG;
+        }
+    }
     if (c->phys_on || c->step_prec != ATJUP_PREC_FP64) {
         set_error("set_stage_buffers: the FP64 dry step only");
         return ATJUP_ERR_UNSUPPORTED;

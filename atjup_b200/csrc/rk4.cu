@@ -11,6 +11,8 @@
 // X_{s+1} there, which is what the reference's untouched live fields hold.
 #include "ctx.cuh"
 
+#include <cuda.h>
+
 namespace atjup {
 namespace {
 
@@ -19,7 +21,7 @@ namespace {
 // never read by a stage (the ring wraps 359 -> 0) and is left alone.
 constexpr int TK = 36, TJ = 7, NT = 256, NL = TK * TJ;   // 252 live threads of 256
 constexpr int NCH = 2;   // radial chunks per column tile (the step: 6.69 ms, 6.72 with 3 or 4)
-constexpr int HK = TK + 2, HJ = TJ + 2, HC = HK * HJ;   // halo tile of one plane
+constexpr int HJ = TJ + 2;                               // halo rows of a tile
 constexpr int NX = 5;    // FP64 per-cell inputs besides Y: rho, wall_nue, nue, Q_rad, Q_precip
 
 // Per-cell flags, precomputed from the static mask (atjup_gpu_set_grid): bit 0 solid, 1 solid i+1,
@@ -68,18 +70,42 @@ struct StagePtrs {
     const double *cell_vbar0, *cell_ubar0;
 };
 
+// The halo tiles of the stage input (t, u, v, w) and of p_dyn, p_hydro are copied by the tensor
+// memory accelerator: one cp.async.bulk.tensor per field and plane, issued by one thread, its
+// completion counted on the ring slot's mbarrier. A box starts on a 16-byte boundary, OX columns
+// before the tile (k0 - OX; OX = 2 doubles or 4 floats), and is TK + 2 OX wide and HJ rows high
+// (j0 - 1 .. j0 + TJ; rows outside the grid arrive as zeros, and only cells that are never
+// integrated read them). Boxes are padded to 128 bytes in shared memory.
+template <typename T>
+struct Box3 {
+    static constexpr int OX = 16 / (int)sizeof(T);
+    static constexpr int W = TK + 2 * OX;
+    static constexpr int BYTES = W * HJ * (int)sizeof(T);
+    static constexpr int PAD = (BYTES + 127) / 128 * 128 / (int)sizeof(T);
+};
+
+// the tensor maps of the stage input's four fields and of p_dyn, p_hydro: [im][jm][KP] arrays,
+// boxes of Box3<T>::W x HJ x 1
+struct __align__(64) StageMaps {
+    CUtensorMap x[4];
+    CUtensorMap p[2];
+};
+
 template <typename TI, typename TA>
-struct __align__(16) StageSmem {
-    double ptile[3][2][HC];   // p_dyn, p_hydro of planes i, i+1, i+2 (in flight), one-cell halo in j, k
+struct __align__(128) StageSmem {
+    TI tile[3][4][Box3<TI>::PAD];            // stage input t, u, v, w of planes i, i+1, i+2
+    double ptile[3][2][Box3<double>::PAD];   // p_dyn, p_hydro of the same planes
+    unsigned long long bar[4];               // the TMA barrier of each ring slot (three used)
     double ps[3][NT];         // p_stat at the cells of the same three planes
     double Yx[2][4][NT];      // time-level-n t, u, v, w of planes i and i+1 (stages 1-3)
     double ex[2][NX][NT];     // FP64 per-cell inputs of planes i and i+1
     GeoIJ geo[2][TJ];         // geometry rows of planes i and i+1
     double cm[2][2][TJ];      // cell-hold means (v, u) of planes i and i+1
-    TI tile[3][4][HC];        // stage input t, u, v, w of planes i, i+1, i+2, one-cell halo
     TA ax[2][4][NT];          // accumulators of planes i and i+1 (stages 1-3)
     uint8_t nb[2][NT];        // per-cell flags of planes i and i+1
 };
+// two blocks per SM: 228 KB of shared memory per SM, 1 KB of it reserved per block
+static_assert(2 * (sizeof(StageSmem<double, double>) + 1024) <= 233472, "two FP64 stage blocks per SM");
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -99,27 +125,90 @@ __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1
 
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 
-// Issue the asynchronous copies of plane i's halo tiles and p_stat into ring slot i % 3.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// One thread: the tensor copies of plane i's six halo boxes into ring slot i % 3, their bytes
+// expected on the slot's barrier. The fence orders the block's earlier plain writes to the slot
+// (the seam patches) before the copies' writes.
 template <typename TI, typename TA>
-__device__ __forceinline__ void issue_tile(StageSmem<TI, TA>& S, const StagePtrs& a,
-                                           const StageConst& q, int i, int j0, int k0, int tid) {
+__device__ __forceinline__ void issue_boxes(StageSmem<TI, TA>& S, const StageMaps& M, int i,
+                                            int j0, int k0) {
     const int sl = i % 3;
-    const size_t base = (size_t)i * q.jm * q.KP;
-    for (int e = tid; e < 6 * HC; e += NT) {
-        const int f = e / HC, h = e - f * HC;
-        const int hj = h / HK, hk = h - hj * HK;
-        int j = j0 - 1 + hj;
-        j = j < 0 ? 0 : (j > q.jm - 1 ? q.jm - 1 : j);
-        int k = k0 - 1 + hk;          // the ring of km-1 meridians: k-1 of 0 is km-2, k+1 of km-2 is 0
-        k = (k < 0) ? q.km - 2 : (k >= q.km - 1 ? 0 : k);   // (beyond km-1: unused lanes)
-        const size_t o = base + (size_t)j * q.KP + k;
-        if (f < 4) cp_async(&S.tile[sl][f][h], static_cast<const TI*>(a.X[f]) + o);
-        else cp_async8(&S.ptile[sl][f - 4][h], (f == 4 ? a.p_dyn : a.p_hydro) + o);
+    const unsigned bar = smem_u32(&S.bar[sl]);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                 ::"r"(bar), "r"((unsigned)(4 * Box3<TI>::BYTES + 2 * Box3<double>::BYTES)) : "memory");
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        const CUtensorMap* map = f < 4 ? &M.x[f] : &M.p[f - 4];
+        const unsigned dst = f < 4 ? smem_u32(S.tile[sl][f]) : smem_u32(S.ptile[sl][f - 4]);
+        const int x = k0 - (f < 4 ? Box3<TI>::OX : Box3<double>::OX);
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];\n"
+            ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(j0 - 1), "r"(i),
+              "r"(bar) : "memory");
     }
+}
+
+// Wait for slot sl's copies (phase parity par), at most TMA_SPIN polls; false when they did not
+// arrive (the block then abandons the stage and poisons its cells).
+constexpr int TMA_SPIN = 1 << 22;
+__device__ __forceinline__ bool wait_boxes(const unsigned long long* bar, unsigned par) {
+    const unsigned a = smem_u32(bar);
+    for (int n = 0; n < TMA_SPIN; n++) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(ok) : "r"(a), "r"(par) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// The ring of km-1 meridians: the box's column of k = -1 (left tile) takes k = km-2, and the
+// column of k = km-1 (the tile holding km-2) takes k = 0. Patch thread t < 54 of the left tile, or
+// 64 <= t < 118 of the right, owns field (t mod 64) / 9, row (t mod 64) % 9 of that column:
+// wrap_src reads its value from global memory, wrap_put stores it into the landed box.
+__device__ __forceinline__ int wrap_role(int tid, int k0, const StageConst& q) {
+    const int t = tid & 63;
+    if (t >= 54) return -1;
+    if (tid < 64) return k0 == 0 ? t : -1;
+    if (tid < 128) return (k0 + TK >= q.km - 1) ? 64 + t : -1;
+    return -1;
+}
+template <typename TI>
+__device__ __forceinline__ double wrap_src(const StagePtrs& a, const StageConst& q, int role, int i,
+                                           int j0) {
+    const int t = role & 63, f = t / 9, r = t % 9;
+    int j = j0 - 1 + r;
+    j = j < 0 ? 0 : (j > q.jm - 1 ? q.jm - 1 : j);
+    const size_t o = ((size_t)i * q.jm + j) * q.KP + (role < 64 ? q.km - 2 : 0);
+    if (f < 4) return (double)static_cast<const TI*>(a.X[f])[o];
+    return (f == 4 ? a.p_dyn : a.p_hydro)[o];
+}
+template <typename TI, typename TA>
+__device__ __forceinline__ void wrap_put(StageSmem<TI, TA>& S, const StageConst& q, int role,
+                                         int i, int k0, double v) {
+    const int t = role & 63, f = t / 9, r = t % 9, sl = i % 3;
+    if (f < 4) {
+        const int col = role < 64 ? Box3<TI>::OX - 1 : Box3<TI>::OX + (q.km - 1 - k0);
+        S.tile[sl][f][r * Box3<TI>::W + col] = (TI)v;
+    } else {
+        const int col = role < 64 ? Box3<double>::OX - 1 : Box3<double>::OX + (q.km - 1 - k0);
+        S.ptile[sl][f - 4][r * Box3<double>::W + col] = v;
+    }
+}
+
+// p_stat at the cells of plane i into ring slot i % 3
+template <typename TI, typename TA>
+__device__ __forceinline__ void issue_ps(StageSmem<TI, TA>& S, const StagePtrs& a,
+                                         const StageConst& q, int i, int j0, int k0, int tid) {
     if (tid < NL) {
         const int tx = tid % TK, ty = tid / TK;
         const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
-        cp_async8(&S.ps[sl][tid], a.p_stat + base + (size_t)j * q.KP + k);
+        cp_async8(&S.ps[i % 3][tid], a.p_stat + (size_t)i * q.jm * q.KP + (size_t)j * q.KP + k);
     }
 }
 
@@ -181,8 +270,8 @@ __device__ __forceinline__ void issue_extra(StageSmem<TI, TA>& S, const StagePtr
 // update y_n + dt/6 acc from the FP64 time-level-n state, and the projection source aux.
 template <typename TI, typename TO, typename TA, typename R>
 __global__ void __launch_bounds__(NT, 2)
-rk_stage_kernel(StagePtrs a, StageConst q) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+rk_stage_kernel(StagePtrs a, StageConst q, const __grid_constant__ StageMaps M) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     StageSmem<TI, TA>& S = *reinterpret_cast<StageSmem<TI, TA>*>(smem_raw);
     const int tid = threadIdx.x;
     const int tx = tid % TK, ty = tid / TK;
@@ -190,27 +279,78 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
     const int k = k0 + tx, j = j0 + ty;
     const bool live = (tid < NL) && (k <= q.km - 2) && (j < q.jm);
     const size_t row = (size_t)q.KP, plane = (size_t)q.jm * row;
-    const int h = (ty + 1) * HK + (tx + 1);           // this cell in the halo tile
+    constexpr int WT = Box3<TI>::W, WP = Box3<double>::W;   // row pitch of the boxes
+    const int hT = (ty + 1) * WT + (tx + Box3<TI>::OX);      // this cell in a stage-input box
+    const int hP = (ty + 1) * WP + (tx + Box3<double>::OX);  // this cell in a pressure box
     // radial chunk [i_lo, i_hi); the march starts one plane below to fill the radial window
     const int per = (q.im + NCH - 1) / NCH;
     const int i_lo = blockIdx.z * per, i_hi = min(q.im, i_lo + per);
     const int i_st = (i_lo > 0) ? i_lo - 1 : 0;
+    const int role = wrap_role(tid, k0, q);
 
-    issue_tile(S, a, q, i_st, j0, k0, tid);
+    if (tid == 0) {
+        for (int sl = 0; sl < 3; sl++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.bar[sl])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    unsigned pend = 0, par = 0;   // per ring slot: boxes in flight; the parity of their phase
+    if (tid == 0) {
+        issue_boxes(S, M, i_st, j0, k0);
+        if (i_st + 1 < q.im) issue_boxes(S, M, i_st + 1, j0, k0);
+    }
+    pend |= 1u << (i_st % 3);
+    if (i_st + 1 < q.im) pend |= 1u << ((i_st + 1) % 3);
+    issue_ps(S, a, q, i_st, j0, k0, tid);
     issue_extra(S, a, q, i_st, j0, k0, tid);
     cp_commit();
-    if (i_st + 1 < q.im) issue_tile(S, a, q, i_st + 1, j0, k0, tid);
+    if (i_st + 1 < q.im) issue_ps(S, a, q, i_st + 1, j0, k0, tid);
     cp_commit();
+    double wnext = 0.0;           // a seam thread's value for the next plane to land
 
     // radial window: the cell's values in plane i-1 (t, u, v, w, p_dyn, p_stat)
     double m_t = 0.0, m_u = 0.0, m_v = 0.0, m_w = 0.0, m_pd = 0.0, m_ps = 0.0;
 
     for (int i = i_st; i < i_hi; i++) {
-        if (i + 2 < q.im && i + 2 <= i_hi) issue_tile(S, a, q, i + 2, j0, k0, tid);
+        const bool next2 = i + 2 < q.im && i + 2 <= i_hi;
+        if (next2) {
+            if (tid == 0) issue_boxes(S, M, i + 2, j0, k0);
+            pend |= 1u << ((i + 2) % 3);
+            issue_ps(S, a, q, i + 2, j0, k0, tid);
+        }
         if (i + 1 < i_hi) issue_extra(S, a, q, i + 1, j0, k0, tid);
         cp_commit();
         cp_wait1();
-        __syncthreads();
+        // the boxes of planes i and i+1 not waited for yet, then their seam columns (planes
+        // i_st and i_st + 1 read directly, later ones prefetched a plane ahead)
+        bool lost = false;
+        for (int p = i; p <= i + 1; p++) {
+            const int sl = p % 3;
+            if (!(pend >> sl & 1u)) continue;
+            if (!wait_boxes(&S.bar[sl], par >> sl & 1u)) lost = true;
+            pend &= ~(1u << sl);
+            par ^= 1u << sl;
+            if (role >= 0 && !lost) {
+                wrap_put(S, q, role, p, k0, p <= i_st + 1 ? wrap_src<TI>(a, q, role, p, j0) : wnext);
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            }
+        }
+        if (role >= 0 && next2) wnext = wrap_src<TI>(a, q, role, i + 2, j0);
+        if (__syncthreads_or(lost)) {
+            // the boxes still in flight (each wait bounded), then every cell of the chunk NaN
+            for (int sl = 0; sl < 3; sl++)
+                if (pend >> sl & 1u) wait_boxes(&S.bar[sl], par >> sl & 1u);
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            if (live)
+                for (int ip = i_lo; ip < i_hi; ip++) {
+                    const size_t c = (size_t)ip * plane + (size_t)j * row + k;
+                    for (int f = 0; f < 4; f++) {
+                        if (q.stage < 3) static_cast<TO*>(a.Xo[f])[c] = (TO)__longlong_as_double(0x7ff8000000000000LL);
+                        else a.Y[f][c] = __longlong_as_double(0x7ff8000000000000LL);
+                    }
+                }
+            return;
+        }
 
         const int cs = i % 3, ns = (i + 1) % 3, xs = i & 1;
         const TI* Tt = S.tile[cs][0];
@@ -232,20 +372,20 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 }
             } else {
                 const GeoIJ& g = S.geo[xs][ty];
-                const R t0 = (R)Tt[h], u0 = (R)Ut[h], v0 = (R)Vt[h];
-                const R w0 = (R)Wt[h];
+                const R t0 = (R)Tt[hT], u0 = (R)Ut[hT], v0 = (R)Vt[hT];
+                const R w0 = (R)Wt[hT];
                 const TI* Tn = S.tile[ns][0];
                 const TI* Un = S.tile[ns][1];
                 const TI* Vn = S.tile[ns][2];
                 const TI* Wn = S.tile[ns][3];
                 // first and second centred differences (RHS_Jup_Turb.cpp:180-254); exp_rm = 1
 #define DERIVS(F, FN, FM, f0, d1r, d2r, d1t, d2t, d1p, d2p)                           \
-    const R d1r = ((R)FN[h] - (R)FM) * (R)q.inv_2dr;                                  \
-    const R d2r = ((R)FN[h] - (R)2.0 * f0 + (R)FM) * (R)q.inv_dr2;                    \
-    const R d1t = ((R)F[h + HK] - (R)F[h - HK]) * (R)q.inv_2dthe;                     \
-    const R d2t = ((R)F[h + HK] - (R)2.0 * f0 + (R)F[h - HK]) * (R)q.inv_dthe2;       \
-    const R d1p = ((R)F[h + 1] - (R)F[h - 1]) * (R)q.inv_2dphi;                       \
-    const R d2p = ((R)F[h + 1] - (R)2.0 * f0 + (R)F[h - 1]) * (R)q.inv_dphi2;
+    const R d1r = ((R)FN[hT] - (R)FM) * (R)q.inv_2dr;                                 \
+    const R d2r = ((R)FN[hT] - (R)2.0 * f0 + (R)FM) * (R)q.inv_dr2;                   \
+    const R d1t = ((R)F[hT + WT] - (R)F[hT - WT]) * (R)q.inv_2dthe;                   \
+    const R d2t = ((R)F[hT + WT] - (R)2.0 * f0 + (R)F[hT - WT]) * (R)q.inv_dthe2;     \
+    const R d1p = ((R)F[hT + 1] - (R)F[hT - 1]) * (R)q.inv_2dphi;                     \
+    const R d2p = ((R)F[hT + 1] - (R)2.0 * f0 + (R)F[hT - 1]) * (R)q.inv_dphi2;
                 DERIVS(Tt, Tn, m_t, t0, dtdr, d2tdr2, dtdthe, d2tdthe2, dtdphi, d2tdphi2)
                 DERIVS(Ut, Un, m_u, u0, dudr, d2udr2, dudthe, d2udthe2, dudphi, d2udphi2)
                 DERIVS(Vt, Vn, m_v, v0, dvdr, d2vdr2, dvdthe, d2vdthe2, dvdphi, d2vdphi2)
@@ -253,13 +393,13 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
 #undef DERIVS
                 // pressure gradients, solid faces mirrored to the local value (RHS_Jup_Turb.cpp:119-130)
                 const bool wall = q.pgrad_wall;
-                const double pc = Pt[h];
-                const double pip = (wall && (nbm & NB_IP)) ? pc : S.ptile[ns][0][h];
+                const double pc = Pt[hP];
+                const double pip = (wall && (nbm & NB_IP)) ? pc : S.ptile[ns][0][hP];
                 const double pim = (wall && (nbm & NB_IM)) ? pc : m_pd;
-                const double pjp = (wall && (nbm & NB_JP)) ? pc : Pt[h + HK];
-                const double pjm = (wall && (nbm & NB_JM)) ? pc : Pt[h - HK];
-                const double pkp = (wall && (nbm & NB_KP)) ? pc : Pt[h + 1];
-                const double pkm = (wall && (nbm & NB_KM)) ? pc : Pt[h - 1];
+                const double pjp = (wall && (nbm & NB_JP)) ? pc : Pt[hP + WP];
+                const double pjm = (wall && (nbm & NB_JM)) ? pc : Pt[hP - WP];
+                const double pkp = (wall && (nbm & NB_KP)) ? pc : Pt[hP + 1];
+                const double pkm = (wall && (nbm & NB_KM)) ? pc : Pt[hP - 1];
                 const R dpdr = (R)((pip - pim) * q.inv_2dr);
                 const R dpdthe = (R)((pjp - pjm) * q.inv_2dthe);
                 const R dpdphi = (R)((pkp - pkm) * q.inv_2dphi);
@@ -317,11 +457,11 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 const R dpdphi_term = (R)q.pgrad_scale * dpdphi * (R)g.inv_rmsinthe;
                 R dphdthe_term = (R)0.0, dphdphi_term = (R)0.0;
                 if (q.use_hp) {
-                    const double hc = Ht[h];
-                    const double hjp = (wall && (nbm & NB_JP)) ? hc : Ht[h + HK];
-                    const double hjm = (wall && (nbm & NB_JM)) ? hc : Ht[h - HK];
-                    const double hkp = (wall && (nbm & NB_KP)) ? hc : Ht[h + 1];
-                    const double hkm = (wall && (nbm & NB_KM)) ? hc : Ht[h - 1];
+                    const double hc = Ht[hP];
+                    const double hjp = (wall && (nbm & NB_JP)) ? hc : Ht[hP + WP];
+                    const double hjm = (wall && (nbm & NB_JM)) ? hc : Ht[hP - WP];
+                    const double hkp = (wall && (nbm & NB_KP)) ? hc : Ht[hP + 1];
+                    const double hkm = (wall && (nbm & NB_KM)) ? hc : Ht[hP - 1];
                     dphdthe_term = (R)((hjp - hjm) * q.inv_2dthe) * (R)g.inv_rm;
                     dphdphi_term = (R)((hkp - hkm) * q.inv_2dphi) * (R)g.inv_rmsinthe;
                 }
@@ -382,7 +522,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 // accumulate (RungeKutta_Jup_Turb.cpp:419-490), form the next stage input / result
                 const R rhs[4] = {rhs_t, rhs_u, rhs_v, rhs_w};
                 if (q.stage == 0) {
-                    const double y0[4] = {(double)Tt[h], (double)Ut[h], (double)Vt[h], (double)Wt[h]};
+                    const double y0[4] = {(double)Tt[hT], (double)Ut[hT], (double)Vt[hT], (double)Wt[hT]};
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
                         if (!q.acc_free) static_cast<TA*>(a.acc[f])[c] = (TA)((R)q.wgt * rhs[f]);
@@ -391,7 +531,7 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
                 } else if (q.acc_free && q.stage < 3) {
                     // acc_free (FP64): stage 1 only forms X2; stage 2 forms X3 and the accumulator
                     // k1 + 2 k2 + 2 k3 with k1 = (X1 - y_n) / c, k2 = (X2 - y_n) / c
-                    const double x2[4] = {(double)Tt[h], (double)Ut[h], (double)Vt[h], (double)Wt[h]};
+                    const double x2[4] = {(double)Tt[hT], (double)Ut[hT], (double)Vt[hT], (double)Wt[hT]};
 #pragma unroll
                     for (int f = 0; f < 4; f++) {
                         const double yn = S.Yx[xs][f][tid];
@@ -422,8 +562,8 @@ rk_stage_kernel(StagePtrs a, StageConst q) {
             }
         }
         if (live) {   // slide the radial window up one plane
-            m_t = (double)Tt[h]; m_u = (double)Ut[h]; m_v = (double)Vt[h]; m_w = (double)Wt[h];
-            m_pd = Pt[h];
+            m_t = (double)Tt[hT]; m_u = (double)Ut[hT]; m_v = (double)Vt[hT]; m_w = (double)Wt[hT];
+            m_pd = Pt[hP];
             m_ps = S.ps[cs][tid];
         }
         __syncthreads();
@@ -554,6 +694,58 @@ int launch_hydrostatic(AtjupCtx* c, const double* v, const double* w) {
     return ATJUP_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (the library does not
+// link against the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult qr{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                             &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// a [im][jm][KP] array of T as a 3-D tensor (x = k, y = j, z = i) read in boxes of
+// Box3<T>::W x HJ x 1; the rows (KP T) and planes are multiples of 16 bytes
+template <typename T>
+static int make_box_map(CUtensorMap* m, const void* base, const AtjupCtx* c) {
+    const EncodeTiled enc = encode_tiled();
+    if (!enc) {
+        set_error("rk_stage: cuTensorMapEncodeTiled is not available");
+        return ATJUP_ERR_CUDA;
+    }
+    if (!base || reinterpret_cast<uintptr_t>(base) % 16) {
+        set_error("rk_stage: a stage buffer is null or not 16-byte aligned");
+        return ATJUP_ERR_ARG;
+    }
+    const AtjupParams& P = c->P;
+    const cuuint64_t dim[3] = {(cuuint64_t)c->KP, (cuuint64_t)P.jm, (cuuint64_t)P.im};
+    const cuuint64_t stride[2] = {(cuuint64_t)c->KP * sizeof(T), (cuuint64_t)P.jm * c->KP * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)Box3<T>::W, (cuuint32_t)HJ, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = enc(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                           3u, const_cast<void*>(base), dim, stride, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("rk_stage: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        return ATJUP_ERR_CUDA;
+    }
+    return ATJUP_OK;
+}
+
 template <typename TI, typename TO, typename TA, typename R>
 static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, const char* name) {
     const AtjupParams& P = c->P;
@@ -564,9 +756,14 @@ static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, 
                                         (int)sizeof(StageSmem<TI, TA>)));
         attr_set = true;
     }
+    StageMaps M;
+    for (int f = 0; f < 4; f++)
+        if (int rc = make_box_map<TI>(&M.x[f], a.X[f], c)) return rc;
+    if (int rc = make_box_map<double>(&M.p[0], a.p_dyn, c)) return rc;
+    if (int rc = make_box_map<double>(&M.p[1], a.p_hydro, c)) return rc;
     dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
     c->launches++;
-    rk_stage_kernel<TI, TO, TA, R><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q);
+    rk_stage_kernel<TI, TO, TA, R><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q, M);
     ATJUP_CHECK_LAUNCH(name);
     return ATJUP_OK;
 }

@@ -230,7 +230,8 @@ int atjup_gpu_rk4_step(AtjupCtx* ctx, int32_t iter_n);
  * stage-major X1 t, u, v, w, X2 .., X3 ..) every following RK step writes its stage inputs there
  * instead of the context's own buffers, so that they outlive the step as the adjoint's checkpoint
  * (atjup_gpu_iteration_adjoint_ckpt); NULL returns to the context's buffers. No counterpart in the
- * reference. ATJUP_ERR_UNSUPPORTED with the physics block or the mixed step. */
+ * reference. Each buffer 16-byte aligned (ATJUP_ERR_ARG otherwise: the stage kernel reads its
+ * input through tensor maps). ATJUP_ERR_UNSUPPORTED with the physics block or the mixed step. */
 int atjup_gpu_set_stage_buffers(AtjupCtx* ctx, double* const bufs[12]);
 
 /* PressureSolverJup::run (PressureSolver.h:144-766) incl. prepareProjectionBoundaries
