@@ -13,6 +13,8 @@
 
 #include <cuda.h>
 
+#include <cstring>
+
 namespace atjup {
 namespace {
 
@@ -84,25 +86,38 @@ struct Box3 {
     static constexpr int PAD = (BYTES + 127) / 128 * 128 / (int)sizeof(T);
 };
 
-// the tensor maps of the stage input's four fields and of p_dyn, p_hydro: [im][jm][KP] arrays,
-// boxes of Box3<T>::W x HJ x 1
+// The per-cell inputs (no halo) are boxes of TK x TJ x 1 at (k0, j0, i): their shared-memory
+// layout [TJ][TK] is the block's thread order, and k0 (a multiple of 36) is a 16-byte boundary.
+template <typename T>
+struct CellBox {
+    static constexpr int BYTES = TK * TJ * (int)sizeof(T);
+};
+
+// The tensor maps of one launch, all over [im][jm][KP] arrays: the stage input's four fields and
+// p_dyn, p_hydro (halo boxes), and the per-cell inputs (cell boxes; only those the stage reads are
+// encoded)
 struct __align__(64) StageMaps {
     CUtensorMap x[4];
     CUtensorMap p[2];
+    CUtensorMap ps;            // p_stat
+    CUtensorMap y[4];          // time-level-n t, u, v, w (stages 1-3)
+    CUtensorMap ax[4];         // the accumulator, or X1 at stage 2 of the FP64 step
+    CUtensorMap ex[NX];        // rho, wall_nue, nue, Q_rad, Q_precip
 };
 
 template <typename TI, typename TA>
 struct __align__(128) StageSmem {
     TI tile[3][4][Box3<TI>::PAD];            // stage input t, u, v, w of planes i, i+1, i+2
     double ptile[3][2][Box3<double>::PAD];   // p_dyn, p_hydro of the same planes
-    unsigned long long bar[4];               // the TMA barrier of each ring slot (three used)
     double ps[3][NT];         // p_stat at the cells of the same three planes
     double Yx[2][4][NT];      // time-level-n t, u, v, w of planes i and i+1 (stages 1-3)
     double ex[2][NX][NT];     // FP64 per-cell inputs of planes i and i+1
+    TA ax[2][4][NT];          // accumulators of planes i and i+1 (stages 1-3)
     GeoIJ geo[2][TJ];         // geometry rows of planes i and i+1
     double cm[2][2][TJ];      // cell-hold means (v, u) of planes i and i+1
-    TA ax[2][4][NT];          // accumulators of planes i and i+1 (stages 1-3)
     uint8_t nb[2][NT];        // per-cell flags of planes i and i+1
+    unsigned long long bar[4];    // the barrier of each halo ring slot (three used)
+    unsigned long long barx[2];   // the barrier of each per-cell slot
 };
 // two blocks per SM: 228 KB of shared memory per SM, 1 KB of it reserved per block
 static_assert(2 * (sizeof(StageSmem<double, double>) + 1024) <= 233472, "two FP64 stage blocks per SM");
@@ -129,27 +144,63 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
 }
 
-// One thread: the tensor copies of plane i's six halo boxes into ring slot i % 3, their bytes
-// expected on the slot's barrier. The fence orders the block's earlier plain writes to the slot
-// (the seam patches) before the copies' writes.
+// one tensor copy of the box at (x, y, z) of map into dst, counted on the barrier bar
+__device__ __forceinline__ void tma3(void* dst, const CUtensorMap* map, unsigned bar, int x, int y,
+                                     int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z),
+          "r"(bar) : "memory");
+}
+__device__ __forceinline__ void expect_bytes(unsigned bar, unsigned bytes) {
+    // the fence orders the block's earlier plain writes to the slot (the seam patches) before the
+    // copies' writes
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+// One thread: the tensor copies of plane i's six halo boxes and its p_stat into ring slot i % 3,
+// their bytes expected on the slot's barrier.
 template <typename TI, typename TA>
 __device__ __forceinline__ void issue_boxes(StageSmem<TI, TA>& S, const StageMaps& M, int i,
                                             int j0, int k0) {
     const int sl = i % 3;
     const unsigned bar = smem_u32(&S.bar[sl]);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
-                 ::"r"(bar), "r"((unsigned)(4 * Box3<TI>::BYTES + 2 * Box3<double>::BYTES)) : "memory");
+    expect_bytes(bar, 4 * Box3<TI>::BYTES + 2 * Box3<double>::BYTES + CellBox<double>::BYTES);
 #pragma unroll
-    for (int f = 0; f < 6; f++) {
-        const CUtensorMap* map = f < 4 ? &M.x[f] : &M.p[f - 4];
-        const unsigned dst = f < 4 ? smem_u32(S.tile[sl][f]) : smem_u32(S.ptile[sl][f - 4]);
-        const int x = k0 - (f < 4 ? Box3<TI>::OX : Box3<double>::OX);
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
-            "[%0], [%1, {%2, %3, %4}], [%5];\n"
-            ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(j0 - 1), "r"(i),
-              "r"(bar) : "memory");
+    for (int f = 0; f < 4; f++) tma3(S.tile[sl][f], &M.x[f], bar, k0 - Box3<TI>::OX, j0 - 1, i);
+#pragma unroll
+    for (int f = 0; f < 2; f++) tma3(S.ptile[sl][f], &M.p[f], bar, k0 - Box3<double>::OX, j0 - 1, i);
+    tma3(S.ps[sl], &M.ps, bar, k0, j0, i);
+}
+
+// One thread: the tensor copies of plane i's per-cell inputs into slot i % 2 (the time-level-n
+// state and the accumulator or X1 where the stage reads them, rho, wall_nue, and nue and the
+// heating rates when present).
+template <typename TI, typename TA>
+__device__ __forceinline__ void issue_cells(StageSmem<TI, TA>& S, const StageMaps& M,
+                                            const StageConst& q, int i, int j0, int k0) {
+    const int sl = i & 1;
+    const unsigned bar = smem_u32(&S.barx[sl]);
+    const bool need_y = q.stage > 0, need_ax = q.stage > 0 && (!q.acc_free || q.stage >= 2);
+    unsigned bytes = 2 * CellBox<double>::BYTES;
+    if (need_y) bytes += 4 * CellBox<double>::BYTES;
+    if (need_ax) bytes += 4 * CellBox<TA>::BYTES;
+    if (q.has_nue) bytes += CellBox<double>::BYTES;
+    if (q.has_heating) bytes += 2 * CellBox<double>::BYTES;
+    expect_bytes(bar, bytes);
+    if (need_y)
+        for (int f = 0; f < 4; f++) tma3(S.Yx[sl][f], &M.y[f], bar, k0, j0, i);
+    if (need_ax)
+        for (int f = 0; f < 4; f++) tma3(S.ax[sl][f], &M.ax[f], bar, k0, j0, i);
+    tma3(S.ex[sl][0], &M.ex[0], bar, k0, j0, i);
+    tma3(S.ex[sl][1], &M.ex[1], bar, k0, j0, i);
+    if (q.has_nue) tma3(S.ex[sl][2], &M.ex[2], bar, k0, j0, i);
+    if (q.has_heating) {
+        tma3(S.ex[sl][3], &M.ex[3], bar, k0, j0, i);
+        tma3(S.ex[sl][4], &M.ex[4], bar, k0, j0, i);
     }
 }
 
@@ -201,44 +252,12 @@ __device__ __forceinline__ void wrap_put(StageSmem<TI, TA>& S, const StageConst&
     }
 }
 
-// p_stat at the cells of plane i into ring slot i % 3
-template <typename TI, typename TA>
-__device__ __forceinline__ void issue_ps(StageSmem<TI, TA>& S, const StagePtrs& a,
-                                         const StageConst& q, int i, int j0, int k0, int tid) {
-    if (tid < NL) {
-        const int tx = tid % TK, ty = tid / TK;
-        const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
-        cp_async8(&S.ps[i % 3][tid], a.p_stat + (size_t)i * q.jm * q.KP + (size_t)j * q.KP + k);
-    }
-}
-
-// Issue the copies of plane i's per-cell inputs, geometry rows and cell means into slot i % 2.
+// Issue the copies of plane i's flags, geometry rows and cell means into slot i % 2 (small, or
+// bytes whose rows do not start on 16-byte boundaries: plain asynchronous copies).
 template <typename TI, typename TA>
 __device__ __forceinline__ void issue_extra(StageSmem<TI, TA>& S, const StagePtrs& a,
                                             const StageConst& q, int i, int j0, int k0, int tid) {
     const int sl = i & 1;
-    if (tid < NL) {
-        const int tx = tid % TK, ty = tid / TK;
-        const int j = min(j0 + ty, q.jm - 1), k = min(k0 + tx, q.km - 2);
-        const size_t c = ((size_t)i * q.jm + j) * q.KP + k;
-        if (q.stage > 0) {
-            // the per-cell accumulator, or with acc_free X1 at stage 2 and the accumulator at 3
-            const bool need_ax = !q.acc_free || q.stage >= 2;
-            const void* const* src = (q.acc_free && q.stage == 2) ? a.X1 : (const void* const*)a.acc;
-#pragma unroll
-            for (int f = 0; f < 4; f++) {
-                cp_async8(&S.Yx[sl][f][tid], a.Y[f] + c);
-                if (need_ax) cp_async(&S.ax[sl][f][tid], static_cast<const TA*>(src[f]) + c);
-            }
-        }
-        cp_async8(&S.ex[sl][0][tid], a.rho + c);
-        cp_async8(&S.ex[sl][1][tid], a.wall_nue + c);
-        if (q.has_nue) cp_async8(&S.ex[sl][2][tid], a.nue + c);
-        if (q.has_heating) {
-            cp_async8(&S.ex[sl][3][tid], a.Q_rad + c);
-            cp_async8(&S.ex[sl][4][tid], a.Q_precip + c);
-        }
-    }
     // flags: 4 bytes per copy along a tile row (k0 and the row pitch are multiples of 4)
     if (tid < TJ * (TK / 4) && k0 + 4 * (tid % (TK / 4)) <= q.km - 2) {
         const int ty = tid / (TK / 4), kq = tid % (TK / 4);
@@ -291,20 +310,23 @@ rk_stage_kernel(StagePtrs a, StageConst q, const __grid_constant__ StageMaps M) 
     if (tid == 0) {
         for (int sl = 0; sl < 3; sl++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.bar[sl])) : "memory");
+        for (int sl = 0; sl < 2; sl++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.barx[sl])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
-    unsigned pend = 0, par = 0;   // per ring slot: boxes in flight; the parity of their phase
+    // per ring slot: copies in flight, and the parity of their phase (halo ring, per-cell ring)
+    unsigned pend = 0, par = 0, pendx = 0, parx = 0;
     if (tid == 0) {
         issue_boxes(S, M, i_st, j0, k0);
         if (i_st + 1 < q.im) issue_boxes(S, M, i_st + 1, j0, k0);
+        issue_cells(S, M, q, i_st, j0, k0);
     }
     pend |= 1u << (i_st % 3);
     if (i_st + 1 < q.im) pend |= 1u << ((i_st + 1) % 3);
-    issue_ps(S, a, q, i_st, j0, k0, tid);
+    pendx |= 1u << (i_st & 1);
     issue_extra(S, a, q, i_st, j0, k0, tid);
     cp_commit();
-    if (i_st + 1 < q.im) issue_ps(S, a, q, i_st + 1, j0, k0, tid);
     cp_commit();
     double wnext = 0.0;           // a seam thread's value for the next plane to land
 
@@ -316,9 +338,12 @@ rk_stage_kernel(StagePtrs a, StageConst q, const __grid_constant__ StageMaps M) 
         if (next2) {
             if (tid == 0) issue_boxes(S, M, i + 2, j0, k0);
             pend |= 1u << ((i + 2) % 3);
-            issue_ps(S, a, q, i + 2, j0, k0, tid);
         }
-        if (i + 1 < i_hi) issue_extra(S, a, q, i + 1, j0, k0, tid);
+        if (i + 1 < i_hi) {
+            if (tid == 0) issue_cells(S, M, q, i + 1, j0, k0);
+            pendx |= 1u << ((i + 1) & 1);
+            issue_extra(S, a, q, i + 1, j0, k0, tid);
+        }
         cp_commit();
         cp_wait1();
         // the boxes of planes i and i+1 not waited for yet, then their seam columns (planes
@@ -336,10 +361,18 @@ rk_stage_kernel(StagePtrs a, StageConst q, const __grid_constant__ StageMaps M) 
             }
         }
         if (role >= 0 && next2) wnext = wrap_src<TI>(a, q, role, i + 2, j0);
+        // plane i's per-cell boxes
+        if (pendx >> (i & 1) & 1u) {
+            if (!wait_boxes(&S.barx[i & 1], parx >> (i & 1) & 1u)) lost = true;
+            pendx &= ~(1u << (i & 1));
+            parx ^= 1u << (i & 1);
+        }
         if (__syncthreads_or(lost)) {
-            // the boxes still in flight (each wait bounded), then every cell of the chunk NaN
+            // the copies still in flight (each wait bounded), then every cell of the chunk NaN
             for (int sl = 0; sl < 3; sl++)
                 if (pend >> sl & 1u) wait_boxes(&S.bar[sl], par >> sl & 1u);
+            for (int sl = 0; sl < 2; sl++)
+                if (pendx >> sl & 1u) wait_boxes(&S.barx[sl], parx >> sl & 1u);
             asm volatile("cp.async.wait_all;\n" ::: "memory");
             if (live)
                 for (int ip = i_lo; ip < i_hi; ip++) {
@@ -717,10 +750,12 @@ static EncodeTiled encode_tiled() {
     return fn;
 }
 
-// a [im][jm][KP] array of T as a 3-D tensor (x = k, y = j, z = i) read in boxes of
-// Box3<T>::W x HJ x 1; the rows (KP T) and planes are multiples of 16 bytes
+// a [im][jm][KP] array of T as a 3-D tensor (x = k, y = j, z = i) read in boxes of bw x bh x 1
+// (halo boxes Box3<T>::W x HJ, cell boxes TK x TJ); the rows (KP T) and planes are multiples of
+// 16 bytes
 template <typename T>
-static int make_box_map(CUtensorMap* m, const void* base, const AtjupCtx* c) {
+static int make_box_map(CUtensorMap* m, const void* base, const AtjupCtx* c, int bw = Box3<T>::W,
+                        int bh = HJ) {
     const EncodeTiled enc = encode_tiled();
     if (!enc) {
         set_error("rk_stage: cuTensorMapEncodeTiled is not available");
@@ -733,7 +768,7 @@ static int make_box_map(CUtensorMap* m, const void* base, const AtjupCtx* c) {
     const AtjupParams& P = c->P;
     const cuuint64_t dim[3] = {(cuuint64_t)c->KP, (cuuint64_t)P.jm, (cuuint64_t)P.im};
     const cuuint64_t stride[2] = {(cuuint64_t)c->KP * sizeof(T), (cuuint64_t)P.jm * c->KP * sizeof(T)};
-    const cuuint32_t box[3] = {(cuuint32_t)Box3<T>::W, (cuuint32_t)HJ, 1u};
+    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1u};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
     const CUresult r = enc(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                            3u, const_cast<void*>(base), dim, stride, box, estr,
@@ -757,10 +792,27 @@ static int launch_stage_t(AtjupCtx* c, const StagePtrs& a, const StageConst& q, 
         attr_set = true;
     }
     StageMaps M;
+    memset(&M, 0, sizeof M);
     for (int f = 0; f < 4; f++)
         if (int rc = make_box_map<TI>(&M.x[f], a.X[f], c)) return rc;
     if (int rc = make_box_map<double>(&M.p[0], a.p_dyn, c)) return rc;
     if (int rc = make_box_map<double>(&M.p[1], a.p_hydro, c)) return rc;
+    // the per-cell inputs the stage reads (issue_cells reads the same conditions)
+    if (int rc = make_box_map<double>(&M.ps, a.p_stat, c, TK, TJ)) return rc;
+    const double* ex[NX] = {a.rho, a.wall_nue, a.nue, a.Q_rad, a.Q_precip};
+    for (int e = 0; e < NX; e++) {
+        if ((e == 2 && !q.has_nue) || (e >= 3 && !q.has_heating)) continue;
+        if (int rc = make_box_map<double>(&M.ex[e], ex[e], c, TK, TJ)) return rc;
+    }
+    if (q.stage > 0) {
+        const bool need_ax = !q.acc_free || q.stage >= 2;
+        const void* const* src = (q.acc_free && q.stage == 2) ? a.X1 : (const void* const*)a.acc;
+        for (int f = 0; f < 4; f++) {
+            if (int rc = make_box_map<double>(&M.y[f], a.Y[f], c, TK, TJ)) return rc;
+            if (need_ax)
+                if (int rc = make_box_map<TA>(&M.ax[f], src[f], c, TK, TJ)) return rc;
+        }
+    }
     dim3 grid((P.km - 1 + TK - 1) / TK, (P.jm + TJ - 1) / TJ, NCH);
     c->launches++;
     rk_stage_kernel<TI, TO, TA, R><<<grid, NT, sizeof(StageSmem<TI, TA>), c->stream>>>(a, q, M);
