@@ -8,7 +8,9 @@
 // n state Y and the accumulator at the cell, and writes X_{s+1} and the accumulator; stage 3
 // writes Y itself. Non-integrated cells (radial walls, the three rows next to each pole, the
 // seam copy k = km-1, solid cells) keep their start-of-step values: stages 0-2 copy Y into
-// X_{s+1} there, which is what the reference's untouched live fields hold.
+// X_{s+1} there, which is what the reference's untouched live fields hold. The stage kernel
+// marches a tile of columns up through the radial planes; each plane's inputs reach shared memory
+// two planes ahead as tensor-memory-accelerator copies (cp.async.bulk.tensor on mbarriers).
 #include "ctx.cuh"
 
 #include <cuda.h>
@@ -129,11 +131,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-template <typename T>
-__device__ __forceinline__ void cp_async(T* smem, const T* gmem) {
-    if constexpr (sizeof(T) == 8) cp_async8(smem, gmem);
-    else cp_async4(smem, gmem);
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
