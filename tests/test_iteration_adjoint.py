@@ -111,6 +111,29 @@ def test_dot_product_per_pass(part, it):
     assert np.isfinite(lhs) and rel <= 1e-12
 
 
+def test_stage_buffers_must_be_aligned():
+    """The dynamics stage kernel reads its input through tensor maps, whose base must lie on a
+    16-byte boundary: atjup_gpu_set_stage_buffers refuses a buffer 8 bytes off one
+    (ATJUP_ERR_ARG = 1) and keeps the context's own buffers, so the next step leaves the offered
+    buffers untouched (NaN) and its own state finite."""
+    import ctypes
+
+    import torch
+    p, g, m = prepared((13, 37, 49), 83)
+    xs = m.state_tensors(LIN_FIELDS)
+    stages = [torch.full_like(xs[0], float("nan")) for _ in range(12)]
+    spare = torch.full((xs[0].numel() + 2,), float("nan"), dtype=torch.float64, device=xs[0].device)
+    ptrs = (ctypes.c_void_p * 12)(*[t.data_ptr() for t in stages])
+    ptrs[5] = spare.data_ptr() + 8
+    assert m.L.atjup_gpu_set_stage_buffers(m.ctx, ptrs) == 1
+    m.step(3, False)
+    m.synchronize()
+    assert all(bool(torch.isnan(t).all()) for t in stages)
+    assert bool(torch.isnan(spare).all())
+    assert m.nonfinite_count() == 0
+    m.close()
+
+
 @pytest.mark.parametrize("it", [2, 3], ids=["even", "odd"])
 def test_checkpointed_adjoint_equals_recomputed(it):
     """The adjoint that takes the forward step's own RK stage inputs as its checkpoint
